@@ -1,0 +1,1040 @@
+// CPU oracle for the TEASAR hot path of giorgioangel/brook (v0.1.0).
+//
+// TEST INFRASTRUCTURE ONLY. This file is a plain C++ restatement of the reference algorithm, used
+// by tests/, __graft_entry__.smoke() and bench.py's CPU baseline as the checker. The product
+// (brook_b200) never links, loads or calls it.
+//
+// Everything works on one label volume in Fortran order (x fastest), flat index
+// i = x + sx * (y + sy * z). Each function cites the reference file:line whose behaviour it
+// restates; the tie and rounding rules are the reference's, because its output is the parity target:
+//   * connected components: ids 1..K by ascending first flat index (ccl.cu:25-63, ccl_kernels.cuh:108-133)
+//   * EDT: float32 spacing accumulation along x, float64 lower envelope along y and z, float32
+//     storage, sqrt at the end (edt_kernels.cuh:15-144, edt.cu:12-15)
+//   * border targets (fix_borders): per face a 2D CC + 2D EDT, farthest pixel with the
+//     centroid/centre/corner/edge tie-break, ordered by first pixel, collected in a CPython set
+//     (borders.cu:53-116, point_set.hpp)
+//   * argmax ties -> lowest flat (batched_regular.inc:9-22)
+//   * DAF: 26-connected geometric distance with float32 weights (batched.cu:211-215)
+//   * PDRF: (1 - dbf * M)^(2^s) * scale + daf * inv, no FMA (batched_regular.inc:93-108)
+//   * target order: descending DAF (inf -> 0), ties -> higher flat first (lockstep_order.cu:21-45)
+//   * railroad: vertex-weighted SSSP with the one-ulp step, nearest rail by (dist, flat), warp
+//     backtrace rule (lowest neighbour index on ties) and the dijkstra3d join
+//     (common.cuh:113-127, lockstep_coop.inc:71-305, lockstep_regular.inc:61-155)
+//   * invalidation: claim-order flood in bands of the bottleneck distance, round-synchronous
+//     inside a band, pulls at band boundaries (invalidation_kernels.cuh:11-297)
+//   * assembly: unique vertices sorted by (x,y,z), edges (min,max) sorted unique, unused vertices
+//     dropped, radius = DBF (skeleton.cpp:13-40, assembly.cu:88-160)
+// Soma handling (dbf_max > soma_detection_threshold) is not restated: the oracle reports an
+// error for such objects.
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <numeric>
+#include <queue>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using i64 = int64_t;
+constexpr float kInf = std::numeric_limits<float>::infinity();
+
+// ---------------------------------------------------------------------------------------------
+// Neighbourhood tables. The reference fixes one 26-neighbour order for every kernel
+// (common.cuh:33-47): the six faces (-x,+x,-y,+y,-z,+z), then the xy, yz and xz edges, each pair
+// of signs in lexicographic order, then the eight corners lexicographic with z fastest. The
+// dijkstra3d order (common.cuh:63-76) differs only in the corners. Both are built here from
+// those rules.
+struct Tables {
+  int dx[26], dy[26], dz[26], opp[26], d3rank[26], d3inv[26];
+  Tables() {
+    int k = 0;
+    auto put = [&](int x, int y, int z) { dx[k] = x; dy[k] = y; dz[k] = z; ++k; };
+    put(-1, 0, 0); put(1, 0, 0); put(0, -1, 0); put(0, 1, 0); put(0, 0, -1); put(0, 0, 1);
+    for (int a : {-1, 1}) for (int b : {-1, 1}) put(a, b, 0);
+    for (int a : {-1, 1}) for (int b : {-1, 1}) put(0, a, b);
+    for (int a : {-1, 1}) for (int b : {-1, 1}) put(a, 0, b);
+    for (int a : {-1, 1}) for (int b : {-1, 1}) for (int c : {-1, 1}) put(a, b, c);
+    for (int i = 0; i < 26; ++i)
+      for (int j = 0; j < 26; ++j)
+        if (dx[j] == -dx[i] && dy[j] == -dy[i] && dz[j] == -dz[i]) opp[i] = j;
+    // dijkstra3d corner order: (-,-,-)(+,-,-)(-,+,-)(-,-,+)(+,+,-)(+,-,+)(-,+,+)(+,+,+)
+    const int corners[8][3] = {{-1,-1,-1},{1,-1,-1},{-1,1,-1},{-1,-1,1},{1,1,-1},{1,-1,1},{-1,1,1},{1,1,1}};
+    for (int i = 0; i < 18; ++i) { d3rank[i] = i; d3inv[i] = i; }
+    for (int r = 0; r < 8; ++r)
+      for (int j = 18; j < 26; ++j)
+        if (dx[j] == corners[r][0] && dy[j] == corners[r][1] && dz[j] == corners[r][2]) { d3inv[18 + r] = j; d3rank[j] = 18 + r; }
+  }
+};
+const Tables T;
+
+struct Shape {
+  i64 sx, sy, sz;
+  i64 n() const { return sx * sy * sz; }
+  i64 idx(i64 x, i64 y, i64 z) const { return x + sx * (y + sy * z); }
+  void xyz(i64 i, i64 &x, i64 &y, i64 &z) const { z = i / (sx * sy); i -= z * sx * sy; y = i / sx; x = i - y * sx; }
+  bool inside(i64 x, i64 y, i64 z) const { return x >= 0 && y >= 0 && z >= 0 && x < sx && y < sy && z < sz; }
+};
+
+inline uint32_t fbits(float f) { uint32_t b; std::memcpy(&b, &f, 4); return b; }
+inline float bitsf(uint32_t b) { float f; std::memcpy(&f, &b, 4); return f; }
+
+// ---------------------------------------------------------------------------------------------
+// Connected components (ccl.cu:25-63): 26-connected components of equal nonzero labels. The
+// union-find root of a component is its lowest flat index; ids 1..K follow ascending roots.
+struct Components {
+  std::vector<uint32_t> ids;    // per voxel, 0 = background
+  std::vector<int64_t> mapping; // id -> original label (index 0 unused)
+  std::vector<int64_t> roots;   // id-1 -> first flat index
+};
+
+template <class L>
+Components connected_components(const L *labels, const Shape &s) {
+  const i64 n = s.n();
+  std::vector<i64> parent(n);
+  std::iota(parent.begin(), parent.end(), i64(0));
+  auto find = [&](i64 v) {
+    i64 r = v;
+    while (parent[r] != r) r = parent[r];
+    while (parent[v] != r) { i64 next = parent[v]; parent[v] = r; v = next; }
+    return r;
+  };
+  for (i64 v = 0; v < n; ++v) {
+    if (labels[v] == 0) continue;
+    i64 x, y, z; s.xyz(v, x, y, z);
+    for (int k = 0; k < 26; ++k) {
+      i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+      if (!s.inside(nx, ny, nz)) continue;
+      i64 u = s.idx(nx, ny, nz);
+      if (u <= v || labels[u] != labels[v]) continue;
+      i64 a = find(v), b = find(u);
+      if (a != b) { if (a < b) parent[b] = a; else parent[a] = b; }
+    }
+  }
+  Components c;
+  c.ids.assign(n, 0);
+  c.mapping.push_back(0);
+  std::vector<uint32_t> id_of(n, 0);
+  for (i64 v = 0; v < n; ++v) {
+    if (labels[v] == 0) continue;
+    i64 r = find(v);
+    if (r == v) {  // roots appear in ascending flat order
+      c.roots.push_back(v);
+      c.mapping.push_back(static_cast<int64_t>(labels[v]));
+      id_of[v] = static_cast<uint32_t>(c.roots.size());
+    }
+    c.ids[v] = id_of[r];
+  }
+  return c;
+}
+
+Components components_any(const void *labels, int dtype, const Shape &s) {
+  switch (dtype) {
+    case 0: return connected_components(static_cast<const uint8_t *>(labels), s);
+    case 1: return connected_components(static_cast<const uint16_t *>(labels), s);
+    case 2: return connected_components(static_cast<const uint32_t *>(labels), s);
+    case 3: return connected_components(static_cast<const uint64_t *>(labels), s);
+    case 4: return connected_components(static_cast<const int8_t *>(labels), s);
+    case 5: return connected_components(static_cast<const int16_t *>(labels), s);
+    case 6: return connected_components(static_cast<const int32_t *>(labels), s);
+    case 7: return connected_components(static_cast<const int64_t *>(labels), s);
+    default: throw std::invalid_argument("integer labels required");
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Multi-label anisotropic EDT (edt_kernels.cuh:15-144, edt.cu:12-15). Distance of each voxel to
+// the nearest voxel of a different label; with black_border the volume edge counts as such a
+// voxel. `dims` = 2 skips the z pass (the 2D face transforms of the border targets).
+void edt_pass_x(const uint32_t *lab, float *D, const Shape &s, float w, bool bb) {
+  std::vector<float> acc(s.sx + 2, 0.0f);
+  for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + w;  // one float32 rounding per step
+  for (i64 line = 0; line < s.sy * s.sz; ++line) {
+    const i64 base = s.sx * line;
+    i64 i = 0;
+    while (i < s.sx) {
+      const uint32_t L = lab[base + i];
+      i64 c = i, d = i;
+      while (d + 1 < s.sx && lab[base + d + 1] == L) ++d;
+      const bool leftw = c > 0 || bb, rightw = d < s.sx - 1 || bb;
+      for (i64 p = c; p <= d; ++p) {
+        float best = kInf;
+        if (leftw) { float dd = acc[p - (c - 1)]; float v = dd * dd; if (v < best) best = v; }
+        if (rightw) { float dd = acc[(d + 1) - p]; float v = dd * dd; if (v < best) best = v; }
+        D[base + p] = best;
+      }
+      i = d + 1;
+    }
+  }
+}
+
+// One line of the y / z pass: lower envelope of the parabolas of a run's finite heights and its
+// walls (height 0), evaluated in double. The reference compiles this pass with FMA contraction;
+// the two sums of a product and a height are written as explicit fused operations here (exact
+// for integer spacings, where every product is an integer below 2^53).
+void edt_line_fh(const uint32_t *lab, float *D, i64 base, i64 stride, i64 n, float w, bool bb,
+                 std::vector<i64> &V, std::vector<float> &H, std::vector<double> &Z) {
+  const double w2 = static_cast<double>(w * w);
+  i64 i = 0;
+  while (i < n) {
+    const uint32_t L = lab[base + i * stride];
+    i64 c = i, d = i;
+    while (d + 1 < n && lab[base + (d + 1) * stride] == L) ++d;
+    const bool leftw = c > 0 || bb, rightw = d < n - 1 || bb;
+    int k = -1;
+    auto place = [&](i64 pp, double ph) {
+      bool placed = false;
+      while (k >= 0 && !placed) {
+        const double num = std::fma(w2 * static_cast<double>(pp), static_cast<double>(pp), ph) -
+                           std::fma(w2 * static_cast<double>(V[k]), static_cast<double>(V[k]), static_cast<double>(H[k]));
+        const double s = num / (2.0 * w2 * (static_cast<double>(pp) - static_cast<double>(V[k])));
+        if (s <= Z[k]) --k;
+        else { ++k; V[k] = pp; H[k] = static_cast<float>(ph); Z[k] = s; placed = true; }
+      }
+      if (!placed) { k = 0; V[0] = pp; H[0] = static_cast<float>(ph); Z[0] = -1e300; }
+    };
+    if (leftw) { k = 0; V[0] = c - 1; H[0] = 0.0f; Z[0] = -1e300; }
+    for (i64 p = c; p <= d; ++p) {
+      const float hf = D[base + p * stride];
+      if (!(hf < kInf)) continue;
+      place(p, static_cast<double>(hf));
+    }
+    if (rightw) place(d + 1, 0.0);
+    if (k < 0) {
+      for (i64 q = c; q <= d; ++q) D[base + q * stride] = kInf;
+    } else {
+      int kk = 0;
+      for (i64 q = c; q <= d; ++q) {
+        while (kk < k && Z[kk + 1] < static_cast<double>(q)) ++kk;
+        const double dq = static_cast<double>(q) - static_cast<double>(V[kk]);
+        D[base + q * stride] = static_cast<float>(std::fma(w2 * dq, dq, static_cast<double>(H[kk])));
+      }
+    }
+    i = d + 1;
+  }
+}
+
+std::vector<float> edt(const uint32_t *lab, const Shape &s, const float aniso[3], bool bb, int dims = 3) {
+  std::vector<float> D(s.n());
+  edt_pass_x(lab, D.data(), s, aniso[0], bb);
+  const i64 longest = std::max(s.sy, s.sz) + 3;
+  std::vector<i64> V(longest); std::vector<float> H(longest); std::vector<double> Z(longest);
+  if (dims >= 2)
+    for (i64 z = 0; z < s.sz; ++z)
+      for (i64 x = 0; x < s.sx; ++x) edt_line_fh(lab, D.data(), x + s.sx * s.sy * z, s.sx, s.sy, aniso[1], bb, V, H, Z);
+  if (dims >= 3)
+    for (i64 y = 0; y < s.sy; ++y)
+      for (i64 x = 0; x < s.sx; ++x) edt_line_fh(lab, D.data(), x + s.sx * y, s.sx * s.sy, s.sz, aniso[2], bb, V, H, Z);
+  for (i64 i = 0; i < s.n(); ++i) D[i] = lab[i] == 0 ? 0.0f : std::sqrt(D[i]);
+  return D;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Border targets: CPython 3.12's insertion-ordered hash set of integer 3-tuples (the collection
+// Kimimaro gathers border points in; point_set.hpp restates it for the reference). Tuple hash:
+// CPython's xxHash-based tuplehash; int hash: value mod (2^61 - 1) with the sign kept, -1 -> -2;
+// set probing: 9 linear probes then perturbed jumps; resize when fill * 5 >= mask * 3.
+class TupleSet {
+  struct Slot { std::array<i64, 3> p{}; uint64_t h = 0; bool live = false; };
+  std::vector<Slot> table_ = std::vector<Slot>(8);
+  size_t used_ = 0;
+  static uint64_t hash_int(i64 v) {
+    const uint64_t modulus = (uint64_t{1} << 61) - 1;
+    uint64_t mag = v < 0 ? uint64_t(-(v + 1)) + 1 : uint64_t(v);
+    i64 h = static_cast<i64>(mag % modulus);
+    if (v < 0) h = -h;
+    if (h == -1) h = -2;
+    return static_cast<uint64_t>(h);
+  }
+  static uint64_t hash(const std::array<i64, 3> &p) {
+    const uint64_t prime1 = 11400714785074694791ull, prime2 = 14029467366897019727ull, prime5 = 2870177450012600261ull;
+    uint64_t acc = prime5;
+    for (i64 v : p) { acc += hash_int(v) * prime2; acc = (acc << 31) | (acc >> 33); acc *= prime1; }
+    acc += uint64_t{3} ^ (prime5 ^ 3527539ull);
+    return acc == ~uint64_t{0} ? 1546275796ull : acc;
+  }
+  bool place(const std::array<i64, 3> &p, uint64_t h, bool compare) {
+    const size_t mask = table_.size() - 1;
+    size_t i = h & mask; uint64_t perturb = h;
+    for (;;) {
+      const size_t probes = i + 9 <= mask ? 9 : 0;
+      for (size_t j = 0; j <= probes; ++j) {
+        Slot &slot = table_[i + j];
+        if (!slot.live) { slot.p = p; slot.h = h; slot.live = true; return true; }
+        if (compare && slot.h == h && slot.p == p) return false;
+      }
+      perturb >>= 5;
+      i = (i * 5 + 1 + perturb) & mask;
+    }
+  }
+ public:
+  void add(const std::array<i64, 3> &p) {
+    if (!place(p, hash(p), true)) return;
+    ++used_;
+    if (used_ * 5 < (table_.size() - 1) * 3) return;
+    const size_t target = used_ * (used_ > 50000 ? 2 : 4);
+    size_t size = 8;
+    while (size <= target) size *= 2;
+    std::vector<Slot> old = std::move(table_);
+    table_.assign(size, Slot{});
+    for (const Slot &slot : old) if (slot.live) place(slot.p, slot.h, false);
+  }
+  std::vector<std::array<i64, 3>> values() const {
+    std::vector<std::array<i64, 3>> out;
+    for (const Slot &slot : table_) if (slot.live) out.push_back(slot.p);
+    return out;
+  }
+};
+
+// Kimimaro's tie-break keys among a face component's farthest pixels (borders.cu:38-52).
+float sqdist2(float x, float y, float a, float b, float wx, float wy) {
+  const float dx = wx * (x - a), dy = wy * (y - b);
+  return dx * dx + dy * dy;
+}
+std::array<float, 4> border_keys(i64 ix, i64 iy, float cx, float cy, i64 nx, i64 ny, float wx, float wy) {
+  const float x = float(ix), y = float(iy), fx = float(nx), fy = float(ny);
+  const float centre_x = float(double(wx * fx) / 2.0), centre_y = float(double(wy * fy) / 2.0);
+  const float far_x = float(double(fx) - 0.5), far_y = float(double(fy) - 0.5);
+  const float corner = std::min({sqdist2(x, y, -0.5f, -0.5f, wx, wy), sqdist2(x, y, far_x, -0.5f, wx, wy),
+                                 sqdist2(x, y, far_x, far_y, wx, wy), sqdist2(x, y, -0.5f, far_x, wx, wy)});
+  const float edge = float(std::min({double(wx) * (double(x) - 0.5), double(wx) * (double(fx) - 0.5 - double(x)),
+                                     double(wy) * (double(y) - 0.5), double(wy) * (double(fy) - 0.5 - double(y))}));
+  return {sqdist2(x, y, cx, cy, wx, wy), sqdist2(x, y, centre_x, centre_y, wx, wy), corner, edge};
+}
+
+// Per face: a 2D CC of the face's component ids, a 2D EDT with black border, and per face
+// component the farthest pixel (borders.cu:53-116). Returns, per component id, its border points.
+std::vector<std::vector<std::array<i64, 3>>> border_targets(const std::vector<uint32_t> &cc, const Shape &s, size_t count,
+                                                            const float aniso[3]) {
+  std::vector<TupleSet> sets(count + 1);
+  const i64 shape[3] = {s.sx, s.sy, s.sz};
+  const int axes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
+  for (int face = 0; face < 6; ++face) {
+    const int a = axes[face / 2][0], b = axes[face / 2][1], c = axes[face / 2][2];
+    const i64 fixed = face % 2 ? shape[c] - 1 : 0, fx = shape[a], fy = shape[b];
+    // the face as a (fy, fx) plane: plane x = the b coordinate, plane y = the a coordinate
+    const Shape ps{fy, fx, 1};
+    std::vector<uint32_t> plane(fx * fy);
+    for (i64 pa = 0; pa < fx; ++pa)
+      for (i64 pb = 0; pb < fy; ++pb) {
+        i64 p[3]; p[a] = pa; p[b] = pb; p[c] = fixed;
+        plane[pb + fy * pa] = cc[s.idx(p[0], p[1], p[2])];
+      }
+    Components pc = connected_components(plane.data(), ps);
+    const float plane_aniso[3] = {aniso[b], aniso[a], 1.0f};
+    std::vector<float> d = edt(pc.ids.data(), ps, plane_aniso, true, 2);
+    const size_t k = pc.mapping.size();
+    std::vector<float> maxdist(k, 0.0f), sumx(k, 0.0f), sumy(k, 0.0f);
+    std::vector<uint32_t> sizes(k, 0);
+    std::vector<i64> first(k, std::numeric_limits<i64>::max()), pick(k, -1);
+    for (i64 x = 0; x < fx; ++x)
+      for (i64 y = 0; y < fy; ++y) {
+        const size_t i = y + fy * x; const uint32_t label = pc.ids[i];
+        if (!label) continue;
+        sumx[label] += float(x); sumy[label] += float(y); ++sizes[label];
+        if (d[i] > 0) { maxdist[label] = std::max(maxdist[label], d[i]); first[label] = std::min(first[label], x + fx * y); }
+      }
+    const float wx = aniso[a], wy = aniso[b];
+    std::vector<float> cx(k, 0.0f), cy(k, 0.0f);
+    for (size_t label = 1; label < k; ++label)
+      if (sizes[label]) {
+        float px = (wx * sumx[label]) / float(sizes[label]), py = (wy * sumy[label]) / float(sizes[label]);
+        if (px - (wx * float(fx)) / 2.0f < 0) px = px + wx;
+        if (py - (wy * float(fy)) / 2.0f < 0) py = py + wy;
+        cx[label] = float(int(px / wx)); cy[label] = float(int(py / wy));
+      }
+    std::vector<std::array<float, 4>> best(k);
+    for (i64 y = 0; y < fy; ++y)
+      for (i64 x = 0; x < fx; ++x) {
+        const size_t i = y + fy * x; const uint32_t label = pc.ids[i];
+        if (!label || d[i] == 0 || d[i] != maxdist[label]) continue;
+        const auto key = border_keys(x, y, cx[label], cy[label], fx, fy, wx, wy);
+        if (pick[label] < 0 || key < best[label]) { best[label] = key; pick[label] = x + fx * y; }
+      }
+    std::vector<size_t> order;
+    for (size_t label = 1; label < k; ++label) if (pick[label] >= 0) order.push_back(label);
+    std::sort(order.begin(), order.end(), [&](size_t u, size_t v) { return first[u] < first[v]; });
+    for (size_t label : order) {
+      std::array<i64, 3> p{};
+      p[a] = pick[label] % fx; p[b] = pick[label] / fx; p[c] = fixed;
+      sets.at(pc.mapping[label]).add(p);
+    }
+  }
+  std::vector<std::vector<std::array<i64, 3>>> out;
+  for (const auto &set : sets) out.push_back(set.values());
+  return out;
+}
+
+// ---------------------------------------------------------------------------------------------
+// 26-connected geometric distance within one component (the DAF flood, batched.cu:211-232;
+// weights: faces = spacing, edges = |pair|, corners = |spacing|, each rounded to float32 from
+// double). Dijkstra over float32 sums: fl(d + w) is monotone in d, so the fixed point the
+// reference's Bellman-Ford reaches is the one this search settles.
+struct Weights { float w[26]; };
+Weights geometric_weights(const float aniso[3]) {
+  const double x = aniso[0], y = aniso[1], z = aniso[2];
+  Weights W;
+  const float faces[3] = {float(x), float(y), float(z)};
+  for (int k = 0; k < 6; ++k) W.w[k] = faces[k / 2];
+  const double pairs[3] = {std::sqrt(x * x + y * y), std::sqrt(y * y + z * z), std::sqrt(x * x + z * z)};
+  for (int k = 6; k < 18; ++k) W.w[k] = float(pairs[(k - 6) / 4]);
+  for (int k = 18; k < 26; ++k) W.w[k] = float(std::sqrt(x * x + y * y + z * z));
+  return W;
+}
+
+void geometric_flood(const std::vector<uint32_t> &ids, const Shape &s, uint32_t label, i64 source, const Weights &W,
+                     std::vector<float> &dist, const std::vector<i64> &voxels) {
+  for (i64 v : voxels) dist[v] = kInf;
+  using Item = std::pair<float, i64>;
+  std::priority_queue<Item, std::vector<Item>, std::greater<Item>> heap;
+  dist[source] = 0.0f; heap.push({0.0f, source});
+  while (!heap.empty()) {
+    auto [d, u] = heap.top(); heap.pop();
+    if (d > dist[u]) continue;
+    i64 x, y, z; s.xyz(u, x, y, z);
+    for (int k = 0; k < 26; ++k) {
+      const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+      if (!s.inside(nx, ny, nz)) continue;
+      const i64 v = s.idx(nx, ny, nz);
+      if (ids[v] != label) continue;
+      const float cand = d + W.w[k];
+      if (cand < dist[v]) { dist[v] = cand; heap.push({cand, v}); }
+    }
+  }
+}
+
+// argmax over a component's voxels: largest finite value, ties -> lowest flat (batched_regular.inc:9-22)
+i64 argmax(const std::vector<float> &f, const std::vector<i64> &voxels, float &value) {
+  i64 best = -1; value = 0;
+  for (i64 v : voxels) {  // voxels ascend, so strict > keeps the lowest flat among ties
+    const float x = f[v];
+    if (!(x < kInf)) continue;
+    if (best < 0 || fbits(x) > fbits(value)) { best = v; value = x; }
+  }
+  return best;
+}
+
+// ---------------------------------------------------------------------------------------------
+// One vertex-weighted step (common.cuh:113-127): fl(d + f), advanced by one ulp where f > 0 is
+// absorbed, so that distances strictly increase along every step.
+inline float vw_step(float d, float f) {
+  float c = d + f;
+  if (c == d && f > 0.0f && d < kInf) c = bitsf(fbits(d) + 1);
+  return c;
+}
+
+struct Params {
+  double scale, constant, pdrf_scale, pdrf_exponent;
+  double soma_detection, soma_acceptance, soma_scale, soma_constant;
+  int64_t max_paths; int has_max_paths;
+  float anisotropy[3];
+  double dust;
+  int fix_branching, fix_borders;
+};
+
+// Per-object tracing state over the shared volume. Every array is indexed by global flat index;
+// an object only ever touches its own voxels, so objects can be traced concurrently.
+struct Volume {
+  Shape s;
+  const std::vector<uint32_t> *ids;
+  std::vector<float> dbf, pdrf, dist;
+  std::vector<uint8_t> alive, inq;
+  std::vector<uint64_t> key;
+};
+
+constexpr uint64_t kUnclaimed = ~uint64_t{0};
+
+// Railroad (lockstep_coop.inc:71-305 semantics; trace_primitives.cu:282-311): SSSP from `target`
+// over the object's voxels, entering v costs pdrf[v] (vw_step); rails (pdrf == 0) absorb. The
+// nearest rail is the least (distance bits, flat); the path walks back from it by the argmin
+// neighbour distance (non-rail neighbours, lowest table index on ties), after re-picking the join
+// as the last road voxel's first rail in dijkstra3d order (lockstep_regular.inc:61-155).
+// Returns the path target-first, or an empty path when no rail is reachable.
+std::vector<i64> railroad(Volume &V, uint32_t label, i64 target, std::vector<i64> &touched) {
+  const Shape &s = V.s; const auto &ids = *V.ids;
+  if (V.pdrf[target] == 0.0f) return {target};
+  using Item = std::pair<float, i64>;
+  std::priority_queue<Item, std::vector<Item>, std::greater<Item>> heap;
+  touched.clear();
+  V.dist[target] = 0.0f; touched.push_back(target); heap.push({0.0f, target});
+  uint64_t best = ~uint64_t{0};
+  while (!heap.empty()) {
+    auto [d, u] = heap.top();
+    if (best != ~uint64_t{0} && d > bitsf(uint32_t(best >> 32))) break;
+    heap.pop();
+    if (d > V.dist[u]) continue;
+    if (V.pdrf[u] == 0.0f) continue;  // rails absorb
+    i64 x, y, z; s.xyz(u, x, y, z);
+    for (int k = 0; k < 26; ++k) {
+      const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+      if (!s.inside(nx, ny, nz)) continue;
+      const i64 v = s.idx(nx, ny, nz);
+      if (ids[v] != label) continue;
+      const float cand = vw_step(d, V.pdrf[v]);
+      if (cand < V.dist[v]) {
+        if (V.dist[v] == kInf) touched.push_back(v);
+        V.dist[v] = cand;
+        if (V.pdrf[v] == 0.0f) {
+          const uint64_t key = (uint64_t(fbits(cand)) << 32) | uint64_t(uint32_t(v));
+          best = std::min(best, key);
+        }
+        heap.push({cand, v});
+      }
+    }
+  }
+  std::vector<i64> walk;
+  if (best != ~uint64_t{0}) {
+    i64 cur = i64(uint32_t(best));
+    i64 x, y, z; s.xyz(cur, x, y, z);
+    for (int step = 0;; ++step) {
+      int kb = -1;
+      if (cur != target) {
+        uint32_t mb = 0x7f800000u;
+        for (int k = 0; k < 26; ++k) {
+          const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+          if (!s.inside(nx, ny, nz)) continue;
+          const i64 u = s.idx(nx, ny, nz);
+          if (ids[u] != label || V.pdrf[u] == 0.0f) continue;
+          const uint32_t db = fbits(V.dist[u]);
+          if (db < mb) { mb = db; kb = k; }
+        }
+      }
+      if (step == 0 && kb >= 0) {  // the join: u's first rail in dijkstra3d order
+        const i64 ux = x + T.dx[kb], uy = y + T.dy[kb], uz = z + T.dz[kb];
+        for (int r = 0; r < 26; ++r) {
+          const int k = T.d3inv[r];
+          const i64 nx = ux + T.dx[k], ny = uy + T.dy[k], nz = uz + T.dz[k];
+          if (!s.inside(nx, ny, nz)) continue;
+          const i64 v = s.idx(nx, ny, nz);
+          if (ids[v] != label || V.pdrf[v] != 0.0f) continue;
+          x = nx; y = ny; z = nz; cur = v; kb = T.opp[k];
+          break;
+        }
+      }
+      walk.push_back(cur);
+      if (kb < 0) break;
+      x += T.dx[kb]; y += T.dy[kb]; z += T.dz[kb];
+      cur = s.idx(x, y, z);
+    }
+    std::reverse(walk.begin(), walk.end());
+  }
+  for (i64 v : touched) V.dist[v] = kInf;
+  return walk;
+}
+
+// Claim-order invalidation (invalidation_kernels.cuh:105-297; lockstep_coop.inc:530-845). Path
+// vertices still alive become sources (bottleneck M = 0). A claimed voxel u holding (M, s) offers
+// an alive neighbour v of the object the source s when |aniso * (v - s)| < scale * DBF[s] + const,
+// with M' = max(M, |v - s|). Offers inside the current band [k delta, (k+1) delta) claim at once,
+// keeping the least (M bits, source); rounds inside a band are synchronous (every frontier voxel
+// offers from its key at the round boundary). Voxels offered beyond the band wait; at the band
+// boundary each takes the best offer of its claimed neighbours, the smallest of those names the
+// next band, and those inside it are claimed. Returns the number of voxels invalidated.
+i64 invalidate(Volume &V, uint32_t label, const std::vector<i64> &path, const Params &P,
+               std::vector<i64> &touched, std::vector<i64> &frontier, std::vector<i64> &next, std::vector<i64> &far,
+               std::vector<i64> &keep, std::vector<uint64_t> &snap) {
+  const Shape &s = V.s; const auto &ids = *V.ids;
+  const float wx = P.anisotropy[0], wy = P.anisotropy[1], wz = P.anisotropy[2];
+  const float scale = float(P.scale), constant = float(P.constant);
+  const float delta = std::min({wx, wy, wz});
+  touched.clear(); frontier.clear(); far.clear();
+  for (i64 p : path) {
+    if (!V.alive[p]) continue;
+    if (V.key[p] == kUnclaimed) {
+      V.key[p] = uint64_t(uint32_t(p));
+      V.inq[p] = 1; frontier.push_back(p); touched.push_back(p);
+    }
+  }
+  auto distance = [&](i64 vx, i64 vy, i64 vz, i64 src) {
+    i64 qx, qy, qz; s.xyz(src, qx, qy, qz);
+    const float dvx = wx * float(vx - qx), dvy = wy * float(vy - qy), dvz = wz * float(vz - qz);
+    return std::sqrt(dvx * dvx + dvy * dvy + dvz * dvz);
+  };
+  auto reach = [&](i64 src) { return scale * V.dbf[src] + constant; };
+  auto band_of = [&](uint32_t mbits, int kmin) {
+    const float m = bitsf(mbits);
+    int k = int(m / delta);
+    while (float(k + 1) * delta <= m) ++k;
+    while (k > 0 && float(k) * delta > m) --k;
+    return k < kmin ? kmin : k;
+  };
+  int band = 0;
+  for (;;) {
+    uint32_t hi = fbits(float(band + 1) * delta);
+    while (!frontier.empty()) {
+      snap.resize(frontier.size());
+      for (size_t i = 0; i < frontier.size(); ++i) { snap[i] = V.key[frontier[i]]; V.inq[frontier[i]] = 0; }
+      next.clear();
+      for (size_t i = 0; i < frontier.size(); ++i) {
+        const i64 u = frontier[i];
+        const i64 src = i64(uint32_t(snap[i]));
+        const uint32_t mu = uint32_t(snap[i] >> 32);
+        const float maxd = reach(src);
+        i64 x, y, z; s.xyz(u, x, y, z);
+        for (int k = 0; k < 26; ++k) {
+          const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+          if (!s.inside(nx, ny, nz)) continue;
+          const i64 v = s.idx(nx, ny, nz);
+          if (!V.alive[v] || ids[v] != label) continue;
+          const float d = distance(nx, ny, nz, src);
+          if (d >= maxd) continue;
+          uint32_t mb = fbits(d);
+          if (mb < mu) mb = mu;
+          if (mb < hi) {
+            const uint64_t cand = (uint64_t(mb) << 32) | uint64_t(uint32_t(src));
+            if (cand < V.key[v]) {
+              if (V.key[v] == kUnclaimed) touched.push_back(v);
+              V.key[v] = cand;
+              if (V.inq[v] != 1) { V.inq[v] = 1; next.push_back(v); }
+            }
+          } else if (V.key[v] == kUnclaimed && V.inq[v] == 0) {
+            V.inq[v] = 2; far.push_back(v);
+          }
+        }
+      }
+      frontier.swap(next);
+    }
+    if (far.empty()) break;
+    // band boundary: every waiting voxel pulls the best offer of its claimed neighbours
+    std::vector<uint64_t> pulled(far.size(), kUnclaimed);
+    std::vector<uint8_t> state(far.size(), 0);  // 0 no offer, 1 offer, 2 claimed meanwhile
+    uint32_t lowest = 0x7f800000u;
+    for (size_t i = 0; i < far.size(); ++i) {
+      const i64 c = far[i];
+      if (V.key[c] != kUnclaimed) { state[i] = 2; continue; }
+      i64 x, y, z; s.xyz(c, x, y, z);
+      uint64_t bestk = kUnclaimed;
+      for (int k = 0; k < 26; ++k) {
+        const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+        if (!s.inside(nx, ny, nz)) continue;
+        const i64 u = s.idx(nx, ny, nz);
+        if (ids[u] != label || V.key[u] == kUnclaimed) continue;
+        const i64 src = i64(uint32_t(V.key[u]));
+        const float d = distance(x, y, z, src);
+        if (d >= reach(src)) continue;
+        uint32_t mb = fbits(d); const uint32_t mu = uint32_t(V.key[u] >> 32);
+        if (mb < mu) mb = mu;
+        bestk = std::min(bestk, (uint64_t(mb) << 32) | uint64_t(uint32_t(src)));
+      }
+      if (bestk != kUnclaimed) { state[i] = 1; pulled[i] = bestk; lowest = std::min(lowest, uint32_t(bestk >> 32)); }
+    }
+    if (lowest != 0x7f800000u) band = band_of(lowest, band + 1);
+    hi = fbits(float(band + 1) * delta);
+    keep.clear();
+    for (size_t i = 0; i < far.size(); ++i) {
+      const i64 c = far[i];
+      if (state[i] == 2) continue;
+      if (state[i] == 0) { V.inq[c] = 0; continue; }
+      if (uint32_t(pulled[i] >> 32) < hi) {
+        V.key[c] = pulled[i]; touched.push_back(c); frontier.push_back(c); V.inq[c] = 1;
+      } else keep.push_back(c);
+    }
+    far.swap(keep);
+  }
+  for (i64 v : touched) { V.alive[v] = 0; V.key[v] = kUnclaimed; V.inq[v] = 0; }
+  for (i64 v : far) V.inq[v] = 0;
+  return i64(touched.size());
+}
+
+struct ObjectPlan {
+  uint32_t id;
+  i64 root, target;
+  std::vector<i64> voxels;     // ascending flat
+  std::vector<i64> order;      // target order
+  std::vector<i64> manual;     // manual targets in pop order
+  i64 max_paths;
+};
+
+// The trace loop of one object (trace.cu:196-246 order, lockstep.cu:91-183 targets): manual
+// targets first, then the first alive voxel of the target order; railroad; invalidation; the
+// path becomes rails.
+std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, const Params &P) {
+  std::vector<std::vector<i64>> paths;
+  std::vector<i64> touched, frontier, next, far, keep, rtouched;
+  std::vector<uint64_t> snap;
+  if (plan.max_paths <= 0) return paths;
+  V.pdrf[plan.root] = 0.0f;
+  size_t cursor = 0;
+  while (i64(paths.size()) < plan.max_paths) {
+    i64 t = -1;
+    const size_t iter = paths.size();
+    if (iter < plan.manual.size()) t = plan.manual[iter];
+    else {
+      while (cursor < plan.order.size() && !V.alive[plan.order[cursor]]) ++cursor;
+      if (cursor >= plan.order.size()) break;
+      t = plan.order[cursor];
+    }
+    std::vector<i64> path = railroad(V, plan.id, t, rtouched);
+    if (path.empty()) throw std::runtime_error("no rail reachable from a target");
+    invalidate(V, plan.id, path, P, touched, frontier, next, far, keep, snap);
+    for (i64 v : path) V.pdrf[v] = 0.0f;
+    paths.push_back(std::move(path));
+  }
+  return paths;
+}
+
+// consolidate (skeleton.cpp:13-40) on voxel coordinates, then physical vertices and radii.
+struct Skeleton {
+  int64_t label = 0;
+  std::vector<std::array<i64, 3>> vox;
+  std::vector<std::array<uint32_t, 2>> edges;
+};
+
+Skeleton assemble(const std::vector<std::vector<i64>> &paths, const Shape &s) {
+  Skeleton out;
+  std::vector<std::array<i64, 3>> vertices;
+  std::vector<std::array<uint32_t, 2>> edges;
+  for (const auto &path : paths) {
+    if (path.size() < 2) continue;
+    const uint32_t base = uint32_t(vertices.size());
+    for (size_t j = 0; j < path.size(); ++j) {
+      i64 x, y, z; s.xyz(path[j], x, y, z);
+      vertices.push_back({x, y, z});
+      if (j) edges.push_back({uint32_t(base + j - 1), uint32_t(base + j)});
+    }
+  }
+  if (vertices.empty() || edges.empty()) return out;
+  std::vector<uint32_t> order(vertices.size()), inverse(vertices.size());
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return vertices[a] < vertices[b]; });
+  std::vector<std::array<i64, 3>> uniq;
+  for (uint32_t old : order) {
+    if (uniq.empty() || uniq.back() != vertices[old]) uniq.push_back(vertices[old]);
+    inverse[old] = uint32_t(uniq.size() - 1);
+  }
+  std::vector<std::array<uint32_t, 2>> e2;
+  for (auto e : edges) {
+    std::array<uint32_t, 2> f = {inverse[e[0]], inverse[e[1]]};
+    if (f[0] > f[1]) std::swap(f[0], f[1]);
+    if (f[0] != f[1]) e2.push_back(f);
+  }
+  std::sort(e2.begin(), e2.end());
+  e2.erase(std::unique(e2.begin(), e2.end()), e2.end());
+  std::vector<uint8_t> used(uniq.size(), 0);
+  for (auto e : e2) used[e[0]] = used[e[1]] = 1;
+  std::vector<uint32_t> remap(uniq.size(), 0);
+  for (size_t i = 0; i < uniq.size(); ++i)
+    if (used[i]) { remap[i] = uint32_t(out.vox.size()); out.vox.push_back(uniq[i]); }
+  for (auto &e : e2) e = {remap[e[0]], remap[e[1]]};
+  out.edges = std::move(e2);
+  return out;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The whole path (skeletonize.cu:70-183 with the lockstep inputs of batched.cu:177-255).
+struct Result {
+  std::vector<int64_t> labels, vertex_offsets{0}, edge_offsets{0};
+  std::vector<float> vertices, radii;
+  std::vector<uint32_t> edges;
+  std::string error;
+  // stage outputs
+  Components cc;
+  std::vector<float> dbf, daf, pdrf;
+  std::vector<int64_t> roots, targets, boxes;  // boxes: per id lo xyz, hi xyz, count
+  std::vector<std::vector<std::array<i64, 3>>> borders;
+  std::vector<int64_t> orders;                 // concatenated target orders of active ids
+  std::vector<int64_t> order_offsets;          // per id (count+2)
+  std::vector<int64_t> paths_flat, path_offsets{0}, path_labels;
+};
+
+Result run(const void *labels, int dtype, const Shape &s, const Params &P, int threads, int keep_stages) {
+  Result R;
+  const i64 n = s.n();
+  if (n == 0 || double(n) <= P.dust) return R;
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(P.anisotropy[a]) || P.anisotropy[a] <= 0) throw std::invalid_argument("anisotropy must be finite and positive");
+  {
+    const double e = P.pdrf_exponent;
+    if (std::isfinite(e) && e == std::floor(e) && std::fmod(e, 2.0) == 1.0)
+      throw std::invalid_argument("odd pdrf_exponent makes the background penalty negative");
+  }
+  R.cc = components_any(labels, dtype, s);
+  const auto &ids = R.cc.ids;
+  const size_t count = R.cc.roots.size();
+  if (!count) return R;
+  // bounding boxes and counts (preamble.cu:10-29)
+  std::vector<std::array<i64, 7>> box(count + 1, {INT32_MAX, INT32_MAX, INT32_MAX, -1, -1, -1, 0});
+  std::vector<std::vector<i64>> voxels(count + 1);
+  for (i64 v = 0; v < n; ++v) {
+    const uint32_t id = ids[v];
+    if (!id) continue;
+    i64 x, y, z; s.xyz(v, x, y, z);
+    auto &b = box[id];
+    b[0] = std::min(b[0], x); b[1] = std::min(b[1], y); b[2] = std::min(b[2], z);
+    b[3] = std::max(b[3], x); b[4] = std::max(b[4], y); b[5] = std::max(b[5], z); ++b[6];
+    voxels[id].push_back(v);
+  }
+  const bool black_border = count == 1 && box[1][6] == n;
+  Volume V; V.s = s; V.ids = &ids;
+  V.dbf = edt(ids.data(), s, P.anisotropy, black_border);
+  std::vector<std::vector<std::array<i64, 3>>> borders(count + 1);
+  if (P.fix_borders) borders = border_targets(ids, s, count, P.anisotropy);
+  // active objects (batched.cu:187-191): more voxels than dust and a bounding box of 2+ voxels
+  std::vector<uint8_t> active(count + 1, 0);
+  std::vector<float> dbf_max(count + 1, 0.0f);
+  for (size_t id = 1; id <= count; ++id) {
+    const auto &b = box[id];
+    const i64 bbox = (b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1);
+    float m; argmax(V.dbf, voxels[id], m); dbf_max[id] = m;
+    if (double(b[6]) <= P.dust || bbox <= 1) continue;
+    if (double(dbf_max[id]) > P.soma_detection) throw std::invalid_argument("soma objects are not covered by the oracle");
+    active[id] = 1;
+  }
+  const Weights W = geometric_weights(P.anisotropy);
+  std::vector<float> daf(n, kInf);
+  std::vector<ObjectPlan> plans;
+  std::vector<int64_t> roots(count + 1, -1), targets(count + 1, -1);
+  std::vector<float> max_daf(count + 1, 0.0f);
+  for (size_t id = 1; id <= count; ++id) {
+    if (!active[id]) continue;
+    i64 root;
+    if (!borders[id].empty()) { const auto &p = borders[id].back(); root = s.idx(p[0], p[1], p[2]); }
+    else {
+      geometric_flood(ids, s, uint32_t(id), R.cc.roots[id - 1], W, daf, voxels[id]);
+      float m; root = argmax(daf, voxels[id], m);
+    }
+    geometric_flood(ids, s, uint32_t(id), root, W, daf, voxels[id]);
+    float m; const i64 target = argmax(daf, voxels[id], m);
+    roots[id] = root; targets[id] = target; max_daf[id] = m;
+  }
+  // PDRF (batched.cu:234-245, batched_regular.inc:93-108): power-of-two exponents only
+  const double exponent = P.pdrf_exponent;
+  if (!(exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))))
+    throw std::invalid_argument("the oracle covers power-of-two pdrf_exponent only");
+  int squarings = 0;
+  for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+  V.pdrf.assign(n, kInf);
+  {
+    std::vector<float> M(count + 1, 0.0f), inv(count + 1, 0.0f);
+    std::vector<uint8_t> use(count + 1, 0);
+    for (size_t id = 1; id <= count; ++id)
+      if (active[id]) {
+        M[id] = float(1.0 / std::pow(double(dbf_max[id]), 1.01));
+        if (max_daf[id] != 0) { inv[id] = float(1.0 / double(max_daf[id])); use[id] = 2; } else use[id] = 1;
+      }
+    const float scale = float(P.pdrf_scale);
+    for (i64 i = 0; i < n; ++i) {
+      const uint32_t L = ids[i];
+      if (L == 0 || use[L] == 0) continue;
+      float d = V.dbf[i];
+      if (d == 0.0f) d = kInf;
+      float p = 1.0f - d * M[L];
+      for (int k = 0; k < squarings; ++k) p = p * p;
+      p = p * scale;
+      if (use[L] == 2) { float dd = daf[i]; if (std::isinf(dd)) dd = 0.0f; p = p + dd * inv[L]; }
+      V.pdrf[i] = p;
+    }
+  }
+  if (keep_stages) { R.dbf = V.dbf; R.daf = daf; R.pdrf = V.pdrf; }
+  // target orders and manual targets (lockstep.cu:120-142, lockstep_order.cu:21-45)
+  R.order_offsets.assign(count + 2, 0);
+  for (size_t id = 1; id <= count; ++id) {
+    if (!active[id]) continue;
+    ObjectPlan plan;
+    plan.id = uint32_t(id); plan.root = roots[id]; plan.target = targets[id];
+    plan.voxels = voxels[id];
+    plan.order = voxels[id];
+    std::sort(plan.order.begin(), plan.order.end(), [&](i64 a, i64 b) {
+      float x = daf[a], y = daf[b];
+      if (std::isinf(x)) x = 0;
+      if (std::isinf(y)) y = 0;
+      return x == y ? a > b : x > y;
+    });
+    std::vector<std::array<i64, 3>> manual = borders[id];
+    if (!manual.empty()) manual.pop_back();
+    if (manual.empty()) plan.manual.push_back(targets[id]);
+    else for (auto it = manual.rbegin(); it != manual.rend(); ++it) plan.manual.push_back(s.idx((*it)[0], (*it)[1], (*it)[2]));
+    const i64 budget = P.has_max_paths ? P.max_paths : box[id][6];
+    plan.max_paths = i64(plan.manual.size()) >= budget ? 0 : budget;
+    plans.push_back(std::move(plan));
+  }
+  V.dist.assign(n, kInf);
+  V.alive.assign(n, 0);
+  for (i64 i = 0; i < n; ++i) V.alive[i] = ids[i] ? active[ids[i]] : 0;
+  V.inq.assign(n, 0);
+  V.key.assign(n, kUnclaimed);
+  std::vector<std::vector<std::vector<i64>>> traced(plans.size());
+  {
+    std::atomic<size_t> next{0};
+    std::mutex failure;
+    std::string message;
+    // largest objects first, so that a pool of threads finishes together
+    std::vector<size_t> schedule(plans.size());
+    std::iota(schedule.begin(), schedule.end(), size_t(0));
+    std::stable_sort(schedule.begin(), schedule.end(), [&](size_t a, size_t b) { return plans[a].voxels.size() > plans[b].voxels.size(); });
+    auto worker = [&] {
+      for (;;) {
+        const size_t j = next.fetch_add(1);
+        if (j >= schedule.size()) return;
+        const size_t i = schedule[j];
+        try { traced[i] = trace_object(V, plans[i], P); }
+        catch (const std::exception &e) { std::lock_guard<std::mutex> lock(failure); message = e.what(); }
+      }
+    };
+    const int workers = std::max(1, std::min<int>(threads, int(plans.size())));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < workers; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+    if (!message.empty()) throw std::runtime_error(message);
+  }
+  // assembly: one skeleton per original label, components merged in id order (skeletonize.cu:130-181)
+  std::vector<int64_t> label_order;
+  std::vector<std::vector<std::vector<i64>>> merged;
+  for (size_t j = 0; j < plans.size(); ++j) {
+    const int64_t label = R.cc.mapping[plans[j].id];
+    Skeleton sk = assemble(traced[j], s);
+    if (sk.edges.empty()) continue;
+    auto it = std::find(label_order.begin(), label_order.end(), label);
+    if (it == label_order.end()) { label_order.push_back(label); merged.push_back(traced[j]); }
+    else { auto &m = merged[it - label_order.begin()]; m.insert(m.end(), traced[j].begin(), traced[j].end()); }
+  }
+  for (size_t j = 0; j < label_order.size(); ++j) {
+    Skeleton sk = assemble(merged[j], s);
+    R.labels.push_back(label_order[j]);
+    for (const auto &v : sk.vox) {
+      for (int a = 0; a < 3; ++a) R.vertices.push_back(float(v[a]) * P.anisotropy[a]);
+      R.radii.push_back(V.dbf[s.idx(v[0], v[1], v[2])]);
+    }
+    for (const auto &e : sk.edges) { R.edges.push_back(e[0]); R.edges.push_back(e[1]); }
+    R.vertex_offsets.push_back(int64_t(R.radii.size()));
+    R.edge_offsets.push_back(int64_t(R.edges.size() / 2));
+  }
+  if (keep_stages) {
+    R.roots = roots; R.targets = targets; R.borders = borders;
+    R.boxes.clear();
+    for (size_t id = 0; id <= count; ++id) for (int a = 0; a < 7; ++a) R.boxes.push_back(box[id][a]);
+    for (size_t id = 1; id <= count; ++id) {
+      R.order_offsets[id + 1] = R.order_offsets[id];
+      auto it = std::find_if(plans.begin(), plans.end(), [&](const ObjectPlan &p) { return p.id == id; });
+      if (it == plans.end()) continue;
+      R.orders.insert(R.orders.end(), it->order.begin(), it->order.end());
+      R.order_offsets[id + 1] += i64(it->order.size());
+    }
+    for (size_t j = 0; j < plans.size(); ++j)
+      for (const auto &p : traced[j]) {
+        R.paths_flat.insert(R.paths_flat.end(), p.begin(), p.end());
+        R.path_offsets.push_back(i64(R.paths_flat.size()));
+        R.path_labels.push_back(plans[j].id);
+      }
+  }
+  return R;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// C interface for the Python test harness (ctypes).
+extern "C" {
+
+struct oracle_params {
+  double scale, constant, pdrf_scale, pdrf_exponent;
+  double soma_detection, soma_acceptance, soma_scale, soma_constant;
+  int64_t max_paths; int32_t has_max_paths;
+  float anisotropy[3];
+  double dust;
+  int32_t fix_branching, fix_borders;
+};
+
+void *oracle_run(const void *labels, int dtype, int64_t sx, int64_t sy, int64_t sz, const oracle_params *p,
+                 int threads, int keep_stages) {
+  auto *r = new Result();
+  try {
+    Params P{};
+    P.scale = p->scale; P.constant = p->constant; P.pdrf_scale = p->pdrf_scale; P.pdrf_exponent = p->pdrf_exponent;
+    P.soma_detection = p->soma_detection; P.soma_acceptance = p->soma_acceptance;
+    P.soma_scale = p->soma_scale; P.soma_constant = p->soma_constant;
+    P.max_paths = p->max_paths; P.has_max_paths = p->has_max_paths;
+    for (int a = 0; a < 3; ++a) P.anisotropy[a] = p->anisotropy[a];
+    P.dust = p->dust; P.fix_branching = p->fix_branching; P.fix_borders = p->fix_borders;
+    if (!P.fix_branching) throw std::invalid_argument("the oracle covers fix_branching=True");
+    *r = run(labels, dtype, Shape{sx, sy, sz}, P, threads, keep_stages);
+  } catch (const std::exception &e) {
+    r->error = e.what();
+  }
+  return r;
+}
+void oracle_free(void *h) { delete static_cast<Result *>(h); }
+const char *oracle_error(void *h) { return static_cast<Result *>(h)->error.c_str(); }
+
+// Array accessors: name -> (pointer, element count). Element types are fixed per name.
+const void *oracle_array(void *h, const char *name, int64_t *count) {
+  auto *r = static_cast<Result *>(h);
+  const std::string k(name);
+  auto give = [&](const auto &v) -> const void * { *count = int64_t(v.size()); return v.data(); };
+  if (k == "labels") return give(r->labels);
+  if (k == "vertex_offsets") return give(r->vertex_offsets);
+  if (k == "edge_offsets") return give(r->edge_offsets);
+  if (k == "vertices") return give(r->vertices);
+  if (k == "radii") return give(r->radii);
+  if (k == "edges") return give(r->edges);
+  if (k == "cc") return give(r->cc.ids);
+  if (k == "mapping") return give(r->cc.mapping);
+  if (k == "cc_roots") return give(r->cc.roots);
+  if (k == "dbf") return give(r->dbf);
+  if (k == "daf") return give(r->daf);
+  if (k == "pdrf") return give(r->pdrf);
+  if (k == "roots") return give(r->roots);
+  if (k == "targets") return give(r->targets);
+  if (k == "boxes") return give(r->boxes);
+  if (k == "orders") return give(r->orders);
+  if (k == "order_offsets") return give(r->order_offsets);
+  if (k == "paths") return give(r->paths_flat);
+  if (k == "path_offsets") return give(r->path_offsets);
+  if (k == "path_labels") return give(r->path_labels);
+  *count = -1;
+  return nullptr;
+}
+// Border points of component `id`, flattened (x, y, z) triples in set order.
+int64_t oracle_borders(void *h, int64_t id, int64_t *out, int64_t capacity) {
+  auto *r = static_cast<Result *>(h);
+  if (id < 0 || size_t(id) >= r->borders.size()) return -1;
+  const auto &b = r->borders[id];
+  for (size_t i = 0; i < b.size() && int64_t(3 * i + 2) < capacity; ++i)
+    for (int a = 0; a < 3; ++a) out[3 * i + a] = b[i][a];
+  return int64_t(b.size());
+}
+
+// Standalone stages, for known-answer tests.
+int oracle_edt(const uint32_t *labels, int64_t sx, int64_t sy, int64_t sz, const float aniso[3], int black_border,
+               int dims, float *out) {
+  try {
+    auto d = edt(labels, Shape{sx, sy, sz}, aniso, black_border != 0, dims);
+    std::copy(d.begin(), d.end(), out);
+    return 0;
+  } catch (...) { return 1; }
+}
+// Railroad on a raw penalty field of one component (all voxels of `labels` equal to 1 belong to it).
+int64_t oracle_railroad(const float *field, const uint32_t *labels, int64_t sx, int64_t sy, int64_t sz,
+                        int64_t target, int64_t *out, int64_t capacity) {
+  Volume V; V.s = Shape{sx, sy, sz};
+  std::vector<uint32_t> ids(labels, labels + V.s.n());
+  V.ids = &ids;
+  V.pdrf.assign(field, field + V.s.n());
+  V.dist.assign(V.s.n(), kInf);
+  std::vector<i64> touched;
+  auto path = railroad(V, 1, target, touched);
+  for (size_t i = 0; i < path.size() && int64_t(i) < capacity; ++i) out[i] = path[i];
+  return int64_t(path.size());
+}
+// Target order rule on a flat (mask, daf) pair: descending daf (inf -> 0), ties -> higher index.
+int64_t oracle_target_order(const uint8_t *mask, const float *daf, int64_t n, int64_t *out) {
+  std::vector<int64_t> order;
+  for (int64_t i = 0; i < n; ++i) if (mask[i]) order.push_back(i);
+  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+    float x = daf[a], y = daf[b];
+    if (std::isinf(x) || x == 0) x = 0;
+    if (std::isinf(y) || y == 0) y = 0;
+    return x == y ? a > b : x > y;
+  });
+  std::copy(order.begin(), order.end(), out);
+  return int64_t(order.size());
+}
+}
