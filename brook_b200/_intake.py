@@ -1,0 +1,141 @@
+"""`skeletonize`: the reference's brook.skeletonize argument surface (src/brook/_intake.py:99-103)
+over the brook_b200 C ABI."""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native
+from ._packed import PackedSkeletons
+
+# The values of the reference's brook.DEFAULT_TEASAR_PARAMS (src/brook/__init__.py:8-17).
+DEFAULT_TEASAR_PARAMS = {
+    "scale": 1.5,
+    "const": 300,
+    "pdrf_scale": 100000,
+    "pdrf_exponent": 4,
+    "soma_acceptance_threshold": 3500,
+    "soma_detection_threshold": 750,
+    "soma_invalidation_const": 300,
+    "soma_invalidation_scale": 2,
+}
+
+# Keys a caller leaves out take kimimaro.trace's defaults, as in the reference (skeleton.hpp:23-27).
+TRACE_DEFAULTS = {
+    "scale": 10.0, "const": 10.0, "pdrf_scale": 5000.0, "pdrf_exponent": 16.0,
+    "soma_detection_threshold": 1100.0, "soma_acceptance_threshold": 4000.0,
+    "soma_invalidation_scale": 0.5, "soma_invalidation_const": 0.0, "max_paths": None,
+}
+
+
+class DimensionError(Exception):
+    """The input volume has unsupported dimensions."""
+
+
+def teasar(params):
+    out = dict(TRACE_DEFAULTS)
+    for key, value in dict(params).items():
+        if key not in out:
+            raise TypeError(f"unexpected TEASAR parameter: {key}")
+        out[key] = value if key == "max_paths" else float(value)
+    return out
+
+
+def format_labels(labels):
+    """Host labels as a 3D integer NumPy array (bool -> uint8, trailing singleton axes dropped,
+    missing axes appended), without rearranging its bytes."""
+    labels = np.asarray(labels)
+    if labels.dtype == bool:
+        labels = labels.view(np.uint8)
+    while labels.ndim > 3 and labels.shape[-1] == 1:
+        labels = labels[..., 0]
+    if labels.ndim > 3:
+        raise DimensionError(f"{labels.ndim} dimensions is not supported (max 3).")
+    while labels.ndim < 3:
+        labels = labels[..., np.newaxis]
+    if labels.dtype.kind not in "ui":
+        raise TypeError("brook_b200: labels must be integer or boolean")
+    return labels
+
+
+def _is_device(labels):
+    return not isinstance(labels, np.ndarray) and (hasattr(labels, "__cuda_array_interface__") or
+                                                   (hasattr(labels, "is_cuda") and labels.is_cuda))
+
+
+def device_volume(labels):
+    """(brook_volume, keep-alive) for a CUDA array (torch tensor or an object with the CUDA array
+    interface); the array is read in place when it is Fortran-ordered."""
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        torch = None
+    if torch is not None and isinstance(labels, torch.Tensor):
+        t = labels
+        if t.dtype == torch.bool:
+            t = t.view(torch.uint8)
+        while t.dim() < 3:
+            t = t.unsqueeze(-1)
+        dtype = np.dtype(str(t.dtype).replace("torch.", ""))
+        strides = [s * t.element_size() for s in t.stride()]
+        return _native.device_volume(t.data_ptr(), tuple(t.shape), strides, dtype), t
+    cai = labels.__cuda_array_interface__
+    shape = tuple(cai["shape"])
+    dtype = np.dtype(cai["typestr"])
+    strides = cai.get("strides") or tuple(int(np.prod(shape[a + 1:])) * dtype.itemsize for a in range(len(shape)))
+    while len(shape) < 3:
+        shape, strides = shape + (1,), tuple(strides) + (dtype.itemsize,)
+    return _native.device_volume(cai["data"][0], shape, strides, dtype), labels
+
+
+def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
+         extra_after, device):
+    opts = _native.options(params, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids,
+                           extra_before, extra_after)
+    ctx = _native.context(device)
+    count = len(volumes)
+    arr = (_native.Volume * max(count, 1))(*volumes)
+    handles = (_native.ctypes.c_void_p * max(count, 1))()
+    if count == 1:
+        _native.check(_native.lib.brook_skeletonize(ctx, arr, _native.ctypes.byref(opts), handles))
+    else:
+        _native.check(_native.lib.brook_skeletonize_batch(ctx, arr, count, _native.ctypes.byref(opts), handles))
+    return [PackedSkeletons.from_arrays(_native.packed_arrays(handles[i])) for i in range(count)]
+
+
+def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), object_ids=None,
+                dust_threshold=1000, progress=False, fix_branching=True, in_place=False, fix_borders=True, parallel=1,
+                parallel_chunk_size=100, extra_targets_before=(), extra_targets_after=(), fill_holes=False,
+                fix_avocados=False, voxel_graph=None, streaming=None, output="skeletons", stream=None, borrow=True,
+                device=0):
+    """Skeletonize a 3D label volume on a B200; a drop-in for the reference's `brook.skeletonize`
+    (and so for `kimimaro.skeletonize`).
+
+    Returns `{label: Skeleton}` for output="skeletons", `PackedSkeletons` (host arrays) for
+    "packed", and the same with CUDA tensors for "packed_device". Device input: a torch CUDA
+    tensor or an array with the CUDA array interface, read in place when Fortran-ordered.
+    `parallel`, `parallel_chunk_size`, `in_place`, `progress`, `stream`, `borrow` and `streaming`
+    are accepted for compatibility. `fill_holes`, `fix_avocados` and `voxel_graph` are not
+    supported by this build and raise.
+    """
+    if output not in ("skeletons", "packed", "packed_device"):
+        raise ValueError("brook_b200: output must be 'skeletons', 'packed' or 'packed_device'")
+    if fill_holes or fix_avocados or voxel_graph is not None:
+        raise NotImplementedError("brook_b200: fill_holes, fix_avocados and voxel_graph are not supported")
+    params = teasar(teasar_params)
+    anisotropy = tuple(float(a) for a in np.asarray(anisotropy, dtype=np.float32))
+    if _is_device(all_labels):
+        volume, keep = device_volume(all_labels)
+    else:
+        keep = format_labels(all_labels)
+        if keep.size <= dust_threshold:
+            packed = PackedSkeletons.empty(anisotropy)
+            return {} if output == "skeletons" else packed
+        volume = _native.host_volume(keep)
+    ids = None if object_ids is None else [int(i) for i in object_ids]
+    packed = _run([volume], params, anisotropy, ids, dust_threshold, fix_branching, fix_borders,
+                  [tuple(int(c) for c in p) for p in extra_targets_before],
+                  [tuple(int(c) for c in p) for p in extra_targets_after], device)[0]
+    del keep
+    if output == "skeletons":
+        return packed.to_skeletons()
+    return packed.to_device() if output == "packed_device" else packed

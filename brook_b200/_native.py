@@ -1,0 +1,211 @@
+"""ctypes binding of the C ABI in include/brook_b200.h (libbrook_b200.so, built in-tree).
+
+The library is the only compute path: importing this module fails loudly when it is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libbrook_b200.so")
+
+ABI_VERSION = 1
+SUCCESS, INVALID_ARGUMENT, OUT_OF_MEMORY, CUDA_ERROR, INTERNAL_ERROR = range(5)
+HOST, DEVICE = 0, 1
+FIX_BRANCHING, FIX_BORDERS, FILTER_OBJECTS, DEVICE_OUTPUT, FILL_HOLES, FIX_AVOCADOS = 1, 2, 4, 8, 16, 32
+
+DTYPES = {np.dtype(np.uint8): 0, np.dtype(np.uint16): 1, np.dtype(np.uint32): 2, np.dtype(np.uint64): 3,
+          np.dtype(np.int8): 4, np.dtype(np.int16): 5, np.dtype(np.int32): 6, np.dtype(np.int64): 7,
+          np.dtype(np.float32): 8, np.dtype(np.float64): 9}
+DTYPE_NAMES = {v: k for k, v in DTYPES.items()}
+
+# Every symbol include/brook_b200.h declares (the CPU tests check the library exports them all).
+EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_context_create", "brook_context_destroy",
+           "brook_context_synchronize", "brook_array_destroy", "brook_array_view", "brook_array_copy_to_host",
+           "brook_connected_components", "brook_components_destroy", "brook_components_view",
+           "brook_components_copy_to_host", "brook_edt", "brook_skeletonize_options_init", "brook_skeletonize",
+           "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy"]
+
+
+class Volume(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_size_t), ("abi_version", ctypes.c_uint32), ("data", ctypes.c_void_p),
+                ("shape", ctypes.c_int64 * 3), ("strides", ctypes.c_int64 * 3), ("dtype", ctypes.c_int),
+                ("memory", ctypes.c_int)]
+
+
+class Teasar(ctypes.Structure):
+    _fields_ = [("scale", ctypes.c_double), ("constant", ctypes.c_double), ("pdrf_scale", ctypes.c_double),
+                ("pdrf_exponent", ctypes.c_double), ("soma_detection_threshold", ctypes.c_double),
+                ("soma_acceptance_threshold", ctypes.c_double), ("soma_invalidation_scale", ctypes.c_double),
+                ("soma_invalidation_const", ctypes.c_double), ("max_paths", ctypes.c_int64),
+                ("has_max_paths", ctypes.c_uint32)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_size_t), ("abi_version", ctypes.c_uint32), ("teasar", Teasar),
+                ("anisotropy", ctypes.c_float * 3), ("dust_threshold", ctypes.c_double), ("flags", ctypes.c_uint32),
+                ("object_ids", ctypes.POINTER(ctypes.c_int64)), ("object_ids_count", ctypes.c_size_t),
+                ("targets_before", ctypes.POINTER(ctypes.c_int64)), ("targets_before_count", ctypes.c_size_t),
+                ("targets_after", ctypes.POINTER(ctypes.c_int64)), ("targets_after_count", ctypes.c_size_t),
+                ("voxel_graph", ctypes.POINTER(Volume))]
+
+
+class SkeletonsView(ctypes.Structure):
+    _fields_ = [("skeleton_count", ctypes.c_size_t), ("vertex_count", ctypes.c_size_t), ("edge_count", ctypes.c_size_t),
+                ("labels", ctypes.POINTER(ctypes.c_int64)), ("vertex_offsets", ctypes.POINTER(ctypes.c_int64)),
+                ("edge_offsets", ctypes.POINTER(ctypes.c_int64)), ("vertices", ctypes.POINTER(ctypes.c_float)),
+                ("edges", ctypes.POINTER(ctypes.c_uint32)), ("radii", ctypes.POINTER(ctypes.c_float)),
+                ("anisotropy", ctypes.c_float * 3)]
+
+
+class BrookError(RuntimeError):
+    """A brook_b200 call failed; `status` is the brook_status code."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"brook_b200: the CUDA library {LIB_PATH} is not built; run brook_b200/build.py "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    sig = {
+        "brook_abi_version": (ctypes.c_uint32, []),
+        "brook_version": (ctypes.c_char_p, []),
+        "brook_last_error": (ctypes.c_char_p, []),
+        "brook_context_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(vp)]),
+        "brook_context_destroy": (None, [vp]),
+        "brook_context_synchronize": (ctypes.c_int, [vp]),
+        "brook_array_destroy": (None, [vp]),
+        "brook_array_view": (ctypes.c_int, [vp, ctypes.POINTER(Volume)]),
+        "brook_array_copy_to_host": (ctypes.c_int, [vp, vp, sz]),
+        "brook_connected_components": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(vp)]),
+        "brook_components_destroy": (None, [vp]),
+        "brook_components_view": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(ctypes.POINTER(ctypes.c_int64)),
+                                                 ctypes.POINTER(ctypes.POINTER(ctypes.c_int64)), ctypes.POINTER(sz)]),
+        "brook_components_copy_to_host": (ctypes.c_int, [vp, vp, sz]),
+        "brook_edt": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
+                                     ctypes.POINTER(vp)]),
+        "brook_skeletonize_options_init": (None, [ctypes.POINTER(Options)]),
+        "brook_skeletonize": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(Options), ctypes.POINTER(vp)]),
+        "brook_skeletonize_batch": (ctypes.c_int, [vp, ctypes.POINTER(Volume), sz, ctypes.POINTER(Options),
+                                                   ctypes.POINTER(vp)]),
+        "brook_skeletons_get_view": (ctypes.c_int, [vp, ctypes.POINTER(SkeletonsView)]),
+        "brook_skeletons_destroy": (None, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status):
+    if status != SUCCESS:
+        raise BrookError(status, lib.brook_last_error().decode(errors="replace"))
+
+
+_contexts: dict = {}
+_lock = threading.Lock()
+
+
+def context(device=0):
+    """One context per (process, thread, device), as the reference's runtime keeps them."""
+    key = (os.getpid(), threading.get_ident(), int(device))
+    with _lock:
+        ctx = _contexts.get(key)
+        if ctx is None:
+            handle = ctypes.c_void_p()
+            check(lib.brook_context_create(int(device), ctypes.byref(handle)))
+            ctx = _contexts[key] = handle
+    return ctx
+
+
+def host_volume(array):
+    """A brook_volume over a NumPy array (any strides); the array must outlive the call."""
+    v = Volume()
+    v.struct_size = ctypes.sizeof(Volume)
+    v.abi_version = ABI_VERSION
+    v.data = array.ctypes.data if array.size else None
+    for a in range(3):
+        v.shape[a] = array.shape[a]
+        v.strides[a] = array.strides[a]
+    v.dtype = DTYPES[array.dtype]
+    v.memory = HOST
+    return v
+
+
+def device_volume(ptr, shape, strides_bytes, dtype):
+    v = Volume()
+    v.struct_size = ctypes.sizeof(Volume)
+    v.abi_version = ABI_VERSION
+    v.data = ptr
+    for a in range(3):
+        v.shape[a] = shape[a]
+        v.strides[a] = strides_bytes[a]
+    v.dtype = DTYPES[np.dtype(dtype)]
+    v.memory = DEVICE
+    return v
+
+
+def options(teasar, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids=None,
+            targets_before=(), targets_after=()):
+    o = Options()
+    lib.brook_skeletonize_options_init(ctypes.byref(o))
+    t = o.teasar
+    t.scale, t.constant, t.pdrf_scale, t.pdrf_exponent = (teasar["scale"], teasar["const"], teasar["pdrf_scale"],
+                                                          teasar["pdrf_exponent"])
+    t.soma_detection_threshold = teasar["soma_detection_threshold"]
+    t.soma_acceptance_threshold = teasar["soma_acceptance_threshold"]
+    t.soma_invalidation_scale = teasar["soma_invalidation_scale"]
+    t.soma_invalidation_const = teasar["soma_invalidation_const"]
+    if teasar.get("max_paths") is not None:
+        t.max_paths, t.has_max_paths = int(teasar["max_paths"]), 1
+    o.anisotropy[:] = [float(a) for a in anisotropy]
+    o.dust_threshold = float(dust_threshold)
+    o.flags = (FIX_BRANCHING if fix_branching else 0) | (FIX_BORDERS if fix_borders else 0)
+    keep = []
+    if object_ids is not None:
+        ids = np.ascontiguousarray(np.asarray(list(object_ids), dtype=np.int64))
+        keep.append(ids)
+        o.flags |= FILTER_OBJECTS
+        o.object_ids = ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        o.object_ids_count = ids.size
+    for name, points in (("targets_before", targets_before), ("targets_after", targets_after)):
+        pts = np.ascontiguousarray(np.asarray(list(points), dtype=np.int64).reshape(-1, 3))
+        if pts.size:
+            keep.append(pts)
+            setattr(o, name, pts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+            setattr(o, name + "_count", pts.shape[0])
+    o._keep = keep  # the arrays the pointers refer to
+    return o
+
+
+def packed_arrays(handle):
+    """Copies a brook_skeletons result into NumPy arrays and releases the handle."""
+    v = SkeletonsView()
+    try:
+        check(lib.brook_skeletons_get_view(handle, ctypes.byref(v)))
+
+        def grab(ptr, count, dtype, shape):
+            if count == 0:
+                return np.zeros(shape, dtype)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype, copy=True).reshape(shape)
+
+        k, nv, ne = v.skeleton_count, v.vertex_count, v.edge_count
+        return dict(labels=grab(v.labels, k, np.int64, (k,)), v_off=grab(v.vertex_offsets, k + 1, np.int64, (k + 1,)),
+                    e_off=grab(v.edge_offsets, k + 1, np.int64, (k + 1,)),
+                    vertices=grab(v.vertices, 3 * nv, np.float32, (nv, 3)), edges=grab(v.edges, 2 * ne, np.uint32, (ne, 2)),
+                    radii=grab(v.radii, nv, np.float32, (nv,)), anisotropy=tuple(float(a) for a in v.anisotropy))
+    finally:
+        lib.brook_skeletons_destroy(handle)

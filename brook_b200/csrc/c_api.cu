@@ -1,0 +1,409 @@
+// The C ABI (include/brook_b200.h): argument checks, input staging into Fortran-ordered device
+// buffers, exception -> brook_status mapping with thread-local error text, result handles.
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/brook_b200.h"
+#include "pipeline.hpp"
+
+#ifndef BROOK_B200_VERSION
+#define BROOK_B200_VERSION "0.1.0"
+#endif
+
+struct brook_context {
+  bk::Context value;
+  explicit brook_context(int device) : value(device) {}
+};
+
+// Device storage that outlives the context that made it (plain cudaMalloc / cudaFree).
+struct DeviceStorage {
+  void *ptr = nullptr;
+  int device = 0;
+  DeviceStorage(size_t bytes, int dev) : device(dev) {
+    if (bytes) {
+      cudaError_t s = cudaMalloc(&ptr, bytes);
+      if (s != cudaSuccess) { cudaGetLastError(); throw bk::CudaError(s, "cudaMalloc"); }
+    }
+  }
+  ~DeviceStorage() {
+    if (ptr) {
+      int previous = -1;
+      cudaGetDevice(&previous);
+      cudaSetDevice(device);
+      cudaFree(ptr);
+      if (previous >= 0) cudaSetDevice(previous);
+    }
+  }
+};
+
+struct brook_array {
+  std::shared_ptr<DeviceStorage> storage;
+  brook_volume view{};
+  size_t bytes = 0;
+};
+
+struct brook_components {
+  std::shared_ptr<DeviceStorage> storage;
+  brook_volume view{};
+  size_t bytes = 0;
+  std::vector<int64_t> mapping, roots;
+};
+
+struct brook_skeletons {
+  bk::Packed packed;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F>
+brook_status protect(F &&fn) noexcept {
+  try {
+    g_error.clear();
+    fn();
+    return BROOK_SUCCESS;
+  } catch (const std::invalid_argument &e) {
+    g_error = e.what();
+    return BROOK_INVALID_ARGUMENT;
+  } catch (const std::bad_alloc &e) {
+    g_error = e.what();
+    return BROOK_OUT_OF_MEMORY;
+  } catch (const bk::CudaError &e) {
+    g_error = e.what();
+    return e.code == cudaErrorMemoryAllocation ? BROOK_OUT_OF_MEMORY : BROOK_CUDA_ERROR;
+  } catch (const std::exception &e) {
+    g_error = e.what();
+    return BROOK_INTERNAL_ERROR;
+  } catch (...) {
+    g_error = "unknown exception";
+    return BROOK_INTERNAL_ERROR;
+  }
+}
+
+void require(bool ok, const char *what = "null brook argument") {
+  if (!ok) throw std::invalid_argument(what);
+}
+
+// A volume gathered into Fortran order on the device (or borrowed when it already is).
+struct Staged {
+  bk::Buffer<unsigned char> owned;
+  bk::DeviceVolume volume;
+};
+
+__global__ void gather_strided(const unsigned char *src, unsigned char *dst, int sx, int sy, int sz, long long s0,
+                               long long s1, long long s2, int b) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)sx * sy * sz;
+  if (i >= n) return;
+  const long long z = i / ((long long)sx * sy), r = i - z * sx * sy, y = r / sx, x = r - y * sx;
+  const unsigned char *p = src + x * s0 + y * s1 + z * s2;
+  unsigned char *q = dst + i * b;
+  for (int k = 0; k < b; ++k) q[k] = p[k];
+}
+
+Staged stage(bk::Context &ctx, const brook_volume &v) {
+  require(v.struct_size >= sizeof(brook_volume) && v.abi_version == BROOK_ABI_VERSION, "incompatible brook_volume");
+  require(v.dtype >= BROOK_U8 && v.dtype <= BROOK_I64, "integer labels required");
+  for (int a = 0; a < 3; ++a) require(v.shape[a] >= 0 && v.shape[a] < (1LL << 31), "invalid volume shape");
+  Staged st;
+  st.volume.dtype = int(v.dtype);
+  st.volume.d = bk::VolumeDims{int(v.shape[0]), int(v.shape[1]), int(v.shape[2])};
+  const long long n = st.volume.d.n();
+  require(n < (1LL << 31) - 1, "volumes of 2^31 voxels or more are not supported");
+  if (n == 0) return st;
+  require(v.data != nullptr);
+  const long long b = (long long)bk::label_bytes(v.dtype);
+  const long long sx = v.shape[0], sy = v.shape[1], sz = v.shape[2];
+  auto matches = [&](long long e0, long long e1, long long e2) {
+    return (sx == 1 || v.strides[0] == e0) && (sy == 1 || v.strides[1] == e1) && (sz == 1 || v.strides[2] == e2);
+  };
+  const bool fortran = matches(b, b * sx, b * sx * sy);
+  const bool c_order = matches(b * sy * sz, b * sz, b);
+  cudaStream_t s = ctx.stream();
+  if (v.memory == BROOK_DEVICE) {
+    cudaPointerAttributes attr{};
+    BK_CUDA(cudaPointerGetAttributes(&attr, v.data));
+    require(attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged, "device volume is not device memory");
+    require(attr.type == cudaMemoryTypeManaged || attr.device == ctx.device(), "device volume is on another device");
+    if (fortran) { st.volume.data = v.data; return st; }
+    st.owned = bk::Buffer<unsigned char>(ctx, n * b);
+    gather_strided<<<bk::blocks_for(n), 256, 0, s>>>(static_cast<const unsigned char *>(v.data), st.owned.data(), int(sx),
+                                                    int(sy), int(sz), v.strides[0], v.strides[1], v.strides[2], int(b));
+    BK_CUDA(cudaGetLastError());
+    st.volume.data = st.owned.data();
+    return st;
+  }
+  require(v.memory == BROOK_HOST, "invalid memory kind");
+  st.owned = bk::Buffer<unsigned char>(ctx, n * b);
+  if (fortran) {
+    BK_CUDA(cudaMemcpyAsync(st.owned.data(), v.data, n * b, cudaMemcpyHostToDevice, s));
+  } else if (c_order) {
+    bk::Buffer<unsigned char> raw(ctx, n * b);
+    BK_CUDA(cudaMemcpyAsync(raw.data(), v.data, n * b, cudaMemcpyHostToDevice, s));
+    gather_strided<<<bk::blocks_for(n), 256, 0, s>>>(raw.data(), st.owned.data(), int(sx), int(sy), int(sz), b * sy * sz,
+                                                    b * sz, b, int(b));
+    BK_CUDA(cudaGetLastError());
+    ctx.synchronize();
+  } else {
+    std::vector<unsigned char> host(n * b);
+    const unsigned char *base = static_cast<const unsigned char *>(v.data);
+    for (long long z = 0; z < sz; ++z)
+      for (long long y = 0; y < sy; ++y)
+        for (long long x = 0; x < sx; ++x)
+          std::memcpy(&host[((z * sy + y) * sx + x) * b], base + x * v.strides[0] + y * v.strides[1] + z * v.strides[2], b);
+    BK_CUDA(cudaMemcpyAsync(st.owned.data(), host.data(), n * b, cudaMemcpyHostToDevice, s));
+    ctx.synchronize();
+  }
+  st.volume.data = st.owned.data();
+  return st;
+}
+
+bk::Options options_of(const brook_skeletonize_options *p) {
+  require(p->struct_size >= sizeof(brook_skeletonize_options) && p->abi_version == BROOK_ABI_VERSION,
+          "incompatible skeletonization options");
+  const uint32_t known = BROOK_FIX_BRANCHING | BROOK_FIX_BORDERS | BROOK_FILTER_OBJECTS | BROOK_DEVICE_OUTPUT |
+                         BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS;
+  require(!(p->flags & ~known), "unknown skeletonization flags");
+  if (p->flags & (BROOK_DEVICE_OUTPUT | BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS))
+    throw std::invalid_argument("device output, fill_holes and fix_avocados are not supported by this build");
+  if (p->voxel_graph) throw std::invalid_argument("voxel_graph is not supported by this build");
+  bk::Options o;
+  auto &t = o.teasar;
+  t.scale = p->teasar.scale;
+  t.constant = p->teasar.constant;
+  t.pdrf_scale = p->teasar.pdrf_scale;
+  t.pdrf_exponent = p->teasar.pdrf_exponent;
+  t.soma_detection = p->teasar.soma_detection_threshold;
+  t.soma_acceptance = p->teasar.soma_acceptance_threshold;
+  t.soma_scale = p->teasar.soma_invalidation_scale;
+  t.soma_constant = p->teasar.soma_invalidation_const;
+  if (p->teasar.has_max_paths) t.max_paths = p->teasar.max_paths;
+  for (int a = 0; a < 3; ++a) o.anisotropy[a] = p->anisotropy[a];
+  o.dust = p->dust_threshold;
+  o.fix_branching = (p->flags & BROOK_FIX_BRANCHING) != 0;
+  o.fix_borders = (p->flags & BROOK_FIX_BORDERS) != 0;
+  if (p->flags & BROOK_FILTER_OBJECTS) {
+    require(p->object_ids || !p->object_ids_count);
+    o.object_ids = std::vector<int64_t>(p->object_ids, p->object_ids + p->object_ids_count);
+  }
+  auto points = [](const int64_t *data, size_t count) {
+    require(data || !count);
+    std::vector<bk::Point> out;
+    for (size_t i = 0; i < count; ++i) out.push_back({data[3 * i], data[3 * i + 1], data[3 * i + 2]});
+    return out;
+  };
+  o.targets_before = points(p->targets_before, p->targets_before_count);
+  o.targets_after = points(p->targets_after, p->targets_after_count);
+  return o;
+}
+
+__global__ void narrow_ids(const uint32_t *ids, void *out, long long n, int bytes) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t v = ids[i];
+  if (bytes == 1) static_cast<uint8_t *>(out)[i] = uint8_t(v);
+  else if (bytes == 2) static_cast<uint16_t *>(out)[i] = uint16_t(v);
+  else static_cast<uint32_t *>(out)[i] = v;
+}
+
+brook_volume device_view(const void *data, brook_dtype dtype, bk::VolumeDims d) {
+  brook_volume v{};
+  v.struct_size = sizeof(v);
+  v.abi_version = BROOK_ABI_VERSION;
+  v.data = data;
+  v.dtype = dtype;
+  v.memory = BROOK_DEVICE;
+  v.shape[0] = d.sx; v.shape[1] = d.sy; v.shape[2] = d.sz;
+  const size_t b = dtype == BROOK_F32 ? 4 : bk::label_bytes(dtype);
+  v.strides[0] = int64_t(b); v.strides[1] = int64_t(b) * d.sx; v.strides[2] = int64_t(b) * d.sx * d.sy;
+  return v;
+}
+
+brook_status skeletonize_many(brook_context *ctx, const brook_volume *volumes, size_t count,
+                              const brook_skeletonize_options *p, brook_skeletons **out) {
+  return protect([&] {
+    require(ctx && (volumes || !count) && p && out);
+    for (size_t i = 0; i < count; ++i) out[i] = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    const bk::Options options = options_of(p);
+    std::vector<Staged> staged;
+    std::vector<bk::DeviceVolume> vols;
+    for (size_t i = 0; i < count; ++i) {
+      staged.push_back(stage(ctx->value, volumes[i]));
+      vols.push_back(staged.back().volume);
+    }
+    auto results = bk::skeletonize(ctx->value, vols, options);
+    ctx->value.synchronize();
+    std::vector<std::unique_ptr<brook_skeletons>> handles;
+    for (auto &r : results) {
+      handles.emplace_back(new brook_skeletons());
+      handles.back()->packed = std::move(r);
+    }
+    for (size_t i = 0; i < count; ++i) out[i] = handles[i].release();
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t brook_abi_version(void) { return BROOK_ABI_VERSION; }
+const char *brook_version(void) { return BROOK_B200_VERSION; }
+const char *brook_last_error(void) { return g_error.c_str(); }
+
+brook_status brook_context_create(int device, brook_context **out) {
+  return protect([&] {
+    require(out);
+    *out = nullptr;
+    *out = new brook_context(device);
+  });
+}
+void brook_context_destroy(brook_context *ctx) { delete ctx; }
+brook_status brook_context_synchronize(brook_context *ctx) {
+  return protect([&] {
+    require(ctx);
+    ctx->value.synchronize();
+  });
+}
+
+void brook_array_destroy(brook_array *a) { delete a; }
+brook_status brook_array_view(const brook_array *a, brook_volume *out) {
+  return protect([&] {
+    require(a && out);
+    *out = a->view;
+  });
+}
+brook_status brook_array_copy_to_host(const brook_array *a, void *out, size_t bytes) {
+  return protect([&] {
+    require(a && (out || !bytes));
+    require(bytes >= a->bytes, "output buffer too small");
+    bk::DeviceGuard guard(a->storage->device);
+    if (a->bytes) BK_CUDA(cudaMemcpy(out, a->storage->ptr, a->bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+brook_status brook_connected_components(brook_context *ctx, const brook_volume *labels, brook_components **out) {
+  return protect([&] {
+    require(ctx && labels && out);
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    Staged st = stage(ctx->value, *labels);
+    const long long n = st.volume.d.n();
+    bk::Buffer<uint32_t> ids(ctx->value, n > 0 ? n : 1);
+    auto cc = n ? bk::connected_components(ctx->value, st.volume.data, st.volume.dtype, st.volume.d, ids.data())
+                : bk::ComponentsResult{0, {0}, {}};
+    const brook_dtype dtype = cc.count <= 0xFF ? BROOK_U8 : cc.count <= 0xFFFF ? BROOK_U16 : BROOK_U32;
+    const size_t b = bk::label_bytes(dtype);
+    auto handle = std::make_unique<brook_components>();
+    handle->storage = std::make_shared<DeviceStorage>(size_t(n) * b, ctx->value.device());
+    handle->bytes = size_t(n) * b;
+    if (n) {
+      narrow_ids<<<bk::blocks_for(n), 256, 0, ctx->value.stream()>>>(ids.data(), handle->storage->ptr, n, int(b));
+      BK_CUDA(cudaGetLastError());
+    }
+    ctx->value.synchronize();
+    handle->view = device_view(handle->storage->ptr, dtype, st.volume.d);
+    handle->mapping = cc.mapping;
+    if (handle->mapping.empty()) handle->mapping.push_back(0);
+    handle->roots = cc.roots;
+    *out = handle.release();
+  });
+}
+void brook_components_destroy(brook_components *c) { delete c; }
+brook_status brook_components_view(const brook_components *c, brook_volume *labels, const int64_t **mapping,
+                                   const int64_t **roots, size_t *count) {
+  return protect([&] {
+    require(c);
+    if (labels) *labels = c->view;
+    if (mapping) *mapping = c->mapping.data();
+    if (roots) *roots = c->roots.data();
+    if (count) *count = c->roots.size();
+  });
+}
+brook_status brook_components_copy_to_host(const brook_components *c, void *out, size_t bytes) {
+  return protect([&] {
+    require(c && (out || !bytes));
+    require(bytes >= c->bytes, "output buffer too small");
+    bk::DeviceGuard guard(c->storage->device);
+    if (c->bytes) BK_CUDA(cudaMemcpy(out, c->storage->ptr, c->bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+brook_status brook_edt(brook_context *ctx, const brook_volume *labels, const float anisotropy[3], int black_border,
+                       brook_array **out) {
+  return protect([&] {
+    require(ctx && labels && anisotropy && out);
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    Staged st = stage(ctx->value, *labels);
+    const long long n = st.volume.d.n();
+    auto handle = std::make_unique<brook_array>();
+    handle->storage = std::make_shared<DeviceStorage>(size_t(n) * 4, ctx->value.device());
+    handle->bytes = size_t(n) * 4;
+    if (n) {
+      bk::Buffer<uint32_t> ids(ctx->value, n);
+      bk::connected_components(ctx->value, st.volume.data, st.volume.dtype, st.volume.d, ids.data());
+      bk::edt(ctx->value, ids.data(), st.volume.d, anisotropy, black_border != 0, 3,
+              static_cast<float *>(handle->storage->ptr));
+    }
+    ctx->value.synchronize();
+    handle->view = device_view(handle->storage->ptr, BROOK_F32, st.volume.d);
+    *out = handle.release();
+  });
+}
+
+void brook_skeletonize_options_init(brook_skeletonize_options *p) {
+  if (!p) return;
+  *p = brook_skeletonize_options{};
+  p->struct_size = sizeof(*p);
+  p->abi_version = BROOK_ABI_VERSION;
+  p->teasar.scale = 1.5;
+  p->teasar.constant = 300;
+  p->teasar.pdrf_scale = 100000;
+  p->teasar.pdrf_exponent = 4;
+  p->teasar.soma_detection_threshold = 750;
+  p->teasar.soma_acceptance_threshold = 3500;
+  p->teasar.soma_invalidation_scale = 2;
+  p->teasar.soma_invalidation_const = 300;
+  p->anisotropy[0] = p->anisotropy[1] = p->anisotropy[2] = 1;
+  p->dust_threshold = 1000;
+  p->flags = BROOK_FIX_BRANCHING | BROOK_FIX_BORDERS;
+}
+
+brook_status brook_skeletonize(brook_context *ctx, const brook_volume *labels, const brook_skeletonize_options *p,
+                               brook_skeletons **out) {
+  if (!labels) return protect([] { require(false); });
+  return skeletonize_many(ctx, labels, 1, p, out);
+}
+
+brook_status brook_skeletonize_batch(brook_context *ctx, const brook_volume *volumes, size_t count,
+                                     const brook_skeletonize_options *p, brook_skeletons **out) {
+  return skeletonize_many(ctx, volumes, count, p, out);
+}
+
+brook_status brook_skeletons_get_view(const brook_skeletons *r, brook_skeletons_view *out) {
+  return protect([&] {
+    require(r && out);
+    const auto &p = r->packed;
+    out->skeleton_count = p.labels.size();
+    out->vertex_count = p.radii.size();
+    out->edge_count = p.edges.size() / 2;
+    out->labels = p.labels.data();
+    out->vertex_offsets = p.vertex_offsets.data();
+    out->edge_offsets = p.edge_offsets.data();
+    out->vertices = p.vertices.data();
+    out->edges = p.edges.data();
+    out->radii = p.radii.data();
+    for (int a = 0; a < 3; ++a) out->anisotropy[a] = p.anisotropy[a];
+  });
+}
+void brook_skeletons_destroy(brook_skeletons *r) { delete r; }
+
+}  // extern "C"

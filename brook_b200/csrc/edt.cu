@@ -1,0 +1,198 @@
+// Multi-label anisotropic EDT on sm_100a, three separable passes with the reference's arithmetic
+// (edt_kernels.cuh:15-144 of giorgioangel/brook):
+//   x: distance to the walls of each run of equal ids, from a float32 table of accumulated
+//      spacings (one rounding per step); one warp per x-line, coalesced, with run starts and ends
+//      found by warp max/min scans and the starts staged in shared memory;
+//   y, z: float64 lower envelope of parabolas per run, stored as float32; one thread per line,
+//      lines x-consecutive across a warp (coalesced), envelope stacks interleaved across lines;
+//   the last pass takes the square root (background: 0).
+// The reference compiles the envelope with FMA contraction; its two product-plus-height sums are
+// written as explicit fused operations here, everything else rounds per operation (--fmad=false).
+#include <climits>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace bk {
+namespace {
+
+constexpr int kWarpsX = 4;
+
+__global__ void edt_x(const uint32_t *__restrict__ ids, float *__restrict__ D, Dims d, const float *__restrict__ acc,
+                      int bb, int finish) {
+  extern __shared__ int s_start[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long line = (long long)blockIdx.x * kWarpsX + warp;
+  if (line >= (long long)d.sy * d.sz) return;
+  const int sx = d.sx;
+  int *start = s_start + warp * sx;
+  const long long base = line * sx;
+  int carry_start = 0;
+  uint32_t carry_label = 0;
+  for (int c0 = 0; c0 < sx; c0 += 32) {
+    const int p = c0 + lane;
+    const bool in = p < sx;
+    const uint32_t lab = in ? ids[base + p] : 0xFFFFFFFFu;
+    uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, lab, 1);
+    if (lane == 0) prev = carry_label;
+    int st = (in && (p == 0 || lab != prev)) ? p : -1;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int o = __shfl_up_sync(0xFFFFFFFFu, st, off);
+      if (lane >= off) st = max(st, o);
+    }
+    st = max(st, carry_start);
+    if (in) start[p] = st;
+    carry_start = __shfl_sync(0xFFFFFFFFu, st, 31);
+    carry_label = __shfl_sync(0xFFFFFFFFu, lab, 31);
+  }
+  __syncwarp();
+  int carry_end = sx - 1;
+  uint32_t carry_next = 0;
+  for (int c0 = ((sx - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
+    const int p = c0 + lane;
+    const bool in = p < sx;
+    const uint32_t lab = in ? ids[base + p] : 0xFFFFFFFFu;
+    uint32_t next = __shfl_down_sync(0xFFFFFFFFu, lab, 1);
+    if (lane == 31) next = carry_next;
+    int en = (in && (p == sx - 1 || lab != next)) ? p : INT_MAX;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int o = __shfl_down_sync(0xFFFFFFFFu, en, off);
+      if (lane + off < 32) en = min(en, o);
+    }
+    en = min(en, carry_end);
+    if (in) {
+      const int c = start[p];
+      float best = __uint_as_float(BK_INF_BITS);
+      if (c > 0 || bb) { const float dd = acc[p - c + 1]; const float v = __fmul_rn(dd, dd); if (v < best) best = v; }
+      if (en < sx - 1 || bb) { const float dd = acc[en + 1 - p]; const float v = __fmul_rn(dd, dd); if (v < best) best = v; }
+      if (finish) best = lab == 0 ? 0.0f : sqrtf(best);
+      D[base + p] = best;
+    }
+    carry_end = __shfl_sync(0xFFFFFFFFu, en, 0);
+    carry_next = __shfl_sync(0xFFFFFFFFu, lab, 0);
+  }
+}
+
+// One line of the y or z pass. Stacks V/H/Z are interleaved: entry k of this thread's stack is at
+// [k * pitch].
+__global__ void edt_envelope(const uint32_t *__restrict__ ids, float *__restrict__ D, Dims d, int axis, float w, int bb,
+                             long long line0, long long nbatch, int *__restrict__ Vs, float *__restrict__ Hs,
+                             double *__restrict__ Zs, int finish) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= nbatch) return;
+  const long long line = line0 + tid;
+  long long base, stride;
+  int n;
+  if (axis == 1) {
+    const long long x = line % d.sx, z = line / d.sx;
+    if (z >= d.sz) return;
+    base = x + (long long)d.sx * d.sy * z; stride = d.sx; n = d.sy;
+  } else {
+    const long long x = line % d.sx, y = line / d.sx;
+    if (y >= d.sy) return;
+    base = x + (long long)d.sx * y; stride = (long long)d.sx * d.sy; n = d.sz;
+  }
+  int *V = Vs + tid;
+  float *H = Hs + tid;
+  double *Z = Zs + tid;
+  const long long pitch = nbatch;
+  const double w2 = (double)__fmul_rn(w, w);
+  int i = 0;
+  while (i < n) {
+    const uint32_t L = ids[base + (long long)i * stride];
+    int c = i, e = i;
+    while (e + 1 < n && ids[base + (long long)(e + 1) * stride] == L) ++e;
+    const bool leftw = c > 0 || bb, rightw = e < n - 1 || bb;
+    int k = -1;
+    if (leftw) { k = 0; V[0] = c - 1; H[0] = 0.0f; Z[0] = -1e300; }
+    for (int p = c; p <= e + 1; ++p) {
+      double ph;
+      if (p <= e) {
+        const float hf = D[base + (long long)p * stride];
+        if (!(hf < __uint_as_float(BK_INF_BITS))) continue;
+        ph = (double)hf;
+      } else {
+        if (!rightw) break;
+        ph = 0.0;
+      }
+      bool placed = false;
+      while (k >= 0 && !placed) {
+        const int vk = V[(long long)k * pitch];
+        const double num = __dsub_rn(__fma_rn(__dmul_rn(w2, (double)p), (double)p, ph),
+                                     __fma_rn(__dmul_rn(w2, (double)vk), (double)vk, (double)H[(long long)k * pitch]));
+        const double s = __ddiv_rn(num, __dmul_rn(__dmul_rn(2.0, w2), __dsub_rn((double)p, (double)vk)));
+        if (s <= Z[(long long)k * pitch]) --k;
+        else {
+          ++k;
+          V[(long long)k * pitch] = p; H[(long long)k * pitch] = (float)ph; Z[(long long)k * pitch] = s;
+          placed = true;
+        }
+      }
+      if (!placed) { k = 0; V[0] = p; H[0] = (float)ph; Z[0] = -1e300; }
+    }
+    if (k < 0) {
+      for (int q = c; q <= e; ++q) {
+        float v = __uint_as_float(BK_INF_BITS);
+        if (finish) v = L == 0 ? 0.0f : v;
+        D[base + (long long)q * stride] = v;
+      }
+    } else {
+      int kk = 0;
+      for (int q = c; q <= e; ++q) {
+        while (kk < k && Z[(long long)(kk + 1) * pitch] < (double)q) ++kk;
+        const int vk = V[(long long)kk * pitch];
+        const double dq = __dsub_rn((double)q, (double)vk);
+        float v = __double2float_rn(__fma_rn(__dmul_rn(w2, dq), dq, (double)H[(long long)kk * pitch]));
+        if (finish) v = L == 0 ? 0.0f : sqrtf(v);
+        D[base + (long long)q * stride] = v;
+      }
+    }
+    i = e + 1;
+  }
+}
+
+}  // namespace
+
+void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3], bool black_border, int dims,
+         float *D) {
+  const Dims d{vd.sx, vd.sy, vd.sz};
+  const long long n = vd.n();
+  if (!n) return;
+  for (int a = 0; a < 3; ++a)
+    if (!(aniso[a] > 0) || !std::isfinite(aniso[a])) throw std::invalid_argument("anisotropy must be finite and positive");
+  if (dims < 2 && (vd.sy != 1 || vd.sz != 1)) throw std::invalid_argument("1D EDT of a volume");
+  if (dims < 3 && vd.sz != 1) throw std::invalid_argument("2D EDT of a volume");
+  cudaStream_t s = ctx.stream();
+  // x pass
+  std::vector<float> acc(vd.sx + 2, 0.0f);
+  for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + aniso[0];
+  Buffer<float> dacc = to_device(ctx, acc);
+  const size_t smem = size_t(kWarpsX) * vd.sx * sizeof(int);
+  if (smem > 200 * 1024) throw std::invalid_argument("x extent too large for the EDT x pass");
+  BK_CUDA(cudaFuncSetAttribute(edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long xlines = (long long)vd.sy * vd.sz;
+  const bool only_x = dims == 1 || (vd.sy == 1 && vd.sz == 1 && dims == 1);
+  edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(ids, D, d, dacc.data(),
+                                                                                black_border ? 1 : 0, only_x ? 1 : 0);
+  BK_CUDA(cudaGetLastError());
+  for (int axis = 1; axis < dims; ++axis) {
+    const int len = axis == 1 ? vd.sy : vd.sz;
+    const long long lines = axis == 1 ? (long long)vd.sx * vd.sz : (long long)vd.sx * vd.sy;
+    const long long budget = 512LL << 20;  // bytes of envelope stacks per batch
+    long long batch = std::max(1LL, std::min(lines, budget / (16LL * (len + 3))));
+    Buffer<int> V(ctx, batch * (len + 3));
+    Buffer<float> H(ctx, batch * (len + 3));
+    Buffer<double> Z(ctx, batch * (len + 3));
+    const int last = axis == dims - 1;
+    for (long long l0 = 0; l0 < lines; l0 += batch) {
+      const long long nb = std::min(batch, lines - l0);
+      edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, axis, aniso[axis], black_border ? 1 : 0, l0, nb,
+                                                      V.data(), H.data(), Z.data(), last);
+      BK_CUDA(cudaGetLastError());
+    }
+  }
+}
+
+}  // namespace bk

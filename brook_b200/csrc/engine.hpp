@@ -1,0 +1,81 @@
+// The object engine: persistent kernels in which one CTA owns one object at a time (objects are
+// pulled from a queue, largest first) and runs that object's whole sequential chain inside the
+// CTA, so that every round of a flood costs a block barrier instead of a grid barrier:
+//   prepare: root search flood + argmax, DAF flood + argmax, the object's PDRF, its root rail;
+//   trace:   target, railroad flood, warp backtrace with the dijkstra3d join, claim-order
+//            invalidation, rails, repeated until the object has no alive voxel left.
+// Objects never read or write another object's voxels (every step is gated by the same-id
+// neighbour mask), so concurrent CTAs need no synchronisation with one another.
+#pragma once
+#include <cstdint>
+
+namespace bk {
+
+constexpr int kEngineThreads = 512;
+
+// Per-voxel flag bits (uint32 per voxel, 0 at rest).
+constexpr unsigned kNearQueued = 1u;   // railroad / flood: in the next near list
+constexpr unsigned kFarQueued = 2u;    // railroad: on the far list
+constexpr unsigned kFront = 4u;        // invalidation: in the next frontier
+constexpr unsigned kWaiting = 8u;      // invalidation: on the waiting list
+
+enum EngineStatus : int {
+  kOk = 0,
+  kBudget = 1,        // a loop bound was reached (never expected; guards against hangs)
+  kNoRail = 2,        // no rail reachable from a target
+  kStoreFull = 3,     // path store region exhausted (cannot happen on a valid field)
+  kRecordsFull = 4,
+};
+
+struct EngineArgs {
+  // Arenas: volumes laid end to end in one flat index space (one arena per volume of a batch).
+  // Arena r starts at arena_offset[r] and has shape arena_dims[3r .. 3r+2]; a voxel's neighbours
+  // never leave its arena (the neighbour mask says so).
+  const int *arena_offset, *arena_dims;
+  const int *obj_arena;  // per object
+  const uint32_t *mask;  // same-id neighbour mask per voxel
+  const float *dbf;
+  float *pdrf;           // penalty; rails are 0
+  float *dist;           // railroad distances, +inf at rest
+  float *daf;            // DAF, +inf before prepare
+  uint32_t *flags;       // 0 at rest
+  uint8_t *alive;
+  unsigned long long *key;  // invalidation keys, all ones at rest
+
+  int nobj;
+  const int *obj_begin;  // offset of the object's voxels in vox and in the list pool
+  const int *obj_count;
+  const int *vox;        // voxels of every object, ascending flat index
+  const int *schedule;   // processing order (object indices)
+  int *queue;            // work counter (starts at 0)
+  int *status;           // per object
+  int *lists;            // 5 lists of F ints: list w of object o at lists + w * F + obj_begin[o]
+  unsigned long long *wide;  // F entries: object o at wide + obj_begin[o]
+  long long F;
+
+  // prepare
+  const int *border_root;  // per object: flat index, or -1 (search)
+  const float *M;          // per object: float(1 / dbf_max^1.01)
+  float pdrf_scale;
+  int squarings;
+  float w[26];             // geometric step weights
+  int *root, *target;
+  float *max_daf;
+
+  // trace
+  const int *order;            // target order of every object at obj_begin
+  const int *manual_begin, *manual_count, *manual;  // manual targets in pop order
+  const long long *max_paths;
+  int *store;                  // path vertices, target first
+  const long long *store_begin, *store_cap;
+  int *rec_start, *rec_len;    // per path: offset in the object's store region, length
+  const long long *rec_begin, *rec_cap;
+  int *npaths, *nstore;
+  float wx, wy, wz, scale, constant, delta;
+};
+
+void launch_prepare(const EngineArgs &a, int grid, cudaStream_t stream);
+void launch_trace(const EngineArgs &a, int grid, cudaStream_t stream);
+int engine_grid(int sm_count, int nobj, bool trace);
+
+}  // namespace bk

@@ -1,0 +1,440 @@
+// Orchestration of the skeletonizer over one flat index space that holds every volume of a call
+// (an arena per volume):
+//   per volume: connected components, boxes, EDT, neighbour masks, border targets, DBF maxima;
+//   every object of every volume at once: prepare (roots, DAF, PDRF), target orders, trace;
+//   assembly into packed skeletons per volume.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <stdexcept>
+
+#include "common.cuh"
+#include "engine.hpp"
+#include "order.hpp"
+#include "pipeline.hpp"
+
+namespace bk {
+namespace {
+
+template <class L>
+__global__ void filter_labels(const L *in, L *out, long long n, const long long *ids, int count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long v = (long long)in[i];
+  int lo = 0, hi = count;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (ids[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  out[i] = (lo < count && ids[lo] == v) ? in[i] : L(0);
+}
+
+__global__ void init_alive(const uint32_t *ids, const int *rank, long long n, uint8_t *alive) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t id = ids[i];
+  alive[i] = (id != 0 && rank[id] >= 0) ? 1 : 0;
+}
+
+__global__ void offset_voxels(int *vox, long long n, int offset) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) vox[i] += offset;
+}
+
+// Compacts the used prefix of every object's store region and gathers the DBF at each vertex.
+__global__ void gather_store(const int *store, const long long *store_begin, const long long *dst_begin,
+                             const int *nstore, int nobj, const float *dbf, int *out, float *radii) {
+  const int o = blockIdx.x;
+  if (o >= nobj) return;
+  const int n = nstore[o];
+  const int *src = store + store_begin[o];
+  const long long dst = dst_begin[o];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int v = src[i];
+    out[dst + i] = v;
+    radii[dst + i] = dbf[v];
+  }
+}
+
+__global__ void gather_records(const int *rs, const int *rl, const long long *rec_begin, const long long *dst_begin,
+                               const int *npaths, int nobj, int *out_start, int *out_len) {
+  const int o = blockIdx.x;
+  if (o >= nobj) return;
+  const int n = npaths[o];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    out_start[dst_begin[o] + i] = rs[rec_begin[o] + i];
+    out_len[dst_begin[o] + i] = rl[rec_begin[o] + i];
+  }
+}
+
+template <class L>
+Buffer<unsigned char> filtered(Context &ctx, const DeviceVolume &v, const std::vector<int64_t> &ids) {
+  std::vector<long long> sorted(ids.begin(), ids.end());
+  std::sort(sorted.begin(), sorted.end());
+  sorted.erase(std::unique(sorted.begin(), sorted.end()), sorted.end());
+  Buffer<long long> d = to_device(ctx, sorted);
+  Buffer<unsigned char> out(ctx, v.d.n() * sizeof(L));
+  filter_labels<L><<<blocks_for(v.d.n()), 256, 0, ctx.stream()>>>(static_cast<const L *>(v.data),
+                                                                  reinterpret_cast<L *>(out.data()), v.d.n(),
+                                                                  d.data(), (int)sorted.size());
+  BK_CUDA(cudaGetLastError());
+  return out;
+}
+
+Buffer<unsigned char> filter_volume(Context &ctx, const DeviceVolume &v, const std::vector<int64_t> &ids) {
+  switch (v.dtype) {
+    case U8: return filtered<uint8_t>(ctx, v, ids);
+    case U16: return filtered<uint16_t>(ctx, v, ids);
+    case U32: return filtered<uint32_t>(ctx, v, ids);
+    case U64: return filtered<uint64_t>(ctx, v, ids);
+    case I8: return filtered<int8_t>(ctx, v, ids);
+    case I16: return filtered<int16_t>(ctx, v, ids);
+    case I32: return filtered<int32_t>(ctx, v, ids);
+    case I64: return filtered<int64_t>(ctx, v, ids);
+    default: throw std::invalid_argument("integer labels required");
+  }
+}
+
+struct VolumeState {
+  VolumeDims d;
+  long long offset = 0;
+  ComponentsResult cc;
+  std::vector<Box> boxes;
+  std::vector<std::vector<Point>> borders;
+  std::vector<float> dbf_max;
+  std::vector<int> object_of;  // id -> global object index, -1 when inactive
+  bool empty = true;
+};
+
+// consolidate (skeleton.cpp:13-40 of the reference): unique vertices sorted by (x, y, z), edges
+// (min, max) sorted and unique, unused vertices dropped.
+struct Assembly {
+  std::vector<std::array<int, 3>> vox;
+  std::vector<float> radii;
+  std::vector<std::array<uint32_t, 2>> edges;
+};
+
+void consolidate(std::vector<std::array<int, 3>> &vertices, std::vector<float> &radii,
+                 std::vector<std::array<uint32_t, 2>> &edges, Assembly &out) {
+  out = Assembly{};
+  if (vertices.empty() || edges.empty()) return;
+  std::vector<uint32_t> order(vertices.size()), inverse(vertices.size());
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return vertices[a] < vertices[b]; });
+  std::vector<std::array<int, 3>> uniq;
+  std::vector<float> urad;
+  for (uint32_t old : order) {
+    if (uniq.empty() || uniq.back() != vertices[old]) { uniq.push_back(vertices[old]); urad.push_back(radii[old]); }
+    inverse[old] = uint32_t(uniq.size() - 1);
+  }
+  std::vector<std::array<uint32_t, 2>> e2;
+  e2.reserve(edges.size());
+  for (auto e : edges) {
+    std::array<uint32_t, 2> f{inverse[e[0]], inverse[e[1]]};
+    if (f[0] > f[1]) std::swap(f[0], f[1]);
+    if (f[0] != f[1]) e2.push_back(f);
+  }
+  std::sort(e2.begin(), e2.end());
+  e2.erase(std::unique(e2.begin(), e2.end()), e2.end());
+  std::vector<uint8_t> used(uniq.size(), 0);
+  for (auto e : e2) used[e[0]] = used[e[1]] = 1;
+  std::vector<uint32_t> remap(uniq.size(), 0);
+  for (size_t i = 0; i < uniq.size(); ++i)
+    if (used[i]) { remap[i] = uint32_t(out.vox.size()); out.vox.push_back(uniq[i]); out.radii.push_back(urad[i]); }
+  for (auto &e : e2) e = {remap[e[0]], remap[e[1]]};
+  out.edges = std::move(e2);
+}
+
+}  // namespace
+
+std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &volumes, const Options &opt) {
+  cudaStream_t s = ctx.stream();
+  const auto &t = opt.teasar;
+  for (float a : opt.anisotropy)
+    if (!std::isfinite(a) || a <= 0) throw std::invalid_argument("anisotropy must be finite and positive");
+  {
+    const double e = t.pdrf_exponent;
+    if (std::isfinite(e) && e == std::floor(e) && std::fmod(e, 2.0) == 1.0)
+      throw std::invalid_argument("odd pdrf_exponent makes the background penalty negative");
+  }
+  if (!opt.fix_branching) throw std::invalid_argument("fix_branching=False is not supported by this build");
+  if (!opt.targets_after.empty()) throw std::invalid_argument("extra_targets_after is not supported by this build");
+  const double exponent = t.pdrf_exponent;
+  if (!(exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))))
+    throw std::invalid_argument("pdrf_exponent must be a power of two in this build");
+  int squarings = 0;
+  for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+
+  std::vector<Packed> results(volumes.size());
+  for (auto &r : results) std::copy(opt.anisotropy.begin(), opt.anisotropy.end(), r.anisotropy.begin());
+  // ---- one flat index space for all volumes
+  std::vector<VolumeState> vs(volumes.size());
+  long long N = 0;
+  for (size_t v = 0; v < volumes.size(); ++v) {
+    vs[v].d = volumes[v].d;
+    vs[v].offset = N;
+    const long long n = volumes[v].d.n();
+    if (n > 0 && double(n) > opt.dust) { N += n; vs[v].empty = false; }
+  }
+  if (N >= (1LL << 31) - 1) throw std::invalid_argument("the volumes of one call must hold fewer than 2^31 voxels");
+  if (N == 0) return results;
+  Buffer<uint32_t> ids(ctx, N), mask(ctx, N);
+  Buffer<float> dbf(ctx, N);
+  const float aniso[3] = {opt.anisotropy[0], opt.anisotropy[1], opt.anisotropy[2]};
+  // ---- per-volume preamble
+  for (size_t v = 0; v < volumes.size(); ++v) {
+    auto &st = vs[v];
+    if (st.empty) continue;
+    const long long n = st.d.n();
+    uint32_t *vid = ids.data() + st.offset;
+    Buffer<unsigned char> masked;
+    const void *labels = volumes[v].data;
+    if (opt.object_ids) {
+      masked = filter_volume(ctx, volumes[v], *opt.object_ids);
+      labels = masked.data();
+    }
+    st.cc = connected_components(ctx, labels, volumes[v].dtype, st.d, vid);
+    const int64_t K = st.cc.count;
+    st.object_of.assign(K + 1, -1);
+    if (!K) { st.empty = true; continue; }
+    st.boxes = analyze(ctx, vid, st.d, K);
+    const bool black_border = K == 1 && st.boxes[1].count == n;
+    edt(ctx, vid, st.d, aniso, black_border, 3, dbf.data() + st.offset);
+    neighbour_mask(ctx, vid, st.d, mask.data() + st.offset);
+    st.borders.assign(K + 1, {});
+    if (opt.fix_borders) st.borders = border_targets(ctx, vid, st.d, K, aniso);
+    st.dbf_max = segment_max(ctx, dbf.data() + st.offset, vid, n, K);
+  }
+  // ---- objects: more voxels than dust and a bounding box of two or more voxels (batched.cu:187-191)
+  struct Object {
+    int volume;
+    uint32_t id;
+    int64_t count;
+  };
+  std::vector<Object> objects;
+  for (size_t v = 0; v < vs.size(); ++v) {
+    auto &st = vs[v];
+    if (st.empty) continue;
+    for (int64_t id = 1; id <= st.cc.count; ++id) {
+      const Box &b = st.boxes[id];
+      const long long bbox = (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
+      if (!b.count || double(b.count) <= opt.dust || bbox <= 1) continue;
+      if (double(st.dbf_max[id]) > t.soma_detection)
+        throw std::invalid_argument("objects with a soma (DBF maximum above soma_detection_threshold) are not supported by this build");
+      st.object_of[id] = int(objects.size());
+      objects.push_back({int(v), uint32_t(id), b.count});
+    }
+  }
+  const int nobj = int(objects.size());
+  if (nobj == 0) return results;
+  // per object: voxel range, arena, border root, manual targets, path budget, store regions
+  std::vector<int> obj_begin(nobj), obj_count(nobj), obj_arena(nobj), border_root(nobj, -1), seg_end(nobj);
+  std::vector<float> M(nobj);
+  std::vector<int> manual_begin(nobj), manual_count(nobj), manual;
+  std::vector<long long> max_paths(nobj), store_begin(nobj), store_cap(nobj), rec_begin(nobj), rec_cap(nobj);
+  long long F = 0, store_total = 0, rec_total = 0;
+  for (int o = 0; o < nobj; ++o) {
+    const auto &ob = objects[o];
+    const auto &st = vs[ob.volume];
+    obj_begin[o] = int(F);
+    obj_count[o] = int(ob.count);
+    F += ob.count;
+    seg_end[o] = int(F);
+    obj_arena[o] = ob.volume;
+    M[o] = float(1.0 / std::pow(double(st.dbf_max[ob.id]), 1.01));
+    const auto &b = st.borders[ob.id];
+    auto flat = [&](const Point &p) { return int(st.offset + p[0] + (long long)st.d.sx * (p[1] + (long long)st.d.sy * p[2])); };
+    if (!b.empty()) border_root[o] = flat(b.back());
+    // manual targets in pop order: the border points except the last (the root), last first;
+    // none: the object's own target (-1, resolved on the device)
+    manual_begin[o] = int(manual.size());
+    if (b.size() > 1) for (size_t i = b.size() - 1; i-- > 0;) manual.push_back(flat(b[i]));
+    else if (b.size() <= 1) manual.push_back(-1);
+    manual_count[o] = int(manual.size()) - manual_begin[o];
+    const int64_t budget = t.max_paths.value_or(ob.count);
+    max_paths[o] = manual_count[o] >= budget ? 0 : budget;
+    store_begin[o] = store_total;
+    store_cap[o] = 2 * ob.count + manual_count[o] + 2;
+    store_total += store_cap[o];
+    rec_begin[o] = rec_total;
+    rec_cap[o] = ob.count + manual_count[o] + 1;
+    rec_total += rec_cap[o];
+  }
+  if (!opt.targets_before.empty()) throw std::invalid_argument("extra_targets_before is not supported by this build");
+  if (F >= (1LL << 31)) throw std::invalid_argument("too many foreground voxels");
+  // object voxel lists, volume by volume into their ranges
+  Buffer<int> vox(ctx, F);
+  for (size_t v = 0; v < vs.size(); ++v) {
+    auto &st = vs[v];
+    if (st.empty) continue;
+    int first = -1, cnt = 0;
+    long long total = 0;
+    for (int64_t id = 1; id <= st.cc.count; ++id)
+      if (st.object_of[id] >= 0) {
+        if (first < 0) first = st.object_of[id];
+        ++cnt;
+        total += obj_count[st.object_of[id]];
+      }
+    if (cnt == 0) continue;
+    std::vector<int> rank(st.cc.count + 1, -1);
+    for (int64_t id = 1; id <= st.cc.count; ++id)
+      if (st.object_of[id] >= 0) rank[id] = st.object_of[id] - first;
+    Buffer<int> drank = to_device(ctx, rank);
+    Buffer<int> local = object_voxels(ctx, ids.data() + st.offset, st.d.n(), drank.data(), cnt, total);
+    offset_voxels<<<blocks_for(total), 256, 0, s>>>(local.data(), total, int(st.offset));
+    BK_CUDA(cudaMemcpyAsync(vox.data() + obj_begin[first], local.data(), total * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  }
+  // global per-voxel state
+  Buffer<float> pdrf(ctx, N), dist(ctx, N), daf(ctx, N);
+  Buffer<uint32_t> flags(ctx, N);
+  Buffer<uint8_t> alive(ctx, N);
+  Buffer<unsigned long long> key(ctx, N);
+  fill_float(ctx, pdrf.data(), N, INFINITY);
+  fill_float(ctx, dist.data(), N, INFINITY);
+  fill_float(ctx, daf.data(), N, INFINITY);
+  flags.zero();
+  alive.zero();
+  key.fill_bytes(0xFF);
+  {
+    // alive: voxels of objects
+    std::vector<int> active_rank;
+    for (size_t v = 0; v < vs.size(); ++v) {
+      auto &st = vs[v];
+      if (st.empty) continue;
+      std::vector<int> r(st.cc.count + 1, -1);
+      for (int64_t id = 1; id <= st.cc.count; ++id) r[id] = st.object_of[id];
+      Buffer<int> dr = to_device(ctx, r);
+      init_alive<<<blocks_for(st.d.n()), 256, 0, s>>>(ids.data() + st.offset, dr.data(), st.d.n(), alive.data() + st.offset);
+      BK_CUDA(cudaGetLastError());
+    }
+  }
+  std::vector<int> arena_offset(vs.size()), arena_dims(3 * vs.size());
+  for (size_t v = 0; v < vs.size(); ++v) {
+    arena_offset[v] = int(vs[v].offset);
+    arena_dims[3 * v] = vs[v].d.sx; arena_dims[3 * v + 1] = vs[v].d.sy; arena_dims[3 * v + 2] = vs[v].d.sz;
+  }
+  std::vector<int> schedule(nobj);
+  std::iota(schedule.begin(), schedule.end(), 0);
+  std::stable_sort(schedule.begin(), schedule.end(), [&](int a, int b) { return obj_count[a] > obj_count[b]; });
+  auto d_arena_offset = to_device(ctx, arena_offset), d_arena_dims = to_device(ctx, arena_dims);
+  auto d_obj_arena = to_device(ctx, obj_arena), d_obj_begin = to_device(ctx, obj_begin), d_obj_count = to_device(ctx, obj_count);
+  auto d_seg_end = to_device(ctx, seg_end), d_schedule = to_device(ctx, schedule), d_border_root = to_device(ctx, border_root);
+  auto d_M = to_device(ctx, M);
+  auto d_manual_begin = to_device(ctx, manual_begin), d_manual_count = to_device(ctx, manual_count);
+  auto d_manual = to_device(ctx, manual.empty() ? std::vector<int>{0} : manual);
+  auto d_max_paths = to_device(ctx, max_paths), d_store_begin = to_device(ctx, store_begin), d_store_cap = to_device(ctx, store_cap);
+  auto d_rec_begin = to_device(ctx, rec_begin), d_rec_cap = to_device(ctx, rec_cap);
+  Buffer<int> queue(ctx, 2), status(ctx, nobj), root(ctx, nobj), target(ctx, nobj), npaths(ctx, nobj), nstore(ctx, nobj);
+  Buffer<float> max_daf(ctx, nobj);
+  Buffer<int> lists(ctx, 5 * F), store(ctx, store_total), rec_start(ctx, rec_total), rec_len(ctx, rec_total);
+  Buffer<unsigned long long> wide(ctx, F);
+  queue.zero();
+  status.zero();
+
+  EngineArgs a{};
+  a.arena_offset = d_arena_offset.data(); a.arena_dims = d_arena_dims.data(); a.obj_arena = d_obj_arena.data();
+  a.mask = mask.data(); a.dbf = dbf.data(); a.pdrf = pdrf.data(); a.dist = dist.data(); a.daf = daf.data();
+  a.flags = flags.data(); a.alive = alive.data(); a.key = key.data();
+  a.nobj = nobj; a.obj_begin = d_obj_begin.data(); a.obj_count = d_obj_count.data(); a.vox = vox.data();
+  a.schedule = d_schedule.data(); a.queue = queue.data(); a.status = status.data();
+  a.lists = lists.data(); a.wide = wide.data(); a.F = F;
+  a.border_root = d_border_root.data(); a.M = d_M.data(); a.pdrf_scale = float(t.pdrf_scale); a.squarings = squarings;
+  {
+    const double x = aniso[0], y = aniso[1], z = aniso[2];
+    const double pairs[3] = {std::sqrt(x * x + y * y), std::sqrt(y * y + z * z), std::sqrt(x * x + z * z)};
+    for (int k = 0; k < 6; ++k) a.w[k] = aniso[k / 2];
+    for (int k = 6; k < 18; ++k) a.w[k] = float(pairs[(k - 6) / 4]);
+    for (int k = 18; k < 26; ++k) a.w[k] = float(std::sqrt(x * x + y * y + z * z));
+  }
+  a.root = root.data(); a.target = target.data(); a.max_daf = max_daf.data();
+  a.manual_begin = d_manual_begin.data(); a.manual_count = d_manual_count.data(); a.manual = d_manual.data();
+  a.max_paths = d_max_paths.data(); a.store = store.data(); a.store_begin = d_store_begin.data(); a.store_cap = d_store_cap.data();
+  a.rec_start = rec_start.data(); a.rec_len = rec_len.data(); a.rec_begin = d_rec_begin.data(); a.rec_cap = d_rec_cap.data();
+  a.npaths = npaths.data(); a.nstore = nstore.data();
+  a.wx = aniso[0]; a.wy = aniso[1]; a.wz = aniso[2];
+  a.scale = float(t.scale); a.constant = float(t.constant);
+  a.delta = std::min({aniso[0], aniso[1], aniso[2]});
+
+  launch_prepare(a, engine_grid(ctx.sm_count(), nobj, false), s);
+  Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), d_seg_end.data(), nobj);
+  a.order = order.data();
+  BK_CUDA(cudaMemsetAsync(queue.data(), 0, sizeof(int), s));
+  launch_trace(a, engine_grid(ctx.sm_count(), nobj, true), s);
+
+  // ---- results
+  const auto st_host = status.download();
+  for (int o = 0; o < nobj; ++o)
+    if (st_host[o] != kOk) {
+      static const char *what[] = {"ok", "a loop bound was reached", "no rail reachable from a target", "path store full",
+                                   "path records full"};
+      throw std::runtime_error(std::string("tracing failed: ") + what[std::min(st_host[o], 4)]);
+    }
+  const auto np = npaths.download(), ns = nstore.download();
+  std::vector<long long> vdst(nobj), rdst(nobj);
+  long long vt = 0, rt = 0;
+  for (int o = 0; o < nobj; ++o) { vdst[o] = vt; vt += ns[o]; rdst[o] = rt; rt += np[o]; }
+  Buffer<int> cstore(ctx, std::max(vt, 1LL)), cstart(ctx, std::max(rt, 1LL)), clen(ctx, std::max(rt, 1LL));
+  Buffer<float> cradii(ctx, std::max(vt, 1LL));
+  auto d_vdst = to_device(ctx, vdst), d_rdst = to_device(ctx, rdst);
+  gather_store<<<nobj, 256, 0, s>>>(store.data(), d_store_begin.data(), d_vdst.data(), nstore.data(), nobj, dbf.data(),
+                                    cstore.data(), cradii.data());
+  gather_records<<<nobj, 256, 0, s>>>(rec_start.data(), rec_len.data(), d_rec_begin.data(), d_rdst.data(), npaths.data(),
+                                      nobj, cstart.data(), clen.data());
+  BK_CUDA(cudaGetLastError());
+  const auto hstore = cstore.download(vt), hstart = cstart.download(rt), hlen = clen.download(rt);
+  const auto hrad = cradii.download(vt);
+  // per volume: skeletons per original label, components merged in id order
+  for (size_t v = 0; v < vs.size(); ++v) {
+    auto &st = vs[v];
+    if (st.empty) continue;
+    Packed &out = results[v];
+    std::vector<int64_t> label_order;
+    std::vector<std::vector<int>> label_objects;
+    for (int64_t id = 1; id <= st.cc.count; ++id) {
+      const int o = st.object_of[id];
+      if (o < 0) continue;
+      bool has_edge = false;
+      for (int p = 0; p < np[o]; ++p) has_edge |= hlen[rdst[o] + p] >= 2;
+      if (!has_edge) continue;
+      const int64_t label = st.cc.mapping[id];
+      auto it = std::find(label_order.begin(), label_order.end(), label);
+      if (it == label_order.end()) { label_order.push_back(label); label_objects.push_back({o}); }
+      else label_objects[it - label_order.begin()].push_back(o);
+    }
+    for (size_t j = 0; j < label_order.size(); ++j) {
+      std::vector<std::array<int, 3>> verts;
+      std::vector<float> rad;
+      std::vector<std::array<uint32_t, 2>> edges;
+      for (int o : label_objects[j])
+        for (int p = 0; p < np[o]; ++p) {
+          const int len = hlen[rdst[o] + p];
+          if (len < 2) continue;
+          const long long base = vdst[o] + hstart[rdst[o] + p];
+          const uint32_t first = uint32_t(verts.size());
+          for (int q = 0; q < len; ++q) {
+            long long g = hstore[base + q] - st.offset;
+            const int z = int(g / ((long long)st.d.sx * st.d.sy));
+            g -= (long long)z * st.d.sx * st.d.sy;
+            const int y = int(g / st.d.sx), x = int(g - (long long)y * st.d.sx);
+            verts.push_back({x, y, z});
+            rad.push_back(hrad[base + q]);
+            if (q) edges.push_back({first + q - 1, first + q});
+          }
+        }
+      Assembly asmb;
+      consolidate(verts, rad, edges, asmb);
+      if (asmb.edges.empty()) continue;
+      out.labels.push_back(label_order[j]);
+      for (size_t i = 0; i < asmb.vox.size(); ++i) {
+        for (int c = 0; c < 3; ++c) out.vertices.push_back(float(asmb.vox[i][c]) * opt.anisotropy[c]);
+        out.radii.push_back(asmb.radii[i]);
+      }
+      for (auto e : asmb.edges) { out.edges.push_back(e[0]); out.edges.push_back(e[1]); }
+      out.vertex_offsets.push_back(int64_t(out.radii.size()));
+      out.edge_offsets.push_back(int64_t(out.edges.size() / 2));
+    }
+  }
+  return results;
+}
+
+}  // namespace bk

@@ -1,0 +1,48 @@
+// Skeletonization of one or several label volumes (the reference's skeletonize / skeletonize_batch,
+// skeletonize.cu:184-198 and batch.cu:430-515 of giorgioangel/brook).
+#pragma once
+#include <array>
+#include <cstdint>
+#include <optional>
+#include <vector>
+
+#include "kernels.hpp"
+
+namespace bk {
+
+// TEASAR parameters; keys a caller leaves out take kimimaro.trace's defaults (skeleton.hpp:23-27).
+struct Teasar {
+  double scale = 10, constant = 10, pdrf_scale = 5000, pdrf_exponent = 16;
+  double soma_detection = 1100, soma_acceptance = 4000, soma_scale = 0.5, soma_constant = 0;
+  std::optional<int64_t> max_paths;
+};
+
+struct Options {
+  Teasar teasar;
+  std::array<float, 3> anisotropy{1, 1, 1};
+  double dust = 1000;
+  bool fix_branching = true, fix_borders = true;
+  std::optional<std::vector<int64_t>> object_ids;
+  std::vector<Point> targets_before, targets_after;
+};
+
+// Packed skeletons of one volume: skeleton k has label labels[k], vertices
+// [vertex_offsets[k], vertex_offsets[k+1]) (x, y, z physical, row major), the same range of
+// radii, and edges [edge_offsets[k], edge_offsets[k+1]) local to the skeleton.
+struct Packed {
+  std::vector<int64_t> labels, vertex_offsets{0}, edge_offsets{0};
+  std::vector<float> vertices, radii;
+  std::vector<uint32_t> edges;
+  std::array<float, 3> anisotropy{1, 1, 1};
+};
+
+// A label volume already on the device, Fortran-ordered (x fastest), borrowed for the call.
+struct DeviceVolume {
+  const void *data = nullptr;
+  int dtype = U32;
+  VolumeDims d;
+};
+
+std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &volumes, const Options &options);
+
+}  // namespace bk

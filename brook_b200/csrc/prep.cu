@@ -1,0 +1,132 @@
+// Preamble kernels: per-component boxes and counts, the neighbour masks every later stage steps
+// through, per-component maxima, fills and face extraction.
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace bk {
+namespace {
+
+// Boxes and counts in one pass (the reference's analyze, preamble.cu:10-29): a run start along x
+// updates the box, a run end its x maximum, and each warp adds its voxels of one id with one
+// atomic (match + popc).
+__global__ void analyze_kernel(const uint32_t *__restrict__ ids, Dims d, int *lo, int *hi, unsigned long long *counts) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = i < d.n();
+  const uint32_t id = in ? ids[i] : 0u;
+  const unsigned peers = __match_any_sync(0xFFFFFFFFu, id);
+  const int leader = __ffs(peers) - 1;
+  if (id != 0 && (threadIdx.x & 31) == leader) atomicAdd(counts + id, (unsigned long long)__popc(peers));
+  if (!in || id == 0) return;
+  int x, y, z;
+  unravel((int)i, d, x, y, z);
+  const bool first = x == 0 || ids[i - 1] != id;
+  const bool last = x == d.sx - 1 || ids[i + 1] != id;
+  int *l = lo + 3 * (long long)id, *h = hi + 3 * (long long)id;
+  if (first) {
+    if (__ldcg(l) > x) atomicMin(l, x);
+    if (__ldcg(l + 1) > y) atomicMin(l + 1, y);
+    if (__ldcg(h + 1) < y) atomicMax(h + 1, y);
+    if (__ldcg(l + 2) > z) atomicMin(l + 2, z);
+    if (__ldcg(h + 2) < z) atomicMax(h + 2, z);
+  }
+  if (last && __ldcg(h) < x) atomicMax(h, x);
+}
+
+__global__ void mask_kernel(const uint32_t *__restrict__ ids, Dims d, uint32_t *__restrict__ mask) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n()) return;
+  const uint32_t id = ids[i];
+  uint32_t m = 0;
+  if (id) {
+    int x, y, z;
+    unravel((int)i, d, x, y, z);
+#pragma unroll
+    for (int k = 0; k < 26; ++k) {
+      const int nx = x + c_dx[k], ny = y + c_dy[k], nz = z + c_dz[k];
+      if (nx < 0 || ny < 0 || nz < 0 || nx >= d.sx || ny >= d.sy || nz >= d.sz) continue;
+      if (ids[i + nbr_offset(k, d)] == id) m |= 1u << k;
+    }
+  }
+  mask[i] = m;
+}
+
+__global__ void segmax_kernel(const float *__restrict__ f, const uint32_t *__restrict__ ids, long long n, unsigned *best) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = i < n;
+  const uint32_t id = in ? ids[i] : 0u;
+  const float v = in ? f[i] : 0.0f;
+  const unsigned bits = (id != 0 && v < __uint_as_float(BK_INF_BITS)) ? __float_as_uint(v) : 0u;
+  const unsigned peers = __match_any_sync(0xFFFFFFFFu, id);
+  const unsigned top = __reduce_max_sync(peers, bits);  // the largest bits of this warp's voxels of the id
+  if (id != 0 && (threadIdx.x & 31) == __ffs(peers) - 1 && __ldcg(best + id) < top) atomicMax(best + id, top);
+}
+
+__global__ void fill_kernel(float *p, long long n, float v) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+__global__ void face_kernel(const uint32_t *__restrict__ ids, Dims d, int a, int b, int c, int fixed, uint32_t *plane) {
+  const int shape[3] = {d.sx, d.sy, d.sz};
+  const long long fx = shape[a], fy = shape[b];
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= fx * fy) return;
+  int p[3];
+  p[a] = (int)(i / fy);
+  p[b] = (int)(i % fy);
+  p[c] = fixed;
+  plane[i] = ids[p[0] + (long long)d.sx * (p[1] + (long long)d.sy * p[2])];
+}
+
+}  // namespace
+
+std::vector<Box> analyze(Context &ctx, const uint32_t *ids, VolumeDims vd, int64_t count) {
+  const Dims d{vd.sx, vd.sy, vd.sz};
+  std::vector<int> lo(3 * (count + 1), INT32_MAX), hi(3 * (count + 1), -1);
+  Buffer<int> dlo = to_device(ctx, lo), dhi = to_device(ctx, hi);
+  Buffer<unsigned long long> counts(ctx, count + 1);
+  counts.zero();
+  analyze_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, d, dlo.data(), dhi.data(), counts.data());
+  BK_CUDA(cudaGetLastError());
+  lo = dlo.download();
+  hi = dhi.download();
+  auto c = counts.download();
+  std::vector<Box> boxes(count + 1);
+  for (int64_t id = 0; id <= count; ++id) {
+    for (int a = 0; a < 3; ++a) { boxes[id].lo[a] = lo[3 * id + a]; boxes[id].hi[a] = hi[3 * id + a]; }
+    boxes[id].count = (int64_t)c[id];
+  }
+  return boxes;
+}
+
+void neighbour_mask(Context &ctx, const uint32_t *ids, VolumeDims vd, uint32_t *out) {
+  if (vd.n() <= 0) return;
+  mask_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, out);
+  BK_CUDA(cudaGetLastError());
+}
+
+std::vector<float> segment_max(Context &ctx, const float *field, const uint32_t *ids, long long n, int64_t count) {
+  Buffer<unsigned> best(ctx, count + 1);
+  best.zero();
+  segmax_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(field, ids, n, best.data());
+  BK_CUDA(cudaGetLastError());
+  auto bits = best.download();
+  std::vector<float> out(count + 1);
+  std::memcpy(out.data(), bits.data(), bits.size() * sizeof(float));
+  return out;
+}
+
+void fill_float(Context &ctx, float *p, long long n, float value) {
+  if (n <= 0) return;
+  fill_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(p, n, value);
+  BK_CUDA(cudaGetLastError());
+}
+
+void extract_face(Context &ctx, const uint32_t *ids, VolumeDims vd, int a, int b, int c, int fixed, uint32_t *plane) {
+  const int shape[3] = {vd.sx, vd.sy, vd.sz};
+  const long long n = (long long)shape[a] * shape[b];
+  face_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, a, b, c, fixed, plane);
+  BK_CUDA(cudaGetLastError());
+}
+
+}  // namespace bk

@@ -1,0 +1,127 @@
+// Host runtime of brook_b200: one context per device with one non-blocking stream, stream-ordered
+// allocations from the device's memory pool, typed device buffers and the error types the C ABI
+// maps to status codes.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace bk {
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const std::string &where)
+      : std::runtime_error(where + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+#define BK_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t bk_status_ = (call);                                                         \
+    if (bk_status_ != cudaSuccess) throw ::bk::CudaError(bk_status_, #call);                 \
+  } while (0)
+
+// Restores the caller's current device when a public call returns.
+class DeviceGuard {
+  int previous_ = -1;
+
+ public:
+  explicit DeviceGuard(int device) {
+    BK_CUDA(cudaGetDevice(&previous_));
+    if (previous_ != device) BK_CUDA(cudaSetDevice(device));
+  }
+  ~DeviceGuard() {
+    if (previous_ >= 0) cudaSetDevice(previous_);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
+class Context {
+ public:
+  explicit Context(int device);
+  ~Context();
+  Context(const Context &) = delete;
+  Context &operator=(const Context &) = delete;
+
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+  int sm_count() const { return sm_count_; }
+  void synchronize() const { BK_CUDA(cudaStreamSynchronize(stream_)); }
+  void *allocate(size_t bytes);
+  void release(void *p);
+  std::mutex &mutex() { return mutex_; }
+  std::map<std::string, double> stats;
+
+ private:
+  int device_ = 0, sm_count_ = 0;
+  cudaStream_t stream_ = nullptr;
+  std::mutex mutex_;
+};
+
+// A typed stream-ordered device allocation owned by one context.
+template <class T>
+class Buffer {
+  Context *ctx_ = nullptr;
+  T *ptr_ = nullptr;
+  size_t count_ = 0;
+
+ public:
+  Buffer() = default;
+  Buffer(Context &ctx, size_t count) : ctx_(&ctx), count_(count) {
+    if (count) ptr_ = static_cast<T *>(ctx.allocate(count * sizeof(T)));
+  }
+  ~Buffer() { reset(); }
+  Buffer(Buffer &&o) noexcept : ctx_(o.ctx_), ptr_(o.ptr_), count_(o.count_) { o.ptr_ = nullptr; o.count_ = 0; }
+  Buffer &operator=(Buffer &&o) noexcept {
+    if (this != &o) { reset(); ctx_ = o.ctx_; ptr_ = o.ptr_; count_ = o.count_; o.ptr_ = nullptr; o.count_ = 0; }
+    return *this;
+  }
+  Buffer(const Buffer &) = delete;
+  Buffer &operator=(const Buffer &) = delete;
+  void reset() {
+    if (ptr_ && ctx_) ctx_->release(ptr_);
+    ptr_ = nullptr;
+    count_ = 0;
+  }
+  T *data() const { return ptr_; }
+  size_t size() const { return count_; }
+  size_t bytes() const { return count_ * sizeof(T); }
+  void zero() const {
+    if (count_) BK_CUDA(cudaMemsetAsync(ptr_, 0, bytes(), ctx_->stream()));
+  }
+  void fill_bytes(int value) const {
+    if (count_) BK_CUDA(cudaMemsetAsync(ptr_, value, bytes(), ctx_->stream()));
+  }
+  void upload(const T *host, size_t n, size_t offset = 0) const {
+    if (n) BK_CUDA(cudaMemcpyAsync(ptr_ + offset, host, n * sizeof(T), cudaMemcpyHostToDevice, ctx_->stream()));
+  }
+  void upload(const std::vector<T> &host) const { upload(host.data(), host.size()); }
+  // Synchronous download of the first n elements.
+  std::vector<T> download(size_t n, size_t offset = 0) const {
+    std::vector<T> out(n);
+    if (n) {
+      BK_CUDA(cudaMemcpyAsync(out.data(), ptr_ + offset, n * sizeof(T), cudaMemcpyDeviceToHost, ctx_->stream()));
+      ctx_->synchronize();
+    }
+    return out;
+  }
+  std::vector<T> download() const { return download(count_); }
+};
+
+template <class T>
+Buffer<T> to_device(Context &ctx, const std::vector<T> &host) {
+  Buffer<T> b(ctx, host.size());
+  b.upload(host);
+  return b;
+}
+
+inline unsigned blocks_for(long long n, int threads = 256) { return static_cast<unsigned>((n + threads - 1) / threads); }
+
+}  // namespace bk

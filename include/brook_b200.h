@@ -1,0 +1,146 @@
+/* brook_b200 C ABI: the skeletonization entry points of giorgioangel/brook's C SDK
+ * (cpp/include/brook/brook.h), implemented for NVIDIA B200 (sm_100a).
+ *
+ * Structures, enumerations and function names are the reference's, so that a consumer of the
+ * reference's C API for this path links against libbrook_b200.so instead. Every declaration below
+ * names the reference declaration it replaces. Calls block; errors return a brook_status and
+ * brook_last_error() holds the text (thread-local, valid until the next call on that thread).
+ * Volumes are indexed (x, y, z) with byte strides; the library works on Fortran-ordered copies.
+ */
+#ifndef BROOK_B200_H
+#define BROOK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* brook.h:15 */
+#define BROOK_ABI_VERSION 1u
+
+typedef struct brook_context brook_context;     /* brook.h:17 */
+typedef struct brook_array brook_array;         /* brook.h:18 */
+typedef struct brook_components brook_components; /* brook.h:19 */
+typedef struct brook_skeletons brook_skeletons; /* brook.h:21 */
+
+/* brook.h:26-29 */
+typedef enum brook_status {
+  BROOK_SUCCESS = 0, BROOK_INVALID_ARGUMENT = 1, BROOK_OUT_OF_MEMORY = 2,
+  BROOK_CUDA_ERROR = 3, BROOK_INTERNAL_ERROR = 4
+} brook_status;
+
+/* brook.h:31-35 */
+typedef enum brook_dtype {
+  BROOK_U8 = 0, BROOK_U16 = 1, BROOK_U32 = 2, BROOK_U64 = 3,
+  BROOK_I8 = 4, BROOK_I16 = 5, BROOK_I32 = 6, BROOK_I64 = 7,
+  BROOK_F32 = 8, BROOK_F64 = 9
+} brook_dtype;
+
+/* brook.h:37 */
+typedef enum brook_memory { BROOK_HOST = 0, BROOK_DEVICE = 1 } brook_memory;
+
+/* brook.h:42-50: data points to logical (0,0,0); byte strides (host strides may be negative).
+ * Zero-initialize and set struct_size/abi_version. Input is borrowed for the call; device input
+ * must be on the context's device and ready before the call. */
+typedef struct brook_volume {
+  size_t struct_size;
+  uint32_t abi_version;
+  const void *data;
+  int64_t shape[3];
+  int64_t strides[3];
+  brook_dtype dtype;
+  brook_memory memory;
+} brook_volume;
+
+/* brook.h:52-58 */
+typedef struct brook_teasar_parameters {
+  double scale, constant, pdrf_scale, pdrf_exponent;
+  double soma_detection_threshold, soma_acceptance_threshold;
+  double soma_invalidation_scale, soma_invalidation_const;
+  int64_t max_paths;
+  uint32_t has_max_paths;
+} brook_teasar_parameters;
+
+/* brook.h:60-67 */
+enum brook_skeletonize_flags {
+  BROOK_FIX_BRANCHING = 1u, BROOK_FIX_BORDERS = 2u, BROOK_FILTER_OBJECTS = 4u,
+  BROOK_DEVICE_OUTPUT = 8u, BROOK_FILL_HOLES = 16u, BROOK_FIX_AVOCADOS = 32u
+};
+
+/* brook.h:68-84 */
+typedef struct brook_skeletonize_options {
+  size_t struct_size;
+  uint32_t abi_version;
+  brook_teasar_parameters teasar;
+  float anisotropy[3];
+  double dust_threshold;
+  uint32_t flags;
+  const int64_t *object_ids;
+  size_t object_ids_count;
+  const int64_t *targets_before;
+  size_t targets_before_count;
+  const int64_t *targets_after;
+  size_t targets_after_count;
+  const brook_volume *voxel_graph;
+} brook_skeletonize_options;
+
+/* brook.h:86-95: host packed result. Offsets have skeleton_count+1 entries; edge indices are
+ * local to each skeleton; vertices row major, physical coordinates. */
+typedef struct brook_skeletons_view {
+  size_t skeleton_count, vertex_count, edge_count;
+  const int64_t *labels, *vertex_offsets, *edge_offsets;
+  const float *vertices;
+  const uint32_t *edges;
+  const float *radii;
+  float anisotropy[3];
+} brook_skeletons_view;
+
+uint32_t brook_abi_version(void);       /* brook.h:147 */
+const char *brook_version(void);        /* brook.h:148 */
+const char *brook_last_error(void);     /* brook.h:150 */
+
+/* brook.h:154: device >= 0 and a Blackwell (compute capability 10.x) GPU. */
+brook_status brook_context_create(int device, brook_context **out);
+void brook_context_destroy(brook_context *context);              /* brook.h:155 */
+brook_status brook_context_synchronize(brook_context *context);  /* brook.h:156 */
+
+/* brook.h:159-162: device arrays owned by the handle */
+void brook_array_destroy(brook_array *array);
+brook_status brook_array_view(const brook_array *array, brook_volume *out);
+brook_status brook_array_copy_to_host(const brook_array *array, void *out, size_t bytes);
+
+/* brook.h:169-177: 26-connected components; ids 1..K by ascending first voxel (Fortran order),
+ * stored in the narrowest unsigned type that holds K. */
+brook_status brook_connected_components(brook_context *context, const brook_volume *labels,
+                                        brook_components **out);
+void brook_components_destroy(brook_components *components);
+brook_status brook_components_view(const brook_components *components, brook_volume *labels,
+                                   const int64_t **mapping, const int64_t **roots, size_t *count);
+brook_status brook_components_copy_to_host(const brook_components *components, void *out, size_t bytes);
+
+/* brook.h:180-181: anisotropic distance to the nearest voxel of another label (float32). */
+brook_status brook_edt(brook_context *context, const brook_volume *labels, const float anisotropy[3],
+                       int black_border, brook_array **out);
+
+/* brook.h:201-203: defaults of the Python skeletonize() (DEFAULT_TEASAR_PARAMS, dust 1000,
+ * fix_branching and fix_borders). */
+void brook_skeletonize_options_init(brook_skeletonize_options *options);
+brook_status brook_skeletonize(brook_context *context, const brook_volume *labels,
+                               const brook_skeletonize_options *options, brook_skeletons **out);
+
+/* The C form of the reference's Python skeletonize_batch (src/brook/batch.py:193; its C++ form
+ * brook::skeletonize_batch, batch.cu:430): `count` volumes traced in one pass of the object
+ * engine; out receives `count` result handles (one per volume, in input order). */
+brook_status brook_skeletonize_batch(brook_context *context, const brook_volume *volumes, size_t count,
+                                     const brook_skeletonize_options *options, brook_skeletons **out);
+
+/* brook.h:238-252 */
+brook_status brook_skeletons_get_view(const brook_skeletons *result, brook_skeletons_view *out);
+void brook_skeletons_destroy(brook_skeletons *result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,242 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and the reference's known answers.
+
+Integer/index results (vertices, edges, labels, offsets) must be identical; radii are compared
+bit-exactly too (both sides compute the same float32 EDT)."""
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+
+import shapes
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "join_digests.json")))
+CFG0_PARAMS = dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_exponent=4)
+
+
+def bk():
+    import brook_b200
+
+    return brook_b200
+
+
+def assert_same(packed, expected, what=""):
+    """packed (brook_b200 PackedSkeletons) equals the oracle's packed result exactly."""
+    e = expected.packed()
+    np.testing.assert_array_equal(packed.labels, e["labels"], err_msg=f"labels {what}")
+    np.testing.assert_array_equal(packed.v_off, e["vertex_offsets"], err_msg=f"vertex offsets {what}")
+    np.testing.assert_array_equal(packed.e_off, e["edge_offsets"], err_msg=f"edge offsets {what}")
+    np.testing.assert_array_equal(packed.vertices, e["vertices"], err_msg=f"vertices {what}")
+    np.testing.assert_array_equal(packed.edges, e["edges"], err_msg=f"edges {what}")
+    np.testing.assert_array_equal(packed.radii.view(np.uint32), e["radii"].view(np.uint32), err_msg=f"radii {what}")
+
+
+def run_both(labels, threads=8, **options):
+    got = bk().skeletonize(labels, output="packed", **options)
+    exp = oracle.skeletonize(labels, threads=threads, **options)
+    return got, exp
+
+
+@pytest.mark.parametrize("case", sorted(shapes.CASES))
+@pytest.mark.parametrize("layout", [np.ascontiguousarray, np.asfortranarray])
+def test_join_digests(gpu, case, layout):
+    make, extra = shapes.CASES[case]
+    opts = dict(shapes.JOIN_OPTIONS, **extra)
+    result = bk().skeletonize(layout(make()), output="packed", **opts)
+    summary = shapes.summary({int(l): (s.vertices, s.edges, s.radii) for l, s in result.to_skeletons().items()})
+    assert summary == {int(k): v for k, v in GOLDEN[case].items()}
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_tubes_match_oracle(gpu, seed):
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((64, 64, 64), objects=8, seed=seed)
+    got, exp = run_both(labels, teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    assert len(got) > 0
+    assert_same(got, exp, f"seed {seed}")
+
+
+def test_cfg0_full_size_matches_oracle(gpu):
+    """The 128^3 uint32 volume of 20 random-walk tubes (seed 0), anisotropy (16,16,40)."""
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((128, 128, 128), objects=20, seed=0)
+    got, exp = run_both(labels, teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    assert len(got) == 20
+    assert_same(got, exp, "cfg0")
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16, np.uint64, np.int32, np.int64])
+def test_dtypes(gpu, dtype):
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((48, 40, 36), objects=6, seed=7, radius=(1.5, 4.0)).astype(dtype)
+    got, exp = run_both(labels, teasar_params=dict(scale=1.0, const=2.0), anisotropy=(4, 4, 4), dust_threshold=20)
+    assert_same(got, exp, str(np.dtype(dtype)))
+
+
+@pytest.mark.parametrize("aniso", [(1, 1, 1), (4, 4, 4), (8, 8, 40), (16, 16, 40)])
+def test_anisotropies(gpu, aniso):
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((40, 56, 48), objects=5, seed=3, radius=(1.5, 5.0))
+    got, exp = run_both(labels, teasar_params=CFG0_PARAMS, anisotropy=aniso, dust_threshold=50)
+    assert_same(got, exp, str(aniso))
+
+
+def test_dense_cells_match_oracle(gpu):
+    """Voronoi cells cut by tubes (the dense-segmentation generator) at 128^3, uint64 ids."""
+    from brook_b200 import synthetic
+
+    labels = synthetic.dense_volume((128, 128, 128), seeds=40, seed=5)
+    got, exp = run_both(labels, teasar_params=CFG0_PARAMS, anisotropy=(8, 8, 40), dust_threshold=100)
+    assert len(got) > 10
+    assert_same(got, exp, "dense")
+
+
+def test_edge_cases(gpu):
+    b = bk()
+    # empty and all-background volumes
+    assert b.skeletonize(np.zeros((0, 4, 4), np.uint32), dust_threshold=0) == {}
+    assert b.skeletonize(np.zeros((16, 16, 16), np.uint32), dust_threshold=0) == {}
+    # a volume at or below the dust threshold
+    assert b.skeletonize(np.ones((4, 4, 4), np.uint32), dust_threshold=64) == {}
+    # single voxels and a 2-voxel object
+    v = np.zeros((8, 8, 8), np.uint32)
+    v[1, 1, 1] = 3
+    v[5, 5, 5] = 4
+    v[5, 5, 6] = 4
+    got, exp = run_both(v, dust_threshold=0, anisotropy=(1, 1, 1))
+    assert_same(got, exp, "tiny")
+    assert list(got.labels) == [4]
+    # one object filling the whole volume: the border is black
+    full = np.ones((12, 10, 9), np.uint16)
+    got, exp = run_both(full, dust_threshold=0, anisotropy=(2, 3, 4))
+    assert_same(got, exp, "full")
+    # a flat (2D) volume and a line
+    flat = shapes.sine_band(6.0, 60.0, 1.6, axis=2)
+    got, exp = run_both(flat, dust_threshold=0, anisotropy=(4, 4, 4), teasar_params=dict(scale=1.0, const=2.0))
+    assert_same(got, exp, "flat")
+    line = np.zeros((30, 1, 1), np.uint8)
+    line[3:27] = 1
+    got, exp = run_both(line, dust_threshold=0)
+    assert_same(got, exp, "line")
+    # two components of one label merge into one skeleton; object_ids filters
+    two = np.zeros((20, 20, 20), np.uint32)
+    two[2:8, 2:4, 2:4] = 9
+    two[12:19, 14:16, 10:12] = 9
+    two[2:18, 10:12, 16:18] = 5
+    got, exp = run_both(two, dust_threshold=0, anisotropy=(1, 1, 1))
+    assert_same(got, exp, "merge")
+    only = b.skeletonize(two, dust_threshold=0, object_ids=[5], output="packed")
+    assert list(only.labels) == [5]
+
+
+def test_fix_borders_off(gpu):
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((64, 64, 64), objects=8, seed=11)
+    got, exp = run_both(labels, teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100,
+                        fix_borders=False)
+    assert_same(got, exp, "no borders")
+
+
+def test_max_paths(gpu):
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((64, 64, 64), objects=6, seed=12)
+    params = dict(CFG0_PARAMS, max_paths=3)
+    got, exp = run_both(labels, teasar_params=params, anisotropy=(16, 16, 40), dust_threshold=100)
+    assert_same(got, exp, "max_paths")
+
+
+def test_device_input_and_layouts(gpu):
+    import torch
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((48, 40, 36), objects=5, seed=21)
+    opts = dict(teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=50)
+    exp = oracle.skeletonize(labels, **opts)
+    for host in (np.asfortranarray(labels), np.ascontiguousarray(labels), labels[:, :, :].transpose(0, 1, 2)):
+        assert_same(bk().skeletonize(host, output="packed", **opts), exp, "host layout")
+    # device tensors: Fortran-ordered (read in place) and C-ordered (gathered on the device)
+    t_c = torch.from_numpy(np.ascontiguousarray(labels)).cuda()
+    assert_same(bk().skeletonize(t_c, output="packed", **opts), exp, "device C")
+    t_f = torch.from_numpy(np.ascontiguousarray(labels.transpose(2, 1, 0))).cuda().permute(2, 1, 0)
+    assert_same(bk().skeletonize(t_f, output="packed", **opts), exp, "device F")
+
+
+def test_batch_identity(gpu):
+    """skeletonize_batch(samples)[i] == skeletonize(samples[i]) for uneven shapes and dtypes."""
+    from brook_b200 import synthetic
+
+    samples = [synthetic.tube_volume((40, 52, 33), objects=4, seed=31),
+               synthetic.tube_volume((64, 30, 45), objects=6, seed=32).astype(np.uint16),
+               np.zeros((10, 10, 10), np.uint32),
+               synthetic.tube_volume((33, 33, 70), objects=3, seed=33).astype(np.uint64)]
+    opts = dict(teasar_params=CFG0_PARAMS, anisotropy=(4, 4, 4), dust_threshold=50)
+    batch = bk().skeletonize_batch(samples, output="packed", **opts)
+    assert len(batch) == len(samples)
+    for i, s in enumerate(samples):
+        assert_same(batch[i], oracle.skeletonize(s, **opts), f"sample {i}")
+
+
+def test_c_abi_known_answers(gpu):
+    """c_smoke.c:7-61 of the reference: components and EDT of {1,1,0,0,0,0,2,2}."""
+    from brook_b200 import _native as n
+
+    lib = n.lib
+    labels = np.array([1, 1, 0, 0, 0, 0, 2, 2], np.uint8).reshape(8, 1, 1, order="F")
+    vol = n.host_volume(labels)
+    ctx = n.context(0)
+    cc = ctypes.c_void_p()
+    n.check(lib.brook_connected_components(ctx, ctypes.byref(vol), ctypes.byref(cc)))
+    view = n.Volume()
+    mapping = ctypes.POINTER(ctypes.c_int64)()
+    roots = ctypes.POINTER(ctypes.c_int64)()
+    count = ctypes.c_size_t()
+    n.check(lib.brook_components_view(cc, ctypes.byref(view), ctypes.byref(mapping), ctypes.byref(roots),
+                                      ctypes.byref(count)))
+    assert count.value == 2 and mapping[1] == 1 and mapping[2] == 2 and roots[0] == 0 and roots[1] == 6
+    out = np.zeros(8, np.uint8)
+    n.check(lib.brook_components_copy_to_host(cc, out.ctypes.data, out.nbytes))
+    assert out.tolist() == labels.ravel().tolist()
+    lib.brook_components_destroy(cc)
+    aniso = (ctypes.c_float * 3)(1, 1, 1)
+    arr = ctypes.c_void_p()
+    n.check(lib.brook_edt(ctx, ctypes.byref(vol), aniso, 0, ctypes.byref(arr)))
+    d = np.zeros(8, np.float32)
+    n.check(lib.brook_array_copy_to_host(arr, d.ctypes.data, d.nbytes))
+    lib.brook_array_destroy(arr)
+    assert d[0] == 2 and d[1] == 1 and d[2] == 0 and d[6] == 1 and d[7] == 2
+    # errors map to status codes with a message
+    bad = n.host_volume(labels)
+    bad.abi_version = 99
+    assert lib.brook_connected_components(ctx, ctypes.byref(bad), ctypes.byref(cc)) == n.INVALID_ARGUMENT
+    assert lib.brook_last_error()
+
+
+def test_edt_matches_oracle(gpu):
+    """The EDT alone, through the C ABI, on multi-label volumes with and without black border."""
+    from brook_b200 import _native as n
+    from brook_b200 import synthetic
+
+    labels = synthetic.dense_volume((96, 80, 70), seeds=20, seed=9).astype(np.uint64)
+    ctx = n.context(0)
+    for aniso, bb in (((1, 1, 1), 0), ((8, 8, 40), 1), ((7.91, 7.91, 7.91), 0)):
+        vol = n.host_volume(np.asfortranarray(labels))
+        arr = ctypes.c_void_p()
+        n.check(n.lib.brook_edt(ctx, ctypes.byref(vol), (ctypes.c_float * 3)(*aniso), bb, ctypes.byref(arr)))
+        d = np.zeros(labels.shape, np.float32, order="F")
+        n.check(n.lib.brook_array_copy_to_host(arr, d.ctypes.data, d.nbytes))
+        n.lib.brook_array_destroy(arr)
+        # the oracle's EDT takes component ids; ids of equal original labels coincide with the labels
+        _, inv = np.unique(labels, return_inverse=True)
+        ids = inv.reshape(labels.shape).astype(np.uint32)
+        exp = oracle.edt(ids, aniso, bool(bb))
+        np.testing.assert_array_equal(d.view(np.uint32), exp.view(np.uint32), err_msg=str(aniso))

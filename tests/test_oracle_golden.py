@@ -1,0 +1,89 @@
+"""The CPU oracle against the reference's own known answers (CPU only)."""
+import itertools
+import json
+import os
+
+import numpy as np
+import pytest
+
+import shapes
+from oracle import oracle
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "join_digests.json")))
+
+
+@pytest.mark.parametrize("case", sorted(shapes.CASES))
+@pytest.mark.parametrize("layout", [np.ascontiguousarray, np.asfortranarray])
+def test_join_digests(case, layout):
+    """Kimimaro 5.8.1 + dijkstra3d 1.15.2 summaries the reference pins (test_package.py:2079-2113)."""
+    make, extra = shapes.CASES[case]
+    result = oracle.skeletonize(layout(make()), **dict(shapes.JOIN_OPTIONS, **extra))
+    assert shapes.summary(result.skeletons()) == {int(k): v for k, v in GOLDEN[case].items()}
+
+
+def _flat(p, shape):
+    return int(np.ravel_multi_index(p, shape, order="F"))
+
+
+def test_railroad_plane_and_wall():
+    """test_package.py:751-778: the lowest-flat nearest rail fixes the last road voxel, and the
+    path joins that voxel's first rail in dijkstra3d order; a walled target has no path."""
+    field = np.ones((9, 9, 9), np.float32, order="F")
+    field[:, :, 0] = 0
+    target = _flat((4, 4, 4), field.shape)
+    road = [(4, 4, 4), (3, 3, 3), (2, 2, 2), (1, 1, 1), (1, 1, 0)]
+    assert oracle.railroad(field, target) == [_flat(p, field.shape) for p in road]
+    walled = field.copy(order="F")
+    walled[2:7, 2:7, 2:7] = np.inf
+    walled[3:6, 3:6, 3:6] = 1
+    assert oracle.railroad(walled, target) == []
+
+
+D3_ORDER = [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1),
+            (-1, -1, 0), (-1, 1, 0), (1, -1, 0), (1, 1, 0), (0, -1, -1), (0, -1, 1), (0, 1, -1), (0, 1, 1),
+            (-1, 0, -1), (-1, 0, 1), (1, 0, -1), (1, 0, 1),
+            (-1, -1, -1), (1, -1, -1), (-1, 1, -1), (-1, -1, 1), (1, 1, -1), (1, -1, 1), (-1, 1, 1), (1, 1, 1)]
+
+
+def test_railroad_join_order():
+    """test_package.py:782-811: every single rail, every pair and all 26 around the target: the
+    path joins the first rail in dijkstra3d's neighbour order."""
+    shape, centre = (5, 5, 5), (2, 2, 2)
+    near = [tuple(c + d for c, d in zip(centre, o)) for o in D3_ORDER]
+    for rails in [(i,) for i in range(26)] + list(itertools.combinations(range(26), 2)) + [tuple(range(26))]:
+        field = np.ones(shape, np.float32, order="F")
+        for i in rails:
+            field[near[i]] = 0
+        assert oracle.railroad(field, _flat(centre, shape)) == [_flat(centre, shape), _flat(near[rails[0]], shape)], rails
+
+
+def test_edt_line():
+    """c_smoke.c:45-61: EDT of an 8-voxel line {1,1,0,0,0,0,2,2}, anisotropy 1, no black border."""
+    labels = np.array([1, 1, 0, 0, 0, 0, 2, 2], np.uint32).reshape(8, 1, 1)
+    d = oracle.edt(labels, (1, 1, 1), False).ravel()
+    assert d[0] == 2 and d[1] == 1 and d[2] == 0 and d[6] == 1 and d[7] == 2
+
+
+def test_target_order_rule():
+    """component_order_smoke.cpp:10-29: descending DAF, infinity and -0 as 0, ties -> higher index,
+    on the reference's own generator (std::mt19937(482))."""
+    bits = np.random.MT19937(0)
+    bits._legacy_seeding(482)
+    raw = lambda: int(bits.random_raw())
+    for n in (1, 17, 1025):
+        for density in (0, 3, 50, 100):
+            for ties in (1, 7, 10000):
+                mask = np.zeros(n, np.uint8)
+                daf = np.zeros(n, np.float32)
+                for i in range(n):
+                    mask[i] = (1 + raw() % 7) if raw() % 100 < density else 0
+                    daf[i] = np.float32(raw() % ties) * np.float32(0.37)
+                    if i % 19 == 0:
+                        daf[i] = np.inf
+                    if i % 23 == 0:
+                        daf[i] = -0.0
+                got = oracle.target_order(mask, daf)
+                key = np.where(np.isinf(daf), 0, daf).astype(np.float64)
+                idx = np.nonzero(mask)[0]
+                expected = sorted(idx.tolist(), key=lambda i: (-key[i], -i))
+                assert got.tolist() == expected
