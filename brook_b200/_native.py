@@ -28,7 +28,7 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_context_synchronize", "brook_array_destroy", "brook_array_view", "brook_array_copy_to_host",
            "brook_connected_components", "brook_components_destroy", "brook_components_view",
            "brook_components_copy_to_host", "brook_edt", "brook_skeletonize_options_init", "brook_skeletonize",
-           "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy"]
+           "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy", "brook_context_stats"]
 
 
 class Volume(ctypes.Structure):
@@ -99,6 +99,7 @@ def _load():
                                                    ctypes.POINTER(vp)]),
         "brook_skeletons_get_view": (ctypes.c_int, [vp, ctypes.POINTER(SkeletonsView)]),
         "brook_skeletons_destroy": (None, [vp]),
+        "brook_context_stats": (ctypes.c_int, [vp, ctypes.c_char_p, sz, ctypes.POINTER(sz)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -209,3 +210,15 @@ def packed_arrays(handle):
                     radii=grab(v.radii, nv, np.float32, (nv,)), anisotropy=tuple(float(a) for a in v.anisotropy))
     finally:
         lib.brook_skeletons_destroy(handle)
+
+
+def stats(device=0):
+    """The statistics of the calling thread's context's last call (stage ms and work counters)."""
+    import json
+
+    ctx = context(device)
+    need = ctypes.c_size_t()
+    check(lib.brook_context_stats(ctx, None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(need.value)
+    check(lib.brook_context_stats(ctx, buf, need.value, None))
+    return json.loads(buf.value.decode())

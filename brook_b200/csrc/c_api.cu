@@ -1,5 +1,7 @@
 // The C ABI (include/brook_b200.h): argument checks, input staging into Fortran-ordered device
 // buffers, exception -> brook_status mapping with thread-local error text, result handles.
+#include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -132,7 +134,7 @@ Staged stage(bk::Context &ctx, const brook_volume &v) {
     if (fortran) { st.volume.data = v.data; return st; }
     st.owned = bk::Buffer<unsigned char>(ctx, n * b);
     gather_strided<<<bk::blocks_for(n), 256, 0, s>>>(static_cast<const unsigned char *>(v.data), st.owned.data(), int(sx),
-                                                    int(sy), int(sz), v.strides[0], v.strides[1], v.strides[2], int(b));
+                                                    int(sy), int(sz), v.strides[0], v.strides[1], v.strides[2], int(b)); ++ctx.launches;
     BK_CUDA(cudaGetLastError());
     st.volume.data = st.owned.data();
     return st;
@@ -145,7 +147,7 @@ Staged stage(bk::Context &ctx, const brook_volume &v) {
     bk::Buffer<unsigned char> raw(ctx, n * b);
     BK_CUDA(cudaMemcpyAsync(raw.data(), v.data, n * b, cudaMemcpyHostToDevice, s));
     gather_strided<<<bk::blocks_for(n), 256, 0, s>>>(raw.data(), st.owned.data(), int(sx), int(sy), int(sz), b * sy * sz,
-                                                    b * sz, b, int(b));
+                                                    b * sz, b, int(b)); ++ctx.launches;
     BK_CUDA(cudaGetLastError());
     ctx.synchronize();
   } else {
@@ -304,7 +306,7 @@ brook_status brook_connected_components(brook_context *ctx, const brook_volume *
     handle->storage = std::make_shared<DeviceStorage>(size_t(n) * b, ctx->value.device());
     handle->bytes = size_t(n) * b;
     if (n) {
-      narrow_ids<<<bk::blocks_for(n), 256, 0, ctx->value.stream()>>>(ids.data(), handle->storage->ptr, n, int(b));
+      narrow_ids<<<bk::blocks_for(n), 256, 0, ctx->value.stream()>>>(ids.data(), handle->storage->ptr, n, int(b)); ++ctx->value.launches;
       BK_CUDA(cudaGetLastError());
     }
     ctx->value.synchronize();
@@ -405,5 +407,26 @@ brook_status brook_skeletons_get_view(const brook_skeletons *r, brook_skeletons_
   });
 }
 void brook_skeletons_destroy(brook_skeletons *r) { delete r; }
+
+brook_status brook_context_stats(brook_context *ctx, char *json, size_t capacity, size_t *length) {
+  return protect([&] {
+    require(ctx);
+    std::string out = "{";
+    bool first = true;
+    for (const auto &kv : ctx->value.stats) {
+      char value[64];
+      std::snprintf(value, sizeof(value), "%.17g", kv.second);
+      out += (first ? "\"" : ", \"") + kv.first + "\": " + value;
+      first = false;
+    }
+    out += "}";
+    if (length) *length = out.size() + 1;
+    if (json && capacity) {
+      const size_t n = std::min(capacity - 1, out.size());
+      std::memcpy(json, out.data(), n);
+      json[n] = 0;
+    }
+  });
+}
 
 }  // extern "C"

@@ -118,9 +118,9 @@ ComponentsResult run(Context &ctx, const L *labels, VolumeDims vd, uint32_t *ids
   ComponentsResult out;
   Buffer<int> parent(ctx, n), rank(ctx, n + 1);
   cudaStream_t s = ctx.stream();
-  init_parent<<<blocks_for(n), 256, 0, s>>>(parent.data(), n);
-  union_forward<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), d);
-  flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n);
+  init_parent<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
+  union_forward<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), d); ++ctx.launches;
+  flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   thrust::counting_iterator<long long> index(0);
   thrust::transform_iterator<RootFlag<L>, thrust::counting_iterator<long long>, int> flags(index, RootFlag<L>{labels, parent.data()});
@@ -128,13 +128,13 @@ ComponentsResult run(Context &ctx, const L *labels, VolumeDims vd, uint32_t *ids
   BK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, flags, rank.data(), n, s));
   Buffer<unsigned char> scratch(ctx, temp);
   BK_CUDA(cub::DeviceScan::ExclusiveSum(scratch.data(), temp, flags, rank.data(), n, s));
-  count_roots<L><<<1, 1, 0, s>>>(labels, parent.data(), rank.data(), n);
+  count_roots<L><<<1, 1, 0, s>>>(labels, parent.data(), rank.data(), n); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   out.count = rank.download(1, n)[0];
   Buffer<long long> roots(ctx, out.count + 1), mapping(ctx, out.count + 1);
   mapping.zero();
   relabel<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), rank.data(), ids, roots.data(),
-                                          mapping.data(), n);
+                                          mapping.data(), n); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   auto r = roots.download(out.count);
   auto m = mapping.download(out.count + 1);

@@ -175,7 +175,7 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
   const long long xlines = (long long)vd.sy * vd.sz;
   const bool only_x = dims == 1 || (vd.sy == 1 && vd.sz == 1 && dims == 1);
   edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(ids, D, d, dacc.data(),
-                                                                                black_border ? 1 : 0, only_x ? 1 : 0);
+                                                                                black_border ? 1 : 0, only_x ? 1 : 0); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   for (int axis = 1; axis < dims; ++axis) {
     const int len = axis == 1 ? vd.sy : vd.sz;
@@ -189,7 +189,7 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
     for (long long l0 = 0; l0 < lines; l0 += batch) {
       const long long nb = std::min(batch, lines - l0);
       edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, axis, aniso[axis], black_border ? 1 : 0, l0, nb,
-                                                      V.data(), H.data(), Z.data(), last);
+                                                      V.data(), H.data(), Z.data(), last); ++ctx.launches;
       BK_CUDA(cudaGetLastError());
     }
   }

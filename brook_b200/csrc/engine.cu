@@ -527,6 +527,8 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, const int *path, int
 __global__ void __launch_bounds__(kEngineThreads) trace_kernel(EngineArgs a) {
   __shared__ Shared sh;
   __shared__ int s_pos;
+  __shared__ unsigned long long s_work[4];
+  if (threadIdx.x < 4) s_work[threadIdx.x] = 0;
   while (next_object(a, sh)) {
     const int o = sh.obj;
     int *L0 = a.lists + sh.begin, *L1 = L0 + a.F, *L2 = L1 + a.F, *L3 = L2 + a.F, *L4 = L3 + a.F;
@@ -574,15 +576,22 @@ __global__ void __launch_bounds__(kEngineThreads) trace_kernel(EngineArgs a) {
       __syncthreads();
       const int len = s_pos;
       const int nt = sh.n_touch;
+      const float D = __uint_as_float(unsigned(rb >> 32));
+      unsigned settled = 0;
       for (int i = threadIdx.x; i < nt; i += blockDim.x) {
         const int v = __ldcg(L4 + i);
+        settled += __ldcg(a.dist + v) <= D;
         a.dist[v] = inf();
         atomicAnd(a.flags + v, ~(kNearQueued | kFarQueued));
       }
+      settled = __reduce_add_sync(0xFFFFFFFFu, settled);
+      if ((threadIdx.x & 31) == 0) atomicAdd(&s_work[0], (unsigned long long)settled);
+      if (threadIdx.x == 0) s_work[1] += nt;
       __syncthreads();
       if (len < 0) { status = kStoreFull; break; }
       if (paths >= rec_cap) { status = kRecordsFull; break; }
       if (!invalidate(a, sh, store + used, len, L0, L1, L2, L3, L4, wide)) { status = kBudget; break; }
+      if (threadIdx.x == 0) { s_work[2] += sh.n_touch; s_work[3] += 1; }
       for (int i = threadIdx.x; i < len; i += blockDim.x) a.pdrf[store[used + i]] = 0.0f;
       if (threadIdx.x == 0) { rec_start[paths] = int(used); rec_len[paths] = len; }
       __syncthreads();
@@ -596,6 +605,7 @@ __global__ void __launch_bounds__(kEngineThreads) trace_kernel(EngineArgs a) {
     }
     __syncthreads();
   }
+  if (threadIdx.x < 4 && s_work[threadIdx.x]) atomicAdd(a.work + threadIdx.x, s_work[threadIdx.x]);
 }
 
 }  // namespace

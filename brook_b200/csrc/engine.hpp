@@ -71,6 +71,9 @@ struct EngineArgs {
   int *rec_start, *rec_len;    // per path: offset in the object's store region, length
   const long long *rec_begin, *rec_cap;
   int *npaths, *nstore;
+  // work counters (added over all objects): [0] voxels a railroad settled (distance <= its rail's),
+  // [1] voxels a railroad touched, [2] voxels invalidated, [3] paths
+  unsigned long long *work;
   float wx, wy, wz, scale, constant, delta;
 };
 

@@ -56,7 +56,7 @@ Buffer<int> object_voxels(Context &ctx, const uint32_t *ids, long long n, const 
   Buffer<uint32_t> keys(ctx, total), keys_out(ctx, total);
   Buffer<int> vox(ctx, total);
   if (total == 0) return vox;
-  object_keys<<<blocks_for(total), 256, 0, s>>>(picked.data(), ids, rank, keys.data(), (int)total);
+  object_keys<<<blocks_for(total), 256, 0, s>>>(picked.data(), ids, rank, keys.data(), (int)total); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   int bits = 1;
   while ((1LL << bits) < nobj) ++bits;
@@ -75,14 +75,14 @@ Buffer<int> target_orders(Context &ctx, const int *vox, const float *daf, long l
   Buffer<int> order(ctx, total > 0 ? total : 1);
   if (total == 0) return order;
   Buffer<unsigned long long> keys(ctx, total), sorted(ctx, total);
-  order_keys<<<blocks_for(total), 256, 0, s>>>(vox, daf, keys.data(), (int)total);
+  order_keys<<<blocks_for(total), 256, 0, s>>>(vox, daf, keys.data(), (int)total); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   size_t temp = 0;
   BK_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, temp, keys.data(), sorted.data(), (int)total, nobj, begin, end, s));
   Buffer<unsigned char> scratch(ctx, temp);
   BK_CUDA(cub::DeviceSegmentedSort::SortKeys(scratch.data(), temp, keys.data(), sorted.data(), (int)total, nobj, begin,
                                              end, s));
-  unpack_order<<<blocks_for(total), 256, 0, s>>>(sorted.data(), order.data(), (int)total);
+  unpack_order<<<blocks_for(total), 256, 0, s>>>(sorted.data(), order.data(), (int)total); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   return order;
 }

@@ -5,6 +5,8 @@
 //   assembly into packed skeletons per volume.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <numeric>
 #include <stdexcept>
 
@@ -76,7 +78,7 @@ Buffer<unsigned char> filtered(Context &ctx, const DeviceVolume &v, const std::v
   Buffer<unsigned char> out(ctx, v.d.n() * sizeof(L));
   filter_labels<L><<<blocks_for(v.d.n()), 256, 0, ctx.stream()>>>(static_cast<const L *>(v.data),
                                                                   reinterpret_cast<L *>(out.data()), v.d.n(),
-                                                                  d.data(), (int)sorted.size());
+                                                                  d.data(), (int)sorted.size()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   return out;
 }
@@ -149,6 +151,9 @@ void consolidate(std::vector<std::array<int, 3>> &vertices, std::vector<float> &
 
 std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &volumes, const Options &opt) {
   cudaStream_t s = ctx.stream();
+  ctx.stats.clear();
+  ctx.launches = 0;
+  StageClock clock(ctx);
   const auto &t = opt.teasar;
   for (float a : opt.anisotropy)
     if (!std::isfinite(a) || a <= 0) throw std::invalid_argument("anisotropy must be finite and positive");
@@ -194,16 +199,22 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       labels = masked.data();
     }
     st.cc = connected_components(ctx, labels, volumes[v].dtype, st.d, vid);
+    clock.mark("ccl");
     const int64_t K = st.cc.count;
     st.object_of.assign(K + 1, -1);
     if (!K) { st.empty = true; continue; }
     st.boxes = analyze(ctx, vid, st.d, K);
+    clock.mark("analyze");
     const bool black_border = K == 1 && st.boxes[1].count == n;
     edt(ctx, vid, st.d, aniso, black_border, 3, dbf.data() + st.offset);
+    clock.mark("edt");
     neighbour_mask(ctx, vid, st.d, mask.data() + st.offset);
+    clock.mark("mask");
     st.borders.assign(K + 1, {});
     if (opt.fix_borders) st.borders = border_targets(ctx, vid, st.d, K, aniso);
+    clock.mark("borders");
     st.dbf_max = segment_max(ctx, dbf.data() + st.offset, vid, n, K);
+    clock.mark("dbf_max");
   }
   // ---- objects: more voxels than dust and a bounding box of two or more voxels (batched.cu:187-191)
   struct Object {
@@ -281,9 +292,10 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       if (st.object_of[id] >= 0) rank[id] = st.object_of[id] - first;
     Buffer<int> drank = to_device(ctx, rank);
     Buffer<int> local = object_voxels(ctx, ids.data() + st.offset, st.d.n(), drank.data(), cnt, total);
-    offset_voxels<<<blocks_for(total), 256, 0, s>>>(local.data(), total, int(st.offset));
+    offset_voxels<<<blocks_for(total), 256, 0, s>>>(local.data(), total, int(st.offset)); ++ctx.launches;
     BK_CUDA(cudaMemcpyAsync(vox.data() + obj_begin[first], local.data(), total * sizeof(int), cudaMemcpyDeviceToDevice, s));
   }
+  clock.mark("object_voxels");
   // global per-voxel state
   Buffer<float> pdrf(ctx, N), dist(ctx, N), daf(ctx, N);
   Buffer<uint32_t> flags(ctx, N);
@@ -304,7 +316,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       std::vector<int> r(st.cc.count + 1, -1);
       for (int64_t id = 1; id <= st.cc.count; ++id) r[id] = st.object_of[id];
       Buffer<int> dr = to_device(ctx, r);
-      init_alive<<<blocks_for(st.d.n()), 256, 0, s>>>(ids.data() + st.offset, dr.data(), st.d.n(), alive.data() + st.offset);
+      init_alive<<<blocks_for(st.d.n()), 256, 0, s>>>(ids.data() + st.offset, dr.data(), st.d.n(), alive.data() + st.offset); ++ctx.launches;
       BK_CUDA(cudaGetLastError());
     }
   }
@@ -327,9 +339,10 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   Buffer<int> queue(ctx, 2), status(ctx, nobj), root(ctx, nobj), target(ctx, nobj), npaths(ctx, nobj), nstore(ctx, nobj);
   Buffer<float> max_daf(ctx, nobj);
   Buffer<int> lists(ctx, 5 * F), store(ctx, store_total), rec_start(ctx, rec_total), rec_len(ctx, rec_total);
-  Buffer<unsigned long long> wide(ctx, F);
+  Buffer<unsigned long long> wide(ctx, F), work(ctx, 4);
   queue.zero();
   status.zero();
+  work.zero();
 
   EngineArgs a{};
   a.arena_offset = d_arena_offset.data(); a.arena_dims = d_arena_dims.data(); a.obj_arena = d_obj_arena.data();
@@ -350,16 +363,30 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.manual_begin = d_manual_begin.data(); a.manual_count = d_manual_count.data(); a.manual = d_manual.data();
   a.max_paths = d_max_paths.data(); a.store = store.data(); a.store_begin = d_store_begin.data(); a.store_cap = d_store_cap.data();
   a.rec_start = rec_start.data(); a.rec_len = rec_len.data(); a.rec_begin = d_rec_begin.data(); a.rec_cap = d_rec_cap.data();
-  a.npaths = npaths.data(); a.nstore = nstore.data();
+  a.npaths = npaths.data(); a.nstore = nstore.data(); a.work = work.data();
   a.wx = aniso[0]; a.wy = aniso[1]; a.wz = aniso[2];
   a.scale = float(t.scale); a.constant = float(t.constant);
   a.delta = std::min({aniso[0], aniso[1], aniso[2]});
 
+  clock.mark("state");
   launch_prepare(a, engine_grid(ctx.sm_count(), nobj, false), s);
+  ++ctx.launches;
+  clock.mark("prepare");
+  if (const char *fields = std::getenv("BROOK_B200_DUMP_FIELDS")) {
+    // diagnostics: the prepared DAF and PDRF (root rails included) as raw float32 files
+    const auto hd = daf.download(), hp = pdrf.download(), hb = dbf.download();
+    for (auto item : {std::make_pair("daf", &hd), std::make_pair("pdrf", &hp), std::make_pair("dbf", &hb)}) {
+      FILE *f = std::fopen((std::string(fields) + "." + item.first).c_str(), "wb");
+      if (f) { std::fwrite(item.second->data(), sizeof(float), item.second->size(), f); std::fclose(f); }
+    }
+  }
   Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), d_seg_end.data(), nobj);
   a.order = order.data();
   BK_CUDA(cudaMemsetAsync(queue.data(), 0, sizeof(int), s));
+  clock.mark("order");
   launch_trace(a, engine_grid(ctx.sm_count(), nobj, true), s);
+  ++ctx.launches;
+  clock.mark("trace");
 
   // ---- results
   const auto st_host = status.download();
@@ -370,6 +397,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       throw std::runtime_error(std::string("tracing failed: ") + what[std::min(st_host[o], 4)]);
     }
   const auto np = npaths.download(), ns = nstore.download();
+  const char *dump = std::getenv("BROOK_B200_DUMP");
   std::vector<long long> vdst(nobj), rdst(nobj);
   long long vt = 0, rt = 0;
   for (int o = 0; o < nobj; ++o) { vdst[o] = vt; vt += ns[o]; rdst[o] = rt; rt += np[o]; }
@@ -377,12 +405,39 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   Buffer<float> cradii(ctx, std::max(vt, 1LL));
   auto d_vdst = to_device(ctx, vdst), d_rdst = to_device(ctx, rdst);
   gather_store<<<nobj, 256, 0, s>>>(store.data(), d_store_begin.data(), d_vdst.data(), nstore.data(), nobj, dbf.data(),
-                                    cstore.data(), cradii.data());
+                                    cstore.data(), cradii.data()); ++ctx.launches;
   gather_records<<<nobj, 256, 0, s>>>(rec_start.data(), rec_len.data(), d_rec_begin.data(), d_rdst.data(), npaths.data(),
-                                      nobj, cstart.data(), clen.data());
+                                      nobj, cstart.data(), clen.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   const auto hstore = cstore.download(vt), hstart = cstart.download(rt), hlen = clen.download(rt);
   const auto hrad = cradii.download(vt);
+  if (dump && *dump) {
+    // diagnostics: the intermediate results a parity investigation compares with the oracle
+    FILE *f = std::fopen(dump, "w");
+    if (f) {
+      const auto hroot = root.download(), htarget = target.download();
+      const auto hmax = max_daf.download();
+      for (size_t v = 0; v < vs.size(); ++v) {
+        const auto &st = vs[v];
+        if (st.empty) continue;
+        for (int64_t id = 1; id <= st.cc.count; ++id) {
+          std::fprintf(f, "borders %zu %lld", v, (long long)id);
+          for (const auto &p : st.borders[id]) std::fprintf(f, " %lld,%lld,%lld", (long long)p[0], (long long)p[1], (long long)p[2]);
+          std::fprintf(f, "\n");
+        }
+      }
+      for (int o = 0; o < nobj; ++o) {
+        std::fprintf(f, "object %d volume %d id %u root %d target %d max_daf %.9g paths %d\n", o, objects[o].volume,
+                     objects[o].id, hroot[o], htarget[o], hmax[o], np[o]);
+        for (int p = 0; p < np[o]; ++p) {
+          std::fprintf(f, "path %d %d:", o, p);
+          for (int q = 0; q < hlen[rdst[o] + p]; ++q) std::fprintf(f, " %d", hstore[vdst[o] + hstart[rdst[o] + p] + q]);
+          std::fprintf(f, "\n");
+        }
+      }
+      std::fclose(f);
+    }
+  }
   // per volume: skeletons per original label, components merged in id order
   for (size_t v = 0; v < vs.size(); ++v) {
     auto &st = vs[v];
@@ -434,6 +489,20 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       out.edge_offsets.push_back(int64_t(out.edges.size() / 2));
     }
   }
+  clock.mark("assembly");
+  clock.finish();
+  const auto w = work.download();
+  ctx.stats["paths"] = double(w[3]);
+  ctx.stats["railroad_settled"] = double(w[0]);
+  ctx.stats["railroad_touched"] = double(w[1]);
+  ctx.stats["invalidated"] = double(w[2]);
+  ctx.stats["objects"] = nobj;
+  ctx.stats["voxels"] = double(N);
+  ctx.stats["foreground"] = double(F);
+  ctx.stats["launches"] = double(ctx.launches);
+  long long kmax = 0;
+  for (const auto &st : vs) kmax = std::max<long long>(kmax, st.cc.count);
+  ctx.stats["label_bytes"] = kmax <= 0xFF ? 1 : kmax <= 0xFFFF ? 2 : kmax <= 0xFFFFFFFFLL ? 4 : 8;
   return results;
 }
 

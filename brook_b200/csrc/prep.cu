@@ -86,7 +86,7 @@ std::vector<Box> analyze(Context &ctx, const uint32_t *ids, VolumeDims vd, int64
   Buffer<int> dlo = to_device(ctx, lo), dhi = to_device(ctx, hi);
   Buffer<unsigned long long> counts(ctx, count + 1);
   counts.zero();
-  analyze_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, d, dlo.data(), dhi.data(), counts.data());
+  analyze_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, d, dlo.data(), dhi.data(), counts.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   lo = dlo.download();
   hi = dhi.download();
@@ -101,14 +101,14 @@ std::vector<Box> analyze(Context &ctx, const uint32_t *ids, VolumeDims vd, int64
 
 void neighbour_mask(Context &ctx, const uint32_t *ids, VolumeDims vd, uint32_t *out) {
   if (vd.n() <= 0) return;
-  mask_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, out);
+  mask_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, out); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
 }
 
 std::vector<float> segment_max(Context &ctx, const float *field, const uint32_t *ids, long long n, int64_t count) {
   Buffer<unsigned> best(ctx, count + 1);
   best.zero();
-  segmax_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(field, ids, n, best.data());
+  segmax_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(field, ids, n, best.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   auto bits = best.download();
   std::vector<float> out(count + 1);
@@ -118,14 +118,14 @@ std::vector<float> segment_max(Context &ctx, const float *field, const uint32_t 
 
 void fill_float(Context &ctx, float *p, long long n, float value) {
   if (n <= 0) return;
-  fill_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(p, n, value);
+  fill_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(p, n, value); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
 }
 
 void extract_face(Context &ctx, const uint32_t *ids, VolumeDims vd, int a, int b, int c, int fixed, uint32_t *plane) {
   const int shape[3] = {vd.sx, vd.sy, vd.sz};
   const long long n = (long long)shape[a] * shape[b];
-  face_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, a, b, c, fixed, plane);
+  face_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, a, b, c, fixed, plane); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
 }
 

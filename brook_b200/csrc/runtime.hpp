@@ -57,7 +57,10 @@ class Context {
   void *allocate(size_t bytes);
   void release(void *p);
   std::mutex &mutex() { return mutex_; }
+  // Per-call statistics: stage times (ms, CUDA events on this context's stream) and work counters.
   std::map<std::string, double> stats;
+  // Kernels of this library launched by the current call.
+  long long launches = 0;
 
  private:
   int device_ = 0, sm_count_ = 0;
@@ -113,6 +116,37 @@ class Buffer {
     return out;
   }
   std::vector<T> download() const { return download(count_); }
+};
+
+// Stage boundaries recorded as CUDA events on the context's stream; finish() adds each stage's
+// elapsed time to ctx.stats["ms_<stage>"].
+class StageClock {
+  Context &ctx_;
+  std::vector<std::pair<std::string, cudaEvent_t>> marks_;
+
+ public:
+  explicit StageClock(Context &ctx) : ctx_(ctx) { mark("start"); }
+  ~StageClock() {
+    for (auto &m : marks_) cudaEventDestroy(m.second);
+  }
+  void mark(const std::string &stage) {
+    cudaEvent_t e;
+    BK_CUDA(cudaEventCreate(&e));
+    BK_CUDA(cudaEventRecord(e, ctx_.stream()));
+    marks_.push_back({stage, e});
+  }
+  void finish() {
+    if (marks_.size() < 2) return;
+    BK_CUDA(cudaEventSynchronize(marks_.back().second));
+    for (size_t i = 1; i < marks_.size(); ++i) {
+      float ms = 0;
+      BK_CUDA(cudaEventElapsedTime(&ms, marks_[i - 1].second, marks_[i].second));
+      ctx_.stats["ms_" + marks_[i].first] += ms;
+    }
+    float total = 0;
+    BK_CUDA(cudaEventElapsedTime(&total, marks_.front().second, marks_.back().second));
+    ctx_.stats["ms_total"] += total;
+  }
 };
 
 template <class T>

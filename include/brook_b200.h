@@ -140,6 +140,13 @@ brook_status brook_skeletonize_batch(brook_context *context, const brook_volume 
 brook_status brook_skeletons_get_view(const brook_skeletons *result, brook_skeletons_view *out);
 void brook_skeletons_destroy(brook_skeletons *result);
 
+/* The statistics of the context's last call as a JSON object (the reference keeps the same map as
+ * Context.stats, runtime.hpp:59 and bindings.cpp:343-347): "ms_<stage>" stage times measured with
+ * CUDA events on the context's stream, and counters (paths, railroad_settled, railroad_touched,
+ * invalidated, objects, voxels, foreground, launches, label_bytes). *length receives the size
+ * needed including the terminating zero; json (capacity bytes) receives as much as fits. */
+brook_status brook_context_stats(brook_context *context, char *json, size_t capacity, size_t *length);
+
 #ifdef __cplusplus
 }
 #endif

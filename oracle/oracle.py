@@ -138,9 +138,15 @@ def _params(teasar_params, anisotropy, dust_threshold, fix_branching, fix_border
     return p
 
 
-def skeletonize(labels, teasar_params=None, anisotropy=(1, 1, 1), dust_threshold=1000, fix_branching=True,
-                fix_borders=True, threads=1, stages=False):
-    """Run the oracle on a 3D label volume (any layout; read as its logical (x, y, z) axes)."""
+# The teasar_params default of the reference's brook.skeletonize (src/brook/__init__.py:8-17).
+DEFAULT_TEASAR_PARAMS = dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_exponent=4, soma_acceptance_threshold=3500,
+                             soma_detection_threshold=750, soma_invalidation_const=300, soma_invalidation_scale=2)
+
+
+def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), dust_threshold=1000,
+                fix_branching=True, fix_borders=True, threads=1, stages=False):
+    """Run the oracle on a 3D label volume (any layout; read as its logical (x, y, z) axes), with
+    the argument defaults of the reference's brook.skeletonize."""
     labels = np.asarray(labels)
     if labels.dtype == bool:
         labels = labels.view(np.uint8)

@@ -99,14 +99,14 @@ def test_dense_cells_match_oracle(gpu):
     assert_same(got, exp, "dense")
 
 
-def test_edge_cases(gpu):
+def test_empty_and_dust(gpu):
     b = bk()
-    # empty and all-background volumes
     assert b.skeletonize(np.zeros((0, 4, 4), np.uint32), dust_threshold=0) == {}
     assert b.skeletonize(np.zeros((16, 16, 16), np.uint32), dust_threshold=0) == {}
-    # a volume at or below the dust threshold
     assert b.skeletonize(np.ones((4, 4, 4), np.uint32), dust_threshold=64) == {}
-    # single voxels and a 2-voxel object
+
+
+def test_tiny_objects(gpu):
     v = np.zeros((8, 8, 8), np.uint32)
     v[1, 1, 1] = 3
     v[5, 5, 5] = 4
@@ -114,11 +114,16 @@ def test_edge_cases(gpu):
     got, exp = run_both(v, dust_threshold=0, anisotropy=(1, 1, 1))
     assert_same(got, exp, "tiny")
     assert list(got.labels) == [4]
-    # one object filling the whole volume: the border is black
+
+
+def test_black_border(gpu):
+    """One object filling the whole volume: the volume edge counts as background."""
     full = np.ones((12, 10, 9), np.uint16)
     got, exp = run_both(full, dust_threshold=0, anisotropy=(2, 3, 4))
     assert_same(got, exp, "full")
-    # a flat (2D) volume and a line
+
+
+def test_flat_and_line(gpu):
     flat = shapes.sine_band(6.0, 60.0, 1.6, axis=2)
     got, exp = run_both(flat, dust_threshold=0, anisotropy=(4, 4, 4), teasar_params=dict(scale=1.0, const=2.0))
     assert_same(got, exp, "flat")
@@ -126,14 +131,17 @@ def test_edge_cases(gpu):
     line[3:27] = 1
     got, exp = run_both(line, dust_threshold=0)
     assert_same(got, exp, "line")
-    # two components of one label merge into one skeleton; object_ids filters
+
+
+def test_split_label_and_object_ids(gpu):
+    """Two components of one label merge into one skeleton; object_ids keeps the listed labels."""
     two = np.zeros((20, 20, 20), np.uint32)
     two[2:8, 2:4, 2:4] = 9
     two[12:19, 14:16, 10:12] = 9
     two[2:18, 10:12, 16:18] = 5
     got, exp = run_both(two, dust_threshold=0, anisotropy=(1, 1, 1))
     assert_same(got, exp, "merge")
-    only = b.skeletonize(two, dust_threshold=0, object_ids=[5], output="packed")
+    only = bk().skeletonize(two, dust_threshold=0, object_ids=[5], output="packed")
     assert list(only.labels) == [5]
 
 
