@@ -1,0 +1,277 @@
+#!/usr/bin/env python
+"""Benchmark of the TEASAR skeletonizer on one B200 node (one process per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config NAME]
+
+A step is one skeletonization of the workload volume. At N = 1 the workload is the dense
+segmentation: a 512^3 uint64 volume of Voronoi cells (600 seeds, seed 1) cut by random-walk tubes
+of radius 3-10, boundaries eroded, anisotropy (8, 8, 40), TEASAR scale 1.5, const 300, PDRF 1e5/4,
+dust 100 (synthetic: the reference's connectomics volumes are not available). With N > 1 every
+rank skeletonizes its own volume of the same kind (seed 1 + rank): replicas, weak scaling.
+
+`value` is voxels/s with the labels already in HBM (device tensor in, packed host skeletons out);
+`e2e` is the same metric through the public API from pinned host memory (host -> device copy of
+the labels and device -> host copy of the skeletons inside the timed region). Times are CUDA
+events on the device, max over ranks. `--impl reference` times the CPU restatement of the
+reference's algorithm (the reference has no CPU implementation of this path) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "dense512": dict(workload="dense segmentation 512x512x512 uint64, 600 Voronoi seeds cut by tubes r=3-10 (seed 1)",
+                     shape=(512, 512, 512), seeds=600, seed=1, kind="dense", dtype="uint64", anisotropy=(8, 8, 40)),
+    "tubes128": dict(workload="128x128x128 uint32, 20 random-walk tubes r=2-6 (seed 0)", shape=(128, 128, 128),
+                     objects=20, seed=0, kind="tubes", dtype="uint32", anisotropy=(16, 16, 40)),
+}
+PARAMS = dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_exponent=4)
+DUST = 100
+METRIC = "voxels/s & skeletons/s, batched/graph vs per-volume on 1 B200; p50/p99 latency"
+
+
+def make_volume(cfg, rank=0):
+    from brook_b200 import synthetic
+
+    if cfg["kind"] == "dense":
+        return synthetic.dense_volume(cfg["shape"], seeds=cfg["seeds"], seed=cfg["seed"] + rank, dtype=np.dtype(cfg["dtype"]))
+    return synthetic.tube_volume(cfg["shape"], objects=cfg["objects"], seed=cfg["seed"] + rank, dtype=np.dtype(cfg["dtype"]))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        query = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={query}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if len(r) > 5 + j and "Active" in r[5 + j]
+                          and "Not" not in r[5 + j]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def result_bytes(packed):
+    return int(packed.vertices.nbytes + packed.edges.nbytes + packed.radii.nbytes + packed.labels.nbytes +
+               packed.v_off.nbytes + packed.e_off.nbytes)
+
+
+def cpu_baseline(volume, cfg, threads):
+    """The oracle (the CPU restatement of the reference's algorithm) on a 256^3 crop of the volume."""
+    from oracle import oracle
+
+    crop = tuple(min(256, s) for s in volume.shape)
+    sample = np.asfortranarray(volume[:crop[0], :crop[1], :crop[2]])
+    t0 = time.perf_counter()
+    oracle.skeletonize(sample, PARAMS, cfg["anisotropy"], DUST, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": sample.size / dt, "unit": "voxels/s", "cores": threads, "kind": "port",
+            "sample": f"{crop[0]}x{crop[1]}x{crop[2]} crop ({sample.size} voxels) of the workload volume, "
+                      f"{dt:.2f} s on {threads} threads"}
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    volume = make_volume(cfg)
+    threads = os.cpu_count() or 1
+    crop = tuple(min(128, s) for s in volume.shape)
+    sample = np.asfortranarray(volume[:crop[0], :crop[1], :crop[2]])
+    for _ in range(args.warmup):
+        oracle.skeletonize(sample, PARAMS, cfg["anisotropy"], DUST, threads=threads)
+    t0 = time.perf_counter()
+    skeletons = 0
+    for _ in range(args.steps):
+        r = oracle.skeletonize(sample, PARAMS, cfg["anisotropy"], DUST, threads=threads)
+        skeletons = len(r.array("labels"))
+    dt = (time.perf_counter() - t0) / args.steps
+    value = sample.size / dt
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "int64/f32", "data": "synthetic",
+           "skeletons_per_s": skeletons / dt,
+           "config": {"workload": cfg["workload"], "sample": f"{crop[0]}x{crop[1]}x{crop[2]} crop per step",
+                      "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST},
+           "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": threads, "kind": "port",
+                            "sample": f"{crop[0]}x{crop[1]}x{crop[2]} crop ({sample.size} voxels) of the workload volume"},
+           "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_ours(args, cfg):
+    import torch
+
+    import brook_b200
+    from brook_b200 import _native
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    volume = make_volume(cfg, rank)
+    # device input: a Fortran-ordered view (x fastest) read in place
+    dev = torch.from_numpy(np.ascontiguousarray(volume.transpose(2, 1, 0))).cuda(local).permute(2, 1, 0)
+    # host input for the end-to-end leg: pinned memory, Fortran order
+    pinned_t = torch.empty(volume.shape[::-1], dtype=dev.dtype, pin_memory=True)
+    pinned_t.numpy()[...] = volume.transpose(2, 1, 0)
+    pinned = pinned_t.numpy().transpose(2, 1, 0)
+    opts = dict(teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST, output="packed", device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        out, stage = None, {}
+        for _ in range(steps):
+            out = fn()
+            for k, v in _native.stats(local).items():
+                stage[k] = stage.get(k, 0.0) + v
+        end.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(end) / steps
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        barrier()
+        return ms, out, {k: v / steps for k, v in stage.items()}
+
+    for _ in range(args.warmup):
+        brook_b200.skeletonize(dev, **opts)
+    with ClockSampler(local) as clocks:
+        ms, packed, stage = timed(lambda: brook_b200.skeletonize(dev, **opts), args.steps)
+    for _ in range(max(1, args.warmup // 2)):
+        brook_b200.skeletonize(pinned, **opts)
+    e2e_ms, packed_h, _ = timed(lambda: brook_b200.skeletonize(pinned, **opts), args.steps)
+    np.testing.assert_array_equal(packed.vertices, packed_h.vertices)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    voxels = volume.size * world
+    skeletons = len(packed) * world
+    value = voxels / (ms / 1e3)
+    # roofline of the dominant kernel (the object engine's trace launch): algorithmic bytes per
+    # launch = settled railroad voxels x (12 + c) + invalidated voxels x (13 + c), c = label bytes
+    c = stage.get("label_bytes", 2)
+    trace_bytes = stage.get("railroad_settled", 0) * (12 + c) + stage.get("invalidated", 0) * (13 + c)
+    stage_ms = {k[3:]: v for k, v in stage.items() if k.startswith("ms_") and k != "ms_total"}
+    dominant = max(stage_ms, key=stage_ms.get) if stage_ms else "trace"
+    peak, source = peaks()
+    achieved = trace_bytes / (stage.get("ms_trace", float("nan")) / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic_dense512.txt")
+    if os.path.exists(tfile):
+        for line in open(tfile):
+            if line.startswith("trace_kernel dram_bytes_per_launch"):
+                traffic = float(line.split("=")[1])
+    out = {
+        "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32/f32", "data": "synthetic",
+        "skeletons_per_s": skeletons / (ms / 1e3),
+        "config": {"workload": cfg["workload"], "voxels_per_gpu": int(volume.size), "objects": int(stage.get("objects", 0)),
+                   "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (labels 1 GiB per step)"},
+        "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
+        "work": {k: stage.get(k) for k in ("paths", "railroad_settled", "railroad_touched", "invalidated", "foreground")},
+        "roofline": {"kernel": "trace_kernel", "stage_dominant": dominant, "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "peak_source": source, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "algorithmic_bytes": trace_bytes},
+        "e2e": {"value": voxels / (e2e_ms / 1e3), "unit": "voxels/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(volume.nbytes), "d2h_bytes_per_step": result_bytes(packed_h)},
+        "gpu_launches": int(stage.get("launches", 0) * args.steps),
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(volume, cfg, os.cpu_count() or 1)
+    print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="dense512", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()
