@@ -28,7 +28,8 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_context_synchronize", "brook_array_destroy", "brook_array_view", "brook_array_copy_to_host",
            "brook_connected_components", "brook_components_destroy", "brook_components_view",
            "brook_components_copy_to_host", "brook_edt", "brook_skeletonize_options_init", "brook_skeletonize",
-           "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy", "brook_context_stats"]
+           "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy", "brook_context_stats",
+           "brook_edt_device_noalloc"]
 
 
 class Volume(ctypes.Structure):
@@ -100,6 +101,8 @@ def _load():
         "brook_skeletons_get_view": (ctypes.c_int, [vp, ctypes.POINTER(SkeletonsView)]),
         "brook_skeletons_destroy": (None, [vp]),
         "brook_context_stats": (ctypes.c_int, [vp, ctypes.c_char_p, sz, ctypes.POINTER(sz)]),
+        "brook_edt_device_noalloc": (ctypes.c_int, [ctypes.POINTER(Volume), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
+                                                    vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -408,6 +408,35 @@ brook_status brook_skeletons_get_view(const brook_skeletons *r, brook_skeletons_
 }
 void brook_skeletons_destroy(brook_skeletons *r) { delete r; }
 
+brook_status brook_edt_device_noalloc(const brook_volume *labels, const float anisotropy[3], int black_border,
+                                      float *out, void *stream) {
+  return protect([&] {
+    require(labels && anisotropy && out);
+    const brook_volume &v = *labels;
+    require(v.struct_size >= sizeof(brook_volume) && v.abi_version == BROOK_ABI_VERSION, "incompatible brook_volume");
+    require(v.memory == BROOK_DEVICE, "brook_edt_device_noalloc reads device memory (memory = BROOK_DEVICE)");
+    require(v.dtype == BROOK_U32, "brook_edt_device_noalloc takes uint32 labels");
+    for (int a = 0; a < 3; ++a) require(v.shape[a] >= 0 && v.shape[a] < (1LL << 31), "invalid volume shape");
+    const bk::VolumeDims d{int(v.shape[0]), int(v.shape[1]), int(v.shape[2])};
+    require(d.n() < (1LL << 31) - 1, "volumes of 2^31 voxels or more are not supported");
+    if (d.n() == 0) return;
+    require(v.data != nullptr);
+    const long long sx = v.shape[0], sy = v.shape[1], sz = v.shape[2];
+    require((sx == 1 || v.strides[0] == 4) && (sy == 1 || v.strides[1] == 4 * sx) && (sz == 1 || v.strides[2] == 4 * sx * sy),
+            "brook_edt_device_noalloc takes Fortran-contiguous labels");
+    int device = 0;
+    BK_CUDA(cudaGetDevice(&device));
+    for (const void *p : {v.data, static_cast<const void *>(out)}) {
+      cudaPointerAttributes attr{};
+      BK_CUDA(cudaPointerGetAttributes(&attr, p));
+      require(attr.type == cudaMemoryTypeManaged || (attr.type == cudaMemoryTypeDevice && attr.device == device),
+              "labels and output must be device memory of the current device");
+    }
+    bk::edt_fixed_scratch(static_cast<const uint32_t *>(v.data), d, anisotropy, black_border != 0, out,
+                          static_cast<cudaStream_t>(stream));
+  });
+}
+
 brook_status brook_context_stats(brook_context *ctx, char *json, size_t capacity, size_t *length) {
   return protect([&] {
     require(ctx);

@@ -9,6 +9,7 @@
 // The reference compiles the envelope with FMA contraction; its two product-plus-height sums are
 // written as explicit fused operations here, everything else rounds per operation (--fmad=false).
 #include <climits>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.hpp"
@@ -190,6 +191,102 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
       const long long nb = std::min(batch, lines - l0);
       edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, axis, aniso[axis], black_border ? 1 : 0, l0, nb,
                                                       V.data(), H.data(), Z.data(), last); ++ctx.launches;
+      BK_CUDA(cudaGetLastError());
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The EDT with a fixed device scratch, for callers that cannot allocate device memory: code that
+// runs inside another framework's memory budget (a caching allocator or a pre-reserved pool that
+// owns the device's free memory), code on a path where an allocation would synchronise the device
+// or fail under memory pressure at the worst moment, and embedded callers that keep a fixed
+// device-memory footprint. The envelope stacks and the spacing table live in one file-scope
+// device array of kFixedScratchBytes (32 MiB) that every GPU loading this library holds until the
+// process exits; nothing is allocated per call.
+namespace {
+
+constexpr size_t kFixedScratchBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned char g_edt_scratch[kFixedScratchBytes];
+
+// acc[k] = the spacing added k times in float32, one rounding per step (the host loop of edt()).
+__global__ void spacing_table(float *acc, int n, float w) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  float a = 0.0f;
+  acc[0] = a;
+  for (int k = 1; k < n; ++k) {
+    a = __fadd_rn(a, w);
+    acc[k] = a;
+  }
+}
+
+std::mutex g_scratch_mutex;
+void *g_scratch_address[256];
+
+// The device address of g_edt_scratch on the current device. Host code cannot use the array's
+// name as a device address (it is a host-side stand-in), so the address is looked up once per
+// device, with that device current, and cached.
+void *fixed_scratch() {
+  int device = 0;
+  BK_CUDA(cudaGetDevice(&device));
+  if (device < 0 || device >= 256) throw std::invalid_argument("device index out of range");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_address[device]) {
+    void *p = nullptr;
+    const cudaError_t status = cudaGetSymbolAddress(&p, g_edt_scratch);
+    if (status != cudaSuccess) {
+      cudaGetLastError();
+      throw CudaError(status, "cudaGetSymbolAddress(EDT scratch)");
+    }
+    g_scratch_address[device] = p;
+  }
+  return g_scratch_address[device];
+}
+
+}  // namespace
+
+size_t edt_fixed_scratch_bytes() { return kFixedScratchBytes; }
+
+// The EDT of uint32 labels (Fortran order) into D on `stream`, using only the fixed scratch. The
+// result equals edt() on the labels' component ids (runs of equal labels along a line are runs of
+// one component). Nothing in the scratch must start at zero: the spacing table is rewritten by
+// every call and every stack entry is written before it is read. Calls that overlap on the GPU
+// (two streams, two threads) share the scratch and race.
+void edt_fixed_scratch(const uint32_t *labels, VolumeDims vd, const float aniso[3], bool black_border, float *D,
+                       cudaStream_t s) {
+  const Dims d{vd.sx, vd.sy, vd.sz};
+  const long long n = vd.n();
+  if (n <= 0) return;
+  for (int a = 0; a < 3; ++a)
+    if (!(aniso[a] > 0) || !std::isfinite(aniso[a])) throw std::invalid_argument("anisotropy must be finite and positive");
+  const size_t smem = size_t(kWarpsX) * vd.sx * sizeof(int);
+  const size_t table = (size_t(vd.sx + 2) * sizeof(float) + 255) / 256 * 256;
+  const size_t line = 16 * size_t(std::max(vd.sy, vd.sz) + 3);
+  if (smem > 200 * 1024 || table + line > kFixedScratchBytes)
+    throw std::invalid_argument("volume too large for the EDT's fixed 32 MiB scratch (x extent at most 12800 and "
+                                "16 * (max(y, z) extent + 3) + 4 * (x extent + 2) bytes within it)");
+  unsigned char *base = static_cast<unsigned char *>(fixed_scratch());
+  float *acc = reinterpret_cast<float *>(base);
+  spacing_table<<<1, 1, 0, s>>>(acc, vd.sx + 2, aniso[0]);
+  BK_CUDA(cudaGetLastError());
+  BK_CUDA(cudaFuncSetAttribute(edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long xlines = (long long)vd.sy * vd.sz;
+  edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(labels, D, d, acc,
+                                                                                black_border ? 1 : 0, 0);
+  BK_CUDA(cudaGetLastError());
+  for (int axis = 1; axis < 3; ++axis) {
+    const int len = axis == 1 ? vd.sy : vd.sz;
+    const long long lines = axis == 1 ? (long long)vd.sx * vd.sz : (long long)vd.sx * vd.sy;
+    const long long room = (long long)((kFixedScratchBytes - table) / (16 * size_t(len + 3)));
+    const long long batch = std::max(1LL, std::min(lines, room));
+    // stacks of one batch: Z (8 bytes per entry, 256-aligned after the table), then V, then H
+    double *Z = reinterpret_cast<double *>(base + table);
+    int *V = reinterpret_cast<int *>(Z + batch * (len + 3));
+    float *H = reinterpret_cast<float *>(V + batch * (len + 3));
+    for (long long l0 = 0; l0 < lines; l0 += batch) {
+      const long long nb = std::min(batch, lines - l0);
+      edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(labels, D, d, axis, aniso[axis], black_border ? 1 : 0, l0, nb,
+                                                      V, H, Z, axis == 2);
       BK_CUDA(cudaGetLastError());
     }
   }

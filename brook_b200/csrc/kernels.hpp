@@ -35,6 +35,11 @@ ComponentsResult connected_components(Context &ctx, const void *labels, int dtyp
 void edt(Context &ctx, const uint32_t *ids, VolumeDims d, const float aniso[3], bool black_border, int dims,
          float *out);
 
+// EDT of uint32 labels with no device allocation (a fixed file-scope scratch in edt.cu); see there.
+void edt_fixed_scratch(const uint32_t *labels, VolumeDims d, const float aniso[3], bool black_border, float *out,
+                       cudaStream_t stream);
+size_t edt_fixed_scratch_bytes();
+
 // ---- preamble (prep.cu) ----
 struct Box {
   int lo[3], hi[3];

@@ -140,6 +140,23 @@ brook_status brook_skeletonize_batch(brook_context *context, const brook_volume 
 brook_status brook_skeletons_get_view(const brook_skeletons *result, brook_skeletons_view *out);
 void brook_skeletons_destroy(brook_skeletons *result);
 
+/* No counterpart in the reference. The EDT of brook_edt for callers that cannot allocate device
+ * memory: code running inside another framework's memory budget (a caching allocator or a
+ * pre-reserved pool that owns the free device memory), code where an allocation would synchronise
+ * the device or fail under memory pressure, and callers that must keep a fixed device footprint.
+ * It allocates nothing and needs no context: labels are Fortran-contiguous uint32 device memory
+ * (memory = BROOK_DEVICE) of the current device, out is the caller's float32 device array of
+ * shape[0]*shape[1]*shape[2] entries, and the work is queued on `stream` (a cudaStream_t; NULL
+ * is the legacy default stream) without synchronising: out is ready when the stream gets there.
+ * The result equals brook_edt's on the same labels. Scratch is one fixed 32 MiB device array of
+ * the library (every GPU that loads the library holds it until the process exits); volumes whose
+ * x extent exceeds 12800 or whose 16 * (max(y, z) extent + 3) + 4 * (x extent + 2) bytes exceed
+ * it are rejected with BROOK_INVALID_ARGUMENT. The first call on a device looks up the array's
+ * device address; make that first call before any stream capture. Calls share the array, so calls
+ * that overlap on the GPU (different streams or threads) race. */
+brook_status brook_edt_device_noalloc(const brook_volume *labels, const float anisotropy[3], int black_border,
+                                      float *out, void *stream);
+
 /* The statistics of the context's last call as a JSON object (the reference keeps the same map as
  * Context.stats, runtime.hpp:59 and bindings.cpp:343-347): "ms_<stage>" stage times measured with
  * CUDA events on the context's stream, and counters (paths, railroad_settled, railroad_touched,

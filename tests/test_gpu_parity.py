@@ -237,7 +237,8 @@ def test_edt_matches_oracle(gpu):
     labels = synthetic.dense_volume((96, 80, 70), seeds=20, seed=9).astype(np.uint64)
     ctx = n.context(0)
     for aniso, bb in (((1, 1, 1), 0), ((8, 8, 40), 1), ((7.91, 7.91, 7.91), 0)):
-        vol = n.host_volume(np.asfortranarray(labels))
+        host = np.asfortranarray(labels)  # kept alive: the volume descriptor borrows its memory
+        vol = n.host_volume(host)
         arr = ctypes.c_void_p()
         n.check(n.lib.brook_edt(ctx, ctypes.byref(vol), (ctypes.c_float * 3)(*aniso), bb, ctypes.byref(arr)))
         d = np.zeros(labels.shape, np.float32, order="F")
