@@ -24,10 +24,15 @@ size_t label_bytes(int dtype) {
 
 namespace {
 
-__device__ __forceinline__ int find_root(const int *parent, int i) {
+// Root of i with path halving (every visited node is pointed at its grandparent). Parents only
+// ever point to smaller indices and a shortcut only skips ancestors, so the racy writes are benign.
+__device__ __forceinline__ int find_root(int *parent, int i) {
   int p = __ldcg(parent + i);
   while (p != i) {
-    i = p;
+    const int g = __ldcg(parent + p);
+    if (g == p) return p;
+    parent[i] = g;
+    i = g;
     p = __ldcg(parent + i);
   }
   return i;
@@ -50,8 +55,11 @@ __global__ void init_parent(int *parent, long long n) {
   if (i < n) parent[i] = (int)i;
 }
 
-// The 13 neighbours with a positive flat offset: dz > 0, or dz == 0 and dy > 0, or dz == dy == 0
-// and dx > 0.
+// The 13 neighbours with a positive flat offset (dz > 0, or dz == 0 and dy > 0, or dz == dy == 0
+// and dx > 0). A face pair of equal labels is always united. An edge pair is skipped when one of
+// its two face-adjacent intermediates has the label (the pair is then joined through it), a corner
+// pair when one of its three face or three edge intermediates has it: by induction over face ->
+// edge -> corner every skipped pair still ends in one component.
 template <class L>
 __global__ void union_forward(const L *labels, int *parent, Dims d) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -60,14 +68,24 @@ __global__ void union_forward(const L *labels, int *parent, Dims d) {
   if (lv == 0) return;
   int x, y, z;
   unravel((int)i, d, x, y, z);
+  auto same = [&](int dx, int dy, int dz) {
+    const int nx = x + dx, ny = y + dy, nz = z + dz;
+    if (nx < 0 || ny < 0 || nz < 0 || nx >= d.sx || ny >= d.sy || nz >= d.sz) return false;
+    return labels[i + dx + (long long)d.sx * (dy + (long long)d.sy * dz)] == lv;
+  };
 #pragma unroll
   for (int k = 0; k < 26; ++k) {
     const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
     if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
-    const int nx = x + dx, ny = y + dy, nz = z + dz;
-    if (nx < 0 || ny < 0 || nx >= d.sx || ny >= d.sy || nz >= d.sz) continue;
-    const int u = (int)i + nbr_offset(k, d);
-    if (labels[u] == lv) unite(parent, (int)i, u);
+    if (!same(dx, dy, dz)) continue;
+    const int nonzero = (dx != 0) + (dy != 0) + (dz != 0);
+    if (nonzero == 2) {
+      if ((dx && same(dx, 0, 0)) || (dy && same(0, dy, 0)) || (dz && same(0, 0, dz))) continue;
+    } else if (nonzero == 3) {
+      if (same(dx, 0, 0) || same(0, dy, 0) || same(0, 0, dz) || same(dx, dy, 0) || same(dx, 0, dz) || same(0, dy, dz))
+        continue;
+    }
+    unite(parent, (int)i, (int)i + nbr_offset(k, d));
   }
 }
 

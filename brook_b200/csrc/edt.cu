@@ -105,6 +105,14 @@ __global__ void edt_envelope(const uint32_t *__restrict__ ids, float *__restrict
     const uint32_t L = ids[base + (long long)i * stride];
     int c = i, e = i;
     while (e + 1 < n && ids[base + (long long)(e + 1) * stride] == L) ++e;
+    if (L == 0) {
+      // A run's envelope only reads and writes the run itself, and background ends at 0: the
+      // background runs are skipped (the last pass writes their zeros).
+      if (finish)
+        for (int q = c; q <= e; ++q) D[base + (long long)q * stride] = 0.0f;
+      i = e + 1;
+      continue;
+    }
     const bool leftw = c > 0 || bb, rightw = e < n - 1 || bb;
     int k = -1;
     if (leftw) { k = 0; V[0] = c - 1; H[0] = 0.0f; Z[0] = -1e300; }
@@ -181,7 +189,7 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
   for (int axis = 1; axis < dims; ++axis) {
     const int len = axis == 1 ? vd.sy : vd.sz;
     const long long lines = axis == 1 ? (long long)vd.sx * vd.sz : (long long)vd.sx * vd.sy;
-    const long long budget = 512LL << 20;  // bytes of envelope stacks per batch
+    const long long budget = 4LL << 30;  // bytes of envelope stacks per batch
     long long batch = std::max(1LL, std::min(lines, budget / (16LL * (len + 3))));
     Buffer<int> V(ctx, batch * (len + 3));
     Buffer<float> H(ctx, batch * (len + 3));

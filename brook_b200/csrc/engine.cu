@@ -1,6 +1,14 @@
-// Object engine kernels (see engine.hpp). Each CTA runs one object's chain; every flood round is
-// "one warp per frontier voxel, one lane per neighbour" followed by a block barrier. State other
-// lanes update with atomics (distances, keys, flags, liveness, rails) is always read through L2.
+// Object engine kernels (see engine.hpp). A "group" — one CTA, or a cluster of kClusterCtas CTAs
+// for a large object — runs one object's chain. Every frontier round has two steps separated by a
+// group barrier: step A stages each frontier voxel (flag cleared, distance read, neighbour mask),
+// step B spreads its (voxel, neighbour) items over every thread of the group, so that thousands of
+// independent relaxations are in flight at once. The group's counters live in the shared memory
+// of its first CTA (distributed shared memory for a cluster, updated with 32-bit atomics only);
+// 64-bit reductions (nearest rail, nearest deferred voxel, argmax) keep one copy per CTA, updated
+// with CTA-local atomics and combined across the group at barriers. State other threads update
+// with atomics (distances, keys, flags, liveness, rails, staged entries) is always read through L2.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "engine.hpp"
 #include "runtime.hpp"
@@ -8,23 +16,36 @@
 namespace bk {
 namespace {
 
-constexpr int kWarps = kEngineThreads / 32;
+namespace cg = cooperative_groups;
+
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr unsigned long long kMinFarNone = 0x7f8000007f800000ull;
 constexpr unsigned long long kClaimedMark = 0xFFFFFFFFFFFFFFFEull;
 
 struct Shared {
+  // the object (written by the group's first CTA, copied by the others)
   int obj, begin, count, status;
-  int a0, sx, sy, sz;  // the object's arena
-  int n_cur, n_next, n_far, n_keep, n_touch, flag;
-  unsigned lowest;
+  int a0, sx, sy, sz;
+  // group counters (used in the first CTA's copy)
+  int cnt[3];  // frontier counters, a ring: current = cnt[r % 3], next = cnt[(r + 1) % 3]
+  int n_far, n_keep, n_touch, flag, len;
   float T;
+  unsigned long long rounds;
+  // per-CTA copies, combined with Group::min_over / max_over
   unsigned long long rb, minfar, best;
+  unsigned lowest, pos;
+  // this CTA's copy of the object's neighbour offsets and step weights
   int off[26];
   float w[26];
 };
 
 __device__ __forceinline__ float inf() { return __uint_as_float(BK_INF_BITS); }
+
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ void unravel3(int i, int sx, int sy, int &x, int &y, int &z) {
   const int sxy = sx * sy;
@@ -34,27 +55,99 @@ __device__ __forceinline__ void unravel3(int i, int sx, int sy, int &x, int &y, 
   x = r - y * sx;
 }
 
-// Minimum of a 64-bit value over the warp (two 32-bit reductions).
-__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
-  const unsigned hi = __reduce_min_sync(kFull, unsigned(v >> 32));
-  const unsigned lo = __reduce_min_sync(kFull, unsigned(v >> 32) == hi ? unsigned(v) : 0xFFFFFFFFu);
-  return (static_cast<unsigned long long>(hi) << 32) | lo;
+__device__ __forceinline__ unsigned long long pack3(int x, int y, int z) {
+  return (unsigned long long)x | ((unsigned long long)y << 21) | ((unsigned long long)z << 42);
+}
+__device__ __forceinline__ void unpack3(unsigned long long p, int &x, int &y, int &z) {
+  x = int(p & 0x1FFFFF);
+  y = int((p >> 21) & 0x1FFFFF);
+  z = int(p >> 42);
 }
 
-// Pulls the next object for this CTA and sets up its arena frame; false when the queue is empty.
-__device__ bool next_object(const EngineArgs &a, Shared &sh) {
+// A group of C CTAs working on one object. For C == 1 it is the CTA.
+template <int C>
+struct Group {
+  __device__ static int rank() {
+    if constexpr (C == 1) return 0;
+    else return int(cg::this_cluster().block_rank());
+  }
+  __device__ static void sync() {
+    if constexpr (C == 1) __syncthreads();
+    else cg::this_cluster().sync();
+  }
+  __device__ static Shared *leader(Shared *own) {
+    if constexpr (C == 1) return own;
+    else return cg::this_cluster().map_shared_rank(own, 0);
+  }
+  __device__ static int tid() { return rank() * int(blockDim.x) + int(threadIdx.x); }
+  // Least / greatest of the group's copies of a per-CTA field (plain loads; call between barriers).
+  __device__ static unsigned long long min_over(unsigned long long *own) {
+    if constexpr (C == 1) return *(volatile unsigned long long *)own;
+    else {
+      unsigned long long r = ~0ull;
+      for (int q = 0; q < C; ++q) {
+        const unsigned long long v = *(volatile unsigned long long *)cg::this_cluster().map_shared_rank(own, q);
+        r = v < r ? v : r;
+      }
+      return r;
+    }
+  }
+  __device__ static unsigned min_over(unsigned *own) {
+    if constexpr (C == 1) return *(volatile unsigned *)own;
+    else {
+      unsigned r = ~0u;
+      for (int q = 0; q < C; ++q) {
+        const unsigned v = *(volatile unsigned *)cg::this_cluster().map_shared_rank(own, q);
+        r = v < r ? v : r;
+      }
+      return r;
+    }
+  }
+  __device__ static unsigned long long max_over(unsigned long long *own) {
+    if constexpr (C == 1) return *(volatile unsigned long long *)own;
+    else {
+      unsigned long long r = 0;
+      for (int q = 0; q < C; ++q) {
+        const unsigned long long v = *(volatile unsigned long long *)cg::this_cluster().map_shared_rank(own, q);
+        r = v > r ? v : r;
+      }
+      return r;
+    }
+  }
+  __device__ static int threads() { return C * int(blockDim.x); }
+  __device__ static bool first() { return rank() == 0 && threadIdx.x == 0; }
+};
+
+template <class T>
+__device__ __forceinline__ T vload(const T *p) { return *(const volatile T *)p; }
+
+// Pulls the next object for this group; false when its queue is empty. The group's first CTA
+// pops and publishes; every CTA copies the object into its own shared memory.
+template <int C>
+__device__ bool next_object(const EngineArgs &a, Shared &sh, Shared *L, bool big) {
+  using G = Group<C>;
+  if (G::first()) {
+    const int j = atomicAdd(a.queue + (big ? 0 : 1), 1);
+    const int limit = big ? a.nbig : a.nobj - a.nbig;
+    L->obj = j < limit ? a.schedule[big ? j : a.nbig + j] : -1;
+    if (L->obj >= 0) {
+      const int o = L->obj;
+      L->begin = a.obj_begin[o];
+      L->count = a.obj_count[o];
+      L->status = a.status[o];  // kOk unless an earlier pass gave up on the object
+      const int r = a.obj_arena[o];
+      L->a0 = a.arena_offset[r];
+      L->sx = a.arena_dims[3 * r];
+      L->sy = a.arena_dims[3 * r + 1];
+      L->sz = a.arena_dims[3 * r + 2];
+    }
+  }
+  G::sync();
   if (threadIdx.x == 0) {
-    const int j = atomicAdd(a.queue, 1);
-    sh.obj = j < a.nobj ? a.schedule[j] : -1;
+    sh.obj = vload(&L->obj);
     if (sh.obj >= 0) {
-      sh.begin = a.obj_begin[sh.obj];
-      sh.count = a.obj_count[sh.obj];
-      sh.status = kOk;
-      const int r = a.obj_arena[sh.obj];
-      sh.a0 = a.arena_offset[r];
-      sh.sx = a.arena_dims[3 * r];
-      sh.sy = a.arena_dims[3 * r + 1];
-      sh.sz = a.arena_dims[3 * r + 2];
+      sh.begin = vload(&L->begin); sh.count = vload(&L->count);
+      sh.a0 = vload(&L->a0); sh.sx = vload(&L->sx); sh.sy = vload(&L->sy); sh.sz = vload(&L->sz);
     }
   }
   __syncthreads();
@@ -63,7 +156,8 @@ __device__ bool next_object(const EngineArgs &a, Shared &sh) {
     sh.off[k] = c_dx[k] + sh.sx * (c_dy[k] + sh.sy * c_dz[k]);
     sh.w[k] = a.w[k];
   }
-  __syncthreads();
+  // every CTA has its copy before the first CTA moves on (or exits, ending its shared memory)
+  G::sync();
   return sh.obj >= 0;
 }
 
@@ -71,57 +165,57 @@ __device__ bool next_object(const EngineArgs &a, Shared &sh) {
 // Geometric flood from `source` over the object's voxels into `d` (+inf at rest on them):
 // Bellman-Ford rounds, fl(d[u] + w[k]). The fixed point is the least float32 path sum, which any
 // schedule reaches. Returns false when the round bound is hit.
-__device__ bool flood_geometric(const EngineArgs &a, Shared &sh, float *d, int source, int *A, int *B) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
+template <int C>
+__device__ bool flood_geometric(const EngineArgs &a, Shared &sh, Shared *L, float *d, int source, int *A, int *B,
+                                unsigned long long *wide) {
+  using G = Group<C>;
+  if (G::first()) {
     d[source] = 0.0f;
     atomicOr(a.flags + source, kNearQueued);
     A[0] = source;
-    sh.n_cur = 1;
-    sh.n_next = 0;
+    L->cnt[0] = 1; L->cnt[1] = 0; L->cnt[2] = 0;
   }
-  __syncthreads();
-  int *cur = A, *nxt = B;
+  G::sync();
   const long long bound = 8LL * sh.count + 256;
-  for (long long round = 0;; ++round) {
-    const int nc = sh.n_cur;
+  for (int r = 0;; ++r) {
+    int *cur = (r & 1) ? B : A, *nxt = (r & 1) ? A : B;
+    const int nc = vload(&L->cnt[r % 3]);
     if (nc == 0) break;
-    if (round >= bound) return false;
-    for (int i = warp; i < nc; i += kWarps) {
-      int u = 0;
-      float du = 0.0f;
-      uint32_t m = 0;
-      if (lane == 0) {
-        u = __ldcg(cur + i);
-        const unsigned was = atomicAnd(a.flags + u, ~kNearQueued);
-        du = __ldcg(d + u + (was >> 30));
-        m = a.mask[u];
-      }
-      u = __shfl_sync(kFull, u, 0);
-      du = __shfl_sync(kFull, du, 0);
-      m = __shfl_sync(kFull, m, 0);
-      if (lane < 26 && ((m >> lane) & 1u)) {
-        const int v = u + sh.off[lane];
-        const float cand = __fadd_rn(du, sh.w[lane]);
-        const float old = atomic_min_pos(d + v, cand);
-        if (old > cand && !(atomicOr(a.flags + v, kNearQueued) & kNearQueued)) nxt[atomicAdd(&sh.n_next, 1)] = v;
-      }
+    if (r >= bound) return false;
+    if (G::first()) L->cnt[(r + 2) % 3] = 0;
+    for (int i = G::tid(); i < nc; i += G::threads()) {
+      const int u = __ldcg(cur + i);
+      const unsigned was = atomicAnd(a.flags + u, ~kNearQueued);
+      const float du = __ldcg(d + u + (was >> 30));
+      wide[i] = (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) { sh.n_cur = sh.n_next; sh.n_next = 0; }
-    int *t = cur; cur = nxt; nxt = t;
-    __syncthreads();
+    G::sync();
+    int *next_count = &L->cnt[(r + 1) % 3];
+    for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
+      const int k = int(j & 31);
+      if (k >= 26) continue;
+      const int i = int(j >> 5);
+      const unsigned long long e = __ldcg(wide + i);
+      if (!((unsigned(e) >> k) & 1u)) continue;
+      const int v = __ldcg(cur + i) + sh.off[k];
+      const float cand = __fadd_rn(__uint_as_float(unsigned(e >> 32)), sh.w[k]);
+      const float old = atomic_min_pos(d + v, cand);
+      if (old > cand && !(atomicOr(a.flags + v, kNearQueued) & kNearQueued)) nxt[atomicAdd(next_count, 1)] = v;
+    }
+    G::sync();
   }
   return true;
 }
 
-// Largest finite value of `f` over the object's voxels, ties -> lowest flat index. Returns the
-// packed key (value bits << 32 | ~flat), 0 when nothing is finite.
-__device__ unsigned long long object_argmax(const EngineArgs &a, Shared &sh, const float *f) {
+// Largest finite value of `f` over the object's voxels, ties -> lowest flat index: the packed key
+// (value bits << 32 | ~flat), 0 when nothing is finite.
+template <int C>
+__device__ unsigned long long object_argmax(const EngineArgs &a, Shared &sh, Shared *L, const float *f) {
+  using G = Group<C>;
   if (threadIdx.x == 0) sh.best = 0;
-  __syncthreads();
+  G::sync();
   unsigned long long best = 0;
-  for (int i = threadIdx.x; i < sh.count; i += blockDim.x) {
+  for (int i = G::tid(); i < sh.count; i += G::threads()) {
     const int v = a.vox[sh.begin + i];
     const float x = __ldcg(f + v);
     if (x < inf()) {
@@ -132,28 +226,40 @@ __device__ unsigned long long object_argmax(const EngineArgs &a, Shared &sh, con
   const unsigned hi = __reduce_max_sync(kFull, unsigned(best >> 32));
   const unsigned lo = __reduce_max_sync(kFull, unsigned(best >> 32) == hi ? unsigned(best) : 0u);
   if ((threadIdx.x & 31) == 0) atomicMax(&sh.best, (static_cast<unsigned long long>(hi) << 32) | lo);
-  __syncthreads();
-  const unsigned long long r = sh.best;
-  __syncthreads();
+  G::sync();
+  const unsigned long long r = G::max_over(&sh.best);
+  G::sync();
   return r;
 }
 
-__global__ void __launch_bounds__(kEngineThreads) prepare_kernel(EngineArgs a) {
+template <int C>
+__device__ void prepare_loop(const EngineArgs &a, bool big) {
+  using G = Group<C>;
   __shared__ Shared sh;
-  while (next_object(a, sh)) {
+  Shared *L = G::leader(&sh);
+  while (next_object<C>(a, sh, L, big)) {
     const int o = sh.obj;
     int *A = a.lists + sh.begin, *B = a.lists + a.F + sh.begin;
+    unsigned long long *wide = a.wide + sh.begin;
     int root = a.border_root[o];
+    bool ok = true;
     if (root < 0) {
       // the farthest voxel (geometric distance) from the object's first voxel
-      if (!flood_geometric(a, sh, a.daf, a.vox[sh.begin], A, B)) { if (threadIdx.x == 0) a.status[o] = kBudget; continue; }
-      const unsigned long long k = object_argmax(a, sh, a.daf);
-      root = int(0xFFFFFFFFu - unsigned(k));
-      for (int i = threadIdx.x; i < sh.count; i += blockDim.x) a.daf[a.vox[sh.begin + i]] = inf();
-      __syncthreads();
+      ok = flood_geometric<C>(a, sh, L, a.daf, a.vox[sh.begin], A, B, wide);
+      if (ok) {
+        const unsigned long long k = object_argmax<C>(a, sh, L, a.daf);
+        root = int(0xFFFFFFFFu - unsigned(k));
+        for (int i = G::tid(); i < sh.count; i += G::threads()) a.daf[a.vox[sh.begin + i]] = inf();
+        G::sync();
+      }
     }
-    if (!flood_geometric(a, sh, a.daf, root, A, B)) { if (threadIdx.x == 0) a.status[o] = kBudget; continue; }
-    const unsigned long long k = object_argmax(a, sh, a.daf);
+    if (ok) ok = flood_geometric<C>(a, sh, L, a.daf, root, A, B, wide);
+    if (!ok) {
+      if (G::first()) a.status[o] = kBudget;
+      G::sync();
+      continue;
+    }
+    const unsigned long long k = object_argmax<C>(a, sh, L, a.daf);
     const float farthest = __uint_as_float(unsigned(k >> 32));
     const int target = int(0xFFFFFFFFu - unsigned(k));
     // PDRF of the object's voxels (the reference's pdrf_lab, batched_regular.inc:93-108):
@@ -161,7 +267,7 @@ __global__ void __launch_bounds__(kEngineThreads) prepare_kernel(EngineArgs a) {
     const float M = a.M[o];
     const bool with_daf = farthest != 0.0f;
     const float inv = with_daf ? __double2float_rn(__ddiv_rn(1.0, (double)farthest)) : 0.0f;
-    for (int i = threadIdx.x; i < sh.count; i += blockDim.x) {
+    for (int i = G::tid(); i < sh.count; i += G::threads()) {
       const int v = a.vox[sh.begin + i];
       float dv = a.dbf[v];
       if (dv == 0.0f) dv = inf();
@@ -175,139 +281,171 @@ __global__ void __launch_bounds__(kEngineThreads) prepare_kernel(EngineArgs a) {
       }
       a.pdrf[v] = p;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    G::sync();
+    if (G::first()) {
       a.pdrf[root] = 0.0f;  // the root is the first rail
       a.root[o] = root;
       a.target[o] = target;
       a.max_daf[o] = farthest;
     }
-    __syncthreads();
+    G::sync();
   }
 }
+
+__global__ void __launch_bounds__(kEngineThreads) prepare_small(EngineArgs a) { prepare_loop<1>(a, false); }
+__global__ void __launch_bounds__(kEngineThreads) prepare_big(EngineArgs a) { prepare_loop<kClusterCtas>(a, true); }
 
 // ---------------------------------------------------------------------------------------------
 // Railroad flood from target t over the object's voxels: entering v costs pdrf[v] (vw_step), rails
 // (pdrf == 0) absorb. Near-far bands: the near band [.., T] is relaxed to convergence, bounded by
 // the best rail found so far; the next band starts at the nearest deferred voxel. Returns the
-// nearest rail as (distance bits << 32 | flat), BK_UNCLAIMED when no rail is reachable, and
-// sets sh.status on a bound. The result is schedule-independent: every voxel at distance <= D
-// (the nearest rail's) is exact when the flood stops.
-__device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, int t, int *A, int *B, int *FA, int *FB,
-                                       int *touched) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// nearest rail as (distance bits << 32 | flat), BK_UNCLAIMED when no rail is reachable, and sets
+// L->status on a bound. The result is schedule-independent: every voxel at distance <= D (the
+// nearest rail's) is exact when the flood stops.
+template <int C>
+__device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *L, int t, int *A, int *B, int *FA,
+                                       int *FB, int *touched, unsigned long long *wide) {
+  using G = Group<C>;
   if (threadIdx.x == 0) {
-    sh.n_touch = 1;
-    touched[0] = t;
     sh.rb = BK_UNCLAIMED;
     sh.minfar = kMinFarNone;
-    sh.n_cur = 0; sh.n_next = 0; sh.n_far = 0; sh.n_keep = 0;
+  }
+  if (G::first()) {
+    L->n_touch = 1;
+    touched[0] = t;
+    L->cnt[0] = 0; L->cnt[1] = 0; L->cnt[2] = 0;
+    L->n_far = 0; L->n_keep = 0;
     a.dist[t] = 0.0f;
     const float ft = __ldcg(a.pdrf + t);
     if (ft == 0.0f) sh.rb = static_cast<unsigned long long>(unsigned(t));
     else {
       A[0] = t;
-      sh.n_cur = 1;
+      L->cnt[0] = 1;
       atomicOr(a.flags + t, kNearQueued);
-      sh.T = fmaxf(__fmul_rn(2.0f, ft), 1e-30f);
+      L->T = fmaxf(__fmul_rn(2.0f, ft), 1e-30f);
     }
   }
-  __syncthreads();
-  if (sh.rb != BK_UNCLAIMED) return sh.rb;
-  int *cur = A, *nxt = B, *far = FA, *keep = FB;
+  G::sync();
+  {
+    const unsigned long long rb = G::min_over(&sh.rb);
+    if (rb != BK_UNCLAIMED) {
+      G::sync();
+      return rb;
+    }
+  }
+  int *far = FA, *keep = FB;
   const long long bound = 16LL * sh.count + 256;
   long long work = 0;
+  int r = 0;
   for (;;) {
-    for (;;) {
-      const int nc = sh.n_cur;
+    for (;; ++r) {
+      int *cur = (r & 1) ? B : A, *nxt = (r & 1) ? A : B;
+      const int nc = vload(&L->cnt[r % 3]);
       if (nc == 0) break;
-      if (++work > bound) { if (threadIdx.x == 0) sh.status = kBudget; __syncthreads(); return BK_UNCLAIMED; }
-      const float T = sh.T;
-      for (int i = warp; i < nc; i += kWarps) {
-        int u = 0;
-        float du = -1.0f, Tb = 0.0f;
-        uint32_t m = 0;
-        if (lane == 0) {
-          u = __ldcg(cur + i);
-          const unsigned was = atomicAnd(a.flags + u, ~kNearQueued);
-          const float fu = __ldcg(a.pdrf + u);
-          const float d = __ldcg(a.dist + u + (was >> 30));
-          const unsigned long long rb = *(volatile unsigned long long *)&sh.rb;
-          Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
-          if (fu != 0.0f && d <= Tb) { du = d; m = a.mask[u]; }
-        }
-        du = __shfl_sync(kFull, du, 0);
-        if (du < 0.0f) continue;
-        u = __shfl_sync(kFull, u, 0);
-        m = __shfl_sync(kFull, m, 0);
-        Tb = __shfl_sync(kFull, Tb, 0);
-        if (lane < 26 && ((m >> lane) & 1u)) {
-          const int v = u + sh.off[lane];
-          const float fv = __ldcg(a.pdrf + v);
-          const float cand = vw_step(du, fv);
-          const float old = atomic_min_pos(a.dist + v, cand);
-          if (old > cand) {
-            if (old == inf()) touched[atomicAdd(&sh.n_touch, 1)] = v;
-            if (fv == 0.0f)
-              atomicMin(&sh.rb, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | unsigned(v));
-            if (cand <= Tb) {
-              if (!(atomicOr(a.flags + v, kNearQueued) & kNearQueued)) nxt[atomicAdd(&sh.n_next, 1)] = v;
-            } else {
-              atomicMin(&sh.minfar, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | __float_as_uint(fv));
-              if (!(atomicOr(a.flags + v, kFarQueued) & kFarQueued)) far[atomicAdd(&sh.n_far, 1)] = v;
-            }
+      if (++work > bound) {
+        if (G::first()) L->status = kBudget;
+        G::sync();
+        return BK_UNCLAIMED;
+      }
+      if (G::first()) { L->cnt[(r + 2) % 3] = 0; L->rounds += 1; }
+      const float T = vload(&L->T);
+      for (int i = G::tid(); i < nc; i += G::threads()) {
+        const int u = __ldcg(cur + i);
+        const unsigned was = atomicAnd(a.flags + u, ~kNearQueued);
+        const float fu = __ldcg(a.pdrf + u);
+        const float du = __ldcg(a.dist + u + (was >> 30));
+        const unsigned long long rb = vload(&sh.rb);
+        const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
+        const bool expand = fu != 0.0f && du <= Tb;
+        wide[i] = expand ? (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u] : 0ull;
+      }
+      G::sync();
+      int *next_count = &L->cnt[(r + 1) % 3];
+      for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
+        const int k = int(j & 31);
+        if (k >= 26) continue;
+        const int i = int(j >> 5);
+        const unsigned long long e = __ldcg(wide + i);
+        if (!((unsigned(e) >> k) & 1u)) continue;
+        const int v = __ldcg(cur + i) + sh.off[k];
+        const float du = __uint_as_float(unsigned(e >> 32));
+        const float fv = __ldcg(a.pdrf + v);
+        const float cand = vw_step(du, fv);
+        const float old = atomic_min_pos(a.dist + v, cand);
+        if (old > cand) {
+          if (old == inf()) touched[atomicAdd(&L->n_touch, 1)] = v;
+          if (fv == 0.0f) atomicMin(&sh.rb, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | unsigned(v));
+          const unsigned long long rb = vload(&sh.rb);
+          const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
+          if (cand <= Tb) {
+            if (!(atomicOr(a.flags + v, kNearQueued) & kNearQueued)) nxt[atomicAdd(next_count, 1)] = v;
+          } else {
+            atomicMin(&sh.minfar, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | __float_as_uint(fv));
+            if (!(atomicOr(a.flags + v, kFarQueued) & kFarQueued)) far[atomicAdd(&L->n_far, 1)] = v;
           }
         }
       }
-      __syncthreads();
-      if (threadIdx.x == 0) { sh.n_cur = sh.n_next; sh.n_next = 0; }
-      int *tmp = cur; cur = nxt; nxt = tmp;
-      __syncthreads();
+      G::sync();
     }
     // band end: the nearest rail is final once it lies inside the band
-    if (threadIdx.x == 0) {
-      sh.flag = 0;
-      if (sh.rb != BK_UNCLAIMED && __uint_as_float(unsigned(sh.rb >> 32)) <= sh.T) sh.flag = 1;
-      else if (sh.minfar == kMinFarNone) sh.flag = 2;
+    if (G::first()) {
+      L->flag = 0;
+      const unsigned long long rb = G::min_over(&sh.rb), minfar = G::min_over(&sh.minfar);
+      sh.rb = rb;
+      if (rb != BK_UNCLAIMED && __uint_as_float(unsigned(rb >> 32)) <= L->T) L->flag = 1;
+      else if (minfar == kMinFarNone) L->flag = 2;
       else {
-        const float d = __uint_as_float(unsigned(sh.minfar >> 32)), f = __uint_as_float(unsigned(sh.minfar));
+        const float d = __uint_as_float(unsigned(minfar >> 32)), f = __uint_as_float(unsigned(minfar));
         float w = __fmul_rn(2.0f, f);
         const float lo = __fmul_rn(5e-4f, d);
         if (!(w > lo)) w = lo;
-        sh.T = __fadd_rn(d, w);
-        sh.minfar = kMinFarNone;
+        L->T = __fadd_rn(d, w);
       }
-      sh.n_keep = 0;
+      L->n_keep = 0;
+    }
+    G::sync();
+    // every CTA takes the combined rail and starts a fresh nearest-deferred minimum
+    if (threadIdx.x == 0) {
+      if (G::rank() != 0) sh.rb = vload(&L->rb);
+      sh.minfar = kMinFarNone;
     }
     __syncthreads();
-    if (sh.flag) return sh.flag == 1 ? sh.rb : BK_UNCLAIMED;
-    // promote deferred voxels inside the new band
-    const int nf = sh.n_far;
-    const unsigned long long rb = sh.rb;
-    const float Tp = rb != BK_UNCLAIMED ? fminf(sh.T, __uint_as_float(unsigned(rb >> 32))) : sh.T;
-    for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+    const int flag = vload(&L->flag);
+    if (flag) {
+      const unsigned long long rb = vload(&sh.rb);
+      G::sync();
+      return flag == 1 ? rb : BK_UNCLAIMED;
+    }
+    // promote deferred voxels inside the new band into the current near list
+    int *cur = (r & 1) ? B : A;
+    const int nf = vload(&L->n_far);
+    const unsigned long long rb = vload(&sh.rb);
+    const float T = vload(&L->T);
+    const float Tp = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
+    int *cur_count = &L->cnt[r % 3];
+    for (int i = G::tid(); i < nf; i += G::threads()) {
       const int w = __ldcg(far + i);
       const float dw = __ldcg(a.dist + w);
       if (dw <= Tp) {
         atomicAnd(a.flags + w, ~kFarQueued);
-        if (!(atomicOr(a.flags + w, kNearQueued) & kNearQueued)) cur[atomicAdd(&sh.n_cur, 1)] = w;
+        if (!(atomicOr(a.flags + w, kNearQueued) & kNearQueued)) cur[atomicAdd(cur_count, 1)] = w;
       } else {
         atomicMin(&sh.minfar, (static_cast<unsigned long long>(__float_as_uint(dw)) << 32) | __float_as_uint(__ldcg(a.pdrf + w)));
-        keep[atomicAdd(&sh.n_keep, 1)] = w;
+        keep[atomicAdd(&L->n_keep, 1)] = w;
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) sh.n_far = sh.n_keep;
+    G::sync();
+    if (G::first()) L->n_far = L->n_keep;
     int *tmp = far; far = keep; keep = tmp;
-    __syncthreads();
+    G::sync();
   }
 }
 
-// Warp 0 walks from the nearest rail back to the target: the step goes to the neighbour of least
+// One warp walks from the nearest rail back to the target: the step goes to the neighbour of least
 // distance (non-rail, lowest neighbour index among ties); at the first step the rail end is
 // re-picked as the last road voxel's first rail in dijkstra3d order (lockstep_regular.inc:61-155).
 // Writes the path target-first to out and returns its length (-1: no room).
-__device__ int backtrace(const EngineArgs &a, Shared &sh, unsigned long long rb, int t, int *out, long long room) {
+__device__ int backtrace(const EngineArgs &a, const Shared &sh, unsigned long long rb, int t, int *out, long long room) {
   const int lane = threadIdx.x & 31;
   int cur = int(unsigned(rb));
   int len = 0;
@@ -352,9 +490,7 @@ __device__ int backtrace(const EngineArgs &a, Shared &sh, unsigned long long rb,
   return len;
 }
 
-__device__ __forceinline__ float straight(const EngineArgs &a, const Shared &sh, int x, int y, int z, int s) {
-  int qx, qy, qz;
-  unravel3(s - sh.a0, sh.sx, sh.sy, qx, qy, qz);
+__device__ __forceinline__ float distance_to(const EngineArgs &a, int x, int y, int z, int qx, int qy, int qz) {
   const float dx = __fmul_rn(a.wx, float(x - qx)), dy = __fmul_rn(a.wy, float(y - qy)), dz = __fmul_rn(a.wz, float(z - qz));
   return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
 }
@@ -377,162 +513,168 @@ __device__ __forceinline__ int band_of(unsigned mbits, float delta, int kmin) {
 // boundary). Offers beyond the band wait; at the boundary each waiting voxel takes the best offer
 // of its claimed neighbours, the smallest names the next band, those inside it are claimed.
 // Claimed voxels die. Returns false when a loop bound is hit.
-__device__ bool invalidate(const EngineArgs &a, Shared &sh, const int *path, int npath, int *A, int *B, int *FA,
-                           int *FB, int *touched, unsigned long long *wide) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) { sh.n_cur = 0; sh.n_next = 0; sh.n_far = 0; sh.n_keep = 0; sh.n_touch = 0; }
-  __syncthreads();
-  for (int i = threadIdx.x; i < npath; i += blockDim.x) {
-    const int p = path[i];
+template <int C>
+__device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int *path, int npath, int *A, int *B,
+                           int *FA, int *FB, int *touched, unsigned long long *wide, unsigned long long *side_u,
+                           unsigned long long *side_s) {
+  using G = Group<C>;
+  if (G::first()) { L->cnt[0] = 0; L->cnt[1] = 0; L->cnt[2] = 0; L->n_far = 0; L->n_keep = 0; L->n_touch = 0; }
+  G::sync();
+  for (int i = G::tid(); i < npath; i += G::threads()) {
+    const int p = __ldcg(path + i);
     if (!__ldcg(a.alive + p)) continue;
     const unsigned long long old = atomicMin(a.key + p, static_cast<unsigned long long>(unsigned(p)));
     if (old == BK_UNCLAIMED) {
       atomicOr(a.flags + p, kFront);
-      A[atomicAdd(&sh.n_cur, 1)] = p;
-      touched[atomicAdd(&sh.n_touch, 1)] = p;
+      A[atomicAdd(&L->cnt[0], 1)] = p;
+      touched[atomicAdd(&L->n_touch, 1)] = p;
     }
   }
-  __syncthreads();
-  int *cur = A, *nxt = B, *far = FA, *keep = FB;
+  G::sync();
+  int *far = FA, *keep = FB;
   const long long bound = 64LL * sh.count + 1024;
   long long work = 0;
-  int band = 0;
+  int band = 0, r = 0;
   for (;;) {
     unsigned hi = __float_as_uint(__fmul_rn(float(band + 1), a.delta));
-    for (;;) {
-      const int nc = sh.n_cur;
+    for (;; ++r) {
+      int *cur = (r & 1) ? B : A, *nxt = (r & 1) ? A : B;
+      const int nc = vload(&L->cnt[r % 3]);
       if (nc == 0) break;
       if (++work > bound) return false;
-      for (int i = threadIdx.x; i < nc; i += blockDim.x) {  // the round boundary's keys
+      if (G::first()) { L->cnt[(r + 2) % 3] = 0; L->rounds += 1ull << 32; }
+      // step A: the round boundary's key of each frontier voxel, and both positions
+      for (int i = G::tid(); i < nc; i += G::threads()) {
         const int u = __ldcg(cur + i);
-        wide[i] = __ldcg(a.key + u);
+        const unsigned long long k = __ldcg(a.key + u);
         atomicAnd(a.flags + u, ~kFront);
+        wide[i] = k;
+        int x, y, z;
+        unravel3(u - sh.a0, sh.sx, sh.sy, x, y, z);
+        side_u[i] = pack3(x, y, z);
+        unravel3(int(unsigned(k)) - sh.a0, sh.sx, sh.sy, x, y, z);
+        side_s[i] = pack3(x, y, z);
       }
-      __syncthreads();
-      for (int i = warp; i < nc; i += kWarps) {
-        int u = 0, s = 0, ux = 0, uy = 0, uz = 0, qx = 0, qy = 0, qz = 0;
-        unsigned mu = 0;
-        uint32_t m = 0;
-        float R = 0.0f;
-        if (lane == 0) {
-          u = __ldcg(cur + i);
-          const unsigned long long k = __ldcg(wide + i);
-          s = int(unsigned(k));
-          mu = unsigned(k >> 32);
-          m = a.mask[u];
-          R = reach(a, s);
-          unravel3(u - sh.a0, sh.sx, sh.sy, ux, uy, uz);
-          unravel3(s - sh.a0, sh.sx, sh.sy, qx, qy, qz);
-        }
-        u = __shfl_sync(kFull, u, 0); s = __shfl_sync(kFull, s, 0); mu = __shfl_sync(kFull, mu, 0);
-        m = __shfl_sync(kFull, m, 0); R = __shfl_sync(kFull, R, 0);
-        ux = __shfl_sync(kFull, ux, 0); uy = __shfl_sync(kFull, uy, 0); uz = __shfl_sync(kFull, uz, 0);
-        qx = __shfl_sync(kFull, qx, 0); qy = __shfl_sync(kFull, qy, 0); qz = __shfl_sync(kFull, qz, 0);
-        if (lane >= 26 || !((m >> lane) & 1u)) continue;
-        const int v = u + sh.off[lane];
+      G::sync();
+      int *next_count = &L->cnt[(r + 1) % 3];
+      for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
+        const int k = int(j & 31);
+        if (k >= 26) continue;
+        const int i = int(j >> 5);
+        const int u = __ldcg(cur + i);
+        if (!((a.mask[u] >> k) & 1u)) continue;
+        const int v = u + sh.off[k];
         if (!__ldcg(a.alive + v)) continue;
-        const float dx = __fmul_rn(a.wx, float(ux + c_dx[lane] - qx));
-        const float dy = __fmul_rn(a.wy, float(uy + c_dy[lane] - qy));
-        const float dz = __fmul_rn(a.wz, float(uz + c_dz[lane] - qz));
-        const float d = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
-        if (d >= R) continue;
+        const unsigned long long ku = __ldcg(wide + i);
+        const int s = int(unsigned(ku));
+        int ux, uy, uz, qx, qy, qz;
+        unpack3(__ldcg(side_u + i), ux, uy, uz);
+        unpack3(__ldcg(side_s + i), qx, qy, qz);
+        const float d = distance_to(a, ux + c_dx[k], uy + c_dy[k], uz + c_dz[k], qx, qy, qz);
+        if (d >= reach(a, s)) continue;
         unsigned mb = __float_as_uint(d);
+        const unsigned mu = unsigned(ku >> 32);
         if (mb < mu) mb = mu;
         if (mb < hi) {
           const unsigned long long cand = (static_cast<unsigned long long>(mb) << 32) | unsigned(s);
           const unsigned long long old = atomicMin(a.key + v, cand);
           if (old > cand) {
-            if (old == BK_UNCLAIMED) touched[atomicAdd(&sh.n_touch, 1)] = v;
-            if (!(atomicOr(a.flags + v, kFront) & kFront)) nxt[atomicAdd(&sh.n_next, 1)] = v;
+            if (old == BK_UNCLAIMED) touched[atomicAdd(&L->n_touch, 1)] = v;
+            if (!(atomicOr(a.flags + v, kFront) & kFront)) nxt[atomicAdd(next_count, 1)] = v;
           }
         } else if (__ldcg(a.key + v) == BK_UNCLAIMED) {
-          if (!(atomicOr(a.flags + v, kWaiting) & kWaiting)) far[atomicAdd(&sh.n_far, 1)] = v;
+          if (!(atomicOr(a.flags + v, kWaiting) & kWaiting)) far[atomicAdd(&L->n_far, 1)] = v;
         }
       }
-      __syncthreads();
-      if (threadIdx.x == 0) { sh.n_cur = sh.n_next; sh.n_next = 0; }
-      int *tmp = cur; cur = nxt; nxt = tmp;
-      __syncthreads();
+      G::sync();
     }
-    const int nf = sh.n_far;
+    const int nf = vload(&L->n_far);
     if (nf == 0) break;
     if (++work > bound) return false;
     // band boundary: every waiting voxel pulls the best offer of its claimed neighbours
-    if (threadIdx.x == 0) { sh.lowest = BK_INF_BITS; sh.n_keep = 0; }
-    __syncthreads();
-    for (int i = warp; i < nf; i += kWarps) {
-      int c = 0;
-      unsigned long long kc = 0;
-      if (lane == 0) { c = __ldcg(far + i); kc = __ldcg(a.key + c); }
-      c = __shfl_sync(kFull, c, 0);
-      kc = __shfl_sync(kFull, kc, 0);
-      if (kc != BK_UNCLAIMED) { if (lane == 0) wide[i] = kClaimedMark; continue; }
-      const uint32_t m = a.mask[c];
-      unsigned long long best = BK_UNCLAIMED;
-      if (lane < 26 && ((m >> lane) & 1u)) {
-        const unsigned long long ku = __ldcg(a.key + c + sh.off[lane]);
-        if (ku != BK_UNCLAIMED) {
-          const int s = int(unsigned(ku));
-          int x, y, z;
-          unravel3(c - sh.a0, sh.sx, sh.sy, x, y, z);
-          const float d = straight(a, sh, x, y, z, s);
-          if (d < reach(a, s)) {
-            unsigned mb = __float_as_uint(d);
-            const unsigned mu = unsigned(ku >> 32);
-            if (mb < mu) mb = mu;
-            best = (static_cast<unsigned long long>(mb) << 32) | unsigned(s);
-          }
-        }
-      }
-      best = warp_min_u64(best);
-      if (lane == 0) {
-        wide[i] = best;
-        if (best != BK_UNCLAIMED) atomicMin(&sh.lowest, unsigned(best >> 32));
-      }
+    if (threadIdx.x == 0) sh.lowest = BK_INF_BITS;
+    if (G::first()) L->n_keep = 0;
+    for (int i = G::tid(); i < nf; i += G::threads()) {
+      const int c = __ldcg(far + i);
+      wide[i] = __ldcg(a.key + c) != BK_UNCLAIMED ? kClaimedMark : BK_UNCLAIMED;
+      int x, y, z;
+      unravel3(c - sh.a0, sh.sx, sh.sy, x, y, z);
+      side_u[i] = pack3(x, y, z);
     }
-    __syncthreads();
-    if (sh.lowest != BK_INF_BITS) band = band_of(sh.lowest, a.delta, band + 1);
+    G::sync();
+    for (long long j = G::tid(); j < (long long)nf * 32; j += G::threads()) {
+      const int k = int(j & 31);
+      if (k >= 26) continue;
+      const int i = int(j >> 5);
+      if (__ldcg(wide + i) == kClaimedMark) continue;
+      const int c = __ldcg(far + i);
+      if (!((a.mask[c] >> k) & 1u)) continue;
+      const unsigned long long ku = __ldcg(a.key + c + sh.off[k]);
+      if (ku == BK_UNCLAIMED) continue;
+      const int s = int(unsigned(ku));
+      int x, y, z, qx, qy, qz;
+      unpack3(__ldcg(side_u + i), x, y, z);
+      unravel3(s - sh.a0, sh.sx, sh.sy, qx, qy, qz);
+      const float d = distance_to(a, x, y, z, qx, qy, qz);
+      if (d >= reach(a, s)) continue;
+      unsigned mb = __float_as_uint(d);
+      const unsigned mu = unsigned(ku >> 32);
+      if (mb < mu) mb = mu;
+      atomicMin(wide + i, (static_cast<unsigned long long>(mb) << 32) | unsigned(s));
+      atomicMin(&sh.lowest, mb);
+    }
+    G::sync();
+    const unsigned lowest = G::min_over(&sh.lowest);
+    if (lowest != BK_INF_BITS) band = band_of(lowest, a.delta, band + 1);
     hi = __float_as_uint(__fmul_rn(float(band + 1), a.delta));
-    for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+    int *cur = (r & 1) ? B : A;
+    int *cur_count = &L->cnt[r % 3];
+    for (int i = G::tid(); i < nf; i += G::threads()) {
       const int c = __ldcg(far + i);
       const unsigned long long b = __ldcg(wide + i);
       if (b == kClaimedMark) continue;
       if (b == BK_UNCLAIMED) { atomicAnd(a.flags + c, ~kWaiting); continue; }
       if (unsigned(b >> 32) < hi) {
         a.key[c] = b;
-        touched[atomicAdd(&sh.n_touch, 1)] = c;
+        touched[atomicAdd(&L->n_touch, 1)] = c;
         atomicAnd(a.flags + c, ~kWaiting);
         atomicOr(a.flags + c, kFront);
-        cur[atomicAdd(&sh.n_cur, 1)] = c;
+        cur[atomicAdd(cur_count, 1)] = c;
       } else {
-        keep[atomicAdd(&sh.n_keep, 1)] = c;
+        keep[atomicAdd(&L->n_keep, 1)] = c;
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) sh.n_far = sh.n_keep;
+    G::sync();
+    if (G::first()) L->n_far = L->n_keep;
     int *tmp = far; far = keep; keep = tmp;
-    __syncthreads();
+    G::sync();
   }
-  const int nt = sh.n_touch;
-  for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+  const int nt = vload(&L->n_touch);
+  for (int i = G::tid(); i < nt; i += G::threads()) {
     const int v = __ldcg(touched + i);
     a.alive[v] = 0;
     a.key[v] = BK_UNCLAIMED;
     atomicAnd(a.flags + v, ~(kFront | kWaiting));
   }
-  __syncthreads();
+  G::sync();
   return true;
 }
 
-__global__ void __launch_bounds__(kEngineThreads) trace_kernel(EngineArgs a) {
+template <int C>
+__device__ void trace_loop(const EngineArgs &a, bool big) {
+  using G = Group<C>;
   __shared__ Shared sh;
-  __shared__ int s_pos;
   __shared__ unsigned long long s_work[4];
+  Shared *L = G::leader(&sh);
   if (threadIdx.x < 4) s_work[threadIdx.x] = 0;
-  while (next_object(a, sh)) {
+  while (next_object<C>(a, sh, L, big)) {
     const int o = sh.obj;
+    if (vload(&L->status) != kOk) {  // preparation failed; its status stands
+      G::sync();
+      continue;
+    }
     int *L0 = a.lists + sh.begin, *L1 = L0 + a.F, *L2 = L1 + a.F, *L3 = L2 + a.F, *L4 = L3 + a.F;
-    unsigned long long *wide = a.wide + sh.begin;
+    unsigned long long *wide = a.wide + sh.begin, *side_u = a.side + sh.begin, *side_s = a.side + a.F + sh.begin;
     int *store = a.store + a.store_begin[o];
     const long long store_cap = a.store_cap[o];
     int *rec_start = a.rec_start + a.rec_begin[o], *rec_len = a.rec_len + a.rec_begin[o];
@@ -544,6 +686,11 @@ __global__ void __launch_bounds__(kEngineThreads) trace_kernel(EngineArgs a) {
     long long paths = 0, used = 0;
     int cursor = 0;
     int status = kOk;
+    unsigned long long t_begin = 0, t_mark = 0, spent[4] = {0, 0, 0, 0};
+    if (G::first()) { L->rounds = 0; t_begin = t_mark = now_ns(); }
+    auto lap = [&](int phase) {
+      if (G::first()) { const unsigned long long t = now_ns(); spent[phase] += t - t_mark; t_mark = t; }
+    };
     while (paths < maxp) {
       // the next target: manual targets first, then the first alive voxel of the order
       int t = -1;
@@ -552,81 +699,124 @@ __global__ void __launch_bounds__(kEngineThreads) trace_kernel(EngineArgs a) {
         if (t < 0) t = a.target[o];  // the object's own target (the DAF argmax)
       } else {
         for (;;) {
-          if (threadIdx.x == 0) s_pos = INT32_MAX;
-          __syncthreads();
-          const int pos = cursor + threadIdx.x;
-          if (pos < sh.count && __ldcg(a.alive + order[pos])) atomicMin(&s_pos, pos);
-          __syncthreads();
-          const int found = s_pos;
-          __syncthreads();
+          if (threadIdx.x == 0) sh.pos = INT32_MAX;
+          G::sync();
+          const int pos = cursor + G::tid();
+          if (pos < sh.count && __ldcg(a.alive + order[pos])) atomicMin(&sh.pos, unsigned(pos));
+          G::sync();
+          const int found = int(G::min_over(&sh.pos));
+          G::sync();
           if (found != INT32_MAX) { cursor = found; t = order[found]; break; }
-          cursor += blockDim.x;
+          cursor += G::threads();
           if (cursor >= sh.count) { cursor = sh.count; break; }
         }
         if (t < 0) break;
       }
-      const unsigned long long rb = railroad(a, sh, t, L0, L1, L2, L3, L4);
-      if (sh.status != kOk) { status = sh.status; break; }
+      lap(0);
+      const unsigned long long rb = railroad<C>(a, sh, L, t, L0, L1, L2, L3, L4, wide);
+      lap(1);
+      if (vload(&L->status) != kOk) { status = vload(&L->status); break; }
       if (rb == BK_UNCLAIMED) { status = kNoRail; break; }
-      // walk (warp 0), then reset the flood's state over the voxels it touched
-      if (threadIdx.x < 32) {
+      // walk (one warp of the first CTA), then reset the flood's state over the voxels it touched
+      if (G::rank() == 0 && threadIdx.x < 32) {
         const int len = backtrace(a, sh, rb, t, store + used, store_cap - used);
-        if (threadIdx.x == 0) s_pos = len;
+        if (threadIdx.x == 0) L->len = len;
       }
-      __syncthreads();
-      const int len = s_pos;
-      const int nt = sh.n_touch;
+      G::sync();
+      const int len = vload(&L->len);
+      const int nt = vload(&L->n_touch);
       const float D = __uint_as_float(unsigned(rb >> 32));
       unsigned settled = 0;
-      for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+      for (int i = G::tid(); i < nt; i += G::threads()) {
         const int v = __ldcg(L4 + i);
         settled += __ldcg(a.dist + v) <= D;
         a.dist[v] = inf();
         atomicAnd(a.flags + v, ~(kNearQueued | kFarQueued));
       }
-      settled = __reduce_add_sync(0xFFFFFFFFu, settled);
+      settled = __reduce_add_sync(kFull, settled);
       if ((threadIdx.x & 31) == 0) atomicAdd(&s_work[0], (unsigned long long)settled);
-      if (threadIdx.x == 0) s_work[1] += nt;
-      __syncthreads();
+      if (G::first()) s_work[1] += nt;
+      G::sync();
+      lap(2);
       if (len < 0) { status = kStoreFull; break; }
       if (paths >= rec_cap) { status = kRecordsFull; break; }
-      if (!invalidate(a, sh, store + used, len, L0, L1, L2, L3, L4, wide)) { status = kBudget; break; }
-      if (threadIdx.x == 0) { s_work[2] += sh.n_touch; s_work[3] += 1; }
-      for (int i = threadIdx.x; i < len; i += blockDim.x) a.pdrf[store[used + i]] = 0.0f;
-      if (threadIdx.x == 0) { rec_start[paths] = int(used); rec_len[paths] = len; }
-      __syncthreads();
+      if (!invalidate<C>(a, sh, L, store + used, len, L0, L1, L2, L3, L4, wide, side_u, side_s)) { status = kBudget; break; }
+      if (G::first()) { s_work[2] += vload(&L->n_touch); s_work[3] += 1; }
+      lap(3);
+      for (int i = G::tid(); i < len; i += G::threads()) a.pdrf[__ldcg(store + used + i)] = 0.0f;
+      if (G::first()) { rec_start[paths] = int(used); rec_len[paths] = len; }
+      G::sync();
       used += len;
       ++paths;
     }
-    if (threadIdx.x == 0) {
+    if (G::first()) {
       a.status[o] = status;
       a.npaths[o] = int(paths);
       a.nstore[o] = int(used);
+      unsigned long long *pr = a.profile + 8LL * o;
+      pr[0] = t_begin; pr[1] = now_ns();
+      for (int q = 0; q < 4; ++q) pr[2 + q] = spent[q];
+      pr[6] = L->rounds & 0xFFFFFFFFull; pr[7] = L->rounds >> 32;
     }
-    __syncthreads();
+    G::sync();
   }
   if (threadIdx.x < 4 && s_work[threadIdx.x]) atomicAdd(a.work + threadIdx.x, s_work[threadIdx.x]);
 }
 
+__global__ void __launch_bounds__(kEngineThreads) trace_small(EngineArgs a) { trace_loop<1>(a, false); }
+__global__ void __launch_bounds__(kEngineThreads) trace_big(EngineArgs a) { trace_loop<kClusterCtas>(a, true); }
+
+int small_grid(const void *kernel, int sm_count, int count) {
+  int per_sm = 1;
+  BK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kEngineThreads, 0));
+  const int full = sm_count * (per_sm < 1 ? 1 : per_sm);
+  return count < full ? count : full;
+}
+
+cudaLaunchConfig_t cluster_config(int clusters, cudaStream_t stream, cudaLaunchAttribute *attr) {
+  cudaLaunchConfig_t config{};
+  config.gridDim = dim3(unsigned(clusters * kClusterCtas));
+  config.blockDim = dim3(kEngineThreads);
+  config.stream = stream;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kClusterCtas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  config.attrs = attr;
+  config.numAttrs = 1;
+  return config;
+}
+
+void launch_pair(const void *small, const void *big, const EngineArgs &a, int nbig, int sm_count, cudaStream_t s_small,
+                 cudaStream_t s_big) {
+  EngineArgs args = a;
+  args.nbig = nbig;
+  void *kargs[] = {&args};
+  if (nbig > 0) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t probe = cluster_config(1, s_big, attr);
+    int cap = 1;
+    BK_CUDA(cudaOccupancyMaxActiveClusters(&cap, big, &probe));
+    cap = cap < 1 ? 1 : cap;
+    // large objects first, on as many clusters as fit; small objects take the slots left over
+    // and those the clusters free when the large-object queue runs dry
+    const int clusters = nbig < cap ? nbig : cap;
+    cudaLaunchConfig_t config = cluster_config(clusters, s_big, attr);
+    BK_CUDA(cudaLaunchKernelExC(&config, big, kargs));
+  }
+  if (a.nobj > nbig)
+    BK_CUDA(cudaLaunchKernel(small, dim3(unsigned(small_grid(small, sm_count, a.nobj - nbig))), dim3(kEngineThreads),
+                             kargs, 0, s_small));
+}
+
 }  // namespace
 
-int engine_grid(int sm_count, int nobj, bool trace) {
-  int per_sm = 1;
-  BK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace ? (const void *)trace_kernel : (const void *)prepare_kernel,
-                                                        kEngineThreads, 0));
-  per_sm = per_sm < 1 ? 1 : per_sm;
-  const int full = sm_count * per_sm;
-  return nobj < full ? (nobj < 1 ? 1 : nobj) : full;
+void launch_prepare(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big) {
+  launch_pair((const void *)prepare_small, (const void *)prepare_big, a, nbig, sm_count, small, big);
 }
 
-void launch_prepare(const EngineArgs &a, int grid, cudaStream_t stream) {
-  prepare_kernel<<<grid, kEngineThreads, 0, stream>>>(a);
-  BK_CUDA(cudaGetLastError());
-}
-
-void launch_trace(const EngineArgs &a, int grid, cudaStream_t stream) {
-  trace_kernel<<<grid, kEngineThreads, 0, stream>>>(a);
-  BK_CUDA(cudaGetLastError());
+void launch_trace(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big) {
+  launch_pair((const void *)trace_small, (const void *)trace_big, a, nbig, sm_count, small, big);
 }
 
 }  // namespace bk

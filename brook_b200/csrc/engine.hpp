@@ -11,7 +11,7 @@
 
 namespace bk {
 
-constexpr int kEngineThreads = 512;
+constexpr int kEngineThreads = 512;  // threads per CTA
 
 // Per-voxel flag bits (uint32 per voxel, 0 at rest).
 constexpr unsigned kNearQueued = 1u;   // railroad / flood: in the next near list
@@ -46,11 +46,13 @@ struct EngineArgs {
   const int *obj_begin;  // offset of the object's voxels in vox and in the list pool
   const int *obj_count;
   const int *vox;        // voxels of every object, ascending flat index
-  const int *schedule;   // processing order (object indices)
-  int *queue;            // work counter (starts at 0)
+  const int *schedule;   // processing order (object indices): large objects first, then the rest
+  int nbig;              // schedule[0, nbig) run on clusters (set by launch_prepare / launch_trace)
+  int *queue;            // two work counters (large, small), both 0 at launch
   int *status;           // per object
   int *lists;            // 5 lists of F ints: list w of object o at lists + w * F + obj_begin[o]
-  unsigned long long *wide;  // F entries: object o at wide + obj_begin[o]
+  unsigned long long *wide;  // F entries: object o at wide + obj_begin[o] (per-entry staging)
+  unsigned long long *side;  // 2F entries: two more staging arrays (packed coordinates)
   long long F;
 
   // prepare
@@ -74,11 +76,25 @@ struct EngineArgs {
   // work counters (added over all objects): [0] voxels a railroad settled (distance <= its rail's),
   // [1] voxels a railroad touched, [2] voxels invalidated, [3] paths
   unsigned long long *work;
+  // per object (8 entries, nanoseconds of %globaltimer): start, end, time in target search,
+  // railroad, backtrace, invalidation; railroad rounds; invalidation rounds
+  unsigned long long *profile;
   float wx, wy, wz, scale, constant, delta;
 };
 
-void launch_prepare(const EngineArgs &a, int grid, cudaStream_t stream);
-void launch_trace(const EngineArgs &a, int grid, cudaStream_t stream);
-int engine_grid(int sm_count, int nobj, bool trace);
+// Objects with at least kPrepareClusterVoxels (preparation) / kTraceClusterVoxels (tracing)
+// voxels run on a cluster of kClusterCtas CTAs that share the object's frontiers through
+// distributed shared memory; smaller objects on one CTA each. Tracing keeps clusters for the
+// largest objects only: a cluster spends more CTA-time per object than a lone CTA, which pays
+// only where the object's own chain would otherwise set the kernel's length.
+constexpr int kClusterCtas = 8;
+constexpr int kPrepareClusterVoxels = 8192;
+constexpr int kTraceClusterVoxels = 65536;
+
+// One pass of the engine over two queues (schedule[0, nbig) = large objects, schedule[nbig,
+// nobj) = the rest, each largest first): the large ones on `big` (cluster launch), the rest on
+// `small`, concurrently. queue[0] / queue[1] must be zero.
+void launch_prepare(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big);
+void launch_trace(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big);
 
 }  // namespace bk

@@ -325,9 +325,18 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     arena_offset[v] = int(vs[v].offset);
     arena_dims[3 * v] = vs[v].d.sx; arena_dims[3 * v + 1] = vs[v].d.sy; arena_dims[3 * v + 2] = vs[v].d.sz;
   }
+  // largest objects first; the leading objects above a size threshold go to clusters
   std::vector<int> schedule(nobj);
   std::iota(schedule.begin(), schedule.end(), 0);
   std::stable_sort(schedule.begin(), schedule.end(), [&](int a, int b) { return obj_count[a] > obj_count[b]; });
+  auto leading = [&](const char *knob, long long voxels) {  // knob: tuning override from the environment
+    if (const char *e = std::getenv(knob)) voxels = std::atoll(e);
+    int n = 0;
+    while (n < nobj && obj_count[schedule[n]] >= voxels) ++n;
+    return n;
+  };
+  const int nbig_prepare = leading("BROOK_B200_PREPARE_CLUSTER_VOXELS", kPrepareClusterVoxels);
+  const int nbig_trace = leading("BROOK_B200_TRACE_CLUSTER_VOXELS", kTraceClusterVoxels);
   auto d_arena_offset = to_device(ctx, arena_offset), d_arena_dims = to_device(ctx, arena_dims);
   auto d_obj_arena = to_device(ctx, obj_arena), d_obj_begin = to_device(ctx, obj_begin), d_obj_count = to_device(ctx, obj_count);
   auto d_seg_end = to_device(ctx, seg_end), d_schedule = to_device(ctx, schedule), d_border_root = to_device(ctx, border_root);
@@ -339,7 +348,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   Buffer<int> queue(ctx, 2), status(ctx, nobj), root(ctx, nobj), target(ctx, nobj), npaths(ctx, nobj), nstore(ctx, nobj);
   Buffer<float> max_daf(ctx, nobj);
   Buffer<int> lists(ctx, 5 * F), store(ctx, store_total), rec_start(ctx, rec_total), rec_len(ctx, rec_total);
-  Buffer<unsigned long long> wide(ctx, F), work(ctx, 4);
+  Buffer<unsigned long long> wide(ctx, F), side(ctx, 2 * F), work(ctx, 4), profile(ctx, 8LL * nobj);
   queue.zero();
   status.zero();
   work.zero();
@@ -350,7 +359,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.flags = flags.data(); a.alive = alive.data(); a.key = key.data();
   a.nobj = nobj; a.obj_begin = d_obj_begin.data(); a.obj_count = d_obj_count.data(); a.vox = vox.data();
   a.schedule = d_schedule.data(); a.queue = queue.data(); a.status = status.data();
-  a.lists = lists.data(); a.wide = wide.data(); a.F = F;
+  a.lists = lists.data(); a.wide = wide.data(); a.side = side.data(); a.F = F;
   a.border_root = d_border_root.data(); a.M = d_M.data(); a.pdrf_scale = float(t.pdrf_scale); a.squarings = squarings;
   {
     const double x = aniso[0], y = aniso[1], z = aniso[2];
@@ -363,14 +372,16 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.manual_begin = d_manual_begin.data(); a.manual_count = d_manual_count.data(); a.manual = d_manual.data();
   a.max_paths = d_max_paths.data(); a.store = store.data(); a.store_begin = d_store_begin.data(); a.store_cap = d_store_cap.data();
   a.rec_start = rec_start.data(); a.rec_len = rec_len.data(); a.rec_begin = d_rec_begin.data(); a.rec_cap = d_rec_cap.data();
-  a.npaths = npaths.data(); a.nstore = nstore.data(); a.work = work.data();
+  a.npaths = npaths.data(); a.nstore = nstore.data(); a.work = work.data(); a.profile = profile.data();
   a.wx = aniso[0]; a.wy = aniso[1]; a.wz = aniso[2];
   a.scale = float(t.scale); a.constant = float(t.constant);
   a.delta = std::min({aniso[0], aniso[1], aniso[2]});
 
   clock.mark("state");
-  launch_prepare(a, engine_grid(ctx.sm_count(), nobj, false), s);
-  ++ctx.launches;
+  ctx.fork();
+  launch_prepare(a, nbig_prepare, ctx.sm_count(), s, ctx.side_stream());
+  ctx.join();
+  ctx.launches += (nbig_prepare > 0) + (nobj > nbig_prepare);
   clock.mark("prepare");
   if (const char *fields = std::getenv("BROOK_B200_DUMP_FIELDS")) {
     // diagnostics: the prepared DAF and PDRF (root rails included) as raw float32 files
@@ -382,10 +393,12 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   }
   Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), d_seg_end.data(), nobj);
   a.order = order.data();
-  BK_CUDA(cudaMemsetAsync(queue.data(), 0, sizeof(int), s));
+  BK_CUDA(cudaMemsetAsync(queue.data(), 0, 2 * sizeof(int), s));
   clock.mark("order");
-  launch_trace(a, engine_grid(ctx.sm_count(), nobj, true), s);
-  ++ctx.launches;
+  ctx.fork();
+  launch_trace(a, nbig_trace, ctx.sm_count(), s, ctx.side_stream());
+  ctx.join();
+  ctx.launches += (nbig_trace > 0) + (nobj > nbig_trace);
   clock.mark("trace");
 
   // ---- results
@@ -426,9 +439,13 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
           std::fprintf(f, "\n");
         }
       }
+      const auto hprof = profile.download();
       for (int o = 0; o < nobj; ++o) {
-        std::fprintf(f, "object %d volume %d id %u root %d target %d max_daf %.9g paths %d\n", o, objects[o].volume,
-                     objects[o].id, hroot[o], htarget[o], hmax[o], np[o]);
+        const unsigned long long *pr = hprof.data() + 8LL * o;
+        std::fprintf(f, "object %d volume %d id %u voxels %d root %d target %d max_daf %.9g paths %d "
+                     "t0 %llu t1 %llu target_ns %llu rail_ns %llu back_ns %llu inval_ns %llu rail_rounds %llu inval_rounds %llu\n",
+                     o, objects[o].volume, objects[o].id, obj_count[o], hroot[o], htarget[o], hmax[o], np[o], pr[0], pr[1],
+                     pr[2], pr[3], pr[4], pr[5], pr[6], pr[7]);
         for (int p = 0; p < np[o]; ++p) {
           std::fprintf(f, "path %d %d:", o, p);
           for (int q = 0; q < hlen[rdst[o] + p]; ++q) std::fprintf(f, " %d", hstore[vdst[o] + hstart[rdst[o] + p] + q]);
