@@ -10,6 +10,7 @@
 #include <numeric>
 #include <stdexcept>
 
+#include "assembly.hpp"
 #include "common.cuh"
 #include "engine.hpp"
 #include "order.hpp"
@@ -43,19 +44,15 @@ __global__ void offset_voxels(int *vox, long long n, int offset) {
   if (i < n) vox[i] += offset;
 }
 
-// Compacts the used prefix of every object's store region and gathers the DBF at each vertex.
+// Compacts the used prefix of every object's store region.
 __global__ void gather_store(const int *store, const long long *store_begin, const long long *dst_begin,
-                             const int *nstore, int nobj, const float *dbf, int *out, float *radii) {
+                             const int *nstore, int nobj, int *out) {
   const int o = blockIdx.x;
   if (o >= nobj) return;
   const int n = nstore[o];
   const int *src = store + store_begin[o];
   const long long dst = dst_begin[o];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const int v = src[i];
-    out[dst + i] = v;
-    radii[dst + i] = dbf[v];
-  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) out[dst + i] = src[i];
 }
 
 __global__ void gather_records(const int *rs, const int *rl, const long long *rec_begin, const long long *dst_begin,
@@ -107,45 +104,6 @@ struct VolumeState {
   std::vector<int> object_of;  // id -> global object index, -1 when inactive
   bool empty = true;
 };
-
-// consolidate (skeleton.cpp:13-40 of the reference): unique vertices sorted by (x, y, z), edges
-// (min, max) sorted and unique, unused vertices dropped.
-struct Assembly {
-  std::vector<std::array<int, 3>> vox;
-  std::vector<float> radii;
-  std::vector<std::array<uint32_t, 2>> edges;
-};
-
-void consolidate(std::vector<std::array<int, 3>> &vertices, std::vector<float> &radii,
-                 std::vector<std::array<uint32_t, 2>> &edges, Assembly &out) {
-  out = Assembly{};
-  if (vertices.empty() || edges.empty()) return;
-  std::vector<uint32_t> order(vertices.size()), inverse(vertices.size());
-  std::iota(order.begin(), order.end(), 0u);
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return vertices[a] < vertices[b]; });
-  std::vector<std::array<int, 3>> uniq;
-  std::vector<float> urad;
-  for (uint32_t old : order) {
-    if (uniq.empty() || uniq.back() != vertices[old]) { uniq.push_back(vertices[old]); urad.push_back(radii[old]); }
-    inverse[old] = uint32_t(uniq.size() - 1);
-  }
-  std::vector<std::array<uint32_t, 2>> e2;
-  e2.reserve(edges.size());
-  for (auto e : edges) {
-    std::array<uint32_t, 2> f{inverse[e[0]], inverse[e[1]]};
-    if (f[0] > f[1]) std::swap(f[0], f[1]);
-    if (f[0] != f[1]) e2.push_back(f);
-  }
-  std::sort(e2.begin(), e2.end());
-  e2.erase(std::unique(e2.begin(), e2.end()), e2.end());
-  std::vector<uint8_t> used(uniq.size(), 0);
-  for (auto e : e2) used[e[0]] = used[e[1]] = 1;
-  std::vector<uint32_t> remap(uniq.size(), 0);
-  for (size_t i = 0; i < uniq.size(); ++i)
-    if (used[i]) { remap[i] = uint32_t(out.vox.size()); out.vox.push_back(uniq[i]); out.radii.push_back(urad[i]); }
-  for (auto &e : e2) e = {remap[e[0]], remap[e[1]]};
-  out.edges = std::move(e2);
-}
 
 }  // namespace
 
@@ -415,16 +373,15 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   long long vt = 0, rt = 0;
   for (int o = 0; o < nobj; ++o) { vdst[o] = vt; vt += ns[o]; rdst[o] = rt; rt += np[o]; }
   Buffer<int> cstore(ctx, std::max(vt, 1LL)), cstart(ctx, std::max(rt, 1LL)), clen(ctx, std::max(rt, 1LL));
-  Buffer<float> cradii(ctx, std::max(vt, 1LL));
   auto d_vdst = to_device(ctx, vdst), d_rdst = to_device(ctx, rdst);
-  gather_store<<<nobj, 256, 0, s>>>(store.data(), d_store_begin.data(), d_vdst.data(), nstore.data(), nobj, dbf.data(),
-                                    cstore.data(), cradii.data()); ++ctx.launches;
+  gather_store<<<nobj, 256, 0, s>>>(store.data(), d_store_begin.data(), d_vdst.data(), nstore.data(), nobj, cstore.data());
+  ++ctx.launches;
   gather_records<<<nobj, 256, 0, s>>>(rec_start.data(), rec_len.data(), d_rec_begin.data(), d_rdst.data(), npaths.data(),
                                       nobj, cstart.data(), clen.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
-  const auto hstore = cstore.download(vt), hstart = cstart.download(rt), hlen = clen.download(rt);
-  const auto hrad = cradii.download(vt);
+  const auto hstart = cstart.download(rt), hlen = clen.download(rt);
   if (dump && *dump) {
+    const auto hstore = cstore.download(vt);
     // diagnostics: the intermediate results a parity investigation compares with the oracle
     FILE *f = std::fopen(dump, "w");
     if (f) {
@@ -455,12 +412,16 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       std::fclose(f);
     }
   }
-  // per volume: skeletons per original label, components merged in id order
+  // skeletons: per volume, one per original label (first seen in id order) whose objects made a
+  // path of two or more vertices; the label's objects contribute in id order
+  AssemblyPaths ap;
+  std::vector<std::vector<int64_t>> group_labels(vs.size());
+  std::vector<int> group_begin(vs.size() + 1, 0);
   for (size_t v = 0; v < vs.size(); ++v) {
     auto &st = vs[v];
+    group_begin[v] = ap.groups;
     if (st.empty) continue;
-    Packed &out = results[v];
-    std::vector<int64_t> label_order;
+    std::vector<int64_t> &label_order = group_labels[v];
     std::vector<std::vector<int>> label_objects;
     for (int64_t id = 1; id <= st.cc.count; ++id) {
       const int o = st.object_of[id];
@@ -473,35 +434,44 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       if (it == label_order.end()) { label_order.push_back(label); label_objects.push_back({o}); }
       else label_objects[it - label_order.begin()].push_back(o);
     }
-    for (size_t j = 0; j < label_order.size(); ++j) {
-      std::vector<std::array<int, 3>> verts;
-      std::vector<float> rad;
-      std::vector<std::array<uint32_t, 2>> edges;
+    for (size_t j = 0; j < label_order.size(); ++j, ++ap.groups)
       for (int o : label_objects[j])
         for (int p = 0; p < np[o]; ++p) {
           const int len = hlen[rdst[o] + p];
           if (len < 2) continue;
-          const long long base = vdst[o] + hstart[rdst[o] + p];
-          const uint32_t first = uint32_t(verts.size());
-          for (int q = 0; q < len; ++q) {
-            long long g = hstore[base + q] - st.offset;
-            const int z = int(g / ((long long)st.d.sx * st.d.sy));
-            g -= (long long)z * st.d.sx * st.d.sy;
-            const int y = int(g / st.d.sx), x = int(g - (long long)y * st.d.sx);
-            verts.push_back({x, y, z});
-            rad.push_back(hrad[base + q]);
-            if (q) edges.push_back({first + q - 1, first + q});
-          }
+          ap.src.push_back(int(vdst[o] + hstart[rdst[o] + p]));
+          ap.len.push_back(len);
+          ap.group.push_back(ap.groups);
+          ap.volume.push_back(int(v));
         }
-      Assembly asmb;
-      consolidate(verts, rad, edges, asmb);
-      if (asmb.edges.empty()) continue;
-      out.labels.push_back(label_order[j]);
-      for (size_t i = 0; i < asmb.vox.size(); ++i) {
-        for (int c = 0; c < 3; ++c) out.vertices.push_back(float(asmb.vox[i][c]) * opt.anisotropy[c]);
-        out.radii.push_back(asmb.radii[i]);
-      }
-      for (auto e : asmb.edges) { out.edges.push_back(e[0]); out.edges.push_back(e[1]); }
+  }
+  group_begin[vs.size()] = ap.groups;
+  std::vector<long long> arena_off(vs.size());
+  std::vector<std::array<int, 3>> arena_dim(vs.size());
+  for (size_t v = 0; v < vs.size(); ++v) {
+    arena_off[v] = vs[v].offset;
+    arena_dim[v] = {vs[v].d.sx, vs[v].d.sy, vs[v].d.sz};
+  }
+  AssemblyResult asmb = assemble(ctx, cstore.data(), dbf.data(), ap, arena_off, arena_dim, aniso);
+  const long long V = asmb.vertex_offsets.back(), E = asmb.edge_offsets.back();
+  std::vector<float> hvert(3 * V), hrad(V);
+  std::vector<uint32_t> hedge(2 * E);
+  if (V) {
+    BK_CUDA(cudaMemcpyAsync(hvert.data(), asmb.vertices.data(), hvert.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+    BK_CUDA(cudaMemcpyAsync(hrad.data(), asmb.radii.data(), hrad.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+  }
+  if (E) BK_CUDA(cudaMemcpyAsync(hedge.data(), asmb.edges.data(), hedge.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  ctx.synchronize();
+  for (size_t v = 0; v < vs.size(); ++v) {
+    Packed &out = results[v];
+    for (int g = group_begin[v]; g < group_begin[v + 1]; ++g) {
+      const int64_t v0 = asmb.vertex_offsets[g], v1 = asmb.vertex_offsets[g + 1];
+      const int64_t e0 = asmb.edge_offsets[g], e1 = asmb.edge_offsets[g + 1];
+      if (e1 == e0) continue;
+      out.labels.push_back(group_labels[v][g - group_begin[v]]);
+      out.vertices.insert(out.vertices.end(), hvert.begin() + 3 * v0, hvert.begin() + 3 * v1);
+      out.radii.insert(out.radii.end(), hrad.begin() + v0, hrad.begin() + v1);
+      out.edges.insert(out.edges.end(), hedge.begin() + 2 * e0, hedge.begin() + 2 * e1);
       out.vertex_offsets.push_back(int64_t(out.radii.size()));
       out.edge_offsets.push_back(int64_t(out.edges.size() / 2));
     }
