@@ -33,6 +33,11 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     "dense512": dict(workload="dense segmentation 512x512x512 uint64, 600 Voronoi seeds cut by tubes r=3-10 (seed 1)",
                      shape=(512, 512, 512), seeds=600, seed=1, kind="dense", dtype="uint64", anisotropy=(8, 8, 40)),
+    "batch64": dict(workload="64 uneven uint32 volumes (edges log-uniform 64-256), 10-80 tubes r=1-8, ~5% arbors (seed 2)",
+                    seed=2, kind="batch", dtype="uint32", anisotropy=(4, 4, 4)),
+    "serve": dict(workload="Poisson request stream at 50/200/800 req/s (seed 4), volume edges log-uniform 32-384, "
+                       "1 tube per 64^3 voxels, uint32/uint64 50/50, 80 GB admission cap",
+                  seed=4, kind="serve", rates=(50, 200, 800), requests=300, anisotropy=(16, 16, 40)),
     "tubes128": dict(workload="128x128x128 uint32, 20 random-walk tubes r=2-6 (seed 0)", shape=(128, 128, 128),
                      objects=20, seed=0, kind="tubes", dtype="uint32", anisotropy=(16, 16, 40)),
 }
@@ -43,6 +48,9 @@ METRIC = "voxels/s & skeletons/s, batched/graph vs per-volume on 1 B200; p50/p99
 
 def make_volume(cfg, rank=0):
     from brook_b200 import synthetic
+
+    if cfg["kind"] == "batch":
+        return synthetic.uneven_batch(seed=cfg["seed"] + rank)
 
     if cfg["kind"] == "dense":
         return synthetic.dense_volume(cfg["shape"], seeds=cfg["seeds"], seed=cfg["seed"] + rank, dtype=np.dtype(cfg["dtype"]))
@@ -153,6 +161,150 @@ def run_reference(args, cfg):
                             "sample": f"{crop[0]}x{crop[1]}x{crop[2]} crop ({sample.size} voxels) of the workload volume"},
            "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
+
+
+def run_batch(args, cfg):
+    """The uneven batch: one skeletonize_batch call per step (all 64 volumes in one launch of each
+    engine kernel) against the same volumes through 64 plain skeletonize calls."""
+    import torch
+
+    import brook_b200
+    from brook_b200 import _native
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    volumes = make_volume(cfg, rank)
+    devs = [torch.from_numpy(np.ascontiguousarray(v.transpose(2, 1, 0))).cuda(local).permute(2, 1, 0) for v in volumes]
+    opts = dict(teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST, device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        out, stage = None, {}
+        for _ in range(steps):
+            out = fn()
+            for k, v in _native.stats(local).items():
+                stage[k] = stage.get(k, 0.0) + v
+        end.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(end) / steps
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        barrier()
+        return ms, out, {k: v / steps for k, v in stage.items()}
+
+    batched = lambda: brook_b200.skeletonize_batch(devs, output="packed", **opts)  # noqa: E731
+    plain = lambda: [brook_b200.skeletonize(d, output="packed", **opts) for d in devs]  # noqa: E731
+    for _ in range(args.warmup):
+        batched()
+    with ClockSampler(local) as clocks:
+        ms, out, stage = timed(batched, args.steps)
+    plain()
+    plain_ms, plain_out, _ = timed(plain, max(1, args.steps // 2))
+    # identical skeletons both ways
+    for i, p in enumerate(plain_out):
+        q = out[i]
+        assert list(p.labels) == list(q.labels)
+        np.testing.assert_array_equal(p.vertices, q.vertices)
+        np.testing.assert_array_equal(p.edges, q.edges)
+    # end to end from pinned host memory
+    pinned = []
+    for v in volumes:
+        t = torch.empty(v.shape[::-1], dtype=torch.int32, pin_memory=True)
+        t.numpy().view(np.uint32)[...] = v.transpose(2, 1, 0)
+        pinned.append(t.numpy().view(np.uint32).transpose(2, 1, 0))
+    e2e_ms, out_h, _ = timed(lambda: brook_b200.skeletonize_batch(pinned, output="packed", **opts), args.steps)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    skeletons = len(out.labels) * world
+    voxels = sum(int(v.size) for v in volumes) * world
+    stage_ms = {k[3:]: v for k, v in stage.items() if k.startswith("ms_") and k != "ms_total"}
+    out_line = {
+        "metric": METRIC, "value": skeletons / (ms / 1e3), "unit": "skeletons/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32/f32", "data": "synthetic", "voxels_per_s": voxels / (ms / 1e3),
+        "per_volume": {"skeletons_per_s": skeletons / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                       "speedup_batched": plain_ms / ms, "identical": True},
+        "config": {"workload": cfg["workload"], "volumes": len(volumes), "voxels_per_gpu": voxels // world,
+                   "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (0.75 GB of labels per step)"},
+        "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
+        "e2e": {"value": skeletons / (e2e_ms / 1e3), "unit": "skeletons/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(sum(v.nbytes for v in volumes)),
+                "d2h_bytes_per_step": int(out_h.packed.vertices.nbytes + out_h.packed.edges.nbytes +
+                                          out_h.packed.radii.nbytes)},
+        "gpu_launches": int(stage.get("launches", 0) * args.steps),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(out_line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_serve(args, cfg):
+    """The request loop: each rate's stream replayed in real time through the continuous-batching
+    server and through the plain per-request path (one worker, one request per call)."""
+    import torch
+
+    from brook_b200 import serving, synthetic
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:  # requests are served by one GPU; other ranks have nothing to do
+        return
+    base = synthetic.serving_requests(cfg["requests"], 1.0, seed=cfg["seed"])  # arrivals at rate 1, rescaled below
+    opts = dict(teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST, device=local,
+                memory_cap=80e9)
+    warm = [(0.0, v) for _, v in base[:8]]
+    serving.replay(warm, lambda: serving.Server(workers=2, **opts))
+    rates, total = {}, None
+    with ClockSampler(local) as clocks:
+        for rate in cfg["rates"]:
+            stream = [(t / rate, v) for t, v in base]
+            row = {}
+            for name, factory in (("batched", lambda: serving.Server(workers=2, **opts)),
+                                  ("per_request", lambda: serving.Server(workers=1, max_batch=1, **opts))):
+                t0 = time.perf_counter()
+                done = serving.replay(stream, factory)
+                wall = time.perf_counter() - t0
+                skel = sum(len(r.future.result()) for r in done)
+                lat = serving.percentiles([r.latency * 1e3 for r in done])
+                row[name] = {"p50_ms": lat["p50"], "p99_ms": lat["p99"], "skeletons_per_s": skel / wall,
+                             "requests_per_s": len(done) / wall, "wall_s": wall}
+                total = skel
+            rates[str(rate)] = row
+    head = rates[str(cfg["rates"][1])]["batched"]
+    voxels = int(sum(v.size for _, v in base))
+    print(json.dumps({
+        "metric": METRIC, "value": head["skeletons_per_s"], "unit": "skeletons/s", "n_gpus": 1,
+        "steps": len(cfg["rates"]), "warmup": 1, "ms_per_step": head["wall_s"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32", "data": "synthetic",
+        "latency_ms": rates, "skeletons_per_stream": total,
+        "config": {"workload": cfg["workload"], "requests_per_rate": cfg["requests"], "voxels_per_stream": voxels,
+                   "value_rate": cfg["rates"][1], "anisotropy": cfg["anisotropy"], "teasar": PARAMS,
+                   "dust_threshold": DUST, "workers": 2, "timing": "wall clock per request, arrival to result"},
+        "e2e": {"value": head["skeletons_per_s"], "unit": "skeletons/s",
+                "h2d_bytes_per_step": int(sum(v.nbytes for _, v in base)), "d2h_bytes_per_step": None},
+        "clocks": clocks.summary(),
+    }))
 
 
 def run_ours(args, cfg):
@@ -269,6 +421,10 @@ def main():
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, cfg)
+    elif cfg["kind"] == "batch":
+        run_batch(args, cfg)
+    elif cfg["kind"] == "serve":
+        run_serve(args, cfg)
     else:
         run_ours(args, cfg)
 

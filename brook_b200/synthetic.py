@@ -48,8 +48,9 @@ def _ball(radius):
     return _BALLS[key]
 
 
-def _walk(rng, shape, start, steps, branch_p, sigma=0.2):
-    """Centres of a random walk of unit steps (and of its branches) inside `shape`."""
+def _walk(rng, shape, start, steps, branch_p, sigma=0.2, limit=None):
+    """Centres of a random walk of unit steps (and of its branches) inside `shape`; with `limit`,
+    at most that many centres over the walk and all its branches."""
     out = []
     stack = [(tuple(float(c) for c in start), tuple(rng.normal(size=3)), int(steps))]
     hi = [float(s - 1) for s in shape]
@@ -73,6 +74,8 @@ def _walk(rng, shape, start, steps, branch_p, sigma=0.2):
             if pz < 0 or pz > hi[2]:
                 hz, pz = -hz, min(max(pz, 0.0), hi[2])
             out.append((px, py, pz))
+            if limit is not None and len(out) >= limit:
+                return np.asarray(out, np.float64).reshape(-1, 3)
             left = remaining - step - 1
             if coins is not None and coins[step] < branch_p and left > 10:
                 stack.append(((px, py, pz), tuple(rng.normal(size=3)), int(left * rng.uniform(0.3, 0.8))))
@@ -121,7 +124,8 @@ def tube_volume(shape=(128, 128, 128), objects=20, seed=0, steps=(200, 600), rad
         arbor = arbor_fraction > 0 and rng.random() < arbor_fraction
         n = int(rng.integers(arbor_steps[0], arbor_steps[1] + 1)) if arbor else int(rng.integers(steps[0], steps[1] + 1))
         start = rng.uniform(0, np.asarray(shape) - 1)
-        centres = _walk(rng, shape, start, n, 0.02 if arbor else branch_p)
+        # an arbor: a trunk of a third of its steps whose branches take the rest
+        centres = _walk(rng, shape, start, n // 3, 0.02, limit=n) if arbor else _walk(rng, shape, start, n, branch_p)
         _paint(vol, centres, rng.uniform(*radius), label)
     return vol.numpy(dtype)
 
