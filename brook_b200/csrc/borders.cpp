@@ -99,27 +99,68 @@ std::array<float, 4> tie_keys(int64_t ix, int64_t iy, float cx, float cy, int64_
 
 }  // namespace
 
-std::vector<std::vector<Point>> border_targets(Context &ctx, const uint32_t *ids, VolumeDims d, int64_t count,
-                                               const float aniso[3]) {
-  std::vector<TupleSet> sets(count + 1);
-  const int shape[3] = {d.sx, d.sy, d.sz};
+std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const uint32_t *ids,
+                                                            const std::vector<BorderVolume> &volumes,
+                                                            const float aniso[3]) {
+  // faces grouped by axis pair t: (a, b) = (x, y), (x, z), (y, z); within a group volume-major,
+  // the low face (c = 0) before the high one
   const int axes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
-  for (int face = 0; face < 6; ++face) {
-    const int a = axes[face / 2][0], b = axes[face / 2][1], c = axes[face / 2][2];
-    const int fixed = face % 2 ? shape[c] - 1 : 0;
-    const int64_t fx = shape[a], fy = shape[b];
-    const VolumeDims pd{int(fy), int(fx), 1};
-    Buffer<uint32_t> plane(ctx, fx * fy);
-    extract_face(ctx, ids, d, a, b, c, fixed, plane.data());
-    Buffer<uint32_t> plane_ids(ctx, fx * fy);
-    ComponentsResult pc = connected_components(ctx, plane.data(), U32, pd, plane_ids.data());
-    if (pc.count == 0) continue;
-    const float plane_aniso[3] = {aniso[b], aniso[a], 1.0f};
-    Buffer<float> dist(ctx, fx * fy);
-    edt(ctx, plane_ids.data(), pd, plane_aniso, true, 2, dist.data());
-    const std::vector<uint32_t> lab = plane_ids.download();
-    const std::vector<float> dd = dist.download();
-    const size_t k = size_t(pc.count) + 1;
+  std::vector<Face> faces;
+  int W = 1, H = 1;
+  long long packed = 0;
+  for (int t = 0; t < 3; ++t)
+    for (const auto &v : volumes)
+      for (int side = 0; side < 2; ++side) {
+        const int a = axes[t][0], b = axes[t][1], c = axes[t][2];
+        const int shape[3] = {v.d.sx, v.d.sy, v.d.sz};
+        Face f{v.offset, v.d, a, b, c, side ? shape[c] - 1 : 0, packed};
+        packed += (long long)f.fx() * f.fy();
+        W = std::max(W, f.fy());
+        H = std::max(H, f.fx());
+        faces.push_back(f);
+      }
+  std::vector<std::vector<std::vector<Point>>> out(volumes.size());
+  for (size_t v = 0; v < volumes.size(); ++v) out[v].resize(size_t(volumes[v].count) + 1);
+  if (volumes.empty()) return out;
+  if (faces.size() > 65535) throw std::invalid_argument("too many volumes for one border pass");
+  const long long slice = (long long)W * H, S = (long long)faces.size();
+  if (slice * S >= (1LL << 31) - 1) throw std::invalid_argument("border faces exceed 2^31 pixels");
+  Buffer<uint32_t> stack(ctx, slice * S), stack_ids(ctx, slice * S);
+  extract_faces(ctx, ids, faces, W, H, stack.data());
+  const VolumeDims sd{W, H, int(S)};
+  ComponentsResult pc = connected_components(ctx, stack.data(), U32, sd, stack_ids.data(), true);
+  if (pc.count == 0) return out;
+  // 2D EDT (black border) of each group with its own spacing: the slice's x axis is b, y is a
+  Buffer<float> dist(ctx, slice * S);
+  const long long per_group = 2LL * (long long)volumes.size();
+  for (int t = 0; t < 3; ++t) {
+    const float plane_aniso[3] = {aniso[axes[t][1]], aniso[axes[t][0]], 1.0f};
+    const long long first = per_group * t;
+    edt(ctx, stack_ids.data() + slice * first, VolumeDims{W, H, int(per_group)}, plane_aniso, true, 2,
+        dist.data() + slice * first);
+  }
+  Buffer<uint32_t> pids(ctx, std::max(packed, 1LL));
+  Buffer<float> pdist(ctx, std::max(packed, 1LL));
+  pack_faces(ctx, stack_ids.data(), dist.data(), faces, W, H, pids.data(), pdist.data());
+  const std::vector<uint32_t> labs = pids.download(packed);
+  const std::vector<float> dds = pdist.download(packed);
+  // per volume and component id, the picks in the reference's face order (each volume's faces
+  // come in that order in the stack)
+  std::vector<std::vector<TupleSet>> sets(volumes.size());
+  for (size_t v = 0; v < volumes.size(); ++v) sets[v].resize(size_t(volumes[v].count) + 1);
+  for (size_t fi = 0; fi < faces.size(); ++fi) {
+    const Face &f = faces[fi];
+    const size_t v = size_t(fi % per_group) / 2;
+    const int a = f.a, b = f.b, c = f.c;
+    const int64_t fx = f.fx(), fy = f.fy();
+    const uint32_t *lab = labs.data() + f.packed;
+    const float *dd = dds.data() + f.packed;
+    // the face's component ids form one contiguous range (ids follow the stack's flat order)
+    uint32_t lo = UINT32_MAX, hi = 0;
+    for (int64_t i = 0; i < fx * fy; ++i)
+      if (lab[i]) { lo = std::min(lo, lab[i]); hi = std::max(hi, lab[i]); }
+    if (hi == 0) continue;
+    const size_t k = size_t(hi - lo) + 1;
     std::vector<float> maxdist(k, 0.0f), sumx(k, 0.0f), sumy(k, 0.0f);
     std::vector<uint32_t> sizes(k, 0);
     std::vector<int64_t> first(k, std::numeric_limits<int64_t>::max()), pick(k, -1);
@@ -127,8 +168,8 @@ std::vector<std::vector<Point>> border_targets(Context &ctx, const uint32_t *ids
     for (int64_t x = 0; x < fx; ++x)
       for (int64_t y = 0; y < fy; ++y) {
         const size_t i = size_t(y + fy * x);
-        const uint32_t l = lab[i];
-        if (!l) continue;
+        if (!lab[i]) continue;
+        const size_t l = lab[i] - lo;
         sumx[l] += float(x);
         sumy[l] += float(y);
         ++sizes[l];
@@ -136,7 +177,7 @@ std::vector<std::vector<Point>> border_targets(Context &ctx, const uint32_t *ids
       }
     const float wx = aniso[a], wy = aniso[b];
     std::vector<float> cx(k, 0.0f), cy(k, 0.0f);
-    for (size_t l = 1; l < k; ++l)
+    for (size_t l = 0; l < k; ++l)
       if (sizes[l]) {
         float px = (wx * sumx[l]) / float(sizes[l]), py = (wy * sumy[l]) / float(sizes[l]);
         if (px - (wx * float(fx)) / 2.0f < 0) px = px + wx;
@@ -148,26 +189,26 @@ std::vector<std::vector<Point>> border_targets(Context &ctx, const uint32_t *ids
     for (int64_t y = 0; y < fy; ++y)
       for (int64_t x = 0; x < fx; ++x) {
         const size_t i = size_t(y + fy * x);
-        const uint32_t l = lab[i];
-        if (!l || dd[i] == 0 || dd[i] != maxdist[l]) continue;
+        if (!lab[i]) continue;
+        const size_t l = lab[i] - lo;
+        if (dd[i] == 0 || dd[i] != maxdist[l]) continue;
         const auto key = tie_keys(x, y, cx[l], cy[l], fx, fy, wx, wy);
         if (pick[l] < 0 || key < best[l]) { best[l] = key; pick[l] = x + fx * y; }
       }
     std::vector<size_t> order;
-    for (size_t l = 1; l < k; ++l)
+    for (size_t l = 0; l < k; ++l)
       if (pick[l] >= 0) order.push_back(l);
-    std::sort(order.begin(), order.end(), [&](size_t u, size_t v) { return first[u] < first[v]; });
+    std::sort(order.begin(), order.end(), [&](size_t u, size_t w) { return first[u] < first[w]; });
     for (size_t l : order) {
       Point p{};
       p[a] = pick[l] % fx;
       p[b] = pick[l] / fx;
-      p[c] = fixed;
-      sets.at(size_t(pc.mapping[l])).add(p);
+      p[c] = f.fixed;
+      sets[v].at(size_t(pc.mapping[lo + l])).add(p);
     }
   }
-  std::vector<std::vector<Point>> out;
-  out.reserve(sets.size());
-  for (const auto &s : sets) out.push_back(s.values());
+  for (size_t v = 0; v < volumes.size(); ++v)
+    for (size_t id = 0; id < sets[v].size(); ++id) out[v][id] = sets[v][id].values();
   return out;
 }
 

@@ -59,9 +59,10 @@ __global__ void init_parent(int *parent, long long n) {
 // and dx > 0). A face pair of equal labels is always united. An edge pair is skipped when one of
 // its two face-adjacent intermediates has the label (the pair is then joined through it), a corner
 // pair when one of its three face or three edge intermediates has it: by induction over face ->
-// edge -> corner every skipped pair still ends in one component.
+// edge -> corner every skipped pair still ends in one component. `planar`: neighbours in the same
+// z-slice only (a stack of independent 2D images).
 template <class L>
-__global__ void union_forward(const L *labels, int *parent, Dims d) {
+__global__ void union_forward(const L *labels, int *parent, Dims d, bool planar) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n()) return;
   const L lv = labels[i];
@@ -77,6 +78,7 @@ __global__ void union_forward(const L *labels, int *parent, Dims d) {
   for (int k = 0; k < 26; ++k) {
     const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
     if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
+    if (planar && dz != 0) continue;
     if (!same(dx, dy, dz)) continue;
     const int nonzero = (dx != 0) + (dy != 0) + (dz != 0);
     if (nonzero == 2) {
@@ -130,14 +132,14 @@ __global__ void relabel(const L *labels, const int *parent, const int *rank, uin
 }
 
 template <class L>
-ComponentsResult run(Context &ctx, const L *labels, VolumeDims vd, uint32_t *ids) {
+ComponentsResult run(Context &ctx, const L *labels, VolumeDims vd, uint32_t *ids, bool planar) {
   const long long n = vd.n();
   const Dims d{vd.sx, vd.sy, vd.sz};
   ComponentsResult out;
   Buffer<int> parent(ctx, n), rank(ctx, n + 1);
   cudaStream_t s = ctx.stream();
   init_parent<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
-  union_forward<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), d); ++ctx.launches;
+  union_forward<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), d, planar); ++ctx.launches;
   flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   thrust::counting_iterator<long long> index(0);
@@ -163,18 +165,19 @@ ComponentsResult run(Context &ctx, const L *labels, VolumeDims vd, uint32_t *ids
 
 }  // namespace
 
-ComponentsResult connected_components(Context &ctx, const void *labels, int dtype, VolumeDims d, uint32_t *ids) {
+ComponentsResult connected_components(Context &ctx, const void *labels, int dtype, VolumeDims d, uint32_t *ids,
+                                      bool planar) {
   if (d.n() <= 0) { ComponentsResult r; r.mapping.assign(1, 0); return r; }
   if (d.n() >= (1LL << 31) - 1) throw std::invalid_argument("volumes of 2^31 voxels or more are not supported");
   switch (dtype) {
-    case U8: return run(ctx, static_cast<const uint8_t *>(labels), d, ids);
-    case U16: return run(ctx, static_cast<const uint16_t *>(labels), d, ids);
-    case U32: return run(ctx, static_cast<const uint32_t *>(labels), d, ids);
-    case U64: return run(ctx, static_cast<const uint64_t *>(labels), d, ids);
-    case I8: return run(ctx, static_cast<const int8_t *>(labels), d, ids);
-    case I16: return run(ctx, static_cast<const int16_t *>(labels), d, ids);
-    case I32: return run(ctx, static_cast<const int32_t *>(labels), d, ids);
-    case I64: return run(ctx, static_cast<const int64_t *>(labels), d, ids);
+    case U8: return run(ctx, static_cast<const uint8_t *>(labels), d, ids, planar);
+    case U16: return run(ctx, static_cast<const uint16_t *>(labels), d, ids, planar);
+    case U32: return run(ctx, static_cast<const uint32_t *>(labels), d, ids, planar);
+    case U64: return run(ctx, static_cast<const uint64_t *>(labels), d, ids, planar);
+    case I8: return run(ctx, static_cast<const int8_t *>(labels), d, ids, planar);
+    case I16: return run(ctx, static_cast<const int16_t *>(labels), d, ids, planar);
+    case I32: return run(ctx, static_cast<const int32_t *>(labels), d, ids, planar);
+    case I64: return run(ctx, static_cast<const int64_t *>(labels), d, ids, planar);
     default: throw std::invalid_argument("connected components require integer labels");
   }
 }

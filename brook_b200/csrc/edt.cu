@@ -172,7 +172,6 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
   for (int a = 0; a < 3; ++a)
     if (!(aniso[a] > 0) || !std::isfinite(aniso[a])) throw std::invalid_argument("anisotropy must be finite and positive");
   if (dims < 2 && (vd.sy != 1 || vd.sz != 1)) throw std::invalid_argument("1D EDT of a volume");
-  if (dims < 3 && vd.sz != 1) throw std::invalid_argument("2D EDT of a volume");
   cudaStream_t s = ctx.stream();
   // x pass
   std::vector<float> acc(vd.sx + 2, 0.0f);

@@ -26,12 +26,14 @@ struct ComponentsResult {
   std::vector<int64_t> roots;    // id - 1 -> first flat index of the component
 };
 // 26-connected components of equal nonzero labels, ids by ascending first flat index, written to
-// ids (per voxel: id 1..K, 0 = background).
-ComponentsResult connected_components(Context &ctx, const void *labels, int dtype, VolumeDims d, uint32_t *ids);
+// ids (per voxel: id 1..K, 0 = background). `planar`: 8-connected within each z-slice only.
+ComponentsResult connected_components(Context &ctx, const void *labels, int dtype, VolumeDims d, uint32_t *ids,
+                                      bool planar = false);
 
 // ---- EDT (edt.cu) ----
 // Squared-then-rooted anisotropic distance of every voxel to the nearest voxel of a different id
-// (the volume edge counts with black_border); background gets 0. dims = 2 skips the z pass.
+// (the volume edge counts with black_border); background gets 0. dims = 2 skips the z pass: every
+// z-slice is then an image of its own.
 void edt(Context &ctx, const uint32_t *ids, VolumeDims d, const float aniso[3], bool black_border, int dims,
          float *out);
 
@@ -51,12 +53,34 @@ void neighbour_mask(Context &ctx, const uint32_t *ids, VolumeDims d, uint32_t *o
 // Per id the largest value of `field` (non-negative, finite), as float bits.
 std::vector<float> segment_max(Context &ctx, const float *field, const uint32_t *ids, long long n, int64_t count);
 void fill_float(Context &ctx, float *p, long long n, float value);
-// Extract one face of `ids` as a (fy, fx, 1) plane: plane[pb + fy * pa] = ids[p[a]=pa, p[b]=pb, p[c]=fixed].
-void extract_face(Context &ctx, const uint32_t *ids, VolumeDims d, int a, int b, int c, int fixed, uint32_t *plane);
+// One face of a volume whose ids start at ids + offset: the pixels with p[c] = fixed, pixel (pa, pb)
+// = (p[a], p[b]), fx = extent of a, fy = extent of b.
+struct Face {
+  long long offset;
+  VolumeDims d;
+  int a, b, c, fixed;
+  long long packed;  // where the face starts in a packed buffer (pixel pb + fy * pa)
+  int fx() const { return a == 0 ? d.sx : a == 1 ? d.sy : d.sz; }
+  int fy() const { return b == 0 ? d.sx : b == 1 ? d.sy : d.sz; }
+};
+// Every face into its own z-slice of a (W, H, faces) stack: stack[pb + W * (pa + H * f)], zero
+// beyond the face's (fy, fx) corner.
+void extract_faces(Context &ctx, const uint32_t *ids, const std::vector<Face> &faces, int W, int H, uint32_t *stack);
+// The faces' pixels of two stack fields, packed face by face (pixel pb + fy * pa at face.packed).
+void pack_faces(Context &ctx, const uint32_t *stack_ids, const float *stack_dist, const std::vector<Face> &faces,
+                int W, int H, uint32_t *ids_out, float *dist_out);
 
 // ---- border targets (borders.cpp) ----
 using Point = std::array<int64_t, 3>;
-std::vector<std::vector<Point>> border_targets(Context &ctx, const uint32_t *ids, VolumeDims d, int64_t count,
-                                               const float aniso[3]);
+// Per volume, per component id: its border targets in the order the reference visits them. All
+// faces of all volumes run through one planar CCL and three planar EDTs.
+struct BorderVolume {
+  long long offset;  // where the volume's ids start
+  VolumeDims d;
+  int64_t count;     // component ids 1..count
+};
+std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const uint32_t *ids,
+                                                            const std::vector<BorderVolume> &volumes,
+                                                            const float aniso[3]);
 
 }  // namespace bk

@@ -169,10 +169,18 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     neighbour_mask(ctx, vid, st.d, mask.data() + st.offset);
     clock.mark("mask");
     st.borders.assign(K + 1, {});
-    if (opt.fix_borders) st.borders = border_targets(ctx, vid, st.d, K, aniso);
-    clock.mark("borders");
     st.dbf_max = segment_max(ctx, dbf.data() + st.offset, vid, n, K);
     clock.mark("dbf_max");
+  }
+  // ---- border targets of every volume in one pass
+  if (opt.fix_borders) {
+    std::vector<BorderVolume> bv;
+    std::vector<size_t> which;
+    for (size_t v = 0; v < vs.size(); ++v)
+      if (!vs[v].empty) { bv.push_back({vs[v].offset, vs[v].d, vs[v].cc.count}); which.push_back(v); }
+    auto picks = border_targets(ctx, ids.data(), bv, aniso);
+    for (size_t j = 0; j < which.size(); ++j) vs[which[j]].borders = std::move(picks[j]);
+    clock.mark("borders");
   }
   // ---- objects: more voxels than dust and a bounding box of two or more voxels (batched.cu:187-191)
   struct Object {

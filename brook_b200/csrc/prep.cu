@@ -1,5 +1,7 @@
 // Preamble kernels: per-component boxes and counts, the neighbour masks every later stage steps
 // through, per-component maxima, fills and face extraction.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.hpp"
 
@@ -66,16 +68,46 @@ __global__ void fill_kernel(float *p, long long n, float v) {
   if (i < n) p[i] = v;
 }
 
-__global__ void face_kernel(const uint32_t *__restrict__ ids, Dims d, int a, int b, int c, int fixed, uint32_t *plane) {
-  const int shape[3] = {d.sx, d.sy, d.sz};
-  const long long fx = shape[a], fy = shape[b];
+struct FaceDesc {
+  long long offset, packed;
+  int sx, sy, sz, a, b, c, fixed;
+};
+
+// grid (ceil(W * H / 256), faces): pixel (pb, pa) of slice f
+__global__ void faces_kernel(const uint32_t *__restrict__ ids, const FaceDesc *faces, int W, int H, uint32_t *stack) {
+  const FaceDesc f = faces[blockIdx.y];
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= fx * fy) return;
-  int p[3];
-  p[a] = (int)(i / fy);
-  p[b] = (int)(i % fy);
-  p[c] = fixed;
-  plane[i] = ids[p[0] + (long long)d.sx * (p[1] + (long long)d.sy * p[2])];
+  if (i >= (long long)W * H) return;
+  const int pb = int(i % W), pa = int(i / W);
+  const int shape[3] = {f.sx, f.sy, f.sz};
+  uint32_t v = 0;
+  if (pa < shape[f.a] && pb < shape[f.b]) {
+    int p[3];
+    p[f.a] = pa;
+    p[f.b] = pb;
+    p[f.c] = f.fixed;
+    v = ids[f.offset + p[0] + (long long)f.sx * (p[1] + (long long)f.sy * p[2])];
+  }
+  stack[i + (long long)W * H * blockIdx.y] = v;
+}
+
+__global__ void pack_kernel(const uint32_t *__restrict__ sids, const float *__restrict__ sdist, const FaceDesc *faces,
+                            int W, int H, uint32_t *ids, float *dist) {
+  const FaceDesc f = faces[blockIdx.y];
+  const int shape[3] = {f.sx, f.sy, f.sz};
+  const int fx = shape[f.a], fy = shape[f.b];
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)fx * fy) return;
+  const int pb = int(i % fy), pa = int(i / fy);
+  const long long src = pb + (long long)W * (pa + (long long)H * blockIdx.y);
+  ids[f.packed + i] = sids[src];
+  dist[f.packed + i] = sdist[src];
+}
+
+Buffer<FaceDesc> face_descs(Context &ctx, const std::vector<Face> &faces) {
+  std::vector<FaceDesc> h;
+  for (const auto &f : faces) h.push_back({f.offset, f.packed, f.d.sx, f.d.sy, f.d.sz, f.a, f.b, f.c, f.fixed});
+  return to_device(ctx, h);
 }
 
 }  // namespace
@@ -122,10 +154,22 @@ void fill_float(Context &ctx, float *p, long long n, float value) {
   BK_CUDA(cudaGetLastError());
 }
 
-void extract_face(Context &ctx, const uint32_t *ids, VolumeDims vd, int a, int b, int c, int fixed, uint32_t *plane) {
-  const int shape[3] = {vd.sx, vd.sy, vd.sz};
-  const long long n = (long long)shape[a] * shape[b];
-  face_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, a, b, c, fixed, plane); ++ctx.launches;
+void extract_faces(Context &ctx, const uint32_t *ids, const std::vector<Face> &faces, int W, int H, uint32_t *stack) {
+  if (faces.empty()) return;
+  Buffer<FaceDesc> desc = face_descs(ctx, faces);
+  faces_kernel<<<dim3(blocks_for((long long)W * H), unsigned(faces.size())), 256, 0, ctx.stream()>>>(
+      ids, desc.data(), W, H, stack); ++ctx.launches;
+  BK_CUDA(cudaGetLastError());
+}
+
+void pack_faces(Context &ctx, const uint32_t *stack_ids, const float *stack_dist, const std::vector<Face> &faces,
+                int W, int H, uint32_t *ids_out, float *dist_out) {
+  if (faces.empty()) return;
+  Buffer<FaceDesc> desc = face_descs(ctx, faces);
+  long long most = 0;
+  for (const auto &f : faces) most = std::max(most, (long long)f.fx() * f.fy());
+  pack_kernel<<<dim3(blocks_for(most), unsigned(faces.size())), 256, 0, ctx.stream()>>>(
+      stack_ids, stack_dist, desc.data(), W, H, ids_out, dist_out); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
 }
 
