@@ -246,6 +246,7 @@ def run_batch(args, cfg):
                    "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST,
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (0.75 GB of labels per step)"},
         "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
+        "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
         "e2e": {"value": skeletons / (e2e_ms / 1e3), "unit": "skeletons/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(sum(v.nbytes for v in volumes)),
                 "d2h_bytes_per_step": int(out_h.packed.vertices.nbytes + out_h.packed.edges.nbytes +
@@ -393,6 +394,7 @@ def run_ours(args, cfg):
                    "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST,
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (labels 1 GiB per step)"},
         "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
+        "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
         "work": {k: stage.get(k) for k in ("paths", "railroad_settled", "railroad_touched", "invalidated", "foreground")},
         "roofline": {"kernel": "trace_kernel", "stage_dominant": dominant, "bound": "hbm", "achieved": achieved,
                      "peak": peak, "peak_source": source, "unit": "GB/s", "frac": achieved / peak,

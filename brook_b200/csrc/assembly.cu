@@ -7,6 +7,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
+#include <string>
 #include <stdexcept>
 
 #include "assembly.hpp"
@@ -148,6 +150,12 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
                         const std::vector<long long> &arena_offset, const std::vector<std::array<int, 3>> &arena_dims,
                         const float anisotropy[3]) {
   cudaStream_t s = ctx.stream();
+  auto host_t = std::chrono::steady_clock::now();
+  auto host_mark = [&](const char *step) {  // host time of each step: ctx.stats["host_ms_assemble_<step>"]
+    const auto now = std::chrono::steady_clock::now();
+    ctx.stats[std::string("host_ms_assemble_") + step] += std::chrono::duration<double, std::milli>(now - host_t).count();
+    host_t = now;
+  };
   AssemblyResult out;
   const int G = paths.groups, npaths = int(paths.src.size());
   out.vertex_offsets.assign(G + 1, 0);
@@ -172,6 +180,7 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
   auto d_occ = to_device(ctx, occ_begin), d_aoff = to_device(ctx, arena_offset);
   auto d_dims = to_device(ctx, dims_flat);
 
+  host_mark("upload");
   // every occurrence: key, index, radius, first-of-path
   Buffer<unsigned long long> keys(ctx, P), sorted(ctx, P);
   Buffer<int> index(ctx, P), order(ctx, P);
@@ -189,6 +198,7 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
     BK_CUDA(cub::DeviceRadixSort::SortPairs(scratch.data(), temp, keys.data(), sorted.data(), index.data(),
                                             order.data(), (int)P, 0, end_bit, s));
   }
+  host_mark("sort");
   // unique vertices (stable sort: a run's head is the earliest occurrence)
   Buffer<int> head(ctx, P), rank(ctx, P), inverse(ctx, P);
   run_heads<<<blocks_for(P), 256, 0, s>>>(sorted.data(), head.data(), P); ++ctx.launches;
@@ -220,7 +230,9 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
     ctx.synchronize();
     return (long long)a + b;
   };
+  host_mark("queue");
   const long long V = tail(used, vrank), E = tail(head, erank);
+  host_mark("counts");
   // per-skeleton counts -> offsets
   Buffer<int> vcount(ctx, G), ecount(ctx, G);
   vcount.zero();
@@ -235,6 +247,7 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
   ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   const auto hv = vcount.download(), he = ecount.download();
+  host_mark("offsets");
   for (int g = 0; g < G; ++g) {
     out.vertex_offsets[g + 1] = out.vertex_offsets[g] + hv[g];
     out.edge_offsets[g + 1] = out.edge_offsets[g] + he[g];

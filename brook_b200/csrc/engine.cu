@@ -1,4 +1,4 @@
-// Object engine kernels (see engine.hpp). A "group" — one CTA, or a cluster of kClusterCtas CTAs
+// Object engine kernels (see engine.hpp). A "group" — one CTA, or a cluster of 4 or 8 CTAs
 // for a large object — runs one object's chain. Every frontier round has two steps separated by a
 // group barrier: step A stages each frontier voxel (flag cleared, distance read, neighbour mask),
 // step B spreads its (voxel, neighbour) items over every thread of the group, so that thousands of
@@ -8,6 +8,10 @@
 // with CTA-local atomics and combined across the group at barriers. State other threads update
 // with atomics (distances, keys, flags, liveness, rails, staged entries) is always read through L2.
 #include <cooperative_groups.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "common.cuh"
 #include "engine.hpp"
@@ -21,6 +25,8 @@ namespace cg = cooperative_groups;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr unsigned long long kMinFarNone = 0x7f8000007f800000ull;
 constexpr unsigned long long kClaimedMark = 0xFFFFFFFFFFFFFFFEull;
+// Resident engine CTAs per SM: 3 x 512 threads at up to 40 registers each.
+constexpr int kEngineCtasPerSm = 3;
 
 struct Shared {
   // the object (written by the group's first CTA, copied by the others)
@@ -292,8 +298,14 @@ __device__ void prepare_loop(const EngineArgs &a, bool big) {
   }
 }
 
-__global__ void __launch_bounds__(kEngineThreads) prepare_small(EngineArgs a) { prepare_loop<1>(a, false); }
-__global__ void __launch_bounds__(kEngineThreads) prepare_big(EngineArgs a) { prepare_loop<kClusterCtas>(a, true); }
+// Every CTA belongs to a cluster. The clusters first take the large objects, one each, then every
+// CTA takes small objects on its own: large objects start first (they set the kernel's length),
+// and no CTA idles while any object is left.
+template <int C>
+__global__ void __launch_bounds__(kEngineThreads, kEngineCtasPerSm) prepare_kernel(EngineArgs a) {
+  prepare_loop<C>(a, true);
+  prepare_loop<1>(a, false);
+}
 
 // ---------------------------------------------------------------------------------------------
 // Railroad flood from target t over the object's voxels: entering v costs pdrf[v] (vw_step), rails
@@ -763,23 +775,19 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
   if (threadIdx.x < 4 && s_work[threadIdx.x]) atomicAdd(a.work + threadIdx.x, s_work[threadIdx.x]);
 }
 
-__global__ void __launch_bounds__(kEngineThreads) trace_small(EngineArgs a) { trace_loop<1>(a, false); }
-__global__ void __launch_bounds__(kEngineThreads) trace_big(EngineArgs a) { trace_loop<kClusterCtas>(a, true); }
-
-int small_grid(const void *kernel, int sm_count, int count) {
-  int per_sm = 1;
-  BK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kEngineThreads, 0));
-  const int full = sm_count * (per_sm < 1 ? 1 : per_sm);
-  return count < full ? count : full;
+template <int C>
+__global__ void __launch_bounds__(kEngineThreads, kEngineCtasPerSm) trace_kernel(EngineArgs a) {
+  trace_loop<C>(a, true);
+  trace_loop<1>(a, false);
 }
 
-cudaLaunchConfig_t cluster_config(int clusters, cudaStream_t stream, cudaLaunchAttribute *attr) {
+cudaLaunchConfig_t cluster_config(int clusters, int ctas, cudaStream_t stream, cudaLaunchAttribute *attr) {
   cudaLaunchConfig_t config{};
-  config.gridDim = dim3(unsigned(clusters * kClusterCtas));
+  config.gridDim = dim3(unsigned(clusters * ctas));
   config.blockDim = dim3(kEngineThreads);
   config.stream = stream;
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kClusterCtas;
+  attr[0].val.clusterDim.x = unsigned(ctas);
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   config.attrs = attr;
@@ -787,36 +795,71 @@ cudaLaunchConfig_t cluster_config(int clusters, cudaStream_t stream, cudaLaunchA
   return config;
 }
 
-void launch_pair(const void *small, const void *big, const EngineArgs &a, int nbig, int sm_count, cudaStream_t s_small,
-                 cudaStream_t s_big) {
+// Resident clusters of `kernel` on the current device (queried once per device and kernel: the
+// query costs far more than a launch).
+int resident_clusters(const void *kernel, int ctas, cudaStream_t stream) {
+  static std::mutex lock;
+  static std::map<std::pair<int, const void *>, int> known;
+  int device = 0;
+  BK_CUDA(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> guard(lock);
+  auto it = known.find({device, kernel});
+  if (it != known.end()) return it->second;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t probe = cluster_config(1, ctas, stream, attr);
+  int cap = 1;
+  BK_CUDA(cudaOccupancyMaxActiveClusters(&cap, kernel, &probe));
+  known[{device, kernel}] = cap;
+  return cap;
+}
+
+// As many clusters as are resident at once (no more than the work needs).
+void launch(const void *kernel, int ctas, const EngineArgs &a, int nbig, cudaStream_t stream) {
   EngineArgs args = a;
   args.nbig = nbig;
   void *kargs[] = {&args};
-  if (nbig > 0) {
-    cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t probe = cluster_config(1, s_big, attr);
-    int cap = 1;
-    BK_CUDA(cudaOccupancyMaxActiveClusters(&cap, big, &probe));
-    cap = cap < 1 ? 1 : cap;
-    // large objects first, on as many clusters as fit; small objects take the slots left over
-    // and those the clusters free when the large-object queue runs dry
-    const int clusters = nbig < cap ? nbig : cap;
-    cudaLaunchConfig_t config = cluster_config(clusters, s_big, attr);
-    BK_CUDA(cudaLaunchKernelExC(&config, big, kargs));
-  }
-  if (a.nobj > nbig)
-    BK_CUDA(cudaLaunchKernel(small, dim3(unsigned(small_grid(small, sm_count, a.nobj - nbig))), dim3(kEngineThreads),
-                             kargs, 0, s_small));
+  cudaLaunchAttribute attr[1];
+  const int cap = resident_clusters(kernel, ctas, stream);
+  const long long need = nbig + (a.nobj - nbig + ctas - 1) / ctas;
+  const int clusters = int(std::max(1LL, std::min<long long>(cap, need)));
+  cudaLaunchConfig_t config = cluster_config(clusters, ctas, stream, attr);
+  BK_CUDA(cudaLaunchKernelExC(&config, kernel, kargs));
 }
 
 }  // namespace
 
-void launch_prepare(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big) {
-  launch_pair((const void *)prepare_small, (const void *)prepare_big, a, nbig, sm_count, small, big);
+long long trace_cluster_voxels(long long foreground) {
+  static std::mutex lock;
+  static std::map<int, long long> known;  // resident engine CTAs per device
+  int device = 0;
+  BK_CUDA(cudaGetDevice(&device));
+  long long ctas = 0;
+  {
+    std::lock_guard<std::mutex> guard(lock);
+    auto it = known.find(device);
+    if (it == known.end()) {
+      int sms = 1, per_sm = 1;
+      BK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+      BK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<kClusterCtas>, kEngineThreads, 0));
+      it = known.emplace(device, std::max(1LL, (long long)sms * per_sm)).first;
+    }
+    ctas = it->second;
+  }
+  return std::max(kTraceClusterFloor, foreground / (2 * ctas));
 }
 
-void launch_trace(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big) {
-  launch_pair((const void *)trace_small, (const void *)trace_big, a, nbig, sm_count, small, big);
+int cluster_ctas(long long largest, long long foreground) {
+  return largest * kWideClusterShare >= foreground ? kWideClusterCtas : kClusterCtas;
+}
+
+void launch_prepare(const EngineArgs &a, int nbig, int ctas, cudaStream_t stream) {
+  if (ctas == kWideClusterCtas) launch((const void *)prepare_kernel<kWideClusterCtas>, ctas, a, nbig, stream);
+  else launch((const void *)prepare_kernel<kClusterCtas>, kClusterCtas, a, nbig, stream);
+}
+
+void launch_trace(const EngineArgs &a, int nbig, int ctas, cudaStream_t stream) {
+  if (ctas == kWideClusterCtas) launch((const void *)trace_kernel<kWideClusterCtas>, ctas, a, nbig, stream);
+  else launch((const void *)trace_kernel<kClusterCtas>, kClusterCtas, a, nbig, stream);
 }
 
 }  // namespace bk

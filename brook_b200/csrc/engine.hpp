@@ -82,19 +82,27 @@ struct EngineArgs {
   float wx, wy, wz, scale, constant, delta;
 };
 
-// Objects with at least kPrepareClusterVoxels (preparation) / kTraceClusterVoxels (tracing)
-// voxels run on a cluster of kClusterCtas CTAs that share the object's frontiers through
-// distributed shared memory; smaller objects on one CTA each. Tracing keeps clusters for the
-// largest objects only: a cluster spends more CTA-time per object than a lone CTA, which pays
-// only where the object's own chain would otherwise set the kernel's length.
-constexpr int kClusterCtas = 8;
+// Objects with at least kPrepareClusterVoxels voxels (preparation) or more voxels than
+// trace_cluster_voxels (tracing) run on a cluster of CTAs that share the object's frontiers
+// through distributed shared memory; smaller objects on one CTA each. Tracing keeps clusters for
+// the objects whose lone-CTA chain would outlast the kernel's even share of the work: a cluster
+// spends more CTA-time per object than a lone CTA, which pays only where the object's own chain
+// would otherwise set the kernel's length. Clusters have kClusterCtas CTAs, or kWideClusterCtas
+// when the largest object holds at least 1/kWideClusterShare of the foreground (its chain is
+// then the kernel's length whatever else runs beside it).
+constexpr int kClusterCtas = 4;
+constexpr int kWideClusterCtas = 8;
+constexpr long long kWideClusterShare = 16;
+int cluster_ctas(long long largest, long long foreground);
 constexpr int kPrepareClusterVoxels = 8192;
-constexpr int kTraceClusterVoxels = 65536;
+constexpr long long kTraceClusterFloor = 16384;
+// Half the foreground voxels per resident engine CTA (largest-first scheduling then leaves the
+// clusters' objects as the only ones longer than a CTA's share), at least kTraceClusterFloor.
+long long trace_cluster_voxels(long long foreground);
 
-// One pass of the engine over two queues (schedule[0, nbig) = large objects, schedule[nbig,
-// nobj) = the rest, each largest first): the large ones on `big` (cluster launch), the rest on
-// `small`, concurrently. queue[0] / queue[1] must be zero.
-void launch_prepare(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big);
-void launch_trace(const EngineArgs &a, int nbig, int sm_count, cudaStream_t small, cudaStream_t big);
+// One pass of the engine: clusters take schedule[0, nbig) (large objects, largest first), then
+// every CTA takes schedule[nbig, nobj) alone. queue[0] and queue[1] must be zero.
+void launch_prepare(const EngineArgs &a, int nbig, int cluster_ctas, cudaStream_t stream);
+void launch_trace(const EngineArgs &a, int nbig, int cluster_ctas, cudaStream_t stream);
 
 }  // namespace bk

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 #include <numeric>
 #include <stdexcept>
 
@@ -302,7 +303,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     return n;
   };
   const int nbig_prepare = leading("BROOK_B200_PREPARE_CLUSTER_VOXELS", kPrepareClusterVoxels);
-  const int nbig_trace = leading("BROOK_B200_TRACE_CLUSTER_VOXELS", kTraceClusterVoxels);
+  const int nbig_trace = leading("BROOK_B200_TRACE_CLUSTER_VOXELS", trace_cluster_voxels(F));
   auto d_arena_offset = to_device(ctx, arena_offset), d_arena_dims = to_device(ctx, arena_dims);
   auto d_obj_arena = to_device(ctx, obj_arena), d_obj_begin = to_device(ctx, obj_begin), d_obj_count = to_device(ctx, obj_count);
   auto d_seg_end = to_device(ctx, seg_end), d_schedule = to_device(ctx, schedule), d_border_root = to_device(ctx, border_root);
@@ -344,10 +345,9 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.delta = std::min({aniso[0], aniso[1], aniso[2]});
 
   clock.mark("state");
-  ctx.fork();
-  launch_prepare(a, nbig_prepare, ctx.sm_count(), s, ctx.side_stream());
-  ctx.join();
-  ctx.launches += (nbig_prepare > 0) + (nobj > nbig_prepare);
+  const int ctas = cluster_ctas(nobj ? obj_count[schedule[0]] : 0, F);
+  launch_prepare(a, nbig_prepare, ctas, s);
+  ++ctx.launches;
   clock.mark("prepare");
   if (const char *fields = std::getenv("BROOK_B200_DUMP_FIELDS")) {
     // diagnostics: the prepared DAF and PDRF (root rails included) as raw float32 files
@@ -357,17 +357,25 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       if (f) { std::fwrite(item.second->data(), sizeof(float), item.second->size(), f); std::fclose(f); }
     }
   }
+  // host-side time of the stages that wait on the device or work on the host, beside their
+  // device-timeline spans: ctx.stats["host_ms_<step>"]
+  auto host_t = std::chrono::steady_clock::now();
+  auto host_mark = [&](const char *step) {
+    const auto now = std::chrono::steady_clock::now();
+    ctx.stats[std::string("host_ms_") + step] += std::chrono::duration<double, std::milli>(now - host_t).count();
+    host_t = now;
+  };
   Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), d_seg_end.data(), nobj);
+  host_mark("order");
   a.order = order.data();
   BK_CUDA(cudaMemsetAsync(queue.data(), 0, 2 * sizeof(int), s));
   clock.mark("order");
-  ctx.fork();
-  launch_trace(a, nbig_trace, ctx.sm_count(), s, ctx.side_stream());
-  ctx.join();
-  ctx.launches += (nbig_trace > 0) + (nobj > nbig_trace);
+  launch_trace(a, nbig_trace, ctas, s);
+  ++ctx.launches;
   clock.mark("trace");
 
   // ---- results
+  host_mark("trace_launch");
   const auto st_host = status.download();
   for (int o = 0; o < nobj; ++o)
     if (st_host[o] != kOk) {
@@ -460,7 +468,9 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     arena_off[v] = vs[v].offset;
     arena_dim[v] = {vs[v].d.sx, vs[v].d.sy, vs[v].d.sz};
   }
+  host_mark("results");
   AssemblyResult asmb = assemble(ctx, cstore.data(), dbf.data(), ap, arena_off, arena_dim, aniso);
+  host_mark("assemble");
   const long long V = asmb.vertex_offsets.back(), E = asmb.edge_offsets.back();
   std::vector<float> hvert(3 * V), hrad(V);
   std::vector<uint32_t> hedge(2 * E);
@@ -484,6 +494,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       out.edge_offsets.push_back(int64_t(out.edges.size() / 2));
     }
   }
+  host_mark("packed");
   clock.mark("assembly");
   clock.finish();
   const auto w = work.download();

@@ -14,9 +14,6 @@ Context::Context(int device) : device_(device) {
   if (prop.major < 10) throw std::invalid_argument("brook_b200 requires a compute capability 10.x (Blackwell) GPU");
   sm_count_ = prop.multiProcessorCount;
   BK_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  BK_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-  BK_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
-  BK_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
   // Keep freed blocks in this process's pool between calls: repeated calls of one shape then
   // allocate nothing from the driver.
   cudaMemPool_t pool;
@@ -31,23 +28,9 @@ Context::~Context() {
     cudaGetDevice(&previous);
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
-    cudaStreamSynchronize(side_);
     cudaStreamDestroy(stream_);
-    cudaStreamDestroy(side_);
-    cudaEventDestroy(fork_);
-    cudaEventDestroy(join_);
     if (previous >= 0) cudaSetDevice(previous);
   }
-}
-
-void Context::fork() const {
-  BK_CUDA(cudaEventRecord(fork_, stream_));
-  BK_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
-}
-
-void Context::join() const {
-  BK_CUDA(cudaEventRecord(join_, side_));
-  BK_CUDA(cudaStreamWaitEvent(stream_, join_, 0));
 }
 
 void *Context::allocate(size_t bytes) {

@@ -1,5 +1,4 @@
-// Host runtime of brook_b200: one context per device with a non-blocking stream (plus a second one
-// for work that runs beside it inside a call), stream-ordered
+// Host runtime of brook_b200: one context per device with one non-blocking stream, stream-ordered
 // allocations from the device's memory pool, typed device buffers and the error types the C ABI
 // maps to status codes.
 #pragma once
@@ -53,12 +52,6 @@ class Context {
 
   int device() const { return device_; }
   cudaStream_t stream() const { return stream_; }
-  // A second stream for kernels that run concurrently with the main stream inside one call:
-  // fork() makes it wait for the main stream's work so far, join() makes the main stream wait
-  // for everything queued on it.
-  cudaStream_t side_stream() const { return side_; }
-  void fork() const;
-  void join() const;
   int sm_count() const { return sm_count_; }
   void synchronize() const { BK_CUDA(cudaStreamSynchronize(stream_)); }
   void *allocate(size_t bytes);
@@ -71,8 +64,7 @@ class Context {
 
  private:
   int device_ = 0, sm_count_ = 0;
-  cudaStream_t stream_ = nullptr, side_ = nullptr;
-  cudaEvent_t fork_ = nullptr, join_ = nullptr;
+  cudaStream_t stream_ = nullptr;
   std::mutex mutex_;
 };
 

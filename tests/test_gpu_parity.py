@@ -71,6 +71,19 @@ def test_cfg0_full_size_matches_oracle(gpu):
     assert_same(got, exp, "cfg0")
 
 
+@pytest.mark.parametrize("cluster_voxels", ["1", "1000000000"])
+def test_cluster_and_lone_cta_paths_match_oracle(gpu, monkeypatch, cluster_voxels):
+    """Every object on a thread-block cluster ("1"), or every object on one CTA: the same skeletons."""
+    from brook_b200 import synthetic
+
+    monkeypatch.setenv("BROOK_B200_PREPARE_CLUSTER_VOXELS", cluster_voxels)
+    monkeypatch.setenv("BROOK_B200_TRACE_CLUSTER_VOXELS", cluster_voxels)
+    labels = synthetic.tube_volume((96, 96, 96), objects=12, seed=3)
+    got, exp = run_both(labels, teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    assert len(got) == 12
+    assert_same(got, exp, f"cluster threshold {cluster_voxels}")
+
+
 @pytest.mark.parametrize("dtype", [np.uint8, np.uint16, np.uint64, np.int32, np.int64])
 def test_dtypes(gpu, dtype):
     from brook_b200 import synthetic
