@@ -33,6 +33,9 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     "dense512": dict(workload="dense segmentation 512x512x512 uint64, 600 Voronoi seeds cut by tubes r=3-10 (seed 1)",
                      shape=(512, 512, 512), seeds=600, seed=1, kind="dense", dtype="uint64", anisotropy=(8, 8, 40)),
+    "dense256": dict(workload="dense segmentation 256x256x256 uint64, 80 Voronoi seeds cut by tubes r=3-10 (seed 5); "
+                          "the profiling case", shape=(256, 256, 256), seeds=80, seed=5, kind="dense", dtype="uint64",
+                     anisotropy=(8, 8, 40)),
     "batch64": dict(workload="64 uneven uint32 volumes (edges log-uniform 64-256), 10-80 tubes r=1-8, ~5% arbors (seed 2)",
                     seed=2, kind="batch", dtype="uint32", anisotropy=(4, 4, 4)),
     "serve": dict(workload="Poisson request stream at 50/200/800 req/s (seed 4), volume edges log-uniform 32-384, "
@@ -392,7 +395,8 @@ def run_ours(args, cfg):
         "skeletons_per_s": skeletons / (ms / 1e3),
         "config": {"workload": cfg["workload"], "voxels_per_gpu": int(volume.size), "objects": int(stage.get("objects", 0)),
                    "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST,
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (labels 1 GiB per step)"},
+                   "parallelism": f"replicas x{world}", "l2": f"labels of {volume.nbytes / 2**20:.0f} MiB per step, "
+                         + ("larger than L2 (126 MB)" if volume.nbytes > 126e6 else "smaller than L2: not flushed")},
         "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
         "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
         "work": {k: stage.get(k) for k in ("paths", "railroad_settled", "railroad_touched", "invalidated", "foreground")},
