@@ -29,7 +29,7 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_connected_components", "brook_components_destroy", "brook_components_view",
            "brook_components_copy_to_host", "brook_edt", "brook_skeletonize_options_init", "brook_skeletonize",
            "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy", "brook_context_stats",
-           "brook_edt_device_noalloc"]
+           "brook_edt_device_noalloc", "brook_skeletons_get_device_view", "brook_skeletons_get_array"]
 
 
 class Volume(ctypes.Structure):
@@ -61,6 +61,16 @@ class SkeletonsView(ctypes.Structure):
                 ("edge_offsets", ctypes.POINTER(ctypes.c_int64)), ("vertices", ctypes.POINTER(ctypes.c_float)),
                 ("edges", ctypes.POINTER(ctypes.c_uint32)), ("radii", ctypes.POINTER(ctypes.c_float)),
                 ("anisotropy", ctypes.c_float * 3)]
+
+
+class SkeletonsDeviceView(ctypes.Structure):
+    _fields_ = [("skeleton_count", ctypes.c_size_t), ("vertex_count", ctypes.c_size_t), ("edge_count", ctypes.c_size_t),
+                ("labels", ctypes.POINTER(ctypes.c_int64)), ("vertex_offsets", ctypes.POINTER(ctypes.c_int64)),
+                ("edge_offsets", ctypes.POINTER(ctypes.c_int64)), ("vertices", Volume), ("edges", Volume),
+                ("radii", Volume), ("anisotropy", ctypes.c_float * 3)]
+
+
+VERTICES, EDGES, RADII = 0, 1, 2
 
 
 class BrookError(RuntimeError):
@@ -103,6 +113,8 @@ def _load():
         "brook_context_stats": (ctypes.c_int, [vp, ctypes.c_char_p, sz, ctypes.POINTER(sz)]),
         "brook_edt_device_noalloc": (ctypes.c_int, [ctypes.POINTER(Volume), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
                                                     vp, vp]),
+        "brook_skeletons_get_device_view": (ctypes.c_int, [vp, ctypes.POINTER(SkeletonsDeviceView)]),
+        "brook_skeletons_get_array": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(vp)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -20,26 +20,7 @@ struct brook_context {
   explicit brook_context(int device) : value(device) {}
 };
 
-// Device storage that outlives the context that made it (plain cudaMalloc / cudaFree).
-struct DeviceStorage {
-  void *ptr = nullptr;
-  int device = 0;
-  DeviceStorage(size_t bytes, int dev) : device(dev) {
-    if (bytes) {
-      cudaError_t s = cudaMalloc(&ptr, bytes);
-      if (s != cudaSuccess) { cudaGetLastError(); throw bk::CudaError(s, "cudaMalloc"); }
-    }
-  }
-  ~DeviceStorage() {
-    if (ptr) {
-      int previous = -1;
-      cudaGetDevice(&previous);
-      cudaSetDevice(device);
-      cudaFree(ptr);
-      if (previous >= 0) cudaSetDevice(previous);
-    }
-  }
-};
+using bk::DeviceStorage;
 
 struct brook_array {
   std::shared_ptr<DeviceStorage> storage;
@@ -56,6 +37,8 @@ struct brook_components {
 
 struct brook_skeletons {
   bk::Packed packed;
+  // a device result's host copy, made by the first brook_skeletons_get_view
+  mutable std::once_flag host_copy;
 };
 
 namespace {
@@ -170,8 +153,8 @@ bk::Options options_of(const brook_skeletonize_options *p) {
   const uint32_t known = BROOK_FIX_BRANCHING | BROOK_FIX_BORDERS | BROOK_FILTER_OBJECTS | BROOK_DEVICE_OUTPUT |
                          BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS;
   require(!(p->flags & ~known), "unknown skeletonization flags");
-  if (p->flags & (BROOK_DEVICE_OUTPUT | BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS))
-    throw std::invalid_argument("device output, fill_holes and fix_avocados are not supported by this build");
+  if (p->flags & (BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS))
+    throw std::invalid_argument("fill_holes and fix_avocados are not supported by this build");
   if (p->voxel_graph) throw std::invalid_argument("voxel_graph is not supported by this build");
   bk::Options o;
   auto &t = o.teasar;
@@ -188,6 +171,7 @@ bk::Options options_of(const brook_skeletonize_options *p) {
   o.dust = p->dust_threshold;
   o.fix_branching = (p->flags & BROOK_FIX_BRANCHING) != 0;
   o.fix_borders = (p->flags & BROOK_FIX_BORDERS) != 0;
+  o.device_output = (p->flags & BROOK_DEVICE_OUTPUT) != 0;
   if (p->flags & BROOK_FILTER_OBJECTS) {
     require(p->object_ids || !p->object_ids_count);
     o.object_ids = std::vector<int64_t>(p->object_ids, p->object_ids + p->object_ids_count);
@@ -225,6 +209,20 @@ brook_volume device_view(const void *data, brook_dtype dtype, bk::VolumeDims d) 
   return v;
 }
 
+// Device view of a row-major (rows x width) array of 4-byte elements: shape (width, rows, 1), x
+// (the element within a row) fastest.
+brook_volume skeleton_view(const DeviceStorage &s, brook_dtype dtype, int width, size_t rows) {
+  brook_volume v{};
+  v.struct_size = sizeof(v);
+  v.abi_version = BROOK_ABI_VERSION;
+  v.data = s.ptr;
+  v.dtype = dtype;
+  v.memory = BROOK_DEVICE;
+  v.shape[0] = width; v.shape[1] = int64_t(rows); v.shape[2] = 1;
+  v.strides[0] = 4; v.strides[1] = 4LL * width; v.strides[2] = 4LL * width * int64_t(rows);
+  return v;
+}
+
 brook_status skeletonize_many(brook_context *ctx, const brook_volume *volumes, size_t count,
                               const brook_skeletonize_options *p, brook_skeletons **out) {
   return protect([&] {
@@ -243,6 +241,11 @@ brook_status skeletonize_many(brook_context *ctx, const brook_volume *volumes, s
     ctx->value.synchronize();
     std::vector<std::unique_ptr<brook_skeletons>> handles;
     for (auto &r : results) {
+      if (options.device_output && !r.on_device()) {  // nothing traced: empty device arrays
+        r.device_vertices = std::make_shared<DeviceStorage>(0, ctx->value.device());
+        r.device_edges = std::make_shared<DeviceStorage>(0, ctx->value.device());
+        r.device_radii = std::make_shared<DeviceStorage>(0, ctx->value.device());
+      }
       handles.emplace_back(new brook_skeletons());
       handles.back()->packed = std::move(r);
     }
@@ -393,6 +396,18 @@ brook_status brook_skeletonize_batch(brook_context *ctx, const brook_volume *vol
 brook_status brook_skeletons_get_view(const brook_skeletons *r, brook_skeletons_view *out) {
   return protect([&] {
     require(r && out);
+    if (r->packed.on_device()) {  // a device result: one host copy, made on first use
+      std::call_once(r->host_copy, [&] {
+        auto &p = const_cast<bk::Packed &>(r->packed);
+        bk::DeviceGuard guard(p.device_vertices->device);
+        p.vertices.resize(p.device_vertices->bytes / sizeof(float));
+        p.radii.resize(p.device_radii->bytes / sizeof(float));
+        p.edges.resize(p.device_edges->bytes / sizeof(uint32_t));
+        if (!p.vertices.empty()) BK_CUDA(cudaMemcpy(p.vertices.data(), p.device_vertices->ptr, p.device_vertices->bytes, cudaMemcpyDeviceToHost));
+        if (!p.radii.empty()) BK_CUDA(cudaMemcpy(p.radii.data(), p.device_radii->ptr, p.device_radii->bytes, cudaMemcpyDeviceToHost));
+        if (!p.edges.empty()) BK_CUDA(cudaMemcpy(p.edges.data(), p.device_edges->ptr, p.device_edges->bytes, cudaMemcpyDeviceToHost));
+      });
+    }
     const auto &p = r->packed;
     out->skeleton_count = p.labels.size();
     out->vertex_count = p.radii.size();
@@ -407,6 +422,44 @@ brook_status brook_skeletons_get_view(const brook_skeletons *r, brook_skeletons_
   });
 }
 void brook_skeletons_destroy(brook_skeletons *r) { delete r; }
+
+brook_status brook_skeletons_get_device_view(const brook_skeletons *r, brook_skeletons_device_view *out) {
+  return protect([&] {
+    require(r && out);
+    *out = {};
+    const auto &p = r->packed;
+    if (!p.on_device()) throw std::invalid_argument("skeleton result was not requested with BROOK_DEVICE_OUTPUT");
+    out->skeleton_count = p.labels.size();
+    out->vertex_count = size_t(p.vertex_offsets.back());
+    out->edge_count = size_t(p.edge_offsets.back());
+    out->labels = p.labels.data();
+    out->vertex_offsets = p.vertex_offsets.data();
+    out->edge_offsets = p.edge_offsets.data();
+    out->vertices = skeleton_view(*p.device_vertices, BROOK_F32, 3, out->vertex_count);
+    out->edges = skeleton_view(*p.device_edges, BROOK_U32, 2, out->edge_count);
+    out->radii = skeleton_view(*p.device_radii, BROOK_F32, 1, out->vertex_count);
+    for (int a = 0; a < 3; ++a) out->anisotropy[a] = p.anisotropy[a];
+  });
+}
+
+brook_status brook_skeletons_get_array(const brook_skeletons *r, brook_skeleton_buffer buffer, brook_array **out) {
+  return protect([&] {
+    require(r && out);
+    *out = nullptr;
+    const auto &p = r->packed;
+    if (!p.on_device()) throw std::invalid_argument("skeleton result was not requested with BROOK_DEVICE_OUTPUT");
+    const size_t V = size_t(p.vertex_offsets.back()), E = size_t(p.edge_offsets.back());
+    auto handle = std::make_unique<brook_array>();
+    switch (buffer) {
+      case BROOK_VERTICES: handle->storage = p.device_vertices; handle->view = skeleton_view(*p.device_vertices, BROOK_F32, 3, V); break;
+      case BROOK_EDGES: handle->storage = p.device_edges; handle->view = skeleton_view(*p.device_edges, BROOK_U32, 2, E); break;
+      case BROOK_RADII: handle->storage = p.device_radii; handle->view = skeleton_view(*p.device_radii, BROOK_F32, 1, V); break;
+      default: throw std::invalid_argument("invalid skeleton buffer");
+    }
+    handle->bytes = handle->storage->bytes;
+    *out = handle.release();
+  });
+}
 
 brook_status brook_edt_device_noalloc(const brook_volume *labels, const float anisotropy[3], int black_border,
                                       float *out, void *stream) {

@@ -472,28 +472,55 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   AssemblyResult asmb = assemble(ctx, cstore.data(), dbf.data(), ap, arena_off, arena_dim, aniso);
   host_mark("assemble");
   const long long V = asmb.vertex_offsets.back(), E = asmb.edge_offsets.back();
-  std::vector<float> hvert(3 * V), hrad(V);
-  std::vector<uint32_t> hedge(2 * E);
-  if (V) {
-    BK_CUDA(cudaMemcpyAsync(hvert.data(), asmb.vertices.data(), hvert.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
-    BK_CUDA(cudaMemcpyAsync(hrad.data(), asmb.radii.data(), hrad.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+  std::vector<float> hvert, hrad;
+  std::vector<uint32_t> hedge;
+  if (!opt.device_output) {
+    hvert.resize(3 * V);
+    hrad.resize(V);
+    hedge.resize(2 * E);
+    if (V) {
+      BK_CUDA(cudaMemcpyAsync(hvert.data(), asmb.vertices.data(), hvert.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+      BK_CUDA(cudaMemcpyAsync(hrad.data(), asmb.radii.data(), hrad.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    if (E) BK_CUDA(cudaMemcpyAsync(hedge.data(), asmb.edges.data(), hedge.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   }
-  if (E) BK_CUDA(cudaMemcpyAsync(hedge.data(), asmb.edges.data(), hedge.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  ctx.synchronize();
   for (size_t v = 0; v < vs.size(); ++v) {
     Packed &out = results[v];
+    // a volume's skeletons are one contiguous range (groups are volume-major; a group without
+    // edges has no vertices either)
+    const int64_t vbase = asmb.vertex_offsets[group_begin[v]], ebase = asmb.edge_offsets[group_begin[v]];
+    const int64_t vend = asmb.vertex_offsets[group_begin[v + 1]], eend = asmb.edge_offsets[group_begin[v + 1]];
     for (int g = group_begin[v]; g < group_begin[v + 1]; ++g) {
-      const int64_t v0 = asmb.vertex_offsets[g], v1 = asmb.vertex_offsets[g + 1];
-      const int64_t e0 = asmb.edge_offsets[g], e1 = asmb.edge_offsets[g + 1];
-      if (e1 == e0) continue;
+      if (asmb.edge_offsets[g + 1] == asmb.edge_offsets[g]) continue;
       out.labels.push_back(group_labels[v][g - group_begin[v]]);
-      out.vertices.insert(out.vertices.end(), hvert.begin() + 3 * v0, hvert.begin() + 3 * v1);
-      out.radii.insert(out.radii.end(), hrad.begin() + v0, hrad.begin() + v1);
-      out.edges.insert(out.edges.end(), hedge.begin() + 2 * e0, hedge.begin() + 2 * e1);
-      out.vertex_offsets.push_back(int64_t(out.radii.size()));
-      out.edge_offsets.push_back(int64_t(out.edges.size() / 2));
+      out.vertex_offsets.push_back(asmb.vertex_offsets[g + 1] - vbase);
+      out.edge_offsets.push_back(asmb.edge_offsets[g + 1] - ebase);
+    }
+    if (opt.device_output) {
+      out.device_vertices = std::make_shared<DeviceStorage>(size_t(vend - vbase) * 3 * sizeof(float), ctx.device());
+      out.device_radii = std::make_shared<DeviceStorage>(size_t(vend - vbase) * sizeof(float), ctx.device());
+      out.device_edges = std::make_shared<DeviceStorage>(size_t(eend - ebase) * 2 * sizeof(uint32_t), ctx.device());
+      if (vend > vbase) {
+        BK_CUDA(cudaMemcpyAsync(out.device_vertices->ptr, asmb.vertices.data() + 3 * vbase, out.device_vertices->bytes,
+                                cudaMemcpyDeviceToDevice, s));
+        BK_CUDA(cudaMemcpyAsync(out.device_radii->ptr, asmb.radii.data() + vbase, out.device_radii->bytes,
+                                cudaMemcpyDeviceToDevice, s));
+      }
+      if (eend > ebase)
+        BK_CUDA(cudaMemcpyAsync(out.device_edges->ptr, asmb.edges.data() + 2 * ebase, out.device_edges->bytes,
+                                cudaMemcpyDeviceToDevice, s));
     }
   }
+  ctx.synchronize();
+  if (!opt.device_output)
+    for (size_t v = 0; v < vs.size(); ++v) {
+      Packed &out = results[v];
+      const int64_t vbase = asmb.vertex_offsets[group_begin[v]], ebase = asmb.edge_offsets[group_begin[v]];
+      const int64_t vend = asmb.vertex_offsets[group_begin[v + 1]], eend = asmb.edge_offsets[group_begin[v + 1]];
+      out.vertices.assign(hvert.begin() + 3 * vbase, hvert.begin() + 3 * vend);
+      out.radii.assign(hrad.begin() + vbase, hrad.begin() + vend);
+      out.edges.assign(hedge.begin() + 2 * ebase, hedge.begin() + 2 * eend);
+    }
   host_mark("packed");
   clock.mark("assembly");
   clock.finish();

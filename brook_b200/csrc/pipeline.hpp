@@ -3,6 +3,7 @@
 #pragma once
 #include <array>
 #include <cstdint>
+#include <memory>
 #include <optional>
 #include <vector>
 
@@ -24,16 +25,21 @@ struct Options {
   bool fix_branching = true, fix_borders = true;
   std::optional<std::vector<int64_t>> object_ids;
   std::vector<Point> targets_before, targets_after;
+  bool device_output = false;  // keep vertices, edges and radii on the device (BROOK_DEVICE_OUTPUT)
 };
 
 // Packed skeletons of one volume: skeleton k has label labels[k], vertices
 // [vertex_offsets[k], vertex_offsets[k+1]) (x, y, z physical, row major), the same range of
 // radii, and edges [edge_offsets[k], edge_offsets[k+1]) local to the skeleton.
+// With device output the three arrays live in `device_*` (same layouts; storage that outlives the
+// context) and the host vectors stay empty.
 struct Packed {
   std::vector<int64_t> labels, vertex_offsets{0}, edge_offsets{0};
   std::vector<float> vertices, radii;
   std::vector<uint32_t> edges;
   std::array<float, 3> anisotropy{1, 1, 1};
+  std::shared_ptr<DeviceStorage> device_vertices, device_edges, device_radii;
+  bool on_device() const { return device_vertices != nullptr; }
 };
 
 // A label volume already on the device, Fortran-ordered (x fastest), borrowed for the call.

@@ -68,6 +68,31 @@ class Context {
   std::mutex mutex_;
 };
 
+// Device storage that outlives the context that made it (plain cudaMalloc / cudaFree on its
+// device): results handed to callers.
+struct DeviceStorage {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  int device = 0;
+  DeviceStorage(size_t n, int dev) : bytes(n), device(dev) {
+    if (n) {
+      cudaError_t s = cudaMalloc(&ptr, n);
+      if (s != cudaSuccess) { cudaGetLastError(); throw CudaError(s, "cudaMalloc"); }
+    }
+  }
+  ~DeviceStorage() {
+    if (ptr) {
+      int previous = -1;
+      cudaGetDevice(&previous);
+      cudaSetDevice(device);
+      cudaFree(ptr);
+      if (previous >= 0) cudaSetDevice(previous);
+    }
+  }
+  DeviceStorage(const DeviceStorage &) = delete;
+  DeviceStorage &operator=(const DeviceStorage &) = delete;
+};
+
 // A typed stream-ordered device allocation owned by one context.
 template <class T>
 class Buffer {

@@ -97,6 +97,19 @@ typedef struct brook_skeletons_view {
   float anisotropy[3];
 } brook_skeletons_view;
 
+/* brook.h:96-101: a result made with BROOK_DEVICE_OUTPUT. Labels and offsets on the host; the
+ * vertices (shape {3, vertex_count, 1}), edges ({2, edge_count, 1}) and radii ({vertex_count, 1,
+ * 1}) are device arrays of the context's device, row major, owned by the result handle. */
+typedef struct brook_skeletons_device_view {
+  size_t skeleton_count, vertex_count, edge_count;
+  const int64_t *labels, *vertex_offsets, *edge_offsets;
+  brook_volume vertices, edges, radii;
+  float anisotropy[3];
+} brook_skeletons_device_view;
+
+/* brook.h:102 */
+typedef enum brook_skeleton_buffer { BROOK_VERTICES = 0, BROOK_EDGES = 1, BROOK_RADII = 2 } brook_skeleton_buffer;
+
 uint32_t brook_abi_version(void);       /* brook.h:147 */
 const char *brook_version(void);        /* brook.h:148 */
 const char *brook_last_error(void);     /* brook.h:150 */
@@ -136,9 +149,13 @@ brook_status brook_skeletonize(brook_context *context, const brook_volume *label
 brook_status brook_skeletonize_batch(brook_context *context, const brook_volume *volumes, size_t count,
                                      const brook_skeletonize_options *options, brook_skeletons **out);
 
-/* brook.h:238-252 */
+/* brook.h:238-252. A device result (BROOK_DEVICE_OUTPUT) is copied to the host on the first call. */
 brook_status brook_skeletons_get_view(const brook_skeletons *result, brook_skeletons_view *out);
 void brook_skeletons_destroy(brook_skeletons *result);
+/* brook.h:232: device arrays of a result made with BROOK_DEVICE_OUTPUT (INVALID_ARGUMENT otherwise). */
+brook_status brook_skeletons_get_device_view(const brook_skeletons *result, brook_skeletons_device_view *out);
+/* brook.h:233: one of those arrays as an array handle sharing the result's storage. */
+brook_status brook_skeletons_get_array(const brook_skeletons *result, brook_skeleton_buffer buffer, brook_array **out);
 
 /* No counterpart in the reference. The EDT of brook_edt for callers that cannot allocate device
  * memory: code running inside another framework's memory budget (a caching allocator or a

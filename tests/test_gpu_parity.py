@@ -242,6 +242,45 @@ def test_c_abi_known_answers(gpu):
     assert lib.brook_last_error()
 
 
+def test_c_abi_device_output(gpu):
+    """BROOK_DEVICE_OUTPUT (brook.h:96-102, 232-233): the device view and array handles hold the
+    same skeletons as the host route; get_view copies a device result to the host; a host result
+    has no device view."""
+    from brook_b200 import _native as n
+    from brook_b200 import _intake, synthetic
+
+    labels = np.asfortranarray(synthetic.tube_volume((64, 64, 64), objects=8, seed=5))
+    vol = n.host_volume(labels)
+    ctx = n.context(0)
+    opts = n.options(_intake.teasar(CFG0_PARAMS), (16, 16, 40), 100, True, True)
+    host = ctypes.c_void_p()
+    n.check(n.lib.brook_skeletonize(ctx, ctypes.byref(vol), ctypes.byref(opts), ctypes.byref(host)))
+    dv = n.SkeletonsDeviceView()
+    assert n.lib.brook_skeletons_get_device_view(host, ctypes.byref(dv)) == n.INVALID_ARGUMENT
+    expected = n.packed_arrays(host)
+    opts.flags |= n.DEVICE_OUTPUT
+    dev = ctypes.c_void_p()
+    n.check(n.lib.brook_skeletonize(ctx, ctypes.byref(vol), ctypes.byref(opts), ctypes.byref(dev)))
+    n.check(n.lib.brook_skeletons_get_device_view(dev, ctypes.byref(dv)))
+    nv, ne = dv.vertex_count, dv.edge_count
+    assert dv.skeleton_count == len(expected["labels"]) and nv == len(expected["radii"]) and ne == len(expected["edges"])
+    assert dv.vertices.memory == 1 and tuple(dv.vertices.shape) == (3, nv, 1) and tuple(dv.edges.shape) == (2, ne, 1)
+    got = {}
+    for name, which, dtype, shape in (("vertices", n.VERTICES, np.float32, (nv, 3)), ("edges", n.EDGES, np.uint32, (ne, 2)),
+                                      ("radii", n.RADII, np.float32, (nv,))):
+        arr = ctypes.c_void_p()
+        n.check(n.lib.brook_skeletons_get_array(dev, which, ctypes.byref(arr)))
+        buf = np.zeros(shape, dtype)
+        n.check(n.lib.brook_array_copy_to_host(arr, buf.ctypes.data, buf.nbytes))
+        n.lib.brook_array_destroy(arr)  # the array handle shares the result's storage
+        got[name] = buf
+    for name in ("vertices", "edges", "radii"):
+        np.testing.assert_array_equal(got[name], expected[name], err_msg=name)
+    copied = n.packed_arrays(dev)  # get_view on a device result, then destroy
+    for name in ("labels", "v_off", "e_off", "vertices", "edges", "radii"):
+        np.testing.assert_array_equal(copied[name], expected[name], err_msg=name)
+
+
 def test_edt_matches_oracle(gpu):
     """The EDT alone, through the C ABI, on multi-label volumes with and without black border."""
     from brook_b200 import _native as n
