@@ -3,6 +3,11 @@
 // root to the smaller), a read-only flatten, and ids from an exclusive scan of the root flags in
 // flat order: id k belongs to the k-th root in ascending flat order, the reference's canonical
 // numbering (ccl.cu:25-63 of giorgioangel/brook) without its host sort.
+//
+// The union runs in two kernels: tile_union labels 32x8x8 tiles in shared memory (labels staged
+// once, union-find on shared indices; a tile's order is the volume's, so a tile root is its
+// component's lowest flat index in the tile) and writes every voxel's tile root as its parent;
+// face_union then unites only the pairs that cross a tile face, on the global parent array.
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -50,25 +55,92 @@ __device__ __forceinline__ void unite(int *parent, int a, int b) {
   }
 }
 
-__global__ void init_parent(int *parent, long long n) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) parent[i] = (int)i;
+constexpr int kTileX = 32, kTileY = 8, kTileZ = 8, kTileN = kTileX * kTileY * kTileZ, kTileThreads = 512;
+
+// Whether the pair (p, p + (dx, dy, dz)) of equal labels is skipped: an edge pair with a face
+// intermediate of the label, a corner pair with a face or edge intermediate of it. `same(a, b, c)`
+// tells whether p + (a, b, c) (inside the volume) has p's label.
+template <class Same>
+__device__ __forceinline__ bool skipped(int dx, int dy, int dz, Same same) {
+  const int nonzero = (dx != 0) + (dy != 0) + (dz != 0);
+  if (nonzero == 2) return (dx && same(dx, 0, 0)) || (dy && same(0, dy, 0)) || (dz && same(0, 0, dz));
+  if (nonzero == 3)
+    return same(dx, 0, 0) || same(0, dy, 0) || same(0, 0, dz) || same(dx, dy, 0) || same(dx, 0, dz) || same(0, dy, dz);
+  return false;
 }
 
-// The 13 neighbours with a positive flat offset (dz > 0, or dz == 0 and dy > 0, or dz == dy == 0
-// and dx > 0). A face pair of equal labels is always united. An edge pair is skipped when one of
-// its two face-adjacent intermediates has the label (the pair is then joined through it), a corner
-// pair when one of its three face or three edge intermediates has it: by induction over face ->
-// edge -> corner every skipped pair still ends in one component. `planar`: neighbours in the same
-// z-slice only (a stack of independent 2D images).
+__device__ __forceinline__ int tile_find(const int *par, int i) {
+  int p = par[i];
+  while (p != i) { i = p; p = par[i]; }
+  return i;
+}
+
+__device__ __forceinline__ void tile_unite(int *par, int a, int b) {
+  a = tile_find(par, a);
+  b = tile_find(par, b);
+  while (a != b) {
+    if (a < b) { int t = a; a = b; b = t; }
+    const int old = atomicCAS(par + a, a, b);
+    if (old == a) return;
+    a = tile_find(par, old);
+    b = tile_find(par, b);
+  }
+}
+
+// grid (x tiles, y tiles, z tiles); parent of every voxel of the tile = its tile root (global).
 template <class L>
-__global__ void union_forward(const L *labels, int *parent, Dims d, bool planar) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__ labels, int *parent, Dims d, bool planar) {
+  __shared__ L lab[kTileN];
+  __shared__ int par[kTileN];
+  const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z0 = blockIdx.z * kTileZ;
+  const int ex = min(kTileX, d.sx - x0), ey = min(kTileY, d.sy - y0), ez = min(kTileZ, d.sz - z0);
+  for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
+    const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
+    const bool in = lx < ex && ly < ey && lz < ez;
+    lab[t] = in ? labels[(x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz))] : L(0);
+    par[t] = t;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
+    const L lv = lab[t];
+    if (lv == L(0)) continue;
+    const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
+    auto same = [&](int a, int b, int c) { return lab[t + a + kTileX * (b + kTileY * c)] == lv; };
+#pragma unroll
+    for (int k = 0; k < 26; ++k) {
+      const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
+      if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
+      if (planar && dz != 0) continue;
+      const int nx = lx + dx, ny = ly + dy, nz = lz + dz;
+      if (nx < 0 || ny < 0 || nx >= ex || ny >= ey || nz >= ez) continue;  // other tiles: face_union
+      if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
+      tile_unite(par, t, t + dx + kTileX * (dy + kTileY * dz));
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
+    const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
+    if (!(lx < ex && ly < ey && lz < ez)) continue;
+    const int r = tile_find(par, t);
+    const int rx = r % kTileX, ry = (r / kTileX) % kTileY, rz = r / (kTileX * kTileY);
+    const long long g = (x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz));
+    parent[g] = int((x0 + rx) + (long long)d.sx * ((y0 + ry) + (long long)d.sy * (z0 + rz)));
+  }
+}
+
+// Pairs that cross a tile face: from every voxel on a face a forward neighbour can cross (both x
+// faces, both y faces — dy = -1 comes with dz = +1 — and the high z face), the forward neighbours
+// in another tile.
+template <class L>
+__global__ void face_union(const L *labels, int *parent, Dims d, bool planar) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n()) return;
-  const L lv = labels[i];
-  if (lv == 0) return;
   int x, y, z;
   unravel((int)i, d, x, y, z);
+  const int lx = x % kTileX, ly = y % kTileY, lz = z % kTileZ;
+  if (lx != 0 && lx != kTileX - 1 && ly != 0 && ly != kTileY - 1 && lz != kTileZ - 1) return;
+  const L lv = labels[i];
+  if (lv == L(0)) return;
   auto same = [&](int dx, int dy, int dz) {
     const int nx = x + dx, ny = y + dy, nz = z + dz;
     if (nx < 0 || ny < 0 || nz < 0 || nx >= d.sx || ny >= d.sy || nz >= d.sz) return false;
@@ -79,14 +151,9 @@ __global__ void union_forward(const L *labels, int *parent, Dims d, bool planar)
     const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
     if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
     if (planar && dz != 0) continue;
-    if (!same(dx, dy, dz)) continue;
-    const int nonzero = (dx != 0) + (dy != 0) + (dz != 0);
-    if (nonzero == 2) {
-      if ((dx && same(dx, 0, 0)) || (dy && same(0, dy, 0)) || (dz && same(0, 0, dz))) continue;
-    } else if (nonzero == 3) {
-      if (same(dx, 0, 0) || same(0, dy, 0) || same(0, 0, dz) || same(dx, dy, 0) || same(dx, 0, dz) || same(0, dy, dz))
-        continue;
-    }
+    const bool crosses = lx + dx < 0 || lx + dx >= kTileX || ly + dy >= kTileY || ly + dy < 0 || lz + dz >= kTileZ;
+    if (!crosses) continue;
+    if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
     unite(parent, (int)i, (int)i + nbr_offset(k, d));
   }
 }
@@ -138,8 +205,10 @@ ComponentsResult run(Context &ctx, const L *labels, VolumeDims vd, uint32_t *ids
   ComponentsResult out;
   Buffer<int> parent(ctx, n), rank(ctx, n + 1);
   cudaStream_t s = ctx.stream();
-  init_parent<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
-  union_forward<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), d, planar); ++ctx.launches;
+  const dim3 tiles((d.sx + kTileX - 1) / kTileX, (d.sy + kTileY - 1) / kTileY, (d.sz + kTileZ - 1) / kTileZ);
+  if (tiles.y > 65535 || tiles.z > 65535) throw std::invalid_argument("volume too large for the tiled union");
+  tile_union<L><<<tiles, kTileThreads, 0, s>>>(labels, parent.data(), d, planar); ++ctx.launches;
+  face_union<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), d, planar); ++ctx.launches;
   flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   thrust::counting_iterator<long long> index(0);
