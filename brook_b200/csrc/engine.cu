@@ -6,7 +6,9 @@
 // of its first CTA (distributed shared memory for a cluster, updated with 32-bit atomics only);
 // 64-bit reductions (nearest rail, nearest deferred voxel, argmax) keep one copy per CTA, updated
 // with CTA-local atomics and combined across the group at barriers. State other threads update
-// with atomics (distances, keys, flags, liveness, rails, staged entries) is always read through L2.
+// with atomics (distances, keys, flags, staged entries) is always read through L2; state that is
+// only written between floods, behind a group barrier (PDRF during a railroad flood, liveness
+// during an invalidation), is read through L1, where a voxel's 26 neighbours find it again.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -364,7 +366,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
       for (int i = G::tid(); i < nc; i += G::threads()) {
         const int u = __ldcg(cur + i);
         const unsigned was = atomicAnd(a.flags + u, ~kNearQueued);
-        const float fu = __ldcg(a.pdrf + u);
+        const float fu = a.pdrf[u];
         const float du = __ldcg(a.dist + u + (was >> 30));
         const unsigned long long rb = vload(&sh.rb);
         const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
@@ -381,7 +383,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
         if (!((unsigned(e) >> k) & 1u)) continue;
         const int v = __ldcg(cur + i) + sh.off[k];
         const float du = __uint_as_float(unsigned(e >> 32));
-        const float fv = __ldcg(a.pdrf + v);
+        const float fv = a.pdrf[v];
         const float cand = vw_step(du, fv);
         const float old = atomic_min_pos(a.dist + v, cand);
         if (old > cand) {
@@ -442,7 +444,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
         atomicAnd(a.flags + w, ~kFarQueued);
         if (!(atomicOr(a.flags + w, kNearQueued) & kNearQueued)) cur[atomicAdd(cur_count, 1)] = w;
       } else {
-        atomicMin(&sh.minfar, (static_cast<unsigned long long>(__float_as_uint(dw)) << 32) | __float_as_uint(__ldcg(a.pdrf + w)));
+        atomicMin(&sh.minfar, (static_cast<unsigned long long>(__float_as_uint(dw)) << 32) | __float_as_uint(a.pdrf[w]));
         keep[atomicAdd(&L->n_keep, 1)] = w;
       }
     }
@@ -469,7 +471,7 @@ __device__ int backtrace(const EngineArgs &a, const Shared &sh, unsigned long lo
       unsigned db = BK_INF_BITS;
       if (lane < 26 && ((m >> lane) & 1u)) {
         const int u = cur + sh.off[lane];
-        if (__ldcg(a.pdrf + u) != 0.0f) db = __float_as_uint(__ldcg(a.dist + u));
+        if (a.pdrf[u] != 0.0f) db = __float_as_uint(__ldcg(a.dist + u));
       }
       const unsigned mb = __reduce_min_sync(kFull, db);
       if (mb < BK_INF_BITS) kb = int(__reduce_min_sync(kFull, db == mb ? unsigned(lane) : 64u));
@@ -478,7 +480,7 @@ __device__ int backtrace(const EngineArgs &a, const Shared &sh, unsigned long lo
       const int u = cur + sh.off[kb];
       const uint32_t mu = a.mask[u];
       unsigned key = 64;
-      if (lane < 26 && ((mu >> lane) & 1u) && __ldcg(a.pdrf + u + sh.off[lane]) == 0.0f) key = unsigned(c_d3rank[lane]);
+      if (lane < 26 && ((mu >> lane) & 1u) && a.pdrf[u + sh.off[lane]] == 0.0f) key = unsigned(c_d3rank[lane]);
       const unsigned r = __reduce_min_sync(kFull, key);
       if (r < 26) {
         const int ks = c_d3inv[r];
@@ -576,7 +578,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
         const int u = __ldcg(cur + i);
         if (!((a.mask[u] >> k) & 1u)) continue;
         const int v = u + sh.off[k];
-        if (!__ldcg(a.alive + v)) continue;
+        if (!a.alive[v]) continue;
         const unsigned long long ku = __ldcg(wide + i);
         const int s = int(unsigned(ku));
         int ux, uy, uz, qx, qy, qz;
