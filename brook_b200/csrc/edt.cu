@@ -8,7 +8,9 @@
 //   the last pass takes the square root (background: 0).
 // The reference compiles the envelope with FMA contraction; its two product-plus-height sums are
 // written as explicit fused operations here, everything else rounds per operation (--fmad=false).
+#include <algorithm>
 #include <climits>
+#include <cmath>
 #include <mutex>
 
 #include "common.cuh"
@@ -76,29 +78,10 @@ __global__ void edt_x(const uint32_t *__restrict__ ids, float *__restrict__ D, D
   }
 }
 
-// One line of the y or z pass. Stacks V/H/Z are interleaved: entry k of this thread's stack is at
-// [k * pitch].
-__global__ void edt_envelope(const uint32_t *__restrict__ ids, float *__restrict__ D, Dims d, int axis, float w, int bb,
-                             long long line0, long long nbatch, int *__restrict__ Vs, float *__restrict__ Hs,
-                             double *__restrict__ Zs, int finish) {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= nbatch) return;
-  const long long line = line0 + tid;
-  long long base, stride;
-  int n;
-  if (axis == 1) {
-    const long long x = line % d.sx, z = line / d.sx;
-    if (z >= d.sz) return;
-    base = x + (long long)d.sx * d.sy * z; stride = d.sx; n = d.sy;
-  } else {
-    const long long x = line % d.sx, y = line / d.sx;
-    if (y >= d.sy) return;
-    base = x + (long long)d.sx * y; stride = (long long)d.sx * d.sy; n = d.sz;
-  }
-  int *V = Vs + tid;
-  float *H = Hs + tid;
-  double *Z = Zs + tid;
-  const long long pitch = nbatch;
+// One line of the y or z pass: n voxels from `base` with `stride`. Stacks V/H/Z are interleaved:
+// entry k of this thread's stack is at [k * pitch].
+__device__ void envelope_line(const uint32_t *__restrict__ ids, float *__restrict__ D, long long base, long long stride,
+                              int n, float w, int bb, int *V, float *H, double *Z, long long pitch, int finish) {
   const double w2 = (double)__fmul_rn(w, w);
   int i = 0;
   while (i < n) {
@@ -162,6 +145,57 @@ __global__ void edt_envelope(const uint32_t *__restrict__ ids, float *__restrict
   }
 }
 
+// Line `line` of the y (axis 1) or z (axis 2) pass of a (sx, sy, sz) volume at `offset`.
+__device__ __forceinline__ bool line_of(long long line, long long offset, Dims d, int axis, long long &base,
+                                        long long &stride, int &n) {
+  const long long x = line % d.sx, rest = line / d.sx;
+  if (axis == 1) {
+    if (rest >= d.sz) return false;
+    base = offset + x + (long long)d.sx * d.sy * rest; stride = d.sx; n = d.sy;
+  } else {
+    if (rest >= d.sy) return false;
+    base = offset + x + (long long)d.sx * rest; stride = (long long)d.sx * d.sy; n = d.sz;
+  }
+  return true;
+}
+
+__global__ void edt_envelope(const uint32_t *__restrict__ ids, float *__restrict__ D, Dims d, int axis, float w, int bb,
+                             long long line0, long long nbatch, int *__restrict__ Vs, float *__restrict__ Hs,
+                             double *__restrict__ Zs, int finish) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= nbatch) return;
+  long long base, stride;
+  int n;
+  if (!line_of(line0 + tid, 0, d, axis, base, stride, n)) return;
+  envelope_line(ids, D, base, stride, n, w, bb, Vs + tid, Hs + tid, Zs + tid, nbatch, finish);
+}
+
+// The y or z pass of several volumes of one flat index space in one launch: volume v's lines are
+// [line_begin[v], line_begin[v + 1]) of the launch's line space.
+struct EnvelopeVolume {
+  long long offset, line_begin;
+  int sx, sy, sz, bb;
+};
+
+__global__ void edt_envelope_volumes(const uint32_t *__restrict__ ids, float *__restrict__ D,
+                                     const EnvelopeVolume *__restrict__ vols, int nvol, int axis, float w,
+                                     long long line0, long long nbatch, int *__restrict__ Vs, float *__restrict__ Hs,
+                                     double *__restrict__ Zs, int finish) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= nbatch) return;
+  const long long line = line0 + tid;
+  int lo = 0, hi = nvol - 1;  // the last volume whose first line is <= line
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (vols[mid].line_begin <= line) lo = mid; else hi = mid - 1;
+  }
+  const EnvelopeVolume v = vols[lo];
+  long long base, stride;
+  int n;
+  if (!line_of(line - v.line_begin, v.offset, Dims{v.sx, v.sy, v.sz}, axis, base, stride, n)) return;
+  envelope_line(ids, D, base, stride, n, w, v.bb, Vs + tid, Hs + tid, Zs + tid, nbatch, finish);
+}
+
 }  // namespace
 
 void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3], bool black_border, int dims,
@@ -198,6 +232,57 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
       const long long nb = std::min(batch, lines - l0);
       edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, axis, aniso[axis], black_border ? 1 : 0, l0, nb,
                                                       V.data(), H.data(), Z.data(), last); ++ctx.launches;
+      BK_CUDA(cudaGetLastError());
+    }
+  }
+}
+
+void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume> &vols, const float aniso[3], float *D) {
+  if (vols.empty()) return;
+  for (int a = 0; a < 3; ++a)
+    if (!(aniso[a] > 0) || !std::isfinite(aniso[a])) throw std::invalid_argument("anisotropy must be finite and positive");
+  cudaStream_t s = ctx.stream();
+  int maxx = 1;
+  for (const auto &v : vols) maxx = std::max(maxx, v.d.sx);
+  // x pass, volume by volume (a warp per line fills the GPU on its own), one spacing table
+  std::vector<float> acc(maxx + 2, 0.0f);
+  for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + aniso[0];
+  Buffer<float> dacc = to_device(ctx, acc);
+  const size_t smem = size_t(kWarpsX) * maxx * sizeof(int);
+  if (smem > 200 * 1024) throw std::invalid_argument("x extent too large for the EDT x pass");
+  BK_CUDA(cudaFuncSetAttribute(edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (const auto &v : vols) {
+    if (!v.d.n()) continue;
+    const long long xlines = (long long)v.d.sy * v.d.sz;
+    edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(
+        ids + v.offset, D + v.offset, Dims{v.d.sx, v.d.sy, v.d.sz}, dacc.data(), v.black_border ? 1 : 0, 0);
+    ++ctx.launches;
+  }
+  BK_CUDA(cudaGetLastError());
+  // y and z passes: every volume's lines in one launch (a thread per line)
+  for (int axis = 1; axis <= 2; ++axis) {
+    std::vector<EnvelopeVolume> table;
+    long long lines = 0;
+    int len = 1;
+    for (const auto &v : vols) {
+      if (!v.d.n()) continue;
+      table.push_back({v.offset, lines, v.d.sx, v.d.sy, v.d.sz, v.black_border ? 1 : 0});
+      lines += axis == 1 ? (long long)v.d.sx * v.d.sz : (long long)v.d.sx * v.d.sy;
+      len = std::max(len, axis == 1 ? v.d.sy : v.d.sz);
+    }
+    if (!lines) continue;
+    Buffer<EnvelopeVolume> dtable = to_device(ctx, table);
+    const long long budget = 4LL << 30;  // bytes of envelope stacks per launch
+    const long long batch = std::max(1LL, std::min(lines, budget / (16LL * (len + 3))));
+    Buffer<int> V(ctx, batch * (len + 3));
+    Buffer<float> H(ctx, batch * (len + 3));
+    Buffer<double> Z(ctx, batch * (len + 3));
+    for (long long l0 = 0; l0 < lines; l0 += batch) {
+      const long long nb = std::min(batch, lines - l0);
+      edt_envelope_volumes<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, dtable.data(), int(table.size()), axis,
+                                                              aniso[axis], l0, nb, V.data(), H.data(), Z.data(),
+                                                              axis == 2 ? 1 : 0);
+      ++ctx.launches;
       BK_CUDA(cudaGetLastError());
     }
   }

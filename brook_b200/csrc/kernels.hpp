@@ -37,6 +37,16 @@ ComponentsResult connected_components(Context &ctx, const void *labels, int dtyp
 void edt(Context &ctx, const uint32_t *ids, VolumeDims d, const float aniso[3], bool black_border, int dims,
          float *out);
 
+// The 3D EDT of several volumes of one flat index space (ids and out share the offsets): the x
+// pass volume by volume, the y and z passes over every volume's lines in one launch each.
+struct EdtVolume {
+  long long offset;
+  VolumeDims d;
+  bool black_border;
+};
+void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume> &volumes, const float aniso[3],
+                 float *out);
+
 // EDT of uint32 labels with no device allocation (a fixed file-scope scratch in edt.cu); see there.
 void edt_fixed_scratch(const uint32_t *labels, VolumeDims d, const float aniso[3], bool black_border, float *out,
                        cudaStream_t stream);

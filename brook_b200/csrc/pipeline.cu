@@ -164,13 +164,22 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     if (!K) { st.empty = true; continue; }
     st.boxes = analyze(ctx, vid, st.d, K);
     clock.mark("analyze");
-    const bool black_border = K == 1 && st.boxes[1].count == n;
-    edt(ctx, vid, st.d, aniso, black_border, 3, dbf.data() + st.offset);
+  }
+  // ---- EDT of every volume at once (the y and z passes of all volumes' lines in one launch each)
+  {
+    std::vector<EdtVolume> ev;
+    for (const auto &st : vs)
+      if (!st.empty) ev.push_back({st.offset, st.d, st.cc.count == 1 && st.boxes[1].count == st.d.n()});
+    edt_volumes(ctx, ids.data(), ev, aniso, dbf.data());
     clock.mark("edt");
+  }
+  for (auto &st : vs) {
+    if (st.empty) continue;
+    uint32_t *vid = ids.data() + st.offset;
     neighbour_mask(ctx, vid, st.d, mask.data() + st.offset);
     clock.mark("mask");
-    st.borders.assign(K + 1, {});
-    st.dbf_max = segment_max(ctx, dbf.data() + st.offset, vid, n, K);
+    st.borders.assign(st.cc.count + 1, {});
+    st.dbf_max = segment_max(ctx, dbf.data() + st.offset, vid, st.d.n(), st.cc.count);
     clock.mark("dbf_max");
   }
   // ---- border targets of every volume in one pass
@@ -357,16 +366,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       if (f) { std::fwrite(item.second->data(), sizeof(float), item.second->size(), f); std::fclose(f); }
     }
   }
-  // host-side time of the stages that wait on the device or work on the host, beside their
-  // device-timeline spans: ctx.stats["host_ms_<step>"]
-  auto host_t = std::chrono::steady_clock::now();
-  auto host_mark = [&](const char *step) {
-    const auto now = std::chrono::steady_clock::now();
-    ctx.stats[std::string("host_ms_") + step] += std::chrono::duration<double, std::milli>(now - host_t).count();
-    host_t = now;
-  };
   Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), d_seg_end.data(), nobj);
-  host_mark("order");
   a.order = order.data();
   BK_CUDA(cudaMemsetAsync(queue.data(), 0, 2 * sizeof(int), s));
   clock.mark("order");
@@ -375,7 +375,6 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   clock.mark("trace");
 
   // ---- results
-  host_mark("trace_launch");
   const auto st_host = status.download();
   for (int o = 0; o < nobj; ++o)
     if (st_host[o] != kOk) {
@@ -468,9 +467,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     arena_off[v] = vs[v].offset;
     arena_dim[v] = {vs[v].d.sx, vs[v].d.sy, vs[v].d.sz};
   }
-  host_mark("results");
   AssemblyResult asmb = assemble(ctx, cstore.data(), dbf.data(), ap, arena_off, arena_dim, aniso);
-  host_mark("assemble");
   const long long V = asmb.vertex_offsets.back(), E = asmb.edge_offsets.back();
   std::vector<float> hvert, hrad;
   std::vector<uint32_t> hedge;
@@ -521,7 +518,6 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       out.radii.assign(hrad.begin() + vbase, hrad.begin() + vend);
       out.edges.assign(hedge.begin() + 2 * ebase, hedge.begin() + 2 * eend);
     }
-  host_mark("packed");
   clock.mark("assembly");
   clock.finish();
   const auto w = work.download();

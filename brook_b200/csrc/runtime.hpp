@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -144,10 +145,12 @@ class Buffer {
 };
 
 // Stage boundaries recorded as CUDA events on the context's stream; finish() adds each stage's
-// elapsed time to ctx.stats["ms_<stage>"].
+// elapsed time to ctx.stats["ms_<stage>"]. Each mark also adds the host time since the previous
+// mark to ctx.stats["host_ms_<stage>"] (near the device time: the device waited for the host).
 class StageClock {
   Context &ctx_;
   std::vector<std::pair<std::string, cudaEvent_t>> marks_;
+  std::chrono::steady_clock::time_point host_ = std::chrono::steady_clock::now();
 
  public:
   explicit StageClock(Context &ctx) : ctx_(ctx) { mark("start"); }
@@ -155,6 +158,9 @@ class StageClock {
     for (auto &m : marks_) cudaEventDestroy(m.second);
   }
   void mark(const std::string &stage) {
+    const auto now = std::chrono::steady_clock::now();
+    if (!marks_.empty()) ctx_.stats["host_ms_" + stage] += std::chrono::duration<double, std::milli>(now - host_).count();
+    host_ = now;
     cudaEvent_t e;
     BK_CUDA(cudaEventCreate(&e));
     BK_CUDA(cudaEventRecord(e, ctx_.stream()));
