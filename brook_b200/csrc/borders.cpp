@@ -1,9 +1,11 @@
-// Border targets (fix_borders): for each of the six faces, a 2D CC and a 2D EDT (black border) of
-// the face's component ids run on the GPU; the host then picks, per face component, the farthest
-// pixel with Kimimaro's tie-break (nearest the component's centroid, then the face centre, the
-// corners and the edges) and collects the picks per 3D component in the insertion order of a
-// CPython set of integer 3-tuples, which decides the reference's root and target order
-// (borders.cu:53-116 and point_set.hpp of giorgioangel/brook).
+// Border targets (fix_borders): every face of every volume goes into one stack of slices; a planar
+// CCL and planar EDTs (black border) run over the stack on the GPU, and per face component the
+// device gathers the pixel count, the coordinate sums, the largest distance, the first pixel with
+// a positive distance and the pixels at the largest distance. The host then picks, per face
+// component, the farthest pixel with Kimimaro's tie-break (nearest the component's centroid, then
+// the face centre, the corners and the edges) and collects the picks per 3D component in the
+// insertion order of a CPython set of integer 3-tuples, which decides the reference's root and
+// target order (borders.cu:53-116 and point_set.hpp of giorgioangel/brook).
 #include <algorithm>
 #include <limits>
 
@@ -107,14 +109,12 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
   const int axes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
   std::vector<Face> faces;
   int W = 1, H = 1;
-  long long packed = 0;
   for (int t = 0; t < 3; ++t)
     for (const auto &v : volumes)
       for (int side = 0; side < 2; ++side) {
         const int a = axes[t][0], b = axes[t][1], c = axes[t][2];
         const int shape[3] = {v.d.sx, v.d.sy, v.d.sz};
-        Face f{v.offset, v.d, a, b, c, side ? shape[c] - 1 : 0, packed};
-        packed += (long long)f.fx() * f.fy();
+        Face f{v.offset, v.d, a, b, c, side ? shape[c] - 1 : 0};
         W = std::max(W, f.fy());
         H = std::max(H, f.fx());
         faces.push_back(f);
@@ -139,72 +139,90 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
     edt(ctx, stack_ids.data() + slice * first, VolumeDims{W, H, int(per_group)}, plane_aniso, true, 2,
         dist.data() + slice * first);
   }
-  Buffer<uint32_t> pids(ctx, std::max(packed, 1LL));
-  Buffer<float> pdist(ctx, std::max(packed, 1LL));
-  pack_faces(ctx, stack_ids.data(), dist.data(), faces, W, H, pids.data(), pdist.data());
-  const std::vector<uint32_t> labs = pids.download(packed);
-  const std::vector<float> dds = pdist.download(packed);
+  // per component: counts, coordinate sums, largest distance, first pixel, and the pixels at the
+  // largest distance, from the device; the host does the per-component selection
+  const FaceStats st = face_stats(ctx, stack_ids.data(), dist.data(), faces, W, H, pc.count);
+  const size_t K = size_t(pc.count) + 1;
+  // a component's face: the stack slice of its first pixel
+  std::vector<int> face_of(K, -1);
+  for (size_t l = 1; l < K; ++l) face_of[l] = int(pc.roots[l - 1] / slice);
+  // Kimimaro's centroid sums are sequential float32 sums over the face in (pa outer, pb inner)
+  // order: exact integers while the total stays within 2^24; larger ones are redone that way
+  const double exact = 16777216.0;
+  std::vector<float> sum_a(K, 0.0f), sum_b(K, 0.0f);
+  std::vector<char> redo_face(faces.size(), 0);
+  for (size_t l = 1; l < K; ++l) {
+    sum_a[l] = float(st.sum_a[l]);
+    sum_b[l] = float(st.sum_b[l]);
+    if (double(st.sum_a[l]) > exact || double(st.sum_b[l]) > exact) redo_face[face_of[l]] = 1;
+  }
+  for (size_t fi = 0; fi < faces.size(); ++fi) {
+    if (!redo_face[fi]) continue;
+    const Face &f = faces[fi];
+    const std::vector<uint32_t> lab = stack_ids.download(size_t(slice), size_t(slice) * fi);
+    std::vector<float> sa(K, 0.0f), sb(K, 0.0f);
+    for (int pa = 0; pa < f.fx(); ++pa)
+      for (int pb = 0; pb < f.fy(); ++pb) {
+        const uint32_t l = lab[size_t(pb) + size_t(W) * pa];
+        if (!l) continue;
+        sa[l] += float(pa);
+        sb[l] += float(pb);
+      }
+    for (size_t l = 1; l < K; ++l)
+      if (face_of[l] == int(fi)) { sum_a[l] = sa[l]; sum_b[l] = sb[l]; }
+  }
+  // per component the pick: among its pixels at the largest distance, the least tie keys, the
+  // first in (pb outer, pa inner) order among equals
+  std::vector<int64_t> pick(K, -1);
+  std::vector<std::array<float, 4>> best(K);
+  std::vector<float> cx(K, 0.0f), cy(K, 0.0f);
+  for (size_t l = 1; l < K; ++l) {
+    if (!st.count[l]) continue;
+    const Face &f = faces[face_of[l]];
+    const float wx = aniso[f.a], wy = aniso[f.b];
+    float px = (wx * sum_a[l]) / float(st.count[l]), py = (wy * sum_b[l]) / float(st.count[l]);
+    if (px - (wx * float(f.fx())) / 2.0f < 0) px = px + wx;
+    if (py - (wy * float(f.fy())) / 2.0f < 0) py = py + wy;
+    cx[l] = float(int(px / wx));
+    cy[l] = float(int(py / wy));
+  }
+  const size_t ncand = st.candidates.size() / 3;
+  std::vector<size_t> cands(ncand);
+  for (size_t j = 0; j < ncand; ++j) cands[j] = j;
+  auto flat = [&](size_t j) {
+    const int l = st.candidates[3 * j];
+    return int64_t(st.candidates[3 * j + 1]) + int64_t(faces[face_of[l]].fx()) * st.candidates[3 * j + 2];
+  };
+  std::sort(cands.begin(), cands.end(), [&](size_t u, size_t w) {
+    const int lu = st.candidates[3 * u], lw = st.candidates[3 * w];
+    return lu != lw ? lu < lw : flat(u) < flat(w);
+  });
+  for (size_t j : cands) {
+    const int l = st.candidates[3 * j];
+    const Face &f = faces[face_of[l]];
+    const auto key = tie_keys(st.candidates[3 * j + 1], st.candidates[3 * j + 2], cx[l], cy[l], f.fx(), f.fy(),
+                              aniso[f.a], aniso[f.b]);
+    if (pick[l] < 0 || key < best[l]) { best[l] = key; pick[l] = flat(j); }
+  }
   // per volume and component id, the picks in the reference's face order (each volume's faces
-  // come in that order in the stack)
+  // come in that order in the stack), within a face by first pixel with a positive distance
+  std::vector<std::vector<size_t>> by_face(faces.size());
+  for (size_t l = 1; l < K; ++l)
+    if (pick[l] >= 0) by_face[face_of[l]].push_back(l);
   std::vector<std::vector<TupleSet>> sets(volumes.size());
   for (size_t v = 0; v < volumes.size(); ++v) sets[v].resize(size_t(volumes[v].count) + 1);
   for (size_t fi = 0; fi < faces.size(); ++fi) {
+    auto &order = by_face[fi];
+    if (order.empty()) continue;
     const Face &f = faces[fi];
     const size_t v = size_t(fi % per_group) / 2;
-    const int a = f.a, b = f.b, c = f.c;
-    const int64_t fx = f.fx(), fy = f.fy();
-    const uint32_t *lab = labs.data() + f.packed;
-    const float *dd = dds.data() + f.packed;
-    // the face's component ids form one contiguous range (ids follow the stack's flat order)
-    uint32_t lo = UINT32_MAX, hi = 0;
-    for (int64_t i = 0; i < fx * fy; ++i)
-      if (lab[i]) { lo = std::min(lo, lab[i]); hi = std::max(hi, lab[i]); }
-    if (hi == 0) continue;
-    const size_t k = size_t(hi - lo) + 1;
-    std::vector<float> maxdist(k, 0.0f), sumx(k, 0.0f), sumy(k, 0.0f);
-    std::vector<uint32_t> sizes(k, 0);
-    std::vector<int64_t> first(k, std::numeric_limits<int64_t>::max()), pick(k, -1);
-    // Kimimaro's sequential float32 centroid sums, x outer
-    for (int64_t x = 0; x < fx; ++x)
-      for (int64_t y = 0; y < fy; ++y) {
-        const size_t i = size_t(y + fy * x);
-        if (!lab[i]) continue;
-        const size_t l = lab[i] - lo;
-        sumx[l] += float(x);
-        sumy[l] += float(y);
-        ++sizes[l];
-        if (dd[i] > 0) { maxdist[l] = std::max(maxdist[l], dd[i]); first[l] = std::min(first[l], x + fx * y); }
-      }
-    const float wx = aniso[a], wy = aniso[b];
-    std::vector<float> cx(k, 0.0f), cy(k, 0.0f);
-    for (size_t l = 0; l < k; ++l)
-      if (sizes[l]) {
-        float px = (wx * sumx[l]) / float(sizes[l]), py = (wy * sumy[l]) / float(sizes[l]);
-        if (px - (wx * float(fx)) / 2.0f < 0) px = px + wx;
-        if (py - (wy * float(fy)) / 2.0f < 0) py = py + wy;
-        cx[l] = float(int(px / wx));
-        cy[l] = float(int(py / wy));
-      }
-    std::vector<std::array<float, 4>> best(k);
-    for (int64_t y = 0; y < fy; ++y)
-      for (int64_t x = 0; x < fx; ++x) {
-        const size_t i = size_t(y + fy * x);
-        if (!lab[i]) continue;
-        const size_t l = lab[i] - lo;
-        if (dd[i] == 0 || dd[i] != maxdist[l]) continue;
-        const auto key = tie_keys(x, y, cx[l], cy[l], fx, fy, wx, wy);
-        if (pick[l] < 0 || key < best[l]) { best[l] = key; pick[l] = x + fx * y; }
-      }
-    std::vector<size_t> order;
-    for (size_t l = 0; l < k; ++l)
-      if (pick[l] >= 0) order.push_back(l);
-    std::sort(order.begin(), order.end(), [&](size_t u, size_t w) { return first[u] < first[w]; });
+    std::sort(order.begin(), order.end(), [&](size_t u, size_t w) { return st.first[u] < st.first[w]; });
     for (size_t l : order) {
       Point p{};
-      p[a] = pick[l] % fx;
-      p[b] = pick[l] / fx;
-      p[c] = f.fixed;
-      sets[v].at(size_t(pc.mapping[lo + l])).add(p);
+      p[f.a] = pick[l] % f.fx();
+      p[f.b] = pick[l] / f.fx();
+      p[f.c] = f.fixed;
+      sets[v].at(size_t(pc.mapping[l])).add(p);
     }
   }
   for (size_t v = 0; v < volumes.size(); ++v)

@@ -69,16 +69,24 @@ struct Face {
   long long offset;
   VolumeDims d;
   int a, b, c, fixed;
-  long long packed;  // where the face starts in a packed buffer (pixel pb + fy * pa)
   int fx() const { return a == 0 ? d.sx : a == 1 ? d.sy : d.sz; }
   int fy() const { return b == 0 ? d.sx : b == 1 ? d.sy : d.sz; }
 };
 // Every face into its own z-slice of a (W, H, faces) stack: stack[pb + W * (pa + H * f)], zero
 // beyond the face's (fy, fx) corner.
 void extract_faces(Context &ctx, const uint32_t *ids, const std::vector<Face> &faces, int W, int H, uint32_t *stack);
-// The faces' pixels of two stack fields, packed face by face (pixel pb + fy * pa at face.packed).
-void pack_faces(Context &ctx, const uint32_t *stack_ids, const float *stack_dist, const std::vector<Face> &faces,
-                int W, int H, uint32_t *ids_out, float *dist_out);
+
+// Per component of a face stack (entry 0 unused): pixel count, sums of pa and pb, the largest
+// positive distance as float bits (0: none), the first pixel pa + fx * pb with a positive
+// distance (all ones: none), and every pixel at its component's largest positive distance as
+// (component, pa, pb) triples.
+struct FaceStats {
+  std::vector<unsigned long long> count, sum_a, sum_b, first;
+  std::vector<unsigned> max_bits;
+  std::vector<int> candidates;
+};
+FaceStats face_stats(Context &ctx, const uint32_t *stack_ids, const float *stack_dist, const std::vector<Face> &faces,
+                     int W, int H, int64_t components);
 
 // ---- border targets (borders.cpp) ----
 using Point = std::array<int64_t, 3>;

@@ -69,7 +69,7 @@ __global__ void fill_kernel(float *p, long long n, float v) {
 }
 
 struct FaceDesc {
-  long long offset, packed;
+  long long offset;
   int sx, sy, sz, a, b, c, fixed;
 };
 
@@ -91,8 +91,12 @@ __global__ void faces_kernel(const uint32_t *__restrict__ ids, const FaceDesc *f
   stack[i + (long long)W * H * blockIdx.y] = v;
 }
 
-__global__ void pack_kernel(const uint32_t *__restrict__ sids, const float *__restrict__ sdist, const FaceDesc *faces,
-                            int W, int H, uint32_t *ids, float *dist) {
+// Per face component (ids of a face stack): pixel count, sums of the face coordinates pa and pb,
+// the largest positive distance (float bits) and the first pixel (pa + fx * pb) with one.
+__global__ void face_stats_kernel(const uint32_t *__restrict__ sids, const float *__restrict__ sdist,
+                                  const FaceDesc *faces, int W, int H, unsigned long long *count,
+                                  unsigned long long *sum_a, unsigned long long *sum_b, unsigned *max_bits,
+                                  unsigned long long *first) {
   const FaceDesc f = faces[blockIdx.y];
   const int shape[3] = {f.sx, f.sy, f.sz};
   const int fx = shape[f.a], fy = shape[f.b];
@@ -100,13 +104,40 @@ __global__ void pack_kernel(const uint32_t *__restrict__ sids, const float *__re
   if (i >= (long long)fx * fy) return;
   const int pb = int(i % fy), pa = int(i / fy);
   const long long src = pb + (long long)W * (pa + (long long)H * blockIdx.y);
-  ids[f.packed + i] = sids[src];
-  dist[f.packed + i] = sdist[src];
+  const uint32_t l = sids[src];
+  if (!l) return;
+  atomicAdd(count + l, 1ull);
+  atomicAdd(sum_a + l, (unsigned long long)pa);
+  atomicAdd(sum_b + l, (unsigned long long)pb);
+  const float d = sdist[src];
+  if (d > 0.0f) {
+    atomicMax(max_bits + l, __float_as_uint(d));
+    atomicMin(first + l, (unsigned long long)(pa + (long long)fx * pb));
+  }
+}
+
+// The pixels at their component's largest positive distance: (component, pa, pb) triples.
+__global__ void face_candidates_kernel(const uint32_t *__restrict__ sids, const float *__restrict__ sdist,
+                                       const FaceDesc *faces, int W, int H, const unsigned *max_bits, int *n,
+                                       int *out, long long capacity) {
+  const FaceDesc f = faces[blockIdx.y];
+  const int shape[3] = {f.sx, f.sy, f.sz};
+  const int fx = shape[f.a], fy = shape[f.b];
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)fx * fy) return;
+  const int pb = int(i % fy), pa = int(i / fy);
+  const long long src = pb + (long long)W * (pa + (long long)H * blockIdx.y);
+  const uint32_t l = sids[src];
+  if (!l) return;
+  const float d = sdist[src];
+  if (!(d > 0.0f) || __float_as_uint(d) != max_bits[l]) return;
+  const int slot = atomicAdd(n, 1);
+  if (slot < capacity) { out[3LL * slot] = int(l); out[3LL * slot + 1] = pa; out[3LL * slot + 2] = pb; }
 }
 
 Buffer<FaceDesc> face_descs(Context &ctx, const std::vector<Face> &faces) {
   std::vector<FaceDesc> h;
-  for (const auto &f : faces) h.push_back({f.offset, f.packed, f.d.sx, f.d.sy, f.d.sz, f.a, f.b, f.c, f.fixed});
+  for (const auto &f : faces) h.push_back({f.offset, f.d.sx, f.d.sy, f.d.sz, f.a, f.b, f.c, f.fixed});
   return to_device(ctx, h);
 }
 
@@ -162,15 +193,38 @@ void extract_faces(Context &ctx, const uint32_t *ids, const std::vector<Face> &f
   BK_CUDA(cudaGetLastError());
 }
 
-void pack_faces(Context &ctx, const uint32_t *stack_ids, const float *stack_dist, const std::vector<Face> &faces,
-                int W, int H, uint32_t *ids_out, float *dist_out) {
-  if (faces.empty()) return;
+FaceStats face_stats(Context &ctx, const uint32_t *stack_ids, const float *stack_dist, const std::vector<Face> &faces,
+                     int W, int H, int64_t components) {
+  FaceStats out;
+  if (faces.empty()) return out;
+  cudaStream_t s = ctx.stream();
   Buffer<FaceDesc> desc = face_descs(ctx, faces);
-  long long most = 0;
-  for (const auto &f : faces) most = std::max(most, (long long)f.fx() * f.fy());
-  pack_kernel<<<dim3(blocks_for(most), unsigned(faces.size())), 256, 0, ctx.stream()>>>(
-      stack_ids, stack_dist, desc.data(), W, H, ids_out, dist_out); ++ctx.launches;
+  const size_t k = size_t(components) + 1;
+  Buffer<unsigned long long> count(ctx, k), sum_a(ctx, k), sum_b(ctx, k), first(ctx, k);
+  Buffer<unsigned> max_bits(ctx, k);
+  count.zero(); sum_a.zero(); sum_b.zero(); max_bits.zero();
+  first.fill_bytes(0xFF);
+  long long most = 0, pixels = 0;
+  for (const auto &f : faces) {
+    most = std::max(most, (long long)f.fx() * f.fy());
+    pixels += (long long)f.fx() * f.fy();
+  }
+  const dim3 grid(blocks_for(most), unsigned(faces.size()));
+  face_stats_kernel<<<grid, 256, 0, s>>>(stack_ids, stack_dist, desc.data(), W, H, count.data(), sum_a.data(),
+                                         sum_b.data(), max_bits.data(), first.data()); ++ctx.launches;
+  Buffer<int> n(ctx, 1), cand(ctx, 3 * std::max(pixels, 1LL));
+  n.zero();
+  face_candidates_kernel<<<grid, 256, 0, s>>>(stack_ids, stack_dist, desc.data(), W, H, max_bits.data(), n.data(),
+                                              cand.data(), pixels); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
+  out.count = count.download();
+  out.sum_a = sum_a.download();
+  out.sum_b = sum_b.download();
+  out.first = first.download();
+  out.max_bits = max_bits.download();
+  const int got = n.download(1)[0];
+  out.candidates = cand.download(3 * size_t(std::min<long long>(got, pixels)));
+  return out;
 }
 
 }  // namespace bk
