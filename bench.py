@@ -41,6 +41,10 @@ CONFIGS = {
     "serve": dict(workload="Poisson request stream at 50/200/800 req/s (seed 4), volume edges log-uniform 32-384, "
                        "1 tube per 64^3 voxels, uint32/uint64 50/50, 80 GB admission cap",
                   seed=4, kind="serve", rates=(50, 200, 800), requests=300, anisotropy=(16, 16, 40)),
+    "chunks1024": dict(workload="dense segmentation 1024x1024x256 uint32, 3000 Voronoi seeds cut by tubes r=3-10 "
+                            "(seed 3): whole in-core, and as 512x512x256 chunks with 64-voxel overlap in one batch",
+                       shape=(1024, 1024, 256), seeds=3000, seed=3, kind="chunks", dtype="uint32",
+                       anisotropy=(16, 16, 40), chunk=(512, 512, 256), overlap=64),
     "tubes128": dict(workload="128x128x128 uint32, 20 random-walk tubes r=2-6 (seed 0)", shape=(128, 128, 128),
                      objects=20, seed=0, kind="tubes", dtype="uint32", anisotropy=(16, 16, 40)),
 }
@@ -55,9 +59,36 @@ def make_volume(cfg, rank=0):
     if cfg["kind"] == "batch":
         return synthetic.uneven_batch(seed=cfg["seed"] + rank)
 
-    if cfg["kind"] == "dense":
+    if cfg["kind"] in ("dense", "chunks"):
         return synthetic.dense_volume(cfg["shape"], seeds=cfg["seeds"], seed=cfg["seed"] + rank, dtype=np.dtype(cfg["dtype"]))
     return synthetic.tube_volume(cfg["shape"], objects=cfg["objects"], seed=cfg["seed"] + rank, dtype=np.dtype(cfg["dtype"]))
+
+
+def stage_roofline(stage, peak):
+    """Per stage: CUDA-event ms, algorithmic bytes (the per-unit figures of the path's measurement
+    plan: N voxels, F object voxels, b input label bytes, c component-id bytes), GB/s and the
+    fraction of the measured HBM peak."""
+    N, F = stage.get("voxels", 0), stage.get("foreground", 0)
+    c = stage.get("label_bytes", 2)
+    nb = stage.get("input_bytes", 0)
+    alg = {
+        "ccl": nb + N * c,                               # read labels, write ids
+        "edt": N * (3 * c + 20),                         # x: N(c+4), y and z: N(c+8) each
+        "mask": N * (4 + 4),                             # ids in, mask out
+        "dbf_max": N * (4 + c),                          # argmax
+        "prepare": 2 * F * (c + 8) + N * (12 + c),       # two DAF floods and the PDRF
+        "order": F * (4 + c) + 4 * F,                    # target-order keys in, order out
+        "trace": stage.get("railroad_settled", 0) * (12 + c) + stage.get("invalidated", 0) * (13 + c),
+        "assembly": stage.get("path_vertices", 0) * 8 + stage.get("vertices", 0) * 16 + stage.get("edges", 0) * 8,
+    }
+    out = {}
+    for name, b in alg.items():
+        ms = stage.get("ms_" + name)
+        if not ms:
+            continue
+        gbs = b / (ms / 1e3) / 1e9
+        out[name] = {"ms": round(ms, 3), "algorithmic_bytes": int(b), "gbs": round(gbs, 2), "frac": round(gbs / peak, 5)}
+    return out
 
 
 def peaks():
@@ -266,6 +297,7 @@ def run_batch(args, cfg):
                    "parallelism": f"volume shards x{world} (longest first), results gathered to rank 0",
                    "l2": "inputs larger than L2 (0.75 GB of labels per step)"},
         "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
+        "stages_roofline": stage_roofline(stage, peaks()[0]),
         "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
         "e2e": {"value": skeletons / (e2e_ms / 1e3), "unit": "skeletons/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(sum(volumes[i].nbytes for i in mine)),
@@ -277,6 +309,60 @@ def run_batch(args, cfg):
     print(json.dumps(out_line))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def run_chunks(args, cfg):
+    """The large volume: skeletonized whole (in-core) and as overlapping chunks in one batch, each
+    with its per-stage HBM figures. The chunks' skeletons are not merged (merging parts is a
+    post-processing step)."""
+    import torch
+
+    import brook_b200
+    from brook_b200 import _native, sharding
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    volume = make_volume(cfg)
+    dev = torch.from_numpy(np.ascontiguousarray(volume.transpose(2, 1, 0))).cuda(local).permute(2, 1, 0)
+    chunks = [dev[c] for c in sharding.iter_chunks(volume.shape, cfg["chunk"], cfg["overlap"])]
+    opts = dict(teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST, device=local)
+    peak, source = peaks()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stage = {}
+        start.record()
+        for _ in range(args.steps):
+            out = fn()
+            for k, v in _native.stats(local).items():
+                stage[k] = stage.get(k, 0.0) + v
+        end.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(end) / args.steps, out, {k: v / args.steps for k, v in stage.items()}
+
+    with ClockSampler(local) as clocks:
+        ms, whole, stage = timed(lambda: brook_b200.skeletonize(dev, output="packed", **opts))
+        cms, parts, cstage = timed(lambda: brook_b200.skeletonize_batch(chunks, output="packed", **opts))
+    voxels = int(volume.size)
+    chunk_voxels = int(sum(c.numel() for c in chunks))
+    print(json.dumps({
+        "metric": METRIC, "value": voxels / (ms / 1e3), "unit": "voxels/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32/f32", "data": "synthetic", "skeletons_per_s": len(whole) / (ms / 1e3),
+        "config": {"workload": cfg["workload"], "voxels": voxels, "anisotropy": cfg["anisotropy"], "teasar": PARAMS,
+                   "dust_threshold": DUST, "chunks": len(chunks), "chunk": cfg["chunk"], "overlap": cfg["overlap"],
+                   "l2": "labels of 1 GiB per step, larger than L2 (126 MB)"},
+        "stages_roofline": stage_roofline(stage, peak), "peak_gbs": peak, "peak_source": source,
+        "chunked": {"ms_per_step": cms, "voxels_per_s": chunk_voxels / (cms / 1e3), "voxels": chunk_voxels,
+                    "skeletons": int(len(parts.labels)), "stages_roofline": stage_roofline(cstage, peak)},
+        "clocks": clocks.summary(),
+    }))
 
 
 def run_serve(args, cfg):
@@ -415,6 +501,7 @@ def run_ours(args, cfg):
                    "parallelism": f"replicas x{world}", "l2": f"labels of {volume.nbytes / 2**20:.0f} MiB per step, "
                          + ("larger than L2 (126 MB)" if volume.nbytes > 126e6 else "smaller than L2: not flushed")},
         "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
+        "stages_roofline": stage_roofline(stage, peaks()[0]),
         "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
         "work": {k: stage.get(k) for k in ("paths", "railroad_settled", "railroad_touched", "invalidated", "foreground")},
         "roofline": {"kernel": "trace_kernel", "stage_dominant": dominant, "bound": "hbm", "achieved": achieved,
@@ -448,6 +535,8 @@ def main():
         run_batch(args, cfg)
     elif cfg["kind"] == "serve":
         run_serve(args, cfg)
+    elif cfg["kind"] == "chunks":
+        run_chunks(args, cfg)
     else:
         run_ours(args, cfg)
 

@@ -532,6 +532,14 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   long long kmax = 0;
   for (const auto &st : vs) kmax = std::max<long long>(kmax, st.cc.count);
   ctx.stats["label_bytes"] = kmax <= 0xFF ? 1 : kmax <= 0xFFFF ? 2 : kmax <= 0xFFFFFFFFLL ? 4 : 8;
+  double input_bytes = 0;
+  for (size_t v = 0; v < vs.size(); ++v)
+    if (volumes[v].d.n() > 0 && double(volumes[v].d.n()) > opt.dust)  // the volumes the call read
+      input_bytes += double(volumes[v].d.n()) * double(label_bytes(volumes[v].dtype));
+  ctx.stats["input_bytes"] = input_bytes;
+  ctx.stats["path_vertices"] = double(vt);
+  ctx.stats["vertices"] = double(V);
+  ctx.stats["edges"] = double(E);
   return results;
 }
 

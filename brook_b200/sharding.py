@@ -30,6 +30,20 @@ def partition(work, world):
     return [sorted(s) for s in shares]
 
 
+def iter_chunks(shape, chunk_shape, overlap=1):
+    """Slices that tile a 3D `shape` with chunks of `chunk_shape` overlapping by `overlap` voxels
+    (the reference's iter_chunks, src/brook/_pool.py:341-350): starts every chunk - overlap voxels
+    along each axis, the last chunk clipped at the edge."""
+    shape, chunk_shape = tuple(map(int, shape)), tuple(map(int, chunk_shape))
+    if len(shape) != 3 or len(chunk_shape) != 3:
+        raise ValueError("shape and chunk_shape must have three entries")
+    starts = [range(0, max(s - overlap, 1), max(c - overlap, 1)) for s, c in zip(shape, chunk_shape)]
+    for x in starts[0]:
+        for y in starts[1]:
+            for z in starts[2]:
+                yield tuple(slice(a, min(a + c, s)) for a, c, s in zip((x, y, z), chunk_shape, shape))
+
+
 def skeletonize_batch_sharded(samples, rank=None, world=None, dst=0, group=None, device=None, **options):
     """The batch `samples` (every rank passes the same list, or at least the same shapes) split over
     the ranks of the default process group; returns BatchedSkeletons for the whole batch on rank
@@ -63,4 +77,4 @@ def skeletonize_batch_sharded(samples, rank=None, world=None, dst=0, group=None,
     return _batch.BatchedSkeletons.concatenate(ordered, anisotropy)
 
 
-__all__ = ["partition", "skeletonize_batch_sharded"]
+__all__ = ["partition", "iter_chunks", "skeletonize_batch_sharded"]

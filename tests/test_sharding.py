@@ -81,3 +81,14 @@ def test_two_ranks_over_gloo_gather_in_batch_order(tmp_path):
     assert set(done[0]).isdisjoint(done[1])
     assert np.load(tmp_path / "labels.npy").tolist() == [11, 12, 13, 14, 15]
     assert np.load(tmp_path / "sample.npy").tolist() == [0, 1, 2, 3, 4]
+
+
+def test_iter_chunks_tiles_with_overlap():
+    chunks = list(sharding.iter_chunks((1024, 1024, 256), (512, 512, 256), overlap=64))
+    assert len(chunks) == 9
+    assert chunks[0] == (slice(0, 512), slice(0, 512), slice(0, 256))
+    assert chunks[-1] == (slice(896, 1024), slice(896, 1024), slice(0, 256))
+    covered = np.zeros((1024, 1024), bool)
+    for c in chunks:
+        covered[c[0], c[1]] = True
+    assert covered.all()
