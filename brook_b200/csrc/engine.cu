@@ -193,8 +193,10 @@ __device__ bool flood_geometric(const EngineArgs &a, Shared &sh, Shared *L, floa
     if (G::first()) L->cnt[(r + 2) % 3] = 0;
     for (int i = G::tid(); i < nc; i += G::threads()) {
       const int u = __ldcg(cur + i);
-      const unsigned was = atomicAnd(a.flags + u, ~kNearQueued);
-      const float du = __ldcg(d + u + (was >> 30));
+      // step A runs between barriers, with no relaxation in flight: the flag clear (a reduction,
+      // nothing to wait for) and the distance read need no order between them
+      atomicAnd(a.flags + u, ~kNearQueued);
+      const float du = __ldcg(d + u);
       wide[i] = (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u];
     }
     G::sync();
@@ -365,9 +367,9 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
       const float T = vload(&L->T);
       for (int i = G::tid(); i < nc; i += G::threads()) {
         const int u = __ldcg(cur + i);
-        const unsigned was = atomicAnd(a.flags + u, ~kNearQueued);
+        atomicAnd(a.flags + u, ~kNearQueued);  // no relaxation in flight during step A
         const float fu = a.pdrf[u];
-        const float du = __ldcg(a.dist + u + (was >> 30));
+        const float du = __ldcg(a.dist + u);
         const unsigned long long rb = vload(&sh.rb);
         const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
         const bool expand = fu != 0.0f && du <= Tb;
