@@ -780,9 +780,17 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
 }
 
 template <int C>
+// The first a.lone_first clusters start on the small objects (each CTA alone, largest first) and
+// then join the large ones; the others take the large objects first. So the longest lone-CTA
+// objects run beside the clusters' objects from the start instead of after them.
 __global__ void __launch_bounds__(kEngineThreads, kEngineCtasPerSm) trace_kernel(EngineArgs a) {
-  trace_loop<C>(a, true);
-  trace_loop<1>(a, false);
+  if (int(blockIdx.x) / C < a.lone_first) {
+    trace_loop<1>(a, false);
+    trace_loop<C>(a, true);
+  } else {
+    trace_loop<C>(a, true);
+    trace_loop<1>(a, false);
+  }
 }
 
 cudaLaunchConfig_t cluster_config(int clusters, int ctas, cudaStream_t stream, cudaLaunchAttribute *attr) {
@@ -818,7 +826,7 @@ int resident_clusters(const void *kernel, int ctas, cudaStream_t stream) {
 }
 
 // As many clusters as are resident at once (no more than the work needs).
-void launch(const void *kernel, int ctas, const EngineArgs &a, int nbig, cudaStream_t stream) {
+void launch(const void *kernel, int ctas, const EngineArgs &a, int nbig, cudaStream_t stream, int lone_percent = 0) {
   EngineArgs args = a;
   args.nbig = nbig;
   void *kargs[] = {&args};
@@ -826,6 +834,7 @@ void launch(const void *kernel, int ctas, const EngineArgs &a, int nbig, cudaStr
   const int cap = resident_clusters(kernel, ctas, stream);
   const long long need = nbig + (a.nobj - nbig + ctas - 1) / ctas;
   const int clusters = int(std::max(1LL, std::min<long long>(cap, need)));
+  args.lone_first = nbig < a.nobj ? clusters * lone_percent / 100 : 0;
   cudaLaunchConfig_t config = cluster_config(clusters, ctas, stream, attr);
   BK_CUDA(cudaLaunchKernelExC(&config, kernel, kargs));
 }
@@ -861,9 +870,9 @@ void launch_prepare(const EngineArgs &a, int nbig, int ctas, cudaStream_t stream
   else launch((const void *)prepare_kernel<kClusterCtas>, kClusterCtas, a, nbig, stream);
 }
 
-void launch_trace(const EngineArgs &a, int nbig, int ctas, cudaStream_t stream) {
-  if (ctas == kWideClusterCtas) launch((const void *)trace_kernel<kWideClusterCtas>, ctas, a, nbig, stream);
-  else launch((const void *)trace_kernel<kClusterCtas>, kClusterCtas, a, nbig, stream);
+void launch_trace(const EngineArgs &a, int nbig, int ctas, int lone_percent, cudaStream_t stream) {
+  if (ctas == kWideClusterCtas) launch((const void *)trace_kernel<kWideClusterCtas>, ctas, a, nbig, stream, lone_percent);
+  else launch((const void *)trace_kernel<kClusterCtas>, kClusterCtas, a, nbig, stream, lone_percent);
 }
 
 }  // namespace bk

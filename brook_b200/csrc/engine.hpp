@@ -48,6 +48,7 @@ struct EngineArgs {
   const int *vox;        // voxels of every object, ascending flat index
   const int *schedule;   // processing order (object indices): large objects first, then the rest
   int nbig;              // schedule[0, nbig) run on clusters (set by launch_prepare / launch_trace)
+  int lone_first;        // trace: clusters [0, lone_first) take the small objects first
   int *queue;            // two work counters (large, small), both 0 at launch
   int *status;           // per object
   int *lists;            // 5 lists of F ints: list w of object o at lists + w * F + obj_begin[o]
@@ -103,6 +104,8 @@ long long trace_cluster_voxels(long long foreground);
 // One pass of the engine: clusters take schedule[0, nbig) (large objects, largest first), then
 // every CTA takes schedule[nbig, nobj) alone. queue[0] and queue[1] must be zero.
 void launch_prepare(const EngineArgs &a, int nbig, int cluster_ctas, cudaStream_t stream);
-void launch_trace(const EngineArgs &a, int nbig, int cluster_ctas, cudaStream_t stream);
+// lone_percent: the share of clusters (percent) whose CTAs take small objects first.
+void launch_trace(const EngineArgs &a, int nbig, int cluster_ctas, int lone_percent, cudaStream_t stream);
+constexpr int kLoneFirstPercent = 15;
 
 }  // namespace bk

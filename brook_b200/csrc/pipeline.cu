@@ -370,7 +370,9 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.order = order.data();
   BK_CUDA(cudaMemsetAsync(queue.data(), 0, 2 * sizeof(int), s));
   clock.mark("order");
-  launch_trace(a, nbig_trace, ctas, s);
+  int lone_percent = kLoneFirstPercent;
+  if (const char *e = std::getenv("BROOK_B200_LONE_FIRST_PERCENT")) lone_percent = std::atoi(e);  // tuning knob
+  launch_trace(a, nbig_trace, ctas, std::max(0, std::min(100, lone_percent)), s);
   ++ctx.launches;
   clock.mark("trace");
 
