@@ -186,15 +186,19 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
   Buffer<int> index(ctx, P), order(ctx, P);
   Buffer<float> radius(ctx, P);
   Buffer<unsigned char> first(ctx, P);
+  host_mark("allocate");
   occurrence_keys<<<npaths, 128, 0, s>>>(store, dbf, d_src.data(), d_len.data(), d_group.data(), d_volume.data(),
                                          d_occ.data(), d_aoff.data(), d_dims.data(), k, keys.data(), index.data(),
                                          radius.data(), first.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
+  host_mark("keys");
   size_t temp = 0;
   BK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, keys.data(), sorted.data(), index.data(), order.data(), (int)P,
                                           0, end_bit, s));
+  host_mark("sort_query");
   {
     Buffer<unsigned char> scratch(ctx, temp);
+    host_mark("sort_scratch");
     BK_CUDA(cub::DeviceRadixSort::SortPairs(scratch.data(), temp, keys.data(), sorted.data(), index.data(),
                                             order.data(), (int)P, 0, end_bit, s));
   }

@@ -522,6 +522,16 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     }
   clock.mark("assembly");
   clock.finish();
+  {
+    // the device memory pool after the call (bytes): reserved from the driver, and in use at the high-water mark
+    cudaMemPool_t pool;
+    BK_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx.device()));
+    uint64_t reserved = 0, high = 0;
+    BK_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    BK_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &high));
+    ctx.stats["pool_reserved_bytes"] = double(reserved);
+    ctx.stats["pool_used_high_bytes"] = double(high);
+  }
   const auto w = work.download();
   ctx.stats["paths"] = double(w[3]);
   ctx.stats["railroad_settled"] = double(w[0]);

@@ -27,24 +27,77 @@ Context::~Context() {
     int previous = -1;
     cudaGetDevice(&previous);
     cudaSetDevice(device_);
+    for (auto &entry : free_)
+      for (void *p : entry.second) cudaFreeAsync(p, stream_);
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
     if (previous >= 0) cudaSetDevice(previous);
   }
 }
 
+namespace {
+
+constexpr size_t kCacheCap = size_t(24) << 30;  // cached bytes kept per context at most
+
+size_t size_class(size_t bytes) {
+  if (bytes <= 256) return 256;
+  int top = 63 - __builtin_clzll((unsigned long long)(bytes - 1));
+  const size_t step = size_t(1) << (top >= 3 ? top - 3 : 0);  // 8 classes per power of two
+  return (bytes + step - 1) / step * step;
+}
+
+}  // namespace
+
 void *Context::allocate(size_t bytes) {
+  const size_t cls = size_class(bytes);
+  auto it = free_.find(cls);
+  if (it != free_.end() && !it->second.empty()) {
+    void *p = it->second.back();
+    it->second.pop_back();
+    cached_ -= cls;
+    return p;
+  }
   void *p = nullptr;
-  cudaError_t status = cudaMallocAsync(&p, bytes, stream_);
+  cudaError_t status = cudaMallocAsync(&p, cls, stream_);
   if (status != cudaSuccess) {
     cudaGetLastError();
-    throw CudaError(status, "cudaMallocAsync(" + std::to_string(bytes) + " bytes)");
+    trim();
+    status = cudaMallocAsync(&p, cls, stream_);
+    if (status != cudaSuccess) {
+      cudaGetLastError();
+      throw CudaError(status, "cudaMallocAsync(" + std::to_string(bytes) + " bytes)");
+    }
   }
+  class_of_[p] = cls;
   return p;
 }
 
 void Context::release(void *p) {
-  if (p) cudaFreeAsync(p, stream_);
+  if (!p) return;
+  auto it = class_of_.find(p);
+  if (it == class_of_.end()) {  // not ours: hand it back as it is
+    cudaFreeAsync(p, stream_);
+    return;
+  }
+  const size_t cls = it->second;
+  if (cached_ + cls > kCacheCap) {
+    class_of_.erase(it);
+    cudaFreeAsync(p, stream_);
+    return;
+  }
+  free_[cls].push_back(p);
+  cached_ += cls;
+}
+
+void Context::trim() {
+  for (auto &entry : free_)
+    for (void *p : entry.second) {
+      class_of_.erase(p);
+      cudaFreeAsync(p, stream_);
+    }
+  free_.clear();
+  cached_ = 0;
+  cudaStreamSynchronize(stream_);
 }
 
 }  // namespace bk

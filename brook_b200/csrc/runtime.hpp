@@ -55,8 +55,14 @@ class Context {
   cudaStream_t stream() const { return stream_; }
   int sm_count() const { return sm_count_; }
   void synchronize() const { BK_CUDA(cudaStreamSynchronize(stream_)); }
+  // Stream-ordered device memory with a per-context cache: a released block goes to a free list
+  // of its size class (8 classes per power of two) and the next allocation of that class reuses
+  // it, in the stream's order, without a driver call. Cached bytes beyond a cap are returned to
+  // the device's pool; when an allocation fails, every cached block is returned and it is tried
+  // once more.
   void *allocate(size_t bytes);
   void release(void *p);
+  void trim();  // returns every cached block to the device's pool
   std::mutex &mutex() { return mutex_; }
   // Per-call statistics: stage times (ms, CUDA events on this context's stream) and work counters.
   std::map<std::string, double> stats;
@@ -67,6 +73,9 @@ class Context {
   int device_ = 0, sm_count_ = 0;
   cudaStream_t stream_ = nullptr;
   std::mutex mutex_;
+  std::map<size_t, std::vector<void *>> free_;  // size class -> cached blocks
+  std::map<void *, size_t> class_of_;           // live and cached blocks -> size class
+  size_t cached_ = 0;
 };
 
 // Device storage that outlives the context that made it (plain cudaMalloc / cudaFree on its
