@@ -12,6 +12,8 @@
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.hpp"
 
@@ -87,9 +89,11 @@ __device__ __forceinline__ void tile_unite(int *par, int a, int b) {
   }
 }
 
-// grid (x tiles, y tiles, z tiles); parent of every voxel of the tile = its tile root (global).
+// grid (x tiles, y tiles, z tiles); parent of every voxel of the tile = its tile root, as an index
+// of the flat space the volume starts at `base` in; background: -1.
 template <class L>
-__global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__ labels, int *parent, Dims d, bool planar) {
+__global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__ labels, int *parent, Dims d, bool planar,
+                                                           long long base) {
   __shared__ L lab[kTileN];
   __shared__ int par[kTileN];
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z0 = blockIdx.z * kTileZ;
@@ -124,7 +128,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__
     const int r = tile_find(par, t);
     const int rx = r % kTileX, ry = (r / kTileX) % kTileY, rz = r / (kTileX * kTileY);
     const long long g = (x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz));
-    parent[g] = int((x0 + rx) + (long long)d.sx * ((y0 + ry) + (long long)d.sy * (z0 + rz)));
+    parent[base + g] = lab[t] == L(0) ? -1 : int(base + (x0 + rx) + (long long)d.sx * ((y0 + ry) + (long long)d.sy * (z0 + rz)));
   }
 }
 
@@ -132,7 +136,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__
 // faces, both y faces — dy = -1 comes with dz = +1 — and the high z face), the forward neighbours
 // in another tile.
 template <class L>
-__global__ void face_union(const L *labels, int *parent, Dims d, bool planar) {
+__global__ void face_union(const L *labels, int *parent, Dims d, bool planar, long long base) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n()) return;
   int x, y, z;
@@ -154,7 +158,7 @@ __global__ void face_union(const L *labels, int *parent, Dims d, bool planar) {
     const bool crosses = lx + dx < 0 || lx + dx >= kTileX || ly + dy >= kTileY || ly + dy < 0 || lz + dz >= kTileZ;
     if (!crosses) continue;
     if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
-    unite(parent, (int)i, (int)i + nbr_offset(k, d));
+    unite(parent, int(base + i), int(base + i) + nbr_offset(k, d));
   }
 }
 
@@ -162,6 +166,7 @@ __global__ void flatten(int *parent, long long n) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int p = parent[i];
+  if (p < 0) return;  // background
   while (true) {
     const int q = __ldcg(parent + p);
     if (q == p) break;
@@ -170,85 +175,125 @@ __global__ void flatten(int *parent, long long n) {
   parent[i] = p;
 }
 
-template <class L>
 struct RootFlag {
-  const L *labels;
   const int *parent;
-  __device__ int operator()(long long i) const { return labels[i] != 0 && parent[i] == (int)i; }
+  __device__ int operator()(long long i) const { return parent[i] == (int)i; }
 };
 
-// rank[n] = number of roots (the exclusive scan's total)
-template <class L>
-__global__ void count_roots(const L *labels, const int *parent, int *rank, long long n) {
-  rank[n] = rank[n - 1] + ((labels[n - 1] != 0 && parent[n - 1] == (int)(n - 1)) ? 1 : 0);
+// Each volume's first rank, and the total: bounds[v] = rank[offset_v], bounds[count] = the number
+// of roots in the whole space.
+__global__ void rank_bounds(const int *parent, const int *rank, const long long *offsets, int count, long long n,
+                            int *bounds) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < count) bounds[v] = rank[offsets[v]];
+  if (v == count) bounds[v] = rank[n - 1] + (parent[n - 1] == (int)(n - 1) ? 1 : 0);
 }
 
+// ids of one volume (local ids: rank - first + 1), and per root its local flat index and label.
 template <class L>
 __global__ void relabel(const L *labels, const int *parent, const int *rank, uint32_t *ids, long long *roots,
-                        long long *mapping, long long n) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+                        long long *mapping, long long n, long long base, int first) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const L lv = labels[i];
-  if (lv == 0) { ids[i] = 0; return; }
-  const int r = parent[i];
-  ids[i] = (uint32_t)rank[r] + 1u;
-  if (r == (int)i) {
-    roots[rank[i]] = i;
-    mapping[rank[i] + 1] = (long long)lv;
+  const int r = parent[base + i];
+  if (r < 0) { ids[i] = 0; return; }
+  ids[i] = uint32_t(rank[r] - first + 1);
+  if (r == int(base + i)) {
+    roots[rank[r]] = i;
+    mapping[rank[r] + 1] = (long long)labels[i];
   }
 }
 
-template <class L>
-ComponentsResult run(Context &ctx, const L *labels, VolumeDims vd, uint32_t *ids, bool planar) {
-  const long long n = vd.n();
-  const Dims d{vd.sx, vd.sy, vd.sz};
-  ComponentsResult out;
-  Buffer<int> parent(ctx, n), rank(ctx, n + 1);
-  cudaStream_t s = ctx.stream();
-  const dim3 tiles((d.sx + kTileX - 1) / kTileX, (d.sy + kTileY - 1) / kTileY, (d.sz + kTileZ - 1) / kTileZ);
-  if (tiles.y > 65535 || tiles.z > 65535) throw std::invalid_argument("volume too large for the tiled union");
-  tile_union<L><<<tiles, kTileThreads, 0, s>>>(labels, parent.data(), d, planar); ++ctx.launches;
-  face_union<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), d, planar); ++ctx.launches;
-  flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
-  BK_CUDA(cudaGetLastError());
-  thrust::counting_iterator<long long> index(0);
-  thrust::transform_iterator<RootFlag<L>, thrust::counting_iterator<long long>, int> flags(index, RootFlag<L>{labels, parent.data()});
-  size_t temp = 0;
-  BK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, flags, rank.data(), n, s));
-  Buffer<unsigned char> scratch(ctx, temp);
-  BK_CUDA(cub::DeviceScan::ExclusiveSum(scratch.data(), temp, flags, rank.data(), n, s));
-  count_roots<L><<<1, 1, 0, s>>>(labels, parent.data(), rank.data(), n); ++ctx.launches;
-  BK_CUDA(cudaGetLastError());
-  out.count = rank.download(1, n)[0];
-  Buffer<long long> roots(ctx, out.count + 1), mapping(ctx, out.count + 1);
-  mapping.zero();
-  relabel<L><<<blocks_for(n), 256, 0, s>>>(labels, parent.data(), rank.data(), ids, roots.data(),
-                                          mapping.data(), n); ++ctx.launches;
-  BK_CUDA(cudaGetLastError());
-  auto r = roots.download(out.count);
-  auto m = mapping.download(out.count + 1);
-  out.roots.assign(r.begin(), r.end());
-  out.mapping.assign(m.begin(), m.end());
-  return out;
+template <class F>
+void for_dtype(int dtype, const void *labels, F &&f) {
+  switch (dtype) {
+    case U8: f(static_cast<const uint8_t *>(labels)); break;
+    case U16: f(static_cast<const uint16_t *>(labels)); break;
+    case U32: f(static_cast<const uint32_t *>(labels)); break;
+    case U64: f(static_cast<const uint64_t *>(labels)); break;
+    case I8: f(static_cast<const int8_t *>(labels)); break;
+    case I16: f(static_cast<const int16_t *>(labels)); break;
+    case I32: f(static_cast<const int32_t *>(labels)); break;
+    case I64: f(static_cast<const int64_t *>(labels)); break;
+    default: throw std::invalid_argument("connected components require integer labels");
+  }
 }
 
 }  // namespace
 
+std::vector<ComponentsResult> connected_components(Context &ctx, const std::vector<CcVolume> &volumes, uint32_t *ids,
+                                                   bool planar) {
+  std::vector<ComponentsResult> out(volumes.size());
+  long long n = 0;
+  for (const auto &v : volumes) {
+    if (v.offset != n) throw std::invalid_argument("component volumes must be contiguous in their flat space");
+    n += v.d.n();
+  }
+  if (n >= (1LL << 31) - 1) throw std::invalid_argument("volumes of 2^31 voxels or more are not supported");
+  for (auto &r : out) r.mapping.assign(1, 0);
+  if (n <= 0) return out;
+  cudaStream_t s = ctx.stream();
+  Buffer<int> parent(ctx, n), rank(ctx, n);
+  // union within each volume, then one flatten and one scan over all of them
+  for (const auto &v : volumes) {
+    if (!v.d.n()) continue;
+    const Dims d{v.d.sx, v.d.sy, v.d.sz};
+    const dim3 tiles((d.sx + kTileX - 1) / kTileX, (d.sy + kTileY - 1) / kTileY, (d.sz + kTileZ - 1) / kTileZ);
+    if (tiles.y > 65535 || tiles.z > 65535) throw std::invalid_argument("volume too large for the tiled union");
+    for_dtype(v.dtype, v.labels, [&](auto labels) {
+      using L = std::remove_const_t<std::remove_pointer_t<decltype(labels)>>;
+      tile_union<L><<<tiles, kTileThreads, 0, s>>>(labels, parent.data(), d, planar, v.offset); ++ctx.launches;
+      face_union<L><<<blocks_for(v.d.n()), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset); ++ctx.launches;
+    });
+  }
+  flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
+  BK_CUDA(cudaGetLastError());
+  thrust::counting_iterator<long long> index(0);
+  thrust::transform_iterator<RootFlag, thrust::counting_iterator<long long>, int> flags(index, RootFlag{parent.data()});
+  size_t temp = 0;
+  BK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, flags, rank.data(), n, s));
+  {
+    Buffer<unsigned char> scratch(ctx, temp);
+    BK_CUDA(cub::DeviceScan::ExclusiveSum(scratch.data(), temp, flags, rank.data(), n, s));
+  }
+  std::vector<long long> offsets;
+  for (const auto &v : volumes) offsets.push_back(v.offset < n ? v.offset : n - 1);
+  Buffer<long long> d_offsets = to_device(ctx, offsets);
+  Buffer<int> bounds(ctx, volumes.size() + 1);
+  rank_bounds<<<blocks_for((long long)volumes.size() + 1), 256, 0, s>>>(parent.data(), rank.data(), d_offsets.data(),
+                                                                      int(volumes.size()), n, bounds.data()); ++ctx.launches;
+  BK_CUDA(cudaGetLastError());
+  std::vector<int> b = bounds.download();
+  for (size_t i = 0; i < volumes.size(); ++i)
+    if (!volumes[i].d.n()) b[i] = i + 1 < volumes.size() ? b[i + 1] : b[volumes.size()];  // empty: no roots
+  const long long total = b[volumes.size()];
+  Buffer<long long> roots(ctx, total + 1), mapping(ctx, total + 1);
+  for (size_t i = 0; i < volumes.size(); ++i) {
+    const auto &v = volumes[i];
+    if (!v.d.n()) continue;
+    for_dtype(v.dtype, v.labels, [&](auto labels) {
+      using L = std::remove_const_t<std::remove_pointer_t<decltype(labels)>>;
+      relabel<L><<<blocks_for(v.d.n()), 256, 0, s>>>(labels, parent.data(), rank.data(), ids + v.offset, roots.data(),
+                                                      mapping.data(), v.d.n(), v.offset, b[i]); ++ctx.launches;
+    });
+  }
+  BK_CUDA(cudaGetLastError());
+  const auto hr = roots.download(total), hm = mapping.download(total + 1);
+  for (size_t i = 0; i < volumes.size(); ++i) {
+    const long long first = b[i], count = (i + 1 < volumes.size() ? b[i + 1] : total) - first;
+    out[i].count = volumes[i].d.n() ? count : 0;
+    if (!out[i].count) continue;
+    out[i].roots.assign(hr.begin() + first, hr.begin() + first + count);
+    out[i].mapping.assign(1, 0);
+    out[i].mapping.insert(out[i].mapping.end(), hm.begin() + first + 1, hm.begin() + first + 1 + count);
+  }
+  return out;
+}
+
 ComponentsResult connected_components(Context &ctx, const void *labels, int dtype, VolumeDims d, uint32_t *ids,
                                       bool planar) {
-  if (d.n() <= 0) { ComponentsResult r; r.mapping.assign(1, 0); return r; }
-  if (d.n() >= (1LL << 31) - 1) throw std::invalid_argument("volumes of 2^31 voxels or more are not supported");
-  switch (dtype) {
-    case U8: return run(ctx, static_cast<const uint8_t *>(labels), d, ids, planar);
-    case U16: return run(ctx, static_cast<const uint16_t *>(labels), d, ids, planar);
-    case U32: return run(ctx, static_cast<const uint32_t *>(labels), d, ids, planar);
-    case U64: return run(ctx, static_cast<const uint64_t *>(labels), d, ids, planar);
-    case I8: return run(ctx, static_cast<const int8_t *>(labels), d, ids, planar);
-    case I16: return run(ctx, static_cast<const int16_t *>(labels), d, ids, planar);
-    case I32: return run(ctx, static_cast<const int32_t *>(labels), d, ids, planar);
-    case I64: return run(ctx, static_cast<const int64_t *>(labels), d, ids, planar);
-    default: throw std::invalid_argument("connected components require integer labels");
-  }
+  label_bytes(dtype);  // rejects non-integer labels
+  return connected_components(ctx, std::vector<CcVolume>{{labels, dtype, d, 0}}, ids, planar)[0];
 }
 
 }  // namespace bk

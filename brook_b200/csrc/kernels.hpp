@@ -29,6 +29,16 @@ struct ComponentsResult {
 // ids (per voxel: id 1..K, 0 = background). `planar`: 8-connected within each z-slice only.
 ComponentsResult connected_components(Context &ctx, const void *labels, int dtype, VolumeDims d, uint32_t *ids,
                                       bool planar = false);
+// The same for several volumes laid out back to back in one flat space (offsets in order, no
+// gaps): ids + offset receives each volume's ids; one flatten, scan and download for all.
+struct CcVolume {
+  const void *labels;
+  int dtype;
+  VolumeDims d;
+  long long offset;
+};
+std::vector<ComponentsResult> connected_components(Context &ctx, const std::vector<CcVolume> &volumes, uint32_t *ids,
+                                                   bool planar = false);
 
 // ---- EDT (edt.cu) ----
 // Squared-then-rooted anisotropic distance of every voxel to the nearest voxel of a different id

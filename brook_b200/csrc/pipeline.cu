@@ -145,24 +145,31 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   Buffer<uint32_t> ids(ctx, N), mask(ctx, N);
   Buffer<float> dbf(ctx, N);
   const float aniso[3] = {opt.anisotropy[0], opt.anisotropy[1], opt.anisotropy[2]};
-  // ---- per-volume preamble
-  for (size_t v = 0; v < volumes.size(); ++v) {
-    auto &st = vs[v];
-    if (st.empty) continue;
-    const long long n = st.d.n();
-    uint32_t *vid = ids.data() + st.offset;
-    Buffer<unsigned char> masked;
-    const void *labels = volumes[v].data;
-    if (opt.object_ids) {
-      masked = filter_volume(ctx, volumes[v], *opt.object_ids);
-      labels = masked.data();
+  // ---- connected components of every volume at once, then boxes per volume
+  std::vector<Buffer<unsigned char>> masked(volumes.size());
+  {
+    std::vector<CcVolume> cv;
+    std::vector<size_t> which;
+    for (size_t v = 0; v < volumes.size(); ++v) {
+      if (vs[v].empty) continue;
+      const void *labels = volumes[v].data;
+      if (opt.object_ids) {
+        masked[v] = filter_volume(ctx, volumes[v], *opt.object_ids);
+        labels = masked[v].data();
+      }
+      cv.push_back({labels, volumes[v].dtype, vs[v].d, vs[v].offset});
+      which.push_back(v);
     }
-    st.cc = connected_components(ctx, labels, volumes[v].dtype, st.d, vid);
+    auto cc = connected_components(ctx, cv, ids.data());
+    for (size_t j = 0; j < which.size(); ++j) vs[which[j]].cc = std::move(cc[j]);
     clock.mark("ccl");
+  }
+  for (auto &st : vs) {
+    if (st.empty) continue;
     const int64_t K = st.cc.count;
     st.object_of.assign(K + 1, -1);
     if (!K) { st.empty = true; continue; }
-    st.boxes = analyze(ctx, vid, st.d, K);
+    st.boxes = analyze(ctx, ids.data() + st.offset, st.d, K);
     clock.mark("analyze");
   }
   // ---- EDT of every volume at once (the y and z passes of all volumes' lines in one launch each)
