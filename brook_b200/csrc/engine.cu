@@ -27,8 +27,9 @@ namespace cg = cooperative_groups;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr unsigned long long kMinFarNone = 0x7f8000007f800000ull;
 constexpr unsigned long long kClaimedMark = 0xFFFFFFFFFFFFFFFEull;
-// Resident engine CTAs per SM: 3 x 512 threads at up to 40 registers each.
-constexpr int kEngineCtasPerSm = 3;
+// Resident engine CTAs per SM: 4 x 512 threads (full occupancy) at up to 32 registers each; the
+// spills this forces cost less than the latency the extra warps hide.
+constexpr int kEngineCtasPerSm = 4;
 
 struct Shared {
   // the object (written by the group's first CTA, copied by the others)

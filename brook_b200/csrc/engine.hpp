@@ -106,6 +106,6 @@ long long trace_cluster_voxels(long long foreground);
 void launch_prepare(const EngineArgs &a, int nbig, int cluster_ctas, cudaStream_t stream);
 // lone_percent: the share of clusters (percent) whose CTAs take small objects first.
 void launch_trace(const EngineArgs &a, int nbig, int cluster_ctas, int lone_percent, cudaStream_t stream);
-constexpr int kLoneFirstPercent = 15;
+constexpr int kLoneFirstPercent = 10;
 
 }  // namespace bk
