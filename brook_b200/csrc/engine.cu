@@ -682,6 +682,7 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
   using G = Group<C>;
   __shared__ Shared sh;
   __shared__ unsigned long long s_work[4];
+  __shared__ unsigned long long s_prof[6];  // start, last lap, time in the four phases
   Shared *L = G::leader(&sh);
   if (threadIdx.x < 4) s_work[threadIdx.x] = 0;
   while (next_object<C>(a, sh, L, big)) {
@@ -703,10 +704,14 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
     long long paths = 0, used = 0;
     int cursor = 0;
     int status = kOk;
-    unsigned long long t_begin = 0, t_mark = 0, spent[4] = {0, 0, 0, 0};
-    if (G::first()) { L->rounds = 0; t_begin = t_mark = now_ns(); }
+    // per-object phase timers, kept in shared memory by the first thread (registers are scarce)
+    if (G::first()) {
+      L->rounds = 0;
+      s_prof[0] = s_prof[1] = now_ns();
+      s_prof[2] = s_prof[3] = s_prof[4] = s_prof[5] = 0;
+    }
     auto lap = [&](int phase) {
-      if (G::first()) { const unsigned long long t = now_ns(); spent[phase] += t - t_mark; t_mark = t; }
+      if (G::first()) { const unsigned long long t = now_ns(); s_prof[2 + phase] += t - s_prof[1]; s_prof[1] = t; }
     };
     while (paths < maxp) {
       // the next target: manual targets first, then the first alive voxel of the order
@@ -771,8 +776,8 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
       a.npaths[o] = int(paths);
       a.nstore[o] = int(used);
       unsigned long long *pr = a.profile + 8LL * o;
-      pr[0] = t_begin; pr[1] = now_ns();
-      for (int q = 0; q < 4; ++q) pr[2 + q] = spent[q];
+      pr[0] = s_prof[0]; pr[1] = now_ns();
+      for (int q = 0; q < 4; ++q) pr[2 + q] = s_prof[2 + q];
       pr[6] = L->rounds & 0xFFFFFFFFull; pr[7] = L->rounds >> 32;
     }
     G::sync();
