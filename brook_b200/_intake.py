@@ -88,9 +88,11 @@ def device_volume(labels):
 
 
 def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
-         extra_after, device):
+         extra_after, device, device_output=False):
     opts = _native.options(params, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids,
                            extra_before, extra_after)
+    if device_output:
+        opts.flags |= _native.DEVICE_OUTPUT
     ctx = _native.context(device)
     count = len(volumes)
     arr = (_native.Volume * max(count, 1))(*volumes)
@@ -99,7 +101,8 @@ def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching,
         _native.check(_native.lib.brook_skeletonize(ctx, arr, _native.ctypes.byref(opts), handles))
     else:
         _native.check(_native.lib.brook_skeletonize_batch(ctx, arr, count, _native.ctypes.byref(opts), handles))
-    return [PackedSkeletons.from_arrays(_native.packed_arrays(handles[i])) for i in range(count)]
+    grab = _native.packed_device_arrays if device_output else _native.packed_arrays
+    return [PackedSkeletons.from_arrays(grab(handles[i])) for i in range(count)]
 
 
 def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), object_ids=None,
@@ -134,8 +137,9 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     ids = None if object_ids is None else [int(i) for i in object_ids]
     packed = _run([volume], params, anisotropy, ids, dust_threshold, fix_branching, fix_borders,
                   [tuple(int(c) for c in p) for p in extra_targets_before],
-                  [tuple(int(c) for c in p) for p in extra_targets_after], device)[0]
+                  [tuple(int(c) for c in p) for p in extra_targets_after], device,
+                  device_output=output == "packed_device")[0]
     del keep
     if output == "skeletons":
         return packed.to_skeletons()
-    return packed.to_device() if output == "packed_device" else packed
+    return packed

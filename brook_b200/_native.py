@@ -227,6 +227,51 @@ def packed_arrays(handle):
         lib.brook_skeletons_destroy(handle)
 
 
+class _DeviceResult:
+    """Owns a brook_skeletons device result; its arrays are exposed without copies (CUDA array
+    interface) and the result is destroyed when the last array viewing it goes away."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __del__(self):
+        if self.handle:
+            lib.brook_skeletons_destroy(self.handle)
+            self.handle = None
+
+
+class _DeviceArray:
+    def __init__(self, owner, ptr, shape, typestr):
+        self.owner = owner  # keeps the result alive
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (int(ptr or 0), False),
+                                         "version": 3, "strides": None}
+
+
+def packed_device_arrays(handle):
+    """A BROOK_DEVICE_OUTPUT result as host metadata and torch CUDA tensors over the result's own
+    device arrays (no copy); the handle lives as long as those tensors."""
+    import torch
+
+    v = SkeletonsDeviceView()
+    owner = _DeviceResult(handle)
+    check(lib.brook_skeletons_get_device_view(handle, ctypes.byref(v)))
+    k, nv, ne = v.skeleton_count, v.vertex_count, v.edge_count
+
+    def host(ptr, count):
+        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(np.int64, copy=True) if count else np.zeros(0, np.int64)
+
+    def device(vol, shape, typestr, dtype):
+        if not np.prod(shape):
+            return torch.zeros(shape, dtype=dtype, device="cuda")
+        return torch.as_tensor(_DeviceArray(owner, vol.data, shape, typestr), device="cuda")
+
+    return dict(labels=host(v.labels, k), v_off=host(v.vertex_offsets, k + 1), e_off=host(v.edge_offsets, k + 1),
+                vertices=device(v.vertices, (nv, 3), "<f4", torch.float32),
+                edges=device(v.edges, (ne, 2), "<u4", torch.uint32),
+                radii=device(v.radii, (nv,), "<f4", torch.float32),
+                anisotropy=tuple(float(a) for a in v.anisotropy))
+
+
 def stats(device=0):
     """The statistics of the calling thread's context's last call (stage ms and work counters)."""
     import json

@@ -281,6 +281,26 @@ def test_c_abi_device_output(gpu):
         np.testing.assert_array_equal(copied[name], expected[name], err_msg=name)
 
 
+def test_packed_device_output_matches_host(gpu):
+    """output="packed_device": torch CUDA tensors over the result's own device arrays (no copy),
+    equal to the host route, and still valid after the call's other objects are gone."""
+    import torch
+
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((64, 64, 64), objects=8, seed=6)
+    opts = dict(teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    host = bk().skeletonize(labels, output="packed", **opts)
+    dev = bk().skeletonize(labels, output="packed_device", **opts)
+    assert isinstance(dev.vertices, torch.Tensor) and dev.vertices.is_cuda
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dev.labels, host.labels)
+    np.testing.assert_array_equal(dev.v_off, host.v_off)
+    np.testing.assert_array_equal(dev.vertices.cpu().numpy(), host.vertices)
+    np.testing.assert_array_equal(dev.edges.cpu().numpy(), host.edges)
+    np.testing.assert_array_equal(dev.radii.cpu().numpy(), host.radii)
+
+
 def test_edt_matches_oracle(gpu):
     """The EDT alone, through the C ABI, on multi-label volumes with and without black border."""
     from brook_b200 import _native as n
