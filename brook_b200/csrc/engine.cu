@@ -699,6 +699,9 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
     const long long rec_cap = a.rec_cap[o];
     const int mcount = a.manual_count[o];
     const int *manual = a.manual + a.manual_begin[o];
+    const int acount = a.after_count[o];
+    const int *after = a.after + a.after_begin[o];
+    int after_used = 0;
     const int *order = a.order + sh.begin;
     const long long maxp = a.max_paths[o];
     long long paths = 0, used = 0;
@@ -714,7 +717,8 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
       if (G::first()) { const unsigned long long t = now_ns(); s_prof[2 + phase] += t - s_prof[1]; s_prof[1] = t; }
     };
     while (paths < maxp) {
-      // the next target: manual targets first, then the first alive voxel of the order
+      // the next target: manual targets first, then the first alive voxel of the order, then the
+      // targets after (trace.cu:209-212)
       int t = -1;
       if (paths < mcount) {
         t = manual[paths];
@@ -732,6 +736,7 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
           cursor += G::threads();
           if (cursor >= sh.count) { cursor = sh.count; break; }
         }
+        if (t < 0 && after_used < acount) t = after[after_used++];
         if (t < 0) break;
       }
       lap(0);

@@ -68,6 +68,7 @@ struct EngineArgs {
   // trace
   const int *order;            // target order of every object at obj_begin
   const int *manual_begin, *manual_count, *manual;  // manual targets in pop order
+  const int *after_begin, *after_count, *after;     // targets once no voxel is alive, in pop order
   const long long *max_paths;
   int *store;                  // path vertices, target first
   const long long *store_begin, *store_cap;

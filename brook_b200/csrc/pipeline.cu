@@ -122,7 +122,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       throw std::invalid_argument("odd pdrf_exponent makes the background penalty negative");
   }
   if (!opt.fix_branching) throw std::invalid_argument("fix_branching=False is not supported by this build");
-  if (!opt.targets_after.empty()) throw std::invalid_argument("extra_targets_after is not supported by this build");
+  if ((!opt.targets_before.empty() || !opt.targets_after.empty()) && volumes.size() != 1)
+    throw std::invalid_argument("extra targets are given for one volume at a time");
   const double exponent = t.pdrf_exponent;
   if (!(exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))))
     throw std::invalid_argument("pdrf_exponent must be a power of two in this build");
@@ -221,6 +222,33 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   }
   const int nobj = int(objects.size());
   if (nobj == 0) return results;
+  // extra targets by the component they fall on (skeletonize.cu:16-25, 61-65 of the reference): a
+  // negative coordinate counts from the end of its axis; a point outside the volume is an error;
+  // points on the background or on objects that are not traced are dropped
+  std::vector<std::vector<int>> before_of(nobj), after_of(nobj);
+  if (!opt.targets_before.empty() || !opt.targets_after.empty()) {
+    const auto &st = vs[0];
+    std::vector<long long> flats;
+    for (int list = 0; list < 2; ++list)
+      for (auto p : list ? opt.targets_after : opt.targets_before) {
+        const long long shape[3] = {st.d.sx, st.d.sy, st.d.sz};
+        for (int a = 0; a < 3; ++a) {
+          if (p[a] < 0) p[a] += shape[a];
+          if (p[a] < 0 || p[a] >= shape[a]) throw std::invalid_argument("extra target is outside the input volume");
+        }
+        flats.push_back(st.offset + p[0] + shape[0] * (p[1] + shape[1] * p[2]));
+      }
+    std::vector<uint32_t> at(flats.size());
+    for (size_t i = 0; i < flats.size(); ++i)
+      BK_CUDA(cudaMemcpyAsync(&at[i], ids.data() + flats[i], sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    ctx.synchronize();
+    for (size_t i = 0; i < flats.size(); ++i) {
+      const int o = at[i] ? st.object_of[at[i]] : -1;
+      if (o < 0) continue;
+      (i < opt.targets_before.size() ? before_of : after_of)[o].push_back(int(flats[i]));
+    }
+  }
+  std::vector<int> after_begin(nobj), after_count(nobj), after;
   // per object: voxel range, arena, border root, manual targets, path budget, store regions
   std::vector<int> obj_begin(nobj), obj_count(nobj), obj_arena(nobj), border_root(nobj, -1), seg_end(nobj);
   std::vector<float> M(nobj);
@@ -239,22 +267,28 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     const auto &b = st.borders[ob.id];
     auto flat = [&](const Point &p) { return int(st.offset + p[0] + (long long)st.d.sx * (p[1] + (long long)st.d.sy * p[2])); };
     if (!b.empty()) border_root[o] = flat(b.back());
-    // manual targets in pop order: the border points except the last (the root), last first;
-    // none: the object's own target (-1, resolved on the device)
+    // manual targets in pop order: the border points except the last (the root), then the extra
+    // targets before, all last first (lockstep.cu:127-134); none: the object's own target (-1,
+    // resolved on the device). Extra targets after: last first, once no voxel is alive.
+    std::vector<int> listed;
+    for (size_t i = 0; i + 1 < b.size(); ++i) listed.push_back(flat(b[i]));
+    listed.insert(listed.end(), before_of[o].begin(), before_of[o].end());
     manual_begin[o] = int(manual.size());
-    if (b.size() > 1) for (size_t i = b.size() - 1; i-- > 0;) manual.push_back(flat(b[i]));
-    else if (b.size() <= 1) manual.push_back(-1);
+    if (listed.empty()) manual.push_back(-1);
+    else manual.insert(manual.end(), listed.rbegin(), listed.rend());
     manual_count[o] = int(manual.size()) - manual_begin[o];
+    after_begin[o] = int(after.size());
+    after.insert(after.end(), after_of[o].rbegin(), after_of[o].rend());
+    after_count[o] = int(after.size()) - after_begin[o];
     const int64_t budget = t.max_paths.value_or(ob.count);
-    max_paths[o] = manual_count[o] >= budget ? 0 : budget;
+    max_paths[o] = manual_count[o] + after_count[o] >= budget ? 0 : budget;
     store_begin[o] = store_total;
-    store_cap[o] = 2 * ob.count + manual_count[o] + 2;
+    store_cap[o] = (2 + (long long)after_count[o]) * ob.count + manual_count[o] + 2;
     store_total += store_cap[o];
     rec_begin[o] = rec_total;
-    rec_cap[o] = ob.count + manual_count[o] + 1;
+    rec_cap[o] = ob.count + manual_count[o] + after_count[o] + 1;
     rec_total += rec_cap[o];
   }
-  if (!opt.targets_before.empty()) throw std::invalid_argument("extra_targets_before is not supported by this build");
   if (F >= (1LL << 31)) throw std::invalid_argument("too many foreground voxels");
   // object voxel lists, volume by volume into their ranges
   Buffer<int> vox(ctx, F);
@@ -326,6 +360,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   auto d_M = to_device(ctx, M);
   auto d_manual_begin = to_device(ctx, manual_begin), d_manual_count = to_device(ctx, manual_count);
   auto d_manual = to_device(ctx, manual.empty() ? std::vector<int>{0} : manual);
+  auto d_after_begin = to_device(ctx, after_begin), d_after_count = to_device(ctx, after_count);
+  auto d_after = to_device(ctx, after.empty() ? std::vector<int>{0} : after);
   auto d_max_paths = to_device(ctx, max_paths), d_store_begin = to_device(ctx, store_begin), d_store_cap = to_device(ctx, store_cap);
   auto d_rec_begin = to_device(ctx, rec_begin), d_rec_cap = to_device(ctx, rec_cap);
   Buffer<int> queue(ctx, 2), status(ctx, nobj), root(ctx, nobj), target(ctx, nobj), npaths(ctx, nobj), nstore(ctx, nobj);
@@ -353,6 +389,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   }
   a.root = root.data(); a.target = target.data(); a.max_daf = max_daf.data();
   a.manual_begin = d_manual_begin.data(); a.manual_count = d_manual_count.data(); a.manual = d_manual.data();
+  a.after_begin = d_after_begin.data(); a.after_count = d_after_count.data(); a.after = d_after.data();
   a.max_paths = d_max_paths.data(); a.store = store.data(); a.store_begin = d_store_begin.data(); a.store_cap = d_store_cap.data();
   a.rec_start = rec_start.data(); a.rec_len = rec_len.data(); a.rec_begin = d_rec_begin.data(); a.rec_cap = d_rec_cap.data();
   a.npaths = npaths.data(); a.nstore = nstore.data(); a.work = work.data(); a.profile = profile.data();

@@ -437,6 +437,8 @@ struct Params {
   float anisotropy[3];
   double dust;
   int fix_branching, fix_borders;
+  // extra targets (x, y, z triples): `before` traced first, `after` once no voxel is left
+  std::vector<std::array<i64, 3>> before, after;
 };
 
 // Per-object tracing state over the shared volume. Every array is indexed by global flat index;
@@ -649,27 +651,29 @@ struct ObjectPlan {
   std::vector<i64> voxels;     // ascending flat
   std::vector<i64> order;      // target order
   std::vector<i64> manual;     // manual targets in pop order
+  std::vector<i64> after;      // targets after the automatic ones, in pop order
   i64 max_paths;
 };
 
 // The trace loop of one object (trace.cu:196-246 order, lockstep.cu:91-183 targets): manual
-// targets first, then the first alive voxel of the target order; railroad; invalidation; the
-// path becomes rails.
+// targets first, then the first alive voxel of the target order, then, once no voxel is alive,
+// the targets after (trace.cu:209-212); railroad; invalidation; the path becomes rails.
 std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, const Params &P) {
   std::vector<std::vector<i64>> paths;
   std::vector<i64> touched, frontier, next, far, keep, rtouched;
   std::vector<uint64_t> snap;
   if (plan.max_paths <= 0) return paths;
   V.pdrf[plan.root] = 0.0f;
-  size_t cursor = 0;
+  size_t cursor = 0, after = 0;
   while (i64(paths.size()) < plan.max_paths) {
     i64 t = -1;
     const size_t iter = paths.size();
     if (iter < plan.manual.size()) t = plan.manual[iter];
     else {
       while (cursor < plan.order.size() && !V.alive[plan.order[cursor]]) ++cursor;
-      if (cursor >= plan.order.size()) break;
-      t = plan.order[cursor];
+      if (cursor < plan.order.size()) t = plan.order[cursor];
+      else if (after < plan.after.size()) t = plan.after[after++];
+      else break;
     }
     std::vector<i64> path = railroad(V, plan.id, t, rtouched);
     if (path.empty()) throw std::runtime_error("no rail reachable from a target");
@@ -833,6 +837,19 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
     }
   }
   if (keep_stages) { R.dbf = V.dbf; R.daf = daf; R.pdrf = V.pdrf; }
+  // extra targets by the component they fall on (skeletonize.cu:16-25, 61-65): a negative
+  // coordinate counts from the end of its axis; a point outside the volume is an error
+  std::vector<std::vector<i64>> before_of(count + 1), after_of(count + 1);
+  for (int list = 0; list < 2; ++list)
+    for (auto p : list ? P.after : P.before) {
+      const i64 shape[3] = {s.sx, s.sy, s.sz};
+      for (int a = 0; a < 3; ++a) {
+        if (p[a] < 0) p[a] += shape[a];
+        if (p[a] < 0 || p[a] >= shape[a]) throw std::invalid_argument("extra target is outside the input volume");
+      }
+      const i64 flat = s.idx(p[0], p[1], p[2]);
+      (list ? after_of : before_of)[ids[flat]].push_back(flat);
+    }
   // target orders and manual targets (lockstep.cu:120-142, lockstep_order.cu:21-45)
   R.order_offsets.assign(count + 2, 0);
   for (size_t id = 1; id <= count; ++id) {
@@ -847,12 +864,15 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
       if (std::isinf(y)) y = 0;
       return x == y ? a > b : x > y;
     });
-    std::vector<std::array<i64, 3>> manual = borders[id];
+    std::vector<i64> manual;
+    for (const auto &p : borders[id]) manual.push_back(s.idx(p[0], p[1], p[2]));
     if (!manual.empty()) manual.pop_back();
+    manual.insert(manual.end(), before_of[id].begin(), before_of[id].end());
     if (manual.empty()) plan.manual.push_back(targets[id]);
-    else for (auto it = manual.rbegin(); it != manual.rend(); ++it) plan.manual.push_back(s.idx((*it)[0], (*it)[1], (*it)[2]));
+    else plan.manual.assign(manual.rbegin(), manual.rend());
+    plan.after.assign(after_of[id].rbegin(), after_of[id].rend());
     const i64 budget = P.has_max_paths ? P.max_paths : box[id][6];
-    plan.max_paths = i64(plan.manual.size()) >= budget ? 0 : budget;
+    plan.max_paths = i64(plan.manual.size() + plan.after.size()) >= budget ? 0 : budget;
     plans.push_back(std::move(plan));
   }
   V.dist.assign(n, kInf);
@@ -941,6 +961,8 @@ struct oracle_params {
   float anisotropy[3];
   double dust;
   int32_t fix_branching, fix_borders;
+  const int64_t *targets_before; int64_t n_before;  // x, y, z triples
+  const int64_t *targets_after; int64_t n_after;
 };
 
 void *oracle_run(const void *labels, int dtype, int64_t sx, int64_t sy, int64_t sz, const oracle_params *p,
@@ -954,6 +976,10 @@ void *oracle_run(const void *labels, int dtype, int64_t sx, int64_t sy, int64_t 
     P.max_paths = p->max_paths; P.has_max_paths = p->has_max_paths;
     for (int a = 0; a < 3; ++a) P.anisotropy[a] = p->anisotropy[a];
     P.dust = p->dust; P.fix_branching = p->fix_branching; P.fix_borders = p->fix_borders;
+    for (int64_t i = 0; i < p->n_before; ++i)
+      P.before.push_back({p->targets_before[3 * i], p->targets_before[3 * i + 1], p->targets_before[3 * i + 2]});
+    for (int64_t i = 0; i < p->n_after; ++i)
+      P.after.push_back({p->targets_after[3 * i], p->targets_after[3 * i + 1], p->targets_after[3 * i + 2]});
     if (!P.fix_branching) throw std::invalid_argument("the oracle covers fix_branching=True");
     *r = run(labels, dtype, Shape{sx, sy, sz}, P, threads, keep_stages);
   } catch (const std::exception &e) {

@@ -23,7 +23,9 @@ class _Params(ctypes.Structure):
                 ("soma_acceptance", ctypes.c_double), ("soma_scale", ctypes.c_double),
                 ("soma_constant", ctypes.c_double), ("max_paths", ctypes.c_int64), ("has_max_paths", ctypes.c_int32),
                 ("anisotropy", ctypes.c_float * 3), ("dust", ctypes.c_double), ("fix_branching", ctypes.c_int32),
-                ("fix_borders", ctypes.c_int32)]
+                ("fix_borders", ctypes.c_int32), ("targets_before", ctypes.POINTER(ctypes.c_int64)),
+                ("n_before", ctypes.c_int64), ("targets_after", ctypes.POINTER(ctypes.c_int64)),
+                ("n_after", ctypes.c_int64)]
 
 
 _lib = None
@@ -144,7 +146,8 @@ DEFAULT_TEASAR_PARAMS = dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_expon
 
 
 def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), dust_threshold=1000,
-                fix_branching=True, fix_borders=True, threads=1, stages=False):
+                fix_branching=True, fix_borders=True, threads=1, stages=False, extra_targets_before=(),
+                extra_targets_after=()):
     """Run the oracle on a 3D label volume (any layout; read as its logical (x, y, z) axes), with
     the argument defaults of the reference's brook.skeletonize."""
     labels = np.asarray(labels)
@@ -156,6 +159,12 @@ def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1
     if labels.dtype not in _DTYPES:
         raise TypeError(f"unsupported label dtype {labels.dtype}")
     params = _params(teasar_params or {}, anisotropy, dust_threshold, fix_branching, fix_borders)
+    keep = []
+    for name, points in (("targets_before", extra_targets_before), ("targets_after", extra_targets_after)):
+        pts = np.ascontiguousarray(np.asarray(list(points), np.int64).reshape(-1, 3))
+        keep.append(pts)
+        setattr(params, name, pts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        setattr(params, "n_before" if name == "targets_before" else "n_after", pts.shape[0])
     handle = lib().oracle_run(labels.ctypes.data, _DTYPES[labels.dtype], *labels.shape, ctypes.byref(params),
                               int(threads), int(bool(stages)))
     result = OracleResult(handle, labels.shape)

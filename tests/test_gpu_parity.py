@@ -281,6 +281,26 @@ def test_c_abi_device_output(gpu):
         np.testing.assert_array_equal(copied[name], expected[name], err_msg=name)
 
 
+def test_extra_targets_match_oracle(gpu):
+    """extra_targets_before (traced first, after the border targets) and extra_targets_after
+    (traced once no voxel is left), points on the background dropped (lockstep.cu:127-134,
+    trace.cu:209-212)."""
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((64, 64, 64), objects=6, seed=3)
+    pts = {l: np.argwhere(labels == l) for l in (1, 2, 3)}
+    before = [tuple(pts[1][len(pts[1]) // 2]), tuple(pts[2][-1]), tuple(np.argwhere(labels == 0)[0])]
+    after = [tuple(pts[3][0]), tuple(pts[1][-1]), tuple(int(c) - 64 for c in pts[2][len(pts[2]) // 2])]
+    opts = dict(teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    got = bk().skeletonize(labels, output="packed", extra_targets_before=before, extra_targets_after=after, **opts)
+    exp = oracle.skeletonize(labels, threads=8, extra_targets_before=before, extra_targets_after=after, **opts)
+    assert_same(got, exp, "extra targets")
+    plain = oracle.skeletonize(labels, threads=8, **opts)
+    assert not np.array_equal(exp.array("vertices"), plain.array("vertices"))  # the targets changed something
+    with pytest.raises(Exception, match="outside"):
+        bk().skeletonize(labels, output="packed", extra_targets_before=[(64, 0, 0)], **opts)
+
+
 def test_packed_device_output_matches_host(gpu):
     """output="packed_device": torch CUDA tensors over the result's own device arrays (no copy),
     equal to the host route, and still valid after the call's other objects are gone."""
