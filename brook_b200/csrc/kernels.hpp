@@ -68,6 +68,16 @@ struct Box {
   int64_t count;
 };
 std::vector<Box> analyze(Context &ctx, const uint32_t *ids, VolumeDims d, int64_t count);
+// Several volumes of one flat index space (ids + offset, component ids 1..count each): one launch
+// per volume, one download for all.
+struct IdVolume {
+  long long offset;
+  VolumeDims d;
+  int64_t count;
+};
+std::vector<std::vector<Box>> analyze(Context &ctx, const uint32_t *ids, const std::vector<IdVolume> &volumes);
+std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, const uint32_t *ids,
+                                            const std::vector<IdVolume> &volumes);
 // 26-bit same-id neighbour mask of every voxel (0 for background).
 void neighbour_mask(Context &ctx, const uint32_t *ids, VolumeDims d, uint32_t *out);
 // Per id the largest value of `field` (non-negative, finite), as float bits.

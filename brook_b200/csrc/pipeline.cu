@@ -165,12 +165,19 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     for (size_t j = 0; j < which.size(); ++j) vs[which[j]].cc = std::move(cc[j]);
     clock.mark("ccl");
   }
-  for (auto &st : vs) {
-    if (st.empty) continue;
-    const int64_t K = st.cc.count;
-    st.object_of.assign(K + 1, -1);
-    if (!K) { st.empty = true; continue; }
-    st.boxes = analyze(ctx, ids.data() + st.offset, st.d, K);
+  {
+    std::vector<IdVolume> iv;
+    std::vector<size_t> which;
+    for (size_t v = 0; v < vs.size(); ++v) {
+      auto &st = vs[v];
+      if (st.empty) continue;
+      st.object_of.assign(st.cc.count + 1, -1);
+      if (!st.cc.count) { st.empty = true; continue; }
+      iv.push_back({st.offset, st.d, st.cc.count});
+      which.push_back(v);
+    }
+    auto boxes = analyze(ctx, ids.data(), iv);
+    for (size_t j = 0; j < which.size(); ++j) vs[which[j]].boxes = std::move(boxes[j]);
     clock.mark("analyze");
   }
   // ---- EDT of every volume at once (the y and z passes of all volumes' lines in one launch each)
@@ -181,13 +188,20 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     edt_volumes(ctx, ids.data(), ev, aniso, dbf.data());
     clock.mark("edt");
   }
-  for (auto &st : vs) {
-    if (st.empty) continue;
-    uint32_t *vid = ids.data() + st.offset;
-    neighbour_mask(ctx, vid, st.d, mask.data() + st.offset);
+  {
+    std::vector<IdVolume> iv;
+    std::vector<size_t> which;
+    for (size_t v = 0; v < vs.size(); ++v) {
+      auto &st = vs[v];
+      if (st.empty) continue;
+      neighbour_mask(ctx, ids.data() + st.offset, st.d, mask.data() + st.offset);
+      st.borders.assign(st.cc.count + 1, {});
+      iv.push_back({st.offset, st.d, st.cc.count});
+      which.push_back(v);
+    }
     clock.mark("mask");
-    st.borders.assign(st.cc.count + 1, {});
-    st.dbf_max = segment_max(ctx, dbf.data() + st.offset, vid, st.d.n(), st.cc.count);
+    auto maxima = segment_max(ctx, dbf.data(), ids.data(), iv);
+    for (size_t j = 0; j < which.size(); ++j) vs[which[j]].dbf_max = std::move(maxima[j]);
     clock.mark("dbf_max");
   }
   // ---- border targets of every volume in one pass

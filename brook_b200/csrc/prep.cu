@@ -168,6 +168,64 @@ void neighbour_mask(Context &ctx, const uint32_t *ids, VolumeDims vd, uint32_t *
   BK_CUDA(cudaGetLastError());
 }
 
+std::vector<std::vector<Box>> analyze(Context &ctx, const uint32_t *ids, const std::vector<IdVolume> &volumes) {
+  std::vector<long long> base(volumes.size() + 1, 0);
+  for (size_t v = 0; v < volumes.size(); ++v) base[v + 1] = base[v] + volumes[v].count + 1;
+  const long long total = base.back();
+  cudaStream_t s = ctx.stream();
+  Buffer<int> dlo(ctx, 3 * total), dhi(ctx, 3 * total);
+  Buffer<unsigned long long> counts(ctx, total);
+  dlo.fill_bytes(0x7F);  // 0x7F7F7F7F: above every coordinate
+  dhi.fill_bytes(0xFF);  // -1
+  counts.zero();
+  for (size_t v = 0; v < volumes.size(); ++v) {
+    const auto &iv = volumes[v];
+    if (!iv.d.n() || !iv.count) continue;
+    analyze_kernel<<<blocks_for(iv.d.n()), 256, 0, s>>>(ids + iv.offset, Dims{iv.d.sx, iv.d.sy, iv.d.sz},
+                                                        dlo.data() + 3 * base[v], dhi.data() + 3 * base[v],
+                                                        counts.data() + base[v]); ++ctx.launches;
+  }
+  BK_CUDA(cudaGetLastError());
+  std::vector<int> lo(3 * total), hi(3 * total);
+  std::vector<unsigned long long> c(total);
+  BK_CUDA(cudaMemcpyAsync(lo.data(), dlo.data(), lo.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BK_CUDA(cudaMemcpyAsync(hi.data(), dhi.data(), hi.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BK_CUDA(cudaMemcpyAsync(c.data(), counts.data(), c.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  ctx.synchronize();
+  std::vector<std::vector<Box>> out(volumes.size());
+  for (size_t v = 0; v < volumes.size(); ++v) {
+    out[v].resize(volumes[v].count + 1);
+    for (int64_t id = 0; id <= volumes[v].count; ++id) {
+      const long long g = base[v] + id;
+      for (int a = 0; a < 3; ++a) { out[v][id].lo[a] = lo[3 * g + a]; out[v][id].hi[a] = hi[3 * g + a]; }
+      out[v][id].count = (int64_t)c[g];
+    }
+  }
+  return out;
+}
+
+std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, const uint32_t *ids,
+                                            const std::vector<IdVolume> &volumes) {
+  std::vector<long long> base(volumes.size() + 1, 0);
+  for (size_t v = 0; v < volumes.size(); ++v) base[v + 1] = base[v] + volumes[v].count + 1;
+  Buffer<unsigned> best(ctx, base.back());
+  best.zero();
+  for (size_t v = 0; v < volumes.size(); ++v) {
+    const auto &iv = volumes[v];
+    if (!iv.d.n() || !iv.count) continue;
+    segmax_kernel<<<blocks_for(iv.d.n()), 256, 0, ctx.stream()>>>(field + iv.offset, ids + iv.offset, iv.d.n(),
+                                                                  best.data() + base[v]); ++ctx.launches;
+  }
+  BK_CUDA(cudaGetLastError());
+  auto bits = best.download();
+  std::vector<std::vector<float>> out(volumes.size());
+  for (size_t v = 0; v < volumes.size(); ++v) {
+    out[v].resize(volumes[v].count + 1);
+    std::memcpy(out[v].data(), bits.data() + base[v], out[v].size() * sizeof(float));
+  }
+  return out;
+}
+
 std::vector<float> segment_max(Context &ctx, const float *field, const uint32_t *ids, long long n, int64_t count) {
   Buffer<unsigned> best(ctx, count + 1);
   best.zero();
