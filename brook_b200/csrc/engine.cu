@@ -130,6 +130,32 @@ struct Group {
 template <class T>
 __device__ __forceinline__ T vload(const T *p) { return *(const volatile T *)p; }
 
+// Per-CTA staging of a round's frontier in shared memory. When every CTA's share of the frontier
+// fits, a CTA stages its own share (step A) and spreads only that share's (voxel, neighbour) items
+// over its threads (step B): the items then read their voxel's staged fields from shared memory
+// instead of L2, which takes one to four dependent L2 round trips out of every item's chain.
+// Larger frontiers go through the global staging arrays, items spread over the whole group.
+constexpr int kStageBytes = 18432;
+constexpr int kFloodStage = kStageBytes / 12;  // distance|mask (8) + voxel (4)
+constexpr int kInvalStage = kStageBytes / 36;  // key (8) + both positions (16) + voxel, mask, reach (12)
+constexpr int kBandStage = kStageBytes / 24;   // best offer (8) + position (8) + voxel, mask (8)
+
+__device__ __forceinline__ unsigned char *stage_bytes() {
+  __shared__ __align__(16) unsigned char buf[kStageBytes];
+  return buf;
+}
+
+// This CTA's share [lo, hi) of n entries, when the largest share fits `cap` (the same answer in
+// every CTA of the group, which all read the same n).
+template <int C>
+__device__ __forceinline__ bool own_share(int n, int cap, int &lo, int &hi) {
+  if ((n + C - 1) / C > cap) return false;
+  const int r = Group<C>::rank();
+  lo = int((long long)n * r / C);
+  hi = int((long long)n * (r + 1) / C);
+  return true;
+}
+
 // Pulls the next object for this group; false when its queue is empty. The group's first CTA
 // pops and publishes; every CTA copies the object into its own shared memory.
 template <int C>
@@ -192,26 +218,46 @@ __device__ bool flood_geometric(const EngineArgs &a, Shared &sh, Shared *L, floa
     if (nc == 0) break;
     if (r >= bound) return false;
     if (G::first()) L->cnt[(r + 2) % 3] = 0;
-    for (int i = G::tid(); i < nc; i += G::threads()) {
-      const int u = __ldcg(cur + i);
-      // step A runs between barriers, with no relaxation in flight: the flag clear (a reduction,
-      // nothing to wait for) and the distance read need no order between them
-      atomicAnd(a.flags + u, ~kNearQueued);
-      const float du = __ldcg(d + u);
-      wide[i] = (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u];
-    }
-    G::sync();
     int *next_count = &L->cnt[(r + 1) % 3];
-    for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
-      const int k = int(j & 31);
-      if (k >= 26) continue;
-      const int i = int(j >> 5);
-      const unsigned long long e = __ldcg(wide + i);
-      if (!((unsigned(e) >> k) & 1u)) continue;
-      const int v = __ldcg(cur + i) + sh.off[k];
+    auto relax = [&](unsigned long long e, int u, int k) {
+      if (!((unsigned(e) >> k) & 1u)) return;
+      const int v = u + sh.off[k];
       const float cand = __fadd_rn(__uint_as_float(unsigned(e >> 32)), sh.w[k]);
       const float old = atomic_min_pos(d + v, cand);
       if (old > cand && !(atomicOr(a.flags + v, kNearQueued) & kNearQueued)) nxt[atomicAdd(next_count, 1)] = v;
+    };
+    // step A runs between barriers, with no relaxation in flight: the flag clear (a reduction,
+    // nothing to wait for) and the distance read need no order between them
+    int lo, hi;
+    if (own_share<C>(nc, kFloodStage, lo, hi)) {
+      unsigned long long *se = reinterpret_cast<unsigned long long *>(stage_bytes());
+      int *su = reinterpret_cast<int *>(se + kFloodStage);
+      for (int i = lo + int(threadIdx.x); i < hi; i += blockDim.x) {
+        const int u = __ldcg(cur + i);
+        atomicAnd(a.flags + u, ~kNearQueued);
+        const float du = __ldcg(d + u);
+        su[i - lo] = u;
+        se[i - lo] = (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u];
+      }
+      G::sync();
+      for (int j = threadIdx.x; j < (hi - lo) * 32; j += blockDim.x) {
+        const int k = j & 31;
+        if (k < 26) relax(se[j >> 5], su[j >> 5], k);
+      }
+    } else {
+      for (int i = G::tid(); i < nc; i += G::threads()) {
+        const int u = __ldcg(cur + i);
+        atomicAnd(a.flags + u, ~kNearQueued);
+        const float du = __ldcg(d + u);
+        wide[i] = (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u];
+      }
+      G::sync();
+      for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
+        const int k = int(j & 31);
+        if (k >= 26) continue;
+        const int i = int(j >> 5);
+        relax(__ldcg(wide + i), __ldcg(cur + i), k);
+      }
     }
     G::sync();
   }
@@ -366,25 +412,21 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
       }
       if (G::first()) { L->cnt[(r + 2) % 3] = 0; L->rounds += 1; }
       const float T = vload(&L->T);
-      for (int i = G::tid(); i < nc; i += G::threads()) {
-        const int u = __ldcg(cur + i);
-        atomicAnd(a.flags + u, ~kNearQueued);  // no relaxation in flight during step A
+      int *next_count = &L->cnt[(r + 1) % 3];
+      // step A: no relaxation is in flight between the barriers
+      auto stage = [&](int u) {
+        atomicAnd(a.flags + u, ~kNearQueued);
         const float fu = a.pdrf[u];
         const float du = __ldcg(a.dist + u);
         const unsigned long long rb = vload(&sh.rb);
         const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
         const bool expand = fu != 0.0f && du <= Tb;
-        wide[i] = expand ? (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u] : 0ull;
-      }
-      G::sync();
-      int *next_count = &L->cnt[(r + 1) % 3];
-      for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
-        const int k = int(j & 31);
-        if (k >= 26) continue;
-        const int i = int(j >> 5);
-        const unsigned long long e = __ldcg(wide + i);
-        if (!((unsigned(e) >> k) & 1u)) continue;
-        const int v = __ldcg(cur + i) + sh.off[k];
+        return expand ? (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u] : 0ull;
+      };
+      // step B: one (voxel, neighbour) item
+      auto relax = [&](unsigned long long e, int u, int k) {
+        if (!((unsigned(e) >> k) & 1u)) return;
+        const int v = u + sh.off[k];
         const float du = __uint_as_float(unsigned(e >> 32));
         const float fv = a.pdrf[v];
         const float cand = vw_step(du, fv);
@@ -400,6 +442,30 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
             atomicMin(&sh.minfar, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | __float_as_uint(fv));
             if (!(atomicOr(a.flags + v, kFarQueued) & kFarQueued)) far[atomicAdd(&L->n_far, 1)] = v;
           }
+        }
+      };
+      int lo, hi;
+      if (own_share<C>(nc, kFloodStage, lo, hi)) {
+        unsigned long long *se = reinterpret_cast<unsigned long long *>(stage_bytes());
+        int *su = reinterpret_cast<int *>(se + kFloodStage);
+        for (int i = lo + int(threadIdx.x); i < hi; i += blockDim.x) {
+          const int u = __ldcg(cur + i);
+          su[i - lo] = u;
+          se[i - lo] = stage(u);
+        }
+        G::sync();
+        for (int j = threadIdx.x; j < (hi - lo) * 32; j += blockDim.x) {
+          const int k = j & 31;
+          if (k < 26) relax(se[j >> 5], su[j >> 5], k);
+        }
+      } else {
+        for (int i = G::tid(); i < nc; i += G::threads()) wide[i] = stage(__ldcg(cur + i));
+        G::sync();
+        for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
+          const int k = int(j & 31);
+          if (k >= 26) continue;
+          const int i = int(j >> 5);
+          relax(__ldcg(wide + i), __ldcg(cur + i), k);
         }
       }
       G::sync();
@@ -560,35 +626,16 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
       if (nc == 0) break;
       if (++work > bound) return false;
       if (G::first()) { L->cnt[(r + 2) % 3] = 0; L->rounds += 1ull << 32; }
-      // step A: the round boundary's key of each frontier voxel, and both positions
-      for (int i = G::tid(); i < nc; i += G::threads()) {
-        const int u = __ldcg(cur + i);
-        const unsigned long long k = __ldcg(a.key + u);
-        atomicAnd(a.flags + u, ~kFront);
-        wide[i] = k;
-        int x, y, z;
-        unravel3(u - sh.a0, sh.sx, sh.sy, x, y, z);
-        side_u[i] = pack3(x, y, z);
-        unravel3(int(unsigned(k)) - sh.a0, sh.sx, sh.sy, x, y, z);
-        side_s[i] = pack3(x, y, z);
-      }
-      G::sync();
       int *next_count = &L->cnt[(r + 1) % 3];
-      for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
-        const int k = int(j & 31);
-        if (k >= 26) continue;
-        const int i = int(j >> 5);
-        const int u = __ldcg(cur + i);
-        if (!((a.mask[u] >> k) & 1u)) continue;
-        const int v = u + sh.off[k];
-        if (!a.alive[v]) continue;
-        const unsigned long long ku = __ldcg(wide + i);
-        const int s = int(unsigned(ku));
-        int ux, uy, uz, qx, qy, qz;
-        unpack3(__ldcg(side_u + i), ux, uy, uz);
-        unpack3(__ldcg(side_s + i), qx, qy, qz);
+      // step B: the offer of claimed u (key ku, positions (ux, uy, uz) and its source's, the
+      // source's reach) to its k-th neighbour; distance and reach checks come before the read of
+      // the neighbour's liveness (all three only filter)
+      auto offer = [&](int u, unsigned long long ku, int k, int ux, int uy, int uz, int qx, int qy, int qz, float rs) {
         const float d = distance_to(a, ux + c_dx[k], uy + c_dy[k], uz + c_dz[k], qx, qy, qz);
-        if (d >= reach(a, s)) continue;
+        if (d >= rs) return;
+        const int v = u + sh.off[k];
+        if (!a.alive[v]) return;
+        const int s = int(unsigned(ku));
         unsigned mb = __float_as_uint(d);
         const unsigned mu = unsigned(ku >> 32);
         if (mb < mu) mb = mu;
@@ -602,6 +649,68 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
         } else if (__ldcg(a.key + v) == BK_UNCLAIMED) {
           if (!(atomicOr(a.flags + v, kWaiting) & kWaiting)) far[atomicAdd(&L->n_far, 1)] = v;
         }
+      };
+      int lo, hi_i;
+      if (own_share<C>(nc, kInvalStage, lo, hi_i)) {
+        // step A: the round boundary's key of each frontier voxel, its mask, both positions and
+        // the source's reach, in this CTA's shared memory
+        unsigned long long *skey = reinterpret_cast<unsigned long long *>(stage_bytes());
+        unsigned long long *spu = skey + kInvalStage, *sps = spu + kInvalStage;
+        int *su = reinterpret_cast<int *>(sps + kInvalStage);
+        unsigned *smask = reinterpret_cast<unsigned *>(su + kInvalStage);
+        float *sreach = reinterpret_cast<float *>(smask + kInvalStage);
+        for (int i = lo + int(threadIdx.x); i < hi_i; i += blockDim.x) {
+          const int u = __ldcg(cur + i);
+          const unsigned long long k = __ldcg(a.key + u);
+          atomicAnd(a.flags + u, ~kFront);
+          const int q = i - lo;
+          su[q] = u;
+          skey[q] = k;
+          smask[q] = a.mask[u];
+          sreach[q] = reach(a, int(unsigned(k)));
+          int x, y, z;
+          unravel3(u - sh.a0, sh.sx, sh.sy, x, y, z);
+          spu[q] = pack3(x, y, z);
+          unravel3(int(unsigned(k)) - sh.a0, sh.sx, sh.sy, x, y, z);
+          sps[q] = pack3(x, y, z);
+        }
+        G::sync();
+        for (int j = threadIdx.x; j < (hi_i - lo) * 32; j += blockDim.x) {
+          const int k = j & 31;
+          if (k >= 26) continue;
+          const int q = j >> 5;
+          if (!((smask[q] >> k) & 1u)) continue;
+          int ux, uy, uz, qx, qy, qz;
+          unpack3(spu[q], ux, uy, uz);
+          unpack3(sps[q], qx, qy, qz);
+          offer(su[q], skey[q], k, ux, uy, uz, qx, qy, qz, sreach[q]);
+        }
+      } else {
+        // step A: the round boundary's key of each frontier voxel, and both positions
+        for (int i = G::tid(); i < nc; i += G::threads()) {
+          const int u = __ldcg(cur + i);
+          const unsigned long long k = __ldcg(a.key + u);
+          atomicAnd(a.flags + u, ~kFront);
+          wide[i] = k;
+          int x, y, z;
+          unravel3(u - sh.a0, sh.sx, sh.sy, x, y, z);
+          side_u[i] = pack3(x, y, z);
+          unravel3(int(unsigned(k)) - sh.a0, sh.sx, sh.sy, x, y, z);
+          side_s[i] = pack3(x, y, z);
+        }
+        G::sync();
+        for (long long j = G::tid(); j < (long long)nc * 32; j += G::threads()) {
+          const int k = int(j & 31);
+          if (k >= 26) continue;
+          const int i = int(j >> 5);
+          const int u = __ldcg(cur + i);
+          if (!((a.mask[u] >> k) & 1u)) continue;
+          const unsigned long long ku = __ldcg(wide + i);
+          int ux, uy, uz, qx, qy, qz;
+          unpack3(__ldcg(side_u + i), ux, uy, uz);
+          unpack3(__ldcg(side_s + i), qx, qy, qz);
+          offer(u, ku, k, ux, uy, uz, qx, qy, qz, reach(a, int(unsigned(ku))));
+        }
       }
       G::sync();
     }
@@ -611,46 +720,23 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
     // band boundary: every waiting voxel pulls the best offer of its claimed neighbours
     if (threadIdx.x == 0) sh.lowest = BK_INF_BITS;
     if (G::first()) L->n_keep = 0;
-    for (int i = G::tid(); i < nf; i += G::threads()) {
-      const int c = __ldcg(far + i);
-      wide[i] = __ldcg(a.key + c) != BK_UNCLAIMED ? kClaimedMark : BK_UNCLAIMED;
-      int x, y, z;
-      unravel3(c - sh.a0, sh.sx, sh.sy, x, y, z);
-      side_u[i] = pack3(x, y, z);
-    }
-    G::sync();
-    for (long long j = G::tid(); j < (long long)nf * 32; j += G::threads()) {
-      const int k = int(j & 31);
-      if (k >= 26) continue;
-      const int i = int(j >> 5);
-      if (__ldcg(wide + i) == kClaimedMark) continue;
-      const int c = __ldcg(far + i);
-      if (!((a.mask[c] >> k) & 1u)) continue;
-      const unsigned long long ku = __ldcg(a.key + c + sh.off[k]);
-      if (ku == BK_UNCLAIMED) continue;
+    // the offer of claimed neighbour key ku to waiting voxel c at (x, y, z), or ~0
+    auto pull = [&](unsigned long long ku, int x, int y, int z) -> unsigned long long {
       const int s = int(unsigned(ku));
-      int x, y, z, qx, qy, qz;
-      unpack3(__ldcg(side_u + i), x, y, z);
+      int qx, qy, qz;
       unravel3(s - sh.a0, sh.sx, sh.sy, qx, qy, qz);
       const float d = distance_to(a, x, y, z, qx, qy, qz);
-      if (d >= reach(a, s)) continue;
+      if (d >= reach(a, s)) return ~0ull;
       unsigned mb = __float_as_uint(d);
       const unsigned mu = unsigned(ku >> 32);
       if (mb < mu) mb = mu;
-      atomicMin(wide + i, (static_cast<unsigned long long>(mb) << 32) | unsigned(s));
       atomicMin(&sh.lowest, mb);
-    }
-    G::sync();
-    const unsigned lowest = G::min_over(&sh.lowest);
-    if (lowest != BK_INF_BITS) band = band_of(lowest, a.delta, band + 1);
-    hi = __float_as_uint(__fmul_rn(float(band + 1), a.delta));
-    int *cur = (r & 1) ? B : A;
-    int *cur_count = &L->cnt[r % 3];
-    for (int i = G::tid(); i < nf; i += G::threads()) {
-      const int c = __ldcg(far + i);
-      const unsigned long long b = __ldcg(wide + i);
-      if (b == kClaimedMark) continue;
-      if (b == BK_UNCLAIMED) { atomicAnd(a.flags + c, ~kWaiting); continue; }
+      return (static_cast<unsigned long long>(mb) << 32) | unsigned(s);
+    };
+    // claim the waiting voxel c with best offer b inside the new band, or keep it waiting
+    auto settle = [&](int c, unsigned long long b, int *cur, int *cur_count) {
+      if (b == kClaimedMark) return;
+      if (b == BK_UNCLAIMED) { atomicAnd(a.flags + c, ~kWaiting); return; }
       if (unsigned(b >> 32) < hi) {
         a.key[c] = b;
         touched[atomicAdd(&L->n_touch, 1)] = c;
@@ -660,6 +746,73 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
       } else {
         keep[atomicAdd(&L->n_keep, 1)] = c;
       }
+    };
+    int lo, hi_f;
+    if (own_share<C>(nf, kBandStage, lo, hi_f)) {
+      // this CTA's waiting voxels in shared memory: nothing writes a key before the claims, which
+      // come after a group barrier, so the pulls only wait for this CTA's staging
+      unsigned long long *sbest = reinterpret_cast<unsigned long long *>(stage_bytes());
+      unsigned long long *spc = sbest + kBandStage;
+      int *sc = reinterpret_cast<int *>(spc + kBandStage);
+      unsigned *smask = reinterpret_cast<unsigned *>(sc + kBandStage);
+      for (int i = lo + int(threadIdx.x); i < hi_f; i += blockDim.x) {
+        const int c = __ldcg(far + i);
+        const int q = i - lo;
+        sc[q] = c;
+        sbest[q] = __ldcg(a.key + c) != BK_UNCLAIMED ? kClaimedMark : BK_UNCLAIMED;
+        smask[q] = a.mask[c];
+        int x, y, z;
+        unravel3(c - sh.a0, sh.sx, sh.sy, x, y, z);
+        spc[q] = pack3(x, y, z);
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < (hi_f - lo) * 32; j += blockDim.x) {
+        const int k = j & 31;
+        if (k >= 26) continue;
+        const int q = j >> 5;
+        if (sbest[q] == kClaimedMark || !((smask[q] >> k) & 1u)) continue;
+        const unsigned long long ku = __ldcg(a.key + sc[q] + sh.off[k]);
+        if (ku == BK_UNCLAIMED) continue;
+        int x, y, z;
+        unpack3(spc[q], x, y, z);
+        const unsigned long long o = pull(ku, x, y, z);
+        if (o != ~0ull) atomicMin(sbest + q, o);
+      }
+      G::sync();
+      const unsigned lowest = G::min_over(&sh.lowest);
+      if (lowest != BK_INF_BITS) band = band_of(lowest, a.delta, band + 1);
+      hi = __float_as_uint(__fmul_rn(float(band + 1), a.delta));
+      int *cur = (r & 1) ? B : A;
+      for (int i = lo + int(threadIdx.x); i < hi_f; i += blockDim.x) settle(sc[i - lo], sbest[i - lo], cur, &L->cnt[r % 3]);
+    } else {
+      for (int i = G::tid(); i < nf; i += G::threads()) {
+        const int c = __ldcg(far + i);
+        wide[i] = __ldcg(a.key + c) != BK_UNCLAIMED ? kClaimedMark : BK_UNCLAIMED;
+        int x, y, z;
+        unravel3(c - sh.a0, sh.sx, sh.sy, x, y, z);
+        side_u[i] = pack3(x, y, z);
+      }
+      G::sync();
+      for (long long j = G::tid(); j < (long long)nf * 32; j += G::threads()) {
+        const int k = int(j & 31);
+        if (k >= 26) continue;
+        const int i = int(j >> 5);
+        if (__ldcg(wide + i) == kClaimedMark) continue;
+        const int c = __ldcg(far + i);
+        if (!((a.mask[c] >> k) & 1u)) continue;
+        const unsigned long long ku = __ldcg(a.key + c + sh.off[k]);
+        if (ku == BK_UNCLAIMED) continue;
+        int x, y, z;
+        unpack3(__ldcg(side_u + i), x, y, z);
+        const unsigned long long o = pull(ku, x, y, z);
+        if (o != ~0ull) atomicMin(wide + i, o);
+      }
+      G::sync();
+      const unsigned lowest = G::min_over(&sh.lowest);
+      if (lowest != BK_INF_BITS) band = band_of(lowest, a.delta, band + 1);
+      hi = __float_as_uint(__fmul_rn(float(band + 1), a.delta));
+      int *cur = (r & 1) ? B : A;
+      for (int i = G::tid(); i < nf; i += G::threads()) settle(__ldcg(far + i), __ldcg(wide + i), cur, &L->cnt[r % 3]);
     }
     G::sync();
     if (G::first()) L->n_far = L->n_keep;

@@ -1,12 +1,23 @@
 #pragma once
 #include <cstdint>
+#include <vector>
 
 #include "runtime.hpp"
 
 namespace bk {
-// Voxels of every object (rank[id] >= 0), grouped by object rank and ascending in flat index.
-Buffer<int> object_voxels(Context &ctx, const uint32_t *ids, long long n, const int *rank, int nobj, long long total);
-// Per object [begin, end): its voxels by descending DAF (inf -> 0), ties -> higher flat first.
-Buffer<int> target_orders(Context &ctx, const int *vox, const float *daf, long long total, const int *begin,
-                          const int *end, int nobj);
+// A volume's range [begin, end) of the arena, and where its id -> object table starts.
+struct ArenaVolume {
+  long long begin, end;
+  int id_base;
+};
+// Voxels of every object over all volumes of the arena in one selection and one sort: grouped by
+// global object index (object_of[id_base + id] >= 0), ascending in arena flat index. The picked
+// voxels are also marked in `alive` (zeroed by the caller). `total` is the objects' voxel count.
+Buffer<int> arena_object_voxels(Context &ctx, const uint32_t *ids, long long n, const std::vector<ArenaVolume> &volumes,
+                                const std::vector<int> &object_of, int nobj, long long total, uint8_t *alive);
+// Per object (voxels [begin[o], begin[o+1]) of the list, the last to `total`): its voxels by
+// descending DAF (inf -> 0), ties -> higher flat first. `largest` is the largest object's voxel
+// count; `wide` forces the (32, 64)-bit key even where 64 bits would hold it.
+Buffer<int> target_orders(Context &ctx, const int *vox, const float *daf, long long total, const int *begin, int nobj,
+                          long long largest, bool wide = false);
 }  // namespace bk

@@ -33,18 +33,6 @@ __global__ void filter_labels(const L *in, L *out, long long n, const long long 
   out[i] = (lo < count && ids[lo] == v) ? in[i] : L(0);
 }
 
-__global__ void init_alive(const uint32_t *ids, const int *rank, long long n, uint8_t *alive) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t id = ids[i];
-  alive[i] = (id != 0 && rank[id] >= 0) ? 1 : 0;
-}
-
-__global__ void offset_voxels(int *vox, long long n, int offset) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) vox[i] += offset;
-}
-
 // Compacts the used prefix of every object's store region.
 __global__ void gather_store(const int *store, const long long *store_begin, const long long *dst_begin,
                              const int *nstore, int nobj, int *out) {
@@ -264,7 +252,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   }
   std::vector<int> after_begin(nobj), after_count(nobj), after;
   // per object: voxel range, arena, border root, manual targets, path budget, store regions
-  std::vector<int> obj_begin(nobj), obj_count(nobj), obj_arena(nobj), border_root(nobj, -1), seg_end(nobj);
+  std::vector<int> obj_begin(nobj), obj_count(nobj), obj_arena(nobj), border_root(nobj, -1);
   std::vector<float> M(nobj);
   std::vector<int> manual_begin(nobj), manual_count(nobj), manual;
   std::vector<long long> max_paths(nobj), store_begin(nobj), store_cap(nobj), rec_begin(nobj), rec_cap(nobj);
@@ -275,7 +263,6 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     obj_begin[o] = int(F);
     obj_count[o] = int(ob.count);
     F += ob.count;
-    seg_end[o] = int(F);
     obj_arena[o] = ob.volume;
     M[o] = float(1.0 / std::pow(double(st.dbf_max[ob.id]), 1.01));
     const auto &b = st.borders[ob.id];
@@ -304,29 +291,6 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     rec_total += rec_cap[o];
   }
   if (F >= (1LL << 31)) throw std::invalid_argument("too many foreground voxels");
-  // object voxel lists, volume by volume into their ranges
-  Buffer<int> vox(ctx, F);
-  for (size_t v = 0; v < vs.size(); ++v) {
-    auto &st = vs[v];
-    if (st.empty) continue;
-    int first = -1, cnt = 0;
-    long long total = 0;
-    for (int64_t id = 1; id <= st.cc.count; ++id)
-      if (st.object_of[id] >= 0) {
-        if (first < 0) first = st.object_of[id];
-        ++cnt;
-        total += obj_count[st.object_of[id]];
-      }
-    if (cnt == 0) continue;
-    std::vector<int> rank(st.cc.count + 1, -1);
-    for (int64_t id = 1; id <= st.cc.count; ++id)
-      if (st.object_of[id] >= 0) rank[id] = st.object_of[id] - first;
-    Buffer<int> drank = to_device(ctx, rank);
-    Buffer<int> local = object_voxels(ctx, ids.data() + st.offset, st.d.n(), drank.data(), cnt, total);
-    offset_voxels<<<blocks_for(total), 256, 0, s>>>(local.data(), total, int(st.offset)); ++ctx.launches;
-    BK_CUDA(cudaMemcpyAsync(vox.data() + obj_begin[first], local.data(), total * sizeof(int), cudaMemcpyDeviceToDevice, s));
-  }
-  clock.mark("object_voxels");
   // global per-voxel state
   Buffer<float> pdrf(ctx, N), dist(ctx, N), daf(ctx, N);
   Buffer<uint32_t> flags(ctx, N);
@@ -338,19 +302,21 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   flags.zero();
   alive.zero();
   key.fill_bytes(0xFF);
-  {
-    // alive: voxels of objects
-    std::vector<int> active_rank;
-    for (size_t v = 0; v < vs.size(); ++v) {
-      auto &st = vs[v];
-      if (st.empty) continue;
-      std::vector<int> r(st.cc.count + 1, -1);
-      for (int64_t id = 1; id <= st.cc.count; ++id) r[id] = st.object_of[id];
-      Buffer<int> dr = to_device(ctx, r);
-      init_alive<<<blocks_for(st.d.n()), 256, 0, s>>>(ids.data() + st.offset, dr.data(), st.d.n(), alive.data() + st.offset); ++ctx.launches;
-      BK_CUDA(cudaGetLastError());
-    }
+  // object voxel lists of all volumes at once (grouped by global object index), marking them alive
+  std::vector<ArenaVolume> listed;
+  std::vector<int> object_table;
+  for (size_t v = 0; v < vs.size(); ++v) {
+    auto &st = vs[v];
+    if (st.empty) continue;
+    bool any = false;
+    for (int64_t id = 1; id <= st.cc.count && !any; ++id) any = st.object_of[id] >= 0;
+    if (!any) continue;
+    listed.push_back({st.offset, st.offset + st.d.n(), int(object_table.size())});
+    object_table.push_back(-1);  // id 0
+    object_table.insert(object_table.end(), st.object_of.begin() + 1, st.object_of.begin() + 1 + st.cc.count);
   }
+  Buffer<int> vox = arena_object_voxels(ctx, ids.data(), N, listed, object_table, nobj, F, alive.data());
+  clock.mark("object_voxels");
   std::vector<int> arena_offset(vs.size()), arena_dims(3 * vs.size());
   for (size_t v = 0; v < vs.size(); ++v) {
     arena_offset[v] = int(vs[v].offset);
@@ -370,7 +336,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   const int nbig_trace = leading("BROOK_B200_TRACE_CLUSTER_VOXELS", trace_cluster_voxels(F));
   auto d_arena_offset = to_device(ctx, arena_offset), d_arena_dims = to_device(ctx, arena_dims);
   auto d_obj_arena = to_device(ctx, obj_arena), d_obj_begin = to_device(ctx, obj_begin), d_obj_count = to_device(ctx, obj_count);
-  auto d_seg_end = to_device(ctx, seg_end), d_schedule = to_device(ctx, schedule), d_border_root = to_device(ctx, border_root);
+  auto d_schedule = to_device(ctx, schedule), d_border_root = to_device(ctx, border_root);
   auto d_M = to_device(ctx, M);
   auto d_manual_begin = to_device(ctx, manual_begin), d_manual_count = to_device(ctx, manual_count);
   auto d_manual = to_device(ctx, manual.empty() ? std::vector<int>{0} : manual);
@@ -424,7 +390,9 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       if (f) { std::fwrite(item.second->data(), sizeof(float), item.second->size(), f); std::fclose(f); }
     }
   }
-  Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), d_seg_end.data(), nobj);
+  const bool wide_order = std::getenv("BROOK_B200_WIDE_ORDER_KEY") != nullptr;  // test knob: the 96-bit key path
+  Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), nobj,
+                                    nobj ? obj_count[schedule[0]] : 0, wide_order);
   a.order = order.data();
   BK_CUDA(cudaMemsetAsync(queue.data(), 0, 2 * sizeof(int), s));
   clock.mark("order");

@@ -84,6 +84,17 @@ def test_cluster_and_lone_cta_paths_match_oracle(gpu, monkeypatch, cluster_voxel
     assert_same(got, exp, f"cluster threshold {cluster_voxels}")
 
 
+def test_wide_target_order_key_matches_oracle(gpu, monkeypatch):
+    """The (32, 64)-bit target-order sort key, used when object, DAF and position need > 64 bits."""
+    from brook_b200 import synthetic
+
+    monkeypatch.setenv("BROOK_B200_WIDE_ORDER_KEY", "1")
+    labels = synthetic.tube_volume((96, 96, 96), objects=12, seed=3)
+    got, exp = run_both(labels, teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    assert len(got) == 12
+    assert_same(got, exp, "wide order key")
+
+
 @pytest.mark.parametrize("dtype", [np.uint8, np.uint16, np.uint64, np.int32, np.int64])
 def test_dtypes(gpu, dtype):
     from brook_b200 import synthetic
