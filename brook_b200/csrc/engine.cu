@@ -240,9 +240,9 @@ __device__ bool flood_geometric(const EngineArgs &a, Shared &sh, Shared *L, floa
         se[i - lo] = (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u];
       }
       G::sync();
-      for (int j = threadIdx.x; j < (hi - lo) * 32; j += blockDim.x) {
-        const int k = j & 31;
-        if (k < 26) relax(se[j >> 5], su[j >> 5], k);
+      for (int j = threadIdx.x; j < (hi - lo) * 26; j += blockDim.x) {
+        const int q = j / 26;
+        relax(se[q], su[q], j - 26 * q);
       }
     } else {
       for (int i = G::tid(); i < nc; i += G::threads()) {
@@ -423,15 +423,9 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
         const bool expand = fu != 0.0f && du <= Tb;
         return expand ? (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u] : 0ull;
       };
-      // step B: one (voxel, neighbour) item
-      auto relax = [&](unsigned long long e, int u, int k) {
-        if (!((unsigned(e) >> k) & 1u)) return;
-        const int v = u + sh.off[k];
-        const float du = __uint_as_float(unsigned(e >> 32));
-        const float fv = a.pdrf[v];
-        const float cand = vw_step(du, fv);
-        const float old = atomic_min_pos(a.dist + v, cand);
-        if (old > cand) {
+      // step B, after the improvement of v to cand (from old)
+      auto improved = [&](int v, float cand, float fv, float old) {
+        {
           if (old == inf()) touched[atomicAdd(&L->n_touch, 1)] = v;
           if (fv == 0.0f) atomicMin(&sh.rb, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | unsigned(v));
           const unsigned long long rb = vload(&sh.rb);
@@ -444,6 +438,15 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
           }
         }
       };
+      // step B: one (voxel, neighbour) item
+      auto relax = [&](unsigned long long e, int u, int k) {
+        if (!((unsigned(e) >> k) & 1u)) return;
+        const int v = u + sh.off[k];
+        const float fv = a.pdrf[v];
+        const float cand = vw_step(__uint_as_float(unsigned(e >> 32)), fv);
+        const float old = atomic_min_pos(a.dist + v, cand);
+        if (old > cand) improved(v, cand, fv, old);
+      };
       int lo, hi;
       if (own_share<C>(nc, kFloodStage, lo, hi)) {
         unsigned long long *se = reinterpret_cast<unsigned long long *>(stage_bytes());
@@ -454,9 +457,9 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
           se[i - lo] = stage(u);
         }
         G::sync();
-        for (int j = threadIdx.x; j < (hi - lo) * 32; j += blockDim.x) {
-          const int k = j & 31;
-          if (k < 26) relax(se[j >> 5], su[j >> 5], k);
+        for (int j = threadIdx.x; j < (hi - lo) * 26; j += blockDim.x) {
+          const int q = j / 26;
+          relax(se[q], su[q], j - 26 * q);
         }
       } else {
         for (int i = G::tid(); i < nc; i += G::threads()) wide[i] = stage(__ldcg(cur + i));
@@ -675,10 +678,8 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
           sps[q] = pack3(x, y, z);
         }
         G::sync();
-        for (int j = threadIdx.x; j < (hi_i - lo) * 32; j += blockDim.x) {
-          const int k = j & 31;
-          if (k >= 26) continue;
-          const int q = j >> 5;
+        for (int j = threadIdx.x; j < (hi_i - lo) * 26; j += blockDim.x) {
+          const int q = j / 26, k = j - 26 * q;
           if (!((smask[q] >> k) & 1u)) continue;
           int ux, uy, uz, qx, qy, qz;
           unpack3(spu[q], ux, uy, uz);
@@ -766,10 +767,8 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
         spc[q] = pack3(x, y, z);
       }
       __syncthreads();
-      for (int j = threadIdx.x; j < (hi_f - lo) * 32; j += blockDim.x) {
-        const int k = j & 31;
-        if (k >= 26) continue;
-        const int q = j >> 5;
+      for (int j = threadIdx.x; j < (hi_f - lo) * 26; j += blockDim.x) {
+        const int q = j / 26, k = j - 26 * q;
         if (sbest[q] == kClaimedMark || !((smask[q] >> k) & 1u)) continue;
         const unsigned long long ku = __ldcg(a.key + sc[q] + sh.off[k]);
         if (ku == BK_UNCLAIMED) continue;
