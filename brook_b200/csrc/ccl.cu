@@ -5,7 +5,8 @@
 // numbering (ccl.cu:25-63 of giorgioangel/brook) without its host sort.
 //
 // The union runs in two kernels: tile_union labels 32x8x8 tiles in shared memory (labels staged
-// once, union-find on shared indices; a tile's order is the volume's, so a tile root is its
+// once, each x run of equal labels linked to its first voxel by a warp ballot, then union-find
+// with path halving on shared indices; a tile's order is the volume's, so a tile root is its
 // component's lowest flat index in the tile) and writes every voxel's tile root as its parent;
 // face_union then unites only the pairs that cross a tile face, on the global parent array.
 #include <cub/cub.cuh>
@@ -71,9 +72,16 @@ __device__ __forceinline__ bool skipped(int dx, int dy, int dz, Same same) {
   return false;
 }
 
-__device__ __forceinline__ int tile_find(const int *par, int i) {
+// Root of i in the tile's shared forest, with path halving (the same benign races as find_root).
+__device__ __forceinline__ int tile_find(int *par, int i) {
   int p = par[i];
-  while (p != i) { i = p; p = par[i]; }
+  while (p != i) {
+    const int g = par[p];
+    if (g == p) return p;
+    par[i] = g;
+    i = g;
+    p = par[i];
+  }
   return i;
 }
 
@@ -98,11 +106,18 @@ __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__
   __shared__ int par[kTileN];
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z0 = blockIdx.z * kTileZ;
   const int ex = min(kTileX, d.sx - x0), ey = min(kTileY, d.sy - y0), ez = min(kTileZ, d.sz - z0);
+  // a tile row is one warp (kTileX == 32): every voxel starts under the first voxel of its run of
+  // equal labels along x, so the x-face pairs are united without a find
+  static_assert(kTileX == 32 && kTileThreads % 32 == 0, "a tile row is one warp");
   for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
     const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
     const bool in = lx < ex && ly < ey && lz < ez;
-    lab[t] = in ? labels[(x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz))] : L(0);
-    par[t] = t;
+    const L lv = in ? labels[(x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz))] : L(0);
+    lab[t] = lv;
+    const L left = __shfl_up_sync(0xFFFFFFFFu, lv, 1);
+    const bool joins = lx > 0 && lv != L(0) && left == lv;
+    const unsigned starts = __ballot_sync(0xFFFFFFFFu, !joins);
+    par[t] = t - lx + (31 - __clz(starts & (0xFFFFFFFFu >> (31 - lx))));
   }
   __syncthreads();
   for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
@@ -114,6 +129,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__
     for (int k = 0; k < 26; ++k) {
       const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
       if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
+      if (dy == 0 && dz == 0) continue;  // the x run, linked at load
       if (planar && dz != 0) continue;
       const int nx = lx + dx, ny = ly + dy, nz = lz + dz;
       if (nx < 0 || ny < 0 || nx >= ex || ny >= ey || nz >= ez) continue;  // other tiles: face_union
@@ -155,10 +171,20 @@ __global__ void face_union(const L *labels, int *parent, Dims d, bool planar, lo
     const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
     if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
     if (planar && dz != 0) continue;
-    const bool crosses = lx + dx < 0 || lx + dx >= kTileX || ly + dy >= kTileY || ly + dy < 0 || lz + dz >= kTileZ;
-    if (!crosses) continue;
+    const bool cx = lx + dx < 0 || lx + dx >= kTileX, cy = ly + dy < 0 || ly + dy >= kTileY, cz = lz + dz >= kTileZ;
+    if (!(cx || cy || cz)) continue;
     if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
-    unite(parent, int(base + i), int(base + i) + nbr_offset(k, d));
+    // The pair one step back along an axis the pair does not cross, with both ends still inside
+    // their tiles, joins the same two tile components (each end is tied to its step-back voxel
+    // inside its tile) and is itself united or skipped by this rule further back; so a pair whose
+    // step-back ends both carry the label adds nothing.
+    long long back = 0;
+    if (!cx && lx >= 1 && lx + dx >= 1) back = 1;
+    else if (!cy && ly >= 1 && ly + dy >= 1) back = d.sx;
+    else if (!planar && !cz && lz >= 1 && lz + dz >= 1) back = (long long)d.sx * d.sy;
+    const long long q = i + nbr_offset(k, d);
+    if (back && labels[i - back] == lv && labels[q - back] == lv) continue;
+    unite(parent, int(base + i), int(base + q));
   }
 }
 

@@ -253,6 +253,67 @@ def test_c_abi_known_answers(gpu):
     assert lib.brook_last_error()
 
 
+def _components_by_first_voxel(labels):
+    """26-connected components of every label (scipy), numbered 1..K by ascending first voxel in
+    Fortran order: the canonical numbering of brook.h:169-177."""
+    from scipy import ndimage
+
+    shape = labels.shape
+    comps = []
+    for value in np.unique(labels):
+        if value == 0:
+            continue
+        lab, count = ndimage.label(labels == value, structure=np.ones((3, 3, 3), bool))
+        flat = lab.ravel(order="F")
+        idx = np.nonzero(flat)[0]
+        first = np.full(count + 1, flat.size, np.int64)
+        np.minimum.at(first, flat[idx], idx)
+        for c in range(1, count + 1):
+            comps.append((int(first[c]), (lab == c), int(value)))
+    comps.sort(key=lambda t: t[0])
+    ids = np.zeros(shape, np.int64)
+    for k, (_, where, _) in enumerate(comps, start=1):
+        ids[where] = k
+    return ids, [t[0] for t in comps], [t[2] for t in comps]
+
+
+@pytest.mark.parametrize("shape,blob", [((70, 45, 37), 3), ((33, 9, 17), 1), ((128, 16, 24), 6), ((5, 300, 4), 2), ((40, 24, 20), 0)])
+def test_connected_components_match_scipy(gpu, shape, blob):
+    """Component ids, roots and labels of blobby random labels with noise, on sizes that are not
+    multiples of the 32x8x8 union tiles, against scipy's 26-connected labelling."""
+    from scipy import ndimage
+    from brook_b200 import _native as n
+
+    rng = np.random.default_rng(sum(shape) + blob)
+    field = ndimage.gaussian_filter(rng.random((5,) + shape), sigma=(0, blob, blob, blob))
+    labels = (np.argmax(field, axis=0) + 1).astype(np.uint64) * 1000003
+    labels[rng.random(shape) < 0.15] = 0
+    labels = np.asfortranarray(labels)
+    expected, roots_expected, values = _components_by_first_voxel(labels)
+    lib = n.lib
+    ctx = n.context(0)
+    vol = n.host_volume(labels)
+    cc = ctypes.c_void_p()
+    n.check(lib.brook_connected_components(ctx, ctypes.byref(vol), ctypes.byref(cc)))
+    view = n.Volume()
+    mapping = ctypes.POINTER(ctypes.c_int64)()
+    roots = ctypes.POINTER(ctypes.c_int64)()
+    count = ctypes.c_size_t()
+    n.check(lib.brook_components_view(cc, ctypes.byref(view), ctypes.byref(mapping), ctypes.byref(roots),
+                                      ctypes.byref(count)))
+    k = count.value
+    assert k == len(roots_expected)
+    dtype = np.uint8 if k <= 0xFF else np.uint16 if k <= 0xFFFF else np.uint32
+    out = np.zeros(labels.size, dtype)
+    n.check(lib.brook_components_copy_to_host(cc, out.ctypes.data, out.nbytes))
+    got_roots = [roots[i] for i in range(k)]
+    got_values = [mapping[i + 1] for i in range(k)]
+    lib.brook_components_destroy(cc)  # the view's arrays end with the handle
+    np.testing.assert_array_equal(out.reshape(shape, order="F").astype(np.int64), expected)
+    assert got_roots == roots_expected
+    assert got_values == values
+
+
 def test_c_abi_device_output(gpu):
     """BROOK_DEVICE_OUTPUT (brook.h:96-102, 232-233): the device view and array handles hold the
     same skeletons as the host route; get_view copies a device result to the host; a host result
