@@ -79,70 +79,105 @@ __global__ void edt_x(const uint32_t *__restrict__ ids, float *__restrict__ D, D
 }
 
 // One line of the y or z pass: n voxels from `base` with `stride`. Stacks V/H/Z are interleaved:
-// entry k of this thread's stack is at [k * pitch].
+// entry k of this thread's stack is at [k * pitch]. One streaming sweep: ids and heights are read
+// four voxels ahead of use (independent loads, so their latency overlaps the envelope work), a run
+// ends where the id changes, and the top of the stack is kept in registers, so that only a pop
+// reads the stack back from memory. The envelope is the reference's per run: parabolas are
+// placed in order with the same float64 operations, and the fill walks the stack forward.
 __device__ void envelope_line(const uint32_t *__restrict__ ids, float *__restrict__ D, long long base, long long stride,
                               int n, float w, int bb, int *V, float *H, double *Z, long long pitch, int finish) {
   const double w2 = (double)__fmul_rn(w, w);
-  int i = 0;
-  while (i < n) {
-    const uint32_t L = ids[base + (long long)i * stride];
-    int c = i, e = i;
-    while (e + 1 < n && ids[base + (long long)(e + 1) * stride] == L) ++e;
+  const float kInf = __uint_as_float(BK_INF_BITS);
+  int c = 0;        // first voxel of the current run
+  uint32_t L = 0;   // its id
+  int k = -1;       // stack top (-1: empty)
+  int vt = 0;       // the top entry, also in memory
+  float ht = 0.0f;
+  double zt = 0.0;
+  auto push = [&](int at, int v, float h, double z) {
+    V[(long long)at * pitch] = v; H[(long long)at * pitch] = h; Z[(long long)at * pitch] = z;
+    vt = v; ht = h; zt = z;
+  };
+  // the parabola of height ph at p joins the lower envelope
+  auto place = [&](int p, double ph) {
+    while (k >= 0) {
+      const double num = __dsub_rn(__fma_rn(__dmul_rn(w2, (double)p), (double)p, ph),
+                                   __fma_rn(__dmul_rn(w2, (double)vt), (double)vt, (double)ht));
+      const double sv = __ddiv_rn(num, __dmul_rn(__dmul_rn(2.0, w2), __dsub_rn((double)p, (double)vt)));
+      if (sv <= zt) {
+        if (--k >= 0) {
+          vt = V[(long long)k * pitch]; ht = H[(long long)k * pitch]; zt = Z[(long long)k * pitch];
+        }
+      } else {
+        ++k;
+        push(k, p, (float)ph, sv);
+        return;
+      }
+    }
+    k = 0;
+    push(0, p, (float)ph, -1e300);
+  };
+  // the run [c, e] ends; rightw: a wall follows it
+  auto finish_run = [&](int e, bool rightw) {
     if (L == 0) {
-      // A run's envelope only reads and writes the run itself, and background ends at 0: the
-      // background runs are skipped (the last pass writes their zeros).
       if (finish)
         for (int q = c; q <= e; ++q) D[base + (long long)q * stride] = 0.0f;
-      i = e + 1;
-      continue;
+      return;
     }
-    const bool leftw = c > 0 || bb, rightw = e < n - 1 || bb;
-    int k = -1;
-    if (leftw) { k = 0; V[0] = c - 1; H[0] = 0.0f; Z[0] = -1e300; }
-    for (int p = c; p <= e + 1; ++p) {
-      double ph;
-      if (p <= e) {
-        const float hf = D[base + (long long)p * stride];
-        if (!(hf < __uint_as_float(BK_INF_BITS))) continue;
-        ph = (double)hf;
-      } else {
-        if (!rightw) break;
-        ph = 0.0;
-      }
-      bool placed = false;
-      while (k >= 0 && !placed) {
-        const int vk = V[(long long)k * pitch];
-        const double num = __dsub_rn(__fma_rn(__dmul_rn(w2, (double)p), (double)p, ph),
-                                     __fma_rn(__dmul_rn(w2, (double)vk), (double)vk, (double)H[(long long)k * pitch]));
-        const double s = __ddiv_rn(num, __dmul_rn(__dmul_rn(2.0, w2), __dsub_rn((double)p, (double)vk)));
-        if (s <= Z[(long long)k * pitch]) --k;
-        else {
-          ++k;
-          V[(long long)k * pitch] = p; H[(long long)k * pitch] = (float)ph; Z[(long long)k * pitch] = s;
-          placed = true;
-        }
-      }
-      if (!placed) { k = 0; V[0] = p; H[0] = (float)ph; Z[0] = -1e300; }
-    }
+    if (rightw) place(e + 1, 0.0);
     if (k < 0) {
-      for (int q = c; q <= e; ++q) {
-        float v = __uint_as_float(BK_INF_BITS);
-        if (finish) v = L == 0 ? 0.0f : v;
-        D[base + (long long)q * stride] = v;
-      }
-    } else {
-      int kk = 0;
-      for (int q = c; q <= e; ++q) {
-        while (kk < k && Z[(long long)(kk + 1) * pitch] < (double)q) ++kk;
-        const int vk = V[(long long)kk * pitch];
-        const double dq = __dsub_rn((double)q, (double)vk);
-        float v = __double2float_rn(__fma_rn(__dmul_rn(w2, dq), dq, (double)H[(long long)kk * pitch]));
-        if (finish) v = L == 0 ? 0.0f : sqrtf(v);
-        D[base + (long long)q * stride] = v;
-      }
+      for (int q = c; q <= e; ++q) D[base + (long long)q * stride] = kInf;
+      return;
     }
-    i = e + 1;
+    // entry kk serves the voxels q up to Z[kk + 1] (the last entry: the rest); the next entry is
+    // read while this one's voxels are written
+    int q = c;
+    int vk = V[0];
+    float hk = H[0];
+    double zn = k > 0 ? Z[pitch] : 0.0;
+    for (int kk = 0; q <= e; ++kk) {
+      int vn = 0;
+      float hn = 0.0f;
+      double znn = 0.0;
+      if (kk < k) {
+        vn = V[(long long)(kk + 1) * pitch];
+        hn = H[(long long)(kk + 1) * pitch];
+        if (kk + 1 < k) znn = Z[(long long)(kk + 2) * pitch];
+      }
+      for (; q <= e && (kk == k || !(zn < (double)q)); ++q) {
+        const double dq = __dsub_rn((double)q, (double)vk);
+        float v = __double2float_rn(__fma_rn(__dmul_rn(w2, dq), dq, (double)hk));
+        if (finish) v = sqrtf(v);
+        D[base + (long long)q * stride] = v;
+      }
+      vk = vn; hk = hn; zn = znn;
+    }
+  };
+  auto step = [&](int p, uint32_t lab, float hf) {
+    if (p == 0 || lab != L) {
+      if (p > 0) finish_run(p - 1, true);
+      c = p;
+      L = lab;
+      k = -1;
+      if (L != 0 && (c > 0 || bb)) { k = 0; push(0, c - 1, 0.0f, -1e300); }
+    }
+    if (L != 0 && hf < kInf) place(p, (double)hf);
+  };
+  auto id_at = [&](int p) { return p < n ? ids[base + (long long)p * stride] : 0u; };
+  auto d_at = [&](int p) { return p < n ? D[base + (long long)p * stride] : 0.0f; };
+  uint32_t a0 = id_at(0), a1 = id_at(1), a2 = id_at(2), a3 = id_at(3);
+  float f0 = d_at(0), f1 = d_at(1), f2 = d_at(2), f3 = d_at(3);
+  for (int p = 0; p < n; p += 4) {
+    const uint32_t b0 = id_at(p + 4), b1 = id_at(p + 5), b2 = id_at(p + 6), b3 = id_at(p + 7);
+    const float g0 = d_at(p + 4), g1 = d_at(p + 5), g2 = d_at(p + 6), g3 = d_at(p + 7);
+    step(p, a0, f0);
+    if (p + 1 < n) step(p + 1, a1, f1);
+    if (p + 2 < n) step(p + 2, a2, f2);
+    if (p + 3 < n) step(p + 3, a3, f3);
+    a0 = b0; a1 = b1; a2 = b2; a3 = b3;
+    f0 = g0; f1 = g1; f2 = g2; f3 = g3;
   }
+  finish_run(n - 1, bb != 0);
 }
 
 // Line `line` of the y (axis 1) or z (axis 2) pass of a (sx, sy, sz) volume at `offset`.
