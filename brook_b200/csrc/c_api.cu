@@ -73,11 +73,32 @@ void require(bool ok, const char *what = "null brook argument") {
   if (!ok) throw std::invalid_argument(what);
 }
 
+// The slab copies of one staged volume: the events the main stream waits on before it reads a
+// slab. On release the host waits for the last one (the caller's buffer is borrowed for the call
+// only) and so does the main stream, so that the staged buffer goes back to the context's cache
+// (in the main stream's order) only after the copies into it.
+struct SlabCopies {
+  cudaStream_t main = nullptr;
+  bk::Slabs slabs;
+  ~SlabCopies() {
+    if (!slabs.empty()) {
+      cudaEventSynchronize(slabs.back().second);
+      cudaStreamWaitEvent(main, slabs.back().second, 0);
+    }
+    for (auto &s : slabs) cudaEventDestroy(s.second);
+  }
+};
+
 // A volume gathered into Fortran order on the device (or borrowed when it already is).
 struct Staged {
   bk::Buffer<unsigned char> owned;
   bk::DeviceVolume volume;
+  std::shared_ptr<SlabCopies> copies;  // released first: the main stream waits for the copies
 };
+
+// Host input in page-locked memory is copied in slabs of about this many bytes on the copy
+// stream; the components' tile unions start on each slab as it arrives.
+constexpr long long kSlabBytes = 64LL << 20;
 
 __global__ void gather_strided(const unsigned char *src, unsigned char *dst, int sx, int sy, int sz, long long s0,
                                long long s1, long long s2, int b) {
@@ -90,7 +111,9 @@ __global__ void gather_strided(const unsigned char *src, unsigned char *dst, int
   for (int k = 0; k < b; ++k) q[k] = p[k];
 }
 
-Staged stage(bk::Context &ctx, const brook_volume &v) {
+// slabs: host input may arrive by slabs (the caller reads it only through connected_components,
+// which waits per slab).
+Staged stage(bk::Context &ctx, const brook_volume &v, bool slabs = false) {
   require(v.struct_size >= sizeof(brook_volume) && v.abi_version == BROOK_ABI_VERSION, "incompatible brook_volume");
   require(v.dtype >= BROOK_U8 && v.dtype <= BROOK_I64, "integer labels required");
   for (int a = 0; a < 3; ++a) require(v.shape[a] >= 0 && v.shape[a] < (1LL << 31), "invalid volume shape");
@@ -124,7 +147,38 @@ Staged stage(bk::Context &ctx, const brook_volume &v) {
   }
   require(v.memory == BROOK_HOST, "invalid memory kind");
   st.owned = bk::Buffer<unsigned char>(ctx, n * b);
-  if (fortran) {
+  bool pinned = false;
+  if (fortran && slabs && n * b >= 2 * kSlabBytes && sz >= 16) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, v.data) == cudaSuccess) pinned = attr.type == cudaMemoryTypeHost;
+    else cudaGetLastError();
+  }
+  if (pinned) {
+    // planes per slab: a multiple of the union tiles' depth (8)
+    const long long plane = b * sx * sy;
+    const int per = int(std::max(8LL, (kSlabBytes / plane) / 8 * 8));
+    cudaStream_t copy = ctx.copy_stream();
+    st.copies = std::make_shared<SlabCopies>();
+    st.copies->main = s;
+    cudaEvent_t ready;  // the staged buffer may be a block the main stream used before
+    BK_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    BK_CUDA(cudaEventRecord(ready, s));
+    const cudaError_t waited = cudaStreamWaitEvent(copy, ready, 0);
+    cudaEventDestroy(ready);
+    BK_CUDA(waited);
+    for (int z0 = 0; z0 < int(sz); z0 += per) {
+      const int z1 = int(std::min<long long>(sz, z0 + per));
+      BK_CUDA(cudaMemcpyAsync(st.owned.data() + z0 * plane, static_cast<const unsigned char *>(v.data) + z0 * plane,
+                              (z1 - z0) * plane, cudaMemcpyHostToDevice, copy));
+      cudaEvent_t e;
+      BK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      const cudaError_t recorded = cudaEventRecord(e, copy);
+      if (recorded != cudaSuccess) cudaEventDestroy(e);
+      BK_CUDA(recorded);
+      st.copies->slabs.push_back({z1, e});
+    }
+    st.volume.slabs = &st.copies->slabs;
+  } else if (fortran) {
     BK_CUDA(cudaMemcpyAsync(st.owned.data(), v.data, n * b, cudaMemcpyHostToDevice, s));
   } else if (c_order) {
     bk::Buffer<unsigned char> raw(ctx, n * b);
@@ -234,7 +288,7 @@ brook_status skeletonize_many(brook_context *ctx, const brook_volume *volumes, s
     std::vector<Staged> staged;
     std::vector<bk::DeviceVolume> vols;
     for (size_t i = 0; i < count; ++i) {
-      staged.push_back(stage(ctx->value, volumes[i]));
+      staged.push_back(stage(ctx->value, volumes[i], true));
       vols.push_back(staged.back().volume);
     }
     auto results = bk::skeletonize(ctx->value, vols, options);

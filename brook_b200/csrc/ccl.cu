@@ -97,14 +97,14 @@ __device__ __forceinline__ void tile_unite(int *par, int a, int b) {
   }
 }
 
-// grid (x tiles, y tiles, z tiles); parent of every voxel of the tile = its tile root, as an index
-// of the flat space the volume starts at `base` in; background: -1.
+// grid (x tiles, y tiles, z tiles from tz0); parent of every voxel of the tile = its tile root, as
+// an index of the flat space the volume starts at `base` in; background: -1.
 template <class L>
 __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__ labels, int *parent, Dims d, bool planar,
-                                                           long long base) {
+                                                           long long base, int tz0) {
   __shared__ L lab[kTileN];
   __shared__ int par[kTileN];
-  const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z0 = blockIdx.z * kTileZ;
+  const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z0 = (tz0 + int(blockIdx.z)) * kTileZ;
   const int ex = min(kTileX, d.sx - x0), ey = min(kTileY, d.sy - y0), ez = min(kTileZ, d.sz - z0);
   // a tile row is one warp (kTileX == 32): every voxel starts under the first voxel of its run of
   // equal labels along x, so the x-face pairs are united without a find
@@ -150,11 +150,12 @@ __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__
 
 // Pairs that cross a tile face: from every voxel on a face a forward neighbour can cross (both x
 // faces, both y faces — dy = -1 comes with dz = +1 — and the high z face), the forward neighbours
-// in another tile.
+// in another tile; for the voxels [i0, i1) of the volume.
 template <class L>
-__global__ void face_union(const L *labels, int *parent, Dims d, bool planar, long long base) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n()) return;
+__global__ void face_union(const L *labels, int *parent, Dims d, bool planar, long long base, long long i0,
+                           long long i1) {
+  const long long i = i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
   int x, y, z;
   unravel((int)i, d, x, y, z);
   const int lx = x % kTileX, ly = y % kTileY, lz = z % kTileZ;
@@ -268,8 +269,36 @@ std::vector<ComponentsResult> connected_components(Context &ctx, const std::vect
     if (tiles.y > 65535 || tiles.z > 65535) throw std::invalid_argument("volume too large for the tiled union");
     for_dtype(v.dtype, v.labels, [&](auto labels) {
       using L = std::remove_const_t<std::remove_pointer_t<decltype(labels)>>;
-      tile_union<L><<<tiles, kTileThreads, 0, s>>>(labels, parent.data(), d, planar, v.offset); ++ctx.launches;
-      face_union<L><<<blocks_for(v.d.n()), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset); ++ctx.launches;
+      if (!v.slabs) {
+        tile_union<L><<<tiles, kTileThreads, 0, s>>>(labels, parent.data(), d, planar, v.offset, 0); ++ctx.launches;
+        face_union<L><<<blocks_for(v.d.n()), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset, 0, v.d.n());
+        ++ctx.launches;
+        return;
+      }
+      // labels still arriving by slabs: each slab's tiles once it is there; the cross-tile pairs
+      // of a slab once the next slab (its +z neighbours) is there too
+      const long long plane = (long long)d.sx * d.sy;
+      int z_done = 0, z_pending = 0;  // planes united within tiles; first plane without face pairs
+      for (const auto &slab : *v.slabs) {
+        BK_CUDA(cudaStreamWaitEvent(s, slab.second, 0));
+        const int z_end = slab.first;
+        const int tz0 = z_done / kTileZ, tz1 = (z_end + kTileZ - 1) / kTileZ;
+        if (tz1 > tz0) {
+          tile_union<L><<<dim3(tiles.x, tiles.y, unsigned(tz1 - tz0)), kTileThreads, 0, s>>>(labels, parent.data(), d,
+                                                                                             planar, v.offset, tz0);
+          ++ctx.launches;
+        }
+        z_done = z_end;
+        // planes [z_pending, z_end - 1): their +z neighbours have arrived
+        const int z_ready = z_end == d.sz ? d.sz : z_end - 1;
+        if (z_ready > z_pending) {
+          const long long i0 = z_pending * plane, i1 = z_ready * plane;
+          face_union<L><<<blocks_for(i1 - i0), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset, i0, i1);
+          ++ctx.launches;
+          z_pending = z_ready;
+        }
+      }
+      if (z_done != d.sz || z_pending != d.sz) throw std::logic_error("slabs do not cover the volume");
     });
   }
   flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;

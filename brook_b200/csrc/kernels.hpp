@@ -31,11 +31,16 @@ ComponentsResult connected_components(Context &ctx, const void *labels, int dtyp
                                       bool planar = false);
 // The same for several volumes laid out back to back in one flat space (offsets in order, no
 // gaps): ids + offset receives each volume's ids; one flatten, scan and download for all.
+// Slabs of a volume still being copied to the device: z planes [previous end, end) are there once
+// the event has completed (events in copy order, the last end is the volume's depth; each end but
+// the last is a multiple of 8, the union tiles' depth).
+using Slabs = std::vector<std::pair<int, cudaEvent_t>>;
 struct CcVolume {
   const void *labels;
   int dtype;
   VolumeDims d;
   long long offset;
+  const Slabs *slabs = nullptr;  // null: the labels are all there
 };
 std::vector<ComponentsResult> connected_components(Context &ctx, const std::vector<CcVolume> &volumes, uint32_t *ids,
                                                    bool planar = false);

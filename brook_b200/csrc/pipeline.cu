@@ -142,11 +142,14 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     for (size_t v = 0; v < volumes.size(); ++v) {
       if (vs[v].empty) continue;
       const void *labels = volumes[v].data;
+      const Slabs *slabs = volumes[v].slabs;
       if (opt.object_ids) {
+        if (slabs && !slabs->empty()) BK_CUDA(cudaStreamWaitEvent(s, slabs->back().second, 0));
         masked[v] = filter_volume(ctx, volumes[v], *opt.object_ids);
         labels = masked[v].data();
+        slabs = nullptr;
       }
-      cv.push_back({labels, volumes[v].dtype, vs[v].d, vs[v].offset});
+      cv.push_back({labels, volumes[v].dtype, vs[v].d, vs[v].offset, slabs});
       which.push_back(v);
     }
     auto cc = connected_components(ctx, cv, ids.data());

@@ -47,6 +47,7 @@ struct DeviceVolume {
   const void *data = nullptr;
   int dtype = U32;
   VolumeDims d;
+  const Slabs *slabs = nullptr;  // non-null: still arriving by slabs (kernels.hpp)
 };
 
 std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &volumes, const Options &options);

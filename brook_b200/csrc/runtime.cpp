@@ -22,11 +22,23 @@ Context::Context(int device) : device_(device) {
   BK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
 }
 
+cudaStream_t Context::copy_stream() {
+  if (!copy_) {
+    DeviceGuard guard(device_);
+    BK_CUDA(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+  }
+  return copy_;
+}
+
 Context::~Context() {
   if (stream_) {
     int previous = -1;
     cudaGetDevice(&previous);
     cudaSetDevice(device_);
+    if (copy_) {
+      cudaStreamSynchronize(copy_);
+      cudaStreamDestroy(copy_);
+    }
     for (auto &entry : free_)
       for (void *p : entry.second) cudaFreeAsync(p, stream_);
     cudaStreamSynchronize(stream_);

@@ -53,6 +53,9 @@ class Context {
 
   int device() const { return device_; }
   cudaStream_t stream() const { return stream_; }
+  // A second stream, for host-to-device copies that overlap the main stream's kernels (created on
+  // first use). The main stream waits on its events before it reads what they copied.
+  cudaStream_t copy_stream();
   int sm_count() const { return sm_count_; }
   void synchronize() const { BK_CUDA(cudaStreamSynchronize(stream_)); }
   // Stream-ordered device memory with a per-context cache: a released block goes to a free list
@@ -71,7 +74,7 @@ class Context {
 
  private:
   int device_ = 0, sm_count_ = 0;
-  cudaStream_t stream_ = nullptr;
+  cudaStream_t stream_ = nullptr, copy_ = nullptr;
   std::mutex mutex_;
   std::map<size_t, std::vector<void *>> free_;  // size class -> cached blocks
   std::map<void *, size_t> class_of_;           // live and cached blocks -> size class

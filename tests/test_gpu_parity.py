@@ -353,6 +353,31 @@ def test_c_abi_device_output(gpu):
         np.testing.assert_array_equal(copied[name], expected[name], err_msg=name)
 
 
+def test_pinned_host_input_by_slabs_matches_device_input(gpu):
+    """Host input in page-locked memory (256 MiB of uint64 here) is copied in slabs on a copy stream
+    and the components' unions start on each slab as it arrives: the same skeletons as device
+    input, also with object_ids (which waits for every slab first)."""
+    import torch
+    from brook_b200 import synthetic
+
+    labels = synthetic.tube_volume((512, 256, 256), objects=12, seed=21).astype(np.uint64)
+    dev = torch.from_numpy(np.ascontiguousarray(labels.transpose(2, 1, 0))).cuda().permute(2, 1, 0)
+    pinned_t = torch.empty(labels.shape[::-1], dtype=torch.uint64, pin_memory=True)
+    pinned_t.numpy()[...] = labels.transpose(2, 1, 0)
+    pinned = pinned_t.numpy().transpose(2, 1, 0)
+    opts = dict(teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    chosen = [int(x) for x in np.unique(labels)[1:6:2]]
+    for extra in ({}, {"object_ids": chosen}):
+        a = bk().skeletonize(dev, output="packed", **opts, **extra)
+        b = bk().skeletonize(pinned, output="packed", **opts, **extra)
+        assert len(a) > 0
+        np.testing.assert_array_equal(a.labels, b.labels)
+        np.testing.assert_array_equal(a.v_off, b.v_off)
+        np.testing.assert_array_equal(a.vertices, b.vertices)
+        np.testing.assert_array_equal(a.edges, b.edges)
+        np.testing.assert_array_equal(a.radii.view(np.uint32), b.radii.view(np.uint32))
+
+
 def test_extra_targets_match_oracle(gpu):
     """extra_targets_before (traced first, after the border targets) and extra_targets_after
     (traced once no voxel is left), points on the background dropped (lockstep.cu:127-134,
