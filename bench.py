@@ -22,6 +22,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -106,7 +107,9 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv")
+        # the raw samples: a temporary file unless BENCH_CLOCKS_DIR names a folder to keep them in
+        folder = os.environ.get("BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(folder, f"clocks_{index}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
