@@ -1,8 +1,11 @@
 // Object engine kernels (see engine.hpp). A "group" — one CTA, or a cluster of 4 or 8 CTAs
 // for a large object — runs one object's chain. Every frontier round has two steps separated by a
 // group barrier: step A stages each frontier voxel (flag cleared, distance read, neighbour mask),
-// step B spreads its (voxel, neighbour) items over every thread of the group, so that thousands of
-// independent relaxations are in flight at once. The group's counters live in the shared memory
+// step B spreads its 26 (voxel, neighbour) items densely over the threads, so that thousands of
+// independent relaxations are in flight at once. When every CTA's share of the frontier fits its
+// shared-memory staging, each CTA stages its own share there and runs only that share's items
+// (an item then reads its voxel's fields without an L2 round trip); larger frontiers are staged
+// in HBM and their items spread over the whole group. The group's counters live in the shared memory
 // of its first CTA (distributed shared memory for a cluster, updated with 32-bit atomics only);
 // 64-bit reductions (nearest rail, nearest deferred voxel, argmax) keep one copy per CTA, updated
 // with CTA-local atomics and combined across the group at barriers. State other threads update
