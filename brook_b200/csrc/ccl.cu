@@ -125,6 +125,14 @@ __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__
     if (lv == L(0)) continue;
     const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
     auto same = [&](int a, int b, int c) { return lab[t + a + kTileX * (b + kTileY * c)] == lv; };
+    // Inside a region of one label: when the +y and +z neighbours (in this tile) carry the label,
+    // every other forward pair has one of them as a face intermediate and is skipped, so those
+    // two unions are all (in a plane, the +y one).
+    if (ly + 1 < ey && same(0, 1, 0) && (planar || (lz + 1 < ez && same(0, 0, 1)))) {
+      tile_unite(par, t, t + kTileX);
+      if (!planar) tile_unite(par, t, t + kTileX * kTileY);
+      continue;
+    }
 #pragma unroll
     for (int k = 0; k < 26; ++k) {
       const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];

@@ -34,22 +34,38 @@ __global__ void analyze_kernel(const uint32_t *__restrict__ ids, Dims d, int *lo
   if (last && __ldcg(h) < x) atomicMax(h, x);
 }
 
-__global__ void mask_kernel(const uint32_t *__restrict__ ids, Dims d, uint32_t *__restrict__ mask) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n()) return;
-  const uint32_t id = ids[i];
-  uint32_t m = 0;
-  if (id) {
-    int x, y, z;
-    unravel((int)i, d, x, y, z);
-#pragma unroll
-    for (int k = 0; k < 26; ++k) {
-      const int nx = x + c_dx[k], ny = y + c_dy[k], nz = z + c_dz[k];
-      if (nx < 0 || ny < 0 || nz < 0 || nx >= d.sx || ny >= d.sy || nz >= d.sz) continue;
-      if (ids[i + nbr_offset(k, d)] == id) m |= 1u << k;
-    }
+// The mask of a 32x8x8 block of voxels from a shared-memory copy of the block's ids with a
+// one-voxel halo (outside the volume: 0, which no voxel's id equals); block (32, 8) threads, grid
+// (x blocks, y blocks, z blocks).
+constexpr int kMaskX = 32, kMaskY = 8, kMaskZ = 8;
+
+__global__ void __launch_bounds__(kMaskX * kMaskY) mask_kernel(const uint32_t *__restrict__ ids, Dims d,
+                                                              uint32_t *__restrict__ mask) {
+  constexpr int HX = kMaskX + 2, HY = kMaskY + 2, HZ = kMaskZ + 2;
+  __shared__ uint32_t s[HZ * HY * HX];
+  const int x0 = blockIdx.x * kMaskX, y0 = blockIdx.y * kMaskY, z0 = blockIdx.z * kMaskZ;
+  for (int q = threadIdx.x + kMaskX * threadIdx.y; q < HX * HY * HZ; q += kMaskX * kMaskY) {
+    const int hx = q % HX, hy = (q / HX) % HY, hz = q / (HX * HY);
+    const int x = x0 + hx - 1, y = y0 + hy - 1, z = z0 + hz - 1;
+    uint32_t v = 0;
+    if (x >= 0 && y >= 0 && z >= 0 && x < d.sx && y < d.sy && z < d.sz)
+      v = ids[x + (long long)d.sx * (y + (long long)d.sy * z)];
+    s[q] = v;
   }
-  mask[i] = m;
+  __syncthreads();
+  const int lx = threadIdx.x, ly = threadIdx.y, x = x0 + lx, y = y0 + ly;
+  if (x >= d.sx || y >= d.sy) return;
+  for (int lz = 0; lz < kMaskZ && z0 + lz < d.sz; ++lz) {
+    const int c = (lx + 1) + HX * ((ly + 1) + HY * (lz + 1));
+    const uint32_t id = s[c];
+    uint32_t m = 0;
+    if (id) {
+#pragma unroll
+      for (int k = 0; k < 26; ++k)
+        if (s[c + c_dx[k] + HX * (c_dy[k] + HY * c_dz[k])] == id) m |= 1u << k;
+    }
+    mask[x + (long long)d.sx * (y + (long long)d.sy * (z0 + lz))] = m;
+  }
 }
 
 __global__ void segmax_kernel(const float *__restrict__ f, const uint32_t *__restrict__ ids, long long n, unsigned *best) {
@@ -164,7 +180,9 @@ std::vector<Box> analyze(Context &ctx, const uint32_t *ids, VolumeDims vd, int64
 
 void neighbour_mask(Context &ctx, const uint32_t *ids, VolumeDims vd, uint32_t *out) {
   if (vd.n() <= 0) return;
-  mask_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, out); ++ctx.launches;
+  const dim3 grid((vd.sx + kMaskX - 1) / kMaskX, (vd.sy + kMaskY - 1) / kMaskY, (vd.sz + kMaskZ - 1) / kMaskZ);
+  if (grid.y > 65535 || grid.z > 65535) throw std::invalid_argument("volume too large for the neighbour mask");
+  mask_kernel<<<grid, dim3(kMaskX, kMaskY), 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, out); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
 }
 
