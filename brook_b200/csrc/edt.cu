@@ -20,6 +20,8 @@ namespace bk {
 namespace {
 
 constexpr int kWarpsX = 4;
+// The x pass's dynamic shared memory (kWarpsX line starts per CTA) is at most this.
+constexpr size_t kEdtXMaxSmem = 200 * 1024;
 
 __global__ void edt_x(const uint32_t *__restrict__ ids, float *__restrict__ D, Dims d, const float *__restrict__ acc,
                       int bb, int finish) {
@@ -76,6 +78,22 @@ __global__ void edt_x(const uint32_t *__restrict__ ids, float *__restrict__ D, D
     carry_end = __shfl_sync(0xFFFFFFFFu, en, 0);
     carry_next = __shfl_sync(0xFFFFFFFFu, lab, 0);
   }
+}
+
+// Lets every edt_x launch of this device use up to kEdtXMaxSmem of dynamic shared memory. The
+// limit is a process-wide attribute of the kernel: set per call to the call's own need, it races
+// with other threads' launches of other extents (a launch above the limit another thread just
+// set fails), so it is raised once per device to the bound every launch is checked against.
+void allow_edt_x_smem() {
+  static std::mutex lock;
+  static bool raised[256] = {};
+  int device = 0;
+  BK_CUDA(cudaGetDevice(&device));
+  if (device < 0 || device >= 256) throw std::invalid_argument("device index out of range");
+  std::lock_guard<std::mutex> guard(lock);
+  if (raised[device]) return;
+  BK_CUDA(cudaFuncSetAttribute(edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEdtXMaxSmem));
+  raised[device] = true;
 }
 
 // One line of the y or z pass: n voxels from `base` with `stride`. Stacks V/H/Z are interleaved:
@@ -247,8 +265,8 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
   for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + aniso[0];
   Buffer<float> dacc = to_device(ctx, acc);
   const size_t smem = size_t(kWarpsX) * vd.sx * sizeof(int);
-  if (smem > 200 * 1024) throw std::invalid_argument("x extent too large for the EDT x pass");
-  BK_CUDA(cudaFuncSetAttribute(edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > kEdtXMaxSmem) throw std::invalid_argument("x extent too large for the EDT x pass");
+  allow_edt_x_smem();
   const long long xlines = (long long)vd.sy * vd.sz;
   const bool only_x = dims == 1 || (vd.sy == 1 && vd.sz == 1 && dims == 1);
   edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(ids, D, d, dacc.data(),
@@ -284,8 +302,8 @@ void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume>
   for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + aniso[0];
   Buffer<float> dacc = to_device(ctx, acc);
   const size_t smem = size_t(kWarpsX) * maxx * sizeof(int);
-  if (smem > 200 * 1024) throw std::invalid_argument("x extent too large for the EDT x pass");
-  BK_CUDA(cudaFuncSetAttribute(edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > kEdtXMaxSmem) throw std::invalid_argument("x extent too large for the EDT x pass");
+  allow_edt_x_smem();
   for (const auto &v : vols) {
     if (!v.d.n()) continue;
     const long long xlines = (long long)v.d.sy * v.d.sz;
@@ -389,14 +407,14 @@ void edt_fixed_scratch(const uint32_t *labels, VolumeDims vd, const float aniso[
   const size_t smem = size_t(kWarpsX) * vd.sx * sizeof(int);
   const size_t table = (size_t(vd.sx + 2) * sizeof(float) + 255) / 256 * 256;
   const size_t line = 16 * size_t(std::max(vd.sy, vd.sz) + 3);
-  if (smem > 200 * 1024 || table + line > kFixedScratchBytes)
+  if (smem > kEdtXMaxSmem || table + line > kFixedScratchBytes)
     throw std::invalid_argument("volume too large for the EDT's fixed 32 MiB scratch (x extent at most 12800 and "
                                 "16 * (max(y, z) extent + 3) + 4 * (x extent + 2) bytes within it)");
   unsigned char *base = static_cast<unsigned char *>(fixed_scratch());
   float *acc = reinterpret_cast<float *>(base);
   spacing_table<<<1, 1, 0, s>>>(acc, vd.sx + 2, aniso[0]);
   BK_CUDA(cudaGetLastError());
-  BK_CUDA(cudaFuncSetAttribute(edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_edt_x_smem();
   const long long xlines = (long long)vd.sy * vd.sz;
   edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(labels, D, d, acc,
                                                                                 black_border ? 1 : 0, 0);

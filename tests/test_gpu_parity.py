@@ -314,6 +314,36 @@ def test_connected_components_match_scipy(gpu, shape, blob):
     assert got_values == values
 
 
+def test_threads_with_other_x_extents_do_not_race(gpu):
+    """Threads, each with its own context, run EDTs of different x extents at once (one above the
+    48 KiB default shared-memory limit of the x pass): the limit is a process-wide attribute of the
+    kernel, so no call may lower it for another's launch."""
+    import threading
+    from brook_b200 import _native as n
+
+    errors = []
+
+    def work(sx):
+        try:
+            labels = np.asfortranarray(np.ones((sx, 6, 5), np.uint32))
+            labels[sx // 2] = 2
+            ctx = n.context(0)
+            for _ in range(40):
+                vol = n.host_volume(labels)
+                arr = ctypes.c_void_p()
+                n.check(n.lib.brook_edt(ctx, ctypes.byref(vol), (ctypes.c_float * 3)(1, 1, 1), 0, ctypes.byref(arr)))
+                n.lib.brook_array_destroy(arr)
+        except Exception as e:  # noqa: BLE001 - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(sx,)) for sx in (40, 700, 3500)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+
+
 def test_c_abi_device_output(gpu):
     """BROOK_DEVICE_OUTPUT (brook.h:96-102, 232-233): the device view and array handles hold the
     same skeletons as the host route; get_view copies a device result to the host; a host result
