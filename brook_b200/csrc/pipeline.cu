@@ -1,7 +1,9 @@
 // Orchestration of the skeletonizer over one flat index space that holds every volume of a call
-// (an arena per volume):
-//   per volume: connected components, boxes, EDT, neighbour masks, border targets, DBF maxima;
-//   every object of every volume at once: prepare (roots, DAF, PDRF), target orders, trace;
+// (an arena per volume). Each stage covers every volume at once (launches per volume where a
+// volume's shape sets the grid, one download for all):
+//   connected components (a volume arriving by slabs has its unions queued slab by slab), boxes,
+//   EDT, neighbour masks, DBF maxima, border targets, object voxel lists;
+//   every object of every volume in the engine: prepare (roots, DAF, PDRF), target orders, trace;
 //   assembly into packed skeletons per volume.
 #include <algorithm>
 #include <cmath>
