@@ -87,3 +87,42 @@ def test_target_order_rule():
                 idx = np.nonzero(mask)[0]
                 expected = sorted(idx.tolist(), key=lambda i: (-key[i], -i))
                 assert got.tolist() == expected
+
+
+def _scipy_edt(labels, anisotropy, black_border):
+    """The multi-label EDT in float64: per label, the exact Euclidean distance transform of its
+    voxels (distance to the nearest voxel of another label or background); with black border the
+    volume is padded by background first."""
+    from scipy import ndimage
+
+    pad = 1 if black_border else 0
+    lab = np.pad(labels, pad) if pad else labels
+    out = np.zeros(lab.shape, np.float64)
+    for value in np.unique(lab):
+        if value == 0:
+            continue
+        inside = lab == value
+        if inside.all():  # no other voxel anywhere: the distance is unbounded
+            out[inside] = np.inf
+            continue
+        out[inside] = ndimage.distance_transform_edt(inside, sampling=anisotropy)[inside]
+    return out[pad:lab.shape[0] - pad, pad:lab.shape[1] - pad, pad:lab.shape[2] - pad] if pad else out
+
+
+def test_edt_within_1e6_of_float64():
+    """The float32 EDT (float32 spacing table, float64 envelope) within 1e-6 relative of an exact
+    float64 transform, on multi-label volumes, anisotropic spacings and with black border."""
+    from scipy import ndimage
+
+    rng = np.random.default_rng(11)
+    for shape, aniso, bb in (((30, 24, 18), (1, 1, 1), False), ((26, 20, 22), (8, 8, 40), True),
+                             ((20, 28, 16), (7.91, 7.91, 7.91), False), ((40, 12, 10), (4, 5, 6), True)):
+        field = ndimage.gaussian_filter(rng.random((4,) + shape), sigma=(0, 2, 2, 2))
+        labels = np.asfortranarray((np.argmax(field, axis=0) + 1).astype(np.uint32))
+        labels[rng.random(shape) < 0.05] = 0
+        got = oracle.edt(labels, aniso, bb).astype(np.float64)
+        exp = _scipy_edt(labels, aniso, bb)
+        finite = np.isfinite(exp)
+        assert np.array_equal(np.isfinite(got), finite)
+        rel = np.abs(got[finite] - exp[finite]) / np.maximum(exp[finite], 1e-30)
+        assert rel.max() <= 1e-6, (shape, aniso, bb, rel.max())
