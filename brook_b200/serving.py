@@ -24,8 +24,11 @@ import numpy as np
 from .batch import skeletonize_batch
 
 # Device bytes per voxel beyond the labels: component ids, neighbour masks, DBF, the per-voxel
-# engine state (PDRF, distances, DAF, flags, liveness, claim keys) and union-find / scan scratch.
-STATE_BYTES_PER_VOXEL = 64
+# engine state (PDRF, distances, DAF, flags, liveness, claim keys), union-find / scan scratch, the
+# EDT's envelope stacks, the per-object worklists and the allocator's size-class rounding. The
+# context's high-water marks measured 157 bytes per voxel for a 512^3 dense volume (22 % of it
+# foreground) and 142 for nine overlapping 512x512x256 chunks (44 %).
+STATE_BYTES_PER_VOXEL = 160
 
 
 def footprint(shape, dtype) -> int:
