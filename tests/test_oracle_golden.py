@@ -126,3 +126,30 @@ def test_edt_within_1e6_of_float64():
         assert np.array_equal(np.isfinite(got), finite)
         rel = np.abs(got[finite] - exp[finite]) / np.maximum(exp[finite], 1e-30)
         assert rel.max() <= 1e-6, (shape, aniso, bb, rel.max())
+
+
+def test_oracle_answers_that_follow_from_teasar_alone():
+    """Answers that hold for any TEASAR with the reference's object rules: a one-voxel-thick line
+    is its own skeleton; an object whose bounding box is one voxel, or whose voxel count is within
+    the dust threshold, has none (batched.cu:187-191)."""
+    line = np.zeros((30, 3, 3), np.uint32)
+    line[3:27, 1, 1] = 7
+    p = oracle.skeletonize(line, anisotropy=(4, 5, 6), dust_threshold=0).packed()
+    assert p["labels"].tolist() == [7]
+    verts = p["vertices"].reshape(-1, 3)
+    assert len(verts) == 24 and len(p["edges"].reshape(-1, 2)) == 23
+    assert sorted(verts[:, 0].tolist()) == [4.0 * x for x in range(3, 27)]
+    assert set(verts[:, 1].tolist()) == {5.0} and set(verts[:, 2].tolist()) == {6.0}
+    edges = {tuple(sorted(e)) for e in p["edges"].reshape(-1, 2).tolist()}
+    order = np.argsort(verts[:, 0])
+    assert edges == {tuple(sorted((int(order[i]), int(order[i + 1])))) for i in range(23)}
+
+    dots = np.zeros((10, 10, 10), np.uint32)
+    dots[2, 2, 2] = 1                 # one voxel: no skeleton
+    dots[6, 6, 6] = dots[6, 6, 7] = 2  # two voxels: one edge
+    dots[0:4, 8, 8] = 3               # four voxels
+    p = oracle.skeletonize(dots, anisotropy=(1, 1, 1), dust_threshold=0).packed()
+    assert p["labels"].tolist() == [2, 3]
+    p = oracle.skeletonize(dots, anisotropy=(1, 1, 1), dust_threshold=3).packed()
+    assert p["labels"].tolist() == [3]  # 2 voxels <= dust 3 < 4
+    assert oracle.skeletonize(np.zeros((5, 5, 5), np.uint8), dust_threshold=0).packed()["labels"].size == 0
