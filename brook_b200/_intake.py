@@ -62,6 +62,28 @@ def _is_device(labels):
                                                    (hasattr(labels, "is_cuda") and labels.is_cuda))
 
 
+def producer_stream(labels, stream=None):
+    """The stream handle whose queued work must finish before `labels` (device memory) is read:
+    the caller's `stream` (an int handle or a torch.cuda.Stream), else the array's own CUDA array
+    interface stream, else torch's current stream for a torch tensor, else the legacy default
+    stream. Handles follow the CUDA array interface: 1 legacy default, 2 per-thread default,
+    anything else a cudaStream_t. (The reference's binding fences the same producer,
+    cpp/python/bindings.cpp:104-126.)"""
+    if stream is not None:
+        handle = getattr(stream, "cuda_stream", stream)
+        return int(handle) or 1
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        torch = None
+    if torch is not None and isinstance(labels, torch.Tensor):
+        return int(torch.cuda.current_stream(labels.device).cuda_stream) or 1
+    cai = getattr(labels, "__cuda_array_interface__", None)
+    if cai is not None and cai.get("stream") is not None:
+        return int(cai["stream"]) or 1
+    return 1
+
+
 def device_volume(labels):
     """(brook_volume, keep-alive) for a CUDA array (torch tensor or an object with the CUDA array
     interface); the array is read in place when it is Fortran-ordered."""
@@ -88,19 +110,37 @@ def device_volume(labels):
 
 
 def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
-         extra_after, device, device_output=False):
+         extra_after, device, device_output=False, producers=(), sample_targets=None):
+    """One C call over `volumes`. producers: stream handles the library's stream waits for first
+    (the producers of device inputs). sample_targets: per volume (before, after) point lists of a
+    batch (extra_before / extra_after then stay empty)."""
+    ctypes = _native.ctypes
     opts = _native.options(params, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids,
                            extra_before, extra_after)
     if device_output:
         opts.flags |= _native.DEVICE_OUTPUT
+    lib = _native.load()
     ctx = _native.context(device)
+    for handle in dict.fromkeys(producers):
+        _native.check(lib.brook_context_wait_stream(ctx, int(handle)))
     count = len(volumes)
     arr = (_native.Volume * max(count, 1))(*volumes)
-    handles = (_native.ctypes.c_void_p * max(count, 1))()
-    if count == 1:
-        _native.check(_native.lib.brook_skeletonize(ctx, arr, _native.ctypes.byref(opts), handles))
+    handles = (ctypes.c_void_p * max(count, 1))()
+    if sample_targets is not None:
+        table = (_native.SampleTargets * max(count, 1))()
+        keep = []
+        for i, (before, after) in enumerate(sample_targets):
+            for name, points in (("before", before), ("after", after)):
+                pts = np.ascontiguousarray(np.asarray(list(points), np.int64).reshape(-1, 3))
+                keep.append(pts)
+                if pts.size:
+                    setattr(table[i], name, pts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+                    setattr(table[i], name + "_count", pts.shape[0])
+        _native.check(lib.brook_skeletonize_batch_targets(ctx, arr, count, ctypes.byref(opts), table, handles))
+    elif count == 1:
+        _native.check(lib.brook_skeletonize(ctx, arr, ctypes.byref(opts), handles))
     else:
-        _native.check(_native.lib.brook_skeletonize_batch(ctx, arr, count, _native.ctypes.byref(opts), handles))
+        _native.check(lib.brook_skeletonize_batch(ctx, arr, count, ctypes.byref(opts), handles))
     grab = _native.packed_device_arrays if device_output else _native.packed_arrays
     return [PackedSkeletons.from_arrays(grab(handles[i])) for i in range(count)]
 
@@ -115,10 +155,13 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
 
     Returns `{label: Skeleton}` for output="skeletons", `PackedSkeletons` (host arrays) for
     "packed", and the same with CUDA tensors for "packed_device". Device input: a torch CUDA
-    tensor or an array with the CUDA array interface, read in place when Fortran-ordered.
-    `parallel`, `parallel_chunk_size`, `in_place`, `progress`, `stream`, `borrow` and `streaming`
-    are accepted for compatibility. `fill_holes`, `fix_avocados` and `voxel_graph` are not
-    supported by this build and raise.
+    tensor or an array with the CUDA array interface, read in place when Fortran-ordered; the
+    library's stream first waits for the producer's work (`stream`: the producer's stream handle
+    or torch.cuda.Stream; default: the array's own CUDA array interface stream, torch's current
+    stream for a torch tensor, else the legacy default stream). `parallel`,
+    `parallel_chunk_size`, `in_place`, `progress`, `borrow` and `streaming` are accepted for
+    compatibility. `fill_holes`, `fix_avocados` and `voxel_graph` are not supported by this build
+    and raise.
     """
     if output not in ("skeletons", "packed", "packed_device"):
         raise ValueError("brook_b200: output must be 'skeletons', 'packed' or 'packed_device'")
@@ -126,8 +169,10 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
         raise NotImplementedError("brook_b200: fill_holes, fix_avocados and voxel_graph are not supported")
     params = teasar(teasar_params)
     anisotropy = tuple(float(a) for a in np.asarray(anisotropy, dtype=np.float32))
+    producers = []
     if _is_device(all_labels):
         volume, keep = device_volume(all_labels)
+        producers.append(producer_stream(all_labels, stream))
     else:
         keep = format_labels(all_labels)
         if keep.size <= dust_threshold:
@@ -138,7 +183,7 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     packed = _run([volume], params, anisotropy, ids, dust_threshold, fix_branching, fix_borders,
                   [tuple(int(c) for c in p) for p in extra_targets_before],
                   [tuple(int(c) for c in p) for p in extra_targets_after], device,
-                  device_output=output == "packed_device")[0]
+                  device_output=output == "packed_device", producers=producers)[0]
     del keep
     if output == "skeletons":
         return packed.to_skeletons()

@@ -1,6 +1,8 @@
 """ctypes binding of the C ABI in include/brook_b200.h (libbrook_b200.so, built in-tree).
 
-The library is the only compute path: importing this module fails loudly when it is missing.
+The library is the only compute path. It is loaded on first use (`load()`, or the module
+attribute `lib`), so that importing the package costs nothing; a missing library fails loudly
+there, with no fallback.
 """
 from __future__ import annotations
 
@@ -29,7 +31,9 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_connected_components", "brook_components_destroy", "brook_components_view",
            "brook_components_copy_to_host", "brook_edt", "brook_skeletonize_options_init", "brook_skeletonize",
            "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy", "brook_context_stats",
-           "brook_edt_device_noalloc", "brook_skeletons_get_device_view", "brook_skeletons_get_array"]
+           "brook_edt_device_noalloc", "brook_skeletons_get_device_view", "brook_skeletons_get_array",
+           "brook_array_upload", "brook_array_to_dlpack", "brook_array_to_dlpack_versioned", "brook_components_labels",
+           "brook_skeletonize_batch_targets", "brook_context_wait_stream"]
 
 
 class Volume(ctypes.Structure):
@@ -70,6 +74,11 @@ class SkeletonsDeviceView(ctypes.Structure):
                 ("radii", Volume), ("anisotropy", ctypes.c_float * 3)]
 
 
+class SampleTargets(ctypes.Structure):
+    _fields_ = [("before", ctypes.POINTER(ctypes.c_int64)), ("before_count", ctypes.c_size_t),
+                ("after", ctypes.POINTER(ctypes.c_int64)), ("after_count", ctypes.c_size_t)]
+
+
 VERTICES, EDGES, RADII = 0, 1, 2
 
 
@@ -81,7 +90,27 @@ class BrookError(RuntimeError):
         self.status = status
 
 
-def _load():
+_lib = None
+_load_lock = threading.Lock()
+
+
+def load():
+    """The library handle, loaded on first use."""
+    global _lib
+    if _lib is None:
+        with _load_lock:
+            if _lib is None:
+                _lib = _open()
+    return _lib
+
+
+def __getattr__(name):  # `_native.lib` loads the library on first use
+    if name == "lib":
+        return load()
+    raise AttributeError(name)
+
+
+def _open():
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"brook_b200: the CUDA library {LIB_PATH} is not built; run brook_b200/build.py "
                           "(there is no CPU fallback)")
@@ -115,6 +144,13 @@ def _load():
                                                     vp, vp]),
         "brook_skeletons_get_device_view": (ctypes.c_int, [vp, ctypes.POINTER(SkeletonsDeviceView)]),
         "brook_skeletons_get_array": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(vp)]),
+        "brook_array_upload": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(vp)]),
+        "brook_array_to_dlpack": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
+        "brook_array_to_dlpack_versioned": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.POINTER(vp)]),
+        "brook_components_labels": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
+        "brook_skeletonize_batch_targets": (ctypes.c_int, [vp, ctypes.POINTER(Volume), sz, ctypes.POINTER(Options),
+                                                           ctypes.POINTER(SampleTargets), ctypes.POINTER(vp)]),
+        "brook_context_wait_stream": (ctypes.c_int, [vp, ctypes.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -123,12 +159,9 @@ def _load():
     return lib
 
 
-lib = _load()
-
-
 def check(status):
     if status != SUCCESS:
-        raise BrookError(status, lib.brook_last_error().decode(errors="replace"))
+        raise BrookError(status, load().brook_last_error().decode(errors="replace"))
 
 
 _contexts: dict = {}
@@ -142,7 +175,7 @@ def context(device=0):
         ctx = _contexts.get(key)
         if ctx is None:
             handle = ctypes.c_void_p()
-            check(lib.brook_context_create(int(device), ctypes.byref(handle)))
+            check(load().brook_context_create(int(device), ctypes.byref(handle)))
             ctx = _contexts[key] = handle
     return ctx
 
@@ -177,7 +210,7 @@ def device_volume(ptr, shape, strides_bytes, dtype):
 def options(teasar, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids=None,
             targets_before=(), targets_after=()):
     o = Options()
-    lib.brook_skeletonize_options_init(ctypes.byref(o))
+    load().brook_skeletonize_options_init(ctypes.byref(o))
     t = o.teasar
     t.scale, t.constant, t.pdrf_scale, t.pdrf_exponent = (teasar["scale"], teasar["const"], teasar["pdrf_scale"],
                                                           teasar["pdrf_exponent"])
@@ -211,7 +244,7 @@ def packed_arrays(handle):
     """Copies a brook_skeletons result into NumPy arrays and releases the handle."""
     v = SkeletonsView()
     try:
-        check(lib.brook_skeletons_get_view(handle, ctypes.byref(v)))
+        check(load().brook_skeletons_get_view(handle, ctypes.byref(v)))
 
         def grab(ptr, count, dtype, shape):
             if count == 0:
@@ -224,7 +257,7 @@ def packed_arrays(handle):
                     vertices=grab(v.vertices, 3 * nv, np.float32, (nv, 3)), edges=grab(v.edges, 2 * ne, np.uint32, (ne, 2)),
                     radii=grab(v.radii, nv, np.float32, (nv,)), anisotropy=tuple(float(a) for a in v.anisotropy))
     finally:
-        lib.brook_skeletons_destroy(handle)
+        load().brook_skeletons_destroy(handle)
 
 
 class _DeviceResult:
@@ -236,7 +269,7 @@ class _DeviceResult:
 
     def __del__(self):
         if self.handle:
-            lib.brook_skeletons_destroy(self.handle)
+            load().brook_skeletons_destroy(self.handle)
             self.handle = None
 
 
@@ -254,7 +287,7 @@ def packed_device_arrays(handle):
 
     v = SkeletonsDeviceView()
     owner = _DeviceResult(handle)
-    check(lib.brook_skeletons_get_device_view(handle, ctypes.byref(v)))
+    check(load().brook_skeletons_get_device_view(handle, ctypes.byref(v)))
     k, nv, ne = v.skeleton_count, v.vertex_count, v.edge_count
 
     def host(ptr, count):
@@ -278,7 +311,7 @@ def stats(device=0):
 
     ctx = context(device)
     need = ctypes.c_size_t()
-    check(lib.brook_context_stats(ctx, None, 0, ctypes.byref(need)))
+    check(load().brook_context_stats(ctx, None, 0, ctypes.byref(need)))
     buf = ctypes.create_string_buffer(need.value)
-    check(lib.brook_context_stats(ctx, buf, need.value, None))
+    check(load().brook_context_stats(ctx, buf, need.value, None))
     return json.loads(buf.value.decode())

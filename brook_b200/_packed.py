@@ -31,6 +31,12 @@ class Skeleton:
         return f"Skeleton(id={self.id}, vertices={len(self.vertices)}, edges={len(self.edges)})"
 
 
+def torch_int32():
+    import torch
+
+    return torch.int32
+
+
 @dataclass
 class PackedSkeletons:
     """Skeletons in flat arrays: skeleton k has label `labels[k]`, vertices
@@ -55,7 +61,9 @@ class PackedSkeletons:
     def to_host(self):
         if not self.on_device:
             return self
-        return type(self)(self.labels, self.v_off, self.e_off, self.vertices.cpu().numpy(), self.edges.cpu().numpy(),
+        edges = self.edges.view(torch_int32()).cpu().numpy().view(np.uint32) if self.edges.numel() else \
+            np.zeros((0, 2), np.uint32)
+        return type(self)(self.labels, self.v_off, self.e_off, self.vertices.cpu().numpy(), edges,
                           self.radii.cpu().numpy(), self.anisotropy)
 
     def to_device(self, device=None):
@@ -65,8 +73,8 @@ class PackedSkeletons:
         import torch
 
         dev = torch.device("cuda" if device is None else device)
-        return type(self)(self.labels, self.v_off, self.e_off, torch.from_numpy(self.vertices).to(dev),
-                          torch.from_numpy(self.edges.astype(np.int64)).to(dev).to(torch.int32),
+        edges = torch.from_numpy(np.ascontiguousarray(self.edges, np.uint32).view(np.int32)).to(dev).view(torch.uint32)
+        return type(self)(self.labels, self.v_off, self.e_off, torch.from_numpy(self.vertices).to(dev), edges,
                           torch.from_numpy(self.radii).to(dev), self.anisotropy)
 
     def to_skeletons(self):

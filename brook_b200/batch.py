@@ -8,7 +8,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
-from ._intake import DEFAULT_TEASAR_PARAMS, _is_device, _run, device_volume, format_labels, teasar
+from ._intake import DEFAULT_TEASAR_PARAMS, _is_device, _run, device_volume, format_labels, producer_stream, teasar
 from ._packed import PackedSkeletons
 
 
@@ -83,10 +83,54 @@ class BatchedSkeletons:
             edges.append(p.edges)
             radii.append(p.radii)
         cat = lambda xs, shape, dtype: np.concatenate(xs).astype(dtype, copy=False) if xs else np.zeros(shape, dtype)
+        if parts and parts[0].on_device:  # device arrays stay on the device
+            import torch
+
+            def dcat(xs, shape, dtype):
+                if not xs:
+                    return torch.zeros(shape, dtype=dtype, device="cuda")
+                if dtype == torch.uint32:  # concatenated through a same-width signed view
+                    return torch.cat([x.view(torch.int32) for x in xs]).view(torch.uint32)
+                return torch.cat(xs)
+
+            arrays = (dcat(vertices, (0, 3), torch.float32), dcat(edges, (0, 2), torch.uint32),
+                      dcat(radii, (0,), torch.float32))
+        else:
+            arrays = (cat(vertices, (0, 3), np.float32), cat(edges, (0, 2), np.uint32), cat(radii, (0,), np.float32))
         packed = PackedSkeletons(cat(labels, (0,), np.int64), np.asarray(voff, np.int64), np.asarray(eoff, np.int64),
-                                 cat(vertices, (0, 3), np.float32), cat(edges, (0, 2), np.uint32),
-                                 cat(radii, (0,), np.float32), tuple(float(a) for a in anisotropy))
+                                 *arrays, tuple(float(a) for a in anisotropy))
         return cls(packed, packed.labels, cat(sample, (0,), np.int64), np.asarray(s_off, np.int64))
+
+
+def _is_point(entry):
+    """A single 3-D point, rather than one sample's sequence of points."""
+    if isinstance(entry, np.ndarray):
+        return entry.ndim == 1 and entry.shape[0] == 3
+    if entry is None or isinstance(entry, (str, bytes)):
+        return False
+    try:
+        values = list(entry)
+    except TypeError:
+        return False
+    return len(values) == 3 and all(np.ndim(value) == 0 for value in values)
+
+
+def sample_targets(targets, count, name):
+    """One list of (x, y, z) points per sample, in each sample's own frame, with the rules of the
+    reference's batch (src/brook/batch.py:173-190): None or an empty sequence means no sample has
+    targets; otherwise one entry per sample (None or an empty sequence for a sample without any);
+    a flat list of points is refused."""
+    if targets is None:
+        return None
+    entries = list(targets)
+    if not entries:
+        return None
+    if any(_is_point(entry) for entry in entries):
+        raise ValueError(f"brook_b200: {name} is per sample in a batch: pass one sequence of points for each sample "
+                         f"(an empty sequence for a sample without targets), not one flat list of points")
+    if len(entries) != count:
+        raise ValueError(f"brook_b200: {name} has {len(entries)} entries for {count} samples")
+    return [[] if entry is None else [tuple(int(c) for c in point) for point in entry] for entry in entries]
 
 
 def skeletonize_batch(samples, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), dust_threshold=1000,
@@ -95,33 +139,44 @@ def skeletonize_batch(samples, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(
                       stream=None, borrow=True, voxel_graph=None, device=0):
     """Skeletonize independent samples (host arrays or CUDA arrays; shapes may differ) in one call.
 
-    Returns BatchedSkeletons with CUDA tensors (output="packed_device"), with host arrays
+    `extra_targets_before` / `extra_targets_after` are per sample: a sequence aligned with
+    `samples` holding each sample's own points (an empty sequence or None for a sample without
+    targets). `stream` is the producer's stream that the library waits for before reading device
+    samples (default: each array's own CUDA array interface stream, torch's current stream for
+    torch tensors, else the legacy default stream). Returns BatchedSkeletons with CUDA tensors
+    that the library produced on the device (output="packed_device"), with host arrays
     ("packed"), or a list of {label: Skeleton} dicts ("skeletons")."""
     if output not in ("packed_device", "packed", "skeletons"):
         raise ValueError("brook_b200: output must be 'packed_device', 'packed' or 'skeletons'")
     if fill_holes or fix_avocados or voxel_graph is not None:
         raise NotImplementedError("brook_b200: fill_holes, fix_avocados and voxel_graph are not supported")
-    if any(x for x in (extra_targets_before or [])) or any(x for x in (extra_targets_after or [])):
-        raise NotImplementedError("brook_b200: per-sample extra targets are not supported in batches")
     if isinstance(samples, np.ndarray) and samples.ndim == 4:
         samples = list(samples)
+    samples = list(samples)
+    before = sample_targets(extra_targets_before, len(samples), "extra_targets_before")
+    after = sample_targets(extra_targets_after, len(samples), "extra_targets_after")
+    targets = None
+    if before is not None or after is not None:
+        targets = [(before[i] if before else [], after[i] if after else []) for i in range(len(samples))]
     params = teasar(teasar_params)
     anisotropy = tuple(float(a) for a in np.asarray(anisotropy, dtype=np.float32))
-    volumes, keep = [], []
+    volumes, keep, producers = [], [], []
     for s in samples:
         if _is_device(s):
             v, k = device_volume(s)
+            producers.append(producer_stream(s, stream))
         else:
             k = format_labels(s)
             v = _native.host_volume(k)
         volumes.append(v)
         keep.append(k)
-    parts = _run(volumes, params, anisotropy, None, dust_threshold, fix_branching, fix_borders, [], [], device) \
+    parts = _run(volumes, params, anisotropy, None, dust_threshold, fix_branching, fix_borders, [], [], device,
+                 device_output=output == "packed_device", producers=producers, sample_targets=targets) \
         if volumes else []
     result = BatchedSkeletons.concatenate(parts, anisotropy)
     if output == "skeletons":
         return result.to_skeletons()
-    if output == "packed_device":
+    if output == "packed_device" and not result.on_device:  # an empty batch
         return BatchedSkeletons(result.packed.to_device(), result.labels, result.sample, result.s_off)
     return result
 

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "../../include/brook_b200.h"
+#include "../../include/brook_b200_dlpack.h"
 #include "pipeline.hpp"
 
 #ifndef BROOK_B200_VERSION
@@ -26,6 +27,9 @@ struct brook_array {
   std::shared_ptr<DeviceStorage> storage;
   brook_volume view{};
   size_t bytes = 0;
+  // the array as a tensor for DLPack: extents and strides in elements (a volume: (x, y, z) with
+  // x fastest; a skeleton buffer: its row-major (rows, width) or (rows,) form)
+  std::vector<int64_t> shape, strides;
 };
 
 struct brook_components {
@@ -236,8 +240,10 @@ bk::Options options_of(const brook_skeletonize_options *p) {
     for (size_t i = 0; i < count; ++i) out.push_back({data[3 * i], data[3 * i + 1], data[3 * i + 2]});
     return out;
   };
-  o.targets_before = points(p->targets_before, p->targets_before_count);
-  o.targets_after = points(p->targets_after, p->targets_after_count);
+  if (p->targets_before_count || p->targets_after_count) {
+    o.targets_before.push_back(points(p->targets_before, p->targets_before_count));
+    o.targets_after.push_back(points(p->targets_after, p->targets_after_count));
+  }
   return o;
 }
 
@@ -250,6 +256,12 @@ __global__ void narrow_ids(const uint32_t *ids, void *out, long long n, int byte
   else static_cast<uint32_t *>(out)[i] = v;
 }
 
+size_t element_bytes(brook_dtype t) {
+  if (t == BROOK_F32) return 4;
+  if (t == BROOK_F64) return 8;
+  return bk::label_bytes(t);
+}
+
 brook_volume device_view(const void *data, brook_dtype dtype, bk::VolumeDims d) {
   brook_volume v{};
   v.struct_size = sizeof(v);
@@ -258,7 +270,7 @@ brook_volume device_view(const void *data, brook_dtype dtype, bk::VolumeDims d) 
   v.dtype = dtype;
   v.memory = BROOK_DEVICE;
   v.shape[0] = d.sx; v.shape[1] = d.sy; v.shape[2] = d.sz;
-  const size_t b = dtype == BROOK_F32 ? 4 : bk::label_bytes(dtype);
+  const size_t b = element_bytes(dtype);
   v.strides[0] = int64_t(b); v.strides[1] = int64_t(b) * d.sx; v.strides[2] = int64_t(b) * d.sx * d.sy;
   return v;
 }
@@ -277,14 +289,126 @@ brook_volume skeleton_view(const DeviceStorage &s, brook_dtype dtype, int width,
   return v;
 }
 
+void volume_tensor(brook_array &a) {
+  a.shape = {a.view.shape[0], a.view.shape[1], a.view.shape[2]};
+  a.strides = {1, a.view.shape[0], a.view.shape[0] * a.view.shape[1]};
+}
+
+// A row-major (rows x width) skeleton buffer as a tensor: (rows, width), or (rows,) for width 1.
+void rows_tensor(brook_array &a, int width, size_t rows) {
+  if (width == 1) { a.shape = {int64_t(rows)}; a.strides = {1}; }
+  else { a.shape = {int64_t(rows), width}; a.strides = {width, 1}; }
+}
+
+// A Fortran-ordered device copy of any volume (host or device memory, any strides, any of the
+// ten element types), in the context's stream order; the host waits for the copy.
+brook_array *upload_array(bk::Context &ctx, const brook_volume &v) {
+  require(v.struct_size >= sizeof(brook_volume) && v.abi_version == BROOK_ABI_VERSION, "incompatible brook_volume");
+  require(v.dtype >= BROOK_U8 && v.dtype <= BROOK_F64, "invalid element type");
+  for (int a = 0; a < 3; ++a) require(v.shape[a] >= 0 && v.shape[a] < (1LL << 31), "invalid volume shape");
+  const long long sx = v.shape[0], sy = v.shape[1], sz = v.shape[2], n = sx * sy * sz;
+  const long long b = (long long)element_bytes(v.dtype);
+  auto handle = std::make_unique<brook_array>();
+  handle->storage = std::make_shared<DeviceStorage>(size_t(n * b), ctx.device());
+  handle->bytes = size_t(n * b);
+  handle->view = device_view(handle->storage->ptr, v.dtype, bk::VolumeDims{int(sx), int(sy), int(sz)});
+  volume_tensor(*handle);
+  if (!n) return handle.release();
+  require(v.data != nullptr, "null volume data");
+  require(v.memory == BROOK_HOST || v.memory == BROOK_DEVICE, "invalid memory kind");
+  auto matches = [&](long long e0, long long e1, long long e2) {
+    return (sx == 1 || v.strides[0] == e0) && (sy == 1 || v.strides[1] == e1) && (sz == 1 || v.strides[2] == e2);
+  };
+  const bool fortran = matches(b, b * sx, b * sx * sy);
+  unsigned char *dst = static_cast<unsigned char *>(handle->storage->ptr);
+  cudaStream_t s = ctx.stream();
+  if (v.memory == BROOK_DEVICE) {
+    cudaPointerAttributes attr{};
+    BK_CUDA(cudaPointerGetAttributes(&attr, v.data));
+    require(attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged, "device volume is not device memory");
+    require(attr.type == cudaMemoryTypeManaged || attr.device == ctx.device(), "device volume is on another device");
+    if (fortran) BK_CUDA(cudaMemcpyAsync(dst, v.data, n * b, cudaMemcpyDeviceToDevice, s));
+    else {
+      gather_strided<<<bk::blocks_for(n), 256, 0, s>>>(static_cast<const unsigned char *>(v.data), dst, int(sx), int(sy),
+                                                      int(sz), v.strides[0], v.strides[1], v.strides[2], int(b)); ++ctx.launches;
+      BK_CUDA(cudaGetLastError());
+    }
+  } else if (fortran) {
+    BK_CUDA(cudaMemcpyAsync(dst, v.data, n * b, cudaMemcpyHostToDevice, s));
+  } else {
+    std::vector<unsigned char> host(n * b);
+    const unsigned char *base = static_cast<const unsigned char *>(v.data);
+    for (long long z = 0; z < sz; ++z)
+      for (long long y = 0; y < sy; ++y)
+        for (long long x = 0; x < sx; ++x)
+          std::memcpy(&host[((z * sy + y) * sx + x) * b], base + x * v.strides[0] + y * v.strides[1] + z * v.strides[2], b);
+    BK_CUDA(cudaMemcpyAsync(dst, host.data(), n * b, cudaMemcpyHostToDevice, s));
+    ctx.synchronize();
+  }
+  ctx.synchronize();
+  return handle.release();
+}
+
+// One DLPack export of an array: owns a reference to the array's storage and the extents, so
+// that it outlives the array handle and the context; the consumer's call of the deleter frees it.
+template <class Tensor>
+struct Export {
+  Tensor tensor{};
+  std::shared_ptr<DeviceStorage> storage;
+  std::vector<int64_t> shape, strides;
+};
+
+template <class Tensor>
+void release_export(Tensor *t) noexcept {
+  delete static_cast<Export<Tensor> *>(t->manager_ctx);
+}
+
+template <class Tensor>
+Tensor *export_array(const brook_array &a) {
+  auto e = std::make_unique<Export<Tensor>>();
+  e->storage = a.storage;
+  e->shape = a.shape;
+  e->strides = a.strides;
+  e->tensor.manager_ctx = e.get();
+  e->tensor.deleter = release_export<Tensor>;
+  DLTensor &t = e->tensor.dl_tensor;
+  t.data = a.bytes ? a.storage->ptr : nullptr;
+  t.device = DLDevice{kDLCUDA, int32_t(a.storage->device)};
+  t.ndim = int32_t(e->shape.size());
+  t.shape = e->shape.empty() ? nullptr : e->shape.data();
+  t.strides = e->strides.empty() ? nullptr : e->strides.data();
+  t.byte_offset = 0;
+  const brook_dtype d = a.view.dtype;
+  const uint8_t code = d <= BROOK_U64 ? kDLUInt : d <= BROOK_I64 ? kDLInt : kDLFloat;
+  t.dtype = DLDataType{code, uint8_t(8 * element_bytes(d)), 1};
+  return &e.release()->tensor;
+}
+
 brook_status skeletonize_many(brook_context *ctx, const brook_volume *volumes, size_t count,
-                              const brook_skeletonize_options *p, brook_skeletons **out) {
+                              const brook_skeletonize_options *p, const brook_sample_targets *targets,
+                              brook_skeletons **out) {
   return protect([&] {
     require(ctx && (volumes || !count) && p && out);
     for (size_t i = 0; i < count; ++i) out[i] = nullptr;
     std::lock_guard<std::mutex> lock(ctx->value.mutex());
     bk::DeviceGuard guard(ctx->value.device());
-    const bk::Options options = options_of(p);
+    bk::Options options = options_of(p);
+    if (count > 1 && !options.targets_before.empty())
+      throw std::invalid_argument("the options' extra targets are for one volume: give a batch its targets per sample "
+                                  "(brook_skeletonize_batch_targets)");
+    if (targets) {
+      require(options.targets_before.empty(), "extra targets are given both in the options and per sample");
+      options.targets_before.resize(count);
+      options.targets_after.resize(count);
+      for (size_t i = 0; i < count; ++i) {
+        const brook_sample_targets &t = targets[i];
+        require((t.before || !t.before_count) && (t.after || !t.after_count));
+        for (size_t k = 0; k < t.before_count; ++k)
+          options.targets_before[i].push_back({t.before[3 * k], t.before[3 * k + 1], t.before[3 * k + 2]});
+        for (size_t k = 0; k < t.after_count; ++k)
+          options.targets_after[i].push_back({t.after[3 * k], t.after[3 * k + 1], t.after[3 * k + 2]});
+      }
+    }
     std::vector<Staged> staged;
     std::vector<bk::DeviceVolume> vols;
     for (size_t i = 0; i < count; ++i) {
@@ -346,6 +470,52 @@ brook_status brook_array_copy_to_host(const brook_array *a, void *out, size_t by
   });
 }
 
+brook_status brook_array_upload(brook_context *ctx, const brook_volume *input, brook_array **out) {
+  return protect([&] {
+    require(ctx && input && out);
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    *out = upload_array(ctx->value, *input);
+  });
+}
+
+brook_status brook_array_to_dlpack(const brook_array *a, DLManagedTensor **out) {
+  return protect([&] {
+    require(a && out);
+    *out = nullptr;
+    *out = export_array<DLManagedTensor>(*a);
+  });
+}
+
+brook_status brook_array_to_dlpack_versioned(const brook_array *a, uint32_t max_minor, DLManagedTensorVersioned **out) {
+  return protect([&] {
+    require(a && out);
+    *out = nullptr;
+    DLManagedTensorVersioned *t = export_array<DLManagedTensorVersioned>(*a);
+    t->version = DLPackVersion{DLPACK_MAJOR_VERSION, std::min<uint32_t>(max_minor, DLPACK_MINOR_VERSION)};
+    t->flags = 0;  // shared, writable storage: no copy was made
+    *out = t;
+  });
+}
+
+brook_status brook_context_wait_stream(brook_context *ctx, int64_t producer) {
+  return protect([&] {
+    require(ctx);
+    require(producer >= 0, "invalid producer stream handle");
+    bk::DeviceGuard guard(ctx->value.device());
+    cudaStream_t stream = producer <= 1 ? cudaStreamLegacy
+                          : producer == 2 ? cudaStreamPerThread
+                                          : reinterpret_cast<cudaStream_t>(static_cast<uintptr_t>(producer));
+    cudaEvent_t event = nullptr;
+    BK_CUDA(cudaEventCreateWithFlags(&event, cudaEventDisableTiming));
+    cudaError_t status = cudaEventRecord(event, stream);
+    if (status == cudaSuccess) status = cudaStreamWaitEvent(ctx->value.stream(), event, 0);
+    cudaEventDestroy(event);
+    BK_CUDA(status);
+  });
+}
+
 brook_status brook_connected_components(brook_context *ctx, const brook_volume *labels, brook_components **out) {
   return protect([&] {
     require(ctx && labels && out);
@@ -385,6 +555,19 @@ brook_status brook_components_view(const brook_components *c, brook_volume *labe
     if (count) *count = c->roots.size();
   });
 }
+brook_status brook_components_labels(const brook_components *c, brook_array **out) {
+  return protect([&] {
+    require(c && out);
+    *out = nullptr;
+    auto handle = std::make_unique<brook_array>();
+    handle->storage = c->storage;
+    handle->view = c->view;
+    handle->bytes = c->bytes;
+    volume_tensor(*handle);
+    *out = handle.release();
+  });
+}
+
 brook_status brook_components_copy_to_host(const brook_components *c, void *out, size_t bytes) {
   return protect([&] {
     require(c && (out || !bytes));
@@ -414,6 +597,7 @@ brook_status brook_edt(brook_context *ctx, const brook_volume *labels, const flo
     }
     ctx->value.synchronize();
     handle->view = device_view(handle->storage->ptr, BROOK_F32, st.volume.d);
+    volume_tensor(*handle);
     *out = handle.release();
   });
 }
@@ -439,12 +623,18 @@ void brook_skeletonize_options_init(brook_skeletonize_options *p) {
 brook_status brook_skeletonize(brook_context *ctx, const brook_volume *labels, const brook_skeletonize_options *p,
                                brook_skeletons **out) {
   if (!labels) return protect([] { require(false); });
-  return skeletonize_many(ctx, labels, 1, p, out);
+  return skeletonize_many(ctx, labels, 1, p, nullptr, out);
 }
 
 brook_status brook_skeletonize_batch(brook_context *ctx, const brook_volume *volumes, size_t count,
                                      const brook_skeletonize_options *p, brook_skeletons **out) {
-  return skeletonize_many(ctx, volumes, count, p, out);
+  return skeletonize_many(ctx, volumes, count, p, nullptr, out);
+}
+
+brook_status brook_skeletonize_batch_targets(brook_context *ctx, const brook_volume *volumes, size_t count,
+                                             const brook_skeletonize_options *p, const brook_sample_targets *targets,
+                                             brook_skeletons **out) {
+  return skeletonize_many(ctx, volumes, count, p, targets, out);
 }
 
 brook_status brook_skeletons_get_view(const brook_skeletons *r, brook_skeletons_view *out) {
@@ -505,9 +695,18 @@ brook_status brook_skeletons_get_array(const brook_skeletons *r, brook_skeleton_
     const size_t V = size_t(p.vertex_offsets.back()), E = size_t(p.edge_offsets.back());
     auto handle = std::make_unique<brook_array>();
     switch (buffer) {
-      case BROOK_VERTICES: handle->storage = p.device_vertices; handle->view = skeleton_view(*p.device_vertices, BROOK_F32, 3, V); break;
-      case BROOK_EDGES: handle->storage = p.device_edges; handle->view = skeleton_view(*p.device_edges, BROOK_U32, 2, E); break;
-      case BROOK_RADII: handle->storage = p.device_radii; handle->view = skeleton_view(*p.device_radii, BROOK_F32, 1, V); break;
+      case BROOK_VERTICES:
+        handle->storage = p.device_vertices; handle->view = skeleton_view(*p.device_vertices, BROOK_F32, 3, V);
+        rows_tensor(*handle, 3, V);
+        break;
+      case BROOK_EDGES:
+        handle->storage = p.device_edges; handle->view = skeleton_view(*p.device_edges, BROOK_U32, 2, E);
+        rows_tensor(*handle, 2, E);
+        break;
+      case BROOK_RADII:
+        handle->storage = p.device_radii; handle->view = skeleton_view(*p.device_radii, BROOK_F32, 1, V);
+        rows_tensor(*handle, 1, V);
+        break;
       default: throw std::invalid_argument("invalid skeleton buffer");
     }
     handle->bytes = handle->storage->bytes;

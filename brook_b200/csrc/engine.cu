@@ -133,6 +133,11 @@ struct Group {
 template <class T>
 __device__ __forceinline__ T vload(const T *p) { return *(const volatile T *)p; }
 
+// A loop bound, lowered to the test cap when one is set.
+__device__ __forceinline__ long long capped(const EngineArgs &a, long long bound) {
+  return a.round_limit > 0 && a.round_limit < bound ? a.round_limit : bound;
+}
+
 // Per-CTA staging of a round's frontier in shared memory. When every CTA's share of the frontier
 // fits, a CTA stages its own share (step A) and spreads only that share's (voxel, neighbour) items
 // over its threads (step B): the items then read their voxel's staged fields from shared memory
@@ -214,7 +219,7 @@ __device__ bool flood_geometric(const EngineArgs &a, Shared &sh, Shared *L, floa
     L->cnt[0] = 1; L->cnt[1] = 0; L->cnt[2] = 0;
   }
   G::sync();
-  const long long bound = 8LL * sh.count + 256;
+  const long long bound = capped(a, 8LL * sh.count + 256);
   for (int r = 0;; ++r) {
     int *cur = (r & 1) ? B : A, *nxt = (r & 1) ? A : B;
     const int nc = vload(&L->cnt[r % 3]);
@@ -400,7 +405,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
     }
   }
   int *far = FA, *keep = FB;
-  const long long bound = 16LL * sh.count + 256;
+  const long long bound = capped(a, 16LL * sh.count + 256);
   long long work = 0;
   int r = 0;
   for (;;) {
@@ -621,7 +626,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
   }
   G::sync();
   int *far = FA, *keep = FB;
-  const long long bound = 64LL * sh.count + 1024;
+  const long long bound = capped(a, 64LL * sh.count + 1024);
   long long work = 0;
   int band = 0, r = 0;
   for (;;) {

@@ -82,6 +82,10 @@ struct EngineArgs {
   // railroad, backtrace, invalidation; railroad rounds; invalidation rounds
   unsigned long long *profile;
   float wx, wy, wz, scale, constant, delta;
+  // A lower cap on the round bounds of every flood (0: none). The bounds guard against a loop
+  // that does not end; the cap lets a test make one run out and check that the call fails with
+  // kBudget and leaves the device usable.
+  long long round_limit;
 };
 
 // Objects with at least kPrepareClusterVoxels voxels (preparation) or more voxels than

@@ -112,8 +112,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       throw std::invalid_argument("odd pdrf_exponent makes the background penalty negative");
   }
   if (!opt.fix_branching) throw std::invalid_argument("fix_branching=False is not supported by this build");
-  if ((!opt.targets_before.empty() || !opt.targets_after.empty()) && volumes.size() != 1)
-    throw std::invalid_argument("extra targets are given for one volume at a time");
+  if (opt.targets_before.size() > volumes.size() || opt.targets_after.size() > volumes.size())
+    throw std::invalid_argument("extra targets are given for more volumes than the call holds");
   const double exponent = t.pdrf_exponent;
   if (!(exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))))
     throw std::invalid_argument("pdrf_exponent must be a power of two in this build");
@@ -231,28 +231,37 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   if (nobj == 0) return results;
   // extra targets by the component they fall on (skeletonize.cu:16-25, 61-65 of the reference): a
   // negative coordinate counts from the end of its axis; a point outside the volume is an error;
-  // points on the background or on objects that are not traced are dropped
+  // points on the background or on objects that are not traced are dropped. Each volume's points
+  // are in its own frame.
   std::vector<std::vector<int>> before_of(nobj), after_of(nobj);
-  if (!opt.targets_before.empty() || !opt.targets_after.empty()) {
-    const auto &st = vs[0];
-    std::vector<long long> flats;
-    for (int list = 0; list < 2; ++list)
-      for (auto p : list ? opt.targets_after : opt.targets_before) {
-        const long long shape[3] = {st.d.sx, st.d.sy, st.d.sz};
-        for (int a = 0; a < 3; ++a) {
-          if (p[a] < 0) p[a] += shape[a];
-          if (p[a] < 0 || p[a] >= shape[a]) throw std::invalid_argument("extra target is outside the input volume");
+  {
+    struct Pick { size_t volume; bool after; long long flat; };
+    std::vector<Pick> picks;
+    for (size_t v = 0; v < volumes.size(); ++v)
+      for (int list = 0; list < 2; ++list) {
+        const auto &lists = list ? opt.targets_after : opt.targets_before;
+        if (v >= lists.size()) continue;
+        const auto &st = vs[v];
+        const long long shape[3] = {volumes[v].d.sx, volumes[v].d.sy, volumes[v].d.sz};
+        for (auto p : lists[v]) {
+          for (int a = 0; a < 3; ++a) {
+            if (p[a] < 0) p[a] += shape[a];
+            if (p[a] < 0 || p[a] >= shape[a]) throw std::invalid_argument("extra target is outside the input volume");
+          }
+          if (st.empty) continue;  // a volume at or below the dust threshold traces nothing
+          picks.push_back({v, list == 1, st.offset + p[0] + shape[0] * (p[1] + shape[1] * p[2])});
         }
-        flats.push_back(st.offset + p[0] + shape[0] * (p[1] + shape[1] * p[2]));
       }
-    std::vector<uint32_t> at(flats.size());
-    for (size_t i = 0; i < flats.size(); ++i)
-      BK_CUDA(cudaMemcpyAsync(&at[i], ids.data() + flats[i], sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    ctx.synchronize();
-    for (size_t i = 0; i < flats.size(); ++i) {
-      const int o = at[i] ? st.object_of[at[i]] : -1;
-      if (o < 0) continue;
-      (i < opt.targets_before.size() ? before_of : after_of)[o].push_back(int(flats[i]));
+    if (!picks.empty()) {
+      std::vector<uint32_t> at(picks.size());
+      for (size_t i = 0; i < picks.size(); ++i)
+        BK_CUDA(cudaMemcpyAsync(&at[i], ids.data() + picks[i].flat, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      ctx.synchronize();
+      for (size_t i = 0; i < picks.size(); ++i) {
+        const int o = at[i] ? vs[picks[i].volume].object_of[at[i]] : -1;
+        if (o < 0) continue;
+        (picks[i].after ? after_of : before_of)[o].push_back(int(picks[i].flat));
+      }
     }
   }
   std::vector<int> after_begin(nobj), after_count(nobj), after;
@@ -381,6 +390,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.wx = aniso[0]; a.wy = aniso[1]; a.wz = aniso[2];
   a.scale = float(t.scale); a.constant = float(t.constant);
   a.delta = std::min({aniso[0], aniso[1], aniso[2]});
+  a.round_limit = 0;
+  if (const char *e = std::getenv("BROOK_B200_TEST_ROUND_LIMIT")) a.round_limit = std::atoll(e);  // test knob
 
   clock.mark("state");
   const int ctas = cluster_ctas(nobj ? obj_count[schedule[0]] : 0, F);

@@ -24,7 +24,9 @@ struct Options {
   double dust = 1000;
   bool fix_branching = true, fix_borders = true;
   std::optional<std::vector<int64_t>> object_ids;
-  std::vector<Point> targets_before, targets_after;
+  // extra targets per volume of the call (x, y, z in that volume's frame); volumes beyond the
+  // vectors' ends have none
+  std::vector<std::vector<Point>> targets_before, targets_after;
   bool device_output = false;  // keep vertices, edges and radii on the device (BROOK_DEVICE_OUTPUT)
 };
 

@@ -24,6 +24,10 @@ typedef struct brook_context brook_context;     /* brook.h:17 */
 typedef struct brook_array brook_array;         /* brook.h:18 */
 typedef struct brook_components brook_components; /* brook.h:19 */
 typedef struct brook_skeletons brook_skeletons; /* brook.h:21 */
+/* brook.h:22-24: include brook_b200_dlpack.h (or the standard dlpack/dlpack.h) to read the
+ * exported tensors' fields. */
+typedef struct DLManagedTensor DLManagedTensor;
+typedef struct DLManagedTensorVersioned DLManagedTensorVersioned;
 
 /* brook.h:26-29 */
 typedef enum brook_status {
@@ -119,10 +123,22 @@ brook_status brook_context_create(int device, brook_context **out);
 void brook_context_destroy(brook_context *context);              /* brook.h:155 */
 brook_status brook_context_synchronize(brook_context *context);  /* brook.h:156 */
 
-/* brook.h:159-162: device arrays owned by the handle */
+/* brook.h:159-162: device arrays owned by the handle. brook_array_upload copies a volume (host
+ * or device memory of the context's device, any strides, any of the ten element types) into a
+ * Fortran-ordered device array of the same shape and type; the copy is complete on return. */
+brook_status brook_array_upload(brook_context *context, const brook_volume *input, brook_array **out);
 void brook_array_destroy(brook_array *array);
 brook_status brook_array_view(const brook_array *array, brook_volume *out);
 brook_status brook_array_copy_to_host(const brook_array *array, void *out, size_t bytes);
+/* brook.h:163-167: zero-copy DLPack exports of an array's device storage (kDLCUDA, the array's
+ * device). A volume exports as shape (x, y, z) with strides (1, x, x*y) elements; a skeleton
+ * buffer as its row-major (rows, 3), (rows, 2) or (rows,) form. Each export holds its own
+ * reference to the storage, so it stays valid after the array handle and the context are
+ * destroyed; the consumer calls the returned tensor's deleter exactly once. The versioned form
+ * reports DLPack 1.min(max_minor, 1) and no flags. */
+brook_status brook_array_to_dlpack(const brook_array *array, DLManagedTensor **out);
+brook_status brook_array_to_dlpack_versioned(const brook_array *array, uint32_t max_minor,
+                                             DLManagedTensorVersioned **out);
 
 /* brook.h:169-177: 26-connected components; ids 1..K by ascending first voxel (Fortran order),
  * stored in the narrowest unsigned type that holds K. */
@@ -132,6 +148,9 @@ void brook_components_destroy(brook_components *components);
 brook_status brook_components_view(const brook_components *components, brook_volume *labels,
                                    const int64_t **mapping, const int64_t **roots, size_t *count);
 brook_status brook_components_copy_to_host(const brook_components *components, void *out, size_t bytes);
+/* brook.h:182: the component ids as an array handle sharing the components' storage (it stays
+ * valid after brook_components_destroy). */
+brook_status brook_components_labels(const brook_components *components, brook_array **out);
 
 /* brook.h:180-181: anisotropic distance to the nearest voxel of another label (float32). */
 brook_status brook_edt(brook_context *context, const brook_volume *labels, const float anisotropy[3],
@@ -148,6 +167,29 @@ brook_status brook_skeletonize(brook_context *context, const brook_volume *label
  * engine; out receives `count` result handles (one per volume, in input order). */
 brook_status brook_skeletonize_batch(brook_context *context, const brook_volume *volumes, size_t count,
                                      const brook_skeletonize_options *options, brook_skeletons **out);
+
+/* Per-sample extra targets of a batch (the reference's Python skeletonize_batch takes them as one
+ * sequence per sample, src/brook/batch.py:173-190, 206-220): x, y, z triples in the sample's own
+ * frame, as brook_skeletonize_options' targets_before / targets_after are for one volume. */
+typedef struct brook_sample_targets {
+  const int64_t *before;
+  size_t before_count;
+  const int64_t *after;
+  size_t after_count;
+} brook_sample_targets;
+/* brook_skeletonize_batch with targets[i] for volumes[i] (`count` entries); the options must then
+ * carry no targets of their own. */
+brook_status brook_skeletonize_batch_targets(brook_context *context, const brook_volume *volumes, size_t count,
+                                             const brook_skeletonize_options *options,
+                                             const brook_sample_targets *targets, brook_skeletons **out);
+
+/* Makes the context's stream wait for the work queued so far on a producer's stream, without
+ * blocking the host: call it before passing device memory that a kernel on another stream is
+ * still writing. producer: 0 or 1 the legacy default stream, 2 the per-thread default stream,
+ * anything else a cudaStream_t of the context's device (the CUDA array interface's convention).
+ * The reference's Python binding does the same for every device input (fence_producer,
+ * cpp/python/bindings.cpp:104-120); its C header leaves it to the caller. */
+brook_status brook_context_wait_stream(brook_context *context, int64_t producer);
 
 /* brook.h:238-252. A device result (BROOK_DEVICE_OUTPUT) is copied to the host on the first call. */
 brook_status brook_skeletons_get_view(const brook_skeletons *result, brook_skeletons_view *out);

@@ -1,8 +1,7 @@
 """Writes join_digests.json: the expected summaries of the reference's join tests.
 
-Run in a container that holds the reference checkout (default /root/reference); the expected
-values are read from its test file, where they are written as literals
-(tests/python/test_package.py:2079-2113).
+Usage: python make_golden.py <reference checkout>. The expected values are read from the
+reference's test file, where they are written as literals (tests/python/test_package.py:2079-2113).
 """
 from __future__ import annotations
 
@@ -11,11 +10,10 @@ import os
 import re
 import sys
 
-REFERENCE = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-
-
 def main():
-    text = open(os.path.join(REFERENCE, "tests/python/test_package.py")).read()
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <reference checkout>")
+    text = open(os.path.join(sys.argv[1], "tests/python/test_package.py")).read()
     entry = r"\((\d+), (\d+), ([0-9.]+), \"([0-9a-f]{16})\"\)"
     single = re.search(r"parametrize\(\"axis,digest\", \[(.*?)\]\)", text).group(1)
     out = {}
