@@ -155,21 +155,38 @@ def result_bytes(packed):
                packed.v_off.nbytes + packed.e_off.nbytes)
 
 
-def cpu_baseline(volume, cfg, threads):
-    """The oracle (the CPU restatement of the reference's algorithm) on a 256^3 crop of the volume."""
+def oracle_whole(volume, cfg, threads, steps):
+    """The oracle (the CPU restatement of the reference's algorithm) over the whole workload volume,
+    its work spread over `steps` timed steps: step 0 runs the preamble (components, boxes, EDT,
+    border targets, roots, DAF, PDRF, target orders) and each step traces its share of the objects
+    in the largest-first order; the last step assembles. Returns (seconds of all steps, skeletons,
+    the oracle's per-stage ms)."""
     from oracle import oracle
 
-    crop = tuple(min(256, s) for s in volume.shape)
-    sample = np.asfortranarray(volume[:crop[0], :crop[1], :crop[2]])
     t0 = time.perf_counter()
-    oracle.skeletonize(sample, PARAMS, cfg["anisotropy"], DUST, threads=threads)
-    dt = time.perf_counter() - t0
-    return {"value": sample.size / dt, "unit": "voxels/s", "cores": threads, "kind": "port",
-            "sample": f"{crop[0]}x{crop[1]}x{crop[2]} crop ({sample.size} voxels) of the workload volume, "
-                      f"{dt:.2f} s on {threads} threads"}
+    run = oracle.StagedRun(volume, PARAMS, cfg["anisotropy"], DUST, threads=threads)
+    per = -(-run.objects // steps) if run.objects else 0
+    for k in range(steps):
+        run.trace(k * per, (k + 1) * per)
+    result = run.finish()
+    return time.perf_counter() - t0, len(result.array("labels")), result.stage_ms()
+
+
+def cpu_baseline(volume, cfg, threads):
+    """The oracle on the whole workload volume, on every host core."""
+    dt, skeletons, stages = oracle_whole(volume, cfg, threads, 1)
+    return {"value": volume.size / dt, "unit": "voxels/s", "cores": threads, "kind": "port",
+            "sample": f"the whole {'x'.join(map(str, volume.shape))} workload volume ({volume.size} voxels, "
+                      f"{skeletons} skeletons), {dt:.2f} s on {threads} threads",
+            "stages_ms": {k: round(v, 1) for k, v in stages.items()}}
 
 
 def run_reference(args, cfg):
+    """The reference arm: the CPU restatement of the reference's algorithm (the reference has no
+    CPU implementation of this path; its GPU code is not built here) on the same whole volume as
+    our arm, on all host cores. The W warm-up steps run it on a 64^3 crop; the K timed steps
+    together process the whole volume once (oracle_whole), so value = voxels / time of the K
+    steps. Only rank 0 works; this process never loads libbrook_b200.so."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -177,27 +194,31 @@ def run_reference(args, cfg):
 
     volume = make_volume(cfg)
     threads = os.cpu_count() or 1
-    crop = tuple(min(128, s) for s in volume.shape)
-    sample = np.asfortranarray(volume[:crop[0], :crop[1], :crop[2]])
+    crop = np.asfortranarray(volume[:64, :64, :64])
     for _ in range(args.warmup):
-        oracle.skeletonize(sample, PARAMS, cfg["anisotropy"], DUST, threads=threads)
-    t0 = time.perf_counter()
-    skeletons = 0
-    for _ in range(args.steps):
-        r = oracle.skeletonize(sample, PARAMS, cfg["anisotropy"], DUST, threads=threads)
-        skeletons = len(r.array("labels"))
-    dt = (time.perf_counter() - t0) / args.steps
-    value = sample.size / dt
+        oracle.skeletonize(crop, PARAMS, cfg["anisotropy"], DUST, threads=threads)
+    dt, skeletons, stages = oracle_whole(volume, cfg, threads, args.steps)
+    value = volume.size / dt
+    sample = (f"the whole {'x'.join(map(str, volume.shape))} volume ({volume.size} voxels) once over the "
+              f"{args.steps} timed steps: the preamble in the first, the objects' traces split over all, assembly in "
+              f"the last; warm-up steps on a 64^3 crop")
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "int64/f32", "data": "synthetic",
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32", "data": "synthetic",
            "skeletons_per_s": skeletons / dt,
-           "config": {"workload": cfg["workload"], "sample": f"{crop[0]}x{crop[1]}x{crop[2]} crop per step",
-                      "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST},
-           "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": threads, "kind": "port",
-                            "sample": f"{crop[0]}x{crop[1]}x{crop[2]} crop ({sample.size} voxels) of the workload volume"},
+           "config": config_of(cfg, volume),
+           "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": threads, "kind": "port", "sample": sample,
+                            "stages_ms": {k: round(v, 1) for k, v in stages.items()}},
            "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
+
+
+def config_of(cfg, volume, world=1):
+    """The workload description both arms print (same keys and values for the same workload)."""
+    return {"workload": cfg["workload"], "voxels_per_gpu": int(volume.size), "anisotropy": list(cfg["anisotropy"]),
+            "teasar": PARAMS, "dust_threshold": DUST, "parallelism": f"replicas x{world}",
+            "l2": f"labels of {volume.nbytes / 2**20:.0f} MiB per step, "
+                  + ("larger than L2 (126 MB)" if volume.nbytes > 126e6 else "smaller than L2: not flushed")}
 
 
 def run_batch(args, cfg):
@@ -206,9 +227,6 @@ def run_batch(args, cfg):
     the same batch is split over the ranks (longest-first by voxels, brook_b200.sharding), each
     rank runs its share as one batch and rank 0 gathers the results: strong scaling."""
     import torch
-
-    import brook_b200
-    from brook_b200 import _native, sharding
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -219,6 +237,20 @@ def run_batch(args, cfg):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    line = batch_measurement(cfg, args.steps, args.warmup, rank, world, local, dist)
+    if line is not None:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def batch_measurement(cfg, steps, warmup, rank=0, world=1, local=0, dist=None):
+    """run_batch's measurement; returns rank 0's line (None on the other ranks)."""
+    import torch
+
+    import brook_b200
+    from brook_b200 import _native, sharding
+
     volumes = make_volume(cfg)  # the same batch on every rank
     mine = sharding.partition([v.size for v in volumes], world)[rank]
     devs = {i: torch.from_numpy(np.ascontiguousarray(volumes[i].transpose(2, 1, 0))).cuda(local).permute(2, 1, 0)
@@ -255,12 +287,12 @@ def run_batch(args, cfg):
     else:
         batched = lambda: brook_b200.skeletonize_batch([devs[i] for i in mine], output="packed", **opts)  # noqa: E731
     plain = lambda: [brook_b200.skeletonize(devs[i], output="packed", **opts) for i in mine]  # noqa: E731
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         batched()
     with ClockSampler(local) as clocks:
-        ms, out, stage = timed(batched, args.steps)
+        ms, out, stage = timed(batched, steps)
     plain()
-    plain_ms, plain_out, _ = timed(plain, max(1, args.steps // 2))
+    plain_ms, plain_out, _ = timed(plain, max(1, steps // 2))
     # identical skeletons both ways (rank 0 holds the whole batch; with one rank `mine` is all)
     if out is not None:
         for j, p in enumerate(plain_out):
@@ -279,18 +311,16 @@ def run_batch(args, cfg):
         e2e_fn = lambda: sharding.skeletonize_batch_sharded(host_samples, rank, world, **opts)  # noqa: E731
     else:
         e2e_fn = lambda: brook_b200.skeletonize_batch([pinned[i] for i in mine], output="packed", **opts)  # noqa: E731
-    e2e_ms, out_h, _ = timed(e2e_fn, args.steps)
+    e2e_ms, out_h, _ = timed(e2e_fn, steps)
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
-        return
+        return None
     skeletons = len(out.labels)
     voxels = sum(int(v.size) for v in volumes)
     plain_skeletons = sum(len(p) for p in plain_out)
     stage_ms = {k[3:]: v for k, v in stage.items() if k.startswith("ms_") and k != "ms_total"}
     out_line = {
-        "metric": METRIC, "value": skeletons / (ms / 1e3), "unit": "skeletons/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "metric": METRIC, "value": skeletons / (ms / 1e3), "unit": "skeletons/s", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "int32/f32", "data": "synthetic", "voxels_per_s": voxels / (ms / 1e3),
         "per_volume": {"skeletons_per_s": plain_skeletons / (plain_ms / 1e3), "ms_per_step": plain_ms,
                        "volumes": len(mine), "speedup_batched": (skeletons / ms) / (plain_skeletons / plain_ms),
@@ -306,12 +336,10 @@ def run_batch(args, cfg):
                 "h2d_bytes_per_step": int(sum(volumes[i].nbytes for i in mine)),
                 "d2h_bytes_per_step": int(out_h.packed.vertices.nbytes + out_h.packed.edges.nbytes +
                                           out_h.packed.radii.nbytes)},
-        "gpu_launches": int(stage.get("launches", 0) * args.steps),
+        "gpu_launches": int(stage.get("launches", 0) * steps),
         "clocks": clocks.summary(),
     }
-    print(json.dumps(out_line))
-    if dist is not None:
-        dist.destroy_process_group()
+    return out_line
 
 
 def run_chunks(args, cfg):
@@ -373,13 +401,18 @@ def run_serve(args, cfg):
     server and through the plain per-request path (one worker, one request per call)."""
     import torch
 
-    from brook_b200 import serving, synthetic
-
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if rank != 0:  # requests are served by one GPU; other ranks have nothing to do
         return
+    print(json.dumps(serve_measurement(cfg, local)))
+
+
+def serve_measurement(cfg, local=0):
+    """run_serve's measurement: the line as a dict."""
+    from brook_b200 import serving, synthetic
+
     base = synthetic.serving_requests(cfg["requests"], 1.0, seed=cfg["seed"])  # arrivals at rate 1, rescaled below
     opts = dict(teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST, device=local,
                 memory_cap=80e9)
@@ -403,7 +436,7 @@ def run_serve(args, cfg):
             rates[str(rate)] = row
     head = rates[str(cfg["rates"][1])]["batched"]
     voxels = int(sum(v.size for _, v in base))
-    print(json.dumps({
+    return {
         "metric": METRIC, "value": head["skeletons_per_s"], "unit": "skeletons/s", "n_gpus": 1,
         "steps": len(cfg["rates"]), "warmup": 1, "ms_per_step": head["wall_s"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32", "data": "synthetic",
@@ -414,7 +447,33 @@ def run_serve(args, cfg):
         "e2e": {"value": head["skeletons_per_s"], "unit": "skeletons/s",
                 "h2d_bytes_per_step": int(sum(v.nbytes for _, v in base)), "d2h_bytes_per_step": None},
         "clocks": clocks.summary(),
-    }))
+    }
+
+
+def extra_measurements(local):
+    """The metric's two comparisons beside the headline line, on the same GPU: the 64-volume uneven
+    batch as one skeletonize_batch call against 64 plain calls (skeletons/s both ways, identical
+    skeletons checked), and the request stream's p50/p99 latency at 50/200/800 req/s through the
+    continuous-batching server and the per-request path."""
+    extras = {}
+    try:
+        b = batch_measurement(CONFIGS["batch64"], steps=3, warmup=2, local=local)
+        extras["batch64"] = {
+            "workload": CONFIGS["batch64"]["workload"], "batched_skeletons_per_s": b["value"],
+            "batched_ms_per_call": b["ms_per_step"], "per_volume_skeletons_per_s": b["per_volume"]["skeletons_per_s"],
+            "per_volume_ms_per_64_calls": b["per_volume"]["ms_per_step"],
+            "speedup_batched": b["per_volume"]["speedup_batched"], "identical": b["per_volume"]["identical"],
+            "e2e_batched_skeletons_per_s": b["e2e"]["value"], "stages_ms": b["stages_ms"],
+            "timing": "CUDA events on the device, 3 batched calls and 1 round of 64 plain calls after 2 warm-ups"}
+    except Exception as e:  # the headline line still prints
+        extras["batch64"] = {"error": f"{type(e).__name__}: {e}"}
+    try:
+        v = serve_measurement(CONFIGS["serve"], local)
+        extras["serve"] = {"workload": CONFIGS["serve"]["workload"], "latency_ms": v["latency_ms"],
+                           "timing": "wall clock per request, arrival to result"}
+    except Exception as e:
+        extras["serve"] = {"error": f"{type(e).__name__}: {e}"}
+    return extras
 
 
 def run_ours(args, cfg):
@@ -499,10 +558,8 @@ def run_ours(args, cfg):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/f32", "data": "synthetic",
         "skeletons_per_s": skeletons / (ms / 1e3),
-        "config": {"workload": cfg["workload"], "voxels_per_gpu": int(volume.size), "objects": int(stage.get("objects", 0)),
-                   "anisotropy": cfg["anisotropy"], "teasar": PARAMS, "dust_threshold": DUST,
-                   "parallelism": f"replicas x{world}", "l2": f"labels of {volume.nbytes / 2**20:.0f} MiB per step, "
-                         + ("larger than L2 (126 MB)" if volume.nbytes > 126e6 else "smaller than L2: not flushed")},
+        "config": config_of(cfg, volume, world),
+        "objects": int(stage.get("objects", 0)),
         "stages_ms": {k: round(v, 3) for k, v in sorted(stage_ms.items())},
         "stages_roofline": stage_roofline(stage, peaks()[0]),
         "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
@@ -517,6 +574,8 @@ def run_ours(args, cfg):
     }
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(volume, cfg, os.cpu_count() or 1)
+    if world == 1 and not args.no_extras:
+        out.update(extra_measurements(local))
     print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
@@ -530,6 +589,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="dense512", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batch and serving comparisons")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":

@@ -29,6 +29,8 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <chrono>
+#include <memory>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -86,6 +88,28 @@ struct Shape {
 inline uint32_t fbits(float f) { uint32_t b; std::memcpy(&b, &f, 4); return b; }
 inline float bitsf(uint32_t b) { float f; std::memcpy(&f, &b, 4); return f; }
 
+// fn(begin, end) over [0, n) in chunks of `grain`, on `threads` threads (the caller's among
+// them). Every use below splits work whose items write disjoint data, so the result does not
+// depend on the thread count.
+template <class F>
+void parallel_for(i64 n, int threads, i64 grain, F &&fn) {
+  if (n <= 0) return;
+  const int workers = int(std::max<i64>(1, std::min<i64>(threads, (n + grain - 1) / grain)));
+  if (workers == 1) { fn(i64(0), n); return; }
+  std::atomic<i64> next{0};
+  auto work = [&] {
+    for (;;) {
+      const i64 b = next.fetch_add(grain);
+      if (b >= n) return;
+      fn(b, std::min(n, b + grain));
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < workers; ++t) pool.emplace_back(work);
+  work();
+  for (auto &t : pool) t.join();
+}
+
 // ---------------------------------------------------------------------------------------------
 // Connected components (ccl.cu:25-63): 26-connected components of equal nonzero labels. The
 // union-find root of a component is its lowest flat index; ids 1..K follow ascending roots.
@@ -95,8 +119,11 @@ struct Components {
   std::vector<int64_t> roots;   // id-1 -> first flat index
 };
 
+// Linking the larger root under the smaller one keeps every tree's root at its least flat index,
+// whatever order the unions come in: z-slabs are joined in parallel (every union inside a slab
+// touches only that slab's entries), then the pairs across slab boundaries one by one.
 template <class L>
-Components connected_components(const L *labels, const Shape &s) {
+Components connected_components(const L *labels, const Shape &s, int threads = 1) {
   const i64 n = s.n();
   std::vector<i64> parent(n);
   std::iota(parent.begin(), parent.end(), i64(0));
@@ -106,18 +133,28 @@ Components connected_components(const L *labels, const Shape &s) {
     while (parent[v] != r) { i64 next = parent[v]; parent[v] = r; v = next; }
     return r;
   };
-  for (i64 v = 0; v < n; ++v) {
-    if (labels[v] == 0) continue;
+  auto unite_from = [&](i64 v, i64 zlo, i64 zhi) {  // v's forward neighbours with z in [zlo, zhi)
+    if (labels[v] == 0) return;
     i64 x, y, z; s.xyz(v, x, y, z);
     for (int k = 0; k < 26; ++k) {
       i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
-      if (!s.inside(nx, ny, nz)) continue;
+      if (!s.inside(nx, ny, nz) || nz < zlo || nz >= zhi) continue;
       i64 u = s.idx(nx, ny, nz);
       if (u <= v || labels[u] != labels[v]) continue;
       i64 a = find(v), b = find(u);
       if (a != b) { if (a < b) parent[b] = a; else parent[a] = b; }
     }
-  }
+  };
+  const i64 plane = s.sx * s.sy, depth = std::max<i64>(1, (s.sz + threads - 1) / std::max(threads, 1));
+  const i64 slabs = (s.sz + depth - 1) / depth;
+  parallel_for(slabs, threads, 1, [&](i64 b, i64 e) {
+    for (i64 k = b; k < e; ++k) {
+      const i64 z0 = k * depth, z1 = std::min(s.sz, z0 + depth);
+      for (i64 v = z0 * plane; v < z1 * plane; ++v) unite_from(v, z0, z1);
+    }
+  });
+  for (i64 k = 1; k < slabs; ++k)  // plane z0 - 1 with plane z0
+    for (i64 v = (k * depth - 1) * plane; v < k * depth * plane; ++v) unite_from(v, k * depth, k * depth + 1);
   Components c;
   c.ids.assign(n, 0);
   c.mapping.push_back(0);
@@ -135,16 +172,16 @@ Components connected_components(const L *labels, const Shape &s) {
   return c;
 }
 
-Components components_any(const void *labels, int dtype, const Shape &s) {
+Components components_any(const void *labels, int dtype, const Shape &s, int threads) {
   switch (dtype) {
-    case 0: return connected_components(static_cast<const uint8_t *>(labels), s);
-    case 1: return connected_components(static_cast<const uint16_t *>(labels), s);
-    case 2: return connected_components(static_cast<const uint32_t *>(labels), s);
-    case 3: return connected_components(static_cast<const uint64_t *>(labels), s);
-    case 4: return connected_components(static_cast<const int8_t *>(labels), s);
-    case 5: return connected_components(static_cast<const int16_t *>(labels), s);
-    case 6: return connected_components(static_cast<const int32_t *>(labels), s);
-    case 7: return connected_components(static_cast<const int64_t *>(labels), s);
+    case 0: return connected_components(static_cast<const uint8_t *>(labels), s, threads);
+    case 1: return connected_components(static_cast<const uint16_t *>(labels), s, threads);
+    case 2: return connected_components(static_cast<const uint32_t *>(labels), s, threads);
+    case 3: return connected_components(static_cast<const uint64_t *>(labels), s, threads);
+    case 4: return connected_components(static_cast<const int8_t *>(labels), s, threads);
+    case 5: return connected_components(static_cast<const int16_t *>(labels), s, threads);
+    case 6: return connected_components(static_cast<const int32_t *>(labels), s, threads);
+    case 7: return connected_components(static_cast<const int64_t *>(labels), s, threads);
     default: throw std::invalid_argument("integer labels required");
   }
 }
@@ -153,10 +190,11 @@ Components components_any(const void *labels, int dtype, const Shape &s) {
 // Multi-label anisotropic EDT (edt_kernels.cuh:15-144, edt.cu:12-15). Distance of each voxel to
 // the nearest voxel of a different label; with black_border the volume edge counts as such a
 // voxel. `dims` = 2 skips the z pass (the 2D face transforms of the border targets).
-void edt_pass_x(const uint32_t *lab, float *D, const Shape &s, float w, bool bb) {
+void edt_pass_x(const uint32_t *lab, float *D, const Shape &s, float w, bool bb, int threads) {
   std::vector<float> acc(s.sx + 2, 0.0f);
   for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + w;  // one float32 rounding per step
-  for (i64 line = 0; line < s.sy * s.sz; ++line) {
+  parallel_for(s.sy * s.sz, threads, 256, [&](i64 lb, i64 le) {
+  for (i64 line = lb; line < le; ++line) {
     const i64 base = s.sx * line;
     i64 i = 0;
     while (i < s.sx) {
@@ -173,6 +211,7 @@ void edt_pass_x(const uint32_t *lab, float *D, const Shape &s, float w, bool bb)
       i = d + 1;
     }
   }
+  });
 }
 
 // One line of the y / z pass: lower envelope of the parabolas of a run's finite heights and its
@@ -221,18 +260,30 @@ void edt_line_fh(const uint32_t *lab, float *D, i64 base, i64 stride, i64 n, flo
   }
 }
 
-std::vector<float> edt(const uint32_t *lab, const Shape &s, const float aniso[3], bool bb, int dims = 3) {
+std::vector<float> edt(const uint32_t *lab, const Shape &s, const float aniso[3], bool bb, int dims = 3,
+                       int threads = 1) {
   std::vector<float> D(s.n());
-  edt_pass_x(lab, D.data(), s, aniso[0], bb);
+  edt_pass_x(lab, D.data(), s, aniso[0], bb, threads);
   const i64 longest = std::max(s.sy, s.sz) + 3;
-  std::vector<i64> V(longest); std::vector<float> H(longest); std::vector<double> Z(longest);
+  // every line of a pass is independent: planes (y pass) and rows (z pass) go to the threads
+  auto lines = [&](i64 outer, auto &&line) {
+    parallel_for(outer, threads, 1, [&](i64 b, i64 e) {
+      std::vector<i64> V(longest); std::vector<float> H(longest); std::vector<double> Z(longest);
+      for (i64 o = b; o < e; ++o)
+        for (i64 x = 0; x < s.sx; ++x) line(o, x, V, H, Z);
+    });
+  };
   if (dims >= 2)
-    for (i64 z = 0; z < s.sz; ++z)
-      for (i64 x = 0; x < s.sx; ++x) edt_line_fh(lab, D.data(), x + s.sx * s.sy * z, s.sx, s.sy, aniso[1], bb, V, H, Z);
+    lines(s.sz, [&](i64 z, i64 x, auto &V, auto &H, auto &Z) {
+      edt_line_fh(lab, D.data(), x + s.sx * s.sy * z, s.sx, s.sy, aniso[1], bb, V, H, Z);
+    });
   if (dims >= 3)
-    for (i64 y = 0; y < s.sy; ++y)
-      for (i64 x = 0; x < s.sx; ++x) edt_line_fh(lab, D.data(), x + s.sx * y, s.sx * s.sy, s.sz, aniso[2], bb, V, H, Z);
-  for (i64 i = 0; i < s.n(); ++i) D[i] = lab[i] == 0 ? 0.0f : std::sqrt(D[i]);
+    lines(s.sy, [&](i64 y, i64 x, auto &V, auto &H, auto &Z) {
+      edt_line_fh(lab, D.data(), x + s.sx * y, s.sx * s.sy, s.sz, aniso[2], bb, V, H, Z);
+    });
+  parallel_for(s.n(), threads, 1 << 16, [&](i64 b, i64 e) {
+    for (i64 i = b; i < e; ++i) D[i] = lab[i] == 0 ? 0.0f : std::sqrt(D[i]);
+  });
   return D;
 }
 
@@ -732,7 +783,11 @@ Skeleton assemble(const std::vector<std::vector<i64>> &paths, const Shape &s) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// The whole path (skeletonize.cu:70-183 with the lockstep inputs of batched.cu:177-255).
+// The whole path (skeletonize.cu:70-183 with the lockstep inputs of batched.cu:177-255), in three
+// steps: prepare (components, boxes, EDT, border targets, roots, DAF, PDRF, target orders), trace
+// (objects in largest-first order, any sub-range of that order at a time), finish (assembly).
+struct Staged;
+
 struct Result {
   std::vector<int64_t> labels, vertex_offsets{0}, edge_offsets{0};
   std::vector<float> vertices, radii;
@@ -746,12 +801,38 @@ struct Result {
   std::vector<int64_t> orders;                 // concatenated target orders of active ids
   std::vector<int64_t> order_offsets;          // per id (count+2)
   std::vector<int64_t> paths_flat, path_offsets{0}, path_labels;
+  // wall-clock ms of the steps: components, boxes, edt, borders, daf, pdrf, orders, trace, assembly
+  std::vector<double> stage_ms = std::vector<double>(9, 0.0);
+  std::shared_ptr<Staged> staged;  // between prepare and finish
 };
 
-Result run(const void *labels, int dtype, const Shape &s, const Params &P, int threads, int keep_stages) {
-  Result R;
+struct Staged {
+  Shape s;
+  Params P;
+  Volume V;
+  int keep_stages = 0;
+  std::vector<std::array<i64, 7>> box;
+  std::vector<ObjectPlan> plans;
+  std::vector<size_t> schedule;  // plans, largest first
+  std::vector<std::vector<std::vector<i64>>> traced;
+};
+
+struct Lap {
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  double next() {
+    const auto now = std::chrono::steady_clock::now();
+    const double ms = std::chrono::duration<double, std::milli>(now - t).count();
+    t = now;
+    return ms;
+  }
+};
+
+void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Params &P, int threads, int keep_stages) {
+  auto st = std::make_shared<Staged>();
+  st->s = s; st->P = P; st->keep_stages = keep_stages;
+  R.staged = st;
   const i64 n = s.n();
-  if (n == 0 || double(n) <= P.dust) return R;
+  if (n == 0 || double(n) <= P.dust) return;
   for (int a = 0; a < 3; ++a)
     if (!std::isfinite(P.anisotropy[a]) || P.anisotropy[a] <= 0) throw std::invalid_argument("anisotropy must be finite and positive");
   {
@@ -759,12 +840,15 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
     if (std::isfinite(e) && e == std::floor(e) && std::fmod(e, 2.0) == 1.0)
       throw std::invalid_argument("odd pdrf_exponent makes the background penalty negative");
   }
-  R.cc = components_any(labels, dtype, s);
+  Lap lap;
+  R.cc = components_any(labels, dtype, s, threads);
+  R.stage_ms[0] = lap.next();
   const auto &ids = R.cc.ids;
   const size_t count = R.cc.roots.size();
-  if (!count) return R;
+  if (!count) return;
   // bounding boxes and counts (preamble.cu:10-29)
-  std::vector<std::array<i64, 7>> box(count + 1, {INT32_MAX, INT32_MAX, INT32_MAX, -1, -1, -1, 0});
+  auto &box = st->box;
+  box.assign(count + 1, {INT32_MAX, INT32_MAX, INT32_MAX, -1, -1, -1, 0});
   std::vector<std::vector<i64>> voxels(count + 1);
   for (i64 v = 0; v < n; ++v) {
     const uint32_t id = ids[v];
@@ -775,11 +859,15 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
     b[3] = std::max(b[3], x); b[4] = std::max(b[4], y); b[5] = std::max(b[5], z); ++b[6];
     voxels[id].push_back(v);
   }
+  R.stage_ms[1] = lap.next();
   const bool black_border = count == 1 && box[1][6] == n;
-  Volume V; V.s = s; V.ids = &ids;
-  V.dbf = edt(ids.data(), s, P.anisotropy, black_border);
+  Volume &V = st->V;
+  V.s = s; V.ids = &R.cc.ids;
+  V.dbf = edt(ids.data(), s, P.anisotropy, black_border, 3, threads);
+  R.stage_ms[2] = lap.next();
   std::vector<std::vector<std::array<i64, 3>>> borders(count + 1);
   if (P.fix_borders) borders = border_targets(ids, s, count, P.anisotropy);
+  R.stage_ms[3] = lap.next();
   // active objects (batched.cu:187-191): more voxels than dust and a bounding box of 2+ voxels
   std::vector<uint8_t> active(count + 1, 0);
   std::vector<float> dbf_max(count + 1, 0.0f);
@@ -791,23 +879,27 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
     if (double(dbf_max[id]) > P.soma_detection) throw std::invalid_argument("soma objects are not covered by the oracle");
     active[id] = 1;
   }
+  // roots and DAF per object: every object's floods touch only its own voxels
   const Weights W = geometric_weights(P.anisotropy);
   std::vector<float> daf(n, kInf);
-  std::vector<ObjectPlan> plans;
   std::vector<int64_t> roots(count + 1, -1), targets(count + 1, -1);
   std::vector<float> max_daf(count + 1, 0.0f);
-  for (size_t id = 1; id <= count; ++id) {
-    if (!active[id]) continue;
-    i64 root;
-    if (!borders[id].empty()) { const auto &p = borders[id].back(); root = s.idx(p[0], p[1], p[2]); }
-    else {
-      geometric_flood(ids, s, uint32_t(id), R.cc.roots[id - 1], W, daf, voxels[id]);
-      float m; root = argmax(daf, voxels[id], m);
+  parallel_for(i64(count), threads, 1, [&](i64 b, i64 e) {
+    for (i64 j = b; j < e; ++j) {
+      const size_t id = size_t(j) + 1;
+      if (!active[id]) continue;
+      i64 root;
+      if (!borders[id].empty()) { const auto &p = borders[id].back(); root = s.idx(p[0], p[1], p[2]); }
+      else {
+        geometric_flood(ids, s, uint32_t(id), R.cc.roots[id - 1], W, daf, voxels[id]);
+        float m; root = argmax(daf, voxels[id], m);
+      }
+      geometric_flood(ids, s, uint32_t(id), root, W, daf, voxels[id]);
+      float m; const i64 target = argmax(daf, voxels[id], m);
+      roots[id] = root; targets[id] = target; max_daf[id] = m;
     }
-    geometric_flood(ids, s, uint32_t(id), root, W, daf, voxels[id]);
-    float m; const i64 target = argmax(daf, voxels[id], m);
-    roots[id] = root; targets[id] = target; max_daf[id] = m;
-  }
+  });
+  R.stage_ms[4] = lap.next();
   // PDRF (batched.cu:234-245, batched_regular.inc:93-108): power-of-two exponents only
   const double exponent = P.pdrf_exponent;
   if (!(exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))))
@@ -824,18 +916,21 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
         if (max_daf[id] != 0) { inv[id] = float(1.0 / double(max_daf[id])); use[id] = 2; } else use[id] = 1;
       }
     const float scale = float(P.pdrf_scale);
-    for (i64 i = 0; i < n; ++i) {
-      const uint32_t L = ids[i];
-      if (L == 0 || use[L] == 0) continue;
-      float d = V.dbf[i];
-      if (d == 0.0f) d = kInf;
-      float p = 1.0f - d * M[L];
-      for (int k = 0; k < squarings; ++k) p = p * p;
-      p = p * scale;
-      if (use[L] == 2) { float dd = daf[i]; if (std::isinf(dd)) dd = 0.0f; p = p + dd * inv[L]; }
-      V.pdrf[i] = p;
-    }
+    parallel_for(n, threads, 1 << 16, [&](i64 b, i64 e) {
+      for (i64 i = b; i < e; ++i) {
+        const uint32_t L = ids[i];
+        if (L == 0 || use[L] == 0) continue;
+        float d = V.dbf[i];
+        if (d == 0.0f) d = kInf;
+        float p = 1.0f - d * M[L];
+        for (int k = 0; k < squarings; ++k) p = p * p;
+        p = p * scale;
+        if (use[L] == 2) { float dd = daf[i]; if (std::isinf(dd)) dd = 0.0f; p = p + dd * inv[L]; }
+        V.pdrf[i] = p;
+      }
+    });
   }
+  R.stage_ms[5] = lap.next();
   if (keep_stages) { R.dbf = V.dbf; R.daf = daf; R.pdrf = V.pdrf; }
   // extra targets by the component they fall on (skeletonize.cu:16-25, 61-65): a negative
   // coordinate counts from the end of its axis; a point outside the volume is an error
@@ -851,19 +946,12 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
       (list ? after_of : before_of)[ids[flat]].push_back(flat);
     }
   // target orders and manual targets (lockstep.cu:120-142, lockstep_order.cu:21-45)
-  R.order_offsets.assign(count + 2, 0);
+  auto &plans = st->plans;
   for (size_t id = 1; id <= count; ++id) {
     if (!active[id]) continue;
     ObjectPlan plan;
     plan.id = uint32_t(id); plan.root = roots[id]; plan.target = targets[id];
-    plan.voxels = voxels[id];
-    plan.order = voxels[id];
-    std::sort(plan.order.begin(), plan.order.end(), [&](i64 a, i64 b) {
-      float x = daf[a], y = daf[b];
-      if (std::isinf(x)) x = 0;
-      if (std::isinf(y)) y = 0;
-      return x == y ? a > b : x > y;
-    });
+    plan.voxels = std::move(voxels[id]);
     std::vector<i64> manual;
     for (const auto &p : borders[id]) manual.push_back(s.idx(p[0], p[1], p[2]));
     if (!manual.empty()) manual.pop_back();
@@ -875,37 +963,68 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
     plan.max_paths = i64(plan.manual.size() + plan.after.size()) >= budget ? 0 : budget;
     plans.push_back(std::move(plan));
   }
+  parallel_for(i64(plans.size()), threads, 1, [&](i64 b, i64 e) {
+    for (i64 j = b; j < e; ++j) {
+      ObjectPlan &plan = plans[j];
+      plan.order = plan.voxels;
+      std::sort(plan.order.begin(), plan.order.end(), [&](i64 a, i64 c) {
+        float x = daf[a], y = daf[c];
+        if (std::isinf(x)) x = 0;
+        if (std::isinf(y)) y = 0;
+        return x == y ? a > c : x > y;
+      });
+    }
+  });
+  R.stage_ms[6] = lap.next();
   V.dist.assign(n, kInf);
   V.alive.assign(n, 0);
   for (i64 i = 0; i < n; ++i) V.alive[i] = ids[i] ? active[ids[i]] : 0;
   V.inq.assign(n, 0);
   V.key.assign(n, kUnclaimed);
-  std::vector<std::vector<std::vector<i64>>> traced(plans.size());
-  {
-    std::atomic<size_t> next{0};
-    std::mutex failure;
-    std::string message;
-    // largest objects first, so that a pool of threads finishes together
-    std::vector<size_t> schedule(plans.size());
-    std::iota(schedule.begin(), schedule.end(), size_t(0));
-    std::stable_sort(schedule.begin(), schedule.end(), [&](size_t a, size_t b) { return plans[a].voxels.size() > plans[b].voxels.size(); });
-    auto worker = [&] {
-      for (;;) {
-        const size_t j = next.fetch_add(1);
-        if (j >= schedule.size()) return;
-        const size_t i = schedule[j];
-        try { traced[i] = trace_object(V, plans[i], P); }
-        catch (const std::exception &e) { std::lock_guard<std::mutex> lock(failure); message = e.what(); }
-      }
-    };
-    const int workers = std::max(1, std::min<int>(threads, int(plans.size())));
-    std::vector<std::thread> pool;
-    for (int t = 1; t < workers; ++t) pool.emplace_back(worker);
-    worker();
-    for (auto &t : pool) t.join();
-    if (!message.empty()) throw std::runtime_error(message);
-  }
-  // assembly: one skeleton per original label, components merged in id order (skeletonize.cu:130-181)
+  st->traced.assign(plans.size(), {});
+  // largest objects first, so that a pool of threads finishes together
+  st->schedule.resize(plans.size());
+  std::iota(st->schedule.begin(), st->schedule.end(), size_t(0));
+  std::stable_sort(st->schedule.begin(), st->schedule.end(),
+                   [&](size_t a, size_t b) { return plans[a].voxels.size() > plans[b].voxels.size(); });
+  R.roots = roots; R.targets = targets; R.borders = std::move(borders);
+}
+
+// Traces the objects schedule[begin, end) on `threads` threads (objects never touch each other's
+// voxels, so they run concurrently).
+void trace(Result &R, size_t begin, size_t end, int threads) {
+  Staged &st = *R.staged;
+  end = std::min(end, st.schedule.size());
+  if (begin >= end) return;
+  Lap lap;
+  std::atomic<size_t> next{begin};
+  std::mutex failure;
+  std::string message;
+  auto worker = [&] {
+    for (;;) {
+      const size_t j = next.fetch_add(1);
+      if (j >= end) return;
+      const size_t i = st.schedule[j];
+      try { st.traced[i] = trace_object(st.V, st.plans[i], st.P); }
+      catch (const std::exception &e) { std::lock_guard<std::mutex> lock(failure); message = e.what(); }
+    }
+  };
+  const int workers = std::max(1, std::min<int>(threads, int(end - begin)));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < workers; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+  R.stage_ms[7] += lap.next();
+  if (!message.empty()) throw std::runtime_error(message);
+}
+
+// Assembly: one skeleton per original label, components merged in id order (skeletonize.cu:130-181).
+void finish(Result &R) {
+  Staged &st = *R.staged;
+  Lap lap;
+  const Shape &s = st.s;
+  const auto &plans = st.plans;
+  const auto &traced = st.traced;
   std::vector<int64_t> label_order;
   std::vector<std::vector<std::vector<i64>>> merged;
   for (size_t j = 0; j < plans.size(); ++j) {
@@ -920,17 +1039,18 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
     Skeleton sk = assemble(merged[j], s);
     R.labels.push_back(label_order[j]);
     for (const auto &v : sk.vox) {
-      for (int a = 0; a < 3; ++a) R.vertices.push_back(float(v[a]) * P.anisotropy[a]);
-      R.radii.push_back(V.dbf[s.idx(v[0], v[1], v[2])]);
+      for (int a = 0; a < 3; ++a) R.vertices.push_back(float(v[a]) * st.P.anisotropy[a]);
+      R.radii.push_back(st.V.dbf[s.idx(v[0], v[1], v[2])]);
     }
     for (const auto &e : sk.edges) { R.edges.push_back(e[0]); R.edges.push_back(e[1]); }
     R.vertex_offsets.push_back(int64_t(R.radii.size()));
     R.edge_offsets.push_back(int64_t(R.edges.size() / 2));
   }
-  if (keep_stages) {
-    R.roots = roots; R.targets = targets; R.borders = borders;
+  if (st.keep_stages) {
+    const size_t count = R.cc.roots.size();
     R.boxes.clear();
-    for (size_t id = 0; id <= count; ++id) for (int a = 0; a < 7; ++a) R.boxes.push_back(box[id][a]);
+    for (size_t id = 0; id < st.box.size(); ++id) for (int a = 0; a < 7; ++a) R.boxes.push_back(st.box[id][a]);
+    R.order_offsets.assign(count + 2, 0);
     for (size_t id = 1; id <= count; ++id) {
       R.order_offsets[id + 1] = R.order_offsets[id];
       auto it = std::find_if(plans.begin(), plans.end(), [&](const ObjectPlan &p) { return p.id == id; });
@@ -944,8 +1064,11 @@ Result run(const void *labels, int dtype, const Shape &s, const Params &P, int t
         R.path_offsets.push_back(i64(R.paths_flat.size()));
         R.path_labels.push_back(plans[j].id);
       }
+  } else {
+    R.roots.clear(); R.targets.clear(); R.borders.clear();
   }
-  return R;
+  R.stage_ms[8] = lap.next();
+  R.staged.reset();
 }
 
 }  // namespace
@@ -965,10 +1088,8 @@ struct oracle_params {
   const int64_t *targets_after; int64_t n_after;
 };
 
-void *oracle_run(const void *labels, int dtype, int64_t sx, int64_t sy, int64_t sz, const oracle_params *p,
-                 int threads, int keep_stages) {
-  auto *r = new Result();
-  try {
+namespace {
+Params params_of(const oracle_params *p) {
     Params P{};
     P.scale = p->scale; P.constant = p->constant; P.pdrf_scale = p->pdrf_scale; P.pdrf_exponent = p->pdrf_exponent;
     P.soma_detection = p->soma_detection; P.soma_acceptance = p->soma_acceptance;
@@ -981,11 +1102,63 @@ void *oracle_run(const void *labels, int dtype, int64_t sx, int64_t sy, int64_t 
     for (int64_t i = 0; i < p->n_after; ++i)
       P.after.push_back({p->targets_after[3 * i], p->targets_after[3 * i + 1], p->targets_after[3 * i + 2]});
     if (!P.fix_branching) throw std::invalid_argument("the oracle covers fix_branching=True");
-    *r = run(labels, dtype, Shape{sx, sy, sz}, P, threads, keep_stages);
+    return P;
+}
+}  // namespace
+
+// The whole path in one call.
+void *oracle_run(const void *labels, int dtype, int64_t sx, int64_t sy, int64_t sz, const oracle_params *p,
+                 int threads, int keep_stages) {
+  auto *r = new Result();
+  try {
+    prepare(*r, labels, dtype, Shape{sx, sy, sz}, params_of(p), threads, keep_stages);
+    trace(*r, 0, r->staged->schedule.size(), threads);
+    finish(*r);
   } catch (const std::exception &e) {
     r->error = e.what();
+    r->staged.reset();
   }
   return r;
+}
+
+// The same path in steps: oracle_prepare, then oracle_trace over sub-ranges of the largest-first
+// object order (oracle_objects of them), then oracle_finish. Errors go to oracle_error.
+void *oracle_prepare(const void *labels, int dtype, int64_t sx, int64_t sy, int64_t sz, const oracle_params *p,
+                     int threads) {
+  auto *r = new Result();
+  try {
+    prepare(*r, labels, dtype, Shape{sx, sy, sz}, params_of(p), threads, 0);
+  } catch (const std::exception &e) {
+    r->error = e.what();
+    r->staged.reset();
+  }
+  return r;
+}
+int64_t oracle_objects(void *h) {
+  auto *r = static_cast<Result *>(h);
+  return r->staged ? int64_t(r->staged->schedule.size()) : 0;
+}
+int oracle_trace(void *h, int64_t begin, int64_t end, int threads) {
+  auto *r = static_cast<Result *>(h);
+  if (!r->staged) return 1;
+  try {
+    trace(*r, size_t(std::max<int64_t>(begin, 0)), size_t(std::max<int64_t>(end, 0)), threads);
+    return 0;
+  } catch (const std::exception &e) {
+    r->error = e.what();
+    return 1;
+  }
+}
+int oracle_finish(void *h) {
+  auto *r = static_cast<Result *>(h);
+  if (!r->staged) return 1;
+  try {
+    finish(*r);
+    return 0;
+  } catch (const std::exception &e) {
+    r->error = e.what();
+    return 1;
+  }
 }
 void oracle_free(void *h) { delete static_cast<Result *>(h); }
 const char *oracle_error(void *h) { return static_cast<Result *>(h)->error.c_str(); }
@@ -1015,6 +1188,7 @@ const void *oracle_array(void *h, const char *name, int64_t *count) {
   if (k == "paths") return give(r->paths_flat);
   if (k == "path_offsets") return give(r->path_offsets);
   if (k == "path_labels") return give(r->path_labels);
+  if (k == "stage_ms") return give(r->stage_ms);
   *count = -1;
   return nullptr;
 }

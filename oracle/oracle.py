@@ -59,6 +59,15 @@ def lib():
                                          ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]
         _lib.oracle_target_order.restype = ctypes.c_int64
         _lib.oracle_target_order.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+        _lib.oracle_prepare.restype = ctypes.c_void_p
+        _lib.oracle_prepare.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                        ctypes.POINTER(_Params), ctypes.c_int]
+        _lib.oracle_objects.restype = ctypes.c_int64
+        _lib.oracle_objects.argtypes = [ctypes.c_void_p]
+        _lib.oracle_trace.restype = ctypes.c_int
+        _lib.oracle_trace.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
+        _lib.oracle_finish.restype = ctypes.c_int
+        _lib.oracle_finish.argtypes = [ctypes.c_void_p]
     return _lib
 
 
@@ -71,7 +80,10 @@ _ARRAY_TYPES = {"labels": np.int64, "vertex_offsets": np.int64, "edge_offsets": 
                 "radii": np.float32, "edges": np.uint32, "cc": np.uint32, "mapping": np.int64, "cc_roots": np.int64,
                 "dbf": np.float32, "daf": np.float32, "pdrf": np.float32, "roots": np.int64, "targets": np.int64,
                 "boxes": np.int64, "orders": np.int64, "order_offsets": np.int64, "paths": np.int64,
-                "path_offsets": np.int64, "path_labels": np.int64}
+                "path_offsets": np.int64, "path_labels": np.int64, "stage_ms": np.float64}
+
+# names of the entries of OracleResult.array("stage_ms"): wall-clock ms of each step
+STAGES = ("components", "boxes", "edt", "borders", "daf", "pdrf", "orders", "trace", "assembly")
 
 
 class OracleResult:
@@ -82,9 +94,13 @@ class OracleResult:
         self.shape = shape
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().oracle_free(self._h)
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.oracle_free(self._h)
             self._h = None
+
+    def stage_ms(self):
+        """{step: wall-clock ms} of the run."""
+        return dict(zip(STAGES, self.array("stage_ms").tolist()))
 
     def array(self, name):
         count = ctypes.c_int64(0)
@@ -172,6 +188,38 @@ def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1
     if error:
         raise RuntimeError(f"oracle: {error}")
     return result
+
+
+class StagedRun:
+    """The oracle's path in steps over one volume: prepare() on construction, trace(begin, end)
+    over sub-ranges of the largest-first object order (`objects` of them), finish() for the
+    packed result. Lets a caller spread one volume's work over several timed steps."""
+
+    def __init__(self, labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), dust_threshold=1000,
+                 fix_branching=True, fix_borders=True, threads=1):
+        labels = np.asfortranarray(np.asarray(labels))
+        self.shape = labels.shape
+        self._labels = labels
+        self.params = _params(teasar_params or {}, anisotropy, dust_threshold, fix_branching, fix_borders)
+        self.threads = int(threads)
+        self.result = OracleResult(lib().oracle_prepare(labels.ctypes.data, _DTYPES[labels.dtype], *labels.shape,
+                                                        ctypes.byref(self.params), self.threads), labels.shape)
+        self._check()
+        self.objects = int(lib().oracle_objects(self.result._h))
+
+    def _check(self):
+        error = lib().oracle_error(self.result._h).decode()
+        if error:
+            raise RuntimeError(f"oracle: {error}")
+
+    def trace(self, begin, end):
+        if lib().oracle_trace(self.result._h, int(begin), int(end), self.threads):
+            self._check()
+
+    def finish(self):
+        if lib().oracle_finish(self.result._h):
+            self._check()
+        return self.result
 
 
 def edt(labels, anisotropy=(1, 1, 1), black_border=False, dims=3):

@@ -153,3 +153,25 @@ def test_oracle_answers_that_follow_from_teasar_alone():
     p = oracle.skeletonize(dots, anisotropy=(1, 1, 1), dust_threshold=3).packed()
     assert p["labels"].tolist() == [3]  # 2 voxels <= dust 3 < 4
     assert oracle.skeletonize(np.zeros((5, 5, 5), np.uint8), dust_threshold=0).packed()["labels"].size == 0
+
+
+def test_oracle_threads_and_steps_do_not_change_the_result():
+    """The oracle's threaded preamble (slab-wise components, line-parallel EDT, per-object floods
+    and orders) and its stepped form (oracle.StagedRun: the trace split over sub-ranges of the
+    object order) give the single-threaded one-shot result exactly."""
+    from brook_b200 import synthetic
+
+    labels = synthetic.dense_volume((80, 72, 64), seeds=30, seed=11, dtype=np.uint32)
+    opts = dict(teasar_params=dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_exponent=4), anisotropy=(8, 8, 40),
+                dust_threshold=50)
+    one = oracle.skeletonize(labels, threads=1, stages=True, **opts)
+    many = oracle.skeletonize(labels, threads=6, stages=True, **opts)
+    for name in ("cc", "dbf", "daf", "pdrf", "roots", "targets", "orders", "labels", "vertices", "edges", "radii"):
+        np.testing.assert_array_equal(one.array(name), many.array(name), err_msg=name)
+    run = oracle.StagedRun(labels, threads=3, **opts)
+    assert run.objects > 10
+    for b in range(0, run.objects, 7):
+        run.trace(b, b + 7)
+    stepped = run.finish().packed()
+    for name, value in one.packed().items():
+        np.testing.assert_array_equal(stepped[name], value, err_msg=name)
