@@ -337,7 +337,8 @@ __device__ void prepare_loop(const EngineArgs &a, bool big) {
       float dv = a.dbf[v];
       if (dv == 0.0f) dv = inf();
       float p = __fsub_rn(1.0f, __fmul_rn(dv, M));
-      for (int s = 0; s < a.squarings; ++s) p = __fmul_rn(p, p);
+      if (a.squarings >= 0) for (int s = 0; s < a.squarings; ++s) p = __fmul_rn(p, p);
+      else p = powf(p, a.exponent);  // the reference's powf (trace_primitives.cu:119-129)
       p = __fmul_rn(p, a.pdrf_scale);
       if (with_daf) {
         float dd = __ldcg(a.daf + v);
@@ -348,7 +349,7 @@ __device__ void prepare_loop(const EngineArgs &a, bool big) {
     }
     G::sync();
     if (G::first()) {
-      a.pdrf[root] = 0.0f;  // the root is the first rail
+      if (a.fix_branching) a.pdrf[root] = 0.0f;  // the root is the first rail
       a.root[o] = root;
       a.target[o] = target;
       a.max_daf[o] = farthest;
@@ -377,6 +378,7 @@ template <int C>
 __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *L, int t, int *A, int *B, int *FA,
                                        int *FB, int *touched, unsigned long long *wide) {
   using G = Group<C>;
+  const bool rails = a.fix_branching != 0;  // without rails: a full SSSP from t (the parents' field)
   if (threadIdx.x == 0) {
     sh.rb = BK_UNCLAIMED;
     sh.minfar = kMinFarNone;
@@ -388,7 +390,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
     L->n_far = 0; L->n_keep = 0;
     a.dist[t] = 0.0f;
     const float ft = __ldcg(a.pdrf + t);
-    if (ft == 0.0f) sh.rb = static_cast<unsigned long long>(unsigned(t));
+    if (rails && ft == 0.0f) sh.rb = static_cast<unsigned long long>(unsigned(t));
     else {
       A[0] = t;
       L->cnt[0] = 1;
@@ -428,14 +430,14 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
         const float du = __ldcg(a.dist + u);
         const unsigned long long rb = vload(&sh.rb);
         const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
-        const bool expand = fu != 0.0f && du <= Tb;
+        const bool expand = (fu != 0.0f || !rails) && du <= Tb;
         return expand ? (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u] : 0ull;
       };
       // step B, after the improvement of v to cand (from old)
       auto improved = [&](int v, float cand, float fv, float old) {
         {
           if (old == inf()) touched[atomicAdd(&L->n_touch, 1)] = v;
-          if (fv == 0.0f) atomicMin(&sh.rb, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | unsigned(v));
+          if (rails && fv == 0.0f) atomicMin(&sh.rb, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | unsigned(v));
           const unsigned long long rb = vload(&sh.rb);
           const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
           if (cand <= Tb) {
@@ -579,6 +581,35 @@ __device__ int backtrace(const EngineArgs &a, const Shared &sh, unsigned long lo
     const int x = out[i];
     out[i] = out[len - 1 - i];
     out[len - 1 - i] = x;
+  }
+  __syncwarp();
+  return len;
+}
+
+// Without fix_branching: one warp walks from target t to the root through the parents' field (the
+// object's SSSP distances from the root): each step goes to the neighbour of least distance,
+// lowest neighbour index among ties (vw_assign_parents, sssp_kernels.cuh:89-110). Writes the path
+// target-first to out and returns its length (-1: no room). The walk stops at the first voxel of
+// an earlier path (kOnPath): the parents' field is a tree, so from there it would repeat that
+// path's tail, whose vertices and edges the skeleton already holds and whose voxels are already
+// dead (no invalidation source); the stored paths then total at most the object's voxels plus
+// one per path.
+__device__ int parent_walk(const EngineArgs &a, const Shared &sh, int t, int root, int *out, long long room) {
+  const int lane = threadIdx.x & 31;
+  int cur = t;
+  int len = 0;
+  const long long bound = 2LL * sh.count + 2;
+  for (long long step = 0; step < bound; ++step) {
+    if (len >= room) return -1;
+    if (lane == 0) out[len] = cur;
+    ++len;
+    if (cur == root || (__ldcg(a.flags + cur) & kOnPath) || !(__ldcg(a.dist + cur) < inf())) break;
+    const uint32_t m = a.mask[cur];
+    unsigned db = BK_INF_BITS;
+    if (lane < 26 && ((m >> lane) & 1u)) db = __float_as_uint(__ldcg(a.dist + cur + sh.off[lane]));
+    const unsigned mb = __reduce_min_sync(kFull, db);
+    if (!(mb < BK_INF_BITS)) break;
+    cur += sh.off[__reduce_min_sync(kFull, db == mb ? unsigned(lane) : 64u)];
   }
   __syncwarp();
   return len;
@@ -876,7 +907,20 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
     auto lap = [&](int phase) {
       if (G::first()) { const unsigned long long t = now_ns(); s_prof[2 + phase] += t - s_prof[1]; s_prof[1] = t; }
     };
-    while (paths < maxp) {
+    const bool rails = a.fix_branching != 0;
+    const int root = a.root[o];
+    if (!rails && maxp > 0) {
+      // the parents' field: the object's SSSP from the root, kept until the object is done (its
+      // queue flags are cleared now, its distances at the end)
+      railroad<C>(a, sh, L, root, L0, L1, L2, L3, L4, wide);
+      if (vload(&L->status) != kOk) status = vload(&L->status);
+      const int nt = vload(&L->n_touch);
+      for (int i = G::tid(); i < nt; i += G::threads()) atomicAnd(a.flags + __ldcg(L4 + i), ~(kNearQueued | kFarQueued));
+      if (G::first()) { s_work[0] += nt; s_work[1] += nt; }
+      G::sync();
+      lap(1);
+    }
+    while (status == kOk && paths < maxp) {
       // the next target: manual targets first, then the first alive voxel of the order, then the
       // targets after (trace.cu:209-212)
       int t = -1;
@@ -900,41 +944,58 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
         if (t < 0) break;
       }
       lap(0);
-      const unsigned long long rb = railroad<C>(a, sh, L, t, L0, L1, L2, L3, L4, wide);
-      lap(1);
-      if (vload(&L->status) != kOk) { status = vload(&L->status); break; }
-      if (rb == BK_UNCLAIMED) { status = kNoRail; break; }
-      // walk (one warp of the first CTA), then reset the flood's state over the voxels it touched
-      if (G::rank() == 0 && threadIdx.x < 32) {
-        const int len = backtrace(a, sh, rb, t, store + used, store_cap - used);
-        if (threadIdx.x == 0) L->len = len;
+      if (!rails) {  // the walk to the root through the parents' field
+        if (G::rank() == 0 && threadIdx.x < 32) {
+          const int len = parent_walk(a, sh, t, root, store + used, store_cap - used);
+          if (threadIdx.x == 0) L->len = len;
+        }
+        G::sync();
+        lap(2);
+      } else {
+        const unsigned long long rb = railroad<C>(a, sh, L, t, L0, L1, L2, L3, L4, wide);
+        lap(1);
+        if (vload(&L->status) != kOk) { status = vload(&L->status); break; }
+        if (rb == BK_UNCLAIMED) { status = kNoRail; break; }
+        // walk (one warp of the first CTA), then reset the flood's state over the voxels it touched
+        if (G::rank() == 0 && threadIdx.x < 32) {
+          const int len = backtrace(a, sh, rb, t, store + used, store_cap - used);
+          if (threadIdx.x == 0) L->len = len;
+        }
+        G::sync();
+        const int nt = vload(&L->n_touch);
+        const float D = __uint_as_float(unsigned(rb >> 32));
+        unsigned settled = 0;
+        for (int i = G::tid(); i < nt; i += G::threads()) {
+          const int v = __ldcg(L4 + i);
+          settled += __ldcg(a.dist + v) <= D;
+          a.dist[v] = inf();
+          atomicAnd(a.flags + v, ~(kNearQueued | kFarQueued));
+        }
+        settled = __reduce_add_sync(kFull, settled);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&s_work[0], (unsigned long long)settled);
+        if (G::first()) s_work[1] += nt;
+        G::sync();
+        lap(2);
       }
-      G::sync();
       const int len = vload(&L->len);
-      const int nt = vload(&L->n_touch);
-      const float D = __uint_as_float(unsigned(rb >> 32));
-      unsigned settled = 0;
-      for (int i = G::tid(); i < nt; i += G::threads()) {
-        const int v = __ldcg(L4 + i);
-        settled += __ldcg(a.dist + v) <= D;
-        a.dist[v] = inf();
-        atomicAnd(a.flags + v, ~(kNearQueued | kFarQueued));
-      }
-      settled = __reduce_add_sync(kFull, settled);
-      if ((threadIdx.x & 31) == 0) atomicAdd(&s_work[0], (unsigned long long)settled);
-      if (G::first()) s_work[1] += nt;
-      G::sync();
-      lap(2);
       if (len < 0) { status = kStoreFull; break; }
       if (paths >= rec_cap) { status = kRecordsFull; break; }
       if (!invalidate<C>(a, sh, L, store + used, len, L0, L1, L2, L3, L4, wide, side_u, side_s)) { status = kBudget; break; }
       if (G::first()) { s_work[2] += vload(&L->n_touch); s_work[3] += 1; }
       lap(3);
-      for (int i = G::tid(); i < len; i += G::threads()) a.pdrf[__ldcg(store + used + i)] = 0.0f;
+      if (rails)
+        for (int i = G::tid(); i < len; i += G::threads()) a.pdrf[__ldcg(store + used + i)] = 0.0f;
+      else
+        for (int i = G::tid(); i < len; i += G::threads()) atomicOr(a.flags + __ldcg(store + used + i), kOnPath);
       if (G::first()) { rec_start[paths] = int(used); rec_len[paths] = len; }
       G::sync();
       used += len;
       ++paths;
+    }
+    if (!rails) {  // the parents' field and the path marks go back to rest
+      for (int i = G::tid(); i < sh.count; i += G::threads()) a.dist[a.vox[sh.begin + i]] = inf();
+      for (long long i = G::tid(); i < used; i += G::threads()) atomicAnd(a.flags + __ldcg(store + i), ~kOnPath);
+      G::sync();
     }
     if (G::first()) {
       a.status[o] = status;

@@ -18,6 +18,7 @@ constexpr unsigned kNearQueued = 1u;   // railroad / flood: in the next near lis
 constexpr unsigned kFarQueued = 2u;    // railroad: on the far list
 constexpr unsigned kFront = 4u;        // invalidation: in the next frontier
 constexpr unsigned kWaiting = 8u;      // invalidation: on the waiting list
+constexpr unsigned kOnPath = 16u;      // without fix_branching: on a stored path of the object
 
 enum EngineStatus : int {
   kOk = 0,
@@ -60,7 +61,12 @@ struct EngineArgs {
   const int *border_root;  // per object: flat index, or -1 (search)
   const float *M;          // per object: float(1 / dbf_max^1.01)
   float pdrf_scale;
-  int squarings;
+  int squarings;           // the exponent is 2^squarings; -1: any other exponent (powf)
+  float exponent;
+  // fix_branching: each path runs to the nearest rail (the root, then every earlier path). Without
+  // it, one SSSP from the root over the PDRF is kept for the object's whole trace and each path
+  // walks from its target to the root (trace.cu:151-160, batched_regular.inc:113-152).
+  int fix_branching;
   float w[26];             // geometric step weights
   int *root, *target;
   float *max_daf;

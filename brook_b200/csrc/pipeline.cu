@@ -111,14 +111,16 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     if (std::isfinite(e) && e == std::floor(e) && std::fmod(e, 2.0) == 1.0)
       throw std::invalid_argument("odd pdrf_exponent makes the background penalty negative");
   }
-  if (!opt.fix_branching) throw std::invalid_argument("fix_branching=False is not supported by this build");
   if (opt.targets_before.size() > volumes.size() || opt.targets_after.size() > volumes.size())
     throw std::invalid_argument("extra targets are given for more volumes than the call holds");
+  // a power-of-two exponent is repeated squaring, any other one powf (the reference's lockstep
+  // and per-component arithmetic, batched_regular.inc:93-108 and trace_primitives.cu:119-129)
   const double exponent = t.pdrf_exponent;
-  if (!(exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))))
-    throw std::invalid_argument("pdrf_exponent must be a power of two in this build");
-  int squarings = 0;
-  for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+  int squarings = -1;
+  if (exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))) {
+    squarings = 0;
+    for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+  }
 
   std::vector<Packed> results(volumes.size());
   for (auto &r : results) std::copy(opt.anisotropy.begin(), opt.anisotropy.end(), r.anisotropy.begin());
@@ -374,6 +376,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.schedule = d_schedule.data(); a.queue = queue.data(); a.status = status.data();
   a.lists = lists.data(); a.wide = wide.data(); a.side = side.data(); a.F = F;
   a.border_root = d_border_root.data(); a.M = d_M.data(); a.pdrf_scale = float(t.pdrf_scale); a.squarings = squarings;
+  a.exponent = float(exponent);
+  a.fix_branching = opt.fix_branching ? 1 : 0;
   {
     const double x = aniso[0], y = aniso[1], z = aniso[2];
     const double pairs[3] = {std::sqrt(x * x + y * y), std::sqrt(y * y + z * z), std::sqrt(x * x + z * z)};

@@ -490,6 +490,9 @@ struct Params {
   int fix_branching, fix_borders;
   // extra targets (x, y, z triples): `before` traced first, `after` once no voxel is left
   std::vector<std::array<i64, 3>> before, after;
+  // a PDRF field (float32 per voxel, Fortran order) that replaces the computed one: tests use it
+  // to trace from another implementation's field where the power itself is not bit-reproducible
+  const float *pdrf_field = nullptr;
 };
 
 // Per-object tracing state over the shared volume. Every array is indexed by global flat index;
@@ -579,6 +582,54 @@ std::vector<i64> railroad(Volume &V, uint32_t label, i64 target, std::vector<i64
     std::reverse(walk.begin(), walk.end());
   }
   for (i64 v : touched) V.dist[v] = kInf;
+  return walk;
+}
+
+// fix_branching=False (trace.cu:151-160, trace_primitives.cu:187-211; lockstep batched.cu:246-250,
+// batched_regular.inc:113-152): one vertex-weighted SSSP from the root over the object's PDRF (no
+// rails), kept for the object's whole trace; every path walks from its target to the root through
+// the argmin-distance neighbour (lowest neighbour index among ties). Paths are written
+// target-first, like the railroad's (the assembly does not depend on the order).
+void parental_field(Volume &V, uint32_t label, i64 root, const std::vector<i64> &voxels) {
+  const Shape &s = V.s; const auto &ids = *V.ids;
+  for (i64 v : voxels) V.dist[v] = kInf;
+  using Item = std::pair<float, i64>;
+  std::priority_queue<Item, std::vector<Item>, std::greater<Item>> heap;
+  V.dist[root] = 0.0f; heap.push({0.0f, root});
+  while (!heap.empty()) {
+    auto [d, u] = heap.top(); heap.pop();
+    if (d > V.dist[u]) continue;
+    i64 x, y, z; s.xyz(u, x, y, z);
+    for (int k = 0; k < 26; ++k) {
+      const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+      if (!s.inside(nx, ny, nz)) continue;
+      const i64 v = s.idx(nx, ny, nz);
+      if (ids[v] != label) continue;
+      const float cand = vw_step(d, V.pdrf[v]);
+      if (cand < V.dist[v]) { V.dist[v] = cand; heap.push({cand, v}); }
+    }
+  }
+}
+
+std::vector<i64> parent_walk(const Volume &V, uint32_t label, i64 target, i64 root, i64 limit) {
+  const Shape &s = V.s; const auto &ids = *V.ids;
+  std::vector<i64> walk;
+  i64 cur = target;
+  while (i64(walk.size()) < limit) {
+    walk.push_back(cur);
+    if (cur == root || !(V.dist[cur] < kInf)) break;
+    i64 x, y, z; s.xyz(cur, x, y, z);
+    float best = kInf; i64 next = -1;
+    for (int k = 0; k < 26; ++k) {
+      const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+      if (!s.inside(nx, ny, nz)) continue;
+      const i64 u = s.idx(nx, ny, nz);
+      if (ids[u] != label) continue;
+      if (V.dist[u] < best) { best = V.dist[u]; next = u; }
+    }
+    if (next < 0) break;
+    cur = next;
+  }
   return walk;
 }
 
@@ -714,7 +765,8 @@ std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, co
   std::vector<i64> touched, frontier, next, far, keep, rtouched;
   std::vector<uint64_t> snap;
   if (plan.max_paths <= 0) return paths;
-  V.pdrf[plan.root] = 0.0f;
+  if (P.fix_branching) V.pdrf[plan.root] = 0.0f;  // the root is the first rail
+  else parental_field(V, plan.id, plan.root, plan.voxels);
   size_t cursor = 0, after = 0;
   while (i64(paths.size()) < plan.max_paths) {
     i64 t = -1;
@@ -726,12 +778,16 @@ std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, co
       else if (after < plan.after.size()) t = plan.after[after++];
       else break;
     }
-    std::vector<i64> path = railroad(V, plan.id, t, rtouched);
+    std::vector<i64> path = P.fix_branching ? railroad(V, plan.id, t, rtouched)
+                                            : parent_walk(V, plan.id, t, plan.root, i64(plan.voxels.size()) + 1);
     if (path.empty()) throw std::runtime_error("no rail reachable from a target");
     invalidate(V, plan.id, path, P, touched, frontier, next, far, keep, snap);
-    for (i64 v : path) V.pdrf[v] = 0.0f;
+    if (P.fix_branching)
+      for (i64 v : path) V.pdrf[v] = 0.0f;
     paths.push_back(std::move(path));
   }
+  if (!P.fix_branching)
+    for (i64 v : plan.voxels) V.dist[v] = kInf;
   return paths;
 }
 
@@ -900,12 +956,16 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
     }
   });
   R.stage_ms[4] = lap.next();
-  // PDRF (batched.cu:234-245, batched_regular.inc:93-108): power-of-two exponents only
+  // PDRF (batched.cu:234-245, batched_regular.inc:93-108, trace_primitives.cu:119-129, 213-229):
+  // (1 - dbf * M)^e * scale + daf * inv. A power-of-two e is repeated squaring in float32, as in
+  // the reference; any other e is the reference's powf, restated here as the float64 power
+  // rounded to float32 (within a few ulp of CUDA's powf, not bit for bit).
   const double exponent = P.pdrf_exponent;
-  if (!(exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))))
-    throw std::invalid_argument("the oracle covers power-of-two pdrf_exponent only");
-  int squarings = 0;
-  for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+  int squarings = -1;
+  if (exponent > 0 && exponent < 65536 && exponent == std::floor(exponent) && !(int(exponent) & (int(exponent) - 1))) {
+    squarings = 0;
+    for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+  }
   V.pdrf.assign(n, kInf);
   {
     std::vector<float> M(count + 1, 0.0f), inv(count + 1, 0.0f);
@@ -923,12 +983,17 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
         float d = V.dbf[i];
         if (d == 0.0f) d = kInf;
         float p = 1.0f - d * M[L];
-        for (int k = 0; k < squarings; ++k) p = p * p;
+        if (squarings >= 0) for (int k = 0; k < squarings; ++k) p = p * p;
+        else p = float(std::pow(double(p), exponent));
         p = p * scale;
         if (use[L] == 2) { float dd = daf[i]; if (std::isinf(dd)) dd = 0.0f; p = p + dd * inv[L]; }
         V.pdrf[i] = p;
       }
     });
+  }
+  if (P.pdrf_field) {  // a test's field replaces the computed one over the traced objects' voxels
+    for (i64 i = 0; i < n; ++i)
+      if (ids[i] && active[ids[i]]) V.pdrf[i] = P.pdrf_field[i];
   }
   R.stage_ms[5] = lap.next();
   if (keep_stages) { R.dbf = V.dbf; R.daf = daf; R.pdrf = V.pdrf; }
@@ -1086,6 +1151,7 @@ struct oracle_params {
   int32_t fix_branching, fix_borders;
   const int64_t *targets_before; int64_t n_before;  // x, y, z triples
   const int64_t *targets_after; int64_t n_after;
+  const float *pdrf_field;  // optional (null: computed)
 };
 
 namespace {
@@ -1101,7 +1167,7 @@ Params params_of(const oracle_params *p) {
       P.before.push_back({p->targets_before[3 * i], p->targets_before[3 * i + 1], p->targets_before[3 * i + 2]});
     for (int64_t i = 0; i < p->n_after; ++i)
       P.after.push_back({p->targets_after[3 * i], p->targets_after[3 * i + 1], p->targets_after[3 * i + 2]});
-    if (!P.fix_branching) throw std::invalid_argument("the oracle covers fix_branching=True");
+    P.pdrf_field = p->pdrf_field;
     return P;
 }
 }  // namespace

@@ -25,7 +25,7 @@ class _Params(ctypes.Structure):
                 ("anisotropy", ctypes.c_float * 3), ("dust", ctypes.c_double), ("fix_branching", ctypes.c_int32),
                 ("fix_borders", ctypes.c_int32), ("targets_before", ctypes.POINTER(ctypes.c_int64)),
                 ("n_before", ctypes.c_int64), ("targets_after", ctypes.POINTER(ctypes.c_int64)),
-                ("n_after", ctypes.c_int64)]
+                ("n_after", ctypes.c_int64), ("pdrf_field", ctypes.POINTER(ctypes.c_float))]
 
 
 _lib = None
@@ -163,9 +163,12 @@ DEFAULT_TEASAR_PARAMS = dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_expon
 
 def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), dust_threshold=1000,
                 fix_branching=True, fix_borders=True, threads=1, stages=False, extra_targets_before=(),
-                extra_targets_after=()):
+                extra_targets_after=(), pdrf_field=None):
     """Run the oracle on a 3D label volume (any layout; read as its logical (x, y, z) axes), with
-    the argument defaults of the reference's brook.skeletonize."""
+    the argument defaults of the reference's brook.skeletonize. `pdrf_field` (float32, the
+    volume's shape) replaces the oracle's own PDRF over the traced objects: a test traces from
+    another implementation's field where the power itself is not bit-reproducible (an exponent
+    that is not a power of two)."""
     labels = np.asarray(labels)
     if labels.dtype == bool:
         labels = labels.view(np.uint8)
@@ -181,6 +184,12 @@ def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1
         keep.append(pts)
         setattr(params, name, pts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
         setattr(params, "n_before" if name == "targets_before" else "n_after", pts.shape[0])
+    if pdrf_field is not None:
+        field = np.asfortranarray(np.asarray(pdrf_field, np.float32))
+        if field.shape != labels.shape:
+            raise ValueError("pdrf_field must have the volume's shape")
+        keep.append(field)
+        params.pdrf_field = field.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     handle = lib().oracle_run(labels.ctypes.data, _DTYPES[labels.dtype], *labels.shape, ctypes.byref(params),
                               int(threads), int(bool(stages)))
     result = OracleResult(handle, labels.shape)

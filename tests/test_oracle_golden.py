@@ -128,13 +128,14 @@ def test_edt_within_1e6_of_float64():
         assert rel.max() <= 1e-6, (shape, aniso, bb, rel.max())
 
 
-def test_oracle_answers_that_follow_from_teasar_alone():
-    """Answers that hold for any TEASAR with the reference's object rules: a one-voxel-thick line
-    is its own skeleton; an object whose bounding box is one voxel, or whose voxel count is within
-    the dust threshold, has none (batched.cu:187-191)."""
+@pytest.mark.parametrize("fix_branching", [True, False])
+def test_oracle_answers_that_follow_from_teasar_alone(fix_branching):
+    """Answers that hold for any TEASAR with the reference's object rules, with and without
+    fix_branching: a one-voxel-thick line is its own skeleton; an object whose bounding box is one
+    voxel, or whose voxel count is within the dust threshold, has none (batched.cu:187-191)."""
     line = np.zeros((30, 3, 3), np.uint32)
     line[3:27, 1, 1] = 7
-    p = oracle.skeletonize(line, anisotropy=(4, 5, 6), dust_threshold=0).packed()
+    p = oracle.skeletonize(line, anisotropy=(4, 5, 6), dust_threshold=0, fix_branching=fix_branching).packed()
     assert p["labels"].tolist() == [7]
     verts = p["vertices"].reshape(-1, 3)
     assert len(verts) == 24 and len(p["edges"].reshape(-1, 2)) == 23
@@ -148,11 +149,26 @@ def test_oracle_answers_that_follow_from_teasar_alone():
     dots[2, 2, 2] = 1                 # one voxel: no skeleton
     dots[6, 6, 6] = dots[6, 6, 7] = 2  # two voxels: one edge
     dots[0:4, 8, 8] = 3               # four voxels
-    p = oracle.skeletonize(dots, anisotropy=(1, 1, 1), dust_threshold=0).packed()
+    p = oracle.skeletonize(dots, anisotropy=(1, 1, 1), dust_threshold=0, fix_branching=fix_branching).packed()
     assert p["labels"].tolist() == [2, 3]
-    p = oracle.skeletonize(dots, anisotropy=(1, 1, 1), dust_threshold=3).packed()
+    p = oracle.skeletonize(dots, anisotropy=(1, 1, 1), dust_threshold=3, fix_branching=fix_branching).packed()
     assert p["labels"].tolist() == [3]  # 2 voxels <= dust 3 < 4
     assert oracle.skeletonize(np.zeros((5, 5, 5), np.uint8), dust_threshold=0).packed()["labels"].size == 0
+
+
+def test_branching_off_y_shape_keeps_every_branch_to_the_root():
+    """Without fix_branching every path runs back to the root through one shortest-path tree
+    (trace.cu:151-160): on a one-voxel-thick Y the skeleton is the Y itself, one connected tree."""
+    y = np.zeros((40, 40, 3), np.uint32)
+    for i in range(18):
+        y[20, 2 + i, 1] = 1          # the stem
+        y[20 - i, 20 + i, 1] = 1     # one arm
+        y[20 + i, 20 + i, 1] = 1     # the other
+    p = oracle.skeletonize(y, teasar_params=dict(scale=1, const=1), anisotropy=(1, 1, 1), dust_threshold=0,
+                           fix_branching=False, fix_borders=False).packed()
+    verts = p["vertices"].reshape(-1, 3)
+    assert len(verts) == int((y > 0).sum())
+    assert len(p["edges"].reshape(-1, 2)) == len(verts) - 1  # a tree over every voxel
 
 
 def test_oracle_threads_and_steps_do_not_change_the_result():
