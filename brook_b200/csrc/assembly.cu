@@ -24,22 +24,23 @@ struct KeyLayout {
 
 __global__ void occurrence_keys(const int *store, const float *dbf, const int *src, const int *len, const int *group,
                                 const int *volume, const long long *occ_begin, const long long *arena_offset,
-                                const int *arena_dims, KeyLayout k, unsigned long long *keys, int *index,
-                                float *radius, unsigned char *first) {
+                                const int *arena_dims, const int *arena_origin, KeyLayout k, unsigned long long *keys,
+                                int *index, float *radius, unsigned char *first) {
   const int p = blockIdx.x;
   const int n = len[p], vol = volume[p];
   const long long base = occ_begin[p];
   const int sx = arena_dims[3 * vol], sy = arena_dims[3 * vol + 1];
+  const int ox = arena_origin[3 * vol], oy = arena_origin[3 * vol + 1], oz = arena_origin[3 * vol + 2];
   const unsigned long long g = static_cast<unsigned long long>(group[p]) << k.shift;
   for (int q = threadIdx.x; q < n; q += blockDim.x) {
     const int v = store[src[p] + q];
     long long r = v - arena_offset[vol];
     const int z = int(r / ((long long)sx * sy));
     r -= (long long)z * sx * sy;
-    const int y = int(r / sx), x = int(r - (long long)y * sx);
+    const int y = int(r / sx) + oy, x = int(r - (long long)(y - oy) * sx) + ox;
     const long long o = base + q;
     keys[o] = g | (static_cast<unsigned long long>(x) << (k.by + k.bz)) | (static_cast<unsigned long long>(y) << k.bz) |
-              static_cast<unsigned long long>(z);
+              static_cast<unsigned long long>(z + oz);
     index[o] = int(o);
     radius[o] = dbf[v];
     first[o] = q == 0;
@@ -148,7 +149,7 @@ void exclusive_sum(Context &ctx, const T *in, T *out, long long n) {
 
 AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const AssemblyPaths &paths,
                         const std::vector<long long> &arena_offset, const std::vector<std::array<int, 3>> &arena_dims,
-                        const float anisotropy[3]) {
+                        const std::vector<std::array<int, 3>> &arena_origin, const float anisotropy[3]) {
   cudaStream_t s = ctx.stream();
   auto host_t = std::chrono::steady_clock::now();
   auto host_mark = [&](const char *step) {  // host time of each step: ctx.stats["host_ms_assemble_<step>"]
@@ -167,18 +168,22 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
   if (P >= (1LL << 31)) throw std::invalid_argument("too many path vertices");
   KeyLayout k{};
   int mx = 1, my = 1, mz = 1;
-  for (const auto &d : arena_dims) { mx = std::max(mx, d[0]); my = std::max(my, d[1]); mz = std::max(mz, d[2]); }
+  for (size_t r = 0; r < arena_dims.size(); ++r) {
+    const auto &d = arena_dims[r], &o = arena_origin[r];
+    mx = std::max(mx, d[0] + o[0]); my = std::max(my, d[1] + o[1]); mz = std::max(mz, d[2] + o[2]);
+  }
   k.bx = bits_for(mx); k.by = bits_for(my); k.bz = bits_for(mz);
   k.shift = k.bx + k.by + k.bz;
   const int end_bit = k.shift + bits_for(G);
   if (end_bit > 64) throw std::invalid_argument("skeleton keys exceed 64 bits");
 
-  std::vector<int> dims_flat;
+  std::vector<int> dims_flat, origin_flat;
   for (const auto &d : arena_dims) dims_flat.insert(dims_flat.end(), d.begin(), d.end());
+  for (const auto &o : arena_origin) origin_flat.insert(origin_flat.end(), o.begin(), o.end());
   auto d_src = to_device(ctx, paths.src), d_len = to_device(ctx, paths.len), d_group = to_device(ctx, paths.group);
   auto d_volume = to_device(ctx, paths.volume);
   auto d_occ = to_device(ctx, occ_begin), d_aoff = to_device(ctx, arena_offset);
-  auto d_dims = to_device(ctx, dims_flat);
+  auto d_dims = to_device(ctx, dims_flat), d_origin = to_device(ctx, origin_flat);
 
   host_mark("upload");
   // every occurrence: key, index, radius, first-of-path
@@ -188,8 +193,8 @@ AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const 
   Buffer<unsigned char> first(ctx, P);
   host_mark("allocate");
   occurrence_keys<<<npaths, 128, 0, s>>>(store, dbf, d_src.data(), d_len.data(), d_group.data(), d_volume.data(),
-                                         d_occ.data(), d_aoff.data(), d_dims.data(), k, keys.data(), index.data(),
-                                         radius.data(), first.data()); ++ctx.launches;
+                                         d_occ.data(), d_aoff.data(), d_dims.data(), d_origin.data(), k, keys.data(),
+                                         index.data(), radius.data(), first.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   host_mark("keys");
   size_t temp = 0;

@@ -27,8 +27,10 @@ struct AssemblyResult {
   std::vector<int64_t> vertex_offsets, edge_offsets;  // groups + 1 each
 };
 
+// Arena r starts at arena_offset[r] with shape arena_dims[r]; its voxel (x, y, z) is the output
+// vertex (x, y, z) + arena_origin[r] (a soma's private crop lies at its box corner in its volume).
 AssemblyResult assemble(Context &ctx, const int *store, const float *dbf, const AssemblyPaths &paths,
                         const std::vector<long long> &arena_offset, const std::vector<std::array<int, 3>> &arena_dims,
-                        const float anisotropy[3]);
+                        const std::vector<std::array<int, 3>> &arena_origin, const float anisotropy[3]);
 
 }  // namespace bk

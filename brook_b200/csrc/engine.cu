@@ -208,15 +208,54 @@ __device__ bool next_object(const EngineArgs &a, Shared &sh, Shared *L, bool big
 // Geometric flood from `source` over the object's voxels into `d` (+inf at rest on them):
 // Bellman-Ford rounds, fl(d[u] + w[k]). The fixed point is the least float32 path sum, which any
 // schedule reaches. Returns false when the round bound is hit.
+// The free-space seed of a soma's DAF (sssp_kernels.cuh:14-35): the 26-connected distance from
+// the root through empty space, for voxels within `radius` (float32 physical distance) of it;
+// -1 beyond. One rounding per operation, in the reference's order.
+__device__ float freespace_seed(const EngineArgs &a, int x, int y, int z, int rx, int ry, int rz, float radius) {
+  const float wx = a.wx, wy = a.wy, wz = a.wz;
+  const float rdx = __fmul_rn(wx, float(x - rx)), rdy = __fmul_rn(wy, float(y - ry)), rdz = __fmul_rn(wz, float(z - rz));
+  const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(rdx, rdx), __fmul_rn(rdy, rdy)), __fmul_rn(rdz, rdz));
+  if (r2 > __fmul_rn(radius, radius)) return -1.0f;
+  const float dx = fabsf(float(x - rx)), dy = fabsf(float(y - ry)), dz = fabsf(float(z - rz));
+  const float dxyz = fminf(fminf(dx, dy), dz);
+  const float dxy = fminf(dx, dy), dyz = fminf(dy, dz), dxz = fminf(dx, dz);
+  const float wxx = __fmul_rn(wx, wx), wyy = __fmul_rn(wy, wy), wzz = __fmul_rn(wz, wz);
+  float v = __fmul_rn(dxyz, sqrtf(__fadd_rn(__fadd_rn(wxx, wyy), wzz)));
+  v = __fadd_rn(v, __fmul_rn(wx, __fsub_rn(dx, dxyz)));
+  v = __fadd_rn(v, __fmul_rn(wy, __fsub_rn(dy, dxyz)));
+  v = __fadd_rn(v, __fmul_rn(wz, __fsub_rn(dz, dxyz)));
+  v = __fadd_rn(v, __fmul_rn(__fsub_rn(dxy, dxyz), __fsub_rn(__fsub_rn(sqrtf(__fadd_rn(wxx, wyy)), wx), wy)));
+  v = __fadd_rn(v, __fmul_rn(__fsub_rn(dxz, dxyz), __fsub_rn(__fsub_rn(sqrtf(__fadd_rn(wxx, wzz)), wx), wz)));
+  v = __fadd_rn(v, __fmul_rn(__fsub_rn(dyz, dxyz), __fsub_rn(__fsub_rn(sqrtf(__fadd_rn(wyy, wzz)), wy), wz)));
+  return v;
+}
+
+// seed_radius > 0 (a soma's DAF): every object voxel within it of `source` starts at its
+// free-space seed, and the rounds relax from all of them.
 template <int C>
 __device__ bool flood_geometric(const EngineArgs &a, Shared &sh, Shared *L, float *d, int source, int *A, int *B,
-                                unsigned long long *wide) {
+                                unsigned long long *wide, float seed_radius = 0.0f) {
   using G = Group<C>;
-  if (G::first()) {
+  if (G::first()) { L->cnt[0] = 0; L->cnt[1] = 0; L->cnt[2] = 0; }
+  G::sync();
+  if (seed_radius > 0.0f) {
+    int rx, ry, rz;
+    unravel3(source - sh.a0, sh.sx, sh.sy, rx, ry, rz);
+    for (int i = G::tid(); i < sh.count; i += G::threads()) {
+      const int v = a.vox[sh.begin + i];
+      int x, y, z;
+      unravel3(v - sh.a0, sh.sx, sh.sy, x, y, z);
+      const float s = freespace_seed(a, x, y, z, rx, ry, rz, seed_radius);
+      if (s < 0.0f) continue;
+      d[v] = s;
+      atomicOr(a.flags + v, kNearQueued);
+      A[atomicAdd(&L->cnt[0], 1)] = v;
+    }
+  } else if (G::first()) {
     d[source] = 0.0f;
     atomicOr(a.flags + source, kNearQueued);
     A[0] = source;
-    L->cnt[0] = 1; L->cnt[1] = 0; L->cnt[2] = 0;
+    L->cnt[0] = 1;
   }
   G::sync();
   const long long bound = capped(a, 8LL * sh.count + 256);
@@ -318,7 +357,7 @@ __device__ void prepare_loop(const EngineArgs &a, bool big) {
         G::sync();
       }
     }
-    if (ok) ok = flood_geometric<C>(a, sh, L, a.daf, root, A, B, wide);
+    if (ok) ok = flood_geometric<C>(a, sh, L, a.daf, root, A, B, wide, a.free_radius[o]);
     if (!ok) {
       if (G::first()) a.status[o] = kBudget;
       G::sync();
@@ -615,12 +654,59 @@ __device__ int parent_walk(const EngineArgs &a, const Shared &sh, int t, int roo
   return len;
 }
 
+// Soma trimming of a stored path (trace.cu:222-236), one warp, in place. A vertex is far when its
+// float64 physical distance from the root exceeds the soma radius. With fix_branching (a
+// target-first railroad path) the first vertex stays, then every far vertex, then the root when
+// the rail end is not far. Without it (a target-first walk that stopped at w, the root or a vertex
+// of an earlier trimmed path) the far vertices before w stay, then w: the reference's root-first
+// path [root, far vertices] joins the earlier paths exactly there (its far vertices beyond w are
+// those paths' own). Returns the new length (-1: no room).
+__device__ int soma_trim(const EngineArgs &a, const Shared &sh, int *path, int len, int root, double radius, bool rails,
+                         long long room) {
+  const int lane = threadIdx.x & 31;
+  int rx, ry, rz;
+  unravel3(root - sh.a0, sh.sx, sh.sy, rx, ry, rz);
+  auto far = [&](int v) {
+    int x, y, z;
+    unravel3(v - sh.a0, sh.sx, sh.sy, x, y, z);
+    const double dx = __dmul_rn(double(a.wx), double(x - rx)), dy = __dmul_rn(double(a.wy), double(y - ry)),
+                 dz = __dmul_rn(double(a.wz), double(z - rz));
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz))) > radius;
+  };
+  const int last = path[len - 1];
+  const bool last_far = far(last);
+  // the kept range: [1, len) with the first vertex kept as it is (rails), or [0, len - 1) with the
+  // stop vertex appended (no rails)
+  const int begin = rails ? 1 : 0, end = rails ? len : len - 1;
+  int k = rails ? 1 : 0;
+  for (int base = begin; base < end; base += 32) {
+    const int i = base + lane;
+    const int v = i < end ? path[i] : 0;
+    const bool keep = i < end && far(v);
+    const unsigned ballot = __ballot_sync(kFull, keep);
+    __syncwarp();
+    if (keep) path[k + __popc(ballot & ((1u << lane) - 1u))] = v;
+    k += __popc(ballot);
+    __syncwarp();
+  }
+  if (rails && !last_far) {
+    if (k >= room) return -1;
+    if (lane == 0) path[k] = root;
+    ++k;
+  } else if (!rails) {
+    if (lane == 0) path[k] = last;
+    ++k;
+  }
+  __syncwarp();
+  return k;
+}
+
 __device__ __forceinline__ float distance_to(const EngineArgs &a, int x, int y, int z, int qx, int qy, int qz) {
   const float dx = __fmul_rn(a.wx, float(x - qx)), dy = __fmul_rn(a.wy, float(y - qy)), dz = __fmul_rn(a.wz, float(z - qz));
   return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
 }
-__device__ __forceinline__ float reach(const EngineArgs &a, int s) {
-  return __fadd_rn(__fmul_rn(a.scale, a.dbf[s]), a.constant);
+__device__ __forceinline__ float reach(const EngineArgs &a, int s, float scale, float constant) {
+  return __fadd_rn(__fmul_rn(scale, a.dbf[s]), constant);
 }
 __device__ __forceinline__ int band_of(unsigned mbits, float delta, int kmin) {
   const float m = __uint_as_float(mbits);
@@ -639,8 +725,9 @@ __device__ __forceinline__ int band_of(unsigned mbits, float delta, int kmin) {
 // of its claimed neighbours, the smallest names the next band, those inside it are claimed.
 // Claimed voxels die. Returns false when a loop bound is hit.
 template <int C>
-__device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int *path, int npath, int *A, int *B,
-                           int *FA, int *FB, int *touched, unsigned long long *wide, unsigned long long *side_u,
+__device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int *path, int npath, float rscale,
+                           float rconst, int *A, int *B, int *FA, int *FB, int *touched, unsigned long long *wide,
+                           unsigned long long *side_u,
                            unsigned long long *side_s) {
   using G = Group<C>;
   if (G::first()) { L->cnt[0] = 0; L->cnt[1] = 0; L->cnt[2] = 0; L->n_far = 0; L->n_keep = 0; L->n_touch = 0; }
@@ -709,7 +796,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
           su[q] = u;
           skey[q] = k;
           smask[q] = a.mask[u];
-          sreach[q] = reach(a, int(unsigned(k)));
+          sreach[q] = reach(a, int(unsigned(k)), rscale, rconst);
           int x, y, z;
           unravel3(u - sh.a0, sh.sx, sh.sy, x, y, z);
           spu[q] = pack3(x, y, z);
@@ -749,7 +836,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
           int ux, uy, uz, qx, qy, qz;
           unpack3(__ldcg(side_u + i), ux, uy, uz);
           unpack3(__ldcg(side_s + i), qx, qy, qz);
-          offer(u, ku, k, ux, uy, uz, qx, qy, qz, reach(a, int(unsigned(ku))));
+          offer(u, ku, k, ux, uy, uz, qx, qy, qz, reach(a, int(unsigned(ku)), rscale, rconst));
         }
       }
       G::sync();
@@ -766,7 +853,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
       int qx, qy, qz;
       unravel3(s - sh.a0, sh.sx, sh.sy, qx, qy, qz);
       const float d = distance_to(a, x, y, z, qx, qy, qz);
-      if (d >= reach(a, s)) return ~0ull;
+      if (d >= reach(a, s, rscale, rconst)) return ~0ull;
       unsigned mb = __float_as_uint(d);
       const unsigned mu = unsigned(ku >> 32);
       if (mb < mu) mb = mu;
@@ -909,7 +996,17 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
     };
     const bool rails = a.fix_branching != 0;
     const int root = a.root[o];
-    if (!rails && maxp > 0) {
+    const double soma_radius = a.soma_radius[o];
+    if (soma_radius >= 0.0) {
+      // the soma's ball, from the root with the soma's reach, before any path (trace.cu:199)
+      if (G::first()) store[0] = root;
+      G::sync();
+      if (!invalidate<C>(a, sh, L, store, 1, a.soma_scale, a.soma_constant, L0, L1, L2, L3, L4, wide, side_u, side_s))
+        status = kBudget;
+      if (G::first()) s_work[2] += vload(&L->n_touch);
+      G::sync();
+    }
+    if (!rails && maxp > 0 && status == kOk) {
       // the parents' field: the object's SSSP from the root, kept until the object is done (its
       // queue flags are cleared now, its distances at the end)
       railroad<C>(a, sh, L, root, L0, L1, L2, L3, L4, wide);
@@ -977,10 +1074,21 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
         G::sync();
         lap(2);
       }
-      const int len = vload(&L->len);
+      int len = vload(&L->len);
+      if (soma_radius >= 0.0 && len > 0) {
+        if (G::rank() == 0 && threadIdx.x < 32) {
+          const int n = soma_trim(a, sh, store + used, len, root, soma_radius, rails, store_cap - used);
+          if (threadIdx.x == 0) L->len = n;
+        }
+        G::sync();
+        len = vload(&L->len);
+      }
       if (len < 0) { status = kStoreFull; break; }
       if (paths >= rec_cap) { status = kRecordsFull; break; }
-      if (!invalidate<C>(a, sh, L, store + used, len, L0, L1, L2, L3, L4, wide, side_u, side_s)) { status = kBudget; break; }
+      if (!invalidate<C>(a, sh, L, store + used, len, a.scale, a.constant, L0, L1, L2, L3, L4, wide, side_u, side_s)) {
+        status = kBudget;
+        break;
+      }
       if (G::first()) { s_work[2] += vload(&L->n_touch); s_work[3] += 1; }
       lap(3);
       if (rails)

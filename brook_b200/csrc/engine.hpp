@@ -67,6 +67,12 @@ struct EngineArgs {
   // it, one SSSP from the root over the PDRF is kept for the object's whole trace and each path
   // walks from its target to the root (trace.cu:151-160, batched_regular.inc:113-152).
   int fix_branching;
+  // somata (trace.cu:98-131): per object the free-space radius of its DAF seed (the DBF maximum;
+  // 0: none) and the soma radius its paths are trimmed to (< 0: not a soma); the soma's own ball is
+  // invalidated first with soma_scale / soma_constant as the reach
+  const float *free_radius;
+  const double *soma_radius;
+  float soma_scale, soma_constant;
   float w[26];             // geometric step weights
   int *root, *target;
   float *max_daf;

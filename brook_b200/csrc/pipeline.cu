@@ -57,6 +57,79 @@ __global__ void gather_records(const int *rs, const int *rl, const long long *re
   }
 }
 
+// A box of a volume (ids or DBF) into a contiguous crop: out[c] for crop voxel c of the box at
+// (lx, ly, lz) with extents (cx, cy, cz). With `keep`, crop voxels where keep is 0 get 0.
+template <class T>
+__global__ void gather_box(const T *src, int sx, int sy, int lx, int ly, int lz, int cx, int cy, long long n,
+                           const uint32_t *keep, T *out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long z = i / ((long long)cx * cy), r = i - z * cx * cy, y = r / cx, x = r - y * cx;
+  const T value = src[(x + lx) + (long long)sx * ((y + ly) + (long long)sy * (z + lz))];
+  out[i] = keep && !keep[i] ? T(0) : value;
+}
+
+// fill_voids (trace_primitives.cu:238-253, fillvoids_kernels.cuh): background voxels of the crop
+// not 6-connected to its faces become foreground. Returns how many.
+long long fill_voids(std::vector<uint32_t> &mask, int cx, int cy, int cz) {
+  const long long n = (long long)cx * cy * cz;
+  std::vector<uint8_t> seen(n, 0);
+  std::vector<long long> stack;
+  auto at = [&](long long x, long long y, long long z) { return x + cx * (y + (long long)cy * z); };
+  for (long long z = 0; z < cz; ++z)
+    for (long long y = 0; y < cy; ++y)
+      for (long long x = 0; x < cx; ++x) {
+        const long long v = at(x, y, z);
+        if (mask[v] || !(x == 0 || y == 0 || z == 0 || x == cx - 1 || y == cy - 1 || z == cz - 1)) continue;
+        seen[v] = 1;
+        stack.push_back(v);
+      }
+  const int step[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+  while (!stack.empty()) {
+    const long long u = stack.back();
+    stack.pop_back();
+    const long long z = u / ((long long)cx * cy), r = u - z * cx * cy, y = r / cx, x = r - y * cx;
+    for (const auto &d : step) {
+      const long long nx = x + d[0], ny = y + d[1], nz = z + d[2];
+      if (nx < 0 || ny < 0 || nz < 0 || nx >= cx || ny >= cy || nz >= cz) continue;
+      const long long v = at(nx, ny, nz);
+      if (mask[v] || seen[v]) continue;
+      seen[v] = 1;
+      stack.push_back(v);
+    }
+  }
+  long long filled = 0;
+  for (long long v = 0; v < n; ++v)
+    if (!mask[v] && !seen[v]) { mask[v] = 1; ++filled; }
+  return filled;
+}
+
+// The soma root (trace.cu:55-73, batched.cu:58-105): among the crop voxels at the DBF maximum,
+// sorted by (x, y, z), the first nearest (float64 squared distance, voxel units) to their float32
+// centroid. Returns the crop flat index.
+long long soma_root(const std::vector<float> &dbf, const std::vector<uint32_t> &mask, float maximum, int cx, int cy) {
+  std::vector<std::array<long long, 3>> points;
+  std::array<long long, 3> sum{0, 0, 0};
+  for (long long v = 0; v < (long long)dbf.size(); ++v)
+    if (mask[v] && dbf[v] == maximum) {
+      const long long z = v / ((long long)cx * cy), r = v - z * cx * cy, y = r / cx, x = r - y * cx;
+      points.push_back({x, y, z});
+      sum[0] += x; sum[1] += y; sum[2] += z;
+    }
+  if (points.empty()) throw std::runtime_error("no soma maximum");
+  std::sort(points.begin(), points.end());
+  float centre[3];
+  for (int k = 0; k < 3; ++k) centre[k] = float(double(sum[k]) / double(points.size()));
+  double best = INFINITY;
+  std::array<long long, 3> root = points.front();
+  for (const auto &p : points) {
+    double cost = 0;
+    for (int k = 0; k < 3; ++k) { const double d = double(p[k]) - double(centre[k]); cost += d * d; }
+    if (cost < best) { best = cost; root = p; }
+  }
+  return root[0] + cx * (root[1] + (long long)cy * root[2]);
+}
+
 template <class L>
 Buffer<unsigned char> filtered(Context &ctx, const DeviceVolume &v, const std::vector<int64_t> &ids) {
   std::vector<long long> sorted(ids.begin(), ids.end());
@@ -209,13 +282,31 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     for (size_t j = 0; j < which.size(); ++j) vs[which[j]].borders = std::move(picks[j]);
     clock.mark("borders");
   }
-  // ---- objects: more voxels than dust and a bounding box of two or more voxels (batched.cu:187-191)
+  // ---- objects: more voxels than dust and a bounding box of two or more voxels (batched.cu:187-191).
+  // An object whose DBF maximum passes soma_detection_threshold is a soma candidate: it is prepared
+  // and traced in a private arena, the crop of its box appended to the flat index space
+  // (prepare_component and soma.cu:141-237): its voids filled, the DBF recomputed on the crop when
+  // anything was filled (black border when the fill covers the crop), else the input's; a soma
+  // when the crop's maximum passes soma_acceptance_threshold.
   struct Object {
+    int volume;     // the input volume the object belongs to
+    uint32_t id;
+    int64_t count;  // voxels it is traced with (a candidate's: its filled crop)
+    int arena;      // the engine arena it is traced in (its volume, or its private crop)
+    int soma;       // index into `somas`, or -1
+  };
+  struct SomaArena {
     int volume;
     uint32_t id;
-    int64_t count;
+    std::array<int, 3> lo, dims;
+    long long offset = 0, valid = 0, filled = 0;
+    std::vector<uint32_t> mask;  // the filled crop, 1 / 0
+    float maximum = 0;
+    bool soma = false;
+    long long root = -1;         // crop flat index of the soma root
   };
   std::vector<Object> objects;
+  std::vector<SomaArena> somas;
   for (size_t v = 0; v < vs.size(); ++v) {
     auto &st = vs[v];
     if (st.empty) continue;
@@ -223,21 +314,93 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       const Box &b = st.boxes[id];
       const long long bbox = (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
       if (!b.count || double(b.count) <= opt.dust || bbox <= 1) continue;
-      if (double(st.dbf_max[id]) > t.soma_detection)
-        throw std::invalid_argument("objects with a soma (DBF maximum above soma_detection_threshold) are not supported by this build");
       st.object_of[id] = int(objects.size());
-      objects.push_back({int(v), uint32_t(id), b.count});
+      int soma = -1;
+      if (double(st.dbf_max[id]) > t.soma_detection) {
+        soma = int(somas.size());
+        SomaArena sa;
+        sa.volume = int(v);
+        sa.id = uint32_t(id);
+        for (int a = 0; a < 3; ++a) { sa.lo[a] = b.lo[a]; sa.dims[a] = b.hi[a] - b.lo[a] + 1; }
+        somas.push_back(std::move(sa));
+      }
+      objects.push_back({int(v), uint32_t(id), b.count, int(v), soma});
     }
   }
   const int nobj = int(objects.size());
   if (nobj == 0) return results;
+  long long NT = N;  // voxels of the flat index space, private arenas included
+  if (!somas.empty()) {
+    // the candidates' crops: ids gathered on the device, voids filled on the host
+    for (auto &sa : somas) {
+      const auto &st = vs[sa.volume];
+      const long long n = (long long)sa.dims[0] * sa.dims[1] * sa.dims[2];
+      Buffer<uint32_t> crop(ctx, n);
+      gather_box<uint32_t><<<blocks_for(n), 256, 0, s>>>(ids.data() + st.offset, st.d.sx, st.d.sy, sa.lo[0], sa.lo[1],
+                                                         sa.lo[2], sa.dims[0], sa.dims[1], n, nullptr, crop.data());
+      ++ctx.launches;
+      BK_CUDA(cudaGetLastError());
+      sa.mask = crop.download();
+      for (auto &m : sa.mask) m = m == sa.id ? 1u : 0u;
+      sa.filled = fill_voids(sa.mask, sa.dims[0], sa.dims[1], sa.dims[2]);
+      sa.valid = st.boxes[sa.id].count + sa.filled;
+      sa.offset = NT;
+      NT += n;
+    }
+    if (NT >= (1LL << 31) - 1) throw std::invalid_argument("the volumes of one call must hold fewer than 2^31 voxels");
+    // ids, masks and DBF over the whole space: the volumes', then every private crop's
+    Buffer<uint32_t> ids2(ctx, NT), mask2(ctx, NT);
+    Buffer<float> dbf2(ctx, NT);
+    BK_CUDA(cudaMemcpyAsync(ids2.data(), ids.data(), N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    BK_CUDA(cudaMemcpyAsync(mask2.data(), mask.data(), N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    BK_CUDA(cudaMemcpyAsync(dbf2.data(), dbf.data(), N * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    for (auto &sa : somas) {
+      const auto &st = vs[sa.volume];
+      const long long n = (long long)sa.mask.size();
+      const VolumeDims cd{sa.dims[0], sa.dims[1], sa.dims[2]};
+      ids2.upload(sa.mask.data(), n, sa.offset);
+      if (sa.filled)
+        edt(ctx, ids2.data() + sa.offset, cd, aniso, sa.valid == n, 3, dbf2.data() + sa.offset);
+      else {
+        gather_box<float><<<blocks_for(n), 256, 0, s>>>(dbf.data() + st.offset, st.d.sx, st.d.sy, sa.lo[0], sa.lo[1],
+                                                        sa.lo[2], sa.dims[0], sa.dims[1], n, ids2.data() + sa.offset,
+                                                        dbf2.data() + sa.offset);
+        ++ctx.launches;
+        BK_CUDA(cudaGetLastError());
+      }
+      neighbour_mask(ctx, ids2.data() + sa.offset, cd, mask2.data() + sa.offset);
+      const auto crop_dbf = dbf2.download(n, sa.offset);
+      for (long long c = 0; c < n; ++c)
+        if (sa.mask[c]) sa.maximum = std::max(sa.maximum, crop_dbf[c]);
+      sa.soma = double(sa.maximum) > t.soma_acceptance;
+      if (sa.soma) sa.root = soma_root(crop_dbf, sa.mask, sa.maximum, sa.dims[0], sa.dims[1]);
+    }
+    ids = std::move(ids2);
+    mask = std::move(mask2);
+    dbf = std::move(dbf2);
+    for (auto &ob : objects)
+      if (ob.soma >= 0) {
+        ob.count = somas[ob.soma].valid;
+        ob.arena = int(vs.size()) + ob.soma;
+      }
+    clock.mark("somata");
+  }
+  // a point of a volume (x, y, z) as the flat index of the arena its object is traced in
+  auto arena_flat = [&](const Object &ob, const Point &p) -> int {
+    if (ob.soma < 0) {
+      const auto &st = vs[ob.volume];
+      return int(st.offset + p[0] + (long long)st.d.sx * (p[1] + (long long)st.d.sy * p[2]));
+    }
+    const auto &sa = somas[ob.soma];
+    return int(sa.offset + (p[0] - sa.lo[0]) + (long long)sa.dims[0] * ((p[1] - sa.lo[1]) + (long long)sa.dims[1] * (p[2] - sa.lo[2])));
+  };
   // extra targets by the component they fall on (skeletonize.cu:16-25, 61-65 of the reference): a
   // negative coordinate counts from the end of its axis; a point outside the volume is an error;
   // points on the background or on objects that are not traced are dropped. Each volume's points
   // are in its own frame.
   std::vector<std::vector<int>> before_of(nobj), after_of(nobj);
   {
-    struct Pick { size_t volume; bool after; long long flat; };
+    struct Pick { size_t volume; bool after; long long flat; Point p; };
     std::vector<Pick> picks;
     for (size_t v = 0; v < volumes.size(); ++v)
       for (int list = 0; list < 2; ++list) {
@@ -251,7 +414,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
             if (p[a] < 0 || p[a] >= shape[a]) throw std::invalid_argument("extra target is outside the input volume");
           }
           if (st.empty) continue;  // a volume at or below the dust threshold traces nothing
-          picks.push_back({v, list == 1, st.offset + p[0] + shape[0] * (p[1] + shape[1] * p[2])});
+          picks.push_back({v, list == 1, st.offset + p[0] + shape[0] * (p[1] + shape[1] * p[2]), p});
         }
       }
     if (!picks.empty()) {
@@ -262,37 +425,51 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       for (size_t i = 0; i < picks.size(); ++i) {
         const int o = at[i] ? vs[picks[i].volume].object_of[at[i]] : -1;
         if (o < 0) continue;
-        (picks[i].after ? after_of : before_of)[o].push_back(int(picks[i].flat));
+        (picks[i].after ? after_of : before_of)[o].push_back(arena_flat(objects[o], picks[i].p));
       }
     }
   }
   std::vector<int> after_begin(nobj), after_count(nobj), after;
   // per object: voxel range, arena, border root, manual targets, path budget, store regions
   std::vector<int> obj_begin(nobj), obj_count(nobj), obj_arena(nobj), border_root(nobj, -1);
-  std::vector<float> M(nobj);
+  std::vector<float> M(nobj), free_radius(nobj, 0.0f);
+  std::vector<double> soma_radius(nobj, -1.0);
   std::vector<int> manual_begin(nobj), manual_count(nobj), manual;
   std::vector<long long> max_paths(nobj), store_begin(nobj), store_cap(nobj), rec_begin(nobj), rec_cap(nobj);
   long long F = 0, store_total = 0, rec_total = 0;
   for (int o = 0; o < nobj; ++o) {
     const auto &ob = objects[o];
     const auto &st = vs[ob.volume];
+    const SomaArena *sa = ob.soma >= 0 ? &somas[ob.soma] : nullptr;
+    const bool soma = sa && sa->soma;
     obj_begin[o] = int(F);
     obj_count[o] = int(ob.count);
     F += ob.count;
-    obj_arena[o] = ob.volume;
-    M[o] = float(1.0 / std::pow(double(st.dbf_max[ob.id]), 1.01));
+    obj_arena[o] = ob.arena;
+    // the maximum of the DBF the object is traced with (a candidate's: its crop's)
+    M[o] = float(1.0 / std::pow(double(sa ? sa->maximum : st.dbf_max[ob.id]), 1.01));
     const auto &b = st.borders[ob.id];
-    auto flat = [&](const Point &p) { return int(st.offset + p[0] + (long long)st.d.sx * (p[1] + (long long)st.d.sy * p[2])); };
-    if (!b.empty()) border_root[o] = flat(b.back());
+    auto flat = [&](const Point &p) { return arena_flat(ob, p); };
+    if (soma) {
+      // the soma root, the DAF seeded through free space within the maximum of it, the paths
+      // trimmed to maximum * soma_invalidation_scale + soma_invalidation_const (trace.cu:114-124)
+      border_root[o] = int(sa->offset + sa->root);
+      free_radius[o] = sa->maximum;
+      soma_radius[o] = double(sa->maximum) * t.soma_scale + t.soma_constant;
+    } else if (!b.empty()) border_root[o] = flat(b.back());
     // manual targets in pop order: the border points except the last (the root), then the extra
     // targets before, all last first (lockstep.cu:127-134); none: the object's own target (-1,
-    // resolved on the device). Extra targets after: last first, once no voxel is alive.
+    // resolved on the device). A soma's border root, if any, comes first in the list (traced last
+    // of them), and a soma has no default target (lockstep.cu:131-135, trace.cu:163).
+    // Extra targets after: last first, once no voxel is alive.
     std::vector<int> listed;
+    if (soma && !b.empty()) listed.push_back(flat(b.back()));
     for (size_t i = 0; i + 1 < b.size(); ++i) listed.push_back(flat(b[i]));
     listed.insert(listed.end(), before_of[o].begin(), before_of[o].end());
     manual_begin[o] = int(manual.size());
-    if (listed.empty()) manual.push_back(-1);
-    else manual.insert(manual.end(), listed.rbegin(), listed.rend());
+    if (listed.empty()) {
+      if (!soma) manual.push_back(-1);
+    } else manual.insert(manual.end(), listed.rbegin(), listed.rend());
     manual_count[o] = int(manual.size()) - manual_begin[o];
     after_begin[o] = int(after.size());
     after.insert(after.end(), after_of[o].rbegin(), after_of[o].rend());
@@ -300,7 +477,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     const int64_t budget = t.max_paths.value_or(ob.count);
     max_paths[o] = manual_count[o] + after_count[o] >= budget ? 0 : budget;
     store_begin[o] = store_total;
-    store_cap[o] = (2 + (long long)after_count[o]) * ob.count + manual_count[o] + 2;
+    // a soma's trimmed paths may end with the root: one more vertex per path
+    store_cap[o] = (2 + (soma ? 1 : 0) + (long long)after_count[o]) * ob.count + manual_count[o] + 2;
     store_total += store_cap[o];
     rec_begin[o] = rec_total;
     rec_cap[o] = ob.count + manual_count[o] + after_count[o] + 1;
@@ -308,13 +486,13 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   }
   if (F >= (1LL << 31)) throw std::invalid_argument("too many foreground voxels");
   // global per-voxel state
-  Buffer<float> pdrf(ctx, N), dist(ctx, N), daf(ctx, N);
-  Buffer<uint32_t> flags(ctx, N);
-  Buffer<uint8_t> alive(ctx, N);
-  Buffer<unsigned long long> key(ctx, N);
-  fill_float(ctx, pdrf.data(), N, INFINITY);
-  fill_float(ctx, dist.data(), N, INFINITY);
-  fill_float(ctx, daf.data(), N, INFINITY);
+  Buffer<float> pdrf(ctx, NT), dist(ctx, NT), daf(ctx, NT);
+  Buffer<uint32_t> flags(ctx, NT);
+  Buffer<uint8_t> alive(ctx, NT);
+  Buffer<unsigned long long> key(ctx, NT);
+  fill_float(ctx, pdrf.data(), NT, INFINITY);
+  fill_float(ctx, dist.data(), NT, INFINITY);
+  fill_float(ctx, daf.data(), NT, INFINITY);
   flags.zero();
   alive.zero();
   key.fill_bytes(0xFF);
@@ -329,14 +507,29 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     if (!any) continue;
     listed.push_back({st.offset, st.offset + st.d.n(), int(object_table.size())});
     object_table.push_back(-1);  // id 0
-    object_table.insert(object_table.end(), st.object_of.begin() + 1, st.object_of.begin() + 1 + st.cc.count);
+    for (int64_t id = 1; id <= st.cc.count; ++id) {  // a soma candidate is traced in its crop
+      const int o = st.object_of[id];
+      object_table.push_back(o >= 0 && objects[o].soma >= 0 ? -1 : o);
+    }
   }
-  Buffer<int> vox = arena_object_voxels(ctx, ids.data(), N, listed, object_table, nobj, F, alive.data());
+  for (size_t j = 0; j < somas.size(); ++j) {  // a crop holds its object as id 1
+    const long long n = (long long)somas[j].mask.size();
+    listed.push_back({somas[j].offset, somas[j].offset + n, int(object_table.size())});
+    object_table.push_back(-1);
+    object_table.push_back(vs[somas[j].volume].object_of[somas[j].id]);
+  }
+  Buffer<int> vox = arena_object_voxels(ctx, ids.data(), NT, listed, object_table, nobj, F, alive.data());
   clock.mark("object_voxels");
-  std::vector<int> arena_offset(vs.size()), arena_dims(3 * vs.size());
+  const size_t arenas = vs.size() + somas.size();
+  std::vector<int> arena_offset(arenas), arena_dims(3 * arenas);
   for (size_t v = 0; v < vs.size(); ++v) {
     arena_offset[v] = int(vs[v].offset);
     arena_dims[3 * v] = vs[v].d.sx; arena_dims[3 * v + 1] = vs[v].d.sy; arena_dims[3 * v + 2] = vs[v].d.sz;
+  }
+  for (size_t j = 0; j < somas.size(); ++j) {
+    const size_t r = vs.size() + j;
+    arena_offset[r] = int(somas[j].offset);
+    for (int k = 0; k < 3; ++k) arena_dims[3 * r + k] = somas[j].dims[k];
   }
   // largest objects first; the leading objects above a size threshold go to clusters
   std::vector<int> schedule(nobj);
@@ -353,7 +546,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   auto d_arena_offset = to_device(ctx, arena_offset), d_arena_dims = to_device(ctx, arena_dims);
   auto d_obj_arena = to_device(ctx, obj_arena), d_obj_begin = to_device(ctx, obj_begin), d_obj_count = to_device(ctx, obj_count);
   auto d_schedule = to_device(ctx, schedule), d_border_root = to_device(ctx, border_root);
-  auto d_M = to_device(ctx, M);
+  auto d_M = to_device(ctx, M), d_free_radius = to_device(ctx, free_radius);
+  auto d_soma_radius = to_device(ctx, soma_radius);
   auto d_manual_begin = to_device(ctx, manual_begin), d_manual_count = to_device(ctx, manual_count);
   auto d_manual = to_device(ctx, manual.empty() ? std::vector<int>{0} : manual);
   auto d_after_begin = to_device(ctx, after_begin), d_after_count = to_device(ctx, after_count);
@@ -378,6 +572,10 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.border_root = d_border_root.data(); a.M = d_M.data(); a.pdrf_scale = float(t.pdrf_scale); a.squarings = squarings;
   a.exponent = float(exponent);
   a.fix_branching = opt.fix_branching ? 1 : 0;
+  a.free_radius = d_free_radius.data();
+  a.soma_radius = d_soma_radius.data();
+  a.soma_scale = float(t.soma_scale);
+  a.soma_constant = float(t.soma_constant);
   {
     const double x = aniso[0], y = aniso[1], z = aniso[2];
     const double pairs[3] = {std::sqrt(x * x + y * y), std::sqrt(y * y + z * z), std::sqrt(x * x + z * z)};
@@ -407,7 +605,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     const auto hd = daf.download(), hp = pdrf.download(), hb = dbf.download();
     for (auto item : {std::make_pair("daf", &hd), std::make_pair("pdrf", &hp), std::make_pair("dbf", &hb)}) {
       FILE *f = std::fopen((std::string(fields) + "." + item.first).c_str(), "wb");
-      if (f) { std::fwrite(item.second->data(), sizeof(float), item.second->size(), f); std::fclose(f); }
+      if (f) { std::fwrite(item.second->data(), sizeof(float), size_t(N), f); std::fclose(f); }  // the volumes' part
     }
   }
   const bool wide_order = std::getenv("BROOK_B200_WIDE_ORDER_KEY") != nullptr;  // test knob: the 96-bit key path
@@ -505,17 +703,18 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
           ap.src.push_back(int(vdst[o] + hstart[rdst[o] + p]));
           ap.len.push_back(len);
           ap.group.push_back(ap.groups);
-          ap.volume.push_back(int(v));
+          ap.volume.push_back(obj_arena[o]);
         }
   }
   group_begin[vs.size()] = ap.groups;
-  std::vector<long long> arena_off(vs.size());
-  std::vector<std::array<int, 3>> arena_dim(vs.size());
-  for (size_t v = 0; v < vs.size(); ++v) {
-    arena_off[v] = vs[v].offset;
-    arena_dim[v] = {vs[v].d.sx, vs[v].d.sy, vs[v].d.sz};
+  std::vector<long long> arena_off(arenas);
+  std::vector<std::array<int, 3>> arena_dim(arenas), arena_origin(arenas, {0, 0, 0});
+  for (size_t r = 0; r < arenas; ++r) {
+    arena_off[r] = arena_offset[r];
+    arena_dim[r] = {arena_dims[3 * r], arena_dims[3 * r + 1], arena_dims[3 * r + 2]};
   }
-  AssemblyResult asmb = assemble(ctx, cstore.data(), dbf.data(), ap, arena_off, arena_dim, aniso);
+  for (size_t j = 0; j < somas.size(); ++j) arena_origin[vs.size() + j] = somas[j].lo;
+  AssemblyResult asmb = assemble(ctx, cstore.data(), dbf.data(), ap, arena_off, arena_dim, arena_origin, aniso);
   const long long V = asmb.vertex_offsets.back(), E = asmb.edge_offsets.back();
   std::vector<float> hvert, hrad;
   std::vector<uint32_t> hedge;
@@ -584,6 +783,12 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   ctx.stats["railroad_touched"] = double(w[1]);
   ctx.stats["invalidated"] = double(w[2]);
   ctx.stats["objects"] = nobj;
+  ctx.stats["soma_candidates"] = double(somas.size());
+  {
+    long long n = 0;
+    for (const auto &sa : somas) n += sa.soma ? 1 : 0;
+    ctx.stats["somata"] = double(n);
+  }
   ctx.stats["voxels"] = double(N);
   ctx.stats["foreground"] = double(F);
   ctx.stats["launches"] = double(ctx.launches);

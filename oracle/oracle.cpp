@@ -441,11 +441,14 @@ Weights geometric_weights(const float aniso[3]) {
 }
 
 void geometric_flood(const std::vector<uint32_t> &ids, const Shape &s, uint32_t label, i64 source, const Weights &W,
-                     std::vector<float> &dist, const std::vector<i64> &voxels) {
-  for (i64 v : voxels) dist[v] = kInf;
+                     std::vector<float> &dist, const std::vector<i64> &voxels, const std::vector<float> *seeds = nullptr) {
   using Item = std::pair<float, i64>;
   std::priority_queue<Item, std::vector<Item>, std::greater<Item>> heap;
-  dist[source] = 0.0f; heap.push({0.0f, source});
+  for (i64 v : voxels) {
+    dist[v] = seeds ? (*seeds)[v] : kInf;
+    if (dist[v] < kInf) heap.push({dist[v], v});
+  }
+  if (dist[source] != 0.0f) { dist[source] = 0.0f; heap.push({0.0f, source}); }
   while (!heap.empty()) {
     auto [d, u] = heap.top(); heap.pop();
     if (d > dist[u]) continue;
@@ -641,12 +644,12 @@ std::vector<i64> parent_walk(const Volume &V, uint32_t label, i64 target, i64 ro
 // offers from its key at the round boundary). Voxels offered beyond the band wait; at the band
 // boundary each takes the best offer of its claimed neighbours, the smallest of those names the
 // next band, and those inside it are claimed. Returns the number of voxels invalidated.
-i64 invalidate(Volume &V, uint32_t label, const std::vector<i64> &path, const Params &P,
-               std::vector<i64> &touched, std::vector<i64> &frontier, std::vector<i64> &next, std::vector<i64> &far,
-               std::vector<i64> &keep, std::vector<uint64_t> &snap) {
+i64 invalidate(Volume &V, uint32_t label, const std::vector<i64> &path, const Params &P, double reach_scale,
+               double reach_constant, std::vector<i64> &touched, std::vector<i64> &frontier, std::vector<i64> &next,
+               std::vector<i64> &far, std::vector<i64> &keep, std::vector<uint64_t> &snap) {
   const Shape &s = V.s; const auto &ids = *V.ids;
   const float wx = P.anisotropy[0], wy = P.anisotropy[1], wz = P.anisotropy[2];
-  const float scale = float(P.scale), constant = float(P.constant);
+  const float scale = float(reach_scale), constant = float(reach_constant);
   const float delta = std::min({wx, wy, wz});
   touched.clear(); frontier.clear(); far.clear();
   for (i64 p : path) {
@@ -755,18 +758,53 @@ struct ObjectPlan {
   std::vector<i64> manual;     // manual targets in pop order
   std::vector<i64> after;      // targets after the automatic ones, in pop order
   i64 max_paths;
+  Volume *vol = nullptr;       // the volume the object is traced in (the input, or its own crop)
+  uint32_t label = 0;          // the object's id in that volume
+  std::array<i64, 3> origin{}; // where that volume's (0, 0, 0) lies in the input
+  bool soma = false;
+  double soma_radius = 0;      // paths are trimmed to this distance from the root
 };
 
 // The trace loop of one object (trace.cu:196-246 order, lockstep.cu:91-183 targets): manual
 // targets first, then the first alive voxel of the target order, then, once no voxel is alive,
 // the targets after (trace.cu:209-212); railroad; invalidation; the path becomes rails.
+// Soma trimming (trace.cu:222-236): a path keeps its first vertex and every vertex farther than
+// the soma radius from the root (float64 distance from the float32 root); with fix_branching a
+// rail end within the radius gives way to the root. Without fix_branching the reference's paths
+// are root-first, so the kept first vertex is the root.
+std::vector<i64> trim_to_soma(const Shape &s, const std::vector<i64> &path, i64 root, double radius, const Params &P) {
+  if (path.empty()) return path;
+  i64 rx, ry, rz; s.xyz(root, rx, ry, rz);
+  const double r[3] = {double(float(rx)), double(float(ry)), double(float(rz))};
+  auto far = [&](i64 v) {
+    i64 x, y, z; s.xyz(v, x, y, z);
+    const double p[3] = {double(x), double(y), double(z)};
+    double squared = 0;
+    for (int k = 0; k < 3; ++k) { const double d = double(P.anisotropy[k]) * (p[k] - r[k]); squared += d * d; }
+    return std::sqrt(squared) > radius;
+  };
+  std::vector<i64> ordered = path;
+  if (!P.fix_branching) std::reverse(ordered.begin(), ordered.end());  // root first
+  std::vector<i64> out = {ordered.front()};
+  bool last_far = true;
+  for (i64 v : ordered) {
+    last_far = far(v);
+    if (last_far) out.push_back(v);
+  }
+  if (P.fix_branching && !last_far) out.push_back(root);
+  return out;
+}
+
 std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, const Params &P) {
   std::vector<std::vector<i64>> paths;
   std::vector<i64> touched, frontier, next, far, keep, rtouched;
   std::vector<uint64_t> snap;
+  const uint32_t label = plan.label;
+  if (plan.soma)  // the soma's ball first, with the soma's reach (trace.cu:199)
+    invalidate(V, label, {plan.root}, P, P.soma_scale, P.soma_constant, touched, frontier, next, far, keep, snap);
   if (plan.max_paths <= 0) return paths;
   if (P.fix_branching) V.pdrf[plan.root] = 0.0f;  // the root is the first rail
-  else parental_field(V, plan.id, plan.root, plan.voxels);
+  else parental_field(V, label, plan.root, plan.voxels);
   size_t cursor = 0, after = 0;
   while (i64(paths.size()) < plan.max_paths) {
     i64 t = -1;
@@ -778,10 +816,11 @@ std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, co
       else if (after < plan.after.size()) t = plan.after[after++];
       else break;
     }
-    std::vector<i64> path = P.fix_branching ? railroad(V, plan.id, t, rtouched)
-                                            : parent_walk(V, plan.id, t, plan.root, i64(plan.voxels.size()) + 1);
+    std::vector<i64> path = P.fix_branching ? railroad(V, label, t, rtouched)
+                                            : parent_walk(V, label, t, plan.root, i64(plan.voxels.size()) + 1);
     if (path.empty()) throw std::runtime_error("no rail reachable from a target");
-    invalidate(V, plan.id, path, P, touched, frontier, next, far, keep, snap);
+    if (plan.soma) path = trim_to_soma(V.s, path, plan.root, plan.soma_radius, P);
+    invalidate(V, label, path, P, P.scale, P.constant, touched, frontier, next, far, keep, snap);
     if (P.fix_branching)
       for (i64 v : path) V.pdrf[v] = 0.0f;
     paths.push_back(std::move(path));
@@ -791,23 +830,31 @@ std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, co
   return paths;
 }
 
-// consolidate (skeleton.cpp:13-40) on voxel coordinates, then physical vertices and radii.
+// consolidate (skeleton.cpp:13-40) on voxel coordinates, then physical vertices and radii. A path
+// is a list of input-volume voxel coordinates with the DBF of the volume it was traced in.
 struct Skeleton {
   int64_t label = 0;
   std::vector<std::array<i64, 3>> vox;
+  std::vector<float> radius;
   std::vector<std::array<uint32_t, 2>> edges;
 };
 
-Skeleton assemble(const std::vector<std::vector<i64>> &paths, const Shape &s) {
+struct CoordPath {
+  std::vector<std::array<i64, 3>> pts;
+  std::vector<float> radius;
+};
+
+Skeleton assemble(const std::vector<CoordPath> &paths) {
   Skeleton out;
   std::vector<std::array<i64, 3>> vertices;
+  std::vector<float> radius;
   std::vector<std::array<uint32_t, 2>> edges;
   for (const auto &path : paths) {
-    if (path.size() < 2) continue;
+    if (path.pts.size() < 2) continue;
     const uint32_t base = uint32_t(vertices.size());
-    for (size_t j = 0; j < path.size(); ++j) {
-      i64 x, y, z; s.xyz(path[j], x, y, z);
-      vertices.push_back({x, y, z});
+    for (size_t j = 0; j < path.pts.size(); ++j) {
+      vertices.push_back(path.pts[j]);
+      radius.push_back(path.radius[j]);
       if (j) edges.push_back({uint32_t(base + j - 1), uint32_t(base + j)});
     }
   }
@@ -816,8 +863,9 @@ Skeleton assemble(const std::vector<std::vector<i64>> &paths, const Shape &s) {
   std::iota(order.begin(), order.end(), 0u);
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return vertices[a] < vertices[b]; });
   std::vector<std::array<i64, 3>> uniq;
+  std::vector<float> uniq_radius;
   for (uint32_t old : order) {
-    if (uniq.empty() || uniq.back() != vertices[old]) uniq.push_back(vertices[old]);
+    if (uniq.empty() || uniq.back() != vertices[old]) { uniq.push_back(vertices[old]); uniq_radius.push_back(radius[old]); }
     inverse[old] = uint32_t(uniq.size() - 1);
   }
   std::vector<std::array<uint32_t, 2>> e2;
@@ -832,10 +880,83 @@ Skeleton assemble(const std::vector<std::vector<i64>> &paths, const Shape &s) {
   for (auto e : e2) used[e[0]] = used[e[1]] = 1;
   std::vector<uint32_t> remap(uniq.size(), 0);
   for (size_t i = 0; i < uniq.size(); ++i)
-    if (used[i]) { remap[i] = uint32_t(out.vox.size()); out.vox.push_back(uniq[i]); }
+    if (used[i]) { remap[i] = uint32_t(out.vox.size()); out.vox.push_back(uniq[i]); out.radius.push_back(uniq_radius[i]); }
   for (auto &e : e2) e = {remap[e[0]], remap[e[1]]};
   out.edges = std::move(e2);
   return out;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Somata (trace.cu:98-131, soma.cu:141-237). fill_voids (trace_primitives.cu:238-253,
+// fillvoids_kernels.cuh): background voxels of the crop that are not 6-connected to the crop's
+// faces become foreground. Returns the number filled.
+i64 fill_voids(std::vector<uint32_t> &mask, const Shape &s) {
+  std::vector<uint8_t> seen(mask.size(), 0);
+  std::vector<i64> stack;
+  for (i64 v = 0; v < s.n(); ++v) {
+    if (mask[v]) continue;
+    i64 x, y, z; s.xyz(v, x, y, z);
+    if (x == 0 || y == 0 || z == 0 || x == s.sx - 1 || y == s.sy - 1 || z == s.sz - 1) { seen[v] = 1; stack.push_back(v); }
+  }
+  while (!stack.empty()) {
+    const i64 u = stack.back(); stack.pop_back();
+    i64 x, y, z; s.xyz(u, x, y, z);
+    for (int k = 0; k < 6; ++k) {
+      const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
+      if (!s.inside(nx, ny, nz)) continue;
+      const i64 v = s.idx(nx, ny, nz);
+      if (mask[v] || seen[v]) continue;
+      seen[v] = 1; stack.push_back(v);
+    }
+  }
+  i64 filled = 0;
+  for (i64 v = 0; v < s.n(); ++v)
+    if (!mask[v] && !seen[v]) { mask[v] = 1; ++filled; }
+  return filled;
+}
+
+// The soma root (trace.cu:55-73, batched.cu:58-105): among the voxels at the DBF maximum, sorted
+// by (x, y, z), the first nearest (float64 squared distance, voxel units) to their float32 centroid.
+i64 soma_root(const std::vector<float> &dbf, const std::vector<i64> &voxels, float maximum, const Shape &s) {
+  std::vector<std::array<i64, 3>> points;
+  for (i64 v : voxels)
+    if (dbf[v] == maximum) { i64 x, y, z; s.xyz(v, x, y, z); points.push_back({x, y, z}); }
+  if (points.empty()) throw std::runtime_error("no soma maximum");
+  std::array<i64, 3> sum{0, 0, 0};
+  for (const auto &p : points) for (int k = 0; k < 3; ++k) sum[k] += p[k];
+  std::sort(points.begin(), points.end());
+  float centre[3];
+  for (int k = 0; k < 3; ++k) centre[k] = float(double(sum[k]) / double(points.size()));
+  double best = INFINITY;
+  std::array<i64, 3> root = points.front();
+  for (const auto &p : points) {
+    double cost = 0;
+    for (int k = 0; k < 3; ++k) { const double d = double(p[k]) - double(centre[k]); cost += d * d; }
+    if (cost < best) { best = cost; root = p; }
+  }
+  return s.idx(root[0], root[1], root[2]);
+}
+
+// The free-space seed of a soma's DAF (sssp_kernels.cuh:14-35): every object voxel within the
+// radius (float32 physical distance) of the root starts at its 26-connected distance through
+// empty space.
+void freespace_seed(std::vector<float> &dist, const std::vector<i64> &voxels, const Shape &s, i64 root,
+                    const float a[3], float radius) {
+  i64 rx, ry, rz; s.xyz(root, rx, ry, rz);
+  const float wx = a[0], wy = a[1], wz = a[2];
+  for (i64 v : voxels) {
+    i64 x, y, z; s.xyz(v, x, y, z);
+    const float rdx = wx * float(x - rx), rdy = wy * float(y - ry), rdz = wz * float(z - rz);
+    if (rdx * rdx + rdy * rdy + rdz * rdz > radius * radius) continue;
+    const float dx = std::fabs(float(x - rx)), dy = std::fabs(float(y - ry)), dz = std::fabs(float(z - rz));
+    const float dxyz = std::min(std::min(dx, dy), dz);
+    const float dxy = std::min(dx, dy), dyz = std::min(dy, dz), dxz = std::min(dx, dz);
+    const float val = dxyz * std::sqrt(wx * wx + wy * wy + wz * wz) + wx * (dx - dxyz) + wy * (dy - dxyz) +
+                      wz * (dz - dxyz) + (dxy - dxyz) * (std::sqrt(wx * wx + wy * wy) - wx - wy) +
+                      (dxz - dxyz) * (std::sqrt(wx * wx + wz * wz) - wx - wz) +
+                      (dyz - dxyz) * (std::sqrt(wy * wy + wz * wz) - wy - wz);
+    dist[v] = val;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -862,10 +983,18 @@ struct Result {
   std::shared_ptr<Staged> staged;  // between prepare and finish
 };
 
+// A soma candidate's own crop: its (filled) mask as ids 0/1, and the volume state over it.
+struct PrivateVolume {
+  std::vector<uint32_t> ids;
+  Volume V;
+  std::array<i64, 3> origin{};
+};
+
 struct Staged {
   Shape s;
   Params P;
   Volume V;
+  std::vector<std::unique_ptr<PrivateVolume>> privates;
   int keep_stages = 0;
   std::vector<std::array<i64, 7>> box;
   std::vector<ObjectPlan> plans;
@@ -925,15 +1054,16 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
   if (P.fix_borders) borders = border_targets(ids, s, count, P.anisotropy);
   R.stage_ms[3] = lap.next();
   // active objects (batched.cu:187-191): more voxels than dust and a bounding box of 2+ voxels
-  std::vector<uint8_t> active(count + 1, 0);
+  std::vector<uint8_t> active(count + 1, 0), candidate(count + 1, 0);
   std::vector<float> dbf_max(count + 1, 0.0f);
   for (size_t id = 1; id <= count; ++id) {
     const auto &b = box[id];
     const i64 bbox = (b[3] - b[0] + 1) * (b[4] - b[1] + 1) * (b[5] - b[2] + 1);
     float m; argmax(V.dbf, voxels[id], m); dbf_max[id] = m;
     if (double(b[6]) <= P.dust || bbox <= 1) continue;
-    if (double(dbf_max[id]) > P.soma_detection) throw std::invalid_argument("soma objects are not covered by the oracle");
     active[id] = 1;
+    // a soma candidate is prepared and traced in a crop of its own (its voids filled)
+    if (double(dbf_max[id]) > P.soma_detection) candidate[id] = 1;
   }
   // roots and DAF per object: every object's floods touch only its own voxels
   const Weights W = geometric_weights(P.anisotropy);
@@ -943,7 +1073,7 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
   parallel_for(i64(count), threads, 1, [&](i64 b, i64 e) {
     for (i64 j = b; j < e; ++j) {
       const size_t id = size_t(j) + 1;
-      if (!active[id]) continue;
+      if (!active[id] || candidate[id]) continue;
       i64 root;
       if (!borders[id].empty()) { const auto &p = borders[id].back(); root = s.idx(p[0], p[1], p[2]); }
       else {
@@ -971,7 +1101,7 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
     std::vector<float> M(count + 1, 0.0f), inv(count + 1, 0.0f);
     std::vector<uint8_t> use(count + 1, 0);
     for (size_t id = 1; id <= count; ++id)
-      if (active[id]) {
+      if (active[id] && !candidate[id]) {
         M[id] = float(1.0 / std::pow(double(dbf_max[id]), 1.01));
         if (max_daf[id] != 0) { inv[id] = float(1.0 / double(max_daf[id])); use[id] = 2; } else use[id] = 1;
       }
@@ -993,7 +1123,7 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
   }
   if (P.pdrf_field) {  // a test's field replaces the computed one over the traced objects' voxels
     for (i64 i = 0; i < n; ++i)
-      if (ids[i] && active[ids[i]]) V.pdrf[i] = P.pdrf_field[i];
+      if (ids[i] && active[ids[i]] && !candidate[ids[i]]) V.pdrf[i] = P.pdrf_field[i];
   }
   R.stage_ms[5] = lap.next();
   if (keep_stages) { R.dbf = V.dbf; R.daf = daf; R.pdrf = V.pdrf; }
@@ -1013,9 +1143,10 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
   // target orders and manual targets (lockstep.cu:120-142, lockstep_order.cu:21-45)
   auto &plans = st->plans;
   for (size_t id = 1; id <= count; ++id) {
-    if (!active[id]) continue;
+    if (!active[id] || candidate[id]) continue;
     ObjectPlan plan;
     plan.id = uint32_t(id); plan.root = roots[id]; plan.target = targets[id];
+    plan.vol = &V; plan.label = uint32_t(id);
     plan.voxels = std::move(voxels[id]);
     std::vector<i64> manual;
     for (const auto &p : borders[id]) manual.push_back(s.idx(p[0], p[1], p[2]));
@@ -1028,6 +1159,104 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
     plan.max_paths = i64(plan.manual.size() + plan.after.size()) >= budget ? 0 : budget;
     plans.push_back(std::move(plan));
   }
+  // soma candidates (prepare_component, trace.cu:98-131): the crop of the object's box with its
+  // voids filled; the DBF recomputed on that crop when anything was filled (black border when it
+  // fills the crop), else the input's; a soma when the maximum passes soma_acceptance_threshold:
+  // the root at the maximum nearest the maxima's centroid, the DAF seeded through free space
+  // within the maximum of the root, the border root traced last among the manual targets and no
+  // default target
+  std::vector<size_t> soma_ids;
+  for (size_t id = 1; id <= count; ++id) if (candidate[id]) soma_ids.push_back(id);
+  std::vector<ObjectPlan> soma_plans(soma_ids.size());
+  st->privates.resize(soma_ids.size());
+  parallel_for(i64(soma_ids.size()), threads, 1, [&](i64 b, i64 e) {
+    for (i64 j = b; j < e; ++j) {
+      const size_t id = soma_ids[j];
+      const auto &bx = box[id];
+      auto pv = std::make_unique<PrivateVolume>();
+      const Shape cs{bx[3] - bx[0] + 1, bx[4] - bx[1] + 1, bx[5] - bx[2] + 1};
+      pv->origin = {bx[0], bx[1], bx[2]};
+      pv->ids.assign(cs.n(), 0);
+      std::vector<float> crop_dbf(cs.n(), 0.0f);
+      for (i64 v : voxels[id]) {
+        i64 x, y, z; s.xyz(v, x, y, z);
+        const i64 c = cs.idx(x - bx[0], y - bx[1], z - bx[2]);
+        pv->ids[c] = 1;
+        crop_dbf[c] = V.dbf[v];
+      }
+      const i64 filled = fill_voids(pv->ids, cs);
+      const i64 valid = bx[6] + filled;
+      Volume &PV = pv->V;
+      PV.s = cs; PV.ids = &pv->ids;
+      PV.dbf = filled ? edt(pv->ids.data(), cs, P.anisotropy, valid == cs.n(), 3, 1) : std::move(crop_dbf);
+      std::vector<i64> cvox;
+      for (i64 c = 0; c < cs.n(); ++c) if (pv->ids[c]) cvox.push_back(c);
+      float maximum; argmax(PV.dbf, cvox, maximum);
+      ObjectPlan plan;
+      plan.id = uint32_t(id); plan.vol = &PV; plan.label = 1; plan.origin = pv->origin;
+      plan.soma = double(maximum) > P.soma_acceptance;
+      auto crop_flat = [&](std::array<i64, 3> p) { return cs.idx(p[0] - bx[0], p[1] - bx[1], p[2] - bx[2]); };
+      auto to_crop = [&](i64 v) { i64 x, y, z; s.xyz(v, x, y, z); return cs.idx(x - bx[0], y - bx[1], z - bx[2]); };
+      std::vector<float> cdaf(cs.n(), kInf);
+      i64 root;
+      if (plan.soma) {
+        root = soma_root(PV.dbf, cvox, maximum, cs);
+        plan.soma_radius = double(maximum) * P.soma_scale + P.soma_constant;
+        std::vector<float> seeds(cs.n(), kInf);
+        freespace_seed(seeds, cvox, cs, root, P.anisotropy, maximum);
+        geometric_flood(pv->ids, cs, 1, root, W, cdaf, cvox, &seeds);
+      } else {
+        if (!borders[id].empty()) root = crop_flat(borders[id].back());
+        else {
+          geometric_flood(pv->ids, cs, 1, cvox.front(), W, cdaf, cvox);
+          float m; root = argmax(cdaf, cvox, m);
+        }
+        geometric_flood(pv->ids, cs, 1, root, W, cdaf, cvox);
+      }
+      float far_daf; const i64 target = argmax(cdaf, cvox, far_daf);
+      // PDRF of the crop (the maximum and the farthest DAF of the crop's fields)
+      PV.pdrf.assign(cs.n(), kInf);
+      const float M = float(1.0 / std::pow(double(maximum), 1.01));
+      const float inv = far_daf != 0 ? float(1.0 / double(far_daf)) : 0.0f;
+      for (i64 c : cvox) {
+        float d = PV.dbf[c];
+        if (d == 0.0f) d = kInf;
+        float q = 1.0f - d * M;
+        if (squarings >= 0) for (int k = 0; k < squarings; ++k) q = q * q;
+        else q = float(std::pow(double(q), exponent));
+        q = q * float(P.pdrf_scale);
+        if (far_daf != 0) { float dd = cdaf[c]; if (std::isinf(dd)) dd = 0.0f; q = q + dd * inv; }
+        PV.pdrf[c] = q;
+      }
+      std::vector<i64> manual;
+      for (const auto &p : borders[id]) manual.push_back(crop_flat(p));
+      if (!manual.empty()) manual.pop_back();
+      if (plan.soma && !borders[id].empty()) manual.insert(manual.begin(), crop_flat(borders[id].back()));
+      for (i64 v : before_of[id]) manual.push_back(to_crop(v));
+      if (manual.empty() && !plan.soma) plan.manual.push_back(target);
+      else plan.manual.assign(manual.rbegin(), manual.rend());
+      for (auto it = after_of[id].rbegin(); it != after_of[id].rend(); ++it) plan.after.push_back(to_crop(*it));
+      const i64 budget = P.has_max_paths ? P.max_paths : valid;
+      plan.max_paths = i64(plan.manual.size() + plan.after.size()) >= budget ? 0 : budget;
+      plan.root = root; plan.target = target;
+      plan.voxels = cvox;
+      plan.order = cvox;
+      std::sort(plan.order.begin(), plan.order.end(), [&](i64 a, i64 c) {
+        float x = cdaf[a], y = cdaf[c];
+        if (std::isinf(x)) x = 0;
+        if (std::isinf(y)) y = 0;
+        return x == y ? a > c : x > y;
+      });
+      PV.dist.assign(cs.n(), kInf);
+      PV.alive.assign(pv->ids.begin(), pv->ids.end());
+      PV.inq.assign(cs.n(), 0);
+      PV.key.assign(cs.n(), kUnclaimed);
+      auto to_input = [&](i64 c) { i64 x, y, z; cs.xyz(c, x, y, z); return s.idx(x + bx[0], y + bx[1], z + bx[2]); };
+      roots[id] = to_input(root); targets[id] = to_input(target);
+      soma_plans[j] = std::move(plan);
+      st->privates[j] = std::move(pv);
+    }
+  });
   parallel_for(i64(plans.size()), threads, 1, [&](i64 b, i64 e) {
     for (i64 j = b; j < e; ++j) {
       ObjectPlan &plan = plans[j];
@@ -1040,10 +1269,11 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
       });
     }
   });
+  for (auto &plan : soma_plans) plans.push_back(std::move(plan));
   R.stage_ms[6] = lap.next();
   V.dist.assign(n, kInf);
   V.alive.assign(n, 0);
-  for (i64 i = 0; i < n; ++i) V.alive[i] = ids[i] ? active[ids[i]] : 0;
+  for (i64 i = 0; i < n; ++i) V.alive[i] = ids[i] ? active[ids[i]] && !candidate[ids[i]] : 0;
   V.inq.assign(n, 0);
   V.key.assign(n, kUnclaimed);
   st->traced.assign(plans.size(), {});
@@ -1070,7 +1300,7 @@ void trace(Result &R, size_t begin, size_t end, int threads) {
       const size_t j = next.fetch_add(1);
       if (j >= end) return;
       const size_t i = st.schedule[j];
-      try { st.traced[i] = trace_object(st.V, st.plans[i], st.P); }
+      try { st.traced[i] = trace_object(*st.plans[i].vol, st.plans[i], st.P); }
       catch (const std::exception &e) { std::lock_guard<std::mutex> lock(failure); message = e.what(); }
     }
   };
@@ -1087,25 +1317,45 @@ void trace(Result &R, size_t begin, size_t end, int threads) {
 void finish(Result &R) {
   Staged &st = *R.staged;
   Lap lap;
-  const Shape &s = st.s;
   const auto &plans = st.plans;
   const auto &traced = st.traced;
+  // every path in input coordinates with the radii of the volume it was traced in; components of
+  // one label merge in id order (plans are in id order, the soma candidates' last, so sort)
+  std::vector<size_t> by_id(plans.size());
+  std::iota(by_id.begin(), by_id.end(), size_t(0));
+  std::stable_sort(by_id.begin(), by_id.end(), [&](size_t a, size_t b) { return plans[a].id < plans[b].id; });
+  auto coords = [&](size_t j) {
+    const ObjectPlan &plan = plans[j];
+    const Volume &PV = *plan.vol;
+    std::vector<CoordPath> out;
+    for (const auto &path : traced[j]) {
+      CoordPath cp;
+      for (i64 v : path) {
+        i64 x, y, z; PV.s.xyz(v, x, y, z);
+        cp.pts.push_back({x + plan.origin[0], y + plan.origin[1], z + plan.origin[2]});
+        cp.radius.push_back(PV.dbf[v]);
+      }
+      out.push_back(std::move(cp));
+    }
+    return out;
+  };
   std::vector<int64_t> label_order;
-  std::vector<std::vector<std::vector<i64>>> merged;
-  for (size_t j = 0; j < plans.size(); ++j) {
+  std::vector<std::vector<CoordPath>> merged;
+  for (size_t j : by_id) {
     const int64_t label = R.cc.mapping[plans[j].id];
-    Skeleton sk = assemble(traced[j], s);
+    auto cps = coords(j);
+    Skeleton sk = assemble(cps);
     if (sk.edges.empty()) continue;
     auto it = std::find(label_order.begin(), label_order.end(), label);
-    if (it == label_order.end()) { label_order.push_back(label); merged.push_back(traced[j]); }
-    else { auto &m = merged[it - label_order.begin()]; m.insert(m.end(), traced[j].begin(), traced[j].end()); }
+    if (it == label_order.end()) { label_order.push_back(label); merged.push_back(std::move(cps)); }
+    else { auto &m = merged[it - label_order.begin()]; m.insert(m.end(), cps.begin(), cps.end()); }
   }
   for (size_t j = 0; j < label_order.size(); ++j) {
-    Skeleton sk = assemble(merged[j], s);
+    Skeleton sk = assemble(merged[j]);
     R.labels.push_back(label_order[j]);
-    for (const auto &v : sk.vox) {
-      for (int a = 0; a < 3; ++a) R.vertices.push_back(float(v[a]) * st.P.anisotropy[a]);
-      R.radii.push_back(st.V.dbf[s.idx(v[0], v[1], v[2])]);
+    for (size_t q = 0; q < sk.vox.size(); ++q) {
+      for (int a = 0; a < 3; ++a) R.vertices.push_back(float(sk.vox[q][a]) * st.P.anisotropy[a]);
+      R.radii.push_back(sk.radius[q]);
     }
     for (const auto &e : sk.edges) { R.edges.push_back(e[0]); R.edges.push_back(e[1]); }
     R.vertex_offsets.push_back(int64_t(R.radii.size()));
@@ -1119,13 +1369,13 @@ void finish(Result &R) {
     for (size_t id = 1; id <= count; ++id) {
       R.order_offsets[id + 1] = R.order_offsets[id];
       auto it = std::find_if(plans.begin(), plans.end(), [&](const ObjectPlan &p) { return p.id == id; });
-      if (it == plans.end()) continue;
+      if (it == plans.end() || it->vol != &st.V) continue;  // a soma candidate's order is in its crop
       R.orders.insert(R.orders.end(), it->order.begin(), it->order.end());
       R.order_offsets[id + 1] += i64(it->order.size());
     }
-    for (size_t j = 0; j < plans.size(); ++j)
-      for (const auto &p : traced[j]) {
-        R.paths_flat.insert(R.paths_flat.end(), p.begin(), p.end());
+    for (size_t j : by_id)
+      for (const auto &cp : coords(j)) {
+        for (const auto &q : cp.pts) R.paths_flat.push_back(st.s.idx(q[0], q[1], q[2]));
         R.path_offsets.push_back(i64(R.paths_flat.size()));
         R.path_labels.push_back(plans[j].id);
       }

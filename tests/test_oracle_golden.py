@@ -191,3 +191,55 @@ def test_oracle_threads_and_steps_do_not_change_the_result():
     stepped = run.finish().packed()
     for name, value in one.packed().items():
         np.testing.assert_array_equal(stepped[name], value, err_msg=name)
+
+
+def _soma_with_processes(size=72, centre=36, radius=12):
+    """The reference's soma test shape (test_package.py:343-366): a ball with a three-voxel-thick
+    process along each axis through its centre."""
+    grid = np.indices((size,) * 3) - centre
+    labels = ((grid ** 2).sum(axis=0) <= radius ** 2).astype(np.uint8)
+    for axis in range(3):
+        tube = [slice(centre - 1, centre + 2)] * 3
+        tube[axis] = slice(2, size - 2)
+        labels[tuple(tube)] = 1
+    return np.asfortranarray(labels)
+
+
+SOMA_PARAMS = dict(scale=1.5, const=2, pdrf_scale=100000, pdrf_exponent=4, soma_detection_threshold=6,
+                   soma_acceptance_threshold=9, soma_invalidation_scale=1.0, soma_invalidation_const=2)
+
+
+def _components(vertices, edges):
+    parent = list(range(len(vertices)))
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    for a, b in edges:
+        parent[find(a)] = find(b)
+    return len({find(i) for i in range(len(vertices))})
+
+
+@pytest.mark.parametrize("fix_branching", [True, False])
+@pytest.mark.parametrize("hollow", [False, True])
+def test_soma_paths_stay_attached(fix_branching, hollow):
+    """The reference's soma known answers (test_package.py:343-366), with and without
+    fix_branching: every process is traced, the soma root (the centre) is a vertex, and the
+    skeleton is one connected tree. `hollow` adds a cavity inside the soma: the filled crop's
+    recomputed DBF gives the same answers."""
+    labels = _soma_with_processes()
+    if hollow:
+        labels[33:40, 30:34, 33:40] = 0  # a void the processes do not cross, filled before tracing
+    verts, edges, _ = oracle.skeletonize(labels, teasar_params=SOMA_PARAMS, dust_threshold=0,
+                                         fix_branching=fix_branching, fix_borders=False).skeletons()[1]
+    offsets = np.abs(verts - 36)
+    assert (offsets.max(axis=1) > 30).sum() >= 6, "every process is traced"
+    assert np.any(np.all(verts == 36, axis=1)), "the soma root is a vertex"
+    assert _components(verts, edges) == 1
+    # no path vertex well inside the soma radius (about the ball's radius + 2) but the root: the
+    # paths are trimmed to it
+    inside = np.sqrt((offsets ** 2).sum(axis=1)) <= 10
+    assert inside.sum() == 1
