@@ -1,18 +1,23 @@
 // Connected components on sm_100a: union-find over the 13 forward neighbours of every voxel
 // (the root of a component is its lowest flat index, since links always point from the larger
-// root to the smaller), a read-only flatten, and ids from an exclusive scan of the root flags in
-// flat order: id k belongs to the k-th root in ascending flat order, the reference's canonical
-// numbering (ccl.cu:25-63 of giorgioangel/brook) without its host sort.
+// root to the smaller), and ids from an exclusive scan of the root flags in flat order: id k
+// belongs to the k-th root in ascending flat order, the reference's canonical numbering
+// (ccl.cu:25-63 of giorgioangel/brook) without its host sort.
 //
-// The union runs in two kernels: tile_union labels 32x8x8 tiles in shared memory (labels staged
-// once, each x run of equal labels linked to its first voxel by a warp ballot, then union-find
-// with path halving on shared indices; a tile's order is the volume's, so a tile root is its
-// component's lowest flat index in the tile) and writes every voxel's tile root as its parent;
-// face_union then unites only the pairs that cross a tile face, on the global parent array.
+// The union runs in two kernels: tile_union labels 32x8x8 tiles in shared memory (the tile's
+// labels and a one-voxel halo staged once, each x run of equal labels linked to its first voxel by
+// a warp ballot, then union-find with path halving on shared indices; a tile's order is the
+// volume's, so a tile root is its component's lowest flat index in the tile), writes every
+// voxel's tile root as its parent, and lists the pairs across tile faces that still need a union
+// (from the halo, after the deduplication rules below); union_pairs then unites the listed pairs
+// on the global parent array. A list that overflows its capacity falls back to face_union, which
+// scans every tile-face voxel. Ids come from a scan of the root flags; relabel finds each voxel's
+// root itself (no separate flatten pass).
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
 
+#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
@@ -97,34 +102,94 @@ __device__ __forceinline__ void tile_unite(int *par, int a, int b) {
   }
 }
 
+// The halo of a tile: x in [x0 - 1, x0 + 32], y in [y0 - 1, y0 + 8], z in [z0, z0 + 8] (every
+// forward neighbour of a tile voxel, and every intermediate of such a pair, lies inside it).
+constexpr int kHaloX = kTileX + 2, kHaloY = kTileY + 2, kHaloZ = kTileZ + 1, kHaloN = kHaloX * kHaloY * kHaloZ;
+constexpr int kPairStage = 512;  // cross-tile pairs a tile collects in shared memory before it writes them out
+
+// A list of cross-tile pairs to unite: `count` entries were offered, the first `capacity` kept.
+struct PairList {
+  int2 *pairs;
+  int *count;
+  int capacity;
+};
+
 // grid (x tiles, y tiles, z tiles from tz0); parent of every voxel of the tile = its tile root, as
-// an index of the flat space the volume starts at `base` in; background: -1.
+// an index of the flat space the volume starts at `base` in; background: -1. The cross-tile pairs
+// this tile's voxels start go to `list`; pairs across the tile's +z face only where the plane
+// beyond is there (z0 + 8 < z_ready).
 template <class L>
 __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__ labels, int *parent, Dims d, bool planar,
-                                                           long long base, int tz0) {
-  __shared__ L lab[kTileN];
+                                                           long long base, int tz0, int z_ready, PairList list) {
+  __shared__ L hal[kHaloN];
   __shared__ int par[kTileN];
+  __shared__ int2 staged[kPairStage];
+  __shared__ int nstaged, first;
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z0 = (tz0 + int(blockIdx.z)) * kTileZ;
   const int ex = min(kTileX, d.sx - x0), ey = min(kTileY, d.sy - y0), ez = min(kTileZ, d.sz - z0);
+  const bool zface = !planar && z0 + kTileZ < d.sz && z0 + kTileZ < z_ready;
+  if (threadIdx.x == 0) nstaged = 0;
+  // halo load, rows of 34 along x; outside the volume (or beyond the planes this pass may read)
+  // reads as background, which never equals a voxel's label
+  const int hz_end = planar ? kTileZ : (zface ? kHaloZ : kTileZ);
+  for (int h = threadIdx.x; h < kHaloX * kHaloY * hz_end; h += kTileThreads) {
+    const int hx = h % kHaloX, hy = (h / kHaloX) % kHaloY, hz = h / (kHaloX * kHaloY);
+    const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 + hz;
+    const bool in = gx >= 0 && gy >= 0 && gx < d.sx && gy < d.sy && gz < d.sz;
+    hal[h] = in ? labels[gx + (long long)d.sx * (gy + (long long)d.sy * gz)] : L(0);
+  }
+  for (int h = kHaloX * kHaloY * hz_end + threadIdx.x; h < kHaloN; h += kTileThreads) hal[h] = L(0);
+  __syncthreads();
+  auto at = [](int lx, int ly, int lz) { return (lx + 1) + kHaloX * ((ly + 1) + kHaloY * lz); };
   // a tile row is one warp (kTileX == 32): every voxel starts under the first voxel of its run of
-  // equal labels along x, so the x-face pairs are united without a find
+  // equal labels along x, so the x-face pairs inside the tile are united without a find
   static_assert(kTileX == 32 && kTileThreads % 32 == 0, "a tile row is one warp");
   for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
     const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
     const bool in = lx < ex && ly < ey && lz < ez;
-    const L lv = in ? labels[(x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz))] : L(0);
-    lab[t] = lv;
-    const L left = __shfl_up_sync(0xFFFFFFFFu, lv, 1);
-    const bool joins = lx > 0 && lv != L(0) && left == lv;
+    const L lv = in ? hal[at(lx, ly, lz)] : L(0);
+    const bool joins = lx > 0 && lv != L(0) && hal[at(lx - 1, ly, lz)] == lv;
     const unsigned starts = __ballot_sync(0xFFFFFFFFu, !joins);
     par[t] = t - lx + (31 - __clz(starts & (0xFFFFFFFFu >> (31 - lx))));
   }
   __syncthreads();
   for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
-    const L lv = lab[t];
-    if (lv == L(0)) continue;
     const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
-    auto same = [&](int a, int b, int c) { return lab[t + a + kTileX * (b + kTileY * c)] == lv; };
+    if (!(lx < ex && ly < ey && lz < ez)) continue;
+    const int h = at(lx, ly, lz);
+    const L lv = hal[h];
+    if (lv == L(0)) continue;
+    auto same = [&](int a, int b, int c) { return hal[h + a + kHaloX * (b + kHaloY * c)] == lv; };
+    // pairs that leave the tile: the forward neighbours of a voxel on a face they can cross
+    const bool on_face = lx == 0 || lx == ex - 1 || ly == 0 || ly == ey - 1 || lz == ez - 1;
+    if (on_face) {
+      const long long p = base + (x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz));
+#pragma unroll
+      for (int k = 0; k < 26; ++k) {
+        const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
+        if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
+        if (planar && dz != 0) continue;
+        const bool cx = lx + dx < 0 || lx + dx >= kTileX, cy = ly + dy < 0 || ly + dy >= kTileY, cz = lz + dz >= kTileZ;
+        if (!(cx || cy || cz) || (cz && !zface)) continue;
+        if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
+        // The pair one step back along an axis the pair does not cross, with both ends still
+        // inside their tiles, joins the same two tile components (each end is tied to its
+        // step-back voxel inside its tile) and is itself listed or skipped by this rule further
+        // back; so a pair whose step-back ends both carry the label adds nothing.
+        int bx = 0, by = 0, bz = 0;
+        if (!cx && lx >= 1 && lx + dx >= 1) bx = 1;
+        else if (!cy && ly >= 1 && ly + dy >= 1) by = 1;
+        else if (!planar && !cz && lz >= 1 && lz + dz >= 1) bz = 1;
+        if ((bx | by | bz) && same(-bx, -by, -bz) && same(dx - bx, dy - by, dz - bz)) continue;
+        const int2 pair = make_int2(int(p), int(p + dx + (long long)d.sx * (dy + (long long)d.sy * dz)));
+        const int slot = atomicAdd(&nstaged, 1);
+        if (slot < kPairStage) staged[slot] = pair;
+        else if (*(volatile int *)list.count <= list.capacity) {  // more than the stage holds: to the list
+          const int g = atomicAdd(list.count, 1);                    // (no more adds once it overflowed)
+          if (g < list.capacity) list.pairs[g] = pair;
+        }
+      }
+    }
     // Inside a region of one label: when the +y and +z neighbours (in this tile) carry the label,
     // every other forward pair has one of them as a face intermediate and is skipped, so those
     // two unions are all (in a plane, the +y one).
@@ -140,30 +205,38 @@ __global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__
       if (dy == 0 && dz == 0) continue;  // the x run, linked at load
       if (planar && dz != 0) continue;
       const int nx = lx + dx, ny = ly + dy, nz = lz + dz;
-      if (nx < 0 || ny < 0 || nx >= ex || ny >= ey || nz >= ez) continue;  // other tiles: face_union
+      if (nx < 0 || ny < 0 || nx >= ex || ny >= ey || nz >= ez) continue;  // other tiles: listed above
       if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
       tile_unite(par, t, t + dx + kTileX * (dy + kTileY * dz));
     }
   }
   __syncthreads();
+  if (threadIdx.x == 0) {
+    const int n = min(nstaged, kPairStage);
+    first = n && *(volatile int *)list.count <= list.capacity ? atomicAdd(list.count, n) : list.capacity;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < min(nstaged, kPairStage); i += kTileThreads)
+    if (first + i < list.capacity) list.pairs[first + i] = staged[i];
   for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
     const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
     if (!(lx < ex && ly < ey && lz < ez)) continue;
     const int r = tile_find(par, t);
     const int rx = r % kTileX, ry = (r / kTileX) % kTileY, rz = r / (kTileX * kTileY);
     const long long g = (x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz));
-    parent[base + g] = lab[t] == L(0) ? -1 : int(base + (x0 + rx) + (long long)d.sx * ((y0 + ry) + (long long)d.sy * (z0 + rz)));
+    parent[base + g] = hal[at(lx, ly, lz)] == L(0) ? -1
+                                                   : int(base + (x0 + rx) + (long long)d.sx * ((y0 + ry) + (long long)d.sy * (z0 + rz)));
   }
 }
 
 // Pairs that cross a tile face: from every voxel on a face a forward neighbour can cross (both x
 // faces, both y faces — dy = -1 comes with dz = +1 — and the high z face), the forward neighbours
 // in another tile; for the voxels [i0, i1) of the volume.
+// (The fallback of an overflowing pair list, grid-stride over [i0, i1); and, with only_z, the
+// pairs across the +z faces of the tile layer whose next plane arrived after its tiles ran.)
 template <class L>
-__global__ void face_union(const L *labels, int *parent, Dims d, bool planar, long long base, long long i0,
-                           long long i1) {
-  const long long i = i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1) return;
+__device__ void face_union_at(const L *labels, int *parent, Dims d, bool planar, long long base, long long i,
+                              bool only_z) {
   int x, y, z;
   unravel((int)i, d, x, y, z);
   const int lx = x % kTileX, ly = y % kTileY, lz = z % kTileZ;
@@ -181,12 +254,9 @@ __global__ void face_union(const L *labels, int *parent, Dims d, bool planar, lo
     if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
     if (planar && dz != 0) continue;
     const bool cx = lx + dx < 0 || lx + dx >= kTileX, cy = ly + dy < 0 || ly + dy >= kTileY, cz = lz + dz >= kTileZ;
-    if (!(cx || cy || cz)) continue;
+    if (!(cx || cy || cz) || (only_z && !cz)) continue;
     if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
-    // The pair one step back along an axis the pair does not cross, with both ends still inside
-    // their tiles, joins the same two tile components (each end is tied to its step-back voxel
-    // inside its tile) and is itself united or skipped by this rule further back; so a pair whose
-    // step-back ends both carry the label adds nothing.
+    // the step-back rule of tile_union
     long long back = 0;
     if (!cx && lx >= 1 && lx + dx >= 1) back = 1;
     else if (!cy && ly >= 1 && ly + dy >= 1) back = d.sx;
@@ -197,17 +267,29 @@ __global__ void face_union(const L *labels, int *parent, Dims d, bool planar, lo
   }
 }
 
-__global__ void flatten(int *parent, long long n) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int p = parent[i];
-  if (p < 0) return;  // background
-  while (true) {
-    const int q = __ldcg(parent + p);
-    if (q == p) break;
-    p = q;
+template <class L>
+__global__ void face_union(const L *labels, int *parent, Dims d, bool planar, long long base, long long i0,
+                           long long i1, bool only_z) {
+  for (long long i = i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += (long long)gridDim.x * blockDim.x)
+    face_union_at(labels, parent, d, planar, base, i, only_z);
+}
+
+// Unites the listed pairs; when the list overflowed, scans every tile-face voxel of the volume
+// instead (face_union's rule reaches every pair the list would have held).
+template <class L>
+__global__ void union_pairs(const L *labels, int *parent, Dims d, bool planar, long long base, long long n,
+                            PairList list) {
+  const int offered = *list.count;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (offered > list.capacity) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+      face_union_at(labels, parent, d, planar, base, i, false);
+    return;
   }
-  parent[i] = p;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < offered; j += stride) {
+    const int2 pr = list.pairs[j];
+    unite(parent, pr.x, pr.y);
+  }
 }
 
 struct RootFlag {
@@ -226,12 +308,12 @@ __global__ void rank_bounds(const int *parent, const int *rank, const long long 
 
 // ids of one volume (local ids: rank - first + 1), and per root its local flat index and label.
 template <class L>
-__global__ void relabel(const L *labels, const int *parent, const int *rank, uint32_t *ids, long long *roots,
+__global__ void relabel(const L *labels, int *parent, const int *rank, uint32_t *ids, long long *roots,
                         long long *mapping, long long n, long long base, int first) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int r = parent[base + i];
-  if (r < 0) { ids[i] = 0; return; }
+  if (parent[base + i] < 0) { ids[i] = 0; return; }
+  const int r = find_root(parent, int(base + i));
   ids[i] = uint32_t(rank[r] - first + 1);
   if (r == int(base + i)) {
     roots[rank[r]] = i;
@@ -269,47 +351,71 @@ std::vector<ComponentsResult> connected_components(Context &ctx, const std::vect
   if (n <= 0) return out;
   cudaStream_t s = ctx.stream();
   Buffer<int> parent(ctx, n), rank(ctx, n);
-  // union within each volume, then one flatten and one scan over all of them
-  for (const auto &v : volumes) {
+  // per volume: a list of cross-tile pairs (an eighth of its voxels; beyond that, face_union)
+  long long forced = -1;  // test knob: a pair capacity small enough to overflow (the face_union fallback)
+  if (const char *e = std::getenv("BROOK_B200_TEST_PAIR_CAPACITY")) forced = std::atoll(e);
+  std::vector<long long> cap_begin(volumes.size() + 1, 0);
+  for (size_t i = 0; i < volumes.size(); ++i)
+    cap_begin[i + 1] = cap_begin[i] + (!volumes[i].d.n() ? 0 : forced >= 0 ? forced
+                                                                  : std::max<long long>(4096, volumes[i].d.n() / 8));
+  Buffer<int2> pairs(ctx, std::max<long long>(cap_begin.back(), 1));
+  Buffer<int> pair_count(ctx, volumes.size());
+  pair_count.zero();
+  auto list_of = [&](size_t i) {
+    return PairList{pairs.data() + cap_begin[i], pair_count.data() + i, int(cap_begin[i + 1] - cap_begin[i])};
+  };
+  // union within each volume's tiles (listing the cross-tile pairs), then the listed pairs, then
+  // one scan over all volumes
+  for (size_t vi = 0; vi < volumes.size(); ++vi) {
+    const auto &v = volumes[vi];
     if (!v.d.n()) continue;
     const Dims d{v.d.sx, v.d.sy, v.d.sz};
     const dim3 tiles((d.sx + kTileX - 1) / kTileX, (d.sy + kTileY - 1) / kTileY, (d.sz + kTileZ - 1) / kTileZ);
     if (tiles.y > 65535 || tiles.z > 65535) throw std::invalid_argument("volume too large for the tiled union");
+    const PairList list = list_of(vi);
     for_dtype(v.dtype, v.labels, [&](auto labels) {
       using L = std::remove_const_t<std::remove_pointer_t<decltype(labels)>>;
       if (!v.slabs) {
-        tile_union<L><<<tiles, kTileThreads, 0, s>>>(labels, parent.data(), d, planar, v.offset, 0); ++ctx.launches;
-        face_union<L><<<blocks_for(v.d.n()), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset, 0, v.d.n());
+        tile_union<L><<<tiles, kTileThreads, 0, s>>>(labels, parent.data(), d, planar, v.offset, 0, d.sz, list);
         ++ctx.launches;
         return;
       }
-      // labels still arriving by slabs: each slab's tiles once it is there; the cross-tile pairs
-      // of a slab once the next slab (its +z neighbours) is there too
+      // labels still arriving by slabs (ends are multiples of the tiles' depth): each slab's tiles
+      // once it is there, the +z face pairs of a slab's last tile layer once the next slab is too
       const long long plane = (long long)d.sx * d.sy;
-      int z_done = 0, z_pending = 0;  // planes united within tiles; first plane without face pairs
+      int z_done = 0;
       for (const auto &slab : *v.slabs) {
         BK_CUDA(cudaStreamWaitEvent(s, slab.second, 0));
         const int z_end = slab.first;
         const int tz0 = z_done / kTileZ, tz1 = (z_end + kTileZ - 1) / kTileZ;
         if (tz1 > tz0) {
           tile_union<L><<<dim3(tiles.x, tiles.y, unsigned(tz1 - tz0)), kTileThreads, 0, s>>>(labels, parent.data(), d,
-                                                                                             planar, v.offset, tz0);
+                                                                                             planar, v.offset, tz0,
+                                                                                             z_end, list);
+          ++ctx.launches;
+        }
+        if (z_done > 0 && !planar) {  // the previous slab's last plane, now that its +z plane is here
+          const long long i0 = (long long)(z_done - 1) * plane;
+          face_union<L><<<blocks_for(plane), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset, i0, i0 + plane,
+                                                          true);
           ++ctx.launches;
         }
         z_done = z_end;
-        // planes [z_pending, z_end - 1): their +z neighbours have arrived
-        const int z_ready = z_end == d.sz ? d.sz : z_end - 1;
-        if (z_ready > z_pending) {
-          const long long i0 = z_pending * plane, i1 = z_ready * plane;
-          face_union<L><<<blocks_for(i1 - i0), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset, i0, i1);
-          ++ctx.launches;
-          z_pending = z_ready;
-        }
       }
-      if (z_done != d.sz || z_pending != d.sz) throw std::logic_error("slabs do not cover the volume");
+      if (z_done != d.sz) throw std::logic_error("slabs do not cover the volume");
     });
   }
-  flatten<<<blocks_for(n), 256, 0, s>>>(parent.data(), n); ++ctx.launches;
+  for (size_t vi = 0; vi < volumes.size(); ++vi) {
+    const auto &v = volumes[vi];
+    if (!v.d.n()) continue;
+    const Dims d{v.d.sx, v.d.sy, v.d.sz};
+    for_dtype(v.dtype, v.labels, [&](auto labels) {
+      using L = std::remove_const_t<std::remove_pointer_t<decltype(labels)>>;
+      union_pairs<L><<<std::max(1, 8 * ctx.sm_count()), 256, 0, s>>>(labels, parent.data(), d, planar, v.offset,
+                                                                     v.d.n(), list_of(vi));
+      ++ctx.launches;
+    });
+  }
   BK_CUDA(cudaGetLastError());
   thrust::counting_iterator<long long> index(0);
   thrust::transform_iterator<RootFlag, thrust::counting_iterator<long long>, int> flags(index, RootFlag{parent.data()});

@@ -277,12 +277,17 @@ def _components_by_first_voxel(labels):
     return ids, [t[0] for t in comps], [t[2] for t in comps]
 
 
+@pytest.mark.parametrize("pair_capacity", [None, "0", "5"])
 @pytest.mark.parametrize("shape,blob", [((70, 45, 37), 3), ((33, 9, 17), 1), ((128, 16, 24), 6), ((5, 300, 4), 2), ((40, 24, 20), 0)])
-def test_connected_components_match_scipy(gpu, shape, blob):
+def test_connected_components_match_scipy(gpu, monkeypatch, shape, blob, pair_capacity):
     """Component ids, roots and labels of blobby random labels with noise, on sizes that are not
-    multiples of the 32x8x8 union tiles, against scipy's 26-connected labelling."""
+    multiples of the 32x8x8 union tiles, against scipy's 26-connected labelling; also with the
+    list of cross-tile pairs overflowing (capacity 0 or 5), where the face scan takes over."""
     from scipy import ndimage
     from brook_b200 import _native as n
+
+    if pair_capacity is not None:
+        monkeypatch.setenv("BROOK_B200_TEST_PAIR_CAPACITY", pair_capacity)
 
     rng = np.random.default_rng(sum(shape) + blob)
     field = ndimage.gaussian_filter(rng.random((5,) + shape), sigma=(0, blob, blob, blob))
