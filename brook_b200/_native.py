@@ -33,7 +33,8 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_skeletonize_batch", "brook_skeletons_get_view", "brook_skeletons_destroy", "brook_context_stats",
            "brook_edt_device_noalloc", "brook_skeletons_get_device_view", "brook_skeletons_get_array",
            "brook_array_upload", "brook_array_to_dlpack", "brook_array_to_dlpack_versioned", "brook_components_labels",
-           "brook_skeletonize_batch_targets", "brook_context_wait_stream"]
+           "brook_skeletonize_batch_targets", "brook_context_wait_stream", "brook_autotune",
+           "brook_context_set_tuning"]
 
 
 class Volume(ctypes.Structure):
@@ -72,6 +73,11 @@ class SkeletonsDeviceView(ctypes.Structure):
                 ("labels", ctypes.POINTER(ctypes.c_int64)), ("vertex_offsets", ctypes.POINTER(ctypes.c_int64)),
                 ("edge_offsets", ctypes.POINTER(ctypes.c_int64)), ("vertices", Volume), ("edges", Volume),
                 ("radii", Volume), ("anisotropy", ctypes.c_float * 3)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("trace_cluster_ctas", ctypes.c_int32), ("trace_cluster_voxels", ctypes.c_int64),
+                ("prepare_cluster_voxels", ctypes.c_int64), ("lone_first_percent", ctypes.c_int32)]
 
 
 class SampleTargets(ctypes.Structure):
@@ -151,6 +157,10 @@ def _open():
         "brook_skeletonize_batch_targets": (ctypes.c_int, [vp, ctypes.POINTER(Volume), sz, ctypes.POINTER(Options),
                                                            ctypes.POINTER(SampleTargets), ctypes.POINTER(vp)]),
         "brook_context_wait_stream": (ctypes.c_int, [vp, ctypes.c_int64]),
+        "brook_autotune": (ctypes.c_int, [vp, ctypes.POINTER(Volume), sz, ctypes.POINTER(Options),
+                                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Tuning),
+                                          ctypes.POINTER(ctypes.c_double)]),
+        "brook_context_set_tuning": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(Tuning)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -177,6 +187,9 @@ def context(device=0):
             handle = ctypes.c_void_p()
             check(load().brook_context_create(int(device), ctypes.byref(handle)))
             ctx = _contexts[key] = handle
+            from . import tuning
+
+            tuning.install_saved(handle, int(device))
     return ctx
 
 

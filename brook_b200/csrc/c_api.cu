@@ -1,6 +1,7 @@
 // The C ABI (include/brook_b200.h): argument checks, input staging into Fortran-ordered device
 // buffers, exception -> brook_status mapping with thread-local error text, result handles.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -10,6 +11,7 @@
 
 #include "../../include/brook_b200.h"
 #include "../../include/brook_b200_dlpack.h"
+#include "engine.hpp"
 #include "pipeline.hpp"
 
 #ifndef BROOK_B200_VERSION
@@ -740,6 +742,105 @@ brook_status brook_edt_device_noalloc(const brook_volume *labels, const float an
     }
     bk::edt_fixed_scratch(static_cast<const uint32_t *>(v.data), d, anisotropy, black_border != 0, out,
                           static_cast<cudaStream_t>(stream));
+  });
+}
+
+namespace {
+bk::Tuning tuning_of(const brook_tuning &t) {
+  bk::Tuning out;
+  out.trace_cluster_ctas = t.trace_cluster_ctas;
+  out.trace_cluster_voxels = t.trace_cluster_voxels;
+  out.prepare_cluster_voxels = t.prepare_cluster_voxels;
+  out.lone_first_percent = t.lone_first_percent;
+  return out;
+}
+brook_tuning tuning_to_c(const bk::Tuning &t) {
+  brook_tuning out{};
+  out.trace_cluster_ctas = t.trace_cluster_ctas;
+  out.trace_cluster_voxels = t.trace_cluster_voxels;
+  out.prepare_cluster_voxels = t.prepare_cluster_voxels;
+  out.lone_first_percent = t.lone_first_percent;
+  return out;
+}
+}  // namespace
+
+brook_status brook_autotune(brook_context *ctx, const brook_volume *volumes, size_t count,
+                            const brook_skeletonize_options *p, uint64_t *workload_class, brook_tuning *best,
+                            double *best_ms) {
+  return protect([&] {
+    require(ctx && (volumes || !count) && p);
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    bk::Context &c = ctx->value;
+    const bk::Options options = options_of(p);
+    std::vector<Staged> staged;
+    std::vector<bk::DeviceVolume> vols;
+    for (size_t i = 0; i < count; ++i) {
+      staged.push_back(stage(c, volumes[i]));
+      vols.push_back(staged.back().volume);
+    }
+    // one candidate: the engine's device time (prepare, target orders, trace), best of two calls
+    auto measure = [&](const bk::Tuning &t) {
+      double ms = INFINITY;
+      for (int rep = 0; rep < 2; ++rep) {
+        c.forced = &t;
+        try {
+          bk::skeletonize(c, vols, options);
+        } catch (...) {
+          c.forced = nullptr;
+          throw;
+        }
+        c.forced = nullptr;
+        c.synchronize();
+        ms = std::min(ms, c.stats["ms_prepare"] + c.stats["ms_order"] + c.stats["ms_trace"]);
+      }
+      return ms;
+    };
+    bk::Tuning chosen;
+    double chosen_ms = measure(chosen);  // the built-in rule
+    const unsigned long long cls = c.last_class;
+    const double foreground = c.stats["foreground"];
+    auto consider = [&](bk::Tuning t) {
+      const double ms = measure(t);
+      if (ms < chosen_ms) { chosen_ms = ms; chosen = t; }
+    };
+    // coordinate search: cluster width, the trace's cluster threshold, the lone-first share, the
+    // preparation's cluster threshold
+    for (int ctas : {bk::kClusterCtas, bk::kWideClusterCtas}) {
+      bk::Tuning t = chosen;
+      t.trace_cluster_ctas = ctas;
+      consider(t);
+    }
+    const long long rule = bk::trace_cluster_voxels((long long)foreground);
+    for (double f : {0.5, 2.0, 4.0}) {
+      bk::Tuning t = chosen;
+      t.trace_cluster_voxels = std::max(1LL, (long long)(double(rule) * f));
+      consider(t);
+    }
+    for (int percent : {0, 25}) {
+      bk::Tuning t = chosen;
+      t.lone_first_percent = percent;
+      consider(t);
+    }
+    for (long long v : {4096LL, 32768LL}) {
+      bk::Tuning t = chosen;
+      t.prepare_cluster_voxels = v;
+      consider(t);
+    }
+    c.tuning[cls] = chosen;
+    c.stats["autotune_ms"] = chosen_ms;
+    if (workload_class) *workload_class = cls;
+    if (best) *best = tuning_to_c(chosen);
+    if (best_ms) *best_ms = chosen_ms;
+  });
+}
+
+brook_status brook_context_set_tuning(brook_context *ctx, uint64_t workload_class, const brook_tuning *t) {
+  return protect([&] {
+    require(ctx);
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    if (t) ctx->value.tuning[workload_class] = tuning_of(*t);
+    else ctx->value.tuning.erase(workload_class);
   });
 }
 

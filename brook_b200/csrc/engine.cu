@@ -49,6 +49,11 @@ struct Shared {
   // this CTA's copy of the object's neighbour offsets and step weights
   int off[26];
   float w[26];
+  // trace: the object's root, its soma radius (< 0: none) and the loop's step (0 the soma's ball,
+  // 1 the parents' field, 2 paths)
+  double soma_radius;
+  int root, step;
+  float rscale, rconst;  // invalidation: reach = rscale * DBF[source] + rconst
 };
 
 __device__ __forceinline__ float inf() { return __uint_as_float(BK_INF_BITS); }
@@ -417,7 +422,7 @@ template <int C>
 __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *L, int t, int *A, int *B, int *FA,
                                        int *FB, int *touched, unsigned long long *wide) {
   using G = Group<C>;
-  const bool rails = a.fix_branching != 0;  // without rails: a full SSSP from t (the parents' field)
+  // without fix_branching there are no rails: a full SSSP from t (the parents' field)
   if (threadIdx.x == 0) {
     sh.rb = BK_UNCLAIMED;
     sh.minfar = kMinFarNone;
@@ -429,7 +434,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
     L->n_far = 0; L->n_keep = 0;
     a.dist[t] = 0.0f;
     const float ft = __ldcg(a.pdrf + t);
-    if (rails && ft == 0.0f) sh.rb = static_cast<unsigned long long>(unsigned(t));
+    if (a.fix_branching && ft == 0.0f) sh.rb = static_cast<unsigned long long>(unsigned(t));
     else {
       A[0] = t;
       L->cnt[0] = 1;
@@ -469,14 +474,15 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
         const float du = __ldcg(a.dist + u);
         const unsigned long long rb = vload(&sh.rb);
         const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
-        const bool expand = (fu != 0.0f || !rails) && du <= Tb;
+        const bool expand = (fu != 0.0f || !a.fix_branching) && du <= Tb;
         return expand ? (static_cast<unsigned long long>(__float_as_uint(du)) << 32) | a.mask[u] : 0ull;
       };
       // step B, after the improvement of v to cand (from old)
       auto improved = [&](int v, float cand, float fv, float old) {
         {
           if (old == inf()) touched[atomicAdd(&L->n_touch, 1)] = v;
-          if (rails && fv == 0.0f) atomicMin(&sh.rb, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | unsigned(v));
+          if (a.fix_branching && fv == 0.0f)
+            atomicMin(&sh.rb, (static_cast<unsigned long long>(__float_as_uint(cand)) << 32) | unsigned(v));
           const unsigned long long rb = vload(&sh.rb);
           const float Tb = rb != BK_UNCLAIMED ? fminf(T, __uint_as_float(unsigned(rb >> 32))) : T;
           if (cand <= Tb) {
@@ -725,9 +731,8 @@ __device__ __forceinline__ int band_of(unsigned mbits, float delta, int kmin) {
 // of its claimed neighbours, the smallest names the next band, those inside it are claimed.
 // Claimed voxels die. Returns false when a loop bound is hit.
 template <int C>
-__device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int *path, int npath, float rscale,
-                           float rconst, int *A, int *B, int *FA, int *FB, int *touched, unsigned long long *wide,
-                           unsigned long long *side_u,
+__device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int *path, int npath, int *A, int *B,
+                           int *FA, int *FB, int *touched, unsigned long long *wide, unsigned long long *side_u,
                            unsigned long long *side_s) {
   using G = Group<C>;
   if (G::first()) { L->cnt[0] = 0; L->cnt[1] = 0; L->cnt[2] = 0; L->n_far = 0; L->n_keep = 0; L->n_touch = 0; }
@@ -796,7 +801,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
           su[q] = u;
           skey[q] = k;
           smask[q] = a.mask[u];
-          sreach[q] = reach(a, int(unsigned(k)), rscale, rconst);
+          sreach[q] = reach(a, int(unsigned(k)), sh.rscale, sh.rconst);
           int x, y, z;
           unravel3(u - sh.a0, sh.sx, sh.sy, x, y, z);
           spu[q] = pack3(x, y, z);
@@ -836,7 +841,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
           int ux, uy, uz, qx, qy, qz;
           unpack3(__ldcg(side_u + i), ux, uy, uz);
           unpack3(__ldcg(side_s + i), qx, qy, qz);
-          offer(u, ku, k, ux, uy, uz, qx, qy, qz, reach(a, int(unsigned(ku)), rscale, rconst));
+          offer(u, ku, k, ux, uy, uz, qx, qy, qz, reach(a, int(unsigned(ku)), sh.rscale, sh.rconst));
         }
       }
       G::sync();
@@ -853,7 +858,7 @@ __device__ bool invalidate(const EngineArgs &a, Shared &sh, Shared *L, const int
       int qx, qy, qz;
       unravel3(s - sh.a0, sh.sx, sh.sy, qx, qy, qz);
       const float d = distance_to(a, x, y, z, qx, qy, qz);
-      if (d >= reach(a, s, rscale, rconst)) return ~0ull;
+      if (d >= reach(a, s, sh.rscale, sh.rconst)) return ~0ull;
       unsigned mb = __float_as_uint(d);
       const unsigned mu = unsigned(ku >> 32);
       if (mb < mu) mb = mu;
@@ -994,72 +999,65 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
     auto lap = [&](int phase) {
       if (G::first()) { const unsigned long long t = now_ns(); s_prof[2 + phase] += t - s_prof[1]; s_prof[1] = t; }
     };
-    const bool rails = a.fix_branching != 0;
-    const int root = a.root[o];
-    const double soma_radius = a.soma_radius[o];
-    if (soma_radius >= 0.0) {
-      // the soma's ball, from the root with the soma's reach, before any path (trace.cu:199)
-      if (G::first()) store[0] = root;
-      G::sync();
-      if (!invalidate<C>(a, sh, L, store, 1, a.soma_scale, a.soma_constant, L0, L1, L2, L3, L4, wide, side_u, side_s))
-        status = kBudget;
-      if (G::first()) s_work[2] += vload(&L->n_touch);
-      G::sync();
+    // The loop's steps, each with one flood: first the soma's ball (a soma: an invalidation from the
+    // root with the soma's reach, trace.cu:199), then the parents' field (without fix_branching:
+    // the object's SSSP from the root, kept until the object is done), then the paths. Every flood
+    // function has this one call site, which keeps the kernel's registers for the paths' loop.
+    if (threadIdx.x == 0) {
+      sh.root = a.root[o];
+      sh.soma_radius = a.soma_radius[o];
+      sh.step = sh.soma_radius >= 0.0 ? 0 : (a.fix_branching ? 2 : 1);
     }
-    if (!rails && maxp > 0 && status == kOk) {
-      // the parents' field: the object's SSSP from the root, kept until the object is done (its
-      // queue flags are cleared now, its distances at the end)
-      railroad<C>(a, sh, L, root, L0, L1, L2, L3, L4, wide);
-      if (vload(&L->status) != kOk) status = vload(&L->status);
-      const int nt = vload(&L->n_touch);
-      for (int i = G::tid(); i < nt; i += G::threads()) atomicAnd(a.flags + __ldcg(L4 + i), ~(kNearQueued | kFarQueued));
-      if (G::first()) { s_work[0] += nt; s_work[1] += nt; }
-      G::sync();
-      lap(1);
-    }
-    while (status == kOk && paths < maxp) {
-      // the next target: manual targets first, then the first alive voxel of the order, then the
-      // targets after (trace.cu:209-212)
-      int t = -1;
-      if (paths < mcount) {
-        t = manual[paths];
-        if (t < 0) t = a.target[o];  // the object's own target (the DAF argmax)
-      } else {
-        for (;;) {
-          if (threadIdx.x == 0) sh.pos = INT32_MAX;
-          G::sync();
-          const int pos = cursor + G::tid();
-          if (pos < sh.count && __ldcg(a.alive + order[pos])) atomicMin(&sh.pos, unsigned(pos));
-          G::sync();
-          const int found = int(G::min_over(&sh.pos));
-          G::sync();
-          if (found != INT32_MAX) { cursor = found; t = order[found]; break; }
-          cursor += G::threads();
-          if (cursor >= sh.count) { cursor = sh.count; break; }
+    __syncthreads();
+    while (status == kOk) {
+      const int step = sh.step;  // 0: the soma's ball, 1: the parents' field, 2: paths
+      int t = -1, len = 1;
+      if (step == 2) {
+        if (paths >= maxp) break;
+        // the next target: manual targets first, then the first alive voxel of the order, then the
+        // targets after (trace.cu:209-212)
+        if (paths < mcount) {
+          t = manual[paths];
+          if (t < 0) t = a.target[o];  // the object's own target (the DAF argmax)
+        } else {
+          for (;;) {
+            if (threadIdx.x == 0) sh.pos = INT32_MAX;
+            G::sync();
+            const int pos = cursor + G::tid();
+            if (pos < sh.count && __ldcg(a.alive + order[pos])) atomicMin(&sh.pos, unsigned(pos));
+            G::sync();
+            const int found = int(G::min_over(&sh.pos));
+            G::sync();
+            if (found != INT32_MAX) { cursor = found; t = order[found]; break; }
+            cursor += G::threads();
+            if (cursor >= sh.count) { cursor = sh.count; break; }
+          }
+          if (t < 0 && after_used < acount) t = after[after_used++];
+          if (t < 0) break;
         }
-        if (t < 0 && after_used < acount) t = after[after_used++];
-        if (t < 0) break;
+        lap(0);
       }
-      lap(0);
-      if (!rails) {  // the walk to the root through the parents' field
-        if (G::rank() == 0 && threadIdx.x < 32) {
-          const int len = parent_walk(a, sh, t, root, store + used, store_cap - used);
-          if (threadIdx.x == 0) L->len = len;
-        }
+      if (step == 0) {
+        if (G::first()) store[used] = sh.root;  // the ball's one source (the slot is reused)
         G::sync();
-        lap(2);
-      } else {
-        const unsigned long long rb = railroad<C>(a, sh, L, t, L0, L1, L2, L3, L4, wide);
+      } else if (step == 1 || a.fix_branching) {
+        const unsigned long long rb = railroad<C>(a, sh, L, step == 1 ? sh.root : t, L0, L1, L2, L3, L4, wide);
         lap(1);
         if (vload(&L->status) != kOk) { status = vload(&L->status); break; }
+        const int nt = vload(&L->n_touch);
+        if (step == 1) {  // the parents' field stays; its queue flags are cleared now
+          for (int i = G::tid(); i < nt; i += G::threads()) atomicAnd(a.flags + __ldcg(L4 + i), ~(kNearQueued | kFarQueued));
+          if (G::first()) { s_work[0] += nt; s_work[1] += nt; sh.step = 2; }
+          G::sync();
+          continue;
+        }
         if (rb == BK_UNCLAIMED) { status = kNoRail; break; }
         // walk (one warp of the first CTA), then reset the flood's state over the voxels it touched
         if (G::rank() == 0 && threadIdx.x < 32) {
-          const int len = backtrace(a, sh, rb, t, store + used, store_cap - used);
-          if (threadIdx.x == 0) L->len = len;
+          const int n = backtrace(a, sh, rb, t, store + used, store_cap - used);
+          if (threadIdx.x == 0) L->len = n;
         }
         G::sync();
-        const int nt = vload(&L->n_touch);
         const float D = __uint_as_float(unsigned(rb >> 32));
         unsigned settled = 0;
         for (int i = G::tid(); i < nt; i += G::threads()) {
@@ -1073,25 +1071,47 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
         if (G::first()) s_work[1] += nt;
         G::sync();
         lap(2);
-      }
-      int len = vload(&L->len);
-      if (soma_radius >= 0.0 && len > 0) {
+      } else {  // the walk to the root through the parents' field
         if (G::rank() == 0 && threadIdx.x < 32) {
-          const int n = soma_trim(a, sh, store + used, len, root, soma_radius, rails, store_cap - used);
+          const int n = parent_walk(a, sh, t, sh.root, store + used, store_cap - used);
           if (threadIdx.x == 0) L->len = n;
         }
         G::sync();
-        len = vload(&L->len);
+        lap(2);
       }
-      if (len < 0) { status = kStoreFull; break; }
-      if (paths >= rec_cap) { status = kRecordsFull; break; }
-      if (!invalidate<C>(a, sh, L, store + used, len, a.scale, a.constant, L0, L1, L2, L3, L4, wide, side_u, side_s)) {
+      if (step == 2) {
+        len = vload(&L->len);
+        if (sh.soma_radius >= 0.0 && len > 0) {
+          if (G::rank() == 0 && threadIdx.x < 32) {
+            const int n = soma_trim(a, sh, store + used, len, sh.root, sh.soma_radius, a.fix_branching != 0,
+                                    store_cap - used);
+            if (threadIdx.x == 0) L->len = n;
+          }
+          G::sync();
+          len = vload(&L->len);
+        }
+        if (len < 0) { status = kStoreFull; break; }
+        if (paths >= rec_cap) { status = kRecordsFull; break; }
+      }
+      const bool ball = step == 0;
+      if (threadIdx.x == 0) {  // the reach of the invalidation's sources (the soma's for its ball)
+        sh.rscale = ball ? a.soma_scale : a.scale;
+        sh.rconst = ball ? a.soma_constant : a.constant;
+      }
+      __syncthreads();
+      if (!invalidate<C>(a, sh, L, store + used, len, L0, L1, L2, L3, L4, wide, side_u, side_s)) {
         status = kBudget;
         break;
       }
+      if (ball) {
+        if (G::first()) { s_work[2] += vload(&L->n_touch); sh.step = a.fix_branching ? 2 : 1; }
+        else if (threadIdx.x == 0) sh.step = a.fix_branching ? 2 : 1;
+        G::sync();
+        continue;
+      }
       if (G::first()) { s_work[2] += vload(&L->n_touch); s_work[3] += 1; }
       lap(3);
-      if (rails)
+      if (a.fix_branching)
         for (int i = G::tid(); i < len; i += G::threads()) a.pdrf[__ldcg(store + used + i)] = 0.0f;
       else
         for (int i = G::tid(); i < len; i += G::threads()) atomicOr(a.flags + __ldcg(store + used + i), kOnPath);
@@ -1100,7 +1120,7 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
       used += len;
       ++paths;
     }
-    if (!rails) {  // the parents' field and the path marks go back to rest
+    if (!a.fix_branching) {  // the parents' field and the path marks go back to rest
       for (int i = G::tid(); i < sh.count; i += G::threads()) a.dist[a.vox[sh.begin + i]] = inf();
       for (long long i = G::tid(); i < used; i += G::threads()) atomicAnd(a.flags + __ldcg(store + i), ~kOnPath);
       G::sync();
@@ -1208,6 +1228,16 @@ int cluster_ctas(long long largest, long long foreground) {
 void launch_prepare(const EngineArgs &a, int nbig, int ctas, cudaStream_t stream) {
   if (ctas == kWideClusterCtas) launch((const void *)prepare_kernel<kWideClusterCtas>, ctas, a, nbig, stream);
   else launch((const void *)prepare_kernel<kClusterCtas>, kClusterCtas, a, nbig, stream);
+}
+
+void prepare_engine_launches(int ctas, cudaStream_t stream) {
+  if (ctas == kWideClusterCtas) {
+    resident_clusters((const void *)prepare_kernel<kWideClusterCtas>, ctas, stream);
+    resident_clusters((const void *)trace_kernel<kWideClusterCtas>, ctas, stream);
+  } else {
+    resident_clusters((const void *)prepare_kernel<kClusterCtas>, kClusterCtas, stream);
+    resident_clusters((const void *)trace_kernel<kClusterCtas>, kClusterCtas, stream);
+  }
 }
 
 void launch_trace(const EngineArgs &a, int nbig, int ctas, int lone_percent, cudaStream_t stream) {

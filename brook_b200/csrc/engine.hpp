@@ -124,5 +124,8 @@ void launch_prepare(const EngineArgs &a, int nbig, int cluster_ctas, cudaStream_
 // lone_percent: the share of clusters (percent) whose CTAs take small objects first.
 void launch_trace(const EngineArgs &a, int nbig, int cluster_ctas, int lone_percent, cudaStream_t stream);
 constexpr int kLoneFirstPercent = 10;
+// The device queries the launches above make (resident clusters per kernel), done ahead so that
+// a stream capture of the launches holds launches only.
+void prepare_engine_launches(int cluster_ctas, cudaStream_t stream);
 
 }  // namespace bk

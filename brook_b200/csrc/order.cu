@@ -170,42 +170,68 @@ Buffer<int> arena_object_voxels(Context &ctx, const uint32_t *ids, long long n, 
   return vox;
 }
 
-Buffer<int> target_orders(Context &ctx, const int *vox, const float *daf, long long total, const int *begin, int nobj,
-                          long long largest, bool wide) {
-  cudaStream_t s = ctx.stream();
-  Buffer<int> order(ctx, total > 0 ? total : 1);
-  if (total == 0) return order;
+OrderPlan plan_target_orders(Context &ctx, long long total, int nobj, long long largest, bool wide) {
+  OrderPlan p;
+  p.total = total;
+  p.nobj = nobj;
+  p.order = Buffer<int>(ctx, total > 0 ? total : 1);
+  if (total == 0) return p;
   auto bits_for = [](long long values) {  // bits that hold 0 .. values-1
     int b = 0;
     while ((1LL << b) < values) ++b;
     return b;
   };
-  const int lbits = bits_for(largest), end_bit = lbits + 31 + bits_for(nobj);
-  size_t temp = 0;
-  if (!wide && end_bit <= 64) {
-    Buffer<unsigned long long> keys(ctx, total), sorted(ctx, total);
-    order_keys64<<<blocks_for(total), 256, 0, s>>>(vox, daf, begin, nobj, lbits, keys.data(), (int)total);
+  p.lbits = bits_for(largest);
+  p.end_bit = p.lbits + 31 + bits_for(nobj);
+  p.wide = wide || p.end_bit > 64;
+  const size_t key_bytes = p.wide ? sizeof(WideKey) : sizeof(unsigned long long);
+  p.keys = Buffer<unsigned char>(ctx, total * key_bytes);
+  p.sorted = Buffer<unsigned char>(ctx, total * key_bytes);
+  // the scratch size is a host computation (no stream work)
+  if (!p.wide)
+    BK_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, p.temp, reinterpret_cast<unsigned long long *>(p.keys.data()),
+                                           reinterpret_cast<unsigned long long *>(p.sorted.data()), (int)total, 0,
+                                           p.end_bit, ctx.stream()));
+  else
+    BK_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, p.temp, reinterpret_cast<WideKey *>(p.keys.data()),
+                                           reinterpret_cast<WideKey *>(p.sorted.data()), (int)total, WideKeyParts{}, 0,
+                                           p.end_bit, ctx.stream()));
+  p.scratch = Buffer<unsigned char>(ctx, p.temp > 0 ? p.temp : 1);
+  return p;
+}
+
+void run_target_orders(Context &ctx, OrderPlan &p, const int *vox, const float *daf, const int *begin) {
+  if (p.total == 0) return;
+  cudaStream_t s = ctx.stream();
+  const long long total = p.total;
+  size_t temp = p.temp;
+  if (!p.wide) {
+    auto *keys = reinterpret_cast<unsigned long long *>(p.keys.data());
+    auto *sorted = reinterpret_cast<unsigned long long *>(p.sorted.data());
+    order_keys64<<<blocks_for(total), 256, 0, s>>>(vox, daf, begin, p.nobj, p.lbits, keys, (int)total);
     ++ctx.launches;
     BK_CUDA(cudaGetLastError());
-    BK_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, temp, keys.data(), sorted.data(), (int)total, 0, end_bit, s));
-    Buffer<unsigned char> scratch(ctx, temp);
-    BK_CUDA(cub::DeviceRadixSort::SortKeys(scratch.data(), temp, keys.data(), sorted.data(), (int)total, 0, end_bit, s));
-    unpack_order64<<<blocks_for(total), 256, 0, s>>>(sorted.data(), vox, begin, lbits, order.data(), (int)total);
+    BK_CUDA(cub::DeviceRadixSort::SortKeys(p.scratch.data(), temp, keys, sorted, (int)total, 0, p.end_bit, s));
+    unpack_order64<<<blocks_for(total), 256, 0, s>>>(sorted, vox, begin, p.lbits, p.order.data(), (int)total);
   } else {
-    Buffer<WideKey> keys(ctx, total), sorted(ctx, total);
-    order_keys96<<<blocks_for(total), 256, 0, s>>>(vox, daf, begin, nobj, lbits, keys.data(), (int)total);
+    auto *keys = reinterpret_cast<WideKey *>(p.keys.data());
+    auto *sorted = reinterpret_cast<WideKey *>(p.sorted.data());
+    order_keys96<<<blocks_for(total), 256, 0, s>>>(vox, daf, begin, p.nobj, p.lbits, keys, (int)total);
     ++ctx.launches;
     BK_CUDA(cudaGetLastError());
-    BK_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, temp, keys.data(), sorted.data(), (int)total, WideKeyParts{}, 0,
-                                           end_bit, s));
-    Buffer<unsigned char> scratch(ctx, temp);
-    BK_CUDA(cub::DeviceRadixSort::SortKeys(scratch.data(), temp, keys.data(), sorted.data(), (int)total, WideKeyParts{},
-                                           0, end_bit, s));
-    unpack_order96<<<blocks_for(total), 256, 0, s>>>(sorted.data(), vox, begin, lbits, order.data(), (int)total);
+    BK_CUDA(cub::DeviceRadixSort::SortKeys(p.scratch.data(), temp, keys, sorted, (int)total, WideKeyParts{}, 0,
+                                           p.end_bit, s));
+    unpack_order96<<<blocks_for(total), 256, 0, s>>>(sorted, vox, begin, p.lbits, p.order.data(), (int)total);
   }
   ++ctx.launches;
   BK_CUDA(cudaGetLastError());
-  return order;
+}
+
+Buffer<int> target_orders(Context &ctx, const int *vox, const float *daf, long long total, const int *begin, int nobj,
+                          long long largest, bool wide) {
+  OrderPlan p = plan_target_orders(ctx, total, nobj, largest, wide);
+  run_target_orders(ctx, p, vox, daf, begin);
+  return std::move(p.order);
 }
 
 }  // namespace bk

@@ -158,6 +158,13 @@ Buffer<unsigned char> filter_volume(Context &ctx, const DeviceVolume &v, const s
   }
 }
 
+// The workload class the tuned launch choices are kept by: the bit lengths of the foreground
+// voxels, of the largest object's voxels and of the object count.
+unsigned long long workload_class(long long foreground, long long largest, int objects) {
+  auto bits = [](long long v) { int b = 0; while (v > 0) { ++b; v >>= 1; } return (unsigned long long)b; };
+  return (bits(foreground) << 16) | (bits(largest) << 8) | bits(objects);
+}
+
 struct VolumeState {
   VolumeDims d;
   long long offset = 0;
@@ -535,14 +542,23 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   std::vector<int> schedule(nobj);
   std::iota(schedule.begin(), schedule.end(), 0);
   std::stable_sort(schedule.begin(), schedule.end(), [&](int a, int b) { return obj_count[a] > obj_count[b]; });
+  // the engine's launch choices: a test's environment knob, else the autotuner's (or the saved)
+  // choice for this workload class, else the built-in rule
+  const long long largest = nobj ? obj_count[schedule[0]] : 0;
+  ctx.last_class = workload_class(F, largest, nobj);
+  Tuning tune;
+  if (ctx.forced) tune = *ctx.forced;
+  else if (auto it = ctx.tuning.find(ctx.last_class); it != ctx.tuning.end()) tune = it->second;
   auto leading = [&](const char *knob, long long voxels) {  // knob: tuning override from the environment
     if (const char *e = std::getenv(knob)) voxels = std::atoll(e);
     int n = 0;
     while (n < nobj && obj_count[schedule[n]] >= voxels) ++n;
     return n;
   };
-  const int nbig_prepare = leading("BROOK_B200_PREPARE_CLUSTER_VOXELS", kPrepareClusterVoxels);
-  const int nbig_trace = leading("BROOK_B200_TRACE_CLUSTER_VOXELS", trace_cluster_voxels(F));
+  const int nbig_prepare = leading("BROOK_B200_PREPARE_CLUSTER_VOXELS",
+                                   tune.prepare_cluster_voxels > 0 ? tune.prepare_cluster_voxels : kPrepareClusterVoxels);
+  const int nbig_trace = leading("BROOK_B200_TRACE_CLUSTER_VOXELS",
+                                 tune.trace_cluster_voxels > 0 ? tune.trace_cluster_voxels : trace_cluster_voxels(F));
   auto d_arena_offset = to_device(ctx, arena_offset), d_arena_dims = to_device(ctx, arena_dims);
   auto d_obj_arena = to_device(ctx, obj_arena), d_obj_begin = to_device(ctx, obj_begin), d_obj_count = to_device(ctx, obj_count);
   auto d_schedule = to_device(ctx, schedule), d_border_root = to_device(ctx, border_root);
@@ -596,29 +612,61 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   if (const char *e = std::getenv("BROOK_B200_TEST_ROUND_LIMIT")) a.round_limit = std::atoll(e);  // test knob
 
   clock.mark("state");
-  const int ctas = cluster_ctas(nobj ? obj_count[schedule[0]] : 0, F);
-  launch_prepare(a, nbig_prepare, ctas, s);
-  ++ctx.launches;
-  clock.mark("prepare");
-  if (const char *fields = std::getenv("BROOK_B200_DUMP_FIELDS")) {
-    // diagnostics: the prepared DAF and PDRF (root rails included) as raw float32 files
-    const auto hd = daf.download(), hp = pdrf.download(), hb = dbf.download();
-    for (auto item : {std::make_pair("daf", &hd), std::make_pair("pdrf", &hp), std::make_pair("dbf", &hb)}) {
-      FILE *f = std::fopen((std::string(fields) + "." + item.first).c_str(), "wb");
-      if (f) { std::fwrite(item.second->data(), sizeof(float), size_t(N), f); std::fclose(f); }  // the volumes' part
-    }
-  }
-  const bool wide_order = std::getenv("BROOK_B200_WIDE_ORDER_KEY") != nullptr;  // test knob: the 96-bit key path
-  Buffer<int> order = target_orders(ctx, vox.data(), daf.data(), F, d_obj_begin.data(), nobj,
-                                    nobj ? obj_count[schedule[0]] : 0, wide_order);
-  a.order = order.data();
-  BK_CUDA(cudaMemsetAsync(queue.data(), 0, 2 * sizeof(int), s));
-  clock.mark("order");
-  int lone_percent = kLoneFirstPercent;
+  const int ctas = tune.trace_cluster_ctas == kWideClusterCtas || tune.trace_cluster_ctas == kClusterCtas
+                       ? tune.trace_cluster_ctas
+                       : cluster_ctas(largest, F);
+  int lone_percent = tune.lone_first_percent >= 0 ? tune.lone_first_percent : kLoneFirstPercent;
   if (const char *e = std::getenv("BROOK_B200_LONE_FIRST_PERCENT")) lone_percent = std::atoi(e);  // tuning knob
-  launch_trace(a, nbig_trace, ctas, std::max(0, std::min(100, lone_percent)), s);
-  ++ctx.launches;
-  clock.mark("trace");
+  lone_percent = std::max(0, std::min(100, lone_percent));
+  const char *fields = std::getenv("BROOK_B200_DUMP_FIELDS");
+  const bool wide_order = std::getenv("BROOK_B200_WIDE_ORDER_KEY") != nullptr;  // test knob: the 96-bit key path
+  OrderPlan orders = plan_target_orders(ctx, F, nobj, largest, wide_order);
+  a.order = orders.order.data();
+  // the engine's launches, prepare -> target orders -> trace, as one CUDA graph (every buffer is
+  // made above; the graph holds kernels, a memset and the stage marks): one submission per call,
+  // and the context's executable graph is updated in place while the topology holds
+  const char *graph_knob = std::getenv("BROOK_B200_GRAPH");
+  const bool as_graph = !fields && !(graph_knob && std::string(graph_knob) == "0");
+  auto engine = [&] {
+    launch_prepare(a, nbig_prepare, ctas, s);
+    ++ctx.launches;
+    clock.mark("prepare");
+    if (fields) {
+      // diagnostics: the prepared DAF and PDRF (root rails included) as raw float32 files
+      const auto hd = daf.download(), hp = pdrf.download(), hb = dbf.download();
+      for (auto item : {std::make_pair("daf", &hd), std::make_pair("pdrf", &hp), std::make_pair("dbf", &hb)}) {
+        FILE *f = std::fopen((std::string(fields) + "." + item.first).c_str(), "wb");
+        if (f) { std::fwrite(item.second->data(), sizeof(float), size_t(N), f); std::fclose(f); }  // the volumes' part
+      }
+    }
+    run_target_orders(ctx, orders, vox.data(), daf.data(), d_obj_begin.data());
+    BK_CUDA(cudaMemsetAsync(queue.data(), 0, 2 * sizeof(int), s));
+    clock.mark("order");
+    launch_trace(a, nbig_trace, ctas, lone_percent, s);
+    ++ctx.launches;
+    clock.mark("trace");
+  };
+  if (as_graph) {
+    prepare_engine_launches(ctas, s);  // device queries, before the capture
+    BK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    clock.capturing(true);
+    try {
+      engine();
+    } catch (...) {
+      clock.capturing(false);
+      cudaGraph_t broken = nullptr;
+      cudaStreamEndCapture(s, &broken);
+      if (broken) cudaGraphDestroy(broken);
+      cudaGetLastError();
+      throw;
+    }
+    clock.capturing(false);
+    cudaGraph_t graph = nullptr;
+    BK_CUDA(cudaStreamEndCapture(s, &graph));
+    ctx.launch_graph(graph);
+  } else {
+    engine();
+  }
 
   // ---- results
   const auto st_host = status.download();

@@ -30,11 +30,36 @@ cudaStream_t Context::copy_stream() {
   return copy_;
 }
 
+void Context::launch_graph(cudaGraph_t graph) {
+  if (engine_exec_) {
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(engine_exec_, graph, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(engine_exec_);
+      engine_exec_ = nullptr;
+    } else stats["graph_updates"] += 1;
+  }
+  if (!engine_exec_) {
+    const cudaError_t made = cudaGraphInstantiate(&engine_exec_, graph, 0);
+    if (made != cudaSuccess) {
+      engine_exec_ = nullptr;
+      cudaGraphDestroy(graph);
+      throw CudaError(made, "cudaGraphInstantiate");
+    }
+    stats["graph_instantiations"] += 1;
+  }
+  const cudaError_t launched = cudaGraphLaunch(engine_exec_, stream_);
+  cudaGraphDestroy(graph);
+  BK_CUDA(launched);
+  stats["graph_launches"] += 1;
+}
+
 Context::~Context() {
   if (stream_) {
     int previous = -1;
     cudaGetDevice(&previous);
     cudaSetDevice(device_);
+    if (engine_exec_) cudaGraphExecDestroy(engine_exec_);
     if (copy_) {
       cudaStreamSynchronize(copy_);
       cudaStreamDestroy(copy_);

@@ -44,6 +44,14 @@ class DeviceGuard {
   DeviceGuard &operator=(const DeviceGuard &) = delete;
 };
 
+// Launch choices of the object engine for one workload class (0 / -1: the built-in rule).
+struct Tuning {
+  int trace_cluster_ctas = 0;             // CTAs per cluster for the large objects: 4 or 8
+  long long trace_cluster_voxels = 0;     // objects above this trace on clusters
+  long long prepare_cluster_voxels = 0;   // objects from this size prepare on clusters
+  int lone_first_percent = -1;            // share of clusters that start on the small objects
+};
+
 class Context {
  public:
   explicit Context(int device);
@@ -71,6 +79,14 @@ class Context {
   std::map<std::string, double> stats;
   // Kernels of this library launched by the current call.
   long long launches = 0;
+  // Tuned engine launch choices by workload class (see workload_class in the pipeline), filled by
+  // the autotuner or from a saved table; `forced` overrides them while the autotuner measures.
+  std::map<unsigned long long, Tuning> tuning;
+  const Tuning *forced = nullptr;
+  unsigned long long last_class = 0;  // the workload class of the last call
+  // Launches a captured graph of the engine's launches: the context keeps one executable graph and
+  // updates it in place when the new graph has the same topology (else instantiates it anew).
+  void launch_graph(cudaGraph_t graph);
 
  private:
   int device_ = 0, sm_count_ = 0;
@@ -79,6 +95,7 @@ class Context {
   std::map<size_t, std::vector<void *>> free_;  // size class -> cached blocks
   std::map<void *, size_t> class_of_;           // live and cached blocks -> size class
   size_t cached_ = 0;
+  cudaGraphExec_t engine_exec_ = nullptr;
 };
 
 // Device storage that outlives the context that made it (plain cudaMalloc / cudaFree on its
@@ -163,9 +180,13 @@ class StageClock {
   Context &ctx_;
   std::vector<std::pair<std::string, cudaEvent_t>> marks_;
   std::chrono::steady_clock::time_point host_ = std::chrono::steady_clock::now();
+  bool capturing_ = false;
 
  public:
   explicit StageClock(Context &ctx) : ctx_(ctx) { mark("start"); }
+  // While the stream is captured into a graph, marks become event record nodes of the graph (they
+  // record when the graph runs).
+  void capturing(bool on) { capturing_ = on; }
   ~StageClock() {
     for (auto &m : marks_) cudaEventDestroy(m.second);
   }
@@ -175,8 +196,8 @@ class StageClock {
     host_ = now;
     cudaEvent_t e;
     BK_CUDA(cudaEventCreate(&e));
-    BK_CUDA(cudaEventRecord(e, ctx_.stream()));
     marks_.push_back({stage, e});
+    BK_CUDA(cudaEventRecordWithFlags(e, ctx_.stream(), capturing_ ? cudaEventRecordExternal : cudaEventRecordDefault));
   }
   void finish() {
     if (marks_.size() < 2) return;

@@ -216,6 +216,29 @@ brook_status brook_skeletons_get_array(const brook_skeletons *result, brook_skel
 brook_status brook_edt_device_noalloc(const brook_volume *labels, const float anisotropy[3], int black_border,
                                       float *out, void *stream);
 
+/* No counterpart in the reference's C header (the reference sizes its cooperative grids by a timed
+ * probe, cooperative.cu:18-47). The object engine's launch choices for one workload class: the
+ * CTAs per thread-block cluster of the large objects (4 or 8), the voxel counts from which objects
+ * prepare / trace on clusters, and the percent of clusters that start on the small objects.
+ * 0 (-1 for the percent) keeps the built-in rule. A workload class is a key of the foreground
+ * voxel count, the largest object's voxel count and the object count (their bit lengths). */
+typedef struct brook_tuning {
+  int32_t trace_cluster_ctas;
+  int64_t trace_cluster_voxels;
+  int64_t prepare_cluster_voxels;
+  int32_t lone_first_percent;
+} brook_tuning;
+/* Measures the engine (prepare and trace, CUDA events) on these volumes with candidate launch
+ * choices (a coordinate search from the built-in rule, each candidate timed twice), installs the
+ * fastest in the context for the volumes' workload class and returns the class, the choice and
+ * its time. Calls of that class through this context then use it. */
+brook_status brook_autotune(brook_context *context, const brook_volume *volumes, size_t count,
+                            const brook_skeletonize_options *options, uint64_t *workload_class,
+                            brook_tuning *best, double *best_ms);
+/* Installs (or, with tuning NULL, removes) the launch choice of a workload class, e.g. one a
+ * program saved from an earlier brook_autotune. */
+brook_status brook_context_set_tuning(brook_context *context, uint64_t workload_class, const brook_tuning *tuning);
+
 /* The statistics of the context's last call as a JSON object (the reference keeps the same map as
  * Context.stats, runtime.hpp:59 and bindings.cpp:343-347): "ms_<stage>" stage times measured with
  * CUDA events on the context's stream, and counters (paths, railroad_settled, railroad_touched,

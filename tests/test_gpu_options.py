@@ -77,3 +77,49 @@ def test_pdrf_exponent_not_a_power_of_two(gpu, monkeypatch, exponent, fix_branch
     assert_same(got, traced, f"exponent {exponent}")
     with pytest.raises(Exception, match="odd"):
         bk().skeletonize(labels, output="packed", **dict(opts, teasar_params=dict(params, pdrf_exponent=3)))
+
+
+def test_engine_graph_matches_eager_launches(gpu, monkeypatch):
+    """The engine's launches (prepare, target orders, trace) run as one CUDA graph per call; the
+    context updates its executable graph in place for the next call. The skeletons equal those of
+    the same launches made one by one (BROOK_B200_GRAPH=0) and the oracle's."""
+    from brook_b200 import _native, synthetic
+
+    labels = synthetic.tube_volume((64, 64, 64), objects=8, seed=9)
+    opts = dict(teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    first = bk().skeletonize(labels, output="packed", **opts)
+    stats = _native.stats()
+    assert stats["graph_launches"] == 1 and stats["ms_trace"] > 0 and stats["ms_prepare"] > 0
+    second = bk().skeletonize(labels, output="packed", **opts)
+    assert _native.stats().get("graph_updates", 0) + _native.stats().get("graph_instantiations", 0) == 1
+    monkeypatch.setenv("BROOK_B200_GRAPH", "0")
+    eager = bk().skeletonize(labels, output="packed", **opts)
+    assert "graph_launches" not in _native.stats()
+    exp = oracle.skeletonize(labels, threads=8, **opts)
+    for got in (first, second, eager):
+        assert_same(got, exp, "graph / eager")
+
+
+def test_autotune_installs_a_choice_that_keeps_the_skeletons(gpu, monkeypatch, tmp_path):
+    """brook_b200.tuning.autotune measures launch choices on the caller's volumes, installs the
+    fastest for their workload class and saves it; a new context loads it; the skeletons do not
+    depend on the choice."""
+    from brook_b200 import _native, synthetic, tuning
+
+    monkeypatch.setenv("BROOK_B200_TUNING_CACHE", str(tmp_path / "tuning.json"))
+    labels = synthetic.tube_volume((96, 96, 64), objects=12, seed=5)
+    opts = dict(teasar_params=CFG0_PARAMS, anisotropy=(16, 16, 40), dust_threshold=100)
+    result = tuning.autotune(labels, **opts)
+    assert result["engine_ms"] > 0 and result["tuning"]["trace_cluster_ctas"] in (0, 4, 8)
+    saved = tuning._read()
+    assert any(result["workload_class"] in entries for entries in saved.values())
+    got = bk().skeletonize(labels, output="packed", **opts)
+    assert_same(got, oracle.skeletonize(labels, threads=8, **opts), "tuned")
+    # every candidate choice gives the same skeletons
+    for ctas, percent in ((8, 0), (4, 25)):
+        t = _native.Tuning(ctas, 1, 1, percent)
+        ctx = _native.context(0)
+        _native.check(_native.load().brook_context_set_tuning(ctx, int(result["workload_class"], 16), t))
+        assert_same(bk().skeletonize(labels, output="packed", **opts),
+                    oracle.skeletonize(labels, threads=8, **opts), f"choice {ctas}/{percent}")
+    _native.check(_native.load().brook_context_set_tuning(_native.context(0), int(result["workload_class"], 16), None))
