@@ -308,12 +308,15 @@ __global__ void rank_bounds(const int *parent, const int *rank, const long long 
 
 // ids of one volume (local ids: rank - first + 1), and per root its local flat index and label.
 template <class L>
-__global__ void relabel(const L *labels, int *parent, const int *rank, uint32_t *ids, long long *roots,
+__global__ void relabel(const L *labels, const int *parent, const int *rank, uint32_t *ids, long long *roots,
                         long long *mapping, long long n, long long base, int first) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (parent[base + i] < 0) { ids[i] = 0; return; }
-  const int r = find_root(parent, int(base + i));
+  int r = parent[base + i];
+  if (r < 0) { ids[i] = 0; return; }
+  // a read-only walk to the root (every voxel of a tile passes through its tile root, so writing
+  // shortcuts here would make thousands of threads write the same entries)
+  for (int q = __ldcg(parent + r); q != r; q = __ldcg(parent + r)) r = q;
   ids[i] = uint32_t(rank[r] - first + 1);
   if (r == int(base + i)) {
     roots[rank[r]] = i;

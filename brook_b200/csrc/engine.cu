@@ -1047,7 +1047,8 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
         const int nt = vload(&L->n_touch);
         if (step == 1) {  // the parents' field stays; its queue flags are cleared now
           for (int i = G::tid(); i < nt; i += G::threads()) atomicAnd(a.flags + __ldcg(L4 + i), ~(kNearQueued | kFarQueued));
-          if (G::first()) { s_work[0] += nt; s_work[1] += nt; sh.step = 2; }
+          if (G::first()) { s_work[0] += nt; s_work[1] += nt; }
+          if (threadIdx.x == 0) sh.step = 2;  // every CTA of the group moves on (each has its own copy)
           G::sync();
           continue;
         }
@@ -1104,8 +1105,8 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
         break;
       }
       if (ball) {
-        if (G::first()) { s_work[2] += vload(&L->n_touch); sh.step = a.fix_branching ? 2 : 1; }
-        else if (threadIdx.x == 0) sh.step = a.fix_branching ? 2 : 1;
+        if (G::first()) s_work[2] += vload(&L->n_touch);
+        if (threadIdx.x == 0) sh.step = a.fix_branching ? 2 : 1;  // every CTA of the group moves on
         G::sync();
         continue;
       }
