@@ -11,6 +11,7 @@ __version__ = "0.1.0"
 from ._intake import DEFAULT_TEASAR_PARAMS, DimensionError, skeletonize  # noqa: E402
 from ._packed import PackedSkeletons, Skeleton  # noqa: E402
 from .batch import BatchedSkeletons, skeletonize_batch  # noqa: E402
+from .chunked import merge_fragments, skeletonize_chunked  # noqa: E402
 
-__all__ = ["skeletonize", "skeletonize_batch", "BatchedSkeletons", "PackedSkeletons", "Skeleton",
-           "DEFAULT_TEASAR_PARAMS", "DimensionError", "__version__"]
+__all__ = ["skeletonize", "skeletonize_batch", "skeletonize_chunked", "merge_fragments", "BatchedSkeletons",
+           "PackedSkeletons", "Skeleton", "DEFAULT_TEASAR_PARAMS", "DimensionError", "__version__"]

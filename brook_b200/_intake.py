@@ -111,9 +111,18 @@ def device_volume(labels):
 
 def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
          extra_after, device, device_output=False, producers=(), sample_targets=None):
-    """One C call over `volumes`. producers: stream handles the library's stream waits for first
-    (the producers of device inputs). sample_targets: per volume (before, after) point lists of a
-    batch (extra_before / extra_after then stay empty)."""
+    """One C call over `volumes`, as PackedSkeletons. producers: stream handles the library's
+    stream waits for first (the producers of device inputs). sample_targets: per volume (before,
+    after) point lists of a batch (extra_before / extra_after then stay empty)."""
+    handles = _run_handles(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders,
+                           extra_before, extra_after, device, device_output, producers, sample_targets)
+    grab = _native.packed_device_arrays if device_output else _native.packed_arrays
+    return [PackedSkeletons.from_arrays(grab(h)) for h in handles]
+
+
+def _run_handles(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
+                 extra_after, device, device_output=False, producers=(), sample_targets=None):
+    """_run's C call; returns the raw result handles (the caller destroys them)."""
     ctypes = _native.ctypes
     opts = _native.options(params, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids,
                            extra_before, extra_after)
@@ -141,8 +150,7 @@ def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching,
         _native.check(lib.brook_skeletonize(ctx, arr, ctypes.byref(opts), handles))
     else:
         _native.check(lib.brook_skeletonize_batch(ctx, arr, count, ctypes.byref(opts), handles))
-    grab = _native.packed_device_arrays if device_output else _native.packed_arrays
-    return [PackedSkeletons.from_arrays(grab(handles[i])) for i in range(count)]
+    return [handles[i] for i in range(count)]
 
 
 def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), object_ids=None,

@@ -34,7 +34,7 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_edt_device_noalloc", "brook_skeletons_get_device_view", "brook_skeletons_get_array",
            "brook_array_upload", "brook_array_to_dlpack", "brook_array_to_dlpack_versioned", "brook_components_labels",
            "brook_skeletonize_batch_targets", "brook_context_wait_stream", "brook_autotune",
-           "brook_context_set_tuning"]
+           "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons"]
 
 
 class Volume(ctypes.Structure):
@@ -161,6 +161,9 @@ def _open():
                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Tuning),
                                           ctypes.POINTER(ctypes.c_double)]),
         "brook_context_set_tuning": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(Tuning)]),
+        "brook_skeletons_create": (ctypes.c_int, [ctypes.POINTER(SkeletonsView), ctypes.POINTER(vp)]),
+        "brook_merge_skeletons": (ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_float), sz,
+                                                 ctypes.POINTER(vp)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -12,6 +12,7 @@
 #include "../../include/brook_b200.h"
 #include "../../include/brook_b200_dlpack.h"
 #include "engine.hpp"
+#include "merge.hpp"
 #include "pipeline.hpp"
 
 #ifndef BROOK_B200_VERSION
@@ -832,6 +833,56 @@ brook_status brook_autotune(brook_context *ctx, const brook_volume *volumes, siz
     if (workload_class) *workload_class = cls;
     if (best) *best = tuning_to_c(chosen);
     if (best_ms) *best_ms = chosen_ms;
+  });
+}
+
+brook_status brook_skeletons_create(const brook_skeletons_view *v, brook_skeletons **out) {
+  return protect([&] {
+    require(v && out);
+    *out = nullptr;
+    const size_t k = v->skeleton_count, nv = v->vertex_count, ne = v->edge_count;
+    require((v->labels || !k) && v->vertex_offsets && v->edge_offsets, "incomplete skeletons view");
+    require((v->vertices && v->radii) || !nv, "incomplete skeletons view");
+    require(v->edges || !ne, "incomplete skeletons view");
+    require(v->vertex_offsets[0] == 0 && v->edge_offsets[0] == 0 && size_t(v->vertex_offsets[k]) == nv &&
+                size_t(v->edge_offsets[k]) == ne,
+            "inconsistent skeleton offsets");
+    auto handle = std::make_unique<brook_skeletons>();
+    bk::Packed &p = handle->packed;
+    p.labels.assign(v->labels, v->labels + k);
+    p.vertex_offsets.assign(v->vertex_offsets, v->vertex_offsets + k + 1);
+    p.edge_offsets.assign(v->edge_offsets, v->edge_offsets + k + 1);
+    for (size_t i = 0; i < k; ++i)
+      require(p.vertex_offsets[i] <= p.vertex_offsets[i + 1] && p.edge_offsets[i] <= p.edge_offsets[i + 1],
+              "inconsistent skeleton offsets");
+    p.vertices.assign(v->vertices, v->vertices + 3 * nv);
+    p.radii.assign(v->radii, v->radii + nv);
+    p.edges.assign(v->edges, v->edges + 2 * ne);
+    for (int a = 0; a < 3; ++a) p.anisotropy[a] = v->anisotropy[a];
+    *out = handle.release();
+  });
+}
+
+brook_status brook_merge_skeletons(brook_context *ctx, const brook_skeletons *const *fragments, const float *origins,
+                                   size_t count, brook_skeletons **out) {
+  return protect([&] {
+    require(ctx && out && (fragments || !count));
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    std::vector<const bk::Packed *> parts;
+    std::vector<std::array<float, 3>> shifts;
+    for (size_t i = 0; i < count; ++i) {
+      require(fragments[i] != nullptr);
+      const bk::Packed &p = fragments[i]->packed;
+      if (p.on_device()) require(p.device_vertices->device == ctx->value.device(), "a fragment is on another device");
+      parts.push_back(&p);
+      shifts.push_back(origins ? std::array<float, 3>{origins[3 * i], origins[3 * i + 1], origins[3 * i + 2]}
+                               : std::array<float, 3>{0, 0, 0});
+    }
+    auto handle = std::make_unique<brook_skeletons>();
+    handle->packed = bk::merge_fragments(ctx->value, parts, shifts);
+    *out = handle.release();
   });
 }
 

@@ -216,6 +216,18 @@ brook_status brook_skeletons_get_array(const brook_skeletons *result, brook_skel
 brook_status brook_edt_device_noalloc(const brook_volume *labels, const float anisotropy[3], int black_border,
                                       float *out, void *stream);
 
+/* No counterpart in the reference's C header (its Python binding builds the same from packed
+ * arrays, PackedSkeletons.to_core): a host result handle holding a copy of a packed view, e.g. to
+ * merge skeletons a program kept as arrays. */
+brook_status brook_skeletons_create(const brook_skeletons_view *view, brook_skeletons **out);
+/* brook.h:244-247: one skeleton per label over `count` fragments (the pieces of overlapping chunks),
+ * fragment i's vertices shifted by origins[3i .. 3i+2] (physical units; NULL: no shift). Vertices
+ * of one label at the same physical point merge (the first fragment's radius), edges are mapped,
+ * deduplicated and sorted, vertices on no edge are dropped, labels come out ascending. The result
+ * is a device result (as with BROOK_DEVICE_OUTPUT). */
+brook_status brook_merge_skeletons(brook_context *context, const brook_skeletons *const *fragments,
+                                   const float *origins, size_t count, brook_skeletons **out);
+
 /* No counterpart in the reference's C header (the reference sizes its cooperative grids by a timed
  * probe, cooperative.cu:18-47). The object engine's launch choices for one workload class: the
  * CTAs per thread-block cluster of the large objects (4 or 8), the voxel counts from which objects

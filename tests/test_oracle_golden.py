@@ -243,3 +243,33 @@ def test_soma_paths_stay_attached(fix_branching, hollow):
     # paths are trimmed to it
     inside = np.sqrt((offsets ** 2).sum(axis=1)) <= 10
     assert inside.sum() == 1
+
+
+def test_merge_restatement_joins_overlapping_chunks_of_a_line():
+    """The merge of fragments (oracle/merge.py): a one-voxel line cut into two chunks overlapping
+    by one voxel merges back into the whole line's skeleton, and a label seen in one chunk only
+    passes through."""
+    from oracle import merge as om
+
+    line = np.zeros((40, 3, 3), np.uint32)
+    line[2:38, 1, 1] = 5
+    line[30:33, 0, 0] = 9
+    aniso = (4, 5, 6)
+    opts = dict(teasar_params=dict(scale=1, const=1), anisotropy=aniso, dust_threshold=0, fix_borders=True)
+    whole = oracle.skeletonize(line, **opts).packed()
+    parts = [oracle.skeletonize(np.asfortranarray(line[:21]), **opts).packed(),
+             oracle.skeletonize(np.asfortranarray(line[20:]), **opts).packed()]
+    merged = om.merge(parts, [(0, 0, 0), (20 * 4, 0, 0)])
+    assert merged["labels"].tolist() == [5, 9]  # ascending (the whole volume lists 9 first)
+
+    def per_label(p):
+        out = {}
+        for k, l in enumerate(p["labels"].tolist()):
+            v0, v1, e0, e1 = p["vertex_offsets"][k], p["vertex_offsets"][k + 1], p["edge_offsets"][k], p["edge_offsets"][k + 1]
+            out[l] = (p["vertices"].reshape(-1, 3)[v0:v1], p["edges"].reshape(-1, 2)[e0:e1])
+        return out
+
+    got, exp = per_label(merged), per_label(whole)
+    for l in (5, 9):  # vertices and edges; radii are the chunks' own DBF, which differs at the cut
+        np.testing.assert_array_equal(got[l][0], exp[l][0], err_msg=f"vertices {l}")
+        np.testing.assert_array_equal(got[l][1], exp[l][1], err_msg=f"edges {l}")
