@@ -564,6 +564,7 @@ def run_ours(args, cfg):
         "stages_roofline": stage_roofline(stage, peaks()[0]),
         "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
         "work": {k: stage.get(k) for k in ("paths", "railroad_settled", "railroad_touched", "invalidated", "foreground")},
+        "graph": {k: stage.get(k) for k in ("graph_launches", "graph_updates", "graph_instantiations")},
         "roofline": {"kernel": "trace_kernel", "stage_dominant": dominant, "bound": "hbm", "achieved": achieved,
                      "peak": peak, "peak_source": source, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": trace_bytes},

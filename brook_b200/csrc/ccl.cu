@@ -119,8 +119,9 @@ struct PairList {
 // this tile's voxels start go to `list`; pairs across the tile's +z face only where the plane
 // beyond is there (z0 + 8 < z_ready).
 template <class L>
-__global__ void __launch_bounds__(kTileThreads) tile_union(const L *__restrict__ labels, int *parent, Dims d, bool planar,
-                                                           long long base, int tz0, int z_ready, PairList list) {
+__global__ void __launch_bounds__(kTileThreads, 4) tile_union(const L *__restrict__ labels, int *parent, Dims d,
+                                                              bool planar, long long base, int tz0, int z_ready,
+                                                              PairList list) {
   __shared__ L hal[kHaloN];
   __shared__ int par[kTileN];
   __shared__ int2 staged[kPairStage];
@@ -277,8 +278,8 @@ __global__ void face_union(const L *labels, int *parent, Dims d, bool planar, lo
 // Unites the listed pairs; when the list overflowed, scans every tile-face voxel of the volume
 // instead (face_union's rule reaches every pair the list would have held).
 template <class L>
-__global__ void union_pairs(const L *labels, int *parent, Dims d, bool planar, long long base, long long n,
-                            PairList list) {
+__global__ void __launch_bounds__(256, 8) union_pairs(const L *labels, int *parent, Dims d, bool planar, long long base,
+                                                      long long n, PairList list) {
   const int offered = *list.count;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (offered > list.capacity) {

@@ -647,6 +647,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     clock.mark("trace");
   };
   if (as_graph) {
+    const auto graph_start = std::chrono::steady_clock::now();
     prepare_engine_launches(ctas, s);  // device queries, before the capture
     BK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     clock.capturing(true);
@@ -663,7 +664,11 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     clock.capturing(false);
     cudaGraph_t graph = nullptr;
     BK_CUDA(cudaStreamEndCapture(s, &graph));
+    const auto captured = std::chrono::steady_clock::now();
     ctx.launch_graph(graph);
+    const auto launched = std::chrono::steady_clock::now();
+    ctx.stats["host_ms_graph_capture"] = std::chrono::duration<double, std::milli>(captured - graph_start).count();
+    ctx.stats["host_ms_graph_launch"] = std::chrono::duration<double, std::milli>(launched - captured).count();
   } else {
     engine();
   }
