@@ -154,61 +154,69 @@ __global__ void __launch_bounds__(kTileThreads, 4) tile_union(const L *__restric
     par[t] = t - lx + (31 - __clz(starts & (0xFFFFFFFFu >> (31 - lx))));
   }
   __syncthreads();
+  // Every voxel's forward pairs from its 26-bit mask of same-label neighbours. A pair is dropped
+  // (1) when an intermediate voxel (a face neighbour of an edge pair, a face or edge neighbour of a
+  // corner pair) carries the label: both ends are tied to it; (2) when the pair one step back along
+  // x (both ends inside the tile) carries the label at both ends: those ends share x runs with this
+  // pair's ends, which the load linked, and that pair is kept or dropped by the same rules further
+  // back; (3) for a pair that leaves the tile and cannot step back along x, the same along y, then
+  // z, since each end is tied to its step-back voxel inside its own tile. Inside a region of one
+  // label only the first voxel of a tile row keeps its +y and +z pairs.
   for (int t = threadIdx.x; t < kTileN; t += kTileThreads) {
     const int lx = t % kTileX, ly = (t / kTileX) % kTileY, lz = t / (kTileX * kTileY);
-    if (!(lx < ex && ly < ey && lz < ez)) continue;
+    const bool in = lx < ex && ly < ey && lz < ez;
     const int h = at(lx, ly, lz);
-    const L lv = hal[h];
-    if (lv == L(0)) continue;
-    auto same = [&](int a, int b, int c) { return hal[h + a + kHaloX * (b + kHaloY * c)] == lv; };
-    // pairs that leave the tile: the forward neighbours of a voxel on a face they can cross
-    const bool on_face = lx == 0 || lx == ex - 1 || ly == 0 || ly == ey - 1 || lz == ez - 1;
-    if (on_face) {
-      const long long p = base + (x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz));
+    const L lv = in ? hal[h] : L(0);
+    unsigned m = 0;
+    if (lv != L(0)) {
 #pragma unroll
-      for (int k = 0; k < 26; ++k) {
-        const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
-        if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
-        if (planar && dz != 0) continue;
-        const bool cx = lx + dx < 0 || lx + dx >= kTileX, cy = ly + dy < 0 || ly + dy >= kTileY, cz = lz + dz >= kTileZ;
-        if (!(cx || cy || cz) || (cz && !zface)) continue;
-        if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
-        // The pair one step back along an axis the pair does not cross, with both ends still
-        // inside their tiles, joins the same two tile components (each end is tied to its
-        // step-back voxel inside its tile) and is itself listed or skipped by this rule further
-        // back; so a pair whose step-back ends both carry the label adds nothing.
-        int bx = 0, by = 0, bz = 0;
-        if (!cx && lx >= 1 && lx + dx >= 1) bx = 1;
-        else if (!cy && ly >= 1 && ly + dy >= 1) by = 1;
-        else if (!planar && !cz && lz >= 1 && lz + dz >= 1) bz = 1;
-        if ((bx | by | bz) && same(-bx, -by, -bz) && same(dx - bx, dy - by, dz - bz)) continue;
-        const int2 pair = make_int2(int(p), int(p + dx + (long long)d.sx * (dy + (long long)d.sy * dz)));
-        const int slot = atomicAdd(&nstaged, 1);
-        if (slot < kPairStage) staged[slot] = pair;
-        else if (*(volatile int *)list.count <= list.capacity) {  // more than the stage holds: to the list
-          const int g = atomicAdd(list.count, 1);                    // (no more adds once it overflowed)
-          if (g < list.capacity) list.pairs[g] = pair;
+      for (int k = 0; k < 26; ++k)
+        if (lz + c_dz[k] >= 0 && hal[h + c_dx[k] + kHaloX * (c_dy[k] + kHaloY * c_dz[k])] == lv) m |= 1u << k;
+    }
+    const unsigned mprev = __shfl_up_sync(0xFFFFFFFFu, m, 1);  // the x-previous voxel's (same row)
+    if (lv == L(0)) continue;
+    // forward neighbours: +x (1), +y (3), +z (5), the xy edges with +y (7, 9), and every neighbour
+    // with +z (11, 13, 15, 17, 19, 21, 23, 25); in-tile +x pairs are the load's run links
+    unsigned cand = m & 0x2AAAAAAu & (lx == kTileX - 1 ? ~0u : ~2u);
+    if (planar) cand &= 0x28Au;  // +x, +y and the xy edges with +y
+    while (cand) {
+      const int k = __ffs(cand) - 1;
+      cand &= cand - 1;
+      const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
+      const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+      if (nz >= 2) {  // (1): the face intermediates, and a corner's edge intermediates
+        const unsigned fx = dx ? 1u << (dx > 0 ? 1 : 0) : 0u, fy = dy ? 1u << (dy > 0 ? 3 : 2) : 0u,
+                       fz = dz ? 1u << (dz > 0 ? 5 : 4) : 0u;
+        unsigned inter = fx | fy | fz;
+        if (nz == 3)
+          inter |= (1u << (6 + ((dx > 0) << 1) + (dy > 0))) | (1u << (10 + ((dy > 0) << 1) + (dz > 0))) |
+                   (1u << (14 + ((dx > 0) << 1) + (dz > 0)));
+        if (m & inter) continue;
+      }
+      const bool cx = lx + dx < 0 || lx + dx >= kTileX, cy = ly + dy < 0 || ly + dy >= kTileY, cz = lz + dz >= kTileZ;
+      const bool crossing = cx || cy || cz;
+      if (cz && !zface) continue;  // the plane beyond is not here yet: face_union takes it later
+      if (!cx && lx >= 1 && lx + dx >= 1) {  // (2)
+        if ((m & 1u) && ((mprev >> k) & 1u)) continue;
+      } else if (crossing) {  // (3)
+        if (!cy && ly >= 1 && ly + dy >= 1) {
+          if ((m & 4u) && hal[h + dx + kHaloX * ((dy - 1) + kHaloY * dz)] == lv) continue;
+        } else if (!planar && !cz && lz >= 1 && lz + dz >= 1) {
+          if ((m & 16u) && hal[h + dx + kHaloX * (dy + kHaloY * (dz - 1))] == lv) continue;
         }
       }
-    }
-    // Inside a region of one label: when the +y and +z neighbours (in this tile) carry the label,
-    // every other forward pair has one of them as a face intermediate and is skipped, so those
-    // two unions are all (in a plane, the +y one).
-    if (ly + 1 < ey && same(0, 1, 0) && (planar || (lz + 1 < ez && same(0, 0, 1)))) {
-      tile_unite(par, t, t + kTileX);
-      if (!planar) tile_unite(par, t, t + kTileX * kTileY);
-      continue;
-    }
-#pragma unroll
-    for (int k = 0; k < 26; ++k) {
-      const int dx = c_dx[k], dy = c_dy[k], dz = c_dz[k];
-      if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
-      if (dy == 0 && dz == 0) continue;  // the x run, linked at load
-      if (planar && dz != 0) continue;
-      const int nx = lx + dx, ny = ly + dy, nz = lz + dz;
-      if (nx < 0 || ny < 0 || nx >= ex || ny >= ey || nz >= ez) continue;  // other tiles: listed above
-      if (!same(dx, dy, dz) || skipped(dx, dy, dz, same)) continue;
-      tile_unite(par, t, t + dx + kTileX * (dy + kTileY * dz));
+      if (!crossing) {
+        tile_unite(par, t, t + dx + kTileX * (dy + kTileY * dz));
+        continue;
+      }
+      const long long p = base + (x0 + lx) + (long long)d.sx * ((y0 + ly) + (long long)d.sy * (z0 + lz));
+      const int2 pair = make_int2(int(p), int(p + dx + (long long)d.sx * (dy + (long long)d.sy * dz)));
+      const int slot = atomicAdd(&nstaged, 1);
+      if (slot < kPairStage) staged[slot] = pair;
+      else if (*(volatile int *)list.count <= list.capacity) {  // more than the stage holds: to the list
+        const int g = atomicAdd(list.count, 1);                    // (no more adds once it overflowed)
+        if (g < list.capacity) list.pairs[g] = pair;
+      }
     }
   }
   __syncthreads();

@@ -71,6 +71,31 @@ def test_noalloc_edt_matches_brook_edt_twice(gpu):
         np.testing.assert_array_equal(got.view(np.uint32), exp.view(np.uint32), err_msg=str(aniso))
 
 
+def test_noalloc_edt_over_several_stack_batches(gpu):
+    """A volume whose y and z passes need more envelope stack than the fixed scratch holds at
+    once (256 x 256 x 64: about 68 MB of y-pass stacks), so each pass runs in several batches of
+    lines over the same scratch; twice in a row, equal to brook_edt bit for bit."""
+    import torch
+
+    from brook_b200 import _native as n
+    from brook_b200 import synthetic
+
+    labels = synthetic.dense_volume((256, 256, 64), seeds=25, seed=43)
+    _, inv = np.unique(labels, return_inverse=True)
+    labels = inv.reshape(labels.shape).astype(np.uint32)
+    exp = _edt_reference(labels, (8.0, 8.0, 40.0), False)
+    dev = _device_fortran(labels)
+    stream = torch.cuda.Stream()
+    for _ in range(2):
+        out = torch.full((labels.size,), -1.0, dtype=torch.float32, device="cuda")
+        with torch.cuda.stream(stream):
+            status = _edt_noalloc(dev, out, (8.0, 8.0, 40.0), False, stream)
+        assert status == n.SUCCESS, n.lib.brook_last_error().decode()
+        stream.synchronize()
+        got = out.cpu().numpy().reshape(labels.shape[::-1]).transpose(2, 1, 0)
+        np.testing.assert_array_equal(got.view(np.uint32), exp.view(np.uint32))
+
+
 def test_noalloc_edt_rejects_what_does_not_fit(gpu):
     import torch
 
