@@ -289,6 +289,10 @@ def batch_measurement(cfg, steps, warmup, rank=0, world=1, local=0, dist=None):
     plain = lambda: [brook_b200.skeletonize(devs[i], output="packed", **opts) for i in mine]  # noqa: E731
     for _ in range(warmup):
         batched()
+    if world == 1:  # the engine's launch choices measured on the batch (untimed)
+        from brook_b200 import tuning
+
+        tuning.autotune([devs[i] for i in mine], PARAMS, cfg["anisotropy"], DUST, device=local, save=False)
     with ClockSampler(local) as clocks:
         ms, out, stage = timed(batched, steps)
     plain()
@@ -526,6 +530,13 @@ def run_ours(args, cfg):
 
     for _ in range(args.warmup):
         brook_b200.skeletonize(dev, **opts)
+    # the engine's launch choices measured on this workload (untimed; installed in this context)
+    tuned = None
+    if not args.no_autotune:
+        from brook_b200 import tuning
+
+        tuned = tuning.autotune(dev, PARAMS, cfg["anisotropy"], DUST, device=local, save=False)
+        brook_b200.skeletonize(dev, **opts)
     with ClockSampler(local) as clocks:
         ms, packed, stage = timed(lambda: brook_b200.skeletonize(dev, **opts), args.steps)
     for _ in range(max(1, args.warmup // 2)):
@@ -565,6 +576,7 @@ def run_ours(args, cfg):
         "host_ms": {k[8:]: round(v, 3) for k, v in sorted(stage.items()) if k.startswith("host_ms_")},
         "work": {k: stage.get(k) for k in ("paths", "railroad_settled", "railroad_touched", "invalidated", "foreground")},
         "graph": {k: stage.get(k) for k in ("graph_launches", "graph_updates", "graph_instantiations")},
+        "autotune": tuned,
         "roofline": {"kernel": "trace_kernel", "stage_dominant": dominant, "bound": "hbm", "achieved": achieved,
                      "peak": peak, "peak_source": source, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": trace_bytes},
@@ -591,6 +603,7 @@ def main():
     ap.add_argument("--config", default="dense512", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batch and serving comparisons")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the engine's built-in launch rule")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
