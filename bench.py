@@ -427,15 +427,29 @@ def serve_measurement(cfg, local=0):
         for rate in cfg["rates"]:
             stream = [(t / rate, v) for t, v in base]
             row = {}
-            for name, factory in (("batched", lambda: serving.Server(workers=2, **opts)),
-                                  ("per_request", lambda: serving.Server(workers=1, max_batch=1, **opts))):
+            for name, kw in (("batched", dict(workers=2)), ("per_request", dict(workers=1, max_batch=1))):
+                servers = []
+
+                def factory():
+                    servers.append(serving.Server(**kw, **opts))
+                    return servers[-1]
+
                 t0 = time.perf_counter()
                 done = serving.replay(stream, factory)
                 wall = time.perf_counter() - t0
                 skel = sum(len(r.future.result()) for r in done)
                 lat = serving.percentiles([r.latency * 1e3 for r in done])
+                server = servers[0]
+                slow = max(server.records, key=lambda r: r["end"] - r["start"])
                 row[name] = {"p50_ms": lat["p50"], "p99_ms": lat["p99"], "skeletons_per_s": skel / wall,
-                             "requests_per_s": len(done) / wall, "wall_s": wall}
+                             "requests_per_s": len(done) / wall, "wall_s": wall, "batches": len(server.records),
+                             "hand_backs": server.trims, "state_bytes_per_voxel": server.state_bytes_per_voxel,
+                             "slowest_batch": {"wall_ms": (slow["end"] - slow["start"]) * 1e3,
+                                               "starts_at_s": slow["start"] - t0,
+                                               **{k: slow[k] for k in ("requests", "voxels", "device_ms",
+                                                                      "peak_bytes", "handed_back_first")},
+                                               "host_ms": {k: round(v, 1) for k, v in slow["host_ms"].items()
+                                                           if v >= 1.0}}}
                 total = skel
             rates[str(rate)] = row
     head = rates[str(cfg["rates"][1])]["batched"]

@@ -34,7 +34,7 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_edt_device_noalloc", "brook_skeletons_get_device_view", "brook_skeletons_get_array",
            "brook_array_upload", "brook_array_to_dlpack", "brook_array_to_dlpack_versioned", "brook_components_labels",
            "brook_skeletonize_batch_targets", "brook_context_wait_stream", "brook_autotune",
-           "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons"]
+           "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons", "brook_context_trim"]
 
 
 class Volume(ctypes.Structure):
@@ -129,6 +129,7 @@ def _open():
         "brook_context_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(vp)]),
         "brook_context_destroy": (None, [vp]),
         "brook_context_synchronize": (ctypes.c_int, [vp]),
+        "brook_context_trim": (ctypes.c_int, [vp]),
         "brook_array_destroy": (None, [vp]),
         "brook_array_view": (ctypes.c_int, [vp, ctypes.POINTER(Volume)]),
         "brook_array_copy_to_host": (ctypes.c_int, [vp, vp, sz]),
@@ -177,22 +178,42 @@ def check(status):
         raise BrookError(status, load().brook_last_error().decode(errors="replace"))
 
 
-_contexts: dict = {}
-_lock = threading.Lock()
+class _ThreadContexts(dict):
+    """One thread's contexts by (process, device). Held in a threading.local, so it is released
+    when its thread ends, and every context it holds (streams, kept device blocks, the engine's
+    executable graph) is destroyed with it."""
+
+    def __del__(self):
+        lib = _lib
+        if lib is None:
+            return
+        for (pid, _), handle in self.items():
+            if pid == os.getpid():
+                try:
+                    lib.brook_context_destroy(handle)
+                except Exception:  # interpreter shutdown
+                    pass
+        self.clear()
+
+
+_local = threading.local()
 
 
 def context(device=0):
-    """One context per (process, thread, device), as the reference's runtime keeps them."""
-    key = (os.getpid(), threading.get_ident(), int(device))
-    with _lock:
-        ctx = _contexts.get(key)
-        if ctx is None:
-            handle = ctypes.c_void_p()
-            check(load().brook_context_create(int(device), ctypes.byref(handle)))
-            ctx = _contexts[key] = handle
-            from . import tuning
+    """One context per (process, thread, device), as the reference's runtime keeps them; a thread's
+    contexts are destroyed when the thread ends."""
+    contexts = getattr(_local, "contexts", None)
+    if contexts is None:
+        contexts = _local.contexts = _ThreadContexts()
+    key = (os.getpid(), int(device))
+    ctx = contexts.get(key)
+    if ctx is None:
+        handle = ctypes.c_void_p()
+        check(load().brook_context_create(int(device), ctypes.byref(handle)))
+        ctx = contexts[key] = handle
+        from . import tuning
 
-            tuning.install_saved(handle, int(device))
+        tuning.install_saved(handle, int(device))
     return ctx
 
 
@@ -319,6 +340,11 @@ def packed_device_arrays(handle):
                 edges=device(v.edges, (ne, 2), "<u4", torch.uint32),
                 radii=device(v.radii, (nv,), "<f4", torch.float32),
                 anisotropy=tuple(float(a) for a in v.anisotropy))
+
+
+def trim(device=0):
+    """Returns the device memory the calling thread's context keeps for reuse to the driver."""
+    check(load().brook_context_trim(context(device)))
 
 
 def stats(device=0):

@@ -457,6 +457,18 @@ brook_status brook_context_synchronize(brook_context *ctx) {
   });
 }
 
+brook_status brook_context_trim(brook_context *ctx) {
+  return protect([&] {
+    require(ctx);
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    ctx->value.trim();
+    cudaMemPool_t pool;
+    BK_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->value.device()));
+    BK_CUDA(cudaMemPoolTrimTo(pool, 0));
+  });
+}
+
 void brook_array_destroy(brook_array *a) { delete a; }
 brook_status brook_array_view(const brook_array *a, brook_volume *out) {
   return protect([&] {
@@ -900,7 +912,11 @@ brook_status brook_context_stats(brook_context *ctx, char *json, size_t capacity
     require(ctx);
     std::string out = "{";
     bool first = true;
-    for (const auto &kv : ctx->value.stats) {
+    // the context's own memory at the time of the query beside the last call's figures
+    auto stats = ctx->value.stats;
+    stats["context_cached_bytes"] = double(ctx->value.cached_bytes());
+    stats["context_live_bytes"] = double(ctx->value.live_bytes());
+    for (const auto &kv : stats) {
       char value[64];
       std::snprintf(value, sizeof(value), "%.17g", kv.second);
       out += (first ? "\"" : ", \"") + kv.first + "\": " + value;

@@ -182,6 +182,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   cudaStream_t s = ctx.stream();
   ctx.stats.clear();
   ctx.launches = 0;
+  ctx.reset_peak();
   StageClock clock(ctx);
   const auto &t = opt.teasar;
   for (float a : opt.anisotropy)
@@ -829,6 +830,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     BK_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &high));
     ctx.stats["pool_reserved_bytes"] = double(reserved);
     ctx.stats["pool_used_high_bytes"] = double(high);
+    ctx.stats["context_peak_bytes"] = double(ctx.peak_bytes());  // most this call held at once
   }
   const auto w = work.download();
   ctx.stats["paths"] = double(w[3]);

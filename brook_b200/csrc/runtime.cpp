@@ -92,6 +92,8 @@ void *Context::allocate(size_t bytes) {
     void *p = it->second.back();
     it->second.pop_back();
     cached_ -= cls;
+    live_ += cls;
+    if (live_ > peak_) peak_ = live_;
     return p;
   }
   void *p = nullptr;
@@ -106,6 +108,8 @@ void *Context::allocate(size_t bytes) {
     }
   }
   class_of_[p] = cls;
+  live_ += cls;
+  if (live_ > peak_) peak_ = live_;
   return p;
 }
 
@@ -117,6 +121,7 @@ void Context::release(void *p) {
     return;
   }
   const size_t cls = it->second;
+  live_ -= cls;
   if (cached_ + cls > kCacheCap) {
     class_of_.erase(it);
     cudaFreeAsync(p, stream_);

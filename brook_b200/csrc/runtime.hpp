@@ -74,6 +74,12 @@ class Context {
   void *allocate(size_t bytes);
   void release(void *p);
   void trim();  // returns every cached block to the device's pool
+  // Bytes this context holds: handed out and not released (`live`), kept in its free lists
+  // (`cached`), and the most handed out at once since the last reset_peak().
+  size_t live_bytes() const { return live_; }
+  size_t cached_bytes() const { return cached_; }
+  size_t peak_bytes() const { return peak_; }
+  void reset_peak() { peak_ = live_; }
   std::mutex &mutex() { return mutex_; }
   // Per-call statistics: stage times (ms, CUDA events on this context's stream) and work counters.
   std::map<std::string, double> stats;
@@ -94,7 +100,7 @@ class Context {
   std::mutex mutex_;
   std::map<size_t, std::vector<void *>> free_;  // size class -> cached blocks
   std::map<void *, size_t> class_of_;           // live and cached blocks -> size class
-  size_t cached_ = 0;
+  size_t cached_ = 0, live_ = 0, peak_ = 0;
   cudaGraphExec_t engine_exec_ = nullptr;
 };
 

@@ -122,6 +122,10 @@ const char *brook_last_error(void);     /* brook.h:150 */
 brook_status brook_context_create(int device, brook_context **out);
 void brook_context_destroy(brook_context *context);              /* brook.h:155 */
 brook_status brook_context_synchronize(brook_context *context);  /* brook.h:156 */
+/* No counterpart in the reference. Waits for the context's stream, hands every device block the
+ * context keeps for reuse back to the device's default memory pool and trims that pool, so the
+ * memory returns to the driver. The next call allocates again. */
+brook_status brook_context_trim(brook_context *context);
 
 /* brook.h:159-162: device arrays owned by the handle. brook_array_upload copies a volume (host
  * or device memory of the context's device, any strides, any of the ten element types) into a
