@@ -516,7 +516,8 @@ constexpr uint64_t kUnclaimed = ~uint64_t{0};
 // neighbour distance (non-rail neighbours, lowest table index on ties), after re-picking the join
 // as the last road voxel's first rail in dijkstra3d order (lockstep_regular.inc:61-155).
 // Returns the path target-first, or an empty path when no rail is reachable.
-std::vector<i64> railroad(Volume &V, uint32_t label, i64 target, std::vector<i64> &touched) {
+std::vector<i64> railroad(Volume &V, uint32_t label, i64 target, std::vector<i64> &touched,
+                          bool keep_distances = false) {
   const Shape &s = V.s; const auto &ids = *V.ids;
   if (V.pdrf[target] == 0.0f) return {target};
   using Item = std::pair<float, i64>;
@@ -584,7 +585,8 @@ std::vector<i64> railroad(Volume &V, uint32_t label, i64 target, std::vector<i64
     }
     std::reverse(walk.begin(), walk.end());
   }
-  for (i64 v : touched) V.dist[v] = kInf;
+  if (!keep_distances)
+    for (i64 v : touched) V.dist[v] = kInf;
   return walk;
 }
 
@@ -1539,6 +1541,22 @@ int64_t oracle_railroad(const float *field, const uint32_t *labels, int64_t sx, 
   auto path = railroad(V, 1, target, touched);
   for (size_t i = 0; i < path.size() && int64_t(i) < capacity; ++i) out[i] = path[i];
   return int64_t(path.size());
+}
+// The railroad's float32 distance field of the same search (+inf where it never reached): the
+// SSSP distances the path walks back on, for comparison with a float64 search.
+int oracle_railroad_distances(const float *field, const uint32_t *labels, int64_t sx, int64_t sy, int64_t sz,
+                              int64_t target, float *dist_out) {
+  try {
+    Volume V; V.s = Shape{sx, sy, sz};
+    std::vector<uint32_t> ids(labels, labels + V.s.n());
+    V.ids = &ids;
+    V.pdrf.assign(field, field + V.s.n());
+    V.dist.assign(V.s.n(), kInf);
+    std::vector<i64> touched;
+    railroad(V, 1, target, touched, true);
+    std::copy(V.dist.begin(), V.dist.end(), dist_out);
+    return 0;
+  } catch (...) { return 1; }
 }
 // Target order rule on a flat (mask, daf) pair: descending daf (inf -> 0), ties -> higher index.
 int64_t oracle_target_order(const uint8_t *mask, const float *daf, int64_t n, int64_t *out) {

@@ -57,6 +57,9 @@ def lib():
         _lib.oracle_railroad.restype = ctypes.c_int64
         _lib.oracle_railroad.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                          ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]
+        _lib.oracle_railroad_distances.restype = ctypes.c_int
+        _lib.oracle_railroad_distances.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                                   ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p]
         _lib.oracle_target_order.restype = ctypes.c_int64
         _lib.oracle_target_order.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
         _lib.oracle_prepare.restype = ctypes.c_void_p
@@ -249,6 +252,16 @@ def railroad(field, target, component=None):
     out = np.zeros(field.size, np.int64)
     n = lib().oracle_railroad(field.ctypes.data, comp.ctypes.data, *field.shape, int(target), out.ctypes.data, out.size)
     return out[:n].tolist()
+
+
+def railroad_distances(field, target, component=None):
+    """The railroad's float32 distance field from `target` (+inf where the search never reached)."""
+    field = np.asfortranarray(np.asarray(field, np.float32))
+    comp = np.ones(field.shape, np.uint32, order="F") if component is None else np.asfortranarray(component.astype(np.uint32))
+    out = np.zeros(field.shape, np.float32, order="F")
+    if lib().oracle_railroad_distances(field.ctypes.data, comp.ctypes.data, *field.shape, int(target), out.ctypes.data):
+        raise RuntimeError("oracle railroad failed")
+    return out
 
 
 def target_order(mask, daf):
