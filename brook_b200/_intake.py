@@ -64,8 +64,8 @@ def _is_device(labels):
 
 def producer_stream(labels, stream=None):
     """The stream handle whose queued work must finish before `labels` (device memory) is read:
-    the caller's `stream` (an int handle or a torch.cuda.Stream), else the array's own CUDA array
-    interface stream, else torch's current stream for a torch tensor, else the legacy default
+    the caller's `stream` (an int handle or a torch.cuda.Stream), else torch's current stream for a
+    torch tensor, else the array's own CUDA array interface stream, else the legacy default
     stream. Handles follow the CUDA array interface: 1 legacy default, 2 per-thread default,
     anything else a cudaStream_t. (The reference's binding fences the same producer,
     cpp/python/bindings.cpp:104-126.)"""
