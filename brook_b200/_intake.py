@@ -110,24 +110,26 @@ def device_volume(labels):
 
 
 def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
-         extra_after, device, device_output=False, producers=(), sample_targets=None):
+         extra_after, device, device_output=False, producers=(), sample_targets=None, fill_holes=False):
     """One C call over `volumes`, as PackedSkeletons. producers: stream handles the library's
     stream waits for first (the producers of device inputs). sample_targets: per volume (before,
     after) point lists of a batch (extra_before / extra_after then stay empty)."""
     handles = _run_handles(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders,
-                           extra_before, extra_after, device, device_output, producers, sample_targets)
+                           extra_before, extra_after, device, device_output, producers, sample_targets, fill_holes)
     grab = _native.packed_device_arrays if device_output else _native.packed_arrays
     return [PackedSkeletons.from_arrays(grab(h)) for h in handles]
 
 
 def _run_handles(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
-                 extra_after, device, device_output=False, producers=(), sample_targets=None):
+                 extra_after, device, device_output=False, producers=(), sample_targets=None, fill_holes=False):
     """_run's C call; returns the raw result handles (the caller destroys them)."""
     ctypes = _native.ctypes
     opts = _native.options(params, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids,
                            extra_before, extra_after)
     if device_output:
         opts.flags |= _native.DEVICE_OUTPUT
+    if fill_holes:
+        opts.flags |= _native.FILL_HOLES
     lib = _native.load()
     ctx = _native.context(device)
     for handle in dict.fromkeys(producers):
@@ -166,15 +168,16 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     tensor or an array with the CUDA array interface, read in place when Fortran-ordered; the
     library's stream first waits for the producer's work (`stream`: the producer's stream handle
     or torch.cuda.Stream; default: the array's own CUDA array interface stream, torch's current
-    stream for a torch tensor, else the legacy default stream). `parallel`,
+    stream for a torch tensor, else the legacy default stream). `fill_holes` fills every
+    component's voids before the distance transform (the reference's rule: components in
+    ascending id, a component whose voxels an earlier fill painted is not filled). `parallel`,
     `parallel_chunk_size`, `in_place`, `progress`, `borrow` and `streaming` are accepted for
-    compatibility. `fill_holes`, `fix_avocados` and `voxel_graph` are not supported by this build
-    and raise.
+    compatibility. `fix_avocados` and `voxel_graph` are not supported by this build and raise.
     """
     if output not in ("skeletons", "packed", "packed_device"):
         raise ValueError("brook_b200: output must be 'skeletons', 'packed' or 'packed_device'")
-    if fill_holes or fix_avocados or voxel_graph is not None:
-        raise NotImplementedError("brook_b200: fill_holes, fix_avocados and voxel_graph are not supported")
+    if fix_avocados or voxel_graph is not None:
+        raise NotImplementedError("brook_b200: fix_avocados and voxel_graph are not supported")
     params = teasar(teasar_params)
     anisotropy = tuple(float(a) for a in np.asarray(anisotropy, dtype=np.float32))
     producers = []
@@ -191,7 +194,7 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     packed = _run([volume], params, anisotropy, ids, dust_threshold, fix_branching, fix_borders,
                   [tuple(int(c) for c in p) for p in extra_targets_before],
                   [tuple(int(c) for c in p) for p in extra_targets_after], device,
-                  device_output=output == "packed_device", producers=producers)[0]
+                  device_output=output == "packed_device", producers=producers, fill_holes=fill_holes)[0]
     del keep
     if output == "skeletons":
         return packed.to_skeletons()

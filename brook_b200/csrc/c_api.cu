@@ -214,8 +214,7 @@ bk::Options options_of(const brook_skeletonize_options *p) {
   const uint32_t known = BROOK_FIX_BRANCHING | BROOK_FIX_BORDERS | BROOK_FILTER_OBJECTS | BROOK_DEVICE_OUTPUT |
                          BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS;
   require(!(p->flags & ~known), "unknown skeletonization flags");
-  if (p->flags & (BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS))
-    throw std::invalid_argument("fill_holes and fix_avocados are not supported by this build");
+  if (p->flags & BROOK_FIX_AVOCADOS) throw std::invalid_argument("fix_avocados is not supported by this build");
   if (p->voxel_graph) throw std::invalid_argument("voxel_graph is not supported by this build");
   bk::Options o;
   auto &t = o.teasar;

@@ -81,6 +81,16 @@ struct IdVolume {
   int64_t count;
 };
 std::vector<std::vector<Box>> analyze(Context &ctx, const uint32_t *ids, const std::vector<IdVolume> &volumes);
+// ---- hole filling (holes.cu) ----
+// The components of each volume (ids + offset, boxes by id as analyze gives them) with their voids
+// filled as the reference's fill_all_holes leaves them; returns the voxels filled. The ids change
+// in place; the boxes are the ones before filling.
+struct HoleVolume {
+  long long offset;
+  VolumeDims d;
+  const std::vector<Box> *boxes;
+};
+long long fill_holes(Context &ctx, uint32_t *ids, const std::vector<HoleVolume> &volumes);
 std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, const uint32_t *ids,
                                             const std::vector<IdVolume> &volumes);
 // 26-bit same-id neighbour mask of every voxel (0 for background).

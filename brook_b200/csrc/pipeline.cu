@@ -174,6 +174,7 @@ struct VolumeState {
   std::vector<float> dbf_max;
   std::vector<int> object_of;  // id -> global object index, -1 when inactive
   bool empty = true;
+  bool black_border = false;   // one component filling the volume as given
 };
 
 }  // namespace
@@ -254,13 +255,28 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     }
     auto boxes = analyze(ctx, ids.data(), iv);
     for (size_t j = 0; j < which.size(); ++j) vs[which[j]].boxes = std::move(boxes[j]);
+    // black border from the volume as given, before any void is filled (skeletonize.cu:82-85)
+    for (auto &st : vs) st.black_border = !st.empty && st.cc.count == 1 && st.boxes[1].count == st.d.n();
     clock.mark("analyze");
+    // ---- voids of every component filled (skeletonize.cu:86-90): the ids change, then the boxes
+    // and counts are taken again
+    if (opt.fill_holes && !iv.empty()) {
+      std::vector<HoleVolume> hv;
+      for (size_t j : which) hv.push_back({vs[j].offset, vs[j].d, &vs[j].boxes});
+      const long long filled = fill_holes(ctx, ids.data(), hv);
+      ctx.stats["hole_filled_voxels"] = double(filled);
+      if (filled) {
+        auto again = analyze(ctx, ids.data(), iv);
+        for (size_t j = 0; j < which.size(); ++j) vs[which[j]].boxes = std::move(again[j]);
+      }
+      clock.mark("holes");
+    }
   }
   // ---- EDT of every volume at once (the y and z passes of all volumes' lines in one launch each)
   {
     std::vector<EdtVolume> ev;
     for (const auto &st : vs)
-      if (!st.empty) ev.push_back({st.offset, st.d, st.cc.count == 1 && st.boxes[1].count == st.d.n()});
+      if (!st.empty) ev.push_back({st.offset, st.d, st.black_border});
     edt_volumes(ctx, ids.data(), ev, aniso, dbf.data());
     clock.mark("edt");
   }

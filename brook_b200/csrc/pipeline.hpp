@@ -23,6 +23,7 @@ struct Options {
   std::array<float, 3> anisotropy{1, 1, 1};
   double dust = 1000;
   bool fix_branching = true, fix_borders = true;
+  bool fill_holes = false;  // every component's voids filled before the EDT (BROOK_FILL_HOLES)
   std::optional<std::vector<int64_t>> object_ids;
   // extra targets per volume of the call (x, y, z in that volume's frame); volumes beyond the
   // vectors' ends have none

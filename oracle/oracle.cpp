@@ -491,6 +491,7 @@ struct Params {
   float anisotropy[3];
   double dust;
   int fix_branching, fix_borders;
+  int fill_holes = 0;
   // extra targets (x, y, z triples): `before` traced first, `after` once no voxel is left
   std::vector<std::array<i64, 3>> before, after;
   // a PDRF field (float32 per voxel, Fortran order) that replaces the computed one: tests use it
@@ -917,6 +918,38 @@ i64 fill_voids(std::vector<uint32_t> &mask, const Shape &s) {
   return filled;
 }
 
+// fill_holes (holes.cu:38-67; its call in skeletonize.cu:86-90 and batch.cu:217-220): components
+// in ascending id, each in its original box; the voxels of the current ids equal to the id form a
+// mask whose voids are filled (fill_voids); every voxel of the filled mask is painted with the id,
+// and a painted voxel's earlier nonzero id (another component) disables that component, which is
+// then filled no more. `box` holds the original boxes (lo x y z, hi x y z, count). Returns the
+// voxels filled by the components that were filled.
+i64 fill_all_holes(std::vector<uint32_t> &ids, const Shape &s, const std::vector<std::array<i64, 7>> &box) {
+  std::vector<uint8_t> disabled(box.size(), 0);
+  i64 total = 0;
+  for (size_t id = 1; id < box.size(); ++id) {
+    const auto &b = box[id];
+    if (!b[6] || disabled[id]) continue;
+    const Shape cs{b[3] - b[0] + 1, b[4] - b[1] + 1, b[5] - b[2] + 1};
+    std::vector<uint32_t> mask(cs.n());
+    for (i64 c = 0; c < cs.n(); ++c) {
+      i64 x, y, z; cs.xyz(c, x, y, z);
+      mask[c] = ids[s.idx(x + b[0], y + b[1], z + b[2])] == uint32_t(id) ? 1u : 0u;
+    }
+    const i64 filled = fill_voids(mask, cs);
+    if (!filled) continue;
+    total += filled;
+    for (i64 c = 0; c < cs.n(); ++c) {
+      if (!mask[c]) continue;
+      i64 x, y, z; cs.xyz(c, x, y, z);
+      uint32_t &v = ids[s.idx(x + b[0], y + b[1], z + b[2])];
+      if (v && v != uint32_t(id)) disabled[v] = 1;
+      v = uint32_t(id);
+    }
+  }
+  return total;
+}
+
 // The soma root (trace.cu:55-73, batched.cu:58-105): among the voxels at the DBF maximum, sorted
 // by (x, y, z), the first nearest (float64 squared distance, voxel units) to their float32 centroid.
 i64 soma_root(const std::vector<float> &dbf, const std::vector<i64> &voxels, float maximum, const Shape &s) {
@@ -972,6 +1005,7 @@ struct Result {
   std::vector<float> vertices, radii;
   std::vector<uint32_t> edges;
   std::string error;
+  int64_t filled = 0;  // voxels fill_holes filled
   // stage outputs
   Components cc;
   std::vector<float> dbf, daf, pdrf;
@@ -1047,7 +1081,30 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
     voxels[id].push_back(v);
   }
   R.stage_ms[1] = lap.next();
+  // black border from the volume as given, before any hole is filled (skeletonize.cu:82-85)
   const bool black_border = count == 1 && box[1][6] == n;
+  if (P.fill_holes) {
+    R.filled = fill_all_holes(R.cc.ids, s, box);
+    if (R.filled) {
+      // the boxes, voxel lists and first voxels again (preamble.cu:77-90): a component whose
+      // voxels were all painted keeps its old first voxel and has no voxels
+      box.assign(count + 1, {INT32_MAX, INT32_MAX, INT32_MAX, -1, -1, -1, 0});
+      for (auto &list : voxels) list.clear();
+      std::vector<i64> first(count + 1, -1);
+      for (i64 v = 0; v < n; ++v) {
+        const uint32_t id = ids[v];
+        if (!id) continue;
+        i64 x, y, z; s.xyz(v, x, y, z);
+        auto &b = box[id];
+        b[0] = std::min(b[0], x); b[1] = std::min(b[1], y); b[2] = std::min(b[2], z);
+        b[3] = std::max(b[3], x); b[4] = std::max(b[4], y); b[5] = std::max(b[5], z); ++b[6];
+        voxels[id].push_back(v);
+        if (first[id] < 0) first[id] = v;
+      }
+      for (size_t id = 1; id <= count; ++id)
+        if (first[id] >= 0) R.cc.roots[id - 1] = first[id];
+    }
+  }
   Volume &V = st->V;
   V.s = s; V.ids = &R.cc.ids;
   V.dbf = edt(ids.data(), s, P.anisotropy, black_border, 3, threads);
@@ -1404,6 +1461,7 @@ struct oracle_params {
   const int64_t *targets_before; int64_t n_before;  // x, y, z triples
   const int64_t *targets_after; int64_t n_after;
   const float *pdrf_field;  // optional (null: computed)
+  int32_t fill_holes;
 };
 
 namespace {
@@ -1420,6 +1478,7 @@ Params params_of(const oracle_params *p) {
     for (int64_t i = 0; i < p->n_after; ++i)
       P.after.push_back({p->targets_after[3 * i], p->targets_after[3 * i + 1], p->targets_after[3 * i + 2]});
     P.pdrf_field = p->pdrf_field;
+    P.fill_holes = p->fill_holes;
     return P;
 }
 }  // namespace
@@ -1507,6 +1566,7 @@ const void *oracle_array(void *h, const char *name, int64_t *count) {
   if (k == "path_offsets") return give(r->path_offsets);
   if (k == "path_labels") return give(r->path_labels);
   if (k == "stage_ms") return give(r->stage_ms);
+  if (k == "filled") { *count = 1; return &r->filled; }
   *count = -1;
   return nullptr;
 }

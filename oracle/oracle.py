@@ -25,7 +25,8 @@ class _Params(ctypes.Structure):
                 ("anisotropy", ctypes.c_float * 3), ("dust", ctypes.c_double), ("fix_branching", ctypes.c_int32),
                 ("fix_borders", ctypes.c_int32), ("targets_before", ctypes.POINTER(ctypes.c_int64)),
                 ("n_before", ctypes.c_int64), ("targets_after", ctypes.POINTER(ctypes.c_int64)),
-                ("n_after", ctypes.c_int64), ("pdrf_field", ctypes.POINTER(ctypes.c_float))]
+                ("n_after", ctypes.c_int64), ("pdrf_field", ctypes.POINTER(ctypes.c_float)),
+                ("fill_holes", ctypes.c_int32)]
 
 
 _lib = None
@@ -83,7 +84,8 @@ _ARRAY_TYPES = {"labels": np.int64, "vertex_offsets": np.int64, "edge_offsets": 
                 "radii": np.float32, "edges": np.uint32, "cc": np.uint32, "mapping": np.int64, "cc_roots": np.int64,
                 "dbf": np.float32, "daf": np.float32, "pdrf": np.float32, "roots": np.int64, "targets": np.int64,
                 "boxes": np.int64, "orders": np.int64, "order_offsets": np.int64, "paths": np.int64,
-                "path_offsets": np.int64, "path_labels": np.int64, "stage_ms": np.float64}
+                "path_offsets": np.int64, "path_labels": np.int64, "stage_ms": np.float64,
+                "filled": np.int64}
 
 # names of the entries of OracleResult.array("stage_ms"): wall-clock ms of each step
 STAGES = ("components", "boxes", "edt", "borders", "daf", "pdrf", "orders", "trace", "assembly")
@@ -166,12 +168,12 @@ DEFAULT_TEASAR_PARAMS = dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_expon
 
 def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), dust_threshold=1000,
                 fix_branching=True, fix_borders=True, threads=1, stages=False, extra_targets_before=(),
-                extra_targets_after=(), pdrf_field=None):
+                extra_targets_after=(), pdrf_field=None, fill_holes=False):
     """Run the oracle on a 3D label volume (any layout; read as its logical (x, y, z) axes), with
     the argument defaults of the reference's brook.skeletonize. `pdrf_field` (float32, the
     volume's shape) replaces the oracle's own PDRF over the traced objects: a test traces from
     another implementation's field where the power itself is not bit-reproducible (an exponent
-    that is not a power of two)."""
+    that is not a power of two). With `fill_holes`, array("filled") holds the voxels filled."""
     labels = np.asarray(labels)
     if labels.dtype == bool:
         labels = labels.view(np.uint8)
@@ -181,6 +183,7 @@ def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1
     if labels.dtype not in _DTYPES:
         raise TypeError(f"unsupported label dtype {labels.dtype}")
     params = _params(teasar_params or {}, anisotropy, dust_threshold, fix_branching, fix_borders)
+    params.fill_holes = int(bool(fill_holes))
     keep = []
     for name, points in (("targets_before", extra_targets_before), ("targets_after", extra_targets_after)):
         pts = np.ascontiguousarray(np.asarray(list(points), np.int64).reshape(-1, 3))
