@@ -232,6 +232,7 @@ bk::Options options_of(const brook_skeletonize_options *p) {
   o.fix_branching = (p->flags & BROOK_FIX_BRANCHING) != 0;
   o.fix_borders = (p->flags & BROOK_FIX_BORDERS) != 0;
   o.device_output = (p->flags & BROOK_DEVICE_OUTPUT) != 0;
+  o.fill_holes = (p->flags & BROOK_FILL_HOLES) != 0;
   if (p->flags & BROOK_FILTER_OBJECTS) {
     require(p->object_ids || !p->object_ids_count);
     o.object_ids = std::vector<int64_t>(p->object_ids, p->object_ids + p->object_ids_count);
