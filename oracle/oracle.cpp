@@ -41,6 +41,7 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <map>
 #include <vector>
 
 namespace {
@@ -491,7 +492,7 @@ struct Params {
   float anisotropy[3];
   double dust;
   int fix_branching, fix_borders;
-  int fill_holes = 0;
+  int fill_holes = 0, fix_avocados = 0;
   // extra targets (x, y, z triples): `before` traced first, `after` once no voxel is left
   std::vector<std::array<i64, 3>> before, after;
   // a PDRF field (float32 per voxel, Fortran order) that replaces the computed one: tests use it
@@ -811,17 +812,25 @@ std::vector<std::vector<i64>> trace_object(Volume &V, const ObjectPlan &plan, co
   size_t cursor = 0, after = 0;
   while (i64(paths.size()) < plan.max_paths) {
     i64 t = -1;
+    bool from_order = false;
     const size_t iter = paths.size();
     if (iter < plan.manual.size()) t = plan.manual[iter];
     else {
       while (cursor < plan.order.size() && !V.alive[plan.order[cursor]]) ++cursor;
-      if (cursor < plan.order.size()) t = plan.order[cursor];
+      if (cursor < plan.order.size()) { t = plan.order[cursor]; from_order = true; }
       else if (after < plan.after.size()) t = plan.after[after++];
       else break;
     }
     std::vector<i64> path = P.fix_branching ? railroad(V, label, t, rtouched)
                                             : parent_walk(V, label, t, plan.root, i64(plan.voxels.size()) + 1);
-    if (path.empty()) throw std::runtime_error("no rail reachable from a target");
+    if (path.empty()) {
+      // No rail is reachable from t (an infinite penalty walls it off: a cavity the avocado stage
+      // painted without refreshing the field). A target of the DAF order ends the object, since
+      // it would be picked again and again (trace.cu:218-224); a manual target leaves an empty path.
+      if (from_order) break;
+      paths.push_back({});
+      continue;
+    }
     if (plan.soma) path = trim_to_soma(V.s, path, plan.root, plan.soma_radius, P);
     invalidate(V, label, path, P, P.scale, P.constant, touched, frontier, next, far, keep, snap);
     if (P.fix_branching)
@@ -950,6 +959,253 @@ i64 fill_all_holes(std::vector<uint32_t> &ids, const Shape &s, const std::vector
   return total;
 }
 
+// ---------------------------------------------------------------------------------------------
+// The avocado stage (avocado.cpp:223-239, restating Kimimaro 5.8.1's engage_avocado_protection).
+// Its candidates are iterated in the order of a CPython 3.12 set of ints, restated here from
+// CPython's setobject.c rules: table of 2^k slots (8 at first), hash(k) == k, probe i, then up to 9
+// slots after it, then i = (5 i + 1 + perturb) & mask with perturb >>= 5; a deleted slot is a
+// dummy, and a new key takes the last dummy its probe passed before reaching an empty slot; the
+// table grows to hold 4x the live keys (2x past 50000) when fill reaches 3/5 of it.
+struct PySet {
+  std::vector<i64> key;          // -1 empty, -2 dummy, else the key
+  i64 used = 0, fill = 0;
+  PySet() : key(8, -1) {}
+  i64 mask() const { return i64(key.size()) - 1; }
+  // the slot holding k, or where k would go (the last dummy passed before an empty slot, else
+  // that empty slot)
+  i64 find(i64 k, bool clean) const {
+    uint64_t perturb = uint64_t(k);
+    i64 i = k & mask(), dummy = -1;
+    for (;;) {
+      const i64 probes = i + 9 <= mask() ? 9 : 0;
+      for (i64 j = 0; j <= probes; ++j) {
+        const i64 e = key[i + j];
+        if (e == -1) return dummy >= 0 ? dummy : i + j;
+        if (!clean && e == k) return i + j;
+        if (!clean && e == -2) dummy = i + j;  // the last dummy passed takes the key
+      }
+      perturb >>= 5;
+      i = i64((uint64_t(i) * 5 + 1 + perturb) & uint64_t(mask()));
+    }
+  }
+  void resize(i64 minused) {
+    i64 size = 8;
+    while (size <= minused) size <<= 1;
+    if (size == 8 && i64(key.size()) == 8 && fill == used) return;
+    std::vector<i64> old;
+    old.swap(key);
+    key.assign(size, -1);
+    fill = used;
+    for (i64 e : old) if (e >= 0) key[find(e, true)] = e;
+  }
+  bool contains(i64 k) const { return key[find(k, false)] == k; }
+  void add(i64 k) {
+    const i64 at = find(k, false);
+    if (key[at] == k) return;
+    const bool fresh = key[at] == -1;
+    key[at] = k;
+    ++used;
+    if (fresh && ++fill * 5 >= mask() * 3) resize(used > 50000 ? used * 2 : used * 4);
+  }
+  void discard(i64 k) {
+    const i64 at = find(k, false);
+    if (key[at] == k) { key[at] = -2; --used; }
+  }
+  void difference_update(const PySet &o) {
+    for (i64 e : o.key) if (e >= 0) discard(e);
+    if (fill - used > mask() / 4) resize(used > 50000 ? used * 2 : used * 4);
+  }
+  void update(const PySet &o) {
+    if (&o == this || !o.used) return;
+    if ((fill + o.used) * 5 >= mask() * 3) resize((used + o.used) * 2);
+    if (!fill && key.size() == o.key.size() && o.fill == o.used) { key = o.key; fill = o.fill; used = o.used; return; }
+    if (!fill) {
+      fill = used = o.used;
+      for (i64 e : o.key) if (e >= 0) key[find(e, true)] = e;
+      return;
+    }
+    for (i64 e : o.key) if (e >= 0) add(e);
+  }
+  std::vector<i64> items() const {
+    std::vector<i64> out;
+    for (i64 e : key) if (e >= 0) out.push_back(e);
+    return out;
+  }
+};
+
+// fill_voids 2.1.2 on a binary crop (avocado.cpp:23-52): background reached from the crop's faces
+// becomes 0, everything else 1. In 3D the seeds are, on each face scanned row after row, the first
+// background voxel of every background run (the run state carries over from one row to the next);
+// in 2D every background pixel on the border. The flood is 6- (4-) connected.
+void avocado_fill(std::vector<uint8_t> &m, const i64 s[3], int dims) {
+  std::vector<i64> queue;
+  auto at = [&](const i64 p[3]) { return p[0] + s[0] * (p[1] + s[1] * p[2]); };
+  if (dims == 3) {
+    const int axes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
+    for (const auto &ax : axes)
+      for (int side = 0; side < 2; ++side) {
+        bool background = false;
+        for (i64 v = 0; v < s[ax[1]]; ++v)
+          for (i64 u = 0; u < s[ax[0]]; ++u) {
+            i64 p[3];
+            p[ax[0]] = u; p[ax[1]] = v; p[ax[2]] = side ? s[ax[2]] - 1 : 0;
+            const i64 i = at(p);
+            if (!m[i] && !background) queue.push_back(i);
+            background = !m[i];
+          }
+      }
+    for (i64 i : queue) m[i] = 2;
+  } else {
+    for (i64 y = 0; y < s[1]; ++y)
+      for (i64 x = 0; x < s[0]; ++x) {
+        const i64 i = x + s[0] * y;
+        if (!m[i] && (x == 0 || x == s[0] - 1 || y == 0 || y == s[1] - 1)) { m[i] = 2; queue.push_back(i); }
+      }
+  }
+  for (size_t head = 0; head < queue.size(); ++head) {
+    const i64 i = queue[head];
+    const i64 p[3] = {i % s[0], (i / s[0]) % s[1], i / (s[0] * s[1])};
+    for (int a = 0; a < dims; ++a)
+      for (int d = -1; d <= 1; d += 2) {
+        i64 q[3] = {p[0], p[1], p[2]};
+        q[a] += d;
+        if (q[a] < 0 || q[a] >= s[a]) continue;
+        const i64 j = at(q);
+        if (!m[j]) { m[j] = 2; queue.push_back(j); }
+      }
+  }
+  for (auto &v : m) v = v == 2 ? 0 : 1;
+}
+
+// Each of the crop's six faces filled as a 2D image, in the order (x, y | z low, high),
+// (x, z | y low, high), (y, z | x low, high) (avocado.cpp:53-66).
+void avocado_walls(std::vector<uint8_t> &m, const i64 s[3]) {
+  const int axes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
+  for (const auto &ax : axes)
+    for (int side = 0; side < 2; ++side) {
+      const i64 ps[3] = {s[ax[0]], s[ax[1]], 1};
+      std::vector<uint8_t> plane(ps[0] * ps[1]);
+      auto voxel = [&](i64 u, i64 v) {
+        i64 p[3];
+        p[ax[0]] = u; p[ax[1]] = v; p[ax[2]] = side ? s[ax[2]] - 1 : 0;
+        return p[0] + s[0] * (p[1] + s[1] * p[2]);
+      };
+      for (i64 v = 0; v < ps[1]; ++v)
+        for (i64 u = 0; u < ps[0]; ++u) plane[u + ps[0] * v] = m[voxel(u, v)];
+      avocado_fill(plane, ps, 2);
+      for (i64 v = 0; v < ps[1]; ++v)
+        for (i64 u = 0; u < ps[0]; ++u) m[voxel(u, v)] = plane[u + ps[0] * v];
+    }
+}
+
+// The rays from `c` (avocado.cpp:67-80): along each axis up (to the last voxel) and down (to
+// coordinate 1), each stops at background or at the first other id (a hit). Fewer than three hits:
+// (pit, pit); else the most hit id (the least such id on ties) owns the pit unless more rays than
+// (one, with four or more hits; none with three) missed it.
+std::pair<i64, i64> avocado_fruit(const std::vector<uint32_t> &ids, const Shape &s, const i64 c[3]) {
+  const i64 pit = ids[s.idx(c[0], c[1], c[2])];
+  std::map<i64, int> hits;
+  int rays = 0;
+  const i64 ext[3] = {s.sx, s.sy, s.sz};
+  for (int a = 0; a < 3; ++a)
+    for (int d : {1, -1}) {
+      i64 p[3] = {c[0], c[1], c[2]};
+      for (; d > 0 ? p[a] < ext[a] : p[a] > 0; p[a] += d) {
+        const i64 v = ids[s.idx(p[0], p[1], p[2])];
+        if (!v) break;
+        if (v != pit) { ++hits[v]; ++rays; break; }
+      }
+    }
+  if (rays < 3) return {pit, pit};
+  i64 owner = pit;
+  int most = 0;
+  for (const auto &h : hits)
+    if (h.second > most) { owner = h.first; most = h.second; }
+  if (rays - most > (rays > 3 ? 1 : 0)) return {pit, pit};
+  return {pit, owner};
+}
+
+// The stage on one volume: cc (ids, mapping, first voxels) and its DBF, both changed in place.
+// Up to 20 passes: the ids holding a voxel beyond threshold / 2.5 that no earlier pass left
+// unchanged are the candidates; each candidate's crop (its box at the pass's start) gets its faces'
+// holes filled, its DBF-weighted argmax is the centre of the rays; a pit merges into its owner
+// (the crop's owner voxels join the mask), and the mask's voids are painted with the owner. A pass
+// that merged something refreshes the DBF. Finally the ids are renumbered by first voxel, each new
+// id mapped to the original label of the old id at its last run start (fastremap's get_mapping).
+// Returns the passes run.
+int fix_avocados(Components &cc, std::vector<float> &dbf, const Shape &s, double threshold, const float aniso[3],
+                 bool bb, int threads) {
+  auto &ids = cc.ids;
+  const i64 n = s.n();
+  const size_t table = cc.mapping.size();
+  const std::vector<uint32_t> original = ids;
+  PySet unchanged;
+  int passes = 0;
+  for (; passes < 20; ++passes) {
+    const float cutoff = float(threshold / 2.5);
+    std::vector<uint8_t> present(table, 0);
+    for (i64 i = 0; i < n; ++i) present[dbf[i] > cutoff ? ids[i] : 0] = 1;
+    PySet candidates;
+    for (size_t id = 0; id < table; ++id) if (present[id]) candidates.add(i64(id));
+    candidates.difference_update(unchanged);
+    candidates.discard(0);
+    if (!candidates.used) break;
+    std::vector<std::array<i64, 6>> box(table, {INT64_MAX, INT64_MAX, INT64_MAX, -1, -1, -1});
+    for (i64 i = 0; i < n; ++i)
+      if (ids[i]) {
+        i64 p[3]; s.xyz(i, p[0], p[1], p[2]);
+        auto &b = box[ids[i]];
+        for (int a = 0; a < 3; ++a) { b[a] = std::min(b[a], p[a]); b[3 + a] = std::max(b[3 + a], p[a]); }
+      }
+    PySet cycle, changed;
+    for (i64 label : candidates.items()) {
+      const auto &b = box[label];
+      const i64 cs[3] = {b[3] - b[0] + 1, b[4] - b[1] + 1, b[5] - b[2] + 1};
+      const i64 cn = cs[0] * cs[1] * cs[2];
+      auto global = [&](i64 c) { return s.idx(b[0] + c % cs[0], b[1] + (c / cs[0]) % cs[1], b[2] + c / (cs[0] * cs[1])); };
+      std::vector<uint8_t> m(cn);
+      for (i64 c = 0; c < cn; ++c) m[c] = ids[global(c)] == uint32_t(label);
+      avocado_walls(m, cs);
+      // np.argmax of mask * dbf over the crop in x-fastest order: the first maximum, a NaN wins
+      i64 best = 0;
+      float maximum = float(m[0]) * dbf[global(0)];
+      for (i64 c = 0; c < cn; ++c) {
+        const float v = float(m[c]) * dbf[global(c)];
+        if (!(v <= maximum) && !std::isnan(maximum)) { maximum = v; best = c; }
+      }
+      const i64 centre[3] = {b[0] + best % cs[0], b[1] + (best / cs[0]) % cs[1], b[2] + best / (cs[0] * cs[1])};
+      const auto [pit, owner] = avocado_fruit(ids, s, centre);
+      if (pit == owner && !changed.contains(pit)) cycle.add(pit);
+      else {
+        cycle.discard(pit); cycle.discard(owner);
+        changed.add(pit); changed.add(owner);
+        for (i64 c = 0; c < cn; ++c) m[c] |= ids[global(c)] == uint32_t(owner);
+      }
+      avocado_fill(m, cs, 3);
+      for (i64 c = 0; c < cn; ++c) if (m[c]) ids[global(c)] = uint32_t(owner);
+    }
+    unchanged.update(cycle);
+    if (!changed.used) { ++passes; break; }
+    dbf = edt(ids.data(), s, aniso, bb, 3, threads);
+  }
+  // renumbering by first voxel (avocado.cpp:117-131)
+  std::vector<i64> compact(table, 0);
+  std::vector<int64_t> mapping{0}, roots;
+  i64 previous = -1;
+  for (i64 i = 0; i < n; ++i) {
+    i64 &k = compact[ids[i]];
+    if (ids[i] && !k) { k = i64(roots.size()) + 1; roots.push_back(i); mapping.push_back(0); }
+    ids[i] = uint32_t(k);
+    if (k != previous) {
+      if (k) mapping[k] = original[i] ? cc.mapping[original[i]] : 0;
+      previous = k;
+    }
+  }
+  cc.mapping = std::move(mapping);
+  cc.roots = std::move(roots);
+  return passes;
+}
+
 // The soma root (trace.cu:55-73, batched.cu:58-105): among the voxels at the DBF maximum, sorted
 // by (x, y, z), the first nearest (float64 squared distance, voxel units) to their float32 centroid.
 i64 soma_root(const std::vector<float> &dbf, const std::vector<i64> &voxels, float maximum, const Shape &s) {
@@ -1006,6 +1262,7 @@ struct Result {
   std::vector<uint32_t> edges;
   std::string error;
   int64_t filled = 0;  // voxels fill_holes filled
+  int64_t avocado_passes = 0;
   // stage outputs
   Components cc;
   std::vector<float> dbf, daf, pdrf;
@@ -1065,49 +1322,44 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
   R.cc = components_any(labels, dtype, s, threads);
   R.stage_ms[0] = lap.next();
   const auto &ids = R.cc.ids;
-  const size_t count = R.cc.roots.size();
+  size_t count = R.cc.roots.size();
   if (!count) return;
-  // bounding boxes and counts (preamble.cu:10-29)
+  // bounding boxes and counts (preamble.cu:10-29), and each id's voxels; with `refresh_first` the
+  // first voxels too (preamble.cu:77-90: an id left without voxels keeps its old one)
   auto &box = st->box;
-  box.assign(count + 1, {INT32_MAX, INT32_MAX, INT32_MAX, -1, -1, -1, 0});
-  std::vector<std::vector<i64>> voxels(count + 1);
-  for (i64 v = 0; v < n; ++v) {
-    const uint32_t id = ids[v];
-    if (!id) continue;
-    i64 x, y, z; s.xyz(v, x, y, z);
-    auto &b = box[id];
-    b[0] = std::min(b[0], x); b[1] = std::min(b[1], y); b[2] = std::min(b[2], z);
-    b[3] = std::max(b[3], x); b[4] = std::max(b[4], y); b[5] = std::max(b[5], z); ++b[6];
-    voxels[id].push_back(v);
-  }
+  std::vector<std::vector<i64>> voxels;
+  auto analyze_ids = [&](bool refresh_first) {
+    box.assign(count + 1, {INT32_MAX, INT32_MAX, INT32_MAX, -1, -1, -1, 0});
+    voxels.assign(count + 1, {});
+    for (i64 v = 0; v < n; ++v) {
+      const uint32_t id = ids[v];
+      if (!id) continue;
+      i64 x, y, z; s.xyz(v, x, y, z);
+      auto &b = box[id];
+      b[0] = std::min(b[0], x); b[1] = std::min(b[1], y); b[2] = std::min(b[2], z);
+      b[3] = std::max(b[3], x); b[4] = std::max(b[4], y); b[5] = std::max(b[5], z); ++b[6];
+      if (refresh_first && voxels[id].empty()) R.cc.roots[id - 1] = v;
+      voxels[id].push_back(v);
+    }
+  };
+  analyze_ids(false);
   R.stage_ms[1] = lap.next();
   // black border from the volume as given, before any hole is filled (skeletonize.cu:82-85)
   const bool black_border = count == 1 && box[1][6] == n;
   if (P.fill_holes) {
     R.filled = fill_all_holes(R.cc.ids, s, box);
-    if (R.filled) {
-      // the boxes, voxel lists and first voxels again (preamble.cu:77-90): a component whose
-      // voxels were all painted keeps its old first voxel and has no voxels
-      box.assign(count + 1, {INT32_MAX, INT32_MAX, INT32_MAX, -1, -1, -1, 0});
-      for (auto &list : voxels) list.clear();
-      std::vector<i64> first(count + 1, -1);
-      for (i64 v = 0; v < n; ++v) {
-        const uint32_t id = ids[v];
-        if (!id) continue;
-        i64 x, y, z; s.xyz(v, x, y, z);
-        auto &b = box[id];
-        b[0] = std::min(b[0], x); b[1] = std::min(b[1], y); b[2] = std::min(b[2], z);
-        b[3] = std::max(b[3], x); b[4] = std::max(b[4], y); b[5] = std::max(b[5], z); ++b[6];
-        voxels[id].push_back(v);
-        if (first[id] < 0) first[id] = v;
-      }
-      for (size_t id = 1; id <= count; ++id)
-        if (first[id] >= 0) R.cc.roots[id - 1] = first[id];
-    }
+    if (R.filled) analyze_ids(true);
   }
   Volume &V = st->V;
   V.s = s; V.ids = &R.cc.ids;
   V.dbf = edt(ids.data(), s, P.anisotropy, black_border, 3, threads);
+  if (P.fix_avocados) {
+    // the avocado stage (skeletonize.cu:92-96): ids renumbered, the field refreshed when it merged
+    R.avocado_passes = fix_avocados(R.cc, V.dbf, s, P.soma_detection, P.anisotropy, black_border, threads);
+    count = R.cc.roots.size();
+    if (!count) return;
+    analyze_ids(false);
+  }
   R.stage_ms[2] = lap.next();
   std::vector<std::vector<std::array<i64, 3>>> borders(count + 1);
   if (P.fix_borders) borders = border_targets(ids, s, count, P.anisotropy);
@@ -1330,6 +1582,11 @@ void prepare(Result &R, const void *labels, int dtype, const Shape &s, const Par
   });
   for (auto &plan : soma_plans) plans.push_back(std::move(plan));
   R.stage_ms[6] = lap.next();
+  // A foreground voxel at distance zero (background the avocado stage painted without refreshing
+  // the field) is +inf to the tracer: its penalty (above), invalidation reach and radius
+  // (lockstep.cu:61-82).
+  for (i64 i = 0; i < n; ++i)
+    if (ids[i] && V.dbf[i] == 0.0f) V.dbf[i] = kInf;
   V.dist.assign(n, kInf);
   V.alive.assign(n, 0);
   for (i64 i = 0; i < n; ++i) V.alive[i] = ids[i] ? active[ids[i]] && !candidate[ids[i]] : 0;
@@ -1462,6 +1719,7 @@ struct oracle_params {
   const int64_t *targets_after; int64_t n_after;
   const float *pdrf_field;  // optional (null: computed)
   int32_t fill_holes;
+  int32_t fix_avocados;
 };
 
 namespace {
@@ -1479,6 +1737,7 @@ Params params_of(const oracle_params *p) {
       P.after.push_back({p->targets_after[3 * i], p->targets_after[3 * i + 1], p->targets_after[3 * i + 2]});
     P.pdrf_field = p->pdrf_field;
     P.fill_holes = p->fill_holes;
+    P.fix_avocados = p->fix_avocados;
     return P;
 }
 }  // namespace
@@ -1567,6 +1826,7 @@ const void *oracle_array(void *h, const char *name, int64_t *count) {
   if (k == "path_labels") return give(r->path_labels);
   if (k == "stage_ms") return give(r->stage_ms);
   if (k == "filled") { *count = 1; return &r->filled; }
+  if (k == "avocado_passes") { *count = 1; return &r->avocado_passes; }
   *count = -1;
   return nullptr;
 }
@@ -1617,6 +1877,24 @@ int oracle_railroad_distances(const float *field, const uint32_t *labels, int64_
     std::copy(V.dist.begin(), V.dist.end(), dist_out);
     return 0;
   } catch (...) { return 1; }
+}
+// The CPython set restatement on a script of operations (code, key) pairs: 0 add to A, 1 discard
+// from A, 2 add to B, 3 A -= B (B emptied), 4 A |= B (B emptied), 5 A emptied. Writes A's
+// iteration order; returns its size.
+int64_t oracle_pyset(const int64_t *ops, int64_t n, int64_t *out, int64_t capacity) {
+  PySet A, B;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t code = ops[2 * i], key = ops[2 * i + 1];
+    if (code == 0) A.add(key);
+    else if (code == 1) A.discard(key);
+    else if (code == 2) B.add(key);
+    else if (code == 3) { A.difference_update(B); B = PySet(); }
+    else if (code == 4) { A.update(B); B = PySet(); }
+    else A = PySet();
+  }
+  const auto items = A.items();
+  for (size_t i = 0; i < items.size() && int64_t(i) < capacity; ++i) out[i] = items[i];
+  return int64_t(items.size());
 }
 // Target order rule on a flat (mask, daf) pair: descending daf (inf -> 0), ties -> higher index.
 int64_t oracle_target_order(const uint8_t *mask, const float *daf, int64_t n, int64_t *out) {

@@ -26,7 +26,7 @@ class _Params(ctypes.Structure):
                 ("fix_borders", ctypes.c_int32), ("targets_before", ctypes.POINTER(ctypes.c_int64)),
                 ("n_before", ctypes.c_int64), ("targets_after", ctypes.POINTER(ctypes.c_int64)),
                 ("n_after", ctypes.c_int64), ("pdrf_field", ctypes.POINTER(ctypes.c_float)),
-                ("fill_holes", ctypes.c_int32)]
+                ("fill_holes", ctypes.c_int32), ("fix_avocados", ctypes.c_int32)]
 
 
 _lib = None
@@ -61,6 +61,8 @@ def lib():
         _lib.oracle_railroad_distances.restype = ctypes.c_int
         _lib.oracle_railroad_distances.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                                    ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p]
+        _lib.oracle_pyset.restype = ctypes.c_int64
+        _lib.oracle_pyset.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]
         _lib.oracle_target_order.restype = ctypes.c_int64
         _lib.oracle_target_order.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
         _lib.oracle_prepare.restype = ctypes.c_void_p
@@ -85,7 +87,7 @@ _ARRAY_TYPES = {"labels": np.int64, "vertex_offsets": np.int64, "edge_offsets": 
                 "dbf": np.float32, "daf": np.float32, "pdrf": np.float32, "roots": np.int64, "targets": np.int64,
                 "boxes": np.int64, "orders": np.int64, "order_offsets": np.int64, "paths": np.int64,
                 "path_offsets": np.int64, "path_labels": np.int64, "stage_ms": np.float64,
-                "filled": np.int64}
+                "filled": np.int64, "avocado_passes": np.int64}
 
 # names of the entries of OracleResult.array("stage_ms"): wall-clock ms of each step
 STAGES = ("components", "boxes", "edt", "borders", "daf", "pdrf", "orders", "trace", "assembly")
@@ -168,12 +170,13 @@ DEFAULT_TEASAR_PARAMS = dict(scale=1.5, const=300, pdrf_scale=100000, pdrf_expon
 
 def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1), dust_threshold=1000,
                 fix_branching=True, fix_borders=True, threads=1, stages=False, extra_targets_before=(),
-                extra_targets_after=(), pdrf_field=None, fill_holes=False):
+                extra_targets_after=(), pdrf_field=None, fill_holes=False, fix_avocados=False):
     """Run the oracle on a 3D label volume (any layout; read as its logical (x, y, z) axes), with
     the argument defaults of the reference's brook.skeletonize. `pdrf_field` (float32, the
     volume's shape) replaces the oracle's own PDRF over the traced objects: a test traces from
     another implementation's field where the power itself is not bit-reproducible (an exponent
-    that is not a power of two). With `fill_holes`, array("filled") holds the voxels filled."""
+    that is not a power of two). With `fill_holes`, array("filled") holds the voxels filled; with
+    `fix_avocados`, array("avocado_passes") the avocado stage's passes."""
     labels = np.asarray(labels)
     if labels.dtype == bool:
         labels = labels.view(np.uint8)
@@ -184,6 +187,7 @@ def skeletonize(labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 1, 1
         raise TypeError(f"unsupported label dtype {labels.dtype}")
     params = _params(teasar_params or {}, anisotropy, dust_threshold, fix_branching, fix_borders)
     params.fill_holes = int(bool(fill_holes))
+    params.fix_avocados = int(bool(fix_avocados))
     keep = []
     for name, points in (("targets_before", extra_targets_before), ("targets_after", extra_targets_after)):
         pts = np.ascontiguousarray(np.asarray(list(points), np.int64).reshape(-1, 3))
@@ -265,6 +269,14 @@ def railroad_distances(field, target, component=None):
     if lib().oracle_railroad_distances(field.ctypes.data, comp.ctypes.data, *field.shape, int(target), out.ctypes.data):
         raise RuntimeError("oracle railroad failed")
     return out
+
+
+def pyset_order(ops):
+    """The iteration order of set A after a script of (code, key) operations (oracle_pyset)."""
+    ops = np.ascontiguousarray(np.asarray(ops, np.int64).reshape(-1, 2))
+    out = np.zeros(max(len(ops), 1), np.int64)
+    n = lib().oracle_pyset(ops.ctypes.data, len(ops), out.ctypes.data, out.size)
+    return out[:n].tolist()
 
 
 def target_order(mask, daf):
