@@ -8,30 +8,78 @@
 namespace bk {
 namespace {
 
-// Boxes and counts in one pass (the reference's analyze, preamble.cu:10-29): a run start along x
-// updates the box, a run end its x maximum, and each warp adds its voxels of one id with one
-// atomic (match + popc).
-__global__ void analyze_kernel(const uint32_t *__restrict__ ids, Dims d, int *lo, int *hi, unsigned long long *counts) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = i < d.n();
-  const uint32_t id = in ? ids[i] : 0u;
-  const unsigned peers = __match_any_sync(0xFFFFFFFFu, id);
-  const int leader = __ffs(peers) - 1;
-  if (id != 0 && (threadIdx.x & 31) == leader) atomicAdd(counts + id, (unsigned long long)__popc(peers));
-  if (!in || id == 0) return;
-  int x, y, z;
-  unravel((int)i, d, x, y, z);
-  const bool first = x == 0 || ids[i - 1] != id;
-  const bool last = x == d.sx - 1 || ids[i + 1] != id;
-  int *l = lo + 3 * (long long)id, *h = hi + 3 * (long long)id;
-  if (first) {
-    if (__ldcg(l) > x) atomicMin(l, x);
-    if (__ldcg(l + 1) > y) atomicMin(l + 1, y);
-    if (__ldcg(h + 1) < y) atomicMax(h + 1, y);
-    if (__ldcg(l + 2) > z) atomicMin(l + 2, z);
-    if (__ldcg(h + 2) < z) atomicMax(h + 2, z);
+// Boxes and counts in one pass (the reference's analyze, preamble.cu:10-29). A block takes
+// kChunk consecutive voxels (each warp 32 at a time, coalesced); a warp's voxels of one id are
+// reduced with match + redux (count, low and high x, y, z) and merged into the block's table of
+// kSlots ids in shared memory; the table then goes to the global boxes with one guarded atomic
+// per field and id (an id the table cannot take goes there directly). Dense volumes hold a few ids
+// per chunk, so the global atomics fall from one per row run to one per chunk.
+constexpr int kChunk = 2048, kSlots = 64;
+
+__device__ __forceinline__ int table_slot(uint32_t *keys, uint32_t id) {
+  int h = int((id * 0x9E3779B1u) >> 26);  // kSlots = 64
+  for (int probe = 0; probe < kSlots; ++probe, h = (h + 1) & (kSlots - 1)) {
+    const uint32_t k = keys[h];
+    if (k == id) return h;
+    if (k == 0) {
+      const uint32_t prev = atomicCAS(keys + h, 0u, id);
+      if (prev == 0u || prev == id) return h;
+    }
   }
-  if (last && __ldcg(h) < x) atomicMax(h, x);
+  return -1;
+}
+
+__device__ __forceinline__ void box_update(int *l, int *h, unsigned long long *count, const int lo[3], const int hi[3],
+                                           unsigned n) {
+  atomicAdd(count, (unsigned long long)n);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (__ldcg(l + a) > lo[a]) atomicMin(l + a, lo[a]);
+    if (__ldcg(h + a) < hi[a]) atomicMax(h + a, hi[a]);
+  }
+}
+
+__global__ void __launch_bounds__(256) analyze_kernel(const uint32_t *__restrict__ ids, Dims d, int *lo, int *hi,
+                                                      unsigned long long *counts) {
+  __shared__ uint32_t keys[kSlots];
+  __shared__ unsigned cnt[kSlots];
+  __shared__ int slo[kSlots][3], shi[kSlots][3];
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) {
+    keys[t] = 0;
+    cnt[t] = 0;
+    for (int a = 0; a < 3; ++a) { slo[t][a] = INT32_MAX; shi[t][a] = -1; }
+  }
+  __syncthreads();
+  const long long n = d.n(), begin = (long long)blockIdx.x * kChunk;
+  const int lane = threadIdx.x & 31;
+  for (long long i = begin + threadIdx.x; i < begin + kChunk; i += blockDim.x) {  // warp-uniform bounds
+    const bool in = i < n;
+    const uint32_t id = in ? ids[i] : 0u;
+    int x = 0, y = 0, z = 0;
+    if (in) unravel((int)i, d, x, y, z);
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, id);
+    const int lx = int(__reduce_min_sync(peers, unsigned(x))), hx = int(__reduce_max_sync(peers, unsigned(x)));
+    const int ly = int(__reduce_min_sync(peers, unsigned(y))), hy = int(__reduce_max_sync(peers, unsigned(y)));
+    const int lz = int(__reduce_min_sync(peers, unsigned(z))), hz = int(__reduce_max_sync(peers, unsigned(z)));
+    if (id == 0 || lane != __ffs(peers) - 1) continue;
+    const int l3[3] = {lx, ly, lz}, h3[3] = {hx, hy, hz};
+    const int slot = table_slot(keys, id);
+    if (slot < 0) {
+      box_update(lo + 3 * (long long)id, hi + 3 * (long long)id, counts + id, l3, h3, __popc(peers));
+      continue;
+    }
+    atomicAdd(cnt + slot, unsigned(__popc(peers)));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(&slo[slot][a], l3[a]);
+      atomicMax(&shi[slot][a], h3[a]);
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) {
+    const uint32_t id = keys[t];
+    if (id) box_update(lo + 3 * (long long)id, hi + 3 * (long long)id, counts + id, slo[t], shi[t], cnt[t]);
+  }
 }
 
 // The mask of a 32x8x8 block of voxels from a shared-memory copy of the block's ids with a
@@ -68,15 +116,46 @@ __global__ void __launch_bounds__(kMaskX * kMaskY) mask_kernel(const uint32_t *_
   }
 }
 
-__global__ void segmax_kernel(const float *__restrict__ f, const uint32_t *__restrict__ ids, long long n, unsigned *best) {
+// Per id the largest finite field value (as float bits), by the same block tables as analyze:
+// the warp's maximum of an id (match + redux), then the block's, then one guarded atomic per id
+// and block.
+__global__ void __launch_bounds__(256) segmax_kernel(const float *__restrict__ f, const uint32_t *__restrict__ ids,
+                                                     long long n, unsigned *best) {
+  __shared__ uint32_t keys[kSlots];
+  __shared__ unsigned top[kSlots];
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) { keys[t] = 0; top[t] = 0; }
+  __syncthreads();
+  const long long begin = (long long)blockIdx.x * kChunk;
+  const int lane = threadIdx.x & 31;
+  for (long long i = begin + threadIdx.x; i < begin + kChunk; i += blockDim.x) {
+    const bool in = i < n;
+    const uint32_t id = in ? ids[i] : 0u;
+    const float v = in ? f[i] : 0.0f;
+    const unsigned bits = (id != 0 && v < __uint_as_float(BK_INF_BITS)) ? __float_as_uint(v) : 0u;
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, id);
+    const unsigned m = __reduce_max_sync(peers, bits);  // the largest bits of this warp's voxels of the id
+    if (id == 0 || lane != __ffs(peers) - 1) continue;
+    const int slot = table_slot(keys, id);
+    if (slot < 0) {
+      if (__ldcg(best + id) < m) atomicMax(best + id, m);
+    } else {
+      atomicMax(top + slot, m);
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) {
+    const uint32_t id = keys[t];
+    if (id && __ldcg(best + id) < top[t]) atomicMax(best + id, top[t]);
+  }
+}
+
+__global__ void zero_to_inf_kernel(const uint32_t *__restrict__ ids, float *__restrict__ f, long long n,
+                                   unsigned long long *count) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = i < n;
-  const uint32_t id = in ? ids[i] : 0u;
-  const float v = in ? f[i] : 0.0f;
-  const unsigned bits = (id != 0 && v < __uint_as_float(BK_INF_BITS)) ? __float_as_uint(v) : 0u;
-  const unsigned peers = __match_any_sync(0xFFFFFFFFu, id);
-  const unsigned top = __reduce_max_sync(peers, bits);  // the largest bits of this warp's voxels of the id
-  if (id != 0 && (threadIdx.x & 31) == __ffs(peers) - 1 && __ldcg(best + id) < top) atomicMax(best + id, top);
+  const bool hit = i < n && ids[i] != 0 && f[i] == 0.0f;
+  if (hit) f[i] = __uint_as_float(BK_INF_BITS);
+  const unsigned many = __popc(__ballot_sync(0xFFFFFFFFu, hit));
+  if (many && (threadIdx.x & 31) == 0) atomicAdd(count, (unsigned long long)many);
 }
 
 __global__ void fill_kernel(float *p, long long n, float v) {
@@ -165,7 +244,7 @@ std::vector<Box> analyze(Context &ctx, const uint32_t *ids, VolumeDims vd, int64
   Buffer<int> dlo = to_device(ctx, lo), dhi = to_device(ctx, hi);
   Buffer<unsigned long long> counts(ctx, count + 1);
   counts.zero();
-  analyze_kernel<<<blocks_for(vd.n()), 256, 0, ctx.stream()>>>(ids, d, dlo.data(), dhi.data(), counts.data()); ++ctx.launches;
+  analyze_kernel<<<blocks_for(vd.n(), kChunk), 256, 0, ctx.stream()>>>(ids, d, dlo.data(), dhi.data(), counts.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   lo = dlo.download();
   hi = dhi.download();
@@ -199,7 +278,7 @@ std::vector<std::vector<Box>> analyze(Context &ctx, const uint32_t *ids, const s
   for (size_t v = 0; v < volumes.size(); ++v) {
     const auto &iv = volumes[v];
     if (!iv.d.n() || !iv.count) continue;
-    analyze_kernel<<<blocks_for(iv.d.n()), 256, 0, s>>>(ids + iv.offset, Dims{iv.d.sx, iv.d.sy, iv.d.sz},
+    analyze_kernel<<<blocks_for(iv.d.n(), kChunk), 256, 0, s>>>(ids + iv.offset, Dims{iv.d.sx, iv.d.sy, iv.d.sz},
                                                         dlo.data() + 3 * base[v], dhi.data() + 3 * base[v],
                                                         counts.data() + base[v]); ++ctx.launches;
   }
@@ -231,7 +310,7 @@ std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, co
   for (size_t v = 0; v < volumes.size(); ++v) {
     const auto &iv = volumes[v];
     if (!iv.d.n() || !iv.count) continue;
-    segmax_kernel<<<blocks_for(iv.d.n()), 256, 0, ctx.stream()>>>(field + iv.offset, ids + iv.offset, iv.d.n(),
+    segmax_kernel<<<blocks_for(iv.d.n(), kChunk), 256, 0, ctx.stream()>>>(field + iv.offset, ids + iv.offset, iv.d.n(),
                                                                   best.data() + base[v]); ++ctx.launches;
   }
   BK_CUDA(cudaGetLastError());
@@ -247,12 +326,21 @@ std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, co
 std::vector<float> segment_max(Context &ctx, const float *field, const uint32_t *ids, long long n, int64_t count) {
   Buffer<unsigned> best(ctx, count + 1);
   best.zero();
-  segmax_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(field, ids, n, best.data()); ++ctx.launches;
+  segmax_kernel<<<blocks_for(n, kChunk), 256, 0, ctx.stream()>>>(field, ids, n, best.data()); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   auto bits = best.download();
   std::vector<float> out(count + 1);
   std::memcpy(out.data(), bits.data(), bits.size() * sizeof(float));
   return out;
+}
+
+long long zero_distances_to_infinity(Context &ctx, const uint32_t *ids, float *dbf, long long n) {
+  if (n <= 0) return 0;
+  Buffer<unsigned long long> count(ctx, 1);
+  count.zero();
+  zero_to_inf_kernel<<<blocks_for(n), 256, 0, ctx.stream()>>>(ids, dbf, n, count.data()); ++ctx.launches;
+  BK_CUDA(cudaGetLastError());
+  return (long long)count.download(1)[0];
 }
 
 void fill_float(Context &ctx, float *p, long long n, float value) {
