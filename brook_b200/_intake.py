@@ -110,18 +110,21 @@ def device_volume(labels):
 
 
 def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
-         extra_after, device, device_output=False, producers=(), sample_targets=None, fill_holes=False):
+         extra_after, device, device_output=False, producers=(), sample_targets=None, fill_holes=False,
+         fix_avocados=False):
     """One C call over `volumes`, as PackedSkeletons. producers: stream handles the library's
     stream waits for first (the producers of device inputs). sample_targets: per volume (before,
     after) point lists of a batch (extra_before / extra_after then stay empty)."""
     handles = _run_handles(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders,
-                           extra_before, extra_after, device, device_output, producers, sample_targets, fill_holes)
+                           extra_before, extra_after, device, device_output, producers, sample_targets, fill_holes,
+                           fix_avocados)
     grab = _native.packed_device_arrays if device_output else _native.packed_arrays
     return [PackedSkeletons.from_arrays(grab(h)) for h in handles]
 
 
 def _run_handles(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
-                 extra_after, device, device_output=False, producers=(), sample_targets=None, fill_holes=False):
+                 extra_after, device, device_output=False, producers=(), sample_targets=None, fill_holes=False,
+                 fix_avocados=False):
     """_run's C call; returns the raw result handles (the caller destroys them)."""
     ctypes = _native.ctypes
     opts = _native.options(params, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids,
@@ -130,6 +133,8 @@ def _run_handles(volumes, params, anisotropy, object_ids, dust_threshold, fix_br
         opts.flags |= _native.DEVICE_OUTPUT
     if fill_holes:
         opts.flags |= _native.FILL_HOLES
+    if fix_avocados:
+        opts.flags |= _native.FIX_AVOCADOS
     lib = _native.load()
     ctx = _native.context(device)
     for handle in dict.fromkeys(producers):
@@ -170,14 +175,16 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     or torch.cuda.Stream; default: the array's own CUDA array interface stream, torch's current
     stream for a torch tensor, else the legacy default stream). `fill_holes` fills every
     component's voids before the distance transform (the reference's rule: components in
-    ascending id, a component whose voxels an earlier fill painted is not filled). `parallel`,
+    ascending id, a component whose voxels an earlier fill painted is not filled);
+    `fix_avocados` merges pits (an object whose distance field passes soma_detection_threshold / 2.5
+    and that another object encloses) into the objects around them (Kimimaro's rule). `parallel`,
     `parallel_chunk_size`, `in_place`, `progress`, `borrow` and `streaming` are accepted for
-    compatibility. `fix_avocados` and `voxel_graph` are not supported by this build and raise.
+    compatibility. `voxel_graph` is not supported by this build and raises.
     """
     if output not in ("skeletons", "packed", "packed_device"):
         raise ValueError("brook_b200: output must be 'skeletons', 'packed' or 'packed_device'")
-    if fix_avocados or voxel_graph is not None:
-        raise NotImplementedError("brook_b200: fix_avocados and voxel_graph are not supported")
+    if voxel_graph is not None:
+        raise NotImplementedError("brook_b200: voxel_graph is not supported")
     params = teasar(teasar_params)
     anisotropy = tuple(float(a) for a in np.asarray(anisotropy, dtype=np.float32))
     producers = []
@@ -194,7 +201,8 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     packed = _run([volume], params, anisotropy, ids, dust_threshold, fix_branching, fix_borders,
                   [tuple(int(c) for c in p) for p in extra_targets_before],
                   [tuple(int(c) for c in p) for p in extra_targets_after], device,
-                  device_output=output == "packed_device", producers=producers, fill_holes=fill_holes)[0]
+                  device_output=output == "packed_device", producers=producers, fill_holes=fill_holes,
+                  fix_avocados=fix_avocados)[0]
     del keep
     if output == "skeletons":
         return packed.to_skeletons()

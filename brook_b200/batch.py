@@ -148,8 +148,8 @@ def skeletonize_batch(samples, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(
     ("packed"), or a list of {label: Skeleton} dicts ("skeletons")."""
     if output not in ("packed_device", "packed", "skeletons"):
         raise ValueError("brook_b200: output must be 'packed_device', 'packed' or 'skeletons'")
-    if fix_avocados or voxel_graph is not None:
-        raise NotImplementedError("brook_b200: fix_avocados and voxel_graph are not supported")
+    if voxel_graph is not None:
+        raise NotImplementedError("brook_b200: voxel_graph is not supported")
     if isinstance(samples, np.ndarray) and samples.ndim == 4:
         samples = list(samples)
     samples = list(samples)
@@ -172,7 +172,7 @@ def skeletonize_batch(samples, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(
         keep.append(k)
     parts = _run(volumes, params, anisotropy, None, dust_threshold, fix_branching, fix_borders, [], [], device,
                  device_output=output == "packed_device", producers=producers, sample_targets=targets,
-                 fill_holes=fill_holes) \
+                 fill_holes=fill_holes, fix_avocados=fix_avocados) \
         if volumes else []
     result = BatchedSkeletons.concatenate(parts, anisotropy)
     if output == "skeletons":

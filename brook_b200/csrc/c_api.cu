@@ -214,7 +214,6 @@ bk::Options options_of(const brook_skeletonize_options *p) {
   const uint32_t known = BROOK_FIX_BRANCHING | BROOK_FIX_BORDERS | BROOK_FILTER_OBJECTS | BROOK_DEVICE_OUTPUT |
                          BROOK_FILL_HOLES | BROOK_FIX_AVOCADOS;
   require(!(p->flags & ~known), "unknown skeletonization flags");
-  if (p->flags & BROOK_FIX_AVOCADOS) throw std::invalid_argument("fix_avocados is not supported by this build");
   if (p->voxel_graph) throw std::invalid_argument("voxel_graph is not supported by this build");
   bk::Options o;
   auto &t = o.teasar;
@@ -233,6 +232,7 @@ bk::Options options_of(const brook_skeletonize_options *p) {
   o.fix_borders = (p->flags & BROOK_FIX_BORDERS) != 0;
   o.device_output = (p->flags & BROOK_DEVICE_OUTPUT) != 0;
   o.fill_holes = (p->flags & BROOK_FILL_HOLES) != 0;
+  o.fix_avocados = (p->flags & BROOK_FIX_AVOCADOS) != 0;
   if (p->flags & BROOK_FILTER_OBJECTS) {
     require(p->object_ids || !p->object_ids_count);
     o.object_ids = std::vector<int64_t>(p->object_ids, p->object_ids + p->object_ids_count);

@@ -54,6 +54,7 @@ struct Shared {
   double soma_radius;
   int root, step;
   float rscale, rconst;  // invalidation: reach = rscale * DBF[source] + rconst
+  int skipped;           // manual targets from which no rail was reachable (empty paths)
 };
 
 __device__ __forceinline__ float inf() { return __uint_as_float(BK_INF_BITS); }
@@ -537,7 +538,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
       else if (minfar == kMinFarNone) L->flag = 2;
       else {
         const float d = __uint_as_float(unsigned(minfar >> 32)), f = __uint_as_float(unsigned(minfar));
-        float w = __fmul_rn(2.0f, f);
+        float w = __fmul_rn(a.rail_band, f);
         const float lo = __fmul_rn(5e-4f, d);
         if (!(w > lo)) w = lo;
         L->T = __fadd_rn(d, w);
@@ -1007,17 +1008,20 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
       sh.root = a.root[o];
       sh.soma_radius = a.soma_radius[o];
       sh.step = sh.soma_radius >= 0.0 ? 0 : (a.fix_branching ? 2 : 1);
+      sh.skipped = 0;
     }
     __syncthreads();
     while (status == kOk) {
       const int step = sh.step;  // 0: the soma's ball, 1: the parents' field, 2: paths
       int t = -1, len = 1;
+      bool ordered = false;  // t is the first alive voxel of the DAF order
       if (step == 2) {
-        if (paths >= maxp) break;
+        const long long taken = paths + sh.skipped;  // targets taken so far, empty paths included
+        if (taken >= maxp) break;
         // the next target: manual targets first, then the first alive voxel of the order, then the
         // targets after (trace.cu:209-212)
-        if (paths < mcount) {
-          t = manual[paths];
+        if (taken < mcount) {
+          t = manual[taken];
           if (t < 0) t = a.target[o];  // the object's own target (the DAF argmax)
         } else {
           for (;;) {
@@ -1028,7 +1032,7 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
             G::sync();
             const int found = int(G::min_over(&sh.pos));
             G::sync();
-            if (found != INT32_MAX) { cursor = found; t = order[found]; break; }
+            if (found != INT32_MAX) { cursor = found; t = order[found]; ordered = true; break; }
             cursor += G::threads();
             if (cursor >= sh.count) { cursor = sh.count; break; }
           }
@@ -1052,7 +1056,22 @@ __device__ void trace_loop(const EngineArgs &a, bool big) {
           G::sync();
           continue;
         }
-        if (rb == BK_UNCLAIMED) { status = kNoRail; break; }
+        if (rb == BK_UNCLAIMED) {
+          // No rail is reachable from t: an infinite penalty walls it off (a cavity the avocado
+          // stage painted without refreshing the field). A target of the DAF order would be picked
+          // again and again, so the object ends here (trace.cu:218-224); a manual target leaves an
+          // empty path. Either way the flood's state goes back to rest first.
+          for (int i = G::tid(); i < nt; i += G::threads()) {
+            const int v = __ldcg(L4 + i);
+            a.dist[v] = inf();
+            atomicAnd(a.flags + v, ~(kNearQueued | kFarQueued));
+          }
+          if (G::first()) s_work[1] += nt;
+          if (threadIdx.x == 0 && !ordered) sh.skipped += 1;  // every CTA keeps its own copy
+          G::sync();
+          if (ordered) break;
+          continue;
+        }
         // walk (one warp of the first CTA), then reset the flood's state over the voxels it touched
         if (G::rank() == 0 && threadIdx.x < 32) {
           const int n = backtrace(a, sh, rb, t, store + used, store_cap - used);

@@ -98,6 +98,10 @@ struct EngineArgs {
   // that does not end; the cap lets a test make one run out and check that the call fails with
   // kBudget and leaves the device usable.
   long long round_limit;
+  // The railroad's band past the nearest deferred voxel: its distance plus rail_band times its
+  // penalty (at least 5e-4 of the distance). Any band gives the same distances; wider bands take
+  // fewer band ends and more re-relaxations.
+  float rail_band;
 };
 
 // Objects with at least kPrepareClusterVoxels voxels (preparation) or more voxels than
@@ -124,6 +128,8 @@ void launch_prepare(const EngineArgs &a, int nbig, int cluster_ctas, cudaStream_
 // lone_percent: the share of clusters (percent) whose CTAs take small objects first.
 void launch_trace(const EngineArgs &a, int nbig, int cluster_ctas, int lone_percent, cudaStream_t stream);
 constexpr int kLoneFirstPercent = 10;
+// The railroad band's width in penalties of the nearest deferred voxel (EngineArgs::rail_band).
+constexpr float kRailBand = 2.0f;
 // The device queries the launches above make (resident clusters per kernel), done ahead so that
 // a stream capture of the launches holds launches only.
 void prepare_engine_launches(int cluster_ctas, cudaStream_t stream);

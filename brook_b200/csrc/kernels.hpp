@@ -91,6 +91,17 @@ struct HoleVolume {
   const std::vector<Box> *boxes;
 };
 long long fill_holes(Context &ctx, uint32_t *ids, const std::vector<HoleVolume> &volumes);
+
+// ---- the avocado stage (avocado.cpp) ----
+// One volume's component ids (ids, device, 1..cc.count) and distance field (dbf, device) after the
+// reference's fix_avocados: pits merged into the objects around them, ids renumbered by first voxel
+// (cc's count, mapping and first voxels follow), the field refreshed by the EDT when a pass merged.
+// Returns the passes run.
+int fix_avocados(Context &ctx, uint32_t *ids, float *dbf, VolumeDims d, ComponentsResult &cc, double threshold,
+                 const float aniso[3], bool black_border);
+// A foreground voxel at distance zero (background the avocado stage painted without a refresh)
+// becomes +inf: the tracer's penalty, invalidation reach and radius. Returns how many there were.
+long long zero_distances_to_infinity(Context &ctx, const uint32_t *ids, float *dbf, long long n);
 std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, const uint32_t *ids,
                                             const std::vector<IdVolume> &volumes);
 // 26-bit same-id neighbour mask of every voxel (0 for background).

@@ -280,6 +280,27 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     edt_volumes(ctx, ids.data(), ev, aniso, dbf.data());
     clock.mark("edt");
   }
+  // ---- the avocado stage per volume (skeletonize.cu:92-96): pits merged into the objects around
+  // them, ids renumbered, the field refreshed where a pass merged; then boxes and counts again
+  if (opt.fix_avocados) {
+    int passes = 0;
+    std::vector<IdVolume> iv;
+    std::vector<size_t> which;
+    for (size_t v = 0; v < vs.size(); ++v) {
+      auto &st = vs[v];
+      if (st.empty) continue;
+      passes = std::max(passes, fix_avocados(ctx, ids.data() + st.offset, dbf.data() + st.offset, st.d, st.cc,
+                                             t.soma_detection, aniso, st.black_border));
+      st.object_of.assign(st.cc.count + 1, -1);
+      if (!st.cc.count) { st.empty = true; continue; }
+      iv.push_back({st.offset, st.d, st.cc.count});
+      which.push_back(v);
+    }
+    ctx.stats["avocado_passes"] = passes;
+    auto again = analyze(ctx, ids.data(), iv);
+    for (size_t j = 0; j < which.size(); ++j) vs[which[j]].boxes = std::move(again[j]);
+    clock.mark("avocados");
+  }
   {
     std::vector<IdVolume> iv;
     std::vector<size_t> which;
@@ -409,6 +430,10 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       }
     clock.mark("somata");
   }
+  // After the avocado stage a foreground voxel can hold distance zero (background it painted
+  // without a refresh): +inf to the tracer from here on, in the volumes' part of the space
+  // (lockstep.cu:61-82; a soma's crop keeps its own field).
+  if (opt.fix_avocados) ctx.stats["zero_distances"] = double(zero_distances_to_infinity(ctx, ids.data(), dbf.data(), N));
   // a point of a volume (x, y, z) as the flat index of the arena its object is traced in
   auto arena_flat = [&](const Object &ob, const Point &p) -> int {
     if (ob.soma < 0) {
@@ -627,6 +652,8 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.delta = std::min({aniso[0], aniso[1], aniso[2]});
   a.round_limit = 0;
   if (const char *e = std::getenv("BROOK_B200_TEST_ROUND_LIMIT")) a.round_limit = std::atoll(e);  // test knob
+  a.rail_band = kRailBand;
+  if (const char *e = std::getenv("BROOK_B200_RAIL_BAND")) a.rail_band = float(std::atof(e));  // tuning knob
 
   clock.mark("state");
   const int ctas = tune.trace_cluster_ctas == kWideClusterCtas || tune.trace_cluster_ctas == kClusterCtas

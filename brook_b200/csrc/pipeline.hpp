@@ -24,6 +24,7 @@ struct Options {
   double dust = 1000;
   bool fix_branching = true, fix_borders = true;
   bool fill_holes = false;  // every component's voids filled before the EDT (BROOK_FILL_HOLES)
+  bool fix_avocados = false;  // pits merged into the objects around them after the EDT (BROOK_FIX_AVOCADOS)
   std::optional<std::vector<int64_t>> object_ids;
   // extra targets per volume of the call (x, y, z in that volume's frame); volumes beyond the
   // vectors' ends have none

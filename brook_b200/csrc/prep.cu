@@ -55,14 +55,32 @@ __global__ void __launch_bounds__(256) analyze_kernel(const uint32_t *__restrict
   for (long long i = begin + threadIdx.x; i < begin + kChunk; i += blockDim.x) {  // warp-uniform bounds
     const bool in = i < n;
     const uint32_t id = in ? ids[i] : 0u;
-    int x = 0, y = 0, z = 0;
-    if (in) unravel((int)i, d, x, y, z);
     const unsigned peers = __match_any_sync(0xFFFFFFFFu, id);
-    const int lx = int(__reduce_min_sync(peers, unsigned(x))), hx = int(__reduce_max_sync(peers, unsigned(x)));
-    const int ly = int(__reduce_min_sync(peers, unsigned(y))), hy = int(__reduce_max_sync(peers, unsigned(y)));
-    const int lz = int(__reduce_min_sync(peers, unsigned(z))), hz = int(__reduce_max_sync(peers, unsigned(z)));
+    // the warp's first voxel's position; when the 32 voxels lie in one row (the usual case), an
+    // id's extent along x comes from its lanes and y, z are the row's
+    int x0 = 0, y0 = 0, z0 = 0;
+    if (lane == 0 && in) unravel((int)i, d, x0, y0, z0);
+    x0 = __shfl_sync(0xFFFFFFFFu, x0, 0);
+    y0 = __shfl_sync(0xFFFFFFFFu, y0, 0);
+    z0 = __shfl_sync(0xFFFFFFFFu, z0, 0);
+    const bool one_row = x0 + 31 < d.sx && i - lane + 31 < n;  // warp-uniform
+    int l3[3], h3[3];
+    if (one_row) {
+      l3[0] = x0 + __ffs(peers) - 1;
+      h3[0] = x0 + 31 - __clz(peers);
+      l3[1] = h3[1] = y0;
+      l3[2] = h3[2] = z0;
+    } else {
+      int x = 0, y = 0, z = 0;
+      if (in) unravel((int)i, d, x, y, z);
+      l3[0] = int(__reduce_min_sync(peers, unsigned(x)));
+      h3[0] = int(__reduce_max_sync(peers, unsigned(x)));
+      l3[1] = int(__reduce_min_sync(peers, unsigned(y)));
+      h3[1] = int(__reduce_max_sync(peers, unsigned(y)));
+      l3[2] = int(__reduce_min_sync(peers, unsigned(z)));
+      h3[2] = int(__reduce_max_sync(peers, unsigned(z)));
+    }
     if (id == 0 || lane != __ffs(peers) - 1) continue;
-    const int l3[3] = {lx, ly, lz}, h3[3] = {hx, hy, hz};
     const int slot = table_slot(keys, id);
     if (slot < 0) {
       box_update(lo + 3 * (long long)id, hi + 3 * (long long)id, counts + id, l3, h3, __popc(peers));

@@ -174,3 +174,76 @@ def test_cavity_samples_run(fix_branching):
         out = oracle.skeletonize(sample, CAVITY_PARAMS, dust_threshold=10, fix_branching=fix_branching,
                                  fix_avocados=True, threads=4)
         assert len(out.array("labels")) >= 1
+
+
+# ---- the CUDA path ---------------------------------------------------------------------------------
+
+
+def _gpu(labels, params, anisotropy=(1, 1, 1), **opts):
+    import brook_b200
+    from brook_b200 import _native
+
+    got = brook_b200.skeletonize(labels, params, anisotropy, output="packed", fix_avocados=True, **opts)
+    return got, _native.stats()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fix_branching", [True, False])
+def test_gpu_rule_samples_keep_kimimaros_labels(gpu, fix_branching):
+    from test_gpu_parity import assert_same
+
+    for sample, keys in zip(rule_samples(), RULE_KEYS):
+        got, stats = _gpu(sample, RULE_PARAMS, dust_threshold=0, fix_branching=fix_branching)
+        assert got.labels.tolist() == keys
+        exp = oracle.skeletonize(sample, RULE_PARAMS, dust_threshold=0, fix_branching=fix_branching,
+                                 fix_avocados=True, threads=4)
+        assert stats["avocado_passes"] == int(exp.array("avocado_passes")[0])
+        assert_same(got, exp, f"rule sample {keys}")
+
+
+@pytest.mark.gpu
+def test_gpu_anisotropic_refresh_skeleton(gpu):
+    sample = refresh_sample()
+    params = dict(RULE_PARAMS, soma_detection_threshold=5)
+    vertices = np.arange(1, 6, dtype=np.float32)[:, None] * np.array(REFRESH_ANISOTROPY, np.float32)
+    radii = [0x3f8ccccd, 0x400ccccd, 0x40533334, 0x400ccccd, 0x3f8ccccd]
+    for fix_branching in (True, False):
+        got, _ = _gpu(sample, params, REFRESH_ANISOTROPY, dust_threshold=0, fix_branching=fix_branching)
+        assert got.labels.tolist() == [1]
+        np.testing.assert_array_equal(got.vertices, vertices)
+        np.testing.assert_array_equal(got.edges, [[0, 1], [1, 2], [2, 3], [3, 4]])
+        assert np.asarray(got.radii, np.float32).view(np.uint32).tolist() == radii
+
+
+@pytest.mark.gpu
+def test_gpu_unreachable_cavity_and_cavity_samples(gpu):
+    from test_gpu_parity import assert_same
+
+    got, stats = _gpu(unreachable_cavity(), CAVITY_PARAMS, dust_threshold=10)
+    assert stats["avocado_passes"] == 1 and stats["zero_distances"] > 0
+    exp = oracle.skeletonize(unreachable_cavity(), CAVITY_PARAMS, dust_threshold=10, fix_avocados=True)
+    assert_same(got, exp, "unreachable cavity")
+    assert len(got.vertices) - len(got.edges) == 1
+    for fix_branching in (True, False):
+        for detection in (6, 1000):  # with and without somata
+            params = dict(CAVITY_PARAMS, soma_detection_threshold=detection,
+                          soma_acceptance_threshold=detection + 2)
+            for i, sample in enumerate(cavity_samples()):
+                got, _ = _gpu(sample, params, dust_threshold=10, fix_branching=fix_branching)
+                exp = oracle.skeletonize(sample, params, dust_threshold=10, fix_branching=fix_branching,
+                                         fix_avocados=True, threads=4)
+                assert_same(got, exp, f"cavity sample {i} detection {detection} branching {fix_branching}")
+
+
+@pytest.mark.gpu
+def test_gpu_avocados_in_a_batch(gpu):
+    import brook_b200
+    from test_gpu_parity import assert_same
+
+    samples = rule_samples() + cavity_samples()
+    batch = brook_b200.skeletonize_batch(samples, CAVITY_PARAMS, output="packed", dust_threshold=10,
+                                         fix_avocados=True, fill_holes=True)
+    for i, sample in enumerate(samples):
+        exp = oracle.skeletonize(sample, CAVITY_PARAMS, dust_threshold=10, fix_avocados=True, fill_holes=True,
+                                 threads=4)
+        assert_same(batch[i], exp, f"batch sample {i}")

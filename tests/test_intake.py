@@ -51,7 +51,7 @@ def test_options_outside_the_path_raise_before_any_device_call():
     v = np.ones((4, 4, 4), np.uint32)
     with pytest.raises(ValueError, match="output"):
         brook_b200.skeletonize(v, output="dense")
-    for option in ({"fix_avocados": True}, {"voxel_graph": np.zeros((4, 4, 4), np.uint32)}):
+    for option in ({"voxel_graph": np.zeros((4, 4, 4), np.uint32)},):
         with pytest.raises(NotImplementedError):
             brook_b200.skeletonize(v, **option)
     with pytest.raises(ValueError, match="output"):
