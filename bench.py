@@ -468,11 +468,59 @@ def serve_measurement(cfg, local=0):
     }
 
 
+OPTIONS_CASE = dict(workload="cells with nuclei 256x256x256 uint32, 64 Voronoi cells (seed 6), half with an empty "
+                             "cavity; anisotropy (1, 1, 1)", shape=(256, 256, 256), cells=64, seed=6)
+OPTIONS_PARAMS = dict(scale=1.5, const=10, pdrf_scale=100000, pdrf_exponent=4, soma_detection_threshold=10,
+                      soma_acceptance_threshold=1e6)
+
+
+def options_measurement(local, steps=3):
+    """fill_holes and fix_avocados on a volume that has work for both (enclosed nuclei, empty
+    cavities): per option set the device time of one call (CUDA events, mean of `steps` after a
+    warm-up), the option's own stage and host time, the skeletons, and the oracle's time for the
+    same call on the host cores."""
+    import brook_b200
+    from brook_b200 import _native, synthetic
+    from oracle import oracle
+
+    volume = synthetic.cell_volume(OPTIONS_CASE["shape"], cells=OPTIONS_CASE["cells"], seed=OPTIONS_CASE["seed"])
+    out = {"workload": OPTIONS_CASE["workload"], "teasar": OPTIONS_PARAMS}
+    for name, opts in (("plain", {}), ("fill_holes", dict(fill_holes=True)), ("fix_avocados", dict(fix_avocados=True)),
+                       ("both", dict(fill_holes=True, fix_avocados=True))):
+        call = lambda: brook_b200.skeletonize(volume, OPTIONS_PARAMS, (1, 1, 1), dust_threshold=DUST, output="packed",
+                                              device=local, **opts)
+        call()
+        total, stage, host, skeletons = 0.0, 0.0, 0.0, 0
+        for _ in range(steps):
+            skeletons = len(call())
+            st = _native.stats(local)
+            total += st.get("ms_total", 0.0)
+            for key in ("holes", "avocados"):
+                stage += st.get("ms_" + key, 0.0)
+                host += st.get("host_ms_" + key, 0.0)
+        row = {"ms_per_call": total / steps, "skeletons": skeletons}
+        if opts:
+            row.update({"option_stage_ms": stage / steps, "option_host_ms": host / steps})
+            if "fill_holes" in opts:
+                row["hole_filled_voxels"] = st.get("hole_filled_voxels")
+            if "fix_avocados" in opts:
+                row["avocado_passes"] = st.get("avocado_passes")
+        out[name] = row
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ref = oracle.skeletonize(volume, OPTIONS_PARAMS, (1, 1, 1), DUST, threads=threads, fill_holes=True,
+                             fix_avocados=True)
+    out["cpu_oracle_both"] = {"ms_per_call": (time.perf_counter() - t0) * 1e3, "threads": threads,
+                              "skeletons": len(ref.array("labels"))}
+    return out
+
+
 def extra_measurements(local):
     """The metric's two comparisons beside the headline line, on the same GPU: the 64-volume uneven
     batch as one skeletonize_batch call against 64 plain calls (skeletons/s both ways, identical
     skeletons checked), and the request stream's p50/p99 latency at 50/200/800 req/s through the
-    continuous-batching server and the per-request path."""
+    continuous-batching server and the per-request path; and the fill_holes / fix_avocados options
+    on a volume with enclosed nuclei and cavities."""
     extras = {}
     try:
         b = batch_measurement(CONFIGS["batch64"], steps=3, warmup=2, local=local)
@@ -491,6 +539,10 @@ def extra_measurements(local):
                            "timing": "wall clock per request, arrival to result"}
     except Exception as e:
         extras["serve"] = {"error": f"{type(e).__name__}: {e}"}
+    try:
+        extras["options"] = options_measurement(local)
+    except Exception as e:
+        extras["options"] = {"error": f"{type(e).__name__}: {e}"}
     return extras
 
 

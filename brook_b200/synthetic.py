@@ -21,7 +21,7 @@ import math
 
 import numpy as np
 
-__all__ = ["tube_volume", "dense_volume", "uneven_batch", "serving_requests"]
+__all__ = ["tube_volume", "dense_volume", "cell_volume", "uneven_batch", "serving_requests"]
 
 _BALLS: dict = {}
 
@@ -174,6 +174,64 @@ def dense_volume(shape=(512, 512, 512), seeds=600, seed=1, radius=(3.0, 10.0), s
     lut[1:] = ids[:seeds]
     cells_np = c3.cpu().numpy()  # (z, y, x) C order == Fortran (x, y, z)
     return np.asfortranarray(lut[cells_np].transpose(2, 1, 0))
+
+
+def cell_volume(shape=(256, 256, 256), cells=64, seed=6, nucleus=(0.35, 0.5), cavity_share=0.5, dtype=np.uint32):
+    """Voronoi cells of `cells` uniform seeds filling the volume (boundaries eroded by one voxel),
+    each with a nucleus: a ball of its own label around the seed, of a radius that is a fraction
+    (`nucleus`) of the seed's distance to its nearest other seed; about `cavity_share` of the cells
+    also hold an empty cavity beside the nucleus. The nuclei are the pits the avocado stage merges
+    into their cells, the cavities the voids hole filling fills. Labels: cells 1..cells, nuclei
+    cells+1..2*cells."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    shape = tuple(int(s) for s in shape)
+    dev = _device()
+    points = rng.uniform(4, np.asarray(shape) - 5, size=(cells, 3))
+    seeds_t = torch.from_numpy(points).to(dev)
+    n = int(np.prod(shape))
+    sx, sy = shape[0], shape[1]
+    owner = torch.empty(n, dtype=torch.int64, device=dev)
+    near = torch.empty(n, dtype=torch.float64, device=dev)
+    chunk = 1 << 20
+    for i in range(0, n, chunk):
+        idx = torch.arange(i, min(n, i + chunk), device=dev)
+        coords = torch.stack([idx % sx, (idx // sx) % sy, idx // (sx * sy)], dim=1).to(torch.float64)
+        d = torch.cdist(coords, seeds_t)
+        near[i:i + chunk], owner[i:i + chunk] = d.min(dim=1)
+    labels = (owner + 1).to(torch.int64)
+    spacing = torch.cdist(seeds_t, seeds_t) + torch.eye(cells, device=dev, dtype=torch.float64) * 1e9
+    gap = spacing.min(dim=1).values  # each seed's distance to its nearest other seed
+    frac = torch.from_numpy(rng.uniform(*nucleus, size=cells)).to(dev)
+    radius = gap * frac / 2
+    inside = near <= radius[owner]
+    labels[inside] = owner[inside] + 1 + cells
+    # a cavity: a ball of half the nucleus's radius centred beside it, in half of the cells
+    with_cavity = torch.from_numpy(rng.random(cells) < cavity_share).to(dev)
+    direction = torch.from_numpy(rng.normal(size=(cells, 3))).to(dev)
+    direction = direction / direction.norm(dim=1, keepdim=True)
+    centre = seeds_t + direction * (radius * 1.9)[:, None]
+    for i in range(0, n, chunk):
+        idx = torch.arange(i, min(n, i + chunk), device=dev)
+        o = owner[i:i + chunk]
+        coords = torch.stack([idx % sx, (idx // sx) % sy, idx // (sx * sy)], dim=1).to(torch.float64)
+        dc = (coords - centre[o]).norm(dim=1)
+        hole = with_cavity[o] & (dc <= radius[o] * 0.5) & ~inside[i:i + chunk]
+        labels[i:i + chunk][hole] = 0
+    c3 = labels.view(shape[2], shape[1], shape[0])
+    boundary = torch.zeros_like(c3, dtype=torch.bool)
+    for axis in range(3):
+        a = [slice(None)] * 3
+        b = [slice(None)] * 3
+        a[axis], b[axis] = slice(1, None), slice(None, -1)
+        u, v = c3[tuple(a)], c3[tuple(b)]
+        cell_u, cell_v = (u - 1) % cells, (v - 1) % cells  # a nucleus and its cell stay joined
+        diff = (u != 0) & (v != 0) & (cell_u != cell_v)
+        boundary[tuple(a)] |= diff
+        boundary[tuple(b)] |= diff
+    c3[boundary] = 0
+    return np.asfortranarray(c3.cpu().numpy().astype(dtype).transpose(2, 1, 0))
 
 
 def uneven_batch(count=64, seed=2, edges=(64, 256), tubes=(10, 80), radius=(1.0, 8.0), arbor_fraction=0.05):

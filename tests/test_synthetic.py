@@ -43,3 +43,18 @@ def test_uneven_batch_and_requests_shapes():
     times = [t for t, _ in reqs]
     assert times == sorted(times) and times[0] > 0
     assert {v.dtype for _, v in reqs} <= {np.dtype(np.uint32), np.dtype(np.uint64)}
+
+
+def test_cell_volume_has_enclosed_nuclei_and_cavities():
+    from scipy import ndimage
+
+    v = synthetic.cell_volume((64, 64, 64), cells=8, seed=1)
+    assert v.dtype == np.uint32 and v.flags.f_contiguous
+    labels = set(np.unique(v).tolist()) - {0}
+    assert labels == set(range(1, 17))  # 8 cells and their 8 nuclei
+    for nucleus in range(9, 17):
+        cell = nucleus - 8
+        grown = ndimage.binary_dilation(v == nucleus)
+        ring = np.unique(v[grown & (v != nucleus)])
+        assert set(ring.tolist()) <= {0, cell}  # a nucleus touches only its own cell
+    assert np.array_equal(synthetic.cell_volume((64, 64, 64), cells=8, seed=1), v)
