@@ -419,7 +419,7 @@ def serve_measurement(cfg, local=0):
 
     base = synthetic.serving_requests(cfg["requests"], 1.0, seed=cfg["seed"])  # arrivals at rate 1, rescaled below
     opts = dict(teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST, device=local,
-                memory_cap=80e9)
+                memory_cap=80e9, engine_share=int(os.environ.get("BROOK_B200_SERVE_ENGINE_SHARE", "100")))
     warm = [(0.0, v) for _, v in base[:8]]
     serving.replay(warm, lambda: serving.Server(workers=2, **opts))
     rates, total = {}, None

@@ -34,7 +34,8 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_edt_device_noalloc", "brook_skeletons_get_device_view", "brook_skeletons_get_array",
            "brook_array_upload", "brook_array_to_dlpack", "brook_array_to_dlpack_versioned", "brook_components_labels",
            "brook_skeletonize_batch_targets", "brook_context_wait_stream", "brook_autotune",
-           "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons", "brook_context_trim"]
+           "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons", "brook_context_trim",
+           "brook_context_set_engine_share"]
 
 
 class Volume(ctypes.Structure):
@@ -130,6 +131,7 @@ def _open():
         "brook_context_destroy": (None, [vp]),
         "brook_context_synchronize": (ctypes.c_int, [vp]),
         "brook_context_trim": (ctypes.c_int, [vp]),
+        "brook_context_set_engine_share": (ctypes.c_int, [vp, ctypes.c_int]),
         "brook_array_destroy": (None, [vp]),
         "brook_array_view": (ctypes.c_int, [vp, ctypes.POINTER(Volume)]),
         "brook_array_copy_to_host": (ctypes.c_int, [vp, vp, sz]),
@@ -345,6 +347,12 @@ def packed_device_arrays(handle):
 def trim(device=0):
     """Returns the device memory the calling thread's context keeps for reuse to the driver."""
     check(load().brook_context_trim(context(device)))
+
+
+def set_engine_share(percent, device=0):
+    """The share (percent) of the GPU's resident clusters the calling thread's context's
+    persistent engine launches take (brook_context_set_engine_share)."""
+    check(load().brook_context_set_engine_share(context(device), int(percent)))
 
 
 def stats(device=0):

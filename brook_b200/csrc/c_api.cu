@@ -457,6 +457,14 @@ brook_status brook_context_synchronize(brook_context *ctx) {
   });
 }
 
+brook_status brook_context_set_engine_share(brook_context *ctx, int percent) {
+  return protect([&] {
+    require(ctx && percent >= 1 && percent <= 100, "the engine share is a percentage from 1 to 100");
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    ctx->value.engine_percent = percent;
+  });
+}
+
 brook_status brook_context_trim(brook_context *ctx) {
   return protect([&] {
     require(ctx);

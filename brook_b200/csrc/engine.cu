@@ -440,7 +440,7 @@ __device__ unsigned long long railroad(const EngineArgs &a, Shared &sh, Shared *
       A[0] = t;
       L->cnt[0] = 1;
       atomicOr(a.flags + t, kNearQueued);
-      L->T = fmaxf(__fmul_rn(2.0f, ft), 1e-30f);
+      L->T = fmaxf(__fmul_rn(a.rail_band, ft), 1e-30f);
     }
   }
   G::sync();
@@ -1211,7 +1211,7 @@ void launch(const void *kernel, int ctas, const EngineArgs &a, int nbig, cudaStr
   args.nbig = nbig;
   void *kargs[] = {&args};
   cudaLaunchAttribute attr[1];
-  const int cap = resident_clusters(kernel, ctas, stream);
+  const int cap = std::max(1, resident_clusters(kernel, ctas, stream) * std::min(100, std::max(1, a.grid_percent)) / 100);
   const long long need = nbig + (a.nobj - nbig + ctas - 1) / ctas;
   const int clusters = int(std::max(1LL, std::min<long long>(cap, need)));
   args.lone_first = nbig < a.nobj ? clusters * lone_percent / 100 : 0;

@@ -653,6 +653,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   a.round_limit = 0;
   if (const char *e = std::getenv("BROOK_B200_TEST_ROUND_LIMIT")) a.round_limit = std::atoll(e);  // test knob
   a.rail_band = kRailBand;
+  a.grid_percent = ctx.engine_percent;
   if (const char *e = std::getenv("BROOK_B200_RAIL_BAND")) a.rail_band = float(std::atof(e));  // tuning knob
 
   clock.mark("state");

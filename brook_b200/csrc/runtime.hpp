@@ -89,6 +89,9 @@ class Context {
   // the autotuner or from a saved table; `forced` overrides them while the autotuner measures.
   std::map<unsigned long long, Tuning> tuning;
   const Tuning *forced = nullptr;
+  // The share (percent, 1-100) of the device's resident clusters the engine's persistent launches
+  // take; below 100 another context's kernels find free CTA slots while this one traces.
+  int engine_percent = 100;
   unsigned long long last_class = 0;  // the workload class of the last call
   // Launches a captured graph of the engine's launches: the context keeps one executable graph and
   // updates it in place when the new graph has the same topology (else instantiates it anew).

@@ -62,6 +62,14 @@ def context_stats(device):
     return _native.stats(device)
 
 
+def share_engine(device, percent):
+    """Sets the share of the GPU's resident clusters the calling thread's context's persistent
+    engine launches take (below 100 they leave room for another worker's kernels)."""
+    from . import _native
+
+    _native.set_engine_share(percent, device)
+
+
 def trim_context(device):
     """Hands the calling thread's context's kept blocks back to the driver."""
     from . import _native
@@ -84,19 +92,22 @@ class Request:
 
 
 class Server:
-    """Continuous-batching skeletonization server (see the module docstring).
+    """Continuous-batching skeletonization server (see the module docstring). `engine_share`
+    (percent of the GPU's resident clusters) lets each worker's persistent engine launches leave
+    room for the other workers' kernels.
 
     `submit(volume)` returns a Future whose result is the request's PackedSkeletons; the
     Request object (arrival, start and finish times) is available as `future.request`."""
 
     def __init__(self, teasar_params=None, anisotropy=(1, 1, 1), dust_threshold=1000, fix_branching=True,
-                 fix_borders=True, memory_cap=80e9, workers=2, max_batch=64, device=0):
+                 fix_borders=True, memory_cap=80e9, workers=2, max_batch=64, device=0, engine_share=100):
         from . import DEFAULT_TEASAR_PARAMS
 
         self.options = dict(teasar_params=DEFAULT_TEASAR_PARAMS if teasar_params is None else teasar_params,
                             anisotropy=anisotropy, dust_threshold=dust_threshold, fix_branching=fix_branching,
                             fix_borders=fix_borders, device=device)
         self.device = device
+        self.engine_share = int(engine_share)
         self.memory_cap = int(memory_cap)
         self.max_batch = int(max_batch)
         self.state_bytes_per_voxel = STATE_BYTES_PER_VOXEL
@@ -159,6 +170,11 @@ class Server:
         return batch, need, budget
 
     def _work(self, w):
+        if self.engine_share != 100:
+            try:
+                share_engine(self.device, self.engine_share)
+            except Exception:  # no device: the batches will say so
+                pass
         while True:
             with self._cond:
                 while True:

@@ -126,6 +126,11 @@ brook_status brook_context_synchronize(brook_context *context);  /* brook.h:156 
  * context keeps for reuse back to the device's default memory pool and trims that pool, so the
  * memory returns to the driver. The next call allocates again. */
 brook_status brook_context_trim(brook_context *context);
+/* No counterpart in the reference. The share (percent, 1 to 100, default 100) of the device's
+ * resident thread-block clusters that this context's persistent engine launches take. Below 100,
+ * kernels of other contexts (another request's preamble) run beside them instead of waiting for
+ * them to end; a call alone on the GPU runs faster at 100. */
+brook_status brook_context_set_engine_share(brook_context *context, int percent);
 
 /* brook.h:159-162: device arrays owned by the handle. brook_array_upload copies a volume (host
  * or device memory of the context's device, any strides, any of the ten element types) into a
