@@ -470,7 +470,7 @@ def serve_measurement(cfg, local=0):
 
 OPTIONS_CASE = dict(workload="cells with nuclei 256x256x256 uint32, 64 Voronoi cells (seed 6), half with an empty "
                              "cavity; anisotropy (1, 1, 1)", shape=(256, 256, 256), cells=64, seed=6)
-OPTIONS_PARAMS = dict(scale=1.5, const=10, pdrf_scale=100000, pdrf_exponent=4, soma_detection_threshold=10,
+OPTIONS_PARAMS = dict(scale=1.5, const=10, pdrf_scale=100000, pdrf_exponent=4, soma_detection_threshold=30,
                       soma_acceptance_threshold=1e6)
 
 

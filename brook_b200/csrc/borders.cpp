@@ -7,6 +7,7 @@
 // insertion order of a CPython set of integer 3-tuples, which decides the reference's root and
 // target order (borders.cu:53-116 and point_set.hpp of giorgioangel/brook).
 #include <algorithm>
+#include <chrono>
 #include <limits>
 
 #include "kernels.hpp"
@@ -125,10 +126,18 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
   if (faces.size() > 65535) throw std::invalid_argument("too many volumes for one border pass");
   const long long slice = (long long)W * H, S = (long long)faces.size();
   if (slice * S >= (1LL << 31) - 1) throw std::invalid_argument("border faces exceed 2^31 pixels");
+  // host time of the steps (the device waits on the host in this stage)
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char *step) {
+    const auto now = std::chrono::steady_clock::now();
+    ctx.stats[std::string("host_ms_borders_") + step] += std::chrono::duration<double, std::milli>(now - t0).count();
+    t0 = now;
+  };
   Buffer<uint32_t> stack(ctx, slice * S), stack_ids(ctx, slice * S);
   extract_faces(ctx, ids, faces, W, H, stack.data());
   const VolumeDims sd{W, H, int(S)};
   ComponentsResult pc = connected_components(ctx, stack.data(), U32, sd, stack_ids.data(), true);
+  lap("components");
   if (pc.count == 0) return out;
   // 2D EDT (black border) of each group with its own spacing: the slice's x axis is b, y is a
   Buffer<float> dist(ctx, slice * S);
@@ -142,6 +151,7 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
   // per component: counts, coordinate sums, largest distance, first pixel, and the pixels at the
   // largest distance, from the device; the host does the per-component selection
   const FaceStats st = face_stats(ctx, stack_ids.data(), dist.data(), faces, W, H, pc.count);
+  lap("stats");
   const size_t K = size_t(pc.count) + 1;
   // a component's face: the stack slice of its first pixel
   std::vector<int> face_of(K, -1);
@@ -227,6 +237,7 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
   }
   for (size_t v = 0; v < volumes.size(); ++v)
     for (size_t id = 0; id < sets[v].size(); ++id) out[v][id] = sets[v][id].values();
+  lap("select");
   return out;
 }
 

@@ -247,60 +247,39 @@ constexpr int kMaxRounds = 1 << 20;  // a round that changes nothing ends the fl
 
 }  // namespace
 
-long long fill_holes(Context &ctx, uint32_t *ids, const std::vector<HoleVolume> &volumes) {
+Voids component_voids(Context &ctx, const uint32_t *ids, const std::vector<VoidBox> &boxes) {
   cudaStream_t s = ctx.stream();
-  // eligible components: a box of three or more voxels along every axis that the component does
-  // not fill (no other box can enclose a void)
-  struct Eligible {
-    size_t volume;
-    uint32_t id;
-    long long voxels, words;
-  };
-  std::vector<Eligible> all;
-  for (size_t v = 0; v < volumes.size(); ++v) {
-    const auto &boxes = *volumes[v].boxes;
-    for (size_t id = 1; id < boxes.size(); ++id) {
-      const Box &b = boxes[id];
-      if (!b.count) continue;
-      const int bx = b.hi[0] - b.lo[0] + 1, by = b.hi[1] - b.lo[1] + 1, bz = b.hi[2] - b.lo[2] + 1;
-      const long long n = (long long)bx * by * bz;
-      if (bx <= 2 || by <= 2 || bz <= 2 || n == b.count) continue;
-      all.push_back({v, uint32_t(id), n, (long long)(bx + 31) / 32 * by * bz});
-    }
-  }
-  // the holes of every component, in batches of at most `budget` plane words (256 MiB a plane; a
-  // larger box runs alone)
+  Voids out;
+  out.count.assign(boxes.size(), 0);
+  // the voids of every box, in batches of at most `budget` plane words (256 MiB a plane; a larger
+  // box runs alone)
   constexpr long long budget = 1LL << 26;
-  std::vector<int> hole_voxel, hole_job_volume;
-  std::vector<uint32_t> hole_id, hole_held;
-  std::vector<std::vector<long long>> filled_of(volumes.size());
-  for (size_t v = 0; v < volumes.size(); ++v) filled_of[v].assign(volumes[v].boxes->size(), 0);
-  std::vector<std::pair<size_t, uint32_t>> job_owner;  // per job of the batch: (volume, id)
   size_t next = 0;
-  while (next < all.size()) {
+  while (next < boxes.size()) {
     std::vector<HoleJob> jobs;
+    std::vector<size_t> job_box;
     std::vector<long long> row_begin, ycol_begin, zcol_begin;
     long long words = 0, rows = 0, ycols = 0, zcols = 0;
-    job_owner.clear();
-    while (next < all.size() && (jobs.empty() || words + all[next].words <= budget)) {
-      const auto &e = all[next++];
-      const auto &hv = volumes[e.volume];
-      const Box &b = (*hv.boxes)[e.id];
+    while (next < boxes.size()) {
+      const VoidBox &e = boxes[next];
+      const Box &b = e.box;
       HoleJob J{};
-      J.base = words;
-      J.vol_offset = hv.offset;
-      J.vsx = hv.d.sx;
-      J.vsy = hv.d.sy;
+      J.vol_offset = e.vol_offset;
+      J.vsx = e.d.sx;
+      J.vsy = e.d.sy;
       J.lx = b.lo[0]; J.ly = b.lo[1]; J.lz = b.lo[2];
       J.bx = b.hi[0] - b.lo[0] + 1; J.by = b.hi[1] - b.lo[1] + 1; J.bz = b.hi[2] - b.lo[2] + 1;
       J.words = (J.bx + 31) / 32;
       J.id = e.id;
+      const long long w = (long long)J.words * J.by * J.bz;
+      if (!jobs.empty() && words + w > budget) break;
+      J.base = words;
       jobs.push_back(J);
-      job_owner.push_back({e.volume, e.id});
+      job_box.push_back(next++);
       row_begin.push_back(rows);
       ycol_begin.push_back(ycols);
       zcol_begin.push_back(zcols);
-      words += e.words;
+      words += w;
       rows += (long long)J.by * J.bz;
       ycols += (long long)J.words * J.bz;
       zcols += (long long)J.words * J.by;
@@ -352,13 +331,46 @@ long long fill_holes(Context &ctx, uint32_t *ids, const std::vector<HoleVolume> 
     const auto hv = ov.download(), hj = oj.download();
     const auto hh = oh.download();
     for (long long k = 0; k < H; ++k) {
-      const auto &owner = job_owner[hj[k]];
-      hole_voxel.push_back(hv[k]);
-      hole_job_volume.push_back(int(owner.first));
-      hole_id.push_back(owner.second);
-      hole_held.push_back(hh[k]);
-      filled_of[owner.first][owner.second] += 1;
+      const size_t box = job_box[hj[k]];
+      out.voxel.push_back(hv[k]);
+      out.box.push_back(int(box));
+      out.held.push_back(hh[k]);
+      out.count[box] += 1;
     }
+  }
+  return out;
+}
+
+long long fill_holes(Context &ctx, uint32_t *ids, const std::vector<HoleVolume> &volumes) {
+  cudaStream_t s = ctx.stream();
+  // eligible components: a box of three or more voxels along every axis that the component does
+  // not fill (no other box can enclose a void)
+  std::vector<VoidBox> eligible;
+  std::vector<size_t> volume_of;
+  for (size_t v = 0; v < volumes.size(); ++v) {
+    const auto &boxes = *volumes[v].boxes;
+    for (size_t id = 1; id < boxes.size(); ++id) {
+      const Box &b = boxes[id];
+      if (!b.count) continue;
+      const int bx = b.hi[0] - b.lo[0] + 1, by = b.hi[1] - b.lo[1] + 1, bz = b.hi[2] - b.lo[2] + 1;
+      const long long n = (long long)bx * by * bz;
+      if (bx <= 2 || by <= 2 || bz <= 2 || n == b.count) continue;
+      eligible.push_back({volumes[v].offset, volumes[v].d, b, uint32_t(id)});
+      volume_of.push_back(v);
+    }
+  }
+  const Voids voids = component_voids(ctx, ids, eligible);
+  std::vector<int> hole_voxel, hole_job_volume;
+  std::vector<uint32_t> hole_id, hole_held;
+  std::vector<std::vector<long long>> filled_of(volumes.size());
+  for (size_t v = 0; v < volumes.size(); ++v) filled_of[v].assign(volumes[v].boxes->size(), 0);
+  for (size_t k = 0; k < voids.voxel.size(); ++k) {
+    const size_t j = size_t(voids.box[k]);
+    hole_voxel.push_back(voids.voxel[k]);
+    hole_job_volume.push_back(int(volume_of[j]));
+    hole_id.push_back(eligible[j].id);
+    hole_held.push_back(voids.held[k]);
+    filled_of[volume_of[j]][eligible[j].id] += 1;
   }
   if (hole_voxel.empty()) return 0;
   // the order-dependent part, per volume: ascending ids, a component is filled unless disabled by

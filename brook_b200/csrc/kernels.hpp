@@ -91,6 +91,21 @@ struct HoleVolume {
   const std::vector<Box> *boxes;
 };
 long long fill_holes(Context &ctx, uint32_t *ids, const std::vector<HoleVolume> &volumes);
+// The voids of a component in a box: the box's voxels that are not the id and not 6-connected,
+// through such voxels, to a face of the box (fill_voids' rule). All boxes at once; returns per void
+// voxel its flat index, its box and the id it holds, and per box the count.
+struct VoidBox {
+  long long vol_offset;
+  VolumeDims d;
+  Box box;
+  uint32_t id;
+};
+struct Voids {
+  std::vector<int> voxel, box;
+  std::vector<uint32_t> held;
+  std::vector<long long> count;
+};
+Voids component_voids(Context &ctx, const uint32_t *ids, const std::vector<VoidBox> &boxes);
 
 // ---- the avocado stage (avocado.cpp) ----
 // One volume's component ids (ids, device, 1..cc.count) and distance field (dbf, device) after the

@@ -69,41 +69,6 @@ __global__ void gather_box(const T *src, int sx, int sy, int lx, int ly, int lz,
   out[i] = keep && !keep[i] ? T(0) : value;
 }
 
-// fill_voids (trace_primitives.cu:238-253, fillvoids_kernels.cuh): background voxels of the crop
-// not 6-connected to its faces become foreground. Returns how many.
-long long fill_voids(std::vector<uint32_t> &mask, int cx, int cy, int cz) {
-  const long long n = (long long)cx * cy * cz;
-  std::vector<uint8_t> seen(n, 0);
-  std::vector<long long> stack;
-  auto at = [&](long long x, long long y, long long z) { return x + cx * (y + (long long)cy * z); };
-  for (long long z = 0; z < cz; ++z)
-    for (long long y = 0; y < cy; ++y)
-      for (long long x = 0; x < cx; ++x) {
-        const long long v = at(x, y, z);
-        if (mask[v] || !(x == 0 || y == 0 || z == 0 || x == cx - 1 || y == cy - 1 || z == cz - 1)) continue;
-        seen[v] = 1;
-        stack.push_back(v);
-      }
-  const int step[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
-  while (!stack.empty()) {
-    const long long u = stack.back();
-    stack.pop_back();
-    const long long z = u / ((long long)cx * cy), r = u - z * cx * cy, y = r / cx, x = r - y * cx;
-    for (const auto &d : step) {
-      const long long nx = x + d[0], ny = y + d[1], nz = z + d[2];
-      if (nx < 0 || ny < 0 || nz < 0 || nx >= cx || ny >= cy || nz >= cz) continue;
-      const long long v = at(nx, ny, nz);
-      if (mask[v] || seen[v]) continue;
-      seen[v] = 1;
-      stack.push_back(v);
-    }
-  }
-  long long filled = 0;
-  for (long long v = 0; v < n; ++v)
-    if (!mask[v] && !seen[v]) { mask[v] = 1; ++filled; }
-  return filled;
-}
-
 // The soma root (trace.cu:55-73, batched.cu:58-105): among the crop voxels at the DBF maximum,
 // sorted by (x, y, z), the first nearest (float64 squared distance, voxel units) to their float32
 // centroid. Returns the crop flat index.
@@ -376,8 +341,13 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   if (nobj == 0) return results;
   long long NT = N;  // voxels of the flat index space, private arenas included
   if (!somas.empty()) {
-    // the candidates' crops: ids gathered on the device, voids filled on the host
-    for (auto &sa : somas) {
+    // the candidates' crops: ids gathered on the device; every crop's voids (fill_voids' rule) from
+    // one batched flood over all the boxes
+    std::vector<VoidBox> boxes_of;
+    for (const auto &sa : somas) boxes_of.push_back({vs[sa.volume].offset, vs[sa.volume].d, vs[sa.volume].boxes[sa.id], sa.id});
+    const Voids voids = component_voids(ctx, ids.data(), boxes_of);
+    for (size_t j = 0; j < somas.size(); ++j) {
+      auto &sa = somas[j];
       const auto &st = vs[sa.volume];
       const long long n = (long long)sa.dims[0] * sa.dims[1] * sa.dims[2];
       Buffer<uint32_t> crop(ctx, n);
@@ -387,10 +357,17 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
       BK_CUDA(cudaGetLastError());
       sa.mask = crop.download();
       for (auto &m : sa.mask) m = m == sa.id ? 1u : 0u;
-      sa.filled = fill_voids(sa.mask, sa.dims[0], sa.dims[1], sa.dims[2]);
+      sa.filled = voids.count[j];
       sa.valid = st.boxes[sa.id].count + sa.filled;
       sa.offset = NT;
       NT += n;
+    }
+    for (size_t k = 0; k < voids.voxel.size(); ++k) {
+      auto &sa = somas[size_t(voids.box[k])];
+      const auto &st = vs[sa.volume];
+      const long long local = voids.voxel[k] - st.offset;
+      const long long x = local % st.d.sx, y = (local / st.d.sx) % st.d.sy, z = local / ((long long)st.d.sx * st.d.sy);
+      sa.mask[(x - sa.lo[0]) + sa.dims[0] * ((y - sa.lo[1]) + (long long)sa.dims[1] * (z - sa.lo[2]))] = 1u;
     }
     if (NT >= (1LL << 31) - 1) throw std::invalid_argument("the volumes of one call must hold fewer than 2^31 voxels");
     // ids, masks and DBF over the whole space: the volumes', then every private crop's
