@@ -142,11 +142,10 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
   // 2D EDT (black border) of each group with its own spacing: the slice's x axis is b, y is a
   Buffer<float> dist(ctx, slice * S);
   const long long per_group = 2LL * (long long)volumes.size();
-  for (int t = 0; t < 3; ++t) {
-    const float plane_aniso[3] = {aniso[axes[t][1]], aniso[axes[t][0]], 1.0f};
-    const long long first = per_group * t;
-    edt(ctx, stack_ids.data() + slice * first, VolumeDims{W, H, int(per_group)}, plane_aniso, true, 2,
-        dist.data() + slice * first);
+  {
+    float wx[3], wy[3];
+    for (int t = 0; t < 3; ++t) { wx[t] = aniso[axes[t][1]]; wy[t] = aniso[axes[t][0]]; }
+    edt_planes(ctx, stack_ids.data(), W, H, 3, int(per_group), wx, wy, dist.data());
   }
   // per component: counts, coordinate sums, largest distance, first pixel, and the pixels at the
   // largest distance, from the device; the host does the per-component selection

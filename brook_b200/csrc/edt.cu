@@ -223,6 +223,24 @@ __global__ void edt_envelope(const uint32_t *__restrict__ ids, float *__restrict
   envelope_line(ids, D, base, stride, n, w, bb, Vs + tid, Hs + tid, Zs + tid, nbatch, finish);
 }
 
+// The y pass of a stack of 2D images in groups of `per_group` slices, each group with its own
+// spacing w[group] (the border targets' face stack: one group per axis pair).
+struct GroupSpacing {
+  float w[3];
+};
+__global__ void edt_envelope_groups(const uint32_t *__restrict__ ids, float *__restrict__ D, Dims d, GroupSpacing gs,
+                                    int per_group, int bb, long long line0, long long nbatch, int *__restrict__ Vs,
+                                    float *__restrict__ Hs, double *__restrict__ Zs) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= nbatch) return;
+  long long base, stride;
+  int n;
+  const long long line = line0 + tid;
+  if (!line_of(line, 0, d, 1, base, stride, n)) return;
+  const int group = int((line / d.sx) / per_group);
+  envelope_line(ids, D, base, stride, n, gs.w[group], bb, Vs + tid, Hs + tid, Zs + tid, nbatch, 1);
+}
+
 // The y or z pass of several volumes of one flat index space in one launch: volume v's lines are
 // [line_begin[v], line_begin[v + 1]) of the launch's line space.
 struct EnvelopeVolume {
@@ -287,6 +305,43 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
                                                       V.data(), H.data(), Z.data(), last); ++ctx.launches;
       BK_CUDA(cudaGetLastError());
     }
+  }
+}
+
+void edt_planes(Context &ctx, const uint32_t *ids, int W, int H, int groups, int per_group, const float wx[3],
+                const float wy[3], float *D) {
+  if (groups < 1 || groups > 3 || per_group < 1) throw std::invalid_argument("planar EDT groups out of range");
+  const long long slice = (long long)W * H, S = (long long)groups * per_group;
+  if (!slice) return;
+  cudaStream_t s = ctx.stream();
+  const size_t smem = size_t(kWarpsX) * W * sizeof(int);
+  if (smem > kEdtXMaxSmem) throw std::invalid_argument("x extent too large for the EDT x pass");
+  allow_edt_x_smem();
+  // x passes, one per group (its spacing table)
+  for (int g = 0; g < groups; ++g) {
+    std::vector<float> acc(W + 2, 0.0f);
+    for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + wx[g];
+    Buffer<float> dacc = to_device(ctx, acc);
+    const long long lines = (long long)H * per_group;
+    edt_x<<<(unsigned)((lines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(
+        ids + slice * per_group * g, D + slice * per_group * g, Dims{W, H, per_group}, dacc.data(), 1, 0);
+    ++ctx.launches;
+  }
+  BK_CUDA(cudaGetLastError());
+  // the y pass of every group in one launch
+  const long long lines = (long long)W * S;
+  const long long budget = 4LL << 30;
+  const long long batch = std::max(1LL, std::min(lines, budget / (16LL * (H + 3))));
+  Buffer<int> V(ctx, batch * (H + 3));
+  Buffer<float> Hb(ctx, batch * (H + 3));
+  Buffer<double> Z(ctx, batch * (H + 3));
+  GroupSpacing gs{{wy[0], groups > 1 ? wy[1] : 0.0f, groups > 2 ? wy[2] : 0.0f}};
+  for (long long l0 = 0; l0 < lines; l0 += batch) {
+    const long long nb = std::min(batch, lines - l0);
+    edt_envelope_groups<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, Dims{W, H, int(S)}, gs, per_group, 1, l0, nb,
+                                                            V.data(), Hb.data(), Z.data());
+    ++ctx.launches;
+    BK_CUDA(cudaGetLastError());
   }
 }
 

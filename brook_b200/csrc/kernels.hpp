@@ -61,6 +61,11 @@ struct EdtVolume {
 };
 void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume> &volumes, const float aniso[3],
                  float *out);
+// The black-border 2D EDT of a (W, H, groups * per_group) stack of images whose group g (per_group
+// consecutive slices) has spacing wx[g] along x and wy[g] along y: what edt(..., dims = 2) gives each
+// group, with the y passes of all groups in one launch.
+void edt_planes(Context &ctx, const uint32_t *ids, int W, int H, int groups, int per_group, const float wx[3],
+                const float wy[3], float *out);
 
 // EDT of uint32 labels with no device allocation (a fixed file-scope scratch in edt.cu); see there.
 void edt_fixed_scratch(const uint32_t *labels, VolumeDims d, const float aniso[3], bool black_border, float *out,
