@@ -167,11 +167,15 @@ __global__ void __launch_bounds__(kTileThreads, 4) tile_union(const L *__restric
     const bool in = lx < ex && ly < ey && lz < ez;
     const int h = at(lx, ly, lz);
     const L lv = in ? hal[h] : L(0);
+    // only the bits the rules below read: every forward neighbour (odd k), the backward faces
+    // (0, 2, 4) and the backward-y xy edges (6, 8), which corner pairs use as intermediates
+    constexpr unsigned kRead = 0x2AAAAAAu | 0x155u;
     unsigned m = 0;
     if (lv != L(0)) {
 #pragma unroll
       for (int k = 0; k < 26; ++k)
-        if (lz + c_dz[k] >= 0 && hal[h + c_dx[k] + kHaloX * (c_dy[k] + kHaloY * c_dz[k])] == lv) m |= 1u << k;
+        if (((kRead >> k) & 1u) && lz + c_dz[k] >= 0 && hal[h + c_dx[k] + kHaloX * (c_dy[k] + kHaloY * c_dz[k])] == lv)
+          m |= 1u << k;
     }
     const unsigned mprev = __shfl_up_sync(0xFFFFFFFFu, m, 1);  // the x-previous voxel's (same row)
     if (lv == L(0)) continue;
