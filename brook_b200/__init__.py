@@ -12,6 +12,7 @@ from ._intake import DEFAULT_TEASAR_PARAMS, DimensionError, skeletonize  # noqa:
 from ._packed import PackedSkeletons, Skeleton  # noqa: E402
 from .batch import BatchedSkeletons, skeletonize_batch  # noqa: E402
 from .chunked import merge_fragments, skeletonize_chunked  # noqa: E402
+from . import device_post  # noqa: E402
 
 __all__ = ["skeletonize", "skeletonize_batch", "skeletonize_chunked", "merge_fragments", "BatchedSkeletons",
-           "PackedSkeletons", "Skeleton", "DEFAULT_TEASAR_PARAMS", "DimensionError", "__version__"]
+           "PackedSkeletons", "Skeleton", "DEFAULT_TEASAR_PARAMS", "DimensionError", "device_post", "__version__"]

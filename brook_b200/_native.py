@@ -35,7 +35,8 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_array_upload", "brook_array_to_dlpack", "brook_array_to_dlpack_versioned", "brook_components_labels",
            "brook_skeletonize_batch_targets", "brook_context_wait_stream", "brook_autotune",
            "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons", "brook_context_trim",
-           "brook_context_set_engine_share"]
+           "brook_context_set_engine_share", "brook_postprocess_canonical", "brook_postprocess_step",
+           "brook_skeleton_components", "brook_skeletons_create_device"]
 
 
 class Volume(ctypes.Structure):
@@ -167,6 +168,10 @@ def _open():
         "brook_skeletons_create": (ctypes.c_int, [ctypes.POINTER(SkeletonsView), ctypes.POINTER(vp)]),
         "brook_merge_skeletons": (ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_float), sz,
                                                  ctypes.POINTER(vp)]),
+        "brook_postprocess_canonical": (ctypes.c_int, [vp, vp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(vp)]),
+        "brook_postprocess_step": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(vp)]),
+        "brook_skeleton_components": (ctypes.c_int, [vp, vp, ctypes.POINTER(vp)]),
+        "brook_skeletons_create_device": (ctypes.c_int, [vp, ctypes.POINTER(SkeletonsDeviceView), ctypes.POINTER(vp)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -342,6 +347,69 @@ def packed_device_arrays(handle):
                 edges=device(v.edges, (ne, 2), "<u4", torch.uint32),
                 radii=device(v.radii, (nv,), "<f4", torch.float32),
                 anisotropy=tuple(float(a) for a in v.anisotropy))
+
+
+def skeletons_handle(packed, device=0):
+    """A new brook_skeletons handle holding a copy of PackedSkeletons: host arrays through
+    brook_skeletons_create, CUDA tensors through brook_skeletons_create_device (on the device,
+    ordered after the current torch stream). The caller destroys it."""
+    lib = load()
+    h = ctypes.c_void_p()
+    if not packed.on_device:
+        p = packed
+        keep = [np.ascontiguousarray(p.labels, np.int64), np.ascontiguousarray(p.v_off, np.int64),
+                np.ascontiguousarray(p.e_off, np.int64), np.ascontiguousarray(p.vertices, np.float32).reshape(-1, 3),
+                np.ascontiguousarray(p.edges, np.uint32).reshape(-1, 2), np.ascontiguousarray(p.radii, np.float32)]
+        v = SkeletonsView()
+        v.skeleton_count, v.vertex_count, v.edge_count = len(keep[0]), len(keep[5]), len(keep[4])
+        v.labels = keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        v.vertex_offsets = keep[1].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        v.edge_offsets = keep[2].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        v.vertices = keep[3].ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        v.edges = keep[4].ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        v.radii = keep[5].ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        v.anisotropy[:] = [float(x) for x in p.anisotropy]
+        check(lib.brook_skeletons_create(ctypes.byref(v), ctypes.byref(h)))
+        return h.value
+    import torch
+
+    ctx = context(device)
+    check(lib.brook_context_wait_stream(ctx, torch.cuda.current_stream(device).cuda_stream))
+    tensors = [packed.vertices.contiguous(), packed.edges.contiguous(), packed.radii.contiguous()]
+    meta = [np.ascontiguousarray(packed.labels, np.int64), np.ascontiguousarray(packed.v_off, np.int64),
+            np.ascontiguousarray(packed.e_off, np.int64)]
+    v = SkeletonsDeviceView()
+    v.skeleton_count, v.vertex_count, v.edge_count = len(meta[0]), int(meta[1][-1]), int(meta[2][-1])
+    v.labels = meta[0].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    v.vertex_offsets = meta[1].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    v.edge_offsets = meta[2].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    for field, t, width, code in ((v.vertices, tensors[0], 3, 8), (v.edges, tensors[1], 2, 2), (v.radii, tensors[2], 1, 8)):
+        rows = t.numel() // width
+        field.struct_size, field.abi_version = ctypes.sizeof(Volume), ABI_VERSION
+        field.data = t.data_ptr() if rows else None
+        field.shape[:] = [width, rows, 1]
+        field.strides[:] = [4, 4 * width, 4 * width * rows]
+        field.dtype, field.memory = code, DEVICE
+    v.anisotropy[:] = [float(x) for x in packed.anisotropy]
+    check(lib.brook_skeletons_create_device(ctx, ctypes.byref(v), ctypes.byref(h)))
+    return h.value
+
+
+def array_tensor(array_handle):
+    """A brook_array as a torch tensor over its own device memory (DLPack, no copy); the array
+    handle is released (the export keeps the memory alive)."""
+    import torch
+
+    lib = load()
+    dl = ctypes.c_void_p()
+    try:
+        check(lib.brook_array_to_dlpack(array_handle, ctypes.byref(dl)))
+    finally:
+        lib.brook_array_destroy(array_handle)
+    make = ctypes.pythonapi.PyCapsule_New
+    make.restype = ctypes.py_object
+    make.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+    return torch.utils.dlpack.from_dlpack(make(dl.value, b"dltensor", None))
 
 
 def trim(device=0):

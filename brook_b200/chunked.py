@@ -30,66 +30,69 @@ def physical_origins(starts, anisotropy):
     return [tuple(float(np.float32(np.float32(s[k]) * a[k])) for k in range(3)) for s in starts]
 
 
-def _view_of(packed):
-    """A brook_skeletons_view over a host PackedSkeletons (the arrays must outlive its use)."""
-    p = packed.to_host()
-    keep = [np.ascontiguousarray(p.labels, np.int64), np.ascontiguousarray(p.v_off, np.int64),
-            np.ascontiguousarray(p.e_off, np.int64), np.ascontiguousarray(p.vertices, np.float32).reshape(-1, 3),
-            np.ascontiguousarray(p.edges, np.uint32).reshape(-1, 2), np.ascontiguousarray(p.radii, np.float32)]
-    v = _native.SkeletonsView()
-    v.skeleton_count, v.vertex_count, v.edge_count = len(keep[0]), len(keep[5]), len(keep[4])
-    v.labels = keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
-    v.vertex_offsets = keep[1].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
-    v.edge_offsets = keep[2].ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
-    v.vertices = keep[3].ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-    v.edges = keep[4].ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
-    v.radii = keep[5].ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-    v.anisotropy[:] = [float(x) for x in p.anisotropy]
-    return v, keep
-
-
-def _merge_handles(handles, origins, device, on_device):
+def _merge_handles(handles, origins, device):
+    """The brook_merge_skeletons device result of fragment handles (the caller destroys it)."""
     lib = _native.load()
     ctx = _native.context(device)
     arr = (ctypes.c_void_p * max(len(handles), 1))(*handles)
     flat = (ctypes.c_float * max(3 * len(origins), 1))(*[c for o in origins for c in o])
     out = ctypes.c_void_p()
     _native.check(lib.brook_merge_skeletons(ctx, arr, flat, len(handles), ctypes.byref(out)))
-    grab = _native.packed_device_arrays if on_device else _native.packed_arrays
-    return PackedSkeletons.from_arrays(grab(out))
+    return out.value
+
+
+def _postprocessed(handle, postprocess, device):
+    """The canonical device post-processing of a result handle (which it destroys), as a new
+    handle; `postprocess` is a dict of dust_threshold / tick_threshold (defaults 1500 / 3500)."""
+    lib = _native.load()
+    post = dict(postprocess)
+    unknown = set(post) - {"dust_threshold", "tick_threshold"}
+    if unknown:
+        lib.brook_skeletons_destroy(handle)
+        raise TypeError(f"brook_b200: unknown postprocess keys {sorted(unknown)}")
+    out = ctypes.c_void_p()
+    try:
+        _native.check(lib.brook_postprocess_canonical(_native.context(device), handle,
+                                                      float(post.get("dust_threshold", 1500)),
+                                                      float(post.get("tick_threshold", 3500)), ctypes.byref(out)))
+    finally:
+        lib.brook_skeletons_destroy(handle)
+    return out.value
 
 
 def merge_fragments(parts, origins, on_device=False, device=0):
-    """Merges PackedSkeletons fragments placed at `origins` (physical units) into one skeleton
-    per label, on the device; the result stays there when `on_device`."""
+    """Merges PackedSkeletons fragments (host or device) placed at `origins` (physical units)
+    into one skeleton per label, on the device; the result stays there when `on_device`."""
     parts, origins = list(parts), [tuple(float(c) for c in o) for o in origins]
     if len(parts) != len(origins):
         raise ValueError("fragment/origin count mismatch")
     lib = _native.load()
-    handles, keep = [], []
+    handles = []
     try:
         for p in parts:
-            view, arrays = _view_of(p)
-            keep.append(arrays)
-            h = ctypes.c_void_p()
-            _native.check(lib.brook_skeletons_create(ctypes.byref(view), ctypes.byref(h)))
-            handles.append(h.value)
-        return _merge_handles(handles, origins, device, on_device)
+            handles.append(_native.skeletons_handle(p, device))
+        merged = _merge_handles(handles, origins, device)
     finally:
         for h in handles:
             lib.brook_skeletons_destroy(h)
+    grab = _native.packed_device_arrays if on_device else _native.packed_arrays
+    return PackedSkeletons.from_arrays(grab(merged))
 
 
 def skeletonize_chunked(all_labels, chunk_shape=(512, 512, 512), overlap=1, teasar_params=DEFAULT_TEASAR_PARAMS,
                         anisotropy=(1, 1, 1), dust_threshold=1000, fix_branching=True, output="skeletons",
-                        postprocess=None, memory_budget=None, device=0):
+                        postprocess=None, postprocess_engine="device", memory_budget=None, device=0):
     """Skeletonizes a host volume in chunks of `chunk_shape` overlapping by `overlap` voxels
     (border targets on, as the reference forces) and merges the fragments. Returns
     {label: Skeleton}, PackedSkeletons ("packed") or the same on the device ("packed_device").
-    `memory_budget` (bytes, default: 80 % of the device's free memory) bounds the chunks run
-    together. Post-processing of the merged skeletons is not part of this build (raises)."""
-    if postprocess is not None:
-        raise NotImplementedError("brook_b200: post-processing of merged skeletons is not supported")
+    `postprocess` (a dict of dust_threshold / tick_threshold) runs the canonical post-processing
+    on the merged skeletons on the GPU (postprocess_engine "device", the reference's default;
+    its "kimimaro" CPU engine is not part of this library). `memory_budget` (bytes, default: 80 %
+    of the device's free memory) bounds the chunks run together."""
+    if postprocess_engine not in ("device", "kimimaro"):
+        raise ValueError("brook_b200: postprocess_engine must be 'device' or 'kimimaro'")
+    if postprocess is not None and postprocess_engine != "device":
+        raise NotImplementedError("brook_b200: the CPU (kimimaro) post-processing engine is not part of this library")
     if output not in ("skeletons", "packed", "packed_device"):
         raise ValueError("brook_b200: output must be 'skeletons', 'packed' or 'packed_device'")
     labels = format_labels(all_labels)
@@ -126,10 +129,14 @@ def skeletonize_chunked(all_labels, chunk_shape=(512, 512, 512), overlap=1, teas
             group.append(i)
             group_bytes += need
         flush()
-        merged = _merge_handles(handles, origins, device, on_device=output == "packed_device")
+        merged = _merge_handles(handles, origins, device)
     finally:
         for h in handles:
             lib.brook_skeletons_destroy(h)
+    if postprocess is not None:
+        merged = _postprocessed(merged, postprocess, device)
+    grab = _native.packed_device_arrays if output == "packed_device" else _native.packed_arrays
+    merged = PackedSkeletons.from_arrays(grab(merged))
     if output == "skeletons":
         return merged.to_skeletons()
     return merged

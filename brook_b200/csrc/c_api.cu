@@ -13,6 +13,7 @@
 #include "../../include/brook_b200_dlpack.h"
 #include "engine.hpp"
 #include "merge.hpp"
+#include "post.hpp"
 #include "pipeline.hpp"
 
 #ifndef BROOK_B200_VERSION
@@ -432,6 +433,24 @@ brook_status skeletonize_many(brook_context *ctx, const brook_volume *volumes, s
     }
     for (size_t i = 0; i < count; ++i) out[i] = handles[i].release();
   });
+}
+
+}  // namespace
+
+namespace {
+
+// A post-processing call on the context: its statistics and launch count are the call's own.
+template <class F>
+void post_call(brook_context *ctx, const brook_skeletons *input, F &&body) {
+  require(ctx && input);
+  std::lock_guard<std::mutex> lock(ctx->value.mutex());
+  bk::DeviceGuard guard(ctx->value.device());
+  const bk::Packed &p = input->packed;
+  if (p.on_device()) require(p.device_vertices->device == ctx->value.device(), "the skeletons are on another device");
+  ctx->value.stats.clear();
+  ctx->value.launches = 0;
+  body(p);
+  ctx->value.stats["launches"] = double(ctx->value.launches);
 }
 
 }  // namespace
@@ -883,6 +902,53 @@ brook_status brook_skeletons_create(const brook_skeletons_view *v, brook_skeleto
   });
 }
 
+brook_status brook_skeletons_create_device(brook_context *ctx, const brook_skeletons_device_view *v,
+                                           brook_skeletons **out) {
+  return protect([&] {
+    require(ctx && v && out);
+    *out = nullptr;
+    const size_t k = v->skeleton_count, nv = v->vertex_count, ne = v->edge_count;
+    require((v->labels || !k) && v->vertex_offsets && v->edge_offsets, "incomplete skeletons view");
+    require(v->vertex_offsets[0] == 0 && v->edge_offsets[0] == 0 && size_t(v->vertex_offsets[k]) == nv &&
+                size_t(v->edge_offsets[k]) == ne,
+            "inconsistent skeleton offsets");
+    for (size_t i = 0; i < k; ++i)
+      require(v->vertex_offsets[i] <= v->vertex_offsets[i + 1] && v->edge_offsets[i] <= v->edge_offsets[i + 1],
+              "inconsistent skeleton offsets");
+    // row-major device arrays: (3, V), (2, E), (1, V) elements of 4 bytes
+    auto check_rows = [&](const brook_volume &a, brook_dtype dtype, int width, size_t rows) {
+      require(a.struct_size >= sizeof(brook_volume) && a.abi_version == BROOK_ABI_VERSION, "incompatible brook_volume");
+      if (!rows) return;
+      require(a.data && a.memory == BROOK_DEVICE && a.dtype == dtype, "skeleton arrays must be device arrays");
+      require(a.shape[0] == width && size_t(a.shape[1]) == rows && a.strides[0] == 4 && a.strides[1] == 4LL * width,
+              "skeleton arrays must be row major and contiguous");
+    };
+    check_rows(v->vertices, BROOK_F32, 3, nv);
+    check_rows(v->edges, BROOK_U32, 2, ne);
+    check_rows(v->radii, BROOK_F32, 1, nv);
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    auto handle = std::make_unique<brook_skeletons>();
+    bk::Packed &p = handle->packed;
+    p.labels.assign(v->labels, v->labels + k);
+    p.vertex_offsets.assign(v->vertex_offsets, v->vertex_offsets + k + 1);
+    p.edge_offsets.assign(v->edge_offsets, v->edge_offsets + k + 1);
+    for (int a = 0; a < 3; ++a) p.anisotropy[a] = v->anisotropy[a];
+    const int dev = ctx->value.device();
+    p.device_vertices = std::make_shared<DeviceStorage>(nv * 3 * sizeof(float), dev);
+    p.device_edges = std::make_shared<DeviceStorage>(ne * 2 * sizeof(uint32_t), dev);
+    p.device_radii = std::make_shared<DeviceStorage>(nv * sizeof(float), dev);
+    cudaStream_t st = ctx->value.stream();
+    if (nv) {
+      BK_CUDA(cudaMemcpyAsync(p.device_vertices->ptr, v->vertices.data, nv * 3 * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      BK_CUDA(cudaMemcpyAsync(p.device_radii->ptr, v->radii.data, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
+    if (ne) BK_CUDA(cudaMemcpyAsync(p.device_edges->ptr, v->edges.data, ne * 2 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    ctx->value.synchronize();
+    *out = handle.release();
+  });
+}
+
 brook_status brook_merge_skeletons(brook_context *ctx, const brook_skeletons *const *fragments, const float *origins,
                                    size_t count, brook_skeletons **out) {
   return protect([&] {
@@ -903,6 +969,57 @@ brook_status brook_merge_skeletons(brook_context *ctx, const brook_skeletons *co
     auto handle = std::make_unique<brook_skeletons>();
     handle->packed = bk::merge_fragments(ctx->value, parts, shifts);
     *out = handle.release();
+  });
+}
+
+brook_status brook_postprocess_canonical(brook_context *ctx, const brook_skeletons *input, double dust_threshold,
+                                         double tick_threshold, brook_skeletons **out) {
+  return protect([&] {
+    require(out);
+    *out = nullptr;
+    post_call(ctx, input, [&](const bk::Packed &p) {
+      auto handle = std::make_unique<brook_skeletons>();
+      handle->packed = bk::post_process(ctx->value, p, bk::kPostprocess, dust_threshold, tick_threshold);
+      *out = handle.release();
+    });
+  });
+}
+
+brook_status brook_postprocess_step(brook_context *ctx, const brook_skeletons *input, int step, double threshold,
+                                    brook_skeletons **out) {
+  return protect([&] {
+    require(out);
+    *out = nullptr;
+    require(step >= BROOK_POST_REMOVE_DUST && step <= BROOK_POST_PRUNE_UNUSED, "unknown post-processing step");
+    post_call(ctx, input, [&](const bk::Packed &p) {
+      auto handle = std::make_unique<brook_skeletons>();
+      handle->packed = bk::post_process(ctx->value, p, step, threshold, 0.0);
+      *out = handle.release();
+    });
+  });
+}
+
+brook_status brook_skeleton_components(brook_context *ctx, const brook_skeletons *input, brook_array **out) {
+  return protect([&] {
+    require(out);
+    *out = nullptr;
+    post_call(ctx, input, [&](const bk::Packed &p) {
+      size_t n = 0;
+      auto handle = std::make_unique<brook_array>();
+      handle->storage = bk::skeleton_components(ctx->value, p, &n);
+      brook_volume v{};
+      v.struct_size = sizeof(v);
+      v.abi_version = BROOK_ABI_VERSION;
+      v.data = handle->storage->ptr;
+      v.dtype = BROOK_I64;
+      v.memory = BROOK_DEVICE;
+      v.shape[0] = 1; v.shape[1] = int64_t(n); v.shape[2] = 1;
+      v.strides[0] = 8; v.strides[1] = 8; v.strides[2] = 8LL * int64_t(n);
+      handle->view = v;
+      handle->bytes = n * sizeof(int64_t);
+      rows_tensor(*handle, 1, n);
+      *out = handle.release();
+    });
   });
 }
 

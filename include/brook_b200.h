@@ -229,6 +229,13 @@ brook_status brook_edt_device_noalloc(const brook_volume *labels, const float an
  * arrays, PackedSkeletons.to_core): a host result handle holding a copy of a packed view, e.g. to
  * merge skeletons a program kept as arrays. */
 brook_status brook_skeletons_create(const brook_skeletons_view *view, brook_skeletons **out);
+/* No counterpart in the reference's C header (its Python binding wraps device PackedSkeletons the
+ * same way, PackedSkeletons.to_core): a device result holding a copy, made on the context's stream,
+ * of packed skeletons whose vertices ({3, V}), edges ({2, E}) and radii ({1, V}) are row-major
+ * contiguous device arrays of the context's device; labels and offsets on the host. Work that
+ * produced the arrays on another stream must be ordered before the call (brook_context_wait_stream). */
+brook_status brook_skeletons_create_device(brook_context *context, const brook_skeletons_device_view *view,
+                                           brook_skeletons **out);
 /* brook.h:244-247: one skeleton per label over `count` fragments (the pieces of overlapping chunks),
  * fragment i's vertices shifted by origins[3i .. 3i+2] (physical units; NULL: no shift). Vertices
  * of one label at the same physical point merge (the first fragment's radius), edges are mapped,
@@ -236,6 +243,27 @@ brook_status brook_skeletons_create(const brook_skeletons_view *view, brook_skel
  * is a device result (as with BROOK_DEVICE_OUTPUT). */
 brook_status brook_merge_skeletons(brook_context *context, const brook_skeletons *const *fragments,
                                    const float *origins, size_t count, brook_skeletons **out);
+
+/* brook.h:238-239: canonical post-processing of skeletons (host or device result) on the device:
+ * remove_dust(dust_threshold), remove_loops, join_close_components, remove_ticks(tick_threshold)
+ * and the removal of vertices on no edge, with the reference's tie rules (post.cu:646-650). A
+ * threshold of 0 skips its step. Every label of the input stays, possibly empty. The result is a
+ * device result (as with BROOK_DEVICE_OUTPUT). */
+brook_status brook_postprocess_canonical(brook_context *context, const brook_skeletons *input,
+                                         double dust_threshold, double tick_threshold, brook_skeletons **out);
+/* No counterpart in the reference's C header (its Python binding exposes the same steps as context
+ * methods, src/brook/_device_post.py:23-44): one step of the canonical post-processing on its own;
+ * `threshold` is the dust or tick threshold of those two steps and is ignored by the others. */
+typedef enum brook_post_step {
+  BROOK_POST_REMOVE_DUST = 1, BROOK_POST_REMOVE_LOOPS = 2, BROOK_POST_JOIN_COMPONENTS = 3,
+  BROOK_POST_REMOVE_TICKS = 4, BROOK_POST_PRUNE_UNUSED = 5
+} brook_post_step;
+brook_status brook_postprocess_step(brook_context *context, const brook_skeletons *input, int step,
+                                    double threshold, brook_skeletons **out);
+/* No counterpart in the reference's C header (src/brook/_device_post.py:13-16): the connected
+ * component of every packed vertex, named by the smallest global vertex index in it, as an int64
+ * device array (one row per vertex). */
+brook_status brook_skeleton_components(brook_context *context, const brook_skeletons *input, brook_array **out);
 
 /* No counterpart in the reference's C header (the reference sizes its cooperative grids by a timed
  * probe, cooperative.cu:18-47). The object engine's launch choices for one workload class: the

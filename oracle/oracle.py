@@ -40,7 +40,8 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "oracle.cpp")):
+        newest = max(os.path.getmtime(os.path.join(_HERE, f)) for f in ("oracle.cpp", "post.cpp"))
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < newest:
             build()
         _lib = ctypes.CDLL(_LIB_PATH)
         _lib.oracle_run.restype = ctypes.c_void_p
