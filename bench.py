@@ -515,12 +515,53 @@ def options_measurement(local, steps=3):
     return out
 
 
-def extra_measurements(local):
+def post_measurement(local, packed, steps=3, dust=1500.0, ticks=3500.0):
+    """The canonical post-processing (the reference's defaults: dust 1500, ticks 3500) of the
+    workload's own skeletons on the device: the call's span on the stream (CUDA events, mean of
+    `steps` after a warm-up) and its wall time, each step's time, and the oracle's time for the same
+    input on one host core, the two outputs compared bit for bit."""
+    from brook_b200 import _native, device_post
+    from oracle import post as opost
+
+    dev_in = packed.to_device()
+    device_post.postprocess(dev_in, dust, ticks)
+    span, wall, stages = 0.0, 0.0, {}
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        out = device_post.postprocess(dev_in, dust, ticks)
+        wall += time.perf_counter() - t0
+        st = _native.stats(local)
+        span += st.get("ms_total", 0.0)
+        for k, v in st.items():
+            if k.startswith("ms_post_"):
+                stages[k[8:]] = stages.get(k[8:], 0.0) + v
+    got = out.to_host()
+    host = dict(labels=packed.labels, vertex_offsets=packed.v_off, edge_offsets=packed.e_off, vertices=packed.vertices,
+                edges=packed.edges, radii=packed.radii)
+    t0 = time.perf_counter()
+    ref = opost.postprocess(host, dust, ticks)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    identical = all(np.array_equal(np.asarray(a), np.asarray(b)) for a, b in (
+        (got.labels, ref["labels"]), (got.v_off, ref["vertex_offsets"]), (got.e_off, ref["edge_offsets"]),
+        (got.edges, ref["edges"]), (np.asarray(got.vertices).view(np.uint32), ref["vertices"].view(np.uint32)),
+        (np.asarray(got.radii).view(np.uint32), ref["radii"].view(np.uint32))))
+    return {"workload": f"canonical post-processing (dust {dust:g}, ticks {ticks:g}) of the workload's "
+                        f"{len(packed)} skeletons ({int(packed.v_off[-1])} vertices, {int(packed.e_off[-1])} edges)",
+            "ms_per_call": span / steps, "wall_ms_per_call": wall / steps * 1e3,
+            "stages_ms": {k: round(v / steps, 3) for k, v in sorted(stages.items())},
+            "out_vertices": int(got.v_off[-1]), "out_edges": int(got.e_off[-1]),
+            "cpu_oracle_ms": cpu_ms, "cpu_oracle_threads": 1, "identical": bool(identical),
+            "timing": "CUDA events on the context's stream across the call (host read-backs included), "
+                      "mean of 3 calls after a warm-up"}
+
+
+def extra_measurements(local, packed=None):
     """The metric's two comparisons beside the headline line, on the same GPU: the 64-volume uneven
     batch as one skeletonize_batch call against 64 plain calls (skeletons/s both ways, identical
     skeletons checked), and the request stream's p50/p99 latency at 50/200/800 req/s through the
-    continuous-batching server and the per-request path; and the fill_holes / fix_avocados options
-    on a volume with enclosed nuclei and cavities."""
+    continuous-batching server and the per-request path; the fill_holes / fix_avocados options
+    on a volume with enclosed nuclei and cavities; and the canonical post-processing of the
+    workload's own skeletons (`packed`)."""
     extras = {}
     try:
         b = batch_measurement(CONFIGS["batch64"], steps=3, warmup=2, local=local)
@@ -543,6 +584,11 @@ def extra_measurements(local):
         extras["options"] = options_measurement(local)
     except Exception as e:
         extras["options"] = {"error": f"{type(e).__name__}: {e}"}
+    if packed is not None:
+        try:
+            extras["post"] = post_measurement(local, packed)
+        except Exception as e:
+            extras["post"] = {"error": f"{type(e).__name__}: {e}"}
     return extras
 
 
@@ -654,10 +700,29 @@ def run_ours(args, cfg):
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(volume, cfg, os.cpu_count() or 1)
     if world == 1 and not args.no_extras:
-        out.update(extra_measurements(local))
+        out.update(extra_measurements(local, packed))
     print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def run_post(args, cfg):
+    """Only the canonical post-processing of the configuration's skeletons (one skeletonize call
+    makes them): the post_measurement figures as one JSON line; the profiling entry point of the
+    post-processing kernels."""
+    import torch
+
+    import brook_b200
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    volume = make_volume(cfg)
+    packed = brook_b200.skeletonize(volume, teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST,
+                                    output="packed", device=local)
+    r = post_measurement(local, packed, steps=args.steps)
+    print(json.dumps({"metric": "canonical post-processing ms per call", "value": r["ms_per_call"], "unit": "ms",
+                      "higher_is_better": False, "steps": args.steps, "config": {"workload": cfg["workload"]},
+                      "post": r}))
 
 
 def main():
@@ -670,9 +735,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batch and serving comparisons")
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's built-in launch rule")
+    ap.add_argument("--post-only", action="store_true",
+                    help="time only the canonical post-processing of the configuration's skeletons")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
-    if args.impl == "reference":
+    if args.post_only:
+        run_post(args, cfg)
+    elif args.impl == "reference":
         run_reference(args, cfg)
     elif cfg["kind"] == "batch":
         run_batch(args, cfg)

@@ -2,6 +2,9 @@
 over the brook_b200 C ABI."""
 from __future__ import annotations
 
+import os
+import warnings
+
 import numpy as np
 
 from . import _native
@@ -25,6 +28,13 @@ TRACE_DEFAULTS = {
     "soma_detection_threshold": 1100.0, "soma_acceptance_threshold": 4000.0,
     "soma_invalidation_scale": 0.5, "soma_invalidation_const": 0.0, "max_paths": None,
 }
+
+
+# Device bytes per voxel of an in-core call beyond its labels (the largest measured peak is 157 B at
+# 512^3), and the share of the free device memory an in-core call may take before skeletonize
+# streams the volume instead (the reference's rule, src/brook/_intake.py:43-56).
+_INCORE_BYTES_PER_VOXEL = 160
+_INCORE_MEMORY_FRACTION = 0.5
 
 
 class DimensionError(Exception):
@@ -109,6 +119,42 @@ def device_volume(labels):
     return _native.device_volume(cai["data"][0], shape, strides, dtype), labels
 
 
+def _use_streaming(streaming, labels, device):
+    """streaming as given; else BROOK_STREAMING (0 / off / false / no: in-core); else stream when the
+    in-core state would take more than half the device's free memory, or the volume holds 2^31
+    voxels or more (in-core calls index voxels with 31 bits)."""
+    if streaming is not None:
+        return bool(streaming)
+    env = os.environ.get("BROOK_STREAMING", "").strip().lower()
+    if env:
+        return env not in ("0", "off", "false", "no")
+    if labels.size >= (1 << 31) - 1:
+        return True
+    need = int(labels.size) * (labels.dtype.itemsize + _INCORE_BYTES_PER_VOXEL)
+    if need < (1 << 30):
+        return False
+    import torch
+
+    free, _ = torch.cuda.mem_get_info(device)
+    return need > _INCORE_MEMORY_FRACTION * free
+
+
+def _run_streamed(volume, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
+                  extra_after, device, device_output=False, budget=0):
+    """brook_skeletonize_streamed over a host volume, as PackedSkeletons."""
+    ctypes = _native.ctypes
+    opts = _native.options(params, anisotropy, dust_threshold, fix_branching, fix_borders, object_ids,
+                           extra_before, extra_after)
+    if device_output:
+        opts.flags |= _native.DEVICE_OUTPUT
+    lib = _native.load()
+    out = ctypes.c_void_p()
+    _native.check(lib.brook_skeletonize_streamed(_native.context(device), ctypes.byref(volume), ctypes.byref(opts),
+                                                 int(budget), ctypes.byref(out)))
+    grab = _native.packed_device_arrays if device_output else _native.packed_arrays
+    return PackedSkeletons.from_arrays(grab(out.value))
+
+
 def _run(volumes, params, anisotropy, object_ids, dust_threshold, fix_branching, fix_borders, extra_before,
          extra_after, device, device_output=False, producers=(), sample_targets=None, fill_holes=False,
          fix_avocados=False):
@@ -178,8 +224,12 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     ascending id, a component whose voxels an earlier fill painted is not filled);
     `fix_avocados` merges pits (an object whose distance field passes soma_detection_threshold / 2.5
     and that another object encloses) into the objects around them (Kimimaro's rule). `parallel`,
-    `parallel_chunk_size`, `in_place`, `progress`, `borrow` and `streaming` are accepted for
-    compatibility. `voxel_graph` is not supported by this build and raises.
+    `streaming` (host input only): None streams when the in-core state would take more than half
+    the device's free memory (BROOK_STREAMING overrides), True always, False never; a streamed call
+    gives the same skeletons within a device budget (BROOK_STREAM_BUDGET_MB, default a quarter of
+    the free memory) and refuses fill_holes / fix_avocados, as the reference's does.
+    `parallel_chunk_size`, `in_place`, `progress` and `borrow` are accepted for compatibility.
+    `voxel_graph` is not supported by this build and raises.
     """
     if output not in ("skeletons", "packed", "packed_device"):
         raise ValueError("brook_b200: output must be 'skeletons', 'packed' or 'packed_device'")
@@ -188,7 +238,10 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
     params = teasar(teasar_params)
     anisotropy = tuple(float(a) for a in np.asarray(anisotropy, dtype=np.float32))
     producers = []
+    streamed = False
     if _is_device(all_labels):
+        if streaming:
+            raise NotImplementedError("streaming is a host-input feature")
         volume, keep = device_volume(all_labels)
         producers.append(producer_stream(all_labels, stream))
     else:
@@ -196,13 +249,26 @@ def skeletonize(all_labels, teasar_params=DEFAULT_TEASAR_PARAMS, anisotropy=(1, 
         if keep.size <= dust_threshold:
             packed = PackedSkeletons.empty(anisotropy)
             return {} if output == "skeletons" else packed
+        streamed = _use_streaming(streaming, keep, device)
+        if streamed and (fill_holes or fix_avocados):
+            raise NotImplementedError("brook streaming mode does not support voxel_graph, fill_holes or fix_avocados; "
+                                      "pass streaming=False or process the volume in chunks.")
+        if streamed and streaming is None and not os.environ.get("BROOK_STREAMING", "").strip():
+            warnings.warn(f"brook_b200: a {tuple(keep.shape)} volume does not fit in GPU memory; it is streamed "
+                          "(components by slabs, each traced component in its bounding box). "
+                          "brook_b200.skeletonize_chunked() processes overlapping chunks at in-core speed.",
+                          stacklevel=2)
         volume = _native.host_volume(keep)
     ids = None if object_ids is None else [int(i) for i in object_ids]
-    packed = _run([volume], params, anisotropy, ids, dust_threshold, fix_branching, fix_borders,
-                  [tuple(int(c) for c in p) for p in extra_targets_before],
-                  [tuple(int(c) for c in p) for p in extra_targets_after], device,
-                  device_output=output == "packed_device", producers=producers, fill_holes=fill_holes,
-                  fix_avocados=fix_avocados)[0]
+    before = [tuple(int(c) for c in p) for p in extra_targets_before]
+    after = [tuple(int(c) for c in p) for p in extra_targets_after]
+    if streamed:
+        packed = _run_streamed(volume, params, anisotropy, ids, dust_threshold, fix_branching, fix_borders, before,
+                               after, device, device_output=output == "packed_device")
+    else:
+        packed = _run([volume], params, anisotropy, ids, dust_threshold, fix_branching, fix_borders, before, after,
+                      device, device_output=output == "packed_device", producers=producers, fill_holes=fill_holes,
+                      fix_avocados=fix_avocados)[0]
     del keep
     if output == "skeletons":
         return packed.to_skeletons()

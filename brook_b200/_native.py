@@ -36,7 +36,8 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_skeletonize_batch_targets", "brook_context_wait_stream", "brook_autotune",
            "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons", "brook_context_trim",
            "brook_context_set_engine_share", "brook_postprocess_canonical", "brook_postprocess_step",
-           "brook_skeleton_components", "brook_skeletons_create_device"]
+           "brook_skeleton_components", "brook_skeletons_create_device", "brook_connected_components_streamed",
+           "brook_host_components_destroy", "brook_host_components_view", "brook_skeletonize_streamed"]
 
 
 class Volume(ctypes.Structure):
@@ -172,6 +173,14 @@ def _open():
         "brook_postprocess_step": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(vp)]),
         "brook_skeleton_components": (ctypes.c_int, [vp, vp, ctypes.POINTER(vp)]),
         "brook_skeletons_create_device": (ctypes.c_int, [vp, ctypes.POINTER(SkeletonsDeviceView), ctypes.POINTER(vp)]),
+        "brook_connected_components_streamed": (ctypes.c_int, [vp, ctypes.POINTER(Volume), sz, ctypes.POINTER(vp)]),
+        "brook_host_components_destroy": (None, [vp]),
+        "brook_host_components_view": (ctypes.c_int, [vp, ctypes.POINTER(Volume),
+                                                      ctypes.POINTER(ctypes.POINTER(ctypes.c_int64)),
+                                                      ctypes.POINTER(ctypes.POINTER(ctypes.c_int64)),
+                                                      ctypes.POINTER(sz)]),
+        "brook_skeletonize_streamed": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(Options), sz,
+                                                      ctypes.POINTER(vp)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

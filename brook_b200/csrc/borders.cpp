@@ -102,14 +102,13 @@ std::array<float, 4> tie_keys(int64_t ix, int64_t iy, float cx, float cy, int64_
 
 }  // namespace
 
-std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const uint32_t *ids,
-                                                            const std::vector<BorderVolume> &volumes,
-                                                            const float aniso[3]) {
+std::vector<Face> face_list(const std::vector<BorderVolume> &volumes, int &W, int &H) {
   // faces grouped by axis pair t: (a, b) = (x, y), (x, z), (y, z); within a group volume-major,
   // the low face (c = 0) before the high one
   const int axes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
   std::vector<Face> faces;
-  int W = 1, H = 1;
+  W = 1;
+  H = 1;
   for (int t = 0; t < 3; ++t)
     for (const auto &v : volumes)
       for (int side = 0; side < 2; ++side) {
@@ -120,6 +119,15 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
         H = std::max(H, f.fx());
         faces.push_back(f);
       }
+  return faces;
+}
+
+std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const uint32_t *ids,
+                                                            const std::vector<BorderVolume> &volumes,
+                                                            const float aniso[3], const uint32_t *given_stack) {
+  const int axes[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
+  int W = 1, H = 1;
+  const std::vector<Face> faces = face_list(volumes, W, H);
   std::vector<std::vector<std::vector<Point>>> out(volumes.size());
   for (size_t v = 0; v < volumes.size(); ++v) out[v].resize(size_t(volumes[v].count) + 1);
   if (volumes.empty()) return out;
@@ -134,7 +142,11 @@ std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const 
     t0 = now;
   };
   Buffer<uint32_t> stack(ctx, slice * S), stack_ids(ctx, slice * S);
-  extract_faces(ctx, ids, faces, W, H, stack.data());
+  if (given_stack)
+    BK_CUDA(cudaMemcpyAsync(stack.data(), given_stack, size_t(slice * S) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                            ctx.stream()));
+  else
+    extract_faces(ctx, ids, faces, W, H, stack.data());
   const VolumeDims sd{W, H, int(S)};
   ComponentsResult pc = connected_components(ctx, stack.data(), U32, sd, stack_ids.data(), true);
   lap("components");

@@ -14,6 +14,7 @@
 #include "engine.hpp"
 #include "merge.hpp"
 #include "post.hpp"
+#include "streamed.hpp"
 #include "pipeline.hpp"
 
 #ifndef BROOK_B200_VERSION
@@ -40,6 +41,12 @@ struct brook_components {
   std::shared_ptr<DeviceStorage> storage;
   brook_volume view{};
   size_t bytes = 0;
+  std::vector<int64_t> mapping, roots;
+};
+
+struct brook_host_components {
+  std::vector<unsigned char> ids;  // narrowed to the smallest of u8 / u16 / u32 that holds the count
+  brook_volume view{};
   std::vector<int64_t> mapping, roots;
 };
 
@@ -898,6 +905,85 @@ brook_status brook_skeletons_create(const brook_skeletons_view *v, brook_skeleto
     p.radii.assign(v->radii, v->radii + nv);
     p.edges.assign(v->edges, v->edges + 2 * ne);
     for (int a = 0; a < 3; ++a) p.anisotropy[a] = v->anisotropy[a];
+    *out = handle.release();
+  });
+}
+
+// A host volume of integer labels for the streamed entry points.
+bk::HostVolume host_labels(const brook_volume *v) {
+  require(v, "null volume");
+  require(v->struct_size >= sizeof(brook_volume) && v->abi_version == BROOK_ABI_VERSION, "incompatible brook_volume");
+  require(v->memory == BROOK_HOST, "streamed calls take host volumes");
+  require(v->dtype >= BROOK_U8 && v->dtype <= BROOK_I64, "integer labels required");
+  for (int a = 0; a < 3; ++a) require(v->shape[a] >= 0 && v->shape[a] < (1LL << 31), "invalid volume shape");
+  bk::HostVolume hv;
+  hv.data = v->data;
+  hv.dtype = int(v->dtype);
+  hv.d = bk::VolumeDims{int(v->shape[0]), int(v->shape[1]), int(v->shape[2])};
+  for (int a = 0; a < 3; ++a) hv.strides[a] = v->strides[a];
+  require(hv.data || hv.d.n() == 0);
+  return hv;
+}
+
+brook_status brook_connected_components_streamed(brook_context *ctx, const brook_volume *labels, size_t budget_bytes,
+                                                 brook_host_components **out) {
+  return protect([&] {
+    require(ctx && labels && out);
+    *out = nullptr;
+    const bk::HostVolume hv = host_labels(labels);
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    ctx->value.stats.clear();
+    ctx->value.launches = 0;
+    auto cc = bk::connected_components_streamed(ctx->value, hv, bk::stream_budget(budget_bytes), nullptr);
+    auto handle = std::make_unique<brook_host_components>();
+    const brook_dtype dtype = cc.count <= 0xFF ? BROOK_U8 : cc.count <= 0xFFFF ? BROOK_U16 : BROOK_U32;
+    const size_t b = bk::label_bytes(dtype), n = cc.ids.size();
+    handle->ids.resize(n * b);
+    if (b == 4) std::memcpy(handle->ids.data(), cc.ids.data(), n * 4);
+    else if (b == 2) for (size_t i = 0; i < n; ++i) reinterpret_cast<uint16_t *>(handle->ids.data())[i] = uint16_t(cc.ids[i]);
+    else for (size_t i = 0; i < n; ++i) handle->ids[i] = uint8_t(cc.ids[i]);
+    brook_volume &v = handle->view;
+    v.struct_size = sizeof(v);
+    v.abi_version = BROOK_ABI_VERSION;
+    v.data = handle->ids.data();
+    v.dtype = dtype;
+    v.memory = BROOK_HOST;
+    v.shape[0] = hv.d.sx; v.shape[1] = hv.d.sy; v.shape[2] = hv.d.sz;
+    v.strides[0] = int64_t(b); v.strides[1] = int64_t(b) * hv.d.sx; v.strides[2] = int64_t(b) * hv.d.sx * hv.d.sy;
+    handle->mapping = std::move(cc.mapping);
+    handle->roots = std::move(cc.roots);
+    ctx->value.stats["streamed_slabs"] = cc.slabs;
+    ctx->value.stats["launches"] = double(ctx->value.launches);
+    *out = handle.release();
+  });
+}
+
+void brook_host_components_destroy(brook_host_components *c) { delete c; }
+
+brook_status brook_host_components_view(const brook_host_components *c, brook_volume *labels, const int64_t **mapping,
+                                        const int64_t **roots, size_t *count) {
+  return protect([&] {
+    require(c);
+    if (labels) *labels = c->view;
+    if (mapping) *mapping = c->mapping.data();
+    if (roots) *roots = c->roots.data();
+    if (count) *count = c->roots.size();
+  });
+}
+
+brook_status brook_skeletonize_streamed(brook_context *ctx, const brook_volume *labels,
+                                        const brook_skeletonize_options *p, size_t budget_bytes,
+                                        brook_skeletons **out) {
+  return protect([&] {
+    require(ctx && labels && p && out);
+    *out = nullptr;
+    const bk::HostVolume hv = host_labels(labels);
+    const bk::Options options = options_of(p);
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    auto handle = std::make_unique<brook_skeletons>();
+    handle->packed = bk::skeletonize_streamed(ctx->value, hv, options, budget_bytes);
     *out = handle.release();
   });
 }

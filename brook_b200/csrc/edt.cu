@@ -23,6 +23,8 @@ constexpr int kWarpsX = 4;
 // The x pass's dynamic shared memory (kWarpsX line starts per CTA) is at most this.
 constexpr size_t kEdtXMaxSmem = 200 * 1024;
 
+// bb (here and in the envelope passes): walls beyond the line's ends, bit 0 before the first voxel,
+// bit 1 after the last (a black border sets both).
 __global__ void edt_x(const uint32_t *__restrict__ ids, float *__restrict__ D, Dims d, const float *__restrict__ acc,
                       int bb, int finish) {
   extern __shared__ int s_start[];
@@ -70,8 +72,8 @@ __global__ void edt_x(const uint32_t *__restrict__ ids, float *__restrict__ D, D
     if (in) {
       const int c = start[p];
       float best = __uint_as_float(BK_INF_BITS);
-      if (c > 0 || bb) { const float dd = acc[p - c + 1]; const float v = __fmul_rn(dd, dd); if (v < best) best = v; }
-      if (en < sx - 1 || bb) { const float dd = acc[en + 1 - p]; const float v = __fmul_rn(dd, dd); if (v < best) best = v; }
+      if (c > 0 || (bb & 1)) { const float dd = acc[p - c + 1]; const float v = __fmul_rn(dd, dd); if (v < best) best = v; }
+      if (en < sx - 1 || (bb & 2)) { const float dd = acc[en + 1 - p]; const float v = __fmul_rn(dd, dd); if (v < best) best = v; }
       if (finish) best = lab == 0 ? 0.0f : sqrtf(best);
       D[base + p] = best;
     }
@@ -177,7 +179,7 @@ __device__ void envelope_line(const uint32_t *__restrict__ ids, float *__restric
       c = p;
       L = lab;
       k = -1;
-      if (L != 0 && (c > 0 || bb)) { k = 0; push(0, c - 1, 0.0f, -1e300); }
+      if (L != 0 && (c > 0 || (bb & 1))) { k = 0; push(0, c - 1, 0.0f, -1e300); }
     }
     if (L != 0 && hf < kInf) place(p, (double)hf);
   };
@@ -195,7 +197,7 @@ __device__ void envelope_line(const uint32_t *__restrict__ ids, float *__restric
     a0 = b0; a1 = b1; a2 = b2; a3 = b3;
     f0 = g0; f1 = g1; f2 = g2; f3 = g3;
   }
-  finish_run(n - 1, bb != 0);
+  finish_run(n - 1, (bb & 2) != 0);
 }
 
 // Line `line` of the y (axis 1) or z (axis 2) pass of a (sx, sy, sz) volume at `offset`.
@@ -288,7 +290,7 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
   const long long xlines = (long long)vd.sy * vd.sz;
   const bool only_x = dims == 1 || (vd.sy == 1 && vd.sz == 1 && dims == 1);
   edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(ids, D, d, dacc.data(),
-                                                                                black_border ? 1 : 0, only_x ? 1 : 0); ++ctx.launches;
+                                                                                black_border ? 3 : 0, only_x ? 1 : 0); ++ctx.launches;
   BK_CUDA(cudaGetLastError());
   for (int axis = 1; axis < dims; ++axis) {
     const int len = axis == 1 ? vd.sy : vd.sz;
@@ -301,7 +303,7 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
     const int last = axis == dims - 1;
     for (long long l0 = 0; l0 < lines; l0 += batch) {
       const long long nb = std::min(batch, lines - l0);
-      edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, axis, aniso[axis], black_border ? 1 : 0, l0, nb,
+      edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, axis, aniso[axis], black_border ? 3 : 0, l0, nb,
                                                       V.data(), H.data(), Z.data(), last); ++ctx.launches;
       BK_CUDA(cudaGetLastError());
     }
@@ -324,7 +326,7 @@ void edt_planes(Context &ctx, const uint32_t *ids, int W, int H, int groups, int
     Buffer<float> dacc = to_device(ctx, acc);
     const long long lines = (long long)H * per_group;
     edt_x<<<(unsigned)((lines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(
-        ids + slice * per_group * g, D + slice * per_group * g, Dims{W, H, per_group}, dacc.data(), 1, 0);
+        ids + slice * per_group * g, D + slice * per_group * g, Dims{W, H, per_group}, dacc.data(), 3, 0);
     ++ctx.launches;
   }
   BK_CUDA(cudaGetLastError());
@@ -338,11 +340,17 @@ void edt_planes(Context &ctx, const uint32_t *ids, int W, int H, int groups, int
   GroupSpacing gs{{wy[0], groups > 1 ? wy[1] : 0.0f, groups > 2 ? wy[2] : 0.0f}};
   for (long long l0 = 0; l0 < lines; l0 += batch) {
     const long long nb = std::min(batch, lines - l0);
-    edt_envelope_groups<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, Dims{W, H, int(S)}, gs, per_group, 1, l0, nb,
+    edt_envelope_groups<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, Dims{W, H, int(S)}, gs, per_group, 3, l0, nb,
                                                             V.data(), Hb.data(), Z.data());
     ++ctx.launches;
     BK_CUDA(cudaGetLastError());
   }
+}
+
+// The walls of a volume's lines along `axis`: bit 0 the low end, bit 1 the high end.
+static int walls(const EdtVolume &v, int axis) {
+  if (v.faces < 0) return v.black_border ? 3 : 0;
+  return (v.faces >> (2 * axis)) & 3;
 }
 
 void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume> &vols, const float aniso[3], float *D) {
@@ -363,7 +371,7 @@ void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume>
     if (!v.d.n()) continue;
     const long long xlines = (long long)v.d.sy * v.d.sz;
     edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(
-        ids + v.offset, D + v.offset, Dims{v.d.sx, v.d.sy, v.d.sz}, dacc.data(), v.black_border ? 1 : 0, 0);
+        ids + v.offset, D + v.offset, Dims{v.d.sx, v.d.sy, v.d.sz}, dacc.data(), walls(v, 0), 0);
     ++ctx.launches;
   }
   BK_CUDA(cudaGetLastError());
@@ -374,7 +382,7 @@ void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume>
     int len = 1;
     for (const auto &v : vols) {
       if (!v.d.n()) continue;
-      table.push_back({v.offset, lines, v.d.sx, v.d.sy, v.d.sz, v.black_border ? 1 : 0});
+      table.push_back({v.offset, lines, v.d.sx, v.d.sy, v.d.sz, walls(v, axis)});
       lines += axis == 1 ? (long long)v.d.sx * v.d.sz : (long long)v.d.sx * v.d.sy;
       len = std::max(len, axis == 1 ? v.d.sy : v.d.sz);
     }
@@ -472,7 +480,7 @@ void edt_fixed_scratch(const uint32_t *labels, VolumeDims vd, const float aniso[
   allow_edt_x_smem();
   const long long xlines = (long long)vd.sy * vd.sz;
   edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(labels, D, d, acc,
-                                                                                black_border ? 1 : 0, 0);
+                                                                                black_border ? 3 : 0, 0);
   BK_CUDA(cudaGetLastError());
   for (int axis = 1; axis < 3; ++axis) {
     const int len = axis == 1 ? vd.sy : vd.sz;
@@ -485,7 +493,7 @@ void edt_fixed_scratch(const uint32_t *labels, VolumeDims vd, const float aniso[
     float *H = reinterpret_cast<float *>(V + batch * (len + 3));
     for (long long l0 = 0; l0 < lines; l0 += batch) {
       const long long nb = std::min(batch, lines - l0);
-      edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(labels, D, d, axis, aniso[axis], black_border ? 1 : 0, l0, nb,
+      edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(labels, D, d, axis, aniso[axis], black_border ? 3 : 0, l0, nb,
                                                       V, H, Z, axis == 2);
       BK_CUDA(cudaGetLastError());
     }

@@ -58,6 +58,9 @@ struct EdtVolume {
   long long offset;
   VolumeDims d;
   bool black_border;
+  // Per-face walls (bit 2a: the low face of axis a, bit 2a + 1: its high face) for a crop of a
+  // larger volume; -1: every face or none, by black_border.
+  int faces = -1;
 };
 void edt_volumes(Context &ctx, const uint32_t *ids, const std::vector<EdtVolume> &volumes, const float aniso[3],
                  float *out);
@@ -163,8 +166,12 @@ struct BorderVolume {
   VolumeDims d;
   int64_t count;     // component ids 1..count
 };
+// given_stack: the volumes' faces already in the layout extract_faces writes (a device array of
+// W * H * faces, from face_list's order and extents), used instead of reading them from ids.
 std::vector<std::vector<std::vector<Point>>> border_targets(Context &ctx, const uint32_t *ids,
                                                             const std::vector<BorderVolume> &volumes,
-                                                            const float aniso[3]);
+                                                            const float aniso[3], const uint32_t *given_stack = nullptr);
+// The faces of the volumes in the border stage's stack order, and the stack's slice extents.
+std::vector<Face> face_list(const std::vector<BorderVolume> &volumes, int &W, int &H);
 
 }  // namespace bk

@@ -140,9 +140,16 @@ struct VolumeState {
   std::vector<int> object_of;  // id -> global object index, -1 when inactive
   bool empty = true;
   bool black_border = false;   // one component filling the volume as given
+  int faces = -1;              // the EDT's walls of a crop (DeviceVolume::faces)
+  std::array<int, 3> origin{0, 0, 0};
+  const std::vector<std::vector<Point>> *given_borders = nullptr;
 };
 
 }  // namespace
+
+Buffer<unsigned char> select_labels(Context &ctx, const DeviceVolume &v, const std::vector<int64_t> &ids) {
+  return filter_volume(ctx, v, ids);
+}
 
 std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &volumes, const Options &opt) {
   cudaStream_t s = ctx.stream();
@@ -177,6 +184,9 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   for (size_t v = 0; v < volumes.size(); ++v) {
     vs[v].d = volumes[v].d;
     vs[v].offset = N;
+    vs[v].faces = volumes[v].faces;
+    vs[v].origin = volumes[v].origin;
+    vs[v].given_borders = volumes[v].borders;
     const long long n = volumes[v].d.n();
     if (n > 0 && double(n) > opt.dust) { N += n; vs[v].empty = false; }
   }
@@ -241,7 +251,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   {
     std::vector<EdtVolume> ev;
     for (const auto &st : vs)
-      if (!st.empty) ev.push_back({st.offset, st.d, st.black_border});
+      if (!st.empty) ev.push_back({st.offset, st.d, st.black_border, st.faces});
     edt_volumes(ctx, ids.data(), ev, aniso, dbf.data());
     clock.mark("edt");
   }
@@ -286,8 +296,17 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   if (opt.fix_borders) {
     std::vector<BorderVolume> bv;
     std::vector<size_t> which;
-    for (size_t v = 0; v < vs.size(); ++v)
-      if (!vs[v].empty) { bv.push_back({vs[v].offset, vs[v].d, vs[v].cc.count}); which.push_back(v); }
+    for (size_t v = 0; v < vs.size(); ++v) {
+      if (vs[v].empty) continue;
+      if (vs[v].given_borders) {
+        if (vs[v].given_borders->size() < size_t(vs[v].cc.count) + 1)
+          throw std::invalid_argument("given border targets do not cover the volume's components");
+        vs[v].borders = *vs[v].given_borders;
+        continue;
+      }
+      bv.push_back({vs[v].offset, vs[v].d, vs[v].cc.count});
+      which.push_back(v);
+    }
     auto picks = border_targets(ctx, ids.data(), bv, aniso);
     for (size_t j = 0; j < which.size(); ++j) vs[which[j]].borders = std::move(picks[j]);
     clock.mark("borders");
@@ -788,7 +807,9 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
     arena_off[r] = arena_offset[r];
     arena_dim[r] = {arena_dims[3 * r], arena_dims[3 * r + 1], arena_dims[3 * r + 2]};
   }
-  for (size_t j = 0; j < somas.size(); ++j) arena_origin[vs.size() + j] = somas[j].lo;
+  for (size_t v = 0; v < vs.size(); ++v) arena_origin[v] = vs[v].origin;
+  for (size_t j = 0; j < somas.size(); ++j)
+    for (int k = 0; k < 3; ++k) arena_origin[vs.size() + j][k] = somas[j].lo[k] + vs[somas[j].volume].origin[k];
   AssemblyResult asmb = assemble(ctx, cstore.data(), dbf.data(), ap, arena_off, arena_dim, arena_origin, aniso);
   const long long V = asmb.vertex_offsets.back(), E = asmb.edge_offsets.back();
   std::vector<float> hvert, hrad;

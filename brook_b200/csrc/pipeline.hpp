@@ -52,8 +52,18 @@ struct DeviceVolume {
   int dtype = U32;
   VolumeDims d;
   const Slabs *slabs = nullptr;  // non-null: still arriving by slabs (kernels.hpp)
+  // A crop of a larger volume (the out-of-core path): the EDT's walls per face (EdtVolume::faces;
+  // -1: the black-border rule), the crop's corner in the larger volume (output vertices come out
+  // in that volume's frame), and, when non-null, the border targets per component id (this
+  // volume's frame) to use instead of the ones of this volume's own faces.
+  int faces = -1;
+  std::array<int, 3> origin{0, 0, 0};
+  const std::vector<std::vector<Point>> *borders = nullptr;
 };
 
 std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &volumes, const Options &options);
+
+// The volume's labels with every label not in `ids` set to 0 (same element type, on the device).
+Buffer<unsigned char> select_labels(Context &ctx, const DeviceVolume &v, const std::vector<int64_t> &ids);
 
 }  // namespace bk

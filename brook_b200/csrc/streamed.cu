@@ -1,0 +1,536 @@
+// Out-of-core skeletonization: the reference's streamed mode (brook_skeletonize_streamed and
+// brook_connected_components_streamed, cpp/include/brook/brook.h:173-206; streaming_ccl.cu and
+// streaming_trace.cu:99-162 of giorgioangel/brook) for host volumes whose in-core state does not fit
+// on the device.
+//
+// Components: z-slabs sized to the budget go through the in-core CCL one after another (labels
+// gathered into page-locked staging, ids copied back to host memory); the seam between two slabs
+// gives the pairs (id in the last plane of one, id in the first plane of the next) of 26-adjacent
+// voxels with the same label, one kernel and one radix sort per seam; a union-find over the slabs'
+// ids on the host, by smallest (slab, id), numbers the components by ascending first flat index,
+// which is the in-core numbering; the host id volume is renumbered in place by threads.
+// Skeletons: each traced component (more voxels than dust, a box of two or more voxels) runs in its
+// bounding box as a crop of its own voxels. A crop's EDT has a wall on every face where the box is
+// inside the volume (the voxels beyond belong to other components or the background) and the
+// volume's black-border rule where the box meets the volume's edge, so its distances are the whole
+// volume's; its border targets come from the six faces of the whole volume (planar stage over a
+// face stack built on the host), its extra targets by the component they fall on; vertices come out
+// in the volume's frame. Crops run batched (the in-core pipeline, one call per batch) within the
+// budget, and the crops' skeletons are merged per label on the device (same points, same
+// consolidation: the in-core skeletons), labels in the in-core order.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <thread>
+
+#include "merge.hpp"
+#include "streamed.hpp"
+
+namespace bk {
+namespace {
+
+using u64 = unsigned long long;
+
+// Page-locked host staging.
+struct Pinned {
+  void *data = nullptr;
+  explicit Pinned(size_t bytes) {
+    if (bytes) BK_CUDA(cudaHostAlloc(&data, bytes, cudaHostAllocDefault));
+  }
+  ~Pinned() {
+    if (data) cudaFreeHost(data);
+  }
+  Pinned(const Pinned &) = delete;
+  Pinned &operator=(const Pinned &) = delete;
+};
+
+template <class F>
+void parallel_for(long long n, F &&fn) {
+  const long long threads = std::max(1LL, std::min<long long>(n, std::thread::hardware_concurrency()));
+  if (threads <= 1) {
+    for (long long i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (long long t = 0; t < threads; ++t)
+    pool.emplace_back([&, t] {
+      for (long long i = t; i < n; i += threads) fn(i);
+    });
+  for (auto &th : pool) th.join();
+}
+
+// z planes [z0, z1) of the host volume into an F-ordered buffer.
+void gather_slab(const HostVolume &hv, int z0, int z1, unsigned char *dst) {
+  const size_t b = label_bytes(hv.dtype), sx = size_t(hv.d.sx), sy = size_t(hv.d.sy);
+  const auto *src = static_cast<const unsigned char *>(hv.data);
+  const auto &st = hv.strides;
+  if (st[0] == (long long)b && st[1] == (long long)(b * sx) && st[2] == (long long)(b * sx * sy)) {
+    std::memcpy(dst, src + size_t(z0) * sx * sy * b, size_t(z1 - z0) * sx * sy * b);
+    return;
+  }
+  parallel_for(z1 - z0, [&](long long k) {
+    const long long z = z0 + k;
+    for (size_t y = 0; y < sy; ++y) {
+      unsigned char *out = dst + ((size_t(k) * sy + y) * sx) * b;
+      const unsigned char *row = src + z * st[2] + (long long)y * st[1];
+      if (st[0] == (long long)b) {
+        std::memcpy(out, row, sx * b);
+      } else {
+        for (size_t x = 0; x < sx; ++x) std::memcpy(out + x * b, row + (long long)x * st[0], b);
+      }
+    }
+  });
+}
+
+// The 26-adjacent same-label pairs across a seam: voxel (x, y) of the next slab's first plane and
+// (x + dx, y + dy) of the previous slab's last plane, as (previous id << 32 | next id); all ones
+// where there is none.
+template <class T>
+__global__ void seam_pairs(const T *prev_labels, const uint32_t *prev_ids, const T *next_labels,
+                           const uint32_t *next_ids, int sx, int sy, u64 *pairs) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)sx * sy) return;
+  u64 *out = pairs + 9 * i;
+  for (int k = 0; k < 9; ++k) out[k] = ~0ull;
+  const T l = next_labels[i];
+  if (l == T(0)) return;
+  const int x = int(i % sx), y = int(i / sx);
+  const u64 id = next_ids[i];
+  int k = 0;
+  for (int dy = -1; dy <= 1; ++dy)
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int px = x + dx, py = y + dy;
+      if (px < 0 || py < 0 || px >= sx || py >= sy) continue;
+      const long long j = px + (long long)sx * py;
+      if (prev_labels[j] == l) out[k++] = (u64(prev_ids[j]) << 32) | id;
+    }
+}
+
+void launch_seam(Context &ctx, int dtype, const void *prev_labels, const uint32_t *prev_ids, const void *next_labels,
+                 const uint32_t *next_ids, int sx, int sy, u64 *pairs) {
+  const long long plane = (long long)sx * sy;
+  const unsigned grid = blocks_for(plane);
+  cudaStream_t s = ctx.stream();
+#define BK_SEAM(T)                                                                                              \
+  seam_pairs<T><<<grid, 256, 0, s>>>(static_cast<const T *>(prev_labels), prev_ids,                             \
+                                      static_cast<const T *>(next_labels), next_ids, sx, sy, pairs)
+  switch (dtype) {
+    case U8: BK_SEAM(uint8_t); break;
+    case U16: BK_SEAM(uint16_t); break;
+    case U32: BK_SEAM(uint32_t); break;
+    case U64: BK_SEAM(uint64_t); break;
+    case I8: BK_SEAM(int8_t); break;
+    case I16: BK_SEAM(int16_t); break;
+    case I32: BK_SEAM(int32_t); break;
+    case I64: BK_SEAM(int64_t); break;
+    default: throw std::invalid_argument("integer labels required");
+  }
+#undef BK_SEAM
+  ++ctx.launches;
+  BK_CUDA(cudaGetLastError());
+}
+
+struct UnionFind {
+  std::vector<int64_t> parent;
+  explicit UnionFind(size_t n) : parent(n) { std::iota(parent.begin(), parent.end(), 0); }
+  int64_t find(int64_t x) {
+    while (parent[x] != x) x = parent[x] = parent[parent[x]];
+    return x;
+  }
+  void unite(int64_t a, int64_t b) {
+    a = find(a);
+    b = find(b);
+    if (a != b) parent[std::max(a, b)] = std::min(a, b);
+  }
+};
+
+double ms_since(std::chrono::steady_clock::time_point t) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
+}  // namespace
+
+size_t stream_budget(size_t requested) {
+  if (requested) return requested;  // a slab is at least one plane and a batch one crop, whatever it says
+  if (const char *env = std::getenv("BROOK_STREAM_BUDGET_MB")) {
+    char *end = nullptr;
+    const unsigned long long mb = std::strtoull(env, &end, 10);
+    if (!*env || *end || mb == 0 || mb > (~size_t(0) >> 20))
+      throw std::invalid_argument("BROOK_STREAM_BUDGET_MB must be a positive integer number of MiB");
+    return size_t(mb) << 20;
+  }
+  size_t free = 0, total = 0;
+  BK_CUDA(cudaMemGetInfo(&free, &total));
+  return std::max(free / 4, size_t(64) << 20);
+}
+
+StreamedComponents connected_components_streamed(Context &ctx, const HostVolume &hv, size_t budget,
+                                                 const std::vector<int64_t> *object_ids) {
+  StreamedComponents out;
+  out.d = hv.d;
+  out.mapping.assign(1, 0);
+  out.boxes.assign(1, Box{});
+  const long long n = hv.d.n();
+  if (n <= 0) return out;
+  if (!hv.data) throw std::invalid_argument("null host volume");
+  const size_t b = label_bytes(hv.dtype);
+  const long long plane = (long long)hv.d.sx * hv.d.sy;
+  if (plane >= (1LL << 31) / 9) throw std::invalid_argument("an xy plane of the streamed volume is too large");
+  // a slab: labels, ids, the CCL's scratch and the seam keys per voxel, within the budget
+  const long long depth = std::max(1LL, std::min<long long>(hv.d.sz, (long long)(budget / (size_t(plane) * (b + 40)))));
+  if (plane * depth >= (1LL << 31) - 1) throw std::invalid_argument("a slab of the streamed volume is too large");
+  cudaStream_t s = ctx.stream();
+  Pinned staging(size_t(plane * depth) * std::max<size_t>(b, 4));
+  Buffer<unsigned char> labels(ctx, size_t(plane * depth) * b), prev_labels(ctx, size_t(plane) * b);
+  Buffer<uint32_t> ids(ctx, size_t(plane * depth)), prev_ids(ctx, size_t(plane));
+  Buffer<u64> keys(ctx, 9 * size_t(plane)), sorted(ctx, 9 * size_t(plane));
+  Buffer<int> unique_count(ctx, 1);
+  Buffer<unsigned char> scratch;
+  out.ids.resize(size_t(n));
+  struct Slab {
+    int z0, depth;
+    int64_t base, count;
+    ComponentsResult cc;
+    std::vector<Box> boxes;
+  };
+  std::vector<Slab> slabs;
+  std::vector<std::pair<int64_t, int64_t>> seams;  // node pairs to unite
+  int64_t nodes = 0;
+  for (int z0 = 0; z0 < hv.d.sz; z0 += int(depth)) {
+    Slab sl;
+    sl.z0 = z0;
+    sl.depth = int(std::min<long long>(depth, hv.d.sz - z0));
+    const VolumeDims sd{hv.d.sx, hv.d.sy, sl.depth};
+    const long long m = sd.n();
+    gather_slab(hv, z0, z0 + sl.depth, static_cast<unsigned char *>(staging.data));
+    BK_CUDA(cudaMemcpyAsync(labels.data(), staging.data, size_t(m) * b, cudaMemcpyHostToDevice, s));
+    const void *lab = labels.data();
+    Buffer<unsigned char> selected;
+    if (object_ids) {
+      selected = select_labels(ctx, DeviceVolume{labels.data(), hv.dtype, sd}, *object_ids);
+      lab = selected.data();
+    }
+    sl.cc = connected_components(ctx, lab, hv.dtype, sd, ids.data());
+    sl.count = sl.cc.count;
+    sl.base = nodes;
+    nodes += sl.count;
+    sl.boxes = sl.count ? analyze(ctx, ids.data(), sd, sl.count) : std::vector<Box>(1);
+    if (!slabs.empty()) {
+      launch_seam(ctx, hv.dtype, prev_labels.data(), prev_ids.data(), lab, ids.data(), hv.d.sx, hv.d.sy, keys.data());
+      const int nk = int(9 * plane);
+      auto with_scratch = [&](auto op) {
+        size_t bytes = 0;
+        BK_CUDA(op(nullptr, bytes));
+        bytes = std::max<size_t>(bytes, 16);
+        if (bytes > scratch.size()) scratch = Buffer<unsigned char>(ctx, bytes);
+        BK_CUDA(op(scratch.data(), bytes));
+      };
+      with_scratch([&](void *t, size_t &bb) { return cub::DeviceRadixSort::SortKeys(t, bb, keys.data(), sorted.data(), nk, 0, 64, s); });
+      with_scratch([&](void *t, size_t &bb) {
+        return cub::DeviceSelect::Unique(t, bb, sorted.data(), keys.data(), unique_count.data(), nk, s);
+      });
+      const int u = unique_count.download(1)[0];
+      const auto pairs = keys.download(size_t(u));
+      const Slab &prev = slabs.back();
+      for (u64 key : pairs) {
+        if (key == ~0ull) continue;
+        seams.push_back({prev.base + int64_t(key >> 32) - 1, sl.base + int64_t(uint32_t(key)) - 1});
+      }
+    }
+    // the last plane for the next seam
+    BK_CUDA(cudaMemcpyAsync(prev_labels.data(), static_cast<const unsigned char *>(lab) + size_t(m - plane) * b,
+                            size_t(plane) * b, cudaMemcpyDeviceToDevice, s));
+    BK_CUDA(cudaMemcpyAsync(prev_ids.data(), ids.data() + (m - plane), size_t(plane) * sizeof(uint32_t),
+                            cudaMemcpyDeviceToDevice, s));
+    BK_CUDA(cudaMemcpyAsync(staging.data, ids.data(), size_t(m) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    ctx.synchronize();
+    std::memcpy(out.ids.data() + size_t(z0) * size_t(plane), staging.data, size_t(m) * sizeof(uint32_t));
+    slabs.push_back(std::move(sl));
+  }
+  out.slabs = int(slabs.size());
+  // components across the seams: the smallest (slab, id) of each set names it
+  UnionFind uf(static_cast<size_t>(nodes));
+  for (const auto &p : seams) uf.unite(p.first, p.second);
+  std::vector<uint32_t> gid(static_cast<size_t>(nodes), 0);
+  std::vector<int> slab_of(static_cast<size_t>(nodes));
+  for (size_t k = 0; k < slabs.size(); ++k)
+    for (int64_t j = 0; j < slabs[k].count; ++j) slab_of[size_t(slabs[k].base + j)] = int(k);
+  int64_t count = 0;
+  for (int64_t v = 0; v < nodes; ++v) {
+    const int64_t r = uf.find(v);
+    if (r == v) {
+      if (count >= int64_t(UINT32_MAX) - 1) throw std::invalid_argument("too many components");
+      gid[size_t(v)] = uint32_t(++count);
+      const Slab &sl = slabs[size_t(slab_of[size_t(v)])];
+      const int64_t local = v - sl.base + 1;
+      out.mapping.push_back(sl.cc.mapping[size_t(local)]);
+      out.roots.push_back(int64_t(sl.z0) * plane + sl.cc.roots[size_t(local - 1)]);
+      Box box{};
+      for (int a = 0; a < 3; ++a) { box.lo[a] = INT32_MAX; box.hi[a] = -1; }
+      box.count = 0;
+      out.boxes.push_back(box);
+    } else {
+      gid[size_t(v)] = gid[size_t(r)];
+    }
+  }
+  out.count = count;
+  for (int64_t v = 0; v < nodes; ++v) {
+    const Slab &sl = slabs[size_t(slab_of[size_t(v)])];
+    const Box &in = sl.boxes[size_t(v - sl.base + 1)];
+    Box &o = out.boxes[gid[size_t(v)]];
+    o.count += in.count;
+    for (int a = 0; a < 3; ++a) {
+      const int shift = a == 2 ? sl.z0 : 0;
+      o.lo[a] = std::min(o.lo[a], in.lo[a] + shift);
+      o.hi[a] = std::max(o.hi[a], in.hi[a] + shift);
+    }
+  }
+  // the host ids renumbered, plane by plane on the host's threads
+  std::vector<int> slab_of_z(static_cast<size_t>(hv.d.sz));
+  for (size_t k = 0; k < slabs.size(); ++k)
+    for (int z = slabs[k].z0; z < slabs[k].z0 + slabs[k].depth; ++z) slab_of_z[size_t(z)] = int(k);
+  parallel_for(hv.d.sz, [&](long long z) {
+    const int64_t base = slabs[size_t(slab_of_z[size_t(z)])].base;
+    uint32_t *p = out.ids.data() + size_t(z) * size_t(plane);
+    for (long long i = 0; i < plane; ++i)
+      if (p[i]) p[i] = gid[size_t(base + p[i] - 1)];
+  });
+  return out;
+}
+
+Packed skeletonize_streamed(Context &ctx, const HostVolume &hv, const Options &opt, size_t budget) {
+  if (opt.fill_holes || opt.fix_avocados)
+    throw std::invalid_argument("streamed skeletonization does not support fill_holes or fix_avocados");
+  for (float a : opt.anisotropy)
+    if (!std::isfinite(a) || a <= 0) throw std::invalid_argument("anisotropy must be finite and positive");
+  {
+    const double e = opt.teasar.pdrf_exponent;
+    if (std::isfinite(e) && e == std::floor(e) && std::fmod(e, 2.0) == 1.0)
+      throw std::invalid_argument("odd pdrf_exponent makes the background penalty negative");
+  }
+  if (opt.targets_before.size() > 1 || opt.targets_after.size() > 1)
+    throw std::invalid_argument("extra targets are given for more volumes than the call holds");
+  std::map<std::string, double> stats;
+  long long launches = 0;
+  auto t0 = std::chrono::steady_clock::now();
+  Packed result;
+  result.anisotropy = opt.anisotropy;
+  const long long n = hv.d.n();
+  auto finish = [&](Packed p) {
+    stats["host_ms_streamed_total"] = ms_since(t0);
+    launches += ctx.launches;
+    stats["launches"] = double(launches);
+    ctx.stats = stats;
+    ctx.launches = launches;
+    return p;
+  };
+  if (n <= 0 || double(n) <= opt.dust) {
+    if (opt.device_output) {
+      result.device_vertices = std::make_shared<DeviceStorage>(0, ctx.device());
+      result.device_edges = std::make_shared<DeviceStorage>(0, ctx.device());
+      result.device_radii = std::make_shared<DeviceStorage>(0, ctx.device());
+    }
+    return finish(result);
+  }
+  budget = stream_budget(budget);
+  StreamedComponents cc = connected_components_streamed(ctx, hv, budget, opt.object_ids ? &*opt.object_ids : nullptr);
+  stats["host_ms_streamed_components"] = ms_since(t0);
+  stats["streamed_slabs"] = cc.slabs;
+  stats["objects"] = 0;
+  const int sx = hv.d.sx, sy = hv.d.sy, sz = hv.d.sz;
+  const bool black_border = cc.count == 1 && cc.boxes[1].count == n;
+  // border targets of the whole volume's faces (global frame)
+  std::vector<std::vector<Point>> borders(size_t(cc.count) + 1);
+  if (opt.fix_borders && cc.count) {
+    auto tb = std::chrono::steady_clock::now();
+    const std::vector<BorderVolume> bv{{0, hv.d, cc.count}};
+    int W = 1, H = 1;
+    const std::vector<Face> faces = face_list(bv, W, H);
+    std::vector<uint32_t> stack(size_t(W) * H * faces.size(), 0);
+    for (size_t f = 0; f < faces.size(); ++f) {
+      const Face &fc = faces[f];
+      for (int pa = 0; pa < fc.fx(); ++pa)
+        for (int pb = 0; pb < fc.fy(); ++pb) {
+          long long p[3];
+          p[fc.a] = pa;
+          p[fc.b] = pb;
+          p[fc.c] = fc.fixed;
+          stack[size_t(pb) + size_t(W) * (size_t(pa) + size_t(H) * f)] = cc.ids[size_t(p[0] + sx * (p[1] + sy * p[2]))];
+        }
+    }
+    Buffer<uint32_t> dstack = to_device(ctx, stack);
+    const float aniso[3] = {opt.anisotropy[0], opt.anisotropy[1], opt.anisotropy[2]};
+    borders = border_targets(ctx, nullptr, bv, aniso, dstack.data())[0];
+    stats["host_ms_streamed_borders"] = ms_since(tb);
+  }
+  // extra targets by the component they fall on (a negative coordinate counts from the end)
+  std::vector<std::vector<Point>> before(size_t(cc.count) + 1), after(size_t(cc.count) + 1);
+  for (int list = 0; list < 2; ++list) {
+    const auto &lists = list ? opt.targets_after : opt.targets_before;
+    if (lists.empty()) continue;
+    const long long shape[3] = {sx, sy, sz};
+    for (auto p : lists[0]) {
+      for (int a = 0; a < 3; ++a) {
+        if (p[a] < 0) p[a] += shape[a];
+        if (p[a] < 0 || p[a] >= shape[a]) throw std::invalid_argument("extra target is outside the input volume");
+      }
+      const uint32_t id = cc.ids[size_t(p[0] + sx * (p[1] + sy * p[2]))];
+      if (id) (list ? after : before)[id].push_back(p);
+    }
+  }
+  // the traced components and their crops, batched to the budget (labels and the in-core state)
+  std::vector<int64_t> traced;
+  for (int64_t id = 1; id <= cc.count; ++id) {
+    const Box &bx = cc.boxes[size_t(id)];
+    const long long box = (long long)(bx.hi[0] - bx.lo[0] + 1) * (bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
+    if (!bx.count || double(bx.count) <= opt.dust || box <= 1) continue;
+    traced.push_back(id);
+  }
+  stats["objects"] = double(traced.size());
+  const size_t per_voxel = 4 + 160;
+  std::vector<Packed> pieces;
+  std::vector<int64_t> piece_id;
+  size_t batches = 0;
+  for (size_t i = 0; i < traced.size();) {
+    size_t j = i;
+    long long voxels = 0;
+    while (j < traced.size()) {
+      const Box &bx = cc.boxes[size_t(traced[j])];
+      const long long v = (long long)(bx.hi[0] - bx.lo[0] + 1) * (bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
+      if (j > i && (size_t(voxels + v) * per_voxel > budget || voxels + v >= (1LL << 31) - 1)) break;
+      voxels += v;
+      ++j;
+    }
+    // crops of the batch: 1 on the component's voxels, 0 elsewhere
+    Pinned staging(size_t(voxels) * sizeof(uint32_t));
+    auto *crop_host = static_cast<uint32_t *>(staging.data);
+    std::vector<long long> at(j - i + 1, 0);
+    for (size_t k = i; k < j; ++k) {
+      const Box &bx = cc.boxes[size_t(traced[k])];
+      at[k - i + 1] = at[k - i] + (long long)(bx.hi[0] - bx.lo[0] + 1) * (bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
+    }
+    parallel_for((long long)(j - i), [&](long long q) {
+      const int64_t id = traced[i + size_t(q)];
+      const Box &bx = cc.boxes[size_t(id)];
+      const int cx = bx.hi[0] - bx.lo[0] + 1, cy = bx.hi[1] - bx.lo[1] + 1;
+      uint32_t *dst = crop_host + at[size_t(q)];
+      for (int z = bx.lo[2]; z <= bx.hi[2]; ++z)
+        for (int y = bx.lo[1]; y <= bx.hi[1]; ++y) {
+          const uint32_t *row = cc.ids.data() + size_t(bx.lo[0]) + size_t(sx) * (size_t(y) + size_t(sy) * size_t(z));
+          uint32_t *o = dst + size_t(cx) * (size_t(y - bx.lo[1]) + size_t(cy) * size_t(z - bx.lo[2]));
+          for (int x = 0; x < cx; ++x) o[x] = row[x] == uint32_t(id) ? 1u : 0u;
+        }
+    });
+    Buffer<uint32_t> crops(ctx, size_t(voxels));
+    crops.upload(crop_host, size_t(voxels));
+    std::vector<DeviceVolume> volumes;
+    std::vector<std::vector<std::vector<Point>>> given(j - i);
+    Options o = opt;
+    o.object_ids.reset();
+    o.device_output = false;
+    o.targets_before.assign(j - i, {});
+    o.targets_after.assign(j - i, {});
+    for (size_t k = i; k < j; ++k) {
+      const int64_t id = traced[k];
+      const Box &bx = cc.boxes[size_t(id)];
+      DeviceVolume v;
+      v.data = crops.data() + at[k - i];
+      v.dtype = U32;
+      v.d = VolumeDims{bx.hi[0] - bx.lo[0] + 1, bx.hi[1] - bx.lo[1] + 1, bx.hi[2] - bx.lo[2] + 1};
+      const int shape[3] = {sx, sy, sz};
+      int faces = 0;
+      for (int a = 0; a < 3; ++a) {
+        if (bx.lo[a] > 0 || black_border) faces |= 1 << (2 * a);
+        if (bx.hi[a] < shape[a] - 1 || black_border) faces |= 2 << (2 * a);
+      }
+      v.faces = faces;
+      v.origin = {bx.lo[0], bx.lo[1], bx.lo[2]};
+      auto frame = [&](std::vector<Point> pts) {
+        for (auto &p : pts)
+          for (int a = 0; a < 3; ++a) p[a] -= bx.lo[a];
+        return pts;
+      };
+      given[k - i] = {{}, frame(borders[size_t(id)])};
+      v.borders = &given[k - i];
+      o.targets_before[k - i] = frame(before[size_t(id)]);
+      o.targets_after[k - i] = frame(after[size_t(id)]);
+      volumes.push_back(v);
+    }
+    launches += ctx.launches;
+    auto parts = skeletonize(ctx, volumes, o);
+    for (const auto &kv : ctx.stats) stats[kv.first] += kv.second;
+    launches += ctx.launches;
+    ctx.launches = 0;
+    for (size_t k = i; k < j; ++k) {
+      Packed &p = parts[k - i];
+      if (p.labels.empty()) continue;
+      p.labels[0] = cc.mapping[size_t(traced[k])];
+      pieces.push_back(std::move(p));
+      piece_id.push_back(traced[k]);
+    }
+    ++batches;
+    i = j;
+  }
+  stats["streamed_batches"] = double(batches);
+  stats["streamed_crops"] = double(traced.size());
+  // the pieces merged per label (device), then the labels in the in-core order: by the first
+  // component of each label that made a skeleton
+  std::vector<const Packed *> refs;
+  for (const auto &p : pieces) refs.push_back(&p);
+  std::vector<std::array<float, 3>> zero(refs.size(), {0.0f, 0.0f, 0.0f});
+  Packed merged = merge_fragments(ctx, refs, zero);
+  std::vector<int64_t> order;
+  for (size_t k = 0; k < pieces.size(); ++k)
+    if (std::find(order.begin(), order.end(), pieces[k].labels[0]) == order.end()) order.push_back(pieces[k].labels[0]);
+  const size_t K = merged.labels.size();
+  const size_t V = size_t(merged.vertex_offsets.back()), E = size_t(merged.edge_offsets.back());
+  std::vector<float> mv(3 * V), mr(V);
+  std::vector<uint32_t> me(2 * E);
+  if (V) {
+    BK_CUDA(cudaMemcpy(mv.data(), merged.device_vertices->ptr, mv.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    BK_CUDA(cudaMemcpy(mr.data(), merged.device_radii->ptr, mr.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  }
+  if (E) BK_CUDA(cudaMemcpy(me.data(), merged.device_edges->ptr, me.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  std::map<int64_t, size_t> index;
+  for (size_t k = 0; k < K; ++k) index[merged.labels[k]] = k;
+  for (int64_t label : order) {
+    const size_t k = index.at(label);
+    result.labels.push_back(label);
+    const int64_t v0 = merged.vertex_offsets[k], v1 = merged.vertex_offsets[k + 1];
+    const int64_t e0 = merged.edge_offsets[k], e1 = merged.edge_offsets[k + 1];
+    result.vertices.insert(result.vertices.end(), mv.begin() + 3 * v0, mv.begin() + 3 * v1);
+    result.radii.insert(result.radii.end(), mr.begin() + v0, mr.begin() + v1);
+    result.edges.insert(result.edges.end(), me.begin() + 2 * e0, me.begin() + 2 * e1);
+    result.vertex_offsets.push_back(result.vertex_offsets.back() + (v1 - v0));
+    result.edge_offsets.push_back(result.edge_offsets.back() + (e1 - e0));
+  }
+  if (opt.device_output) {
+    const int dev = ctx.device();
+    result.device_vertices = std::make_shared<DeviceStorage>(result.vertices.size() * sizeof(float), dev);
+    result.device_radii = std::make_shared<DeviceStorage>(result.radii.size() * sizeof(float), dev);
+    result.device_edges = std::make_shared<DeviceStorage>(result.edges.size() * sizeof(uint32_t), dev);
+    if (!result.vertices.empty()) {
+      BK_CUDA(cudaMemcpy(result.device_vertices->ptr, result.vertices.data(), result.vertices.size() * sizeof(float),
+                         cudaMemcpyHostToDevice));
+      BK_CUDA(cudaMemcpy(result.device_radii->ptr, result.radii.data(), result.radii.size() * sizeof(float),
+                         cudaMemcpyHostToDevice));
+    }
+    if (!result.edges.empty())
+      BK_CUDA(cudaMemcpy(result.device_edges->ptr, result.edges.data(), result.edges.size() * sizeof(uint32_t),
+                         cudaMemcpyHostToDevice));
+    result.vertices.clear();
+    result.radii.clear();
+    result.edges.clear();
+  }
+  return finish(result);
+}
+
+}  // namespace bk

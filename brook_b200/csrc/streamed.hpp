@@ -1,0 +1,45 @@
+// Out-of-core skeletonization of host volumes larger than the device's memory (streamed.cu).
+#pragma once
+#include <array>
+#include <vector>
+
+#include "pipeline.hpp"
+
+namespace bk {
+
+// A label volume in host memory with byte strides per axis (x, y, z).
+struct HostVolume {
+  const void *data = nullptr;
+  int dtype = U32;
+  VolumeDims d;
+  std::array<long long, 3> strides{0, 0, 0};
+};
+
+// The components of a host volume, computed slab by slab on the device: ids 1..count by ascending
+// first flat index (the in-core numbering), per voxel in host memory.
+struct StreamedComponents {
+  VolumeDims d;
+  int64_t count = 0;
+  std::vector<uint32_t> ids;      // F order, 0 = background
+  std::vector<int64_t> mapping;   // id -> original label (count + 1 entries)
+  std::vector<int64_t> roots;     // id - 1 -> first flat index
+  std::vector<Box> boxes;         // id -> box and voxel count (entry 0 unused)
+  int slabs = 0;
+};
+
+// The device-memory budget of a streamed call: `requested` bytes, or with 0 the environment's
+// BROOK_STREAM_BUDGET_MB (a positive number of MiB), else a quarter of the device's free memory;
+// at least 64 MiB.
+size_t stream_budget(size_t requested);
+
+StreamedComponents connected_components_streamed(Context &ctx, const HostVolume &labels, size_t budget,
+                                                 const std::vector<int64_t> *object_ids);
+
+// The skeletons skeletonize gives for the whole volume (same skeletons, same order), computed with
+// a bounded device footprint: components from slabs, then every traced component in its bounding
+// box as a crop (EDT walls where the box meets other voxels, the volume's border rule where it
+// meets the volume's edge, border targets from the whole volume's faces), crops batched to the
+// budget, and the crops' skeletons merged per label. fill_holes and fix_avocados are refused.
+Packed skeletonize_streamed(Context &ctx, const HostVolume &labels, const Options &options, size_t budget);
+
+}  // namespace bk

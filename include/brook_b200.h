@@ -24,6 +24,7 @@ typedef struct brook_context brook_context;     /* brook.h:17 */
 typedef struct brook_array brook_array;         /* brook.h:18 */
 typedef struct brook_components brook_components; /* brook.h:19 */
 typedef struct brook_skeletons brook_skeletons; /* brook.h:21 */
+typedef struct brook_host_components brook_host_components; /* brook.h:20 */
 /* brook.h:22-24: include brook_b200_dlpack.h (or the standard dlpack/dlpack.h) to read the
  * exported tensors' fields. */
 typedef struct DLManagedTensor DLManagedTensor;
@@ -229,6 +230,23 @@ brook_status brook_edt_device_noalloc(const brook_volume *labels, const float an
  * arrays, PackedSkeletons.to_core): a host result handle holding a copy of a packed view, e.g. to
  * merge skeletons a program kept as arrays. */
 brook_status brook_skeletons_create(const brook_skeletons_view *view, brook_skeletons **out);
+/* brook.h:171-177: the components of a host volume of any size through slabs of the device
+ * (budget_bytes of device memory; 0: BROOK_STREAM_BUDGET_MB, a positive number of MiB, else a
+ * quarter of the free device memory and at least 64 MiB; a slab holds at least one xy plane). The handle owns the host id volume
+ * (ids 1..count by ascending first flat index, Fortran order, u8 / u16 / u32 by the count), the
+ * mapping id -> label (count + 1 entries) and the first flat index of every component. */
+brook_status brook_connected_components_streamed(brook_context *context, const brook_volume *labels,
+                                                 size_t budget_bytes, brook_host_components **out);
+void brook_host_components_destroy(brook_host_components *components);
+brook_status brook_host_components_view(const brook_host_components *components, brook_volume *labels,
+                                        const int64_t **mapping, const int64_t **roots, size_t *count);
+/* brook.h:202-206: the skeletons brook_skeletonize gives, for a host volume whose in-core state does
+ * not fit on the device (any size, each axis below 2^31): components by slabs, then every traced
+ * component in its bounding box within budget_bytes of device memory (as above). fill_holes and
+ * fix_avocados are refused (BROOK_INVALID_ARGUMENT). */
+brook_status brook_skeletonize_streamed(brook_context *context, const brook_volume *labels,
+                                        const brook_skeletonize_options *options, size_t budget_bytes,
+                                        brook_skeletons **out);
 /* No counterpart in the reference's C header (its Python binding wraps device PackedSkeletons the
  * same way, PackedSkeletons.to_core): a device result holding a copy, made on the context's stream,
  * of packed skeletons whose vertices ({3, V}), edges ({2, E}) and radii ({1, V}) are row-major

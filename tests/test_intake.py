@@ -63,3 +63,18 @@ def test_a_volume_within_the_dust_threshold_is_empty_without_a_device():
     assert brook_b200.skeletonize(v) == {}
     p = brook_b200.skeletonize(v, output="packed", anisotropy=(2, 2, 2))
     assert len(p) == 0 and p.anisotropy == (2.0, 2.0, 2.0)
+
+
+def test_streaming_selection_rule(monkeypatch):
+    """streaming as given, else BROOK_STREAMING, else the in-core footprint rule (small volumes stay
+    in-core without asking the device)."""
+    from brook_b200 import _intake
+
+    small = np.zeros((8, 8, 8), np.uint32)
+    monkeypatch.delenv("BROOK_STREAMING", raising=False)
+    assert _intake._use_streaming(True, small, 0) and not _intake._use_streaming(False, small, 0)
+    assert not _intake._use_streaming(None, small, 0)
+    for value, expected in (("1", True), ("on", True), ("0", False), ("off", False), ("no", False)):
+        monkeypatch.setenv("BROOK_STREAMING", value)
+        assert _intake._use_streaming(None, small, 0) is expected
+    assert _intake._use_streaming(False, small, 0) is False
