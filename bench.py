@@ -46,6 +46,10 @@ CONFIGS = {
                             "(seed 3): whole in-core, and as 512x512x256 chunks with 64-voxel overlap in one batch",
                        shape=(1024, 1024, 256), seeds=3000, seed=3, kind="chunks", dtype="uint32",
                        anisotropy=(16, 16, 40), chunk=(512, 512, 256), overlap=64),
+    "stream1024": dict(workload="dense segmentation 1024x1024x1024 uint32, 4800 Voronoi seeds cut by tubes r=3-10 "
+                            "(seed 4), out of core: its in-core state (about 176 GB) does not fit beside the labels",
+                       shape=(1024, 1024, 1024), seeds=4800, seed=4, kind="streamed", dtype="uint32",
+                       anisotropy=(8, 8, 40)),
     "tubes128": dict(workload="128x128x128 uint32, 20 random-walk tubes r=2-6 (seed 0)", shape=(128, 128, 128),
                      objects=20, seed=0, kind="tubes", dtype="uint32", anisotropy=(16, 16, 40)),
 }
@@ -60,7 +64,7 @@ def make_volume(cfg, rank=0):
     if cfg["kind"] == "batch":
         return synthetic.uneven_batch(seed=cfg["seed"] + rank)
 
-    if cfg["kind"] in ("dense", "chunks"):
+    if cfg["kind"] in ("dense", "chunks", "streamed"):
         return synthetic.dense_volume(cfg["shape"], seeds=cfg["seeds"], seed=cfg["seed"] + rank, dtype=np.dtype(cfg["dtype"]))
     return synthetic.tube_volume(cfg["shape"], objects=cfg["objects"], seed=cfg["seed"] + rank, dtype=np.dtype(cfg["dtype"]))
 
@@ -706,6 +710,40 @@ def run_ours(args, cfg):
         dist.destroy_process_group()
 
 
+def run_streamed(args, cfg):
+    """The out-of-core workload: host labels to host skeletons through skeletonize(streaming=True)
+    (the device budget: a quarter of the free memory), wall clock per call after one warm-up call
+    on a 128^3 crop, with the call's own breakdown (slabs, crop batches, host and device stages)."""
+    import torch
+
+    import brook_b200
+    from brook_b200 import _native
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    volume = make_volume(cfg)
+    torch.cuda.empty_cache()
+    opts = dict(teasar_params=PARAMS, anisotropy=cfg["anisotropy"], dust_threshold=DUST, device=local)
+    brook_b200.skeletonize(np.asfortranarray(volume[:128, :128, :128]), streaming=True, output="packed", **opts)
+    times, stats = [], {}
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        packed = brook_b200.skeletonize(volume, streaming=True, output="packed", **opts)
+        times.append(time.perf_counter() - t0)
+        stats = _native.stats(local)
+    ms = 1e3 * float(np.mean(times))
+    voxels = int(volume.size)
+    print(json.dumps({
+        "metric": METRIC, "value": voxels / (ms / 1e3), "unit": "voxels/s", "n_gpus": 1, "steps": len(times),
+        "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32/f32", "data": "synthetic", "skeletons_per_s": len(packed) / (ms / 1e3),
+        "config": {"workload": cfg["workload"], "voxels": voxels, "anisotropy": cfg["anisotropy"], "teasar": PARAMS,
+                   "dust_threshold": DUST, "timing": "wall clock, host labels in, host skeletons out"},
+        "skeletons": len(packed), "vertices": int(packed.v_off[-1]),
+        "streamed": {k: round(v, 3) for k, v in sorted(stats.items())},
+    }))
+
+
 def run_post(args, cfg):
     """Only the canonical post-processing of the configuration's skeletons (one skeletonize call
     makes them): the post_measurement figures as one JSON line; the profiling entry point of the
@@ -749,6 +787,8 @@ def main():
         run_serve(args, cfg)
     elif cfg["kind"] == "chunks":
         run_chunks(args, cfg)
+    elif cfg["kind"] == "streamed":
+        run_streamed(args, cfg)
     else:
         run_ours(args, cfg)
 

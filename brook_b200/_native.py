@@ -37,7 +37,8 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_context_set_tuning", "brook_skeletons_create", "brook_merge_skeletons", "brook_context_trim",
            "brook_context_set_engine_share", "brook_postprocess_canonical", "brook_postprocess_step",
            "brook_skeleton_components", "brook_skeletons_create_device", "brook_connected_components_streamed",
-           "brook_host_components_destroy", "brook_host_components_view", "brook_skeletonize_streamed"]
+           "brook_host_components_destroy", "brook_host_components_view", "brook_skeletonize_streamed",
+           "brook_edt_streamed"]
 
 
 class Volume(ctypes.Structure):
@@ -181,6 +182,8 @@ def _open():
                                                       ctypes.POINTER(sz)]),
         "brook_skeletonize_streamed": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(Options), sz,
                                                       ctypes.POINTER(vp)]),
+        "brook_edt_streamed": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
+                                              sz, vp, sz]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -972,6 +972,25 @@ brook_status brook_host_components_view(const brook_host_components *c, brook_vo
   });
 }
 
+brook_status brook_edt_streamed(brook_context *ctx, const brook_volume *labels, const float anisotropy[3],
+                                int black_border, size_t budget_bytes, float *output, size_t output_bytes) {
+  return protect([&] {
+    require(ctx && labels && anisotropy);
+    const bk::HostVolume hv = host_labels(labels);
+    const size_t n = size_t(hv.d.n());
+    require(output_bytes / sizeof(float) >= n && (output || !n), "the output does not hold the volume's float32 field");
+    const size_t in_bytes = n * bk::label_bytes(hv.dtype);
+    const auto *a = static_cast<const unsigned char *>(hv.data), *o = reinterpret_cast<const unsigned char *>(output);
+    require(!n || o + n * sizeof(float) <= a || a + in_bytes <= o, "input and output overlap");
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    ctx->value.stats.clear();
+    ctx->value.launches = 0;
+    bk::edt_streamed(ctx->value, hv, anisotropy, black_border != 0, budget_bytes, output);
+    ctx->value.stats["launches"] = double(ctx->value.launches);
+  });
+}
+
 brook_status brook_skeletonize_streamed(brook_context *ctx, const brook_volume *labels,
                                         const brook_skeletonize_options *p, size_t budget_bytes,
                                         brook_skeletons **out) {

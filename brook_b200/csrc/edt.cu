@@ -310,6 +310,53 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3],
   }
 }
 
+void edt_xy_squared(Context &ctx, const uint32_t *ids, VolumeDims vd, const float aniso[3], bool black_border, float *D) {
+  const Dims d{vd.sx, vd.sy, vd.sz};
+  if (!vd.n()) return;
+  cudaStream_t s = ctx.stream();
+  std::vector<float> acc(vd.sx + 2, 0.0f);
+  for (size_t k = 1; k < acc.size(); ++k) acc[k] = acc[k - 1] + aniso[0];
+  Buffer<float> dacc = to_device(ctx, acc);
+  const size_t smem = size_t(kWarpsX) * vd.sx * sizeof(int);
+  if (smem > kEdtXMaxSmem) throw std::invalid_argument("x extent too large for the EDT x pass");
+  allow_edt_x_smem();
+  const long long xlines = (long long)vd.sy * vd.sz;
+  edt_x<<<(unsigned)((xlines + kWarpsX - 1) / kWarpsX), kWarpsX * 32, smem, s>>>(ids, D, d, dacc.data(),
+                                                                                black_border ? 3 : 0, 0);
+  ++ctx.launches;
+  BK_CUDA(cudaGetLastError());
+  const long long lines = (long long)vd.sx * vd.sz;
+  const long long batch = std::max(1LL, std::min(lines, (4LL << 30) / (16LL * (vd.sy + 3))));
+  Buffer<int> V(ctx, batch * (vd.sy + 3));
+  Buffer<float> H(ctx, batch * (vd.sy + 3));
+  Buffer<double> Z(ctx, batch * (vd.sy + 3));
+  for (long long l0 = 0; l0 < lines; l0 += batch) {
+    const long long nb = std::min(batch, lines - l0);
+    edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, 1, aniso[1], black_border ? 3 : 0, l0, nb, V.data(),
+                                                    H.data(), Z.data(), 0);
+    ++ctx.launches;
+    BK_CUDA(cudaGetLastError());
+  }
+}
+
+void edt_z_finish(Context &ctx, const uint32_t *ids, VolumeDims vd, float wz, bool black_border, float *D) {
+  const Dims d{vd.sx, vd.sy, vd.sz};
+  if (!vd.n()) return;
+  cudaStream_t s = ctx.stream();
+  const long long lines = (long long)vd.sx * vd.sy;
+  const long long batch = std::max(1LL, std::min(lines, (4LL << 30) / (16LL * (vd.sz + 3))));
+  Buffer<int> V(ctx, batch * (vd.sz + 3));
+  Buffer<float> H(ctx, batch * (vd.sz + 3));
+  Buffer<double> Z(ctx, batch * (vd.sz + 3));
+  for (long long l0 = 0; l0 < lines; l0 += batch) {
+    const long long nb = std::min(batch, lines - l0);
+    edt_envelope<<<blocks_for(nb, 128), 128, 0, s>>>(ids, D, d, 2, wz, black_border ? 3 : 0, l0, nb, V.data(),
+                                                    H.data(), Z.data(), 1);
+    ++ctx.launches;
+    BK_CUDA(cudaGetLastError());
+  }
+}
+
 void edt_planes(Context &ctx, const uint32_t *ids, int W, int H, int groups, int per_group, const float wx[3],
                 const float wy[3], float *D) {
   if (groups < 1 || groups > 3 || per_group < 1) throw std::invalid_argument("planar EDT groups out of range");

@@ -54,6 +54,12 @@ void edt(Context &ctx, const uint32_t *ids, VolumeDims d, const float aniso[3], 
 
 // The 3D EDT of several volumes of one flat index space (ids and out share the offsets): the x
 // pass volume by volume, the y and z passes over every volume's lines in one launch each.
+// The two halves of edt() for a volume taken in pieces (a host volume streamed through the
+// device): the x and y passes of a stack of z-slices, leaving squared distances (not rooted), and
+// the z pass of a block of whole columns over such squared distances, rooting them. Each line is
+// computed as edt() computes it, so the pieces give edt()'s field.
+void edt_xy_squared(Context &ctx, const uint32_t *ids, VolumeDims d, const float aniso[3], bool black_border, float *D);
+void edt_z_finish(Context &ctx, const uint32_t *ids, VolumeDims d, float wz, bool black_border, float *D);
 struct EdtVolume {
   long long offset;
   VolumeDims d;

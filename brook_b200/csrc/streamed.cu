@@ -306,6 +306,69 @@ StreamedComponents connected_components_streamed(Context &ctx, const HostVolume 
   return out;
 }
 
+void edt_streamed(Context &ctx, const HostVolume &hv, const float aniso[3], bool black_border, size_t budget,
+                  float *out) {
+  for (int a = 0; a < 3; ++a)
+    if (!(aniso[a] > 0) || !std::isfinite(aniso[a])) throw std::invalid_argument("anisotropy must be finite and positive");
+  const long long n = hv.d.n();
+  if (n <= 0) return;
+  budget = stream_budget(budget);
+  StreamedComponents cc = connected_components_streamed(ctx, hv, budget, nullptr);
+  cudaStream_t s = ctx.stream();
+  const int sx = hv.d.sx, sy = hv.d.sy, sz = hv.d.sz;
+  const long long plane = (long long)sx * sy;
+  // device bytes per voxel of a piece: ids, field, and the envelope stacks of its lines
+  const size_t per_voxel = 4 + 4 + 16;
+  // x and y passes, slab by slab: squared distances into `out`
+  {
+    const long long depth = std::max(1LL, std::min<long long>(sz, (long long)(budget / (size_t(plane) * per_voxel))));
+    if (plane * depth >= (1LL << 31) - 1) throw std::invalid_argument("a slab of the streamed volume is too large");
+    Buffer<uint32_t> ids(ctx, size_t(plane * depth));
+    Buffer<float> field(ctx, size_t(plane * depth));
+    Pinned staging(size_t(plane * depth) * 4);
+    for (int z0 = 0; z0 < sz; z0 += int(depth)) {
+      const int dz = int(std::min<long long>(depth, sz - z0));
+      const long long m = plane * dz;
+      std::memcpy(staging.data, cc.ids.data() + size_t(z0) * size_t(plane), size_t(m) * 4);
+      BK_CUDA(cudaMemcpyAsync(ids.data(), staging.data, size_t(m) * 4, cudaMemcpyHostToDevice, s));
+      edt_xy_squared(ctx, ids.data(), VolumeDims{sx, sy, dz}, aniso, black_border, field.data());
+      BK_CUDA(cudaMemcpyAsync(staging.data, field.data(), size_t(m) * 4, cudaMemcpyDeviceToHost, s));
+      ctx.synchronize();
+      std::memcpy(out + size_t(z0) * size_t(plane), staging.data, size_t(m) * 4);
+    }
+  }
+  // z pass, by tiles of whole columns: rows [y0, y0 + ty) of every plane
+  {
+    const long long column = (long long)sx * sz;
+    const long long ty = std::max(1LL, std::min<long long>(sy, (long long)(budget / (size_t(column) * per_voxel))));
+    if (column * ty >= (1LL << 31) - 1) throw std::invalid_argument("a column tile of the streamed volume is too large");
+    const long long tile = column * ty;
+    Buffer<uint32_t> ids(ctx, size_t(tile));
+    Buffer<float> field(ctx, size_t(tile));
+    Pinned id_stage(size_t(tile) * 4), field_stage(size_t(tile) * 4);
+    auto *is = static_cast<uint32_t *>(id_stage.data);
+    auto *fs = static_cast<float *>(field_stage.data);
+    for (int y0 = 0; y0 < sy; y0 += int(ty)) {
+      const int dy = int(std::min<long long>(ty, sy - y0));
+      const size_t rows = size_t(sx) * size_t(dy);
+      parallel_for(sz, [&](long long z) {
+        const size_t from = size_t(z) * size_t(plane) + size_t(y0) * size_t(sx), to = size_t(z) * rows;
+        std::memcpy(is + to, cc.ids.data() + from, rows * 4);
+        std::memcpy(fs + to, out + from, rows * 4);
+      });
+      const size_t m = rows * size_t(sz);
+      BK_CUDA(cudaMemcpyAsync(ids.data(), is, m * 4, cudaMemcpyHostToDevice, s));
+      BK_CUDA(cudaMemcpyAsync(field.data(), fs, m * 4, cudaMemcpyHostToDevice, s));
+      edt_z_finish(ctx, ids.data(), VolumeDims{sx, dy, sz}, aniso[2], black_border, field.data());
+      BK_CUDA(cudaMemcpyAsync(fs, field.data(), m * 4, cudaMemcpyDeviceToHost, s));
+      ctx.synchronize();
+      parallel_for(sz, [&](long long z) {
+        std::memcpy(out + size_t(z) * size_t(plane) + size_t(y0) * size_t(sx), fs + size_t(z) * rows, rows * 4);
+      });
+    }
+  }
+}
+
 Packed skeletonize_streamed(Context &ctx, const HostVolume &hv, const Options &opt, size_t budget) {
   if (opt.fill_holes || opt.fix_avocados)
     throw std::invalid_argument("streamed skeletonization does not support fill_holes or fix_avocados");

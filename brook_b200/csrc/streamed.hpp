@@ -27,13 +27,19 @@ struct StreamedComponents {
   int slabs = 0;
 };
 
-// The device-memory budget of a streamed call: `requested` bytes, or with 0 the environment's
-// BROOK_STREAM_BUDGET_MB (a positive number of MiB), else a quarter of the device's free memory;
-// at least 64 MiB.
+// The device-memory budget of a streamed call: `requested` bytes as given (a slab still holds one
+// plane and a batch one crop), or with 0 the environment's BROOK_STREAM_BUDGET_MB (a positive
+// number of MiB), else a quarter of the device's free memory and at least 64 MiB.
 size_t stream_budget(size_t requested);
 
 StreamedComponents connected_components_streamed(Context &ctx, const HostVolume &labels, size_t budget,
                                                  const std::vector<int64_t> *object_ids);
+
+// The multi-label EDT of a host volume (the in-core brook_edt's field, bit for bit) into `out` (host,
+// n floats, Fortran order): components by slabs, then the x and y passes slab by slab and the z
+// pass by tiles of whole columns, each piece staged through the device within the budget.
+void edt_streamed(Context &ctx, const HostVolume &labels, const float aniso[3], bool black_border, size_t budget,
+                  float *out);
 
 // The skeletons skeletonize gives for the whole volume (same skeletons, same order), computed with
 // a bounded device footprint: components from slabs, then every traced component in its bounding

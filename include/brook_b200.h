@@ -240,6 +240,12 @@ brook_status brook_connected_components_streamed(brook_context *context, const b
 void brook_host_components_destroy(brook_host_components *components);
 brook_status brook_host_components_view(const brook_host_components *components, brook_volume *labels,
                                         const int64_t **mapping, const int64_t **roots, size_t *count);
+/* brook.h:185-191: the multi-label EDT brook_edt gives, for a host volume of any size, into the
+ * caller's host float32 array (output_bytes must cover the volume; Fortran order; input and
+ * output must not overlap): components by slabs, the x and y passes by z-slabs, the z pass by
+ * tiles of whole columns, within budget_bytes of device memory (as above). */
+brook_status brook_edt_streamed(brook_context *context, const brook_volume *labels, const float anisotropy[3],
+                                int black_border, size_t budget_bytes, float *output, size_t output_bytes);
 /* brook.h:202-206: the skeletons brook_skeletonize gives, for a host volume whose in-core state does
  * not fit on the device (any size, each axis below 2^31): components by slabs, then every traced
  * component in its bounding box within budget_bytes of device memory (as above). fill_holes and

@@ -165,3 +165,29 @@ def test_streaming_selection_and_refusals(gpu, monkeypatch):
     d = brook_b200.skeletonize(labels, streaming=True, output="packed_device", **opts)
     assert d.on_device
     assert_packed_equal(d.to_host(), a, "device output")
+
+
+@pytest.mark.parametrize("black_border", [0, 1])
+def test_edt_streamed_equals_in_core(gpu, black_border):
+    """brook_edt_streamed (x/y passes by z-slabs, the z pass by column tiles) gives brook_edt's
+    field bit for bit, C-ordered uint16 input, a budget of a few planes."""
+    from brook_b200 import _native, synthetic
+
+    lib, ctx = _native.load(), _native.context(0)
+    labels = np.ascontiguousarray(synthetic.dense_volume((72, 56, 48), seeds=20, seed=3, dtype=np.uint16))
+    aniso = (ctypes.c_float * 3)(4.0, 4.0, 40.0)
+    vol = _native.host_volume(labels)
+    out = np.zeros(labels.shape, np.float32, order="F")
+    _native.check(lib.brook_edt_streamed(ctx, ctypes.byref(vol), aniso, black_border, 1 << 18, out.ctypes.data,
+                                         out.nbytes))
+    assert _native.stats()["launches"] > 10
+    arr = ctypes.c_void_p()
+    _native.check(lib.brook_edt(ctx, ctypes.byref(vol), aniso, black_border, ctypes.byref(arr)))
+    exp = np.zeros(labels.shape, np.float32, order="F")
+    _native.check(lib.brook_array_copy_to_host(arr, exp.ctypes.data, exp.nbytes))
+    lib.brook_array_destroy(arr)
+    np.testing.assert_array_equal(out.view(np.uint32), exp.view(np.uint32))
+    small = np.zeros(4, np.float32)
+    with pytest.raises(_native.BrookError):
+        _native.check(lib.brook_edt_streamed(ctx, ctypes.byref(vol), aniso, black_border, 0, small.ctypes.data,
+                                             small.nbytes))
