@@ -18,19 +18,19 @@ namespace bk {
 namespace {
 
 // The object of arena voxel i, or -1: the listed volume whose range holds i, then its id's object.
+constexpr int kBlockShift = 12;  // voxels per entry of the volume lookup: 4096
+
 struct ArenaObject {
   const uint32_t *ids;
   const long long *begin, *end;  // per listed volume, ascending
   const int *id_base;            // per listed volume: where its id -> object table starts
   const int *object_of;
+  const int *block_volume;       // per 4096-voxel block: the last volume that begins at or before it
   int nvol;
   __device__ int operator()(long long i) const {
-    int lo = 0, hi = nvol - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(begin + mid) <= i) lo = mid;
-      else hi = mid - 1;
-    }
+    // from the block's volume, forward over the few volumes that begin within the block
+    int lo = __ldg(block_volume + (i >> kBlockShift));
+    while (lo + 1 < nvol && __ldg(begin + lo + 1) <= i) ++lo;
     if (i < __ldg(begin + lo) || i >= __ldg(end + lo)) return -1;
     const uint32_t id = ids[i];
     return id == 0 ? -1 : __ldg(object_of + __ldg(id_base + lo) + int(id));
@@ -144,9 +144,17 @@ Buffer<int> arena_object_voxels(Context &ctx, const uint32_t *ids, long long n, 
     end.push_back(v.end);
     base.push_back(v.id_base);
   }
+  std::vector<int> block_volume(size_t((n >> kBlockShift) + 1), 0);
+  for (size_t b = 0, v = 0; b < block_volume.size(); ++b) {
+    const long long at = (long long)b << kBlockShift;
+    while (v + 1 < begin.size() && begin[v + 1] <= at) ++v;
+    block_volume[b] = int(v);
+  }
   Buffer<long long> d_begin = to_device(ctx, begin), d_end = to_device(ctx, end);
   Buffer<int> d_base = to_device(ctx, base), d_object_of = to_device(ctx, object_of);
-  const ArenaObject at{ids, d_begin.data(), d_end.data(), d_base.data(), d_object_of.data(), int(volumes.size())};
+  Buffer<int> d_block_volume = to_device(ctx, block_volume);
+  const ArenaObject at{ids, d_begin.data(), d_end.data(), d_base.data(), d_object_of.data(), d_block_volume.data(),
+                       int(volumes.size())};
   Buffer<int> picked(ctx, total), count(ctx, 1);
   thrust::counting_iterator<int> index(0);
   size_t temp = 0;

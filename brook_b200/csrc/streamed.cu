@@ -4,7 +4,7 @@
 // on the device.
 //
 // Components: z-slabs sized to the budget go through the in-core CCL one after another (labels
-// gathered into page-locked staging, ids copied back to host memory); the seam between two slabs
+// copied straight from the caller's memory or gathered on the host, ids copied back to host memory); the seam between two slabs
 // gives the pairs (id in the last plane of one, id in the first plane of the next) of 26-adjacent
 // voxels with the same label, one kernel and one radix sort per seam; a union-find over the slabs'
 // ids on the host, by smallest (slab, id), numbers the components by ascending first flat index,
@@ -39,19 +39,6 @@ namespace {
 
 using u64 = unsigned long long;
 
-// Page-locked host staging.
-struct Pinned {
-  void *data = nullptr;
-  explicit Pinned(size_t bytes) {
-    if (bytes) BK_CUDA(cudaHostAlloc(&data, bytes, cudaHostAllocDefault));
-  }
-  ~Pinned() {
-    if (data) cudaFreeHost(data);
-  }
-  Pinned(const Pinned &) = delete;
-  Pinned &operator=(const Pinned &) = delete;
-};
-
 template <class F>
 void parallel_for(long long n, F &&fn) {
   const long long threads = std::max(1LL, std::min<long long>(n, std::thread::hardware_concurrency()));
@@ -67,13 +54,23 @@ void parallel_for(long long n, F &&fn) {
   for (auto &th : pool) th.join();
 }
 
+// A large copy split over the host's threads.
+void parallel_copy(void *dst, const void *src, size_t bytes) {
+  const size_t piece = size_t(16) << 20;
+  const long long pieces = (long long)((bytes + piece - 1) / piece);
+  parallel_for(pieces, [&](long long k) {
+    const size_t at = size_t(k) * piece;
+    std::memcpy(static_cast<char *>(dst) + at, static_cast<const char *>(src) + at, std::min(piece, bytes - at));
+  });
+}
+
 // z planes [z0, z1) of the host volume into an F-ordered buffer.
 void gather_slab(const HostVolume &hv, int z0, int z1, unsigned char *dst) {
   const size_t b = label_bytes(hv.dtype), sx = size_t(hv.d.sx), sy = size_t(hv.d.sy);
   const auto *src = static_cast<const unsigned char *>(hv.data);
   const auto &st = hv.strides;
   if (st[0] == (long long)b && st[1] == (long long)(b * sx) && st[2] == (long long)(b * sx * sy)) {
-    std::memcpy(dst, src + size_t(z0) * sx * sy * b, size_t(z1 - z0) * sx * sy * b);
+    parallel_copy(dst, src + size_t(z0) * sx * sy * b, size_t(z1 - z0) * sx * sy * b);
     return;
   }
   parallel_for(z1 - z0, [&](long long k) {
@@ -188,13 +185,28 @@ StreamedComponents connected_components_streamed(Context &ctx, const HostVolume 
   const long long depth = std::max(1LL, std::min<long long>(hv.d.sz, (long long)(budget / (size_t(plane) * (b + 40)))));
   if (plane * depth >= (1LL << 31) - 1) throw std::invalid_argument("a slab of the streamed volume is too large");
   cudaStream_t s = ctx.stream();
-  Pinned staging(size_t(plane * depth) * std::max<size_t>(b, 4));
+  // Fortran-ordered input is copied to the device straight from the caller's memory; any other
+  // layout is gathered into one of two host buffers (the next slab's while the device works on this
+  // one). Copies from and to pageable memory: page-locking buffers of a slab's size costs more time
+  // than the driver's own staging.
+  const auto &st = hv.strides;
+  const bool fortran = st[0] == (long long)b && st[1] == (long long)b * hv.d.sx && st[2] == (long long)b * plane;
+  std::vector<unsigned char> stage_a(fortran ? 0 : size_t(plane * depth) * b), stage_b(fortran ? 0 : size_t(plane * depth) * b);
+  unsigned char *stages[2] = {stage_a.data(), stage_b.data()};
   Buffer<unsigned char> labels(ctx, size_t(plane * depth) * b), prev_labels(ctx, size_t(plane) * b);
   Buffer<uint32_t> ids(ctx, size_t(plane * depth)), prev_ids(ctx, size_t(plane));
   Buffer<u64> keys(ctx, 9 * size_t(plane)), sorted(ctx, 9 * size_t(plane));
   Buffer<int> unique_count(ctx, 1);
   Buffer<unsigned char> scratch;
   out.ids.resize(size_t(n));
+  {  // fault the pages in on every thread (a copy into fresh pageable memory faults them one by one)
+    const size_t piece = size_t(4) << 20;
+    const long long pieces = (long long)((size_t(n) + piece - 1) / piece);
+    parallel_for(pieces, [&](long long k) {
+      const size_t at = size_t(k) * piece;
+      std::memset(out.ids.data() + at, 0, std::min(piece, size_t(n) - at) * sizeof(uint32_t));
+    });
+  }
   struct Slab {
     int z0, depth;
     int64_t base, count;
@@ -204,55 +216,70 @@ StreamedComponents connected_components_streamed(Context &ctx, const HostVolume 
   std::vector<Slab> slabs;
   std::vector<std::pair<int64_t, int64_t>> seams;  // node pairs to unite
   int64_t nodes = 0;
-  for (int z0 = 0; z0 < hv.d.sz; z0 += int(depth)) {
+  const int nslabs = int((hv.d.sz + depth - 1) / depth);
+  auto slab_z = [&](int k) { return int(std::min<long long>((long long)k * depth, hv.d.sz)); };
+  if (!fortran) gather_slab(hv, 0, slab_z(1), stages[0]);
+  for (int k = 0; k < nslabs; ++k) {
     Slab sl;
-    sl.z0 = z0;
-    sl.depth = int(std::min<long long>(depth, hv.d.sz - z0));
+    sl.z0 = slab_z(k);
+    sl.depth = slab_z(k + 1) - sl.z0;
     const VolumeDims sd{hv.d.sx, hv.d.sy, sl.depth};
     const long long m = sd.n();
-    gather_slab(hv, z0, z0 + sl.depth, static_cast<unsigned char *>(staging.data));
-    BK_CUDA(cudaMemcpyAsync(labels.data(), staging.data, size_t(m) * b, cudaMemcpyHostToDevice, s));
-    const void *lab = labels.data();
-    Buffer<unsigned char> selected;
-    if (object_ids) {
-      selected = select_labels(ctx, DeviceVolume{labels.data(), hv.dtype, sd}, *object_ids);
-      lab = selected.data();
-    }
-    sl.cc = connected_components(ctx, lab, hv.dtype, sd, ids.data());
-    sl.count = sl.cc.count;
-    sl.base = nodes;
-    nodes += sl.count;
-    sl.boxes = sl.count ? analyze(ctx, ids.data(), sd, sl.count) : std::vector<Box>(1);
-    if (!slabs.empty()) {
-      launch_seam(ctx, hv.dtype, prev_labels.data(), prev_ids.data(), lab, ids.data(), hv.d.sx, hv.d.sy, keys.data());
-      const int nk = int(9 * plane);
-      auto with_scratch = [&](auto op) {
-        size_t bytes = 0;
-        BK_CUDA(op(nullptr, bytes));
-        bytes = std::max<size_t>(bytes, 16);
-        if (bytes > scratch.size()) scratch = Buffer<unsigned char>(ctx, bytes);
-        BK_CUDA(op(scratch.data(), bytes));
-      };
-      with_scratch([&](void *t, size_t &bb) { return cub::DeviceRadixSort::SortKeys(t, bb, keys.data(), sorted.data(), nk, 0, 64, s); });
-      with_scratch([&](void *t, size_t &bb) {
-        return cub::DeviceSelect::Unique(t, bb, sorted.data(), keys.data(), unique_count.data(), nk, s);
-      });
-      const int u = unique_count.download(1)[0];
-      const auto pairs = keys.download(size_t(u));
-      const Slab &prev = slabs.back();
-      for (u64 key : pairs) {
-        if (key == ~0ull) continue;
-        seams.push_back({prev.base + int64_t(key >> 32) - 1, sl.base + int64_t(uint32_t(key)) - 1});
+    const unsigned char *from = fortran ? static_cast<const unsigned char *>(hv.data) + size_t(sl.z0) * size_t(plane) * b
+                                        : stages[k % 2];
+    BK_CUDA(cudaMemcpyAsync(labels.data(), from, size_t(m) * b, cudaMemcpyHostToDevice, s));
+    // the next slab's gather runs on a host thread meanwhile (its buffer's last copy has ended:
+    // the stream was synchronised at the end of the previous slab)
+    std::thread next;
+    if (!fortran && k + 1 < nslabs)
+      next = std::thread([&, k] { gather_slab(hv, slab_z(k + 1), slab_z(k + 2), stages[(k + 1) % 2]); });
+    try {
+      const void *lab = labels.data();
+      Buffer<unsigned char> selected;
+      if (object_ids) {
+        selected = select_labels(ctx, DeviceVolume{labels.data(), hv.dtype, sd}, *object_ids);
+        lab = selected.data();
       }
+      sl.cc = connected_components(ctx, lab, hv.dtype, sd, ids.data());
+      sl.count = sl.cc.count;
+      sl.base = nodes;
+      nodes += sl.count;
+      sl.boxes = sl.count ? analyze(ctx, ids.data(), sd, sl.count) : std::vector<Box>(1);
+      if (!slabs.empty()) {
+        launch_seam(ctx, hv.dtype, prev_labels.data(), prev_ids.data(), lab, ids.data(), hv.d.sx, hv.d.sy, keys.data());
+        const int nk = int(9 * plane);
+        auto with_scratch = [&](auto op) {
+          size_t bytes = 0;
+          BK_CUDA(op(nullptr, bytes));
+          bytes = std::max<size_t>(bytes, 16);
+          if (bytes > scratch.size()) scratch = Buffer<unsigned char>(ctx, bytes);
+          BK_CUDA(op(scratch.data(), bytes));
+        };
+        with_scratch([&](void *t, size_t &bb) { return cub::DeviceRadixSort::SortKeys(t, bb, keys.data(), sorted.data(), nk, 0, 64, s); });
+        with_scratch([&](void *t, size_t &bb) {
+          return cub::DeviceSelect::Unique(t, bb, sorted.data(), keys.data(), unique_count.data(), nk, s);
+        });
+        const int u = unique_count.download(1)[0];
+        const auto pairs = keys.download(size_t(u));
+        const Slab &prev = slabs.back();
+        for (u64 key : pairs) {
+          if (key == ~0ull) continue;
+          seams.push_back({prev.base + int64_t(key >> 32) - 1, sl.base + int64_t(uint32_t(key)) - 1});
+        }
+      }
+      // the last plane for the next seam
+      BK_CUDA(cudaMemcpyAsync(prev_labels.data(), static_cast<const unsigned char *>(lab) + size_t(m - plane) * b,
+                              size_t(plane) * b, cudaMemcpyDeviceToDevice, s));
+      BK_CUDA(cudaMemcpyAsync(prev_ids.data(), ids.data() + (m - plane), size_t(plane) * sizeof(uint32_t),
+                              cudaMemcpyDeviceToDevice, s));
+      BK_CUDA(cudaMemcpyAsync(out.ids.data() + size_t(sl.z0) * size_t(plane), ids.data(), size_t(m) * sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, s));
+      ctx.synchronize();
+    } catch (...) {
+      if (next.joinable()) next.join();
+      throw;
     }
-    // the last plane for the next seam
-    BK_CUDA(cudaMemcpyAsync(prev_labels.data(), static_cast<const unsigned char *>(lab) + size_t(m - plane) * b,
-                            size_t(plane) * b, cudaMemcpyDeviceToDevice, s));
-    BK_CUDA(cudaMemcpyAsync(prev_ids.data(), ids.data() + (m - plane), size_t(plane) * sizeof(uint32_t),
-                            cudaMemcpyDeviceToDevice, s));
-    BK_CUDA(cudaMemcpyAsync(staging.data, ids.data(), size_t(m) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    ctx.synchronize();
-    std::memcpy(out.ids.data() + size_t(z0) * size_t(plane), staging.data, size_t(m) * sizeof(uint32_t));
+    if (next.joinable()) next.join();
     slabs.push_back(std::move(sl));
   }
   out.slabs = int(slabs.size());
@@ -325,16 +352,14 @@ void edt_streamed(Context &ctx, const HostVolume &hv, const float aniso[3], bool
     if (plane * depth >= (1LL << 31) - 1) throw std::invalid_argument("a slab of the streamed volume is too large");
     Buffer<uint32_t> ids(ctx, size_t(plane * depth));
     Buffer<float> field(ctx, size_t(plane * depth));
-    Pinned staging(size_t(plane * depth) * 4);
     for (int z0 = 0; z0 < sz; z0 += int(depth)) {
       const int dz = int(std::min<long long>(depth, sz - z0));
       const long long m = plane * dz;
-      std::memcpy(staging.data, cc.ids.data() + size_t(z0) * size_t(plane), size_t(m) * 4);
-      BK_CUDA(cudaMemcpyAsync(ids.data(), staging.data, size_t(m) * 4, cudaMemcpyHostToDevice, s));
+      BK_CUDA(cudaMemcpyAsync(ids.data(), cc.ids.data() + size_t(z0) * size_t(plane), size_t(m) * 4,
+                              cudaMemcpyHostToDevice, s));
       edt_xy_squared(ctx, ids.data(), VolumeDims{sx, sy, dz}, aniso, black_border, field.data());
-      BK_CUDA(cudaMemcpyAsync(staging.data, field.data(), size_t(m) * 4, cudaMemcpyDeviceToHost, s));
+      BK_CUDA(cudaMemcpyAsync(out + size_t(z0) * size_t(plane), field.data(), size_t(m) * 4, cudaMemcpyDeviceToHost, s));
       ctx.synchronize();
-      std::memcpy(out + size_t(z0) * size_t(plane), staging.data, size_t(m) * 4);
     }
   }
   // z pass, by tiles of whole columns: rows [y0, y0 + ty) of every plane
@@ -345,9 +370,10 @@ void edt_streamed(Context &ctx, const HostVolume &hv, const float aniso[3], bool
     const long long tile = column * ty;
     Buffer<uint32_t> ids(ctx, size_t(tile));
     Buffer<float> field(ctx, size_t(tile));
-    Pinned id_stage(size_t(tile) * 4), field_stage(size_t(tile) * 4);
-    auto *is = static_cast<uint32_t *>(id_stage.data);
-    auto *fs = static_cast<float *>(field_stage.data);
+    std::vector<uint32_t> id_stage(static_cast<size_t>(tile));
+    std::vector<float> field_stage(static_cast<size_t>(tile));
+    uint32_t *is = id_stage.data();
+    float *fs = field_stage.data();
     for (int y0 = 0; y0 < sy; y0 += int(ty)) {
       const int dy = int(std::min<long long>(ty, sy - y0));
       const size_t rows = size_t(sx) * size_t(dy);
@@ -449,51 +475,103 @@ Packed skeletonize_streamed(Context &ctx, const HostVolume &hv, const Options &o
       if (id) (list ? after : before)[id].push_back(p);
     }
   }
-  // the traced components and their crops, batched to the budget (labels and the in-core state)
+  // The traced components, grouped into crops: components whose boxes' centres fall in one cell of
+  // a grid of kCell voxels share a crop (the union of their boxes) while it stays within its share
+  // of the budget. Every other voxel of a crop is 0 and each member takes a crop id by its first
+  // voxel in the crop's flat order, which is the crop's own component numbering; its distances,
+  // objects and paths are the same as alone (other components were walls or other objects anyway).
   std::vector<int64_t> traced;
+  auto box_voxels = [](const Box &b) {
+    return (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
+  };
   for (int64_t id = 1; id <= cc.count; ++id) {
     const Box &bx = cc.boxes[size_t(id)];
-    const long long box = (long long)(bx.hi[0] - bx.lo[0] + 1) * (bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
-    if (!bx.count || double(bx.count) <= opt.dust || box <= 1) continue;
+    if (!bx.count || double(bx.count) <= opt.dust || box_voxels(bx) <= 1) continue;
     traced.push_back(id);
   }
   stats["objects"] = double(traced.size());
-  const size_t per_voxel = 4 + 160;
+  const size_t per_voxel = 4 + 160;  // a crop voxel's label and in-core state
+  const long long cap = std::max<long long>(1, std::min<long long>((long long)(budget / per_voxel), (1LL << 31) - 2));
+  constexpr int kCell = 128;
+  const long long crop_cap = std::min<long long>(cap, 64LL << 20);
+  struct Crop {
+    Box box;
+    std::vector<int64_t> members;  // then ordered by crop id
+  };
+  std::vector<Crop> crops;
+  {
+    const long long ncx = (sx + kCell - 1) / kCell, ncy = (sy + kCell - 1) / kCell;
+    std::vector<std::pair<long long, int64_t>> keyed;
+    for (int64_t id : traced) {
+      const Box &b = cc.boxes[size_t(id)];
+      const long long c = ((b.lo[0] + b.hi[0]) / 2) / kCell + ncx * (((b.lo[1] + b.hi[1]) / 2) / kCell +
+                                                                      ncy * (((b.lo[2] + b.hi[2]) / 2) / kCell));
+      keyed.push_back({c, id});
+    }
+    std::sort(keyed.begin(), keyed.end());
+    long long cell = -1;
+    for (const auto &[c, id] : keyed) {
+      const Box &b = cc.boxes[size_t(id)];
+      if (!crops.empty() && c == cell) {
+        Box u = crops.back().box;
+        for (int a = 0; a < 3; ++a) { u.lo[a] = std::min(u.lo[a], b.lo[a]); u.hi[a] = std::max(u.hi[a], b.hi[a]); }
+        if (box_voxels(u) <= crop_cap) {
+          crops.back().box = u;
+          crops.back().members.push_back(id);
+          continue;
+        }
+      }
+      crops.push_back({b, {id}});
+      cell = c;
+    }
+  }
+  std::vector<int> crop_of(size_t(cc.count) + 1, -1);
+  std::vector<uint32_t> local_of(size_t(cc.count) + 1, 0);
+  for (size_t c = 0; c < crops.size(); ++c)
+    for (int64_t id : crops[c].members) crop_of[size_t(id)] = int(c);
   std::vector<Packed> pieces;
-  std::vector<int64_t> piece_id;
+  std::vector<std::pair<int64_t, int64_t>> made;  // (component, label) of every skeleton made
+  std::vector<uint32_t> crop_stage;  // the batch's crops on the host (reused)
   size_t batches = 0;
-  for (size_t i = 0; i < traced.size();) {
+  for (size_t i = 0; i < crops.size();) {
     size_t j = i;
     long long voxels = 0;
-    while (j < traced.size()) {
-      const Box &bx = cc.boxes[size_t(traced[j])];
-      const long long v = (long long)(bx.hi[0] - bx.lo[0] + 1) * (bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
-      if (j > i && (size_t(voxels + v) * per_voxel > budget || voxels + v >= (1LL << 31) - 1)) break;
+    while (j < crops.size()) {
+      const long long v = box_voxels(crops[j].box);
+      if (j > i && (voxels + v > cap || voxels + v >= (1LL << 31) - 1)) break;
       voxels += v;
       ++j;
     }
-    // crops of the batch: 1 on the component's voxels, 0 elsewhere
-    Pinned staging(size_t(voxels) * sizeof(uint32_t));
-    auto *crop_host = static_cast<uint32_t *>(staging.data);
+    crop_stage.resize(size_t(voxels));
+    uint32_t *crop_host = crop_stage.data();
     std::vector<long long> at(j - i + 1, 0);
-    for (size_t k = i; k < j; ++k) {
-      const Box &bx = cc.boxes[size_t(traced[k])];
-      at[k - i + 1] = at[k - i] + (long long)(bx.hi[0] - bx.lo[0] + 1) * (bx.hi[1] - bx.lo[1] + 1) * (bx.hi[2] - bx.lo[2] + 1);
-    }
+    for (size_t k = i; k < j; ++k) at[k - i + 1] = at[k - i] + box_voxels(crops[k].box);
     parallel_for((long long)(j - i), [&](long long q) {
-      const int64_t id = traced[i + size_t(q)];
-      const Box &bx = cc.boxes[size_t(id)];
+      Crop &cr = crops[i + size_t(q)];
+      const Box &bx = cr.box;
       const int cx = bx.hi[0] - bx.lo[0] + 1, cy = bx.hi[1] - bx.lo[1] + 1;
       uint32_t *dst = crop_host + at[size_t(q)];
+      const int me = int(i + size_t(q));
+      uint32_t next = 0;
+      std::vector<int64_t> ordered;
       for (int z = bx.lo[2]; z <= bx.hi[2]; ++z)
         for (int y = bx.lo[1]; y <= bx.hi[1]; ++y) {
           const uint32_t *row = cc.ids.data() + size_t(bx.lo[0]) + size_t(sx) * (size_t(y) + size_t(sy) * size_t(z));
           uint32_t *o = dst + size_t(cx) * (size_t(y - bx.lo[1]) + size_t(cy) * size_t(z - bx.lo[2]));
-          for (int x = 0; x < cx; ++x) o[x] = row[x] == uint32_t(id) ? 1u : 0u;
+          for (int x = 0; x < cx; ++x) {
+            const uint32_t g = row[x];
+            uint32_t v = 0;
+            if (g && crop_of[g] == me) {
+              if (!local_of[g]) { local_of[g] = ++next; ordered.push_back(g); }
+              v = local_of[g];
+            }
+            o[x] = v;
+          }
         }
+      cr.members = std::move(ordered);
     });
-    Buffer<uint32_t> crops(ctx, size_t(voxels));
-    crops.upload(crop_host, size_t(voxels));
+    Buffer<uint32_t> dev_crops(ctx, size_t(voxels));
+    dev_crops.upload(crop_host, size_t(voxels));
     std::vector<DeviceVolume> volumes;
     std::vector<std::vector<std::vector<Point>>> given(j - i);
     Options o = opt;
@@ -502,10 +580,10 @@ Packed skeletonize_streamed(Context &ctx, const HostVolume &hv, const Options &o
     o.targets_before.assign(j - i, {});
     o.targets_after.assign(j - i, {});
     for (size_t k = i; k < j; ++k) {
-      const int64_t id = traced[k];
-      const Box &bx = cc.boxes[size_t(id)];
+      const Crop &cr = crops[k];
+      const Box &bx = cr.box;
       DeviceVolume v;
-      v.data = crops.data() + at[k - i];
+      v.data = dev_crops.data() + at[k - i];
       v.dtype = U32;
       v.d = VolumeDims{bx.hi[0] - bx.lo[0] + 1, bx.hi[1] - bx.lo[1] + 1, bx.hi[2] - bx.lo[2] + 1};
       const int shape[3] = {sx, sy, sz};
@@ -516,43 +594,57 @@ Packed skeletonize_streamed(Context &ctx, const HostVolume &hv, const Options &o
       }
       v.faces = faces;
       v.origin = {bx.lo[0], bx.lo[1], bx.lo[2]};
-      auto frame = [&](std::vector<Point> pts) {
-        for (auto &p : pts)
+      auto frame = [&](const std::vector<Point> &pts, std::vector<Point> &into) {
+        for (auto p : pts) {
           for (int a = 0; a < 3; ++a) p[a] -= bx.lo[a];
-        return pts;
+          into.push_back(p);
+        }
       };
-      given[k - i] = {{}, frame(borders[size_t(id)])};
-      v.borders = &given[k - i];
-      o.targets_before[k - i] = frame(before[size_t(id)]);
-      o.targets_after[k - i] = frame(after[size_t(id)]);
+      auto &g = given[k - i];
+      g.assign(cr.members.size() + 1, {});
+      for (size_t m = 0; m < cr.members.size(); ++m) {
+        const int64_t id = cr.members[m];
+        frame(borders[size_t(id)], g[m + 1]);
+        frame(before[size_t(id)], o.targets_before[k - i]);
+        frame(after[size_t(id)], o.targets_after[k - i]);
+      }
+      v.borders = &g;
       volumes.push_back(v);
     }
     launches += ctx.launches;
     auto parts = skeletonize(ctx, volumes, o);
-    for (const auto &kv : ctx.stats) stats[kv.first] += kv.second;
+    for (const auto &kv : ctx.stats)
+      if (kv.first != "objects") stats[kv.first] += kv.second;
     launches += ctx.launches;
     ctx.launches = 0;
     for (size_t k = i; k < j; ++k) {
       Packed &p = parts[k - i];
       if (p.labels.empty()) continue;
-      p.labels[0] = cc.mapping[size_t(traced[k])];
+      for (auto &label : p.labels) {  // crop id -> component -> its label
+        const int64_t id = crops[k].members[size_t(label) - 1];
+        label = cc.mapping[size_t(id)];
+        made.push_back({id, label});
+      }
       pieces.push_back(std::move(p));
-      piece_id.push_back(traced[k]);
     }
     ++batches;
     i = j;
   }
   stats["streamed_batches"] = double(batches);
-  stats["streamed_crops"] = double(traced.size());
+  stats["streamed_crops"] = double(crops.size());
   // the pieces merged per label (device), then the labels in the in-core order: by the first
   // component of each label that made a skeleton
   std::vector<const Packed *> refs;
   for (const auto &p : pieces) refs.push_back(&p);
   std::vector<std::array<float, 3>> zero(refs.size(), {0.0f, 0.0f, 0.0f});
   Packed merged = merge_fragments(ctx, refs, zero);
+  std::sort(made.begin(), made.end());
   std::vector<int64_t> order;
-  for (size_t k = 0; k < pieces.size(); ++k)
-    if (std::find(order.begin(), order.end(), pieces[k].labels[0]) == order.end()) order.push_back(pieces[k].labels[0]);
+  {
+    std::map<int64_t, bool> seen;
+    for (const auto &m : made)
+      if (!seen[m.second]) { seen[m.second] = true; order.push_back(m.second); }
+  }
   const size_t K = merged.labels.size();
   const size_t V = size_t(merged.vertex_offsets.back()), E = size_t(merged.edge_offsets.back());
   std::vector<float> mv(3 * V), mr(V);

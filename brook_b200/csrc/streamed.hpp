@@ -1,6 +1,7 @@
 // Out-of-core skeletonization of host volumes larger than the device's memory (streamed.cu).
 #pragma once
 #include <array>
+#include <memory>
 #include <vector>
 
 #include "pipeline.hpp"
@@ -15,12 +16,28 @@ struct HostVolume {
   std::array<long long, 3> strides{0, 0, 0};
 };
 
+// A host array that is not initialised when made (a volume's worth of ids is written in full).
+template <class T>
+struct HostArray {
+  std::unique_ptr<T[]> p;
+  size_t n = 0;
+  void resize(size_t count) {
+    p.reset(count ? new T[count] : nullptr);
+    n = count;
+  }
+  T *data() { return p.get(); }
+  const T *data() const { return p.get(); }
+  size_t size() const { return n; }
+  T &operator[](size_t i) { return p[i]; }
+  const T &operator[](size_t i) const { return p[i]; }
+};
+
 // The components of a host volume, computed slab by slab on the device: ids 1..count by ascending
 // first flat index (the in-core numbering), per voxel in host memory.
 struct StreamedComponents {
   VolumeDims d;
   int64_t count = 0;
-  std::vector<uint32_t> ids;      // F order, 0 = background
+  HostArray<uint32_t> ids;        // F order, 0 = background
   std::vector<int64_t> mapping;   // id -> original label (count + 1 entries)
   std::vector<int64_t> roots;     // id - 1 -> first flat index
   std::vector<Box> boxes;         // id -> box and voxel count (entry 0 unused)
