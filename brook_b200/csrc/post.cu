@@ -1105,34 +1105,84 @@ Set remove_loops(Context &ctx, const Set &s) {
 
 // ----------------------------------------------------------------------------- remove_ticks ----
 //
-// One thread per branched tree; the rules are post_kernels.cuh:314-405's (Kimimaro's
-// remove_ticks): chains between critical nodes, measured from the end nearer the first leaf, and
-// the shortest eligible chain removed while it is shorter than the threshold and not between two
-// nodes with one chain left; a branch node left with two chains fuses them.
+// One warp per branched tree; the rules are post_kernels.cuh:314-405's (Kimimaro's remove_ticks):
+// chains between critical nodes (one or three-plus neighbours), each measured as the float32 sum of
+// its edges' float32 lengths from the end nearer the first leaf (lowest local id), and the shortest
+// eligible chain removed while it is shorter than the threshold and not between two nodes with one
+// chain left; a branch node left with two chains fuses them. The result does not depend on the
+// order the tree is walked in, so the warp builds the adjacency with atomics, walks every chain
+// from both of its ends at once (a lane per walk), roots the small tree of critical nodes at the
+// first leaf on one lane to pick each chain's measured end, and runs the heap loop over the chains
+// on one lane; the rows' fate is written back by all lanes.
 
-struct TickWalker {
+// Per-component workspace layout (ints, then doubles); shared by the host (sizes) and the kernel.
+struct TickLayout {
+  long long nv, e0, slots;
+  __host__ __device__ TickLayout(long long nv_, long long e0_) : nv(nv_), e0(e0_), slots(2 * e0_) {}
+  // ints: off (nv + 1), cursor (nv), src, nbr, nrow, wend, wother (slots each), chain_of_row (e0),
+  // chain_at (slots), queue (nv), seen (nv), su, sv, sflag, ver, lhead, ltail, lnext, dead (e0 each),
+  // ihead (nv), ito, inext (3 e0 + 1 each), hlo, hhi, hid, hver (2 e0 + 1 each); wlen as floats (slots)
+  __host__ __device__ long long ints() const {
+    return (nv + 1) + nv + 5 * slots + e0 + slots + 2 * nv + 8 * e0 + nv + 2 * (3 * e0 + 1) + 4 * (2 * e0 + 1) + slots;
+  }
+  __host__ __device__ long long doubles() const { return e0 + (2 * e0 + 1); }  // len, hlen
+};
+
+struct TickState {
   enum : int { kAlive = 1, kEligible = 2 };
   int nv, e0;
   const float *P;
   const int2 *rows;
-  // CSR of the tree
-  int *off, *nbr, *nrow;
-  // walk stack
-  int *s_node, *s_parent, *s_root, *s_chain;
-  float *s_dist;
-  int *bc;
-  // chains
-  int *su, *sv, *sflag, *ver, *lhead, *ltail, *lnext, *dead, *coe;
-  double *len;
-  // incidence lists of chains at nodes
+  int *off, *cursor, *src, *nbr, *nrow, *wend, *wother, *chain_of_row, *chain_at, *queue, *seen;
+  float *wlen;
+  int *su, *sv, *sflag, *ver, *lhead, *ltail, *lnext, *dead;
   int *ihead, *ito, *inext;
-  int in_used = 0;
-  // heap of (len, lo, hi, chain, version)
-  double *hlen;
   int *hlo, *hhi, *hid, *hver;
-  int hn = 0;
+  double *len, *hlen;
+  int in_used = 0, hn = 0;
 
+  __device__ TickState(long long nv_, long long e0_, int *w, double *d) {
+    nv = int(nv_);
+    e0 = int(e0_);
+    const long long slots = 2 * e0_;
+    off = w; w += nv + 1;
+    cursor = w; w += nv;
+    src = w; w += slots;
+    nbr = w; w += slots;
+    nrow = w; w += slots;
+    wend = w; w += slots;
+    wother = w; w += slots;
+    chain_of_row = w; w += e0;
+    chain_at = w; w += slots;
+    queue = w; w += nv;
+    seen = w; w += nv;
+    su = w; w += e0;
+    sv = w; w += e0;
+    sflag = w; w += e0;
+    ver = w; w += e0;
+    lhead = w; w += e0;
+    ltail = w; w += e0;
+    lnext = w; w += e0;
+    dead = w; w += e0;
+    ihead = w; w += nv;
+    ito = w; w += 3 * e0 + 1;
+    inext = w; w += 3 * e0 + 1;
+    hlo = w; w += 2 * e0 + 1;
+    hhi = w; w += 2 * e0 + 1;
+    hid = w; w += 2 * e0 + 1;
+    hver = w; w += 2 * e0 + 1;
+    wlen = reinterpret_cast<float *>(w);
+    len = d;
+    hlen = d + e0;
+  }
   __device__ int deg(int v) const { return off[v + 1] - off[v]; }
+  __device__ float edge(int u, int v) const {
+    float dx = P[3 * u] - P[3 * v], dy = P[3 * u + 1] - P[3 * v + 1], dz = P[3 * u + 2] - P[3 * v + 2];
+    dx *= dx;
+    dy *= dy;
+    dz *= dz;
+    return sqrtf((dx + dy) + dz);
+  }
   __device__ void incident(int v, int s) {
     ito[in_used] = s;
     inext[in_used] = ihead[v];
@@ -1178,165 +1228,170 @@ struct TickWalker {
       i = m;
     }
   }
-
-  __device__ void run(double threshold, int *keep_rows) {
-    // CSR
-    for (int v = 0; v <= nv; ++v) off[v] = 0;
-    for (int r = 0; r < e0; ++r) { ++off[rows[r].x + 1]; ++off[rows[r].y + 1]; }
-    for (int v = 0; v < nv; ++v) off[v + 1] += off[v];
-    for (int v = 0; v < nv; ++v) bc[v] = off[v];  // fill cursors
-    for (int r = 0; r < e0; ++r) {
-      const int a = rows[r].x, b = rows[r].y;
-      nbr[bc[a]] = b; nrow[bc[a]++] = r;
-      nbr[bc[b]] = a; nrow[bc[b]++] = r;
-    }
-    int start = -1;
-    for (int v = 0; v < nv; ++v) {
-      const int d = deg(v);
-      bc[v] = d >= 3 ? d : 0;
-      ihead[v] = -1;
-      if (start < 0 && d == 1) start = v;
-    }
-    if (start < 0) {
-      for (int r = 0; r < e0; ++r) keep_rows[r] = 1;
-      return;
-    }
-    // the chains, walking the tree from the start leaf
-    int ns = 0, sp = 1;
-    s_node[0] = start; s_parent[0] = -1; s_root[0] = start; s_chain[0] = -1; s_dist[0] = 0.0f;
-    while (sp > 0) {
-      --sp;
-      const int node = s_node[sp], parent = s_parent[sp], chain = s_chain[sp];
-      int root = s_root[sp];
-      float dist = s_dist[sp];
-      const int d = deg(node);
-      if ((d == 1 || d >= 3) && node != root) {
-        su[chain] = root;
-        sv[chain] = node;
-        len[chain] = double(dist);
-        ver[chain] = 0;
-        sflag[chain] = kAlive | ((deg(root) == 1 || d == 1) ? kEligible : 0);
-        incident(root, chain);
-        incident(node, chain);
-        if (sflag[chain] & kEligible) push(chain);
-        dist = 0.0f;
-        root = node;
-      }
-      for (int q = off[node]; q < off[node + 1]; ++q) {
-        const int child = nbr[q];
-        if (child == parent) continue;
-        float dx = P[3 * node] - P[3 * child], dy = P[3 * node + 1] - P[3 * child + 1], dz = P[3 * node + 2] - P[3 * child + 2];
-        dx *= dx;
-        dy *= dy;
-        dz *= dz;
-        int ch = chain;
-        if (node == root) {
-          ch = ns++;
-          lhead[ch] = ltail[ch] = ch;
-          lnext[ch] = -1;
-          dead[ch] = 0;
-          sflag[ch] = 0;
-        }
-        coe[nrow[q]] = ch;
-        s_node[sp] = child; s_parent[sp] = node; s_root[sp] = root; s_chain[sp] = ch;
-        s_dist[sp] = dist + sqrtf((dx + dy) + dz);
-        ++sp;
-      }
-    }
-    int nalive = 0;
-    for (int s = 0; s < ns; ++s) nalive += sflag[s] & kAlive;
-    while (nalive > 1) {
-      while (hn > 0 && (!(sflag[hid[0]] & kAlive) || ver[hid[0]] != hver[0])) pop();
-      if (hn == 0) break;
-      const int best = hid[0];
-      const int e1 = su[best], e2 = sv[best];
-      if (bc[e1] == 1 && bc[e2] == 1) break;
-      if (len[best] >= threshold) break;
-      pop();
-      for (int o = lhead[best]; o >= 0; o = lnext[o]) dead[o] = 1;
-      sflag[best] = 0;
-      --nalive;
-      --bc[e1];
-      --bc[e2];
-      for (int t = 0; t < 2; ++t) {
-        const int v = t ? e2 : e1;
-        if (bc[v] != 2) continue;
-        int a = -1, b = -1;
-        for (int k = ihead[v]; k >= 0; k = inext[k]) {
-          const int o = ito[k];
-          if (!(sflag[o] & kAlive) || (su[o] != v && sv[o] != v) || o == a) continue;
-          if (a < 0) a = o; else { b = o; break; }
-        }
-        if (a < 0 || b < 0) { bc[v] = 0; continue; }
-        const int ea = su[a] == v ? sv[a] : su[a], eb = su[b] == v ? sv[b] : su[b];
-        len[a] = (0.0 + len[a]) + len[b];
-        su[a] = ea;
-        sv[a] = eb;
-        sflag[a] = kAlive | kEligible;
-        lnext[ltail[a]] = lhead[b];
-        ltail[a] = ltail[b];
-        sflag[b] = 0;
-        --nalive;
-        incident(eb, a);
-        ++ver[a];
-        push(a);
-        bc[v] = 0;
-      }
-    }
-    for (int r = 0; r < e0; ++r) keep_rows[r] = !dead[coe[r]];
-  }
 };
 
-// Per-component workspace: ints 7 * nv + 1 + 4 * e0 (CSR) + 10 * e0 (chains) + 6 * e0 + 2 (incidence)
-// + 4 * (2 * e0 + 1) (heap); floats nv; doubles e0 + 2 * e0 + 1.
-__host__ __device__ inline long long tick_ints(long long nv, long long e0) {
-  return 7 * nv + 1 + 4 * e0 + 10 * e0 + 6 * e0 + 2 + 4 * (2 * e0 + 1);
-}
-__host__ __device__ inline long long tick_doubles(long long e0) { return 3 * e0 + 1; }
+__host__ __device__ inline long long tick_ints(long long nv, long long e0) { return TickLayout(nv, e0).ints(); }
+__host__ __device__ inline long long tick_doubles(long long e0) { return TickLayout(0, e0).doubles(); }
+
+constexpr int kTickWarps = 4;  // components per block (a warp each)
 
 __global__ void ticks_kernel(int count, const long long *vs, const long long *es, const long long *ibase,
                              const long long *dbase, double threshold, const float *xyz, const int2 *rows, int *iwork,
-                             float *fwork, double *dwork, int *keep_rows) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+                             double *dwork, int *keep_rows) {
+  const int c = blockIdx.x * kTickWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (c >= count) return;
   const long long v0 = vs[c], r0 = es[c];
-  TickWalker t;
-  t.nv = int(vs[c + 1] - v0);
-  t.e0 = int(es[c + 1] - r0);
+  TickState t(vs[c + 1] - v0, es[c + 1] - r0, iwork + ibase[c], dwork + dbase[c]);
   t.P = xyz + 3 * v0;
   t.rows = rows + r0;
-  const int nv = t.nv, e0 = t.e0;
-  int *w = iwork + ibase[c];
-  t.off = w; w += nv + 1;
-  t.s_node = w; w += nv;
-  t.s_parent = w; w += nv;
-  t.s_root = w; w += nv;
-  t.s_chain = w; w += nv;
-  t.bc = w; w += nv;
-  t.ihead = w; w += nv;
-  t.nbr = w; w += 2 * e0;
-  t.nrow = w; w += 2 * e0;
-  t.su = w; w += e0;
-  t.sv = w; w += e0;
-  t.sflag = w; w += e0;
-  t.ver = w; w += e0;
-  t.lhead = w; w += e0;
-  t.ltail = w; w += e0;
-  t.lnext = w; w += e0;
-  t.dead = w; w += e0;
-  t.coe = w; w += e0;
-  w += e0;  // spare
-  t.ito = w; w += 3 * e0 + 1;
-  t.inext = w; w += 3 * e0 + 1;
-  t.hlo = w; w += 2 * e0 + 1;
-  t.hhi = w; w += 2 * e0 + 1;
-  t.hid = w; w += 2 * e0 + 1;
-  t.hver = w; w += 2 * e0 + 1;
-  t.s_dist = fwork + v0;
-  double *d = dwork + dbase[c];
-  t.len = d; d += e0;
-  t.hlen = d;
-  t.run(threshold, keep_rows + r0);
+  const int nv = t.nv, e0 = t.e0, slots = 2 * e0;
+  int *keep = keep_rows + r0;
+  // adjacency: degrees, offsets (warp scan), slots filled with atomics (any order)
+  for (int v = lane; v <= nv; v += 32) t.off[v] = 0;
+  __syncwarp();
+  for (int r = lane; r < e0; r += 32) {
+    atomicAdd(t.off + t.rows[r].x + 1, 1);
+    atomicAdd(t.off + t.rows[r].y + 1, 1);
+  }
+  __syncwarp();
+  int carry = 0;
+  for (int base = 1; base <= nv; base += 32) {
+    const int v = base + lane;
+    int x = v <= nv ? t.off[v] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (v <= nv) t.off[v] = x + carry;
+    carry += __shfl_sync(0xFFFFFFFFu, x, 31);
+  }
+  __syncwarp();
+  for (int v = lane; v < nv; v += 32) t.cursor[v] = t.off[v];
+  __syncwarp();
+  for (int r = lane; r < e0; r += 32) {
+    const int a = t.rows[r].x, b = t.rows[r].y;
+    int q = atomicAdd(t.cursor + a, 1);
+    t.src[q] = a; t.nbr[q] = b; t.nrow[q] = r;
+    q = atomicAdd(t.cursor + b, 1);
+    t.src[q] = b; t.nbr[q] = a; t.nrow[q] = r;
+  }
+  __syncwarp();
+  // every chain walked from each of its ends (a lane per walk): its far end, the slot it arrives
+  // by there, and its float32 length from this end; its rows keyed by the lower of its two slots
+  for (int q = lane; q < slots; q += 32) {
+    const int c0 = t.src[q];
+    if (t.deg(c0) == 2) continue;
+    int prev = c0, cur = t.nbr[q], row = t.nrow[q];
+    float dist = 0.0f + t.edge(prev, cur);
+    while (t.deg(cur) == 2) {
+      const int s0 = t.off[cur];
+      const int k = t.nbr[s0] == prev && t.nrow[s0] == row ? s0 + 1 : s0;
+      const int next = t.nbr[k];
+      row = t.nrow[k];
+      dist = dist + t.edge(cur, next);
+      prev = cur;
+      cur = next;
+    }
+    int back = -1;  // the far end's slot of the chain's last edge
+    for (int k = t.off[cur]; k < t.off[cur + 1]; ++k)
+      if (t.nrow[k] == row) { back = k; break; }
+    t.wend[q] = cur;
+    t.wother[q] = back;
+    t.wlen[q] = dist;
+    const int key = min(q, back);
+    // the rows of the chain, walked again from this end
+    int p2 = c0, c2 = t.nbr[q], r2 = t.nrow[q];
+    t.chain_of_row[r2] = key;
+    while (t.deg(c2) == 2) {
+      const int s0 = t.off[c2];
+      const int k = t.nbr[s0] == p2 && t.nrow[s0] == r2 ? s0 + 1 : s0;
+      r2 = t.nrow[k];
+      t.chain_of_row[r2] = key;
+      p2 = c2;
+      c2 = t.nbr[k];
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    int start = -1;
+    for (int v = 0; v < nv && start < 0; ++v)
+      if (t.deg(v) == 1) start = v;
+    if (start >= 0) {
+      // the tree of critical nodes rooted at the start leaf: each chain from its end nearer it
+      for (int v = 0; v < nv; ++v) { t.seen[v] = 0; t.ihead[v] = -1; }
+      int qh = 0, qt = 0, ns = 0;
+      t.queue[qt++] = start;
+      t.seen[start] = 1;
+      while (qh < qt) {
+        const int u = t.queue[qh++];
+        for (int q = t.off[u]; q < t.off[u + 1]; ++q) {
+          const int d = t.wend[q];
+          if (t.seen[d]) continue;
+          t.seen[d] = 1;
+          t.queue[qt++] = d;
+          const int s = ns++;
+          t.chain_at[min(q, t.wother[q])] = s;
+          t.su[s] = u;
+          t.sv[s] = d;
+          t.len[s] = double(t.wlen[q]);
+          t.ver[s] = 0;
+          t.sflag[s] = TickState::kAlive | ((t.deg(u) == 1 || t.deg(d) == 1) ? TickState::kEligible : 0);
+          t.lhead[s] = t.ltail[s] = s;
+          t.lnext[s] = -1;
+          t.dead[s] = 0;
+          t.incident(u, s);
+          t.incident(d, s);
+          if (t.sflag[s] & TickState::kEligible) t.push(s);
+        }
+      }
+      int* bc = t.cursor;  // the chain count left at each node (its degree for branch nodes, else 0)
+      for (int v = 0; v < nv; ++v) bc[v] = t.deg(v) >= 3 ? t.deg(v) : 0;
+      int nalive = ns;
+      while (nalive > 1) {
+        while (t.hn > 0 && (!(t.sflag[t.hid[0]] & TickState::kAlive) || t.ver[t.hid[0]] != t.hver[0])) t.pop();
+        if (t.hn == 0) break;
+        const int best = t.hid[0];
+        const int e1 = t.su[best], e2 = t.sv[best];
+        if (bc[e1] == 1 && bc[e2] == 1) break;
+        if (t.len[best] >= threshold) break;
+        t.pop();
+        for (int o = t.lhead[best]; o >= 0; o = t.lnext[o]) t.dead[o] = 1;
+        t.sflag[best] = 0;
+        --nalive;
+        --bc[e1];
+        --bc[e2];
+        for (int side = 0; side < 2; ++side) {
+          const int v = side ? e2 : e1;
+          if (bc[v] != 2) continue;
+          int a = -1, b = -1;
+          for (int k = t.ihead[v]; k >= 0; k = t.inext[k]) {
+            const int o = t.ito[k];
+            if (!(t.sflag[o] & TickState::kAlive) || (t.su[o] != v && t.sv[o] != v) || o == a) continue;
+            if (a < 0) a = o; else { b = o; break; }
+          }
+          if (a < 0 || b < 0) { bc[v] = 0; continue; }
+          const int ea = t.su[a] == v ? t.sv[a] : t.su[a], eb = t.su[b] == v ? t.sv[b] : t.su[b];
+          t.len[a] = (0.0 + t.len[a]) + t.len[b];
+          t.su[a] = ea;
+          t.sv[a] = eb;
+          t.sflag[a] = TickState::kAlive | TickState::kEligible;
+          t.lnext[t.ltail[a]] = t.lhead[b];
+          t.ltail[a] = t.ltail[b];
+          t.sflag[b] = 0;
+          --nalive;
+          t.incident(eb, a);
+          ++t.ver[a];
+          t.push(a);
+          bc[v] = 0;
+        }
+      }
+    }
+    t.seen[0] = start;  // tells the lanes whether the tree was walked
+  }
+  __syncwarp();
+  const bool walked = t.seen[0] >= 0;
+  for (int r = lane; r < e0; r += 32) keep[r] = walked ? !t.dead[t.chain_at[t.chain_of_row[r]]] : 1;
 }
 
 __global__ void live_edges(const int *edge_ids, const int *keep_rows, int total, unsigned char *live) {
@@ -1368,11 +1423,10 @@ Set remove_ticks(Context &ctx, const Set &s, double threshold) {
   }
   Buffer<long long> d_ib = to_device(ctx, ib), d_db = to_device(ctx, db);
   Buffer<int> iwork(ctx, size_t(ib.back())), keep_rows(ctx, std::max(a.m, 1));
-  Buffer<float> fwork(ctx, a.n);
   Buffer<double> dwork(ctx, size_t(db.back()));
-  ticks_kernel<<<blocks_for(a.count, 64), 64, 0, st>>>(a.count, a.vs.data(), a.es.data(), d_ib.data(), d_db.data(),
-                                                       threshold, a.xyz.data(), a.rows.data(), iwork.data(),
-                                                       fwork.data(), dwork.data(), keep_rows.data());
+  ticks_kernel<<<(a.count + kTickWarps - 1) / kTickWarps, 32 * kTickWarps, 0, st>>>(
+      a.count, a.vs.data(), a.es.data(), d_ib.data(), d_db.data(), threshold, a.xyz.data(), a.rows.data(),
+      iwork.data(), dwork.data(), keep_rows.data());
   Buffer<unsigned char> live(ctx, g.m);
   live.fill_bytes(1);
   live_edges<<<blocks_for(a.m), 256, 0, st>>>(a.edges.data(), keep_rows.data(), a.m, live.data());
