@@ -1250,14 +1250,11 @@ void launch_prepare(const EngineArgs &a, int nbig, int ctas, cudaStream_t stream
   else launch((const void *)prepare_kernel<kClusterCtas>, kClusterCtas, a, nbig, stream);
 }
 
-void prepare_engine_launches(int ctas, cudaStream_t stream) {
-  if (ctas == kWideClusterCtas) {
-    resident_clusters((const void *)prepare_kernel<kWideClusterCtas>, ctas, stream);
-    resident_clusters((const void *)trace_kernel<kWideClusterCtas>, ctas, stream);
-  } else {
-    resident_clusters((const void *)prepare_kernel<kClusterCtas>, kClusterCtas, stream);
-    resident_clusters((const void *)trace_kernel<kClusterCtas>, kClusterCtas, stream);
-  }
+void prepare_engine_launches(int prepare_ctas, int trace_ctas, cudaStream_t stream) {
+  if (prepare_ctas == kWideClusterCtas) resident_clusters((const void *)prepare_kernel<kWideClusterCtas>, kWideClusterCtas, stream);
+  else resident_clusters((const void *)prepare_kernel<kClusterCtas>, kClusterCtas, stream);
+  if (trace_ctas == kWideClusterCtas) resident_clusters((const void *)trace_kernel<kWideClusterCtas>, kWideClusterCtas, stream);
+  else resident_clusters((const void *)trace_kernel<kClusterCtas>, kClusterCtas, stream);
 }
 
 void launch_trace(const EngineArgs &a, int nbig, int ctas, int lone_percent, cudaStream_t stream) {

@@ -137,6 +137,6 @@ constexpr int kLoneFirstPercent = 10;
 constexpr float kRailBand = 0.5f;
 // The device queries the launches above make (resident clusters per kernel), done ahead so that
 // a stream capture of the launches holds launches only.
-void prepare_engine_launches(int cluster_ctas, cudaStream_t stream);
+void prepare_engine_launches(int prepare_cluster_ctas, int trace_cluster_ctas, cudaStream_t stream);
 
 }  // namespace bk

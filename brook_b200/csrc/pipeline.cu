@@ -656,6 +656,11 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   const int ctas = tune.trace_cluster_ctas == kWideClusterCtas || tune.trace_cluster_ctas == kClusterCtas
                        ? tune.trace_cluster_ctas
                        : cluster_ctas(largest, F);
+  int prepare_ctas = ctas;
+  if (const char *e = std::getenv("BROOK_B200_PREPARE_CLUSTER_CTAS")) {  // tuning knob: 4 or 8
+    const int v = std::atoi(e);
+    if (v == kClusterCtas || v == kWideClusterCtas) prepare_ctas = v;
+  }
   int lone_percent = tune.lone_first_percent >= 0 ? tune.lone_first_percent : kLoneFirstPercent;
   if (const char *e = std::getenv("BROOK_B200_LONE_FIRST_PERCENT")) lone_percent = std::atoi(e);  // tuning knob
   lone_percent = std::max(0, std::min(100, lone_percent));
@@ -669,7 +674,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   const char *graph_knob = std::getenv("BROOK_B200_GRAPH");
   const bool as_graph = !fields && !(graph_knob && std::string(graph_knob) == "0");
   auto engine = [&] {
-    launch_prepare(a, nbig_prepare, ctas, s);
+    launch_prepare(a, nbig_prepare, prepare_ctas, s);
     ++ctx.launches;
     clock.mark("prepare");
     if (fields) {
@@ -689,7 +694,7 @@ std::vector<Packed> skeletonize(Context &ctx, const std::vector<DeviceVolume> &v
   };
   if (as_graph) {
     const auto graph_start = std::chrono::steady_clock::now();
-    prepare_engine_launches(ctas, s);  // device queries, before the capture
+    prepare_engine_launches(prepare_ctas, ctas, s);  // device queries, before the capture
     BK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     clock.capturing(true);
     try {

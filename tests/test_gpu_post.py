@@ -104,3 +104,35 @@ def test_chunked_postprocess(gpu):
     post = dict(dust_threshold=500, tick_threshold=800)
     got = from_packed(bk.skeletonize_chunked(labels, output="packed", postprocess=post, **opts))
     assert_same_packed(got, opost.postprocess(merged, 500, 800), "chunked")
+
+
+def test_degenerate_inputs(gpu):
+    """Empty sets, empty labels, isolated vertices, self loops and duplicate edges in both
+    orientations: every step answers as the oracle does (no zero-size launch, no error)."""
+    from brook_b200 import device_post as dp
+
+    def packed(vs, es, labels):
+        voff, eoff, verts, edges, radii = [0], [0], [], [], []
+        for v, e in zip(vs, es):
+            verts += v
+            edges += e
+            radii += [2.0] * len(v)
+            voff.append(voff[-1] + len(v))
+            eoff.append(eoff[-1] + len(e))
+        return dict(labels=np.asarray(labels, np.int64), vertex_offsets=np.asarray(voff, np.int64),
+                    edge_offsets=np.asarray(eoff, np.int64), vertices=np.asarray(verts, np.float32).reshape(-1, 3),
+                    edges=np.asarray(edges, np.uint32).reshape(-1, 2), radii=np.asarray(radii, np.float32))
+
+    tri = [[0, 0, 0], [1, 0, 0], [0, 1, 0], [5, 5, 0]]
+    cases = [
+        packed([], [], []),                                                   # no labels
+        packed([[]], [[]], [4]),                                              # one empty label
+        packed([[[0, 0, 0]]], [[]], [4]),                                     # one isolated vertex
+        packed([tri, []], [[[0, 1], [1, 2], [2, 0], [0, 0]], []], [4, 9]),    # a self loop beside a cycle
+        packed([tri], [[[0, 1], [1, 0], [1, 2], [2, 1], [2, 0]]], [7]),       # duplicates, both orientations
+        packed([tri, tri], [[[0, 1]], [[2, 3]]], [1, 2]),                     # vertices on no edge
+    ]
+    for i, p in enumerate(cases):
+        for step, t in STEPS:
+            assert_same_packed(device_step(p, step, t), opost.run(p, step, t), f"case {i} {step}({t})")
+        assert_same_packed(from_packed(dp.postprocess(to_packed(p), 1, 1)), opost.postprocess(p, 1, 1), f"case {i}")
