@@ -38,7 +38,7 @@ EXPORTS = ["brook_abi_version", "brook_version", "brook_last_error", "brook_cont
            "brook_context_set_engine_share", "brook_postprocess_canonical", "brook_postprocess_step",
            "brook_skeleton_components", "brook_skeletons_create_device", "brook_connected_components_streamed",
            "brook_host_components_destroy", "brook_host_components_view", "brook_skeletonize_streamed",
-           "brook_edt_streamed"]
+           "brook_edt_streamed", "brook_pdrf_values"]
 
 
 class Volume(ctypes.Structure):
@@ -184,6 +184,8 @@ def _open():
                                                       ctypes.POINTER(vp)]),
         "brook_edt_streamed": (ctypes.c_int, [vp, ctypes.POINTER(Volume), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
                                               sz, vp, sz]),
+        "brook_pdrf_values": (ctypes.c_int, [vp, vp, vp, sz, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -12,6 +12,7 @@
 #include "../../include/brook_b200.h"
 #include "../../include/brook_b200_dlpack.h"
 #include "engine.hpp"
+#include "common.cuh"
 #include "merge.hpp"
 #include "post.hpp"
 #include "streamed.hpp"
@@ -256,6 +257,12 @@ bk::Options options_of(const brook_skeletonize_options *p) {
     o.targets_after.push_back(points(p->targets_after, p->targets_after_count));
   }
   return o;
+}
+
+__global__ void pdrf_values_kernel(const float *dbf, const float *daf, float *out, long long n, float M, float inv,
+                                   float scale, int squarings, float exponent) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = bk::pdrf_value(dbf[i], daf[i], M, inv, scale, squarings, exponent);
 }
 
 __global__ void narrow_ids(const uint32_t *ids, void *out, long long n, int bytes) {
@@ -1125,6 +1132,33 @@ brook_status brook_skeleton_components(brook_context *ctx, const brook_skeletons
       rows_tensor(*handle, 1, n);
       *out = handle.release();
     });
+  });
+}
+
+brook_status brook_pdrf_values(brook_context *ctx, const float *dbf, const float *daf, size_t n, double maximum,
+                               double max_daf, double scale, double exponent, float *out) {
+  return protect([&] {
+    require(ctx && ((dbf && daf && out) || !n));
+    std::lock_guard<std::mutex> lock(ctx->value.mutex());
+    bk::DeviceGuard guard(ctx->value.device());
+    if (!n) return;
+    // the engine's per-object constants (the reference's pdrf, trace_primitives.cu:119-129)
+    const float M = float(1.0 / std::pow(maximum, 1.01));
+    const float inv = max_daf != 0 ? float(1.0 / max_daf) : 0.0f;
+    int squarings = -1;
+    if (exponent > 0 && exponent < 65536 && std::floor(exponent) == exponent && !(int(exponent) & (int(exponent) - 1))) {
+      squarings = 0;
+      for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+    }
+    bk::Buffer<float> d_dbf(ctx->value, n), d_daf(ctx->value, n), d_out(ctx->value, n);
+    d_dbf.upload(dbf, n);
+    d_daf.upload(daf, n);
+    pdrf_values_kernel<<<bk::blocks_for((long long)n), 256, 0, ctx->value.stream()>>>(
+        d_dbf.data(), d_daf.data(), d_out.data(), (long long)n, M, inv, float(scale), squarings, float(exponent));
+    ++ctx->value.launches;
+    BK_CUDA(cudaGetLastError());
+    BK_CUDA(cudaMemcpyAsync(out, d_out.data(), n * sizeof(float), cudaMemcpyDeviceToHost, ctx->value.stream()));
+    ctx->value.synchronize();
   });
 }
 

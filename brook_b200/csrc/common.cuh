@@ -59,4 +59,22 @@ __device__ __forceinline__ float atomic_min_pos(float *addr, float value) {
 // Loads that bypass L1: state that other threads of the block update with atomics.
 template <class T> __device__ __forceinline__ T ld_cg(const T *p) { return __ldcg(p); }
 
+// The penalty of one voxel (the reference's PDRF, batched_regular.inc:93-108 and its fused
+// normalisation, trace_primitives.cu:119-129): a DBF of 0 counts as +inf and an infinite DAF as
+// 0, then (1 - dbf * M) to the power 2^squarings by repeated squaring (squarings < 0: powf with
+// `exponent`), times `scale`, plus daf * inv when inv is not 0; one rounding per operation.
+__device__ __forceinline__ float pdrf_value(float dbf, float daf, float M, float inv, float scale, int squarings,
+                                            float exponent) {
+  if (dbf == 0.0f) dbf = __int_as_float(0x7f800000);
+  float p = __fsub_rn(1.0f, __fmul_rn(dbf, M));
+  if (squarings >= 0) for (int s = 0; s < squarings; ++s) p = __fmul_rn(p, p);
+  else p = powf(p, exponent);
+  p = __fmul_rn(p, scale);
+  if (inv != 0.0f) {
+    if (isinf(daf)) daf = 0.0f;
+    p = __fadd_rn(p, __fmul_rn(daf, inv));
+  }
+  return p;
+}
+
 }  // namespace bk

@@ -379,18 +379,8 @@ __device__ void prepare_loop(const EngineArgs &a, bool big) {
     const float inv = with_daf ? __double2float_rn(__ddiv_rn(1.0, (double)farthest)) : 0.0f;
     for (int i = G::tid(); i < sh.count; i += G::threads()) {
       const int v = a.vox[sh.begin + i];
-      float dv = a.dbf[v];
-      if (dv == 0.0f) dv = inf();
-      float p = __fsub_rn(1.0f, __fmul_rn(dv, M));
-      if (a.squarings >= 0) for (int s = 0; s < a.squarings; ++s) p = __fmul_rn(p, p);
-      else p = powf(p, a.exponent);  // the reference's powf (trace_primitives.cu:119-129)
-      p = __fmul_rn(p, a.pdrf_scale);
-      if (with_daf) {
-        float dd = __ldcg(a.daf + v);
-        if (isinf(dd)) dd = 0.0f;
-        p = __fadd_rn(p, __fmul_rn(dd, inv));
-      }
-      a.pdrf[v] = p;
+      a.pdrf[v] = pdrf_value(a.dbf[v], with_daf ? __ldcg(a.daf + v) : 0.0f, M, inv, a.pdrf_scale, a.squarings,
+                             a.exponent);
     }
     G::sync();
     if (G::first()) {

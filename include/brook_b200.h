@@ -289,6 +289,14 @@ brook_status brook_postprocess_step(brook_context *context, const brook_skeleton
  * device array (one row per vertex). */
 brook_status brook_skeleton_components(brook_context *context, const brook_skeletons *input, brook_array **out);
 
+/* No counterpart in the reference's C header (the reference checks the same arithmetic through its
+ * internal brook::pdrf, cpp/tests/pdrf_fusion_smoke.cu:57-88): the penalty the engine computes for
+ * n voxels of host DBF / DAF values, with an object's DBF maximum `maximum`, its largest DAF
+ * `max_daf` (0: no DAF term), pdrf_scale and pdrf_exponent — the engine's own device arithmetic, for
+ * checks of it. */
+brook_status brook_pdrf_values(brook_context *context, const float *dbf, const float *daf, size_t n, double maximum,
+                               double max_daf, double scale, double exponent, float *out);
+
 /* No counterpart in the reference's C header (the reference sizes its cooperative grids by a timed
  * probe, cooperative.cu:18-47). The object engine's launch choices for one workload class: the
  * CTAs per thread-block cluster of the large objects (4 or 8), the voxel counts from which objects

@@ -1708,6 +1708,35 @@ void finish(Result &R) {
 // C interface for the Python test harness (ctypes).
 extern "C" {
 
+// The penalty of n voxels from their DBF and DAF values, restating the reference's normalisation
+// and PDRF arithmetic (cpp/tests/pdrf_fusion_smoke.cu:10-40, trace_primitives.cu:119-129): a DBF of
+// 0 becomes +inf and an infinite DAF 0; m = float(1 / maximum^1.01), inverse = float(1 / max_daf)
+// when max_daf is not 0; p = 1 - dbf * m, squared log2(exponent) times for a power of two below
+// 65536, else pow; times scale; plus daf * inverse when inverse is not 0. The power other than by
+// squaring is float(pow(double, double)), which CUDA's powf need not match in the last place.
+void oracle_pdrf_values(const float *dbf, const float *daf, int64_t n, double maximum, double max_daf, double scale,
+                        double exponent, float *out) {
+  const float m = float(1.0 / std::pow(maximum, 1.01));
+  const float inverse = max_daf != 0 ? float(1.0 / max_daf) : 0.0f;
+  int squarings = -1;
+  if (exponent > 0 && exponent < 65536 && std::floor(exponent) == exponent && !(int(exponent) & (int(exponent) - 1))) {
+    squarings = 0;
+    for (int e = int(exponent); e > 1; e >>= 1) ++squarings;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    float d = dbf[i], a = daf[i];
+    if (d == 0) d = std::numeric_limits<float>::infinity();
+    if (std::isinf(a)) a = 0;
+    float p = 1.0f - d * m;
+    if (squarings >= 0) for (int k = 0; k < squarings; ++k) p = p * p;
+    else p = float(std::pow(double(p), exponent));
+    p = p * float(scale);
+    if (inverse != 0) p = p + a * inverse;
+    out[i] = p;
+  }
+}
+
+
 struct oracle_params {
   double scale, constant, pdrf_scale, pdrf_exponent;
   double soma_detection, soma_acceptance, soma_scale, soma_constant;

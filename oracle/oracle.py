@@ -286,3 +286,18 @@ def target_order(mask, daf):
     out = np.zeros(mask.size, np.int64)
     n = lib().oracle_target_order(mask.ctypes.data, daf.ctypes.data, mask.size, out.ctypes.data)
     return out[:n]
+
+
+def pdrf_values(dbf, daf, maximum, max_daf, scale, exponent):
+    """The reference's PDRF arithmetic on arrays of DBF / DAF values (oracle_pdrf_values)."""
+    l = lib()
+    if not getattr(l, "_pdrf_ready", False):
+        l.oracle_pdrf_values.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+        l._pdrf_ready = True
+    dbf = np.ascontiguousarray(dbf, np.float32)
+    daf = np.ascontiguousarray(daf, np.float32)
+    out = np.empty_like(dbf)
+    l.oracle_pdrf_values(dbf.ctypes.data, daf.ctypes.data, dbf.size, float(maximum), float(max_daf), float(scale),
+                         float(exponent), out.ctypes.data)
+    return out
