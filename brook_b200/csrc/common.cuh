@@ -12,9 +12,13 @@ namespace bk {
 // common.cuh:33-47 of giorgioangel/brook): faces (-x,+x,-y,+y,-z,+z); the xy, yz and xz edges,
 // each sign pair in lexicographic order; the corners lexicographic with z fastest.
 // Bit k of a voxel's neighbour mask is neighbour k.
-__constant__ int8_t c_dx[26] = {-1, 1, 0, 0, 0, 0, -1, -1, 1, 1, 0, 0, 0, 0, -1, -1, 1, 1, -1, -1, -1, -1, 1, 1, 1, 1};
-__constant__ int8_t c_dy[26] = {0, 0, -1, 1, 0, 0, -1, 1, -1, 1, -1, -1, 1, 1, 0, 0, 0, 0, -1, -1, 1, 1, -1, -1, 1, 1};
-__constant__ int8_t c_dz[26] = {0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1};
+// (The lists as macros too, for kernels that want them as compile-time constants.)
+#define BK_NEIGHBOUR_DX -1, 1, 0, 0, 0, 0, -1, -1, 1, 1, 0, 0, 0, 0, -1, -1, 1, 1, -1, -1, -1, -1, 1, 1, 1, 1
+#define BK_NEIGHBOUR_DY 0, 0, -1, 1, 0, 0, -1, 1, -1, 1, -1, -1, 1, 1, 0, 0, 0, 0, -1, -1, 1, 1, -1, -1, 1, 1
+#define BK_NEIGHBOUR_DZ 0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1
+__constant__ int8_t c_dx[26] = {BK_NEIGHBOUR_DX};
+__constant__ int8_t c_dy[26] = {BK_NEIGHBOUR_DY};
+__constant__ int8_t c_dz[26] = {BK_NEIGHBOUR_DZ};
 // neighbour k -> the index of the opposite offset
 __constant__ int8_t c_opp[26] = {1, 0, 3, 2, 5, 4, 9, 8, 7, 6, 13, 12, 11, 10, 17, 16, 15, 14, 25, 24, 23, 22, 21, 20, 19, 18};
 // dijkstra3d's neighbour order (its railroad joins the first rail in this order): the same faces

@@ -100,38 +100,93 @@ __global__ void __launch_bounds__(256) analyze_kernel(const uint32_t *__restrict
   }
 }
 
-// The mask of a 32x8x8 block of voxels from a shared-memory copy of the block's ids with a
-// one-voxel halo (outside the volume: 0, which no voxel's id equals); block (32, 8) threads, grid
-// (x blocks, y blocks, z blocks).
-constexpr int kMaskX = 32, kMaskY = 8, kMaskZ = 8;
+// The mask of a column of 32x8 voxels and kMaskZ planes. The block streams the column's halo
+// planes (34x10 ids each, 0 outside the volume, which no voxel's id equals) through a ring of
+// kRing shared-memory planes with asynchronous copies (cp.async, zero-filled outside), kRing - 2
+// planes ahead of the plane it computes; each thread holds the 3x3 neighbourhoods of three planes
+// in registers, so a voxel costs nine shared loads (of the plane ahead) and 26 register compares.
+// Vec: rows of a multiple of four ids at a 16-byte aligned base, copied in 16-byte pieces from
+// x0 - 4 (ten per row); otherwise one 4-byte copy per id. Block (32, 8) threads, grid (x blocks,
+// y blocks, z blocks).
+constexpr int kMaskX = 32, kMaskY = 8, kMaskZ = 32, kRing = 8;
+constexpr int kRowWords = kMaskX + 8, kPlaneWords = kRowWords * (kMaskY + 2);  // a row holds x0 - 4 .. x0 + 35
 
-__global__ void __launch_bounds__(kMaskX * kMaskY) mask_kernel(const uint32_t *__restrict__ ids, Dims d,
-                                                              uint32_t *__restrict__ mask) {
-  constexpr int HX = kMaskX + 2, HY = kMaskY + 2, HZ = kMaskZ + 2;
-  __shared__ uint32_t s[HZ * HY * HX];
-  const int x0 = blockIdx.x * kMaskX, y0 = blockIdx.y * kMaskY, z0 = blockIdx.z * kMaskZ;
-  for (int q = threadIdx.x + kMaskX * threadIdx.y; q < HX * HY * HZ; q += kMaskX * kMaskY) {
-    const int hx = q % HX, hy = (q / HX) % HY, hz = q / (HX * HY);
-    const int x = x0 + hx - 1, y = y0 + hy - 1, z = z0 + hz - 1;
-    uint32_t v = 0;
-    if (x >= 0 && y >= 0 && z >= 0 && x < d.sx && y < d.sy && z < d.sz)
-      v = ids[x + (long long)d.sx * (y + (long long)d.sy * z)];
-    s[q] = v;
+__device__ __forceinline__ void copy_async(uint32_t *dst, const uint32_t *src, int bytes, bool in) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(in ? 16 : 0) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(in ? 4 : 0) : "memory");
+}
+
+template <bool Vec>
+__device__ __forceinline__ void mask_plane_copy(uint32_t *slot, const uint32_t *__restrict__ ids, const Dims &d,
+                                                int x0, int y0, int z) {
+  const int t = threadIdx.x + kMaskX * threadIdx.y;
+  const bool zin = z >= 0 && z < d.sz;
+  if (Vec) {
+    if (t >= 10 * (kMaskY + 2)) return;
+    const int row = t / 10, x = x0 - 4 + 4 * (t % 10), y = y0 + row - 1;
+    const bool in = zin && y >= 0 && y < d.sy && x >= 0 && x < d.sx;
+    const uint32_t *src = in ? ids + (x + (long long)d.sx * (y + (long long)d.sy * z)) : ids;
+    copy_async(slot + row * kRowWords + 4 * (t % 10), src, 16, in);
+  } else {
+    for (int q = t; q < (kMaskX + 2) * (kMaskY + 2); q += kMaskX * kMaskY) {
+      const int row = q / (kMaskX + 2), c = q % (kMaskX + 2), x = x0 - 1 + c, y = y0 + row - 1;
+      const bool in = zin && y >= 0 && y < d.sy && x >= 0 && x < d.sx;
+      const uint32_t *src = in ? ids + (x + (long long)d.sx * (y + (long long)d.sy * z)) : ids;
+      copy_async(slot + row * kRowWords + 3 + c, src, 4, in);
+    }
   }
+}
+
+template <bool Vec>
+__global__ void __launch_bounds__(kMaskX * kMaskY, 4) mask_kernel(const uint32_t *__restrict__ ids, Dims d,
+                                                                 uint32_t *__restrict__ mask) {
+  constexpr int8_t DX[26] = {BK_NEIGHBOUR_DX}, DY[26] = {BK_NEIGHBOUR_DY}, DZ[26] = {BK_NEIGHBOUR_DZ};
+  __shared__ __align__(16) uint32_t ring[kRing * kPlaneWords];
+  const int x0 = blockIdx.x * kMaskX, y0 = blockIdx.y * kMaskY, z0 = blockIdx.z * kMaskZ;
+  const int planes = min(kMaskZ, d.sz - z0) + 2;  // halo planes hz = 0 .. planes - 1 are z0 - 1 + hz
+  // halo plane hz lives in slot hz % kRing; one commit group per plane index, empty past the end
+  auto issue = [&](int hz) {
+    if (hz < planes) mask_plane_copy<Vec>(ring + (hz % kRing) * kPlaneWords, ids, d, x0, y0, z0 - 1 + hz);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+#pragma unroll
+  for (int hz = 0; hz < kRing; ++hz) issue(hz);
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 2) : "memory");  // planes 0 and 1
   __syncthreads();
-  const int lx = threadIdx.x, ly = threadIdx.y, x = x0 + lx, y = y0 + ly;
-  if (x >= d.sx || y >= d.sy) return;
-  for (int lz = 0; lz < kMaskZ && z0 + lz < d.sz; ++lz) {
-    const int c = (lx + 1) + HX * ((ly + 1) + HY * (lz + 1));
-    const uint32_t id = s[c];
+  const int lane = threadIdx.x, x = x0 + lane, y = y0 + threadIdx.y;
+  const int col = 3 + lane + kRowWords * threadIdx.y;  // the (-1, -1) corner of this column's 3x3
+  uint32_t w[3][9];                                    // planes z - 1, z, z + 1; index (dy + 1) * 3 + dx + 1
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int j = 0; j < 9; ++j) w[p][j] = ring[p * kPlaneWords + col + j % 3 + kRowWords * (j / 3)];
+  const bool mine = x < d.sx && y < d.sy;
+  for (int lz = 0; lz + 2 < planes; ++lz) {  // block-uniform trip count
+    // groups issued: planes 0 .. lz + kRing - 1; plane lz + 2 must have landed
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 3) : "memory");
+    __syncthreads();  // every copy of plane lz + 2 landed; plane lz (read two steps ago) is free
+    issue(lz + kRing);
+    const uint32_t *next = ring + ((lz + 2) % kRing) * kPlaneWords + col;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) w[2][j] = next[j % 3 + kRowWords * (j / 3)];
+    const uint32_t id = w[1][4];
     uint32_t m = 0;
     if (id) {
 #pragma unroll
       for (int k = 0; k < 26; ++k)
-        if (s[c + c_dx[k] + HX * (c_dy[k] + HY * c_dz[k])] == id) m |= 1u << k;
+        if (w[1 + DZ[k]][(DY[k] + 1) * 3 + DX[k] + 1] == id) m |= 1u << k;
     }
-    mask[x + (long long)d.sx * (y + (long long)d.sy * (z0 + lz))] = m;
+    if (mine) mask[x + (long long)d.sx * (y + (long long)d.sy * (z0 + lz))] = m;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      w[0][j] = w[1][j];
+      w[1][j] = w[2][j];
+    }
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Per id the largest finite field value (as float bits), by the same block tables as analyze:
@@ -165,6 +220,162 @@ __global__ void __launch_bounds__(256) segmax_kernel(const float *__restrict__ f
     const uint32_t id = keys[t];
     if (id && __ldcg(best + id) < top[t]) atomicMax(best + id, top[t]);
   }
+}
+
+// The same maxima four voxels to a thread, for 16-byte aligned fields and ids: one 16-byte load
+// of each, then the thread merges its own runs of one id (a run's maximum, kept where the run
+// starts) and the warp meets once per run position that some lane starts a run at. Inside rows
+// the four voxels mostly share one id, so a warp of 128 voxels needs one match round where the
+// scalar kernel needs four. Runs of id 0 or of maximum 0 change nothing and are skipped.
+constexpr int kQuadChunk = 4096;
+
+__global__ void __launch_bounds__(256) segmax4_kernel(const float *__restrict__ f, const uint32_t *__restrict__ ids,
+                                                      long long n, unsigned *best) {
+  __shared__ uint32_t keys[kSlots];
+  __shared__ unsigned top[kSlots];
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) { keys[t] = 0; top[t] = 0; }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long begin = (long long)blockIdx.x * kQuadChunk;
+#pragma unroll
+  for (int it = 0; it < kQuadChunk / (4 * 256); ++it) {  // the same trip count on every lane
+    const long long i = begin + 4LL * (it * 256 + threadIdx.x);
+    uint32_t id[4];
+    float v[4];
+    if (i + 3 < n) {
+      const uint4 q = *reinterpret_cast<const uint4 *>(ids + i);
+      const float4 x = *reinterpret_cast<const float4 *>(f + i);
+      id[0] = q.x; id[1] = q.y; id[2] = q.z; id[3] = q.w;
+      v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        id[k] = i + k < n ? ids[i + k] : 0u;
+        v[k] = i + k < n ? f[i + k] : 0.0f;
+      }
+    }
+    unsigned run[4];  // run[k]: the maximum of the run of id[k] from voxel k to the thread's last
+#pragma unroll
+    for (int k = 3; k >= 0; --k) {
+      const unsigned bits = (id[k] != 0 && v[k] < __uint_as_float(BK_INF_BITS)) ? __float_as_uint(v[k]) : 0u;
+      run[k] = (k < 3 && id[k] == id[k + 1]) ? max(bits, run[k + 1]) : bits;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const bool has = (k == 0 || id[k] != id[k - 1]) && id[k] != 0 && run[k] != 0;
+      if (!__any_sync(0xFFFFFFFFu, has)) continue;  // warp-uniform
+      const uint32_t key = has ? id[k] : 0u;
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+      const unsigned m = __reduce_max_sync(peers, has ? run[k] : 0u);
+      if (!has || lane != __ffs(peers) - 1) continue;
+      const int slot = table_slot(keys, key);
+      if (slot < 0) {
+        if (__ldcg(best + key) < m) atomicMax(best + key, m);
+      } else {
+        atomicMax(top + slot, m);
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) {
+    const uint32_t id = keys[t];
+    if (id && __ldcg(best + id) < top[t]) atomicMax(best + id, top[t]);
+  }
+}
+
+// Boxes and counts four voxels to a thread, for 16-byte aligned ids in rows of a multiple of four
+// voxels (so a thread's four voxels share y and z): the thread's runs of one id (start x, length)
+// meet the warp's once per run position that some lane starts a run at, as in segmax4_kernel. When
+// the warp's 128 voxels lie in one row, y and z are the row's and only x is reduced.
+__global__ void __launch_bounds__(256) analyze4_kernel(const uint32_t *__restrict__ ids, Dims d, int *lo, int *hi,
+                                                       unsigned long long *counts) {
+  __shared__ uint32_t keys[kSlots];
+  __shared__ unsigned cnt[kSlots];
+  __shared__ int slo[kSlots][3], shi[kSlots][3];
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) {
+    keys[t] = 0;
+    cnt[t] = 0;
+    for (int a = 0; a < 3; ++a) { slo[t][a] = INT32_MAX; shi[t][a] = -1; }
+  }
+  __syncthreads();
+  const long long n = d.n(), begin = (long long)blockIdx.x * kQuadChunk;
+  const int lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int it = 0; it < kQuadChunk / (4 * 256); ++it) {  // the same trip count on every lane
+    const long long i = begin + 4LL * (it * 256 + threadIdx.x);
+    uint32_t id[4];
+    if (i + 3 < n) {
+      const uint4 q = *reinterpret_cast<const uint4 *>(ids + i);
+      id[0] = q.x; id[1] = q.y; id[2] = q.z; id[3] = q.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) id[k] = i + k < n ? ids[i + k] : 0u;
+    }
+    int x = 0, y = 0, z = 0;
+    if (i < n) unravel((int)i, d, x, y, z);
+    const int x0 = __shfl_sync(0xFFFFFFFFu, x, 0);
+    const bool one_row = x0 + 127 < d.sx && i - 4 * lane + 127 < n;  // warp-uniform
+    unsigned len[4];  // len[k]: the length of the run of id[k] from voxel k to the thread's last
+#pragma unroll
+    for (int k = 3; k >= 0; --k) len[k] = (k < 3 && id[k] == id[k + 1]) ? len[k + 1] + 1 : 1u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const bool has = (k == 0 || id[k] != id[k - 1]) && id[k] != 0;
+      if (!__any_sync(0xFFFFFFFFu, has)) continue;  // warp-uniform
+      const uint32_t key = has ? id[k] : 0u;
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+      const unsigned total = __reduce_add_sync(peers, has ? len[k] : 0u);
+      int l3[3], h3[3];
+      l3[0] = int(__reduce_min_sync(peers, unsigned(x + k)));
+      h3[0] = int(__reduce_max_sync(peers, unsigned(x + k + int(len[k]) - 1)));
+      if (one_row) {
+        l3[1] = h3[1] = y;
+        l3[2] = h3[2] = z;
+      } else {
+        l3[1] = int(__reduce_min_sync(peers, unsigned(y)));
+        h3[1] = int(__reduce_max_sync(peers, unsigned(y)));
+        l3[2] = int(__reduce_min_sync(peers, unsigned(z)));
+        h3[2] = int(__reduce_max_sync(peers, unsigned(z)));
+      }
+      if (!has || lane != __ffs(peers) - 1) continue;
+      const int slot = table_slot(keys, key);
+      if (slot < 0) {
+        box_update(lo + 3 * (long long)key, hi + 3 * (long long)key, counts + key, l3, h3, total);
+        continue;
+      }
+      atomicAdd(cnt + slot, total);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        atomicMin(&slo[slot][a], l3[a]);
+        atomicMax(&shi[slot][a], h3[a]);
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kSlots; t += blockDim.x) {
+    const uint32_t id = keys[t];
+    if (id) box_update(lo + 3 * (long long)id, hi + 3 * (long long)id, counts + id, slo[t], shi[t], cnt[t]);
+  }
+}
+
+void launch_analyze(Context &ctx, const uint32_t *ids, Dims d, int *lo, int *hi, unsigned long long *counts) {
+  if (d.n() <= 0) return;
+  if (reinterpret_cast<uintptr_t>(ids) % 16 == 0 && d.sx % 4 == 0) {
+    analyze4_kernel<<<blocks_for(d.n(), kQuadChunk), 256, 0, ctx.stream()>>>(ids, d, lo, hi, counts);
+  } else {
+    analyze_kernel<<<blocks_for(d.n(), kChunk), 256, 0, ctx.stream()>>>(ids, d, lo, hi, counts);
+  }
+  ++ctx.launches;
+}
+
+void launch_segmax(Context &ctx, const float *field, const uint32_t *ids, long long n, unsigned *best) {
+  if (n <= 0) return;
+  if (reinterpret_cast<uintptr_t>(field) % 16 == 0 && reinterpret_cast<uintptr_t>(ids) % 16 == 0) {
+    segmax4_kernel<<<blocks_for(n, kQuadChunk), 256, 0, ctx.stream()>>>(field, ids, n, best);
+  } else {
+    segmax_kernel<<<blocks_for(n, kChunk), 256, 0, ctx.stream()>>>(field, ids, n, best);
+  }
+  ++ctx.launches;
 }
 
 __global__ void zero_to_inf_kernel(const uint32_t *__restrict__ ids, float *__restrict__ f, long long n,
@@ -262,7 +473,7 @@ std::vector<Box> analyze(Context &ctx, const uint32_t *ids, VolumeDims vd, int64
   Buffer<int> dlo = to_device(ctx, lo), dhi = to_device(ctx, hi);
   Buffer<unsigned long long> counts(ctx, count + 1);
   counts.zero();
-  analyze_kernel<<<blocks_for(vd.n(), kChunk), 256, 0, ctx.stream()>>>(ids, d, dlo.data(), dhi.data(), counts.data()); ++ctx.launches;
+  launch_analyze(ctx, ids, d, dlo.data(), dhi.data(), counts.data());
   BK_CUDA(cudaGetLastError());
   lo = dlo.download();
   hi = dhi.download();
@@ -279,7 +490,12 @@ void neighbour_mask(Context &ctx, const uint32_t *ids, VolumeDims vd, uint32_t *
   if (vd.n() <= 0) return;
   const dim3 grid((vd.sx + kMaskX - 1) / kMaskX, (vd.sy + kMaskY - 1) / kMaskY, (vd.sz + kMaskZ - 1) / kMaskZ);
   if (grid.y > 65535 || grid.z > 65535) throw std::invalid_argument("volume too large for the neighbour mask");
-  mask_kernel<<<grid, dim3(kMaskX, kMaskY), 0, ctx.stream()>>>(ids, Dims{vd.sx, vd.sy, vd.sz}, out); ++ctx.launches;
+  const Dims d{vd.sx, vd.sy, vd.sz};
+  if (reinterpret_cast<uintptr_t>(ids) % 16 == 0 && vd.sx % 4 == 0)
+    mask_kernel<true><<<grid, dim3(kMaskX, kMaskY), 0, ctx.stream()>>>(ids, d, out);
+  else
+    mask_kernel<false><<<grid, dim3(kMaskX, kMaskY), 0, ctx.stream()>>>(ids, d, out);
+  ++ctx.launches;
   BK_CUDA(cudaGetLastError());
 }
 
@@ -296,9 +512,8 @@ std::vector<std::vector<Box>> analyze(Context &ctx, const uint32_t *ids, const s
   for (size_t v = 0; v < volumes.size(); ++v) {
     const auto &iv = volumes[v];
     if (!iv.d.n() || !iv.count) continue;
-    analyze_kernel<<<blocks_for(iv.d.n(), kChunk), 256, 0, s>>>(ids + iv.offset, Dims{iv.d.sx, iv.d.sy, iv.d.sz},
-                                                        dlo.data() + 3 * base[v], dhi.data() + 3 * base[v],
-                                                        counts.data() + base[v]); ++ctx.launches;
+    launch_analyze(ctx, ids + iv.offset, Dims{iv.d.sx, iv.d.sy, iv.d.sz}, dlo.data() + 3 * base[v],
+                   dhi.data() + 3 * base[v], counts.data() + base[v]);
   }
   BK_CUDA(cudaGetLastError());
   std::vector<int> lo(3 * total), hi(3 * total);
@@ -328,8 +543,7 @@ std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, co
   for (size_t v = 0; v < volumes.size(); ++v) {
     const auto &iv = volumes[v];
     if (!iv.d.n() || !iv.count) continue;
-    segmax_kernel<<<blocks_for(iv.d.n(), kChunk), 256, 0, ctx.stream()>>>(field + iv.offset, ids + iv.offset, iv.d.n(),
-                                                                  best.data() + base[v]); ++ctx.launches;
+    launch_segmax(ctx, field + iv.offset, ids + iv.offset, iv.d.n(), best.data() + base[v]);
   }
   BK_CUDA(cudaGetLastError());
   auto bits = best.download();
@@ -344,7 +558,7 @@ std::vector<std::vector<float>> segment_max(Context &ctx, const float *field, co
 std::vector<float> segment_max(Context &ctx, const float *field, const uint32_t *ids, long long n, int64_t count) {
   Buffer<unsigned> best(ctx, count + 1);
   best.zero();
-  segmax_kernel<<<blocks_for(n, kChunk), 256, 0, ctx.stream()>>>(field, ids, n, best.data()); ++ctx.launches;
+  launch_segmax(ctx, field, ids, n, best.data());
   BK_CUDA(cudaGetLastError());
   auto bits = best.download();
   std::vector<float> out(count + 1);
