@@ -40,7 +40,7 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        newest = max(os.path.getmtime(os.path.join(_HERE, f)) for f in ("oracle.cpp", "post.cpp"))
+        newest = max(os.path.getmtime(os.path.join(_HERE, f)) for f in ("oracle.cpp", "post.cpp", "graph.cpp"))
         if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < newest:
             build()
         _lib = ctypes.CDLL(_LIB_PATH)
