@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(256) analyze_kernel(const uint32_t *__restrict
 
 // The mask of a column of 32x8 voxels and kMaskZ planes. The block streams the column's halo
 // planes (34x10 ids each, 0 outside the volume, which no voxel's id equals) through a ring of
-// kRing shared-memory planes with asynchronous copies (cp.async, zero-filled outside), kRing - 2
-// planes ahead of the plane it computes; each thread holds the 3x3 neighbourhoods of three planes
+// kRing shared-memory planes with asynchronous copies (cp.async, zero-filled outside), up to
+// kRing - 2 planes ahead of the plane it reads; each thread holds the 3x3 neighbourhoods of three planes
 // in registers, so a voxel costs nine shared loads (of the plane ahead) and 26 register compares.
 // Vec: rows of a multiple of four ids at a 16-byte aligned base, copied in 16-byte pieces from
 // x0 - 4 (ten per row); otherwise one 4-byte copy per id. Block (32, 8) threads, grid (x blocks,
