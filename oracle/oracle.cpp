@@ -57,6 +57,7 @@ constexpr float kInf = std::numeric_limits<float>::infinity();
 // those rules.
 struct Tables {
   int dx[26], dy[26], dz[26], opp[26], d3rank[26], d3inv[26];
+  int bit[26];  // the voxel-graph bit (cc3d's order) that permits step k (common.cuh:48-55)
   Tables() {
     int k = 0;
     auto put = [&](int x, int y, int z) { dx[k] = x; dy[k] = y; dz[k] = z; ++k; };
@@ -74,6 +75,15 @@ struct Tables {
     for (int r = 0; r < 8; ++r)
       for (int j = 18; j < 26; ++j)
         if (dx[j] == corners[r][0] && dy[j] == corners[r][1] && dz[j] == corners[r][2]) { d3inv[18 + r] = j; d3rank[j] = 18 + r; }
+    // cc3d's bit order: faces +x -x +y -y +z -z, the xy edges, the xz and yz edges with +z, then
+    // with -z, the corners with +z, then with -z, x fastest and + before - within each group
+    const int cc3d[26][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1},
+                             {1,1,0},{-1,1,0},{1,-1,0},{-1,-1,0},{1,0,1},{-1,0,1},{0,1,1},{0,-1,1},
+                             {1,0,-1},{-1,0,-1},{0,1,-1},{0,-1,-1},
+                             {1,1,1},{-1,1,1},{1,-1,1},{-1,-1,1},{1,1,-1},{-1,1,-1},{1,-1,-1},{-1,-1,-1}};
+    for (int i = 0; i < 26; ++i)
+      for (int b = 0; b < 26; ++b)
+        if (dx[i] == cc3d[b][0] && dy[i] == cc3d[b][1] && dz[i] == cc3d[b][2]) bit[i] = b;
   }
 };
 const Tables T;
@@ -508,7 +518,14 @@ struct Volume {
   std::vector<float> dbf, pdrf, dist;
   std::vector<uint8_t> alive, inq;
   std::vector<uint64_t> key;
+  const uint32_t *graph = nullptr;  // a voxel graph (cc3d bits per voxel), or none
 };
+
+// Voxel-graph gates (common.cuh:85-100): the step from u along k is permitted by graph[u]'s bit
+// for k (push); the step into v from its neighbour u = v + N[k] is the step u -> v, permitted by
+// graph[u]'s bit for the opposite offset (pull). Without a graph every step is permitted.
+bool push_ok(const Volume &V, i64 u, int k) { return !V.graph || ((V.graph[u] >> T.bit[k]) & 1u); }
+bool pull_ok(const Volume &V, i64 u, int k) { return push_ok(V, u, T.opp[k]); }
 
 constexpr uint64_t kUnclaimed = ~uint64_t{0};
 
@@ -538,7 +555,7 @@ std::vector<i64> railroad(Volume &V, uint32_t label, i64 target, std::vector<i64
       const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
       if (!s.inside(nx, ny, nz)) continue;
       const i64 v = s.idx(nx, ny, nz);
-      if (ids[v] != label) continue;
+      if (ids[v] != label || !push_ok(V, u, k)) continue;
       const float cand = vw_step(d, V.pdrf[v]);
       if (cand < V.dist[v]) {
         if (V.dist[v] == kInf) touched.push_back(v);
@@ -563,19 +580,20 @@ std::vector<i64> railroad(Volume &V, uint32_t label, i64 target, std::vector<i64
           const i64 nx = x + T.dx[k], ny = y + T.dy[k], nz = z + T.dz[k];
           if (!s.inside(nx, ny, nz)) continue;
           const i64 u = s.idx(nx, ny, nz);
-          if (ids[u] != label || V.pdrf[u] == 0.0f) continue;
+          if (ids[u] != label || V.pdrf[u] == 0.0f || !pull_ok(V, u, k)) continue;
           const uint32_t db = fbits(V.dist[u]);
           if (db < mb) { mb = db; kb = k; }
         }
       }
       if (step == 0 && kb >= 0) {  // the join: u's first rail in dijkstra3d order
         const i64 ux = x + T.dx[kb], uy = y + T.dy[kb], uz = z + T.dz[kb];
+        const i64 road = s.idx(ux, uy, uz);
         for (int r = 0; r < 26; ++r) {
           const int k = T.d3inv[r];
           const i64 nx = ux + T.dx[k], ny = uy + T.dy[k], nz = uz + T.dz[k];
           if (!s.inside(nx, ny, nz)) continue;
           const i64 v = s.idx(nx, ny, nz);
-          if (ids[v] != label || V.pdrf[v] != 0.0f) continue;
+          if (ids[v] != label || V.pdrf[v] != 0.0f || !push_ok(V, road, k)) continue;
           x = nx; y = ny; z = nz; cur = v; kb = T.opp[k];
           break;
         }
@@ -1879,9 +1897,19 @@ int oracle_edt(const uint32_t *labels, int64_t sx, int64_t sy, int64_t sz, const
   } catch (...) { return 1; }
 }
 // Railroad on a raw penalty field of one component (all voxels of `labels` equal to 1 belong to it).
+int64_t oracle_railroad_graph(const float *field, const uint32_t *labels, const uint32_t *graph, int64_t sx,
+                              int64_t sy, int64_t sz, int64_t target, int64_t *out, int64_t capacity);
 int64_t oracle_railroad(const float *field, const uint32_t *labels, int64_t sx, int64_t sy, int64_t sz,
                         int64_t target, int64_t *out, int64_t capacity) {
+  return oracle_railroad_graph(field, labels, nullptr, sx, sy, sz, target, out, capacity);
+}
+// The same with a voxel graph (cc3d bits per voxel, or null): relaxations and the join step only
+// where the graph permits, the walk back only over permitted steps (lockstep_regular.inc:108, 123;
+// lockstep_coop.inc:153-245).
+int64_t oracle_railroad_graph(const float *field, const uint32_t *labels, const uint32_t *graph, int64_t sx,
+                              int64_t sy, int64_t sz, int64_t target, int64_t *out, int64_t capacity) {
   Volume V; V.s = Shape{sx, sy, sz};
+  V.graph = graph;
   std::vector<uint32_t> ids(labels, labels + V.s.n());
   V.ids = &ids;
   V.pdrf.assign(field, field + V.s.n());

@@ -56,6 +56,10 @@ def lib():
         _lib.oracle_borders.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]
         _lib.oracle_edt.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        _lib.oracle_railroad_graph.restype = ctypes.c_int64
+        _lib.oracle_railroad_graph.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                               ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                               ctypes.c_int64]
         _lib.oracle_railroad.restype = ctypes.c_int64
         _lib.oracle_railroad.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                          ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]
@@ -254,11 +258,17 @@ def edt(labels, anisotropy=(1, 1, 1), black_border=False, dims=3):
     return out
 
 
-def railroad(field, target, component=None):
+def railroad(field, target, component=None, voxel_graph=None):
+    """The railroad path (target first) over `component` (default: every voxel); `voxel_graph`:
+    cc3d bits per voxel that gate every step (oracle_railroad_graph)."""
     field = np.asfortranarray(np.asarray(field, np.float32))
     comp = np.ones(field.shape, np.uint32, order="F") if component is None else np.asfortranarray(component.astype(np.uint32))
     out = np.zeros(field.size, np.int64)
-    n = lib().oracle_railroad(field.ctypes.data, comp.ctypes.data, *field.shape, int(target), out.ctypes.data, out.size)
+    graph = None if voxel_graph is None else np.asfortranarray(np.asarray(voxel_graph, np.uint32))
+    if graph is not None and graph.shape != field.shape:
+        raise ValueError("voxel_graph must match the field")
+    n = lib().oracle_railroad_graph(field.ctypes.data, comp.ctypes.data, None if graph is None else graph.ctypes.data,
+                                    *field.shape, int(target), out.ctypes.data, out.size)
     return out[:n].tolist()
 
 

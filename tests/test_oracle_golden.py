@@ -57,6 +57,29 @@ def test_railroad_join_order():
         assert oracle.railroad(field, _flat(centre, shape)) == [_flat(centre, shape), _flat(near[rails[0]], shape)], rails
 
 
+def test_railroad_join_order_with_voxel_graph():
+    """test_package.py:802-808: for every pair of rails, the first one's direction cut from the
+    voxel graph at the target: the path joins the second (dijkstra3d 1.15.2's answers)."""
+    from oracle import graph as og
+
+    shape, centre = (5, 5, 5), (2, 2, 2)
+    near = [tuple(c + d for c, d in zip(centre, o)) for o in D3_ORDER]
+    for rails in itertools.combinations(range(26), 2):
+        field = np.ones(shape, np.float32, order="F")
+        for i in rails:
+            field[near[i]] = 0
+        graph = np.full(shape, (1 << 26) - 1, np.uint32, order="F")
+        graph[centre] &= ~np.uint32(1 << og.STEPS.index(D3_ORDER[rails[0]]))
+        path = oracle.railroad(field, _flat(centre, shape), voxel_graph=graph)
+        assert path == [_flat(centre, shape), _flat(near[rails[1]], shape)], rails
+    # an all-permitting graph changes nothing; a graph that permits no step leaves no path
+    field = np.ones(shape, np.float32, order="F")
+    field[near[5]] = 0
+    assert oracle.railroad(field, _flat(centre, shape), voxel_graph=np.full(shape, (1 << 26) - 1, np.uint32)) == \
+        oracle.railroad(field, _flat(centre, shape))
+    assert oracle.railroad(field, _flat(centre, shape), voxel_graph=np.zeros(shape, np.uint32)) == []
+
+
 def test_edt_line():
     """c_smoke.c:45-61: EDT of an 8-voxel line {1,1,0,0,0,0,2,2}, anisotropy 1, no black border."""
     labels = np.array([1, 1, 0, 0, 0, 0, 2, 2], np.uint32).reshape(8, 1, 1)
